@@ -1,0 +1,214 @@
+/* z4c_b200: B200-native Z4c spacetime evolution, C ABI.
+ *
+ * This is the drop-in boundary for the GR-Athena++ Z4c hot path.  Each entry
+ * point replaces one member function of the reference `Z4c` class
+ * (src/z4c/z4c.hpp:448-539) or one GR_Z4c task (src/task_list/gr/
+ * task_list_gr_z4c.cpp); the reference symbol is cited beside it.  All state
+ * lives in device memory owned by a context; host pointers are borrowed for
+ * the duration of a call only.  No C++ types, no torch types, no exceptions
+ * cross this boundary: every call returns Z4C_OK (0) or a negative Z4C_E*
+ * code, and z4c_last_error() returns a message for the last failure.
+ *
+ * Data layout, host and device: one MeshBlock register is the reference's
+ * AthenaArray layout [var][k][j][i] (src/athena_arrays.hpp:192-195), i fastest,
+ * vertex-centred with nn = nx + 1 + 2*Z4C_NG points per axis; a register over
+ * the whole mesh is [block][var][k][j][i] with blocks in the order
+ * l0 + nb0*(l1 + nb1*l2) of their logical location.
+ *
+ * Threading: one context per host thread and CUDA stream; calls on one
+ * context must be serialised by the caller.
+ */
+#ifndef Z4C_B200_H
+#define Z4C_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define Z4C_NG 4           /* ghost vertices per side (reference NGHOST=4)  */
+#define Z4C_NVAR 22        /* evolved variables (z4c.hpp:63-88)             */
+#define Z4C_NADM 17        /* ADM variables (z4c.hpp:100-118)               */
+#define Z4C_NCON 7         /* constraint variables (z4c.hpp:128-137)        */
+
+/* Evolved-variable indices, z4c.hpp:63-88. */
+enum {
+  Z4C_CHI = 0, Z4C_GXX, Z4C_GXY, Z4C_GXZ, Z4C_GYY, Z4C_GYZ, Z4C_GZZ,
+  Z4C_KHAT, Z4C_AXX, Z4C_AXY, Z4C_AXZ, Z4C_AYY, Z4C_AYZ, Z4C_AZZ,
+  Z4C_GAMX, Z4C_GAMY, Z4C_GAMZ, Z4C_THETA, Z4C_ALPHA,
+  Z4C_BETAX, Z4C_BETAY, Z4C_BETAZ
+};
+/* ADM-variable indices, z4c.hpp:100-118. */
+enum {
+  Z4C_ADM_ALPHA = 0, Z4C_ADM_BETAX, Z4C_ADM_BETAY, Z4C_ADM_BETAZ,
+  Z4C_ADM_GXX, Z4C_ADM_GXY, Z4C_ADM_GXZ, Z4C_ADM_GYY, Z4C_ADM_GYZ, Z4C_ADM_GZZ,
+  Z4C_ADM_KXX, Z4C_ADM_KXY, Z4C_ADM_KXZ, Z4C_ADM_KYY, Z4C_ADM_KYZ, Z4C_ADM_KZZ,
+  Z4C_ADM_PSI4
+};
+/* Constraint indices, z4c.hpp:128-137. */
+enum {
+  Z4C_CON_C = 0, Z4C_CON_H, Z4C_CON_M, Z4C_CON_Z, Z4C_CON_MX, Z4C_CON_MY,
+  Z4C_CON_MZ
+};
+
+/* Return codes. */
+#define Z4C_OK 0
+#define Z4C_EINVAL (-1)     /* bad argument                                */
+#define Z4C_ENOMEM (-2)     /* device or host allocation failed            */
+#define Z4C_ECUDA (-3)      /* a CUDA call failed                          */
+#define Z4C_ENONFINITE (-4) /* a NaN/Inf was detected in the state         */
+#define Z4C_ETIMEOUT (-5)   /* a bounded device wait gave up               */
+#define Z4C_ESTATE (-6)     /* call not valid in the context's state       */
+#define Z4C_ENODEV (-7)     /* no usable CUDA device                       */
+
+/* Physical boundary flags per face (inner_x1, outer_x1, inner_x2, ...). */
+#define Z4C_BC_PERIODIC 0
+/* extrapolate_outflow; gr_sommerfeld maps to the same ghost fill for
+ * vertex-centred data (comm/physical_bcs.cpp:445-453). */
+#define Z4C_BC_OUTFLOW 1
+
+/* Registers held by a context (one value per variable per vertex per block). */
+enum {
+  Z4C_REG_U = 0,   /* storage.u    (22 vars)                        */
+  Z4C_REG_U1,      /* storage.u1   (22 vars, low-storage RK)        */
+  Z4C_REG_RHS,     /* storage.rhs  (22 vars)                        */
+  Z4C_REG_ADM,     /* storage.adm  (17 vars)                        */
+  Z4C_REG_CON,     /* storage.con  (7 vars)                         */
+  Z4C_REG_W,       /* work register (22 vars): ping-pong partner of u,
+                      and the scratch u_n of the Butcher integrator   */
+  Z4C_REG_K1,      /* Butcher stage slopes k_1..k_4 (22 vars each)  */
+  Z4C_REG_K2,
+  Z4C_REG_K3,
+  Z4C_REG_K4,
+  Z4C_NREG
+};
+
+/* Time integrators (task_list/time_integrators.hpp). */
+#define Z4C_INTEG_RK4 0     /* low-storage 2S RK4()4[2S], "rk4"  */
+#define Z4C_INTEG_BT_RK4 1  /* classical Butcher RK4, "bt_rk4"   */
+
+/* Run-time options of the Z4c class, z4c.hpp:357-431 with the defaults of
+ * z4c.cpp:318-410 (set by z4c_params_default). */
+typedef struct z4c_params {
+  double chi_psi_power;          /* -4 */
+  double chi_div_floor;          /* -1000 */
+  double diss;                   /* 0 (Kreiss-Oliger strength) */
+  double eps_floor;              /* 1e-12 */
+  double damp_kappa1;            /* 0 */
+  double damp_kappa2;            /* 0 */
+  double lapse_oplog;            /* 2 */
+  double lapse_harmonicf;        /* 1 */
+  double lapse_harmonic;         /* 0 */
+  double lapse_advect;           /* 1 */
+  double lapse_K;                /* 0 */
+  double shift_Gamma;            /* 1 */
+  double shift_alpha2Gamma;      /* 0 */
+  double shift_H;                /* 0 */
+  double shift_advect;           /* 1 */
+  double shift_eta;              /* 2 */
+  double r_max_con;              /* +inf */
+  int tf_force_regularization;   /* 1 */
+  int force_regularization;      /* 0 */
+} z4c_params_t;
+
+/* A uniform single-level mesh of nb[0]*nb[1]*nb[2] MeshBlocks of nx^3 cells
+ * on [xmin, xmax] (reference <mesh> and <meshblock> input blocks). */
+typedef struct z4c_mesh_desc {
+  int nb[3];
+  int nx[3];
+  double xmin[3];
+  double xmax[3];
+  int bc[6];
+} z4c_mesh_desc_t;
+
+typedef struct z4c_ctx z4c_ctx;
+
+/* Fills *p with the reference defaults (z4c.cpp:318-410). */
+void z4c_params_default(z4c_params_t *p);
+/* Message for the last failing call on this thread. */
+const char *z4c_last_error(void);
+
+/* Creates a context on the current CUDA device and allocates every register
+ * (no reference counterpart: replaces Z4c::Z4c's storage allocation,
+ * z4c.cpp:30-217, for all blocks at once). */
+int z4c_create(const z4c_mesh_desc_t *mesh, const z4c_params_t *params,
+               int integrator, z4c_ctx **out);
+int z4c_destroy(z4c_ctx *ctx);
+/* Work is enqueued on this CUDA stream (a cudaStream_t; NULL = default). */
+int z4c_set_stream(z4c_ctx *ctx, void *stream);
+int z4c_sync(z4c_ctx *ctx);
+/* Geometry queries: blocks, vertices per block axis, variables of a register,
+ * vertex spacing and the per-block vertex coordinates (the reference's x?f). */
+int z4c_num_blocks(const z4c_ctx *ctx);
+int z4c_block_nn(const z4c_ctx *ctx, int axis);
+int z4c_reg_nvar(int reg);
+int z4c_dx(const z4c_ctx *ctx, double dx_out[3]);
+int z4c_block_coords(const z4c_ctx *ctx, int block, int axis, double *x_out);
+
+/* Host <-> device copies of a register; block = -1 for the whole mesh.  The
+ * host buffer uses the reference layout (see above). */
+int z4c_upload(z4c_ctx *ctx, int reg, int block, const double *host);
+int z4c_download(z4c_ctx *ctx, int reg, int block, double *host);
+/* Device address of a register (whole mesh), for zero-copy interop. */
+int z4c_device_ptr(z4c_ctx *ctx, int reg, double **dptr);
+
+/* ---- operators; block = -1 runs every block in one batched launch, a block
+ *      index runs that block alone (the per-block launch of the plain path) */
+
+/* Z4c::Z4cRHS (z4c/calculate_z4c_rhs.cpp:29-916), with the 3-D derivative
+ * precompute of Z4c::PrepareZ4cDerivatives (z4c/adm_z4c.cpp:972-1037) fused
+ * in.  Writes the interior of reg_rhs. */
+int z4c_rhs(z4c_ctx *ctx, int reg_u, int reg_rhs, int block);
+/* Z4c::AddZ4cRHS (z4c/add_z4c_rhs.cpp:24-35): u_out += wght * rhs, interior. */
+int z4c_add_rhs(z4c_ctx *ctx, int reg_rhs, double wght, int reg_out, int block);
+/* Z4c::WeightedAve (mesh/weighted_ave.cpp:20-167, VC range):
+ * out = w0*out + w1*in1 + w2*in2 on the interior, with the reference's
+ * special cases for w0 in {0,1} and zero weights. */
+int z4c_weighted_ave(z4c_ctx *ctx, int reg_out, int reg_in1, int reg_in2,
+                     const double w[3], int block);
+/* Z4c::AlgConstr (z4c/z4c.cpp:677-799): all points, in place. */
+int z4c_alg_constr(z4c_ctx *ctx, int reg_u, int block);
+/* Z4c::ADMToZ4c (z4c/adm_z4c.cpp:46-192), including the final AlgConstr. */
+int z4c_adm_to_z4c(z4c_ctx *ctx, int reg_adm, int reg_u, int block);
+/* Z4c::Z4cToADM (z4c/adm_z4c.cpp:200-260). */
+int z4c_z4c_to_adm(z4c_ctx *ctx, int reg_u, int reg_adm, int block);
+/* Z4c::ADMConstraints (z4c/adm_z4c.cpp:382-930), vacuum. */
+int z4c_adm_constraints(z4c_ctx *ctx, int reg_con, int reg_adm, int reg_u,
+                        int block);
+/* GR_Z4c SEND/RECV/SETB_Z4C + PHY_BVAL (comm/comm_registry.cpp:336-382,
+ * comm/physical_bcs.cpp:506-670): same-level vertex-centred ghost fill by
+ * device copy, shared vertices averaged over their owners, then the
+ * physical boundary conditions.  Whole mesh. */
+int z4c_ghost_fill(z4c_ctx *ctx, int reg);
+/* History sums of outputs/history.cpp:168-200 over the whole mesh from the
+ * con and u registers: H^2, M, Mx^2, My^2, Mz^2, Z, Theta^2, C (volume
+ * weighted). */
+int z4c_hst_norms(z4c_ctx *ctx, double out[8]);
+
+/* ---- time stepping ------------------------------------------------------ */
+
+/* One GR_Z4c stage (task_list/gr/task_list_gr_z4c.cpp:142-333) over all
+ * blocks: fused RHS + KO + stage update, ghost fill, AlgConstr.  stage is
+ * 1-based; dt the full step. */
+int z4c_stage(z4c_ctx *ctx, int stage, double dt);
+/* nsteps full steps (gra::evolve::Z4c_Vacuum, src/main.hpp:906-913); the
+ * per-step launch sequence is captured once into a CUDA graph and replayed.
+ * When with_constraints is non-zero the last stage of the last step also
+ * runs Z4cToADM and ADMConstraints. */
+int z4c_evolve(z4c_ctx *ctx, double dt, int nsteps, int with_constraints);
+/* Selects the per-block launch loop (plain path, one RHS launch per block per
+ * stage) instead of the batched launch inside z4c_stage/z4c_evolve. */
+int z4c_set_per_block(z4c_ctx *ctx, int per_block);
+/* Tile shape of the RHS kernel (autotuner output): threads per CTA along
+ * i, j and k.  Returns Z4C_EINVAL for unsupported shapes. */
+int z4c_set_tile(z4c_ctx *ctx, int ti, int tj, int tk);
+int z4c_get_tile(const z4c_ctx *ctx, int tile_out[3]);
+/* Scans a register for NaN/Inf (z4c/z4c_utils.cpp:18-150 is_finite_*):
+ * Z4C_OK if all finite, Z4C_ENONFINITE otherwise. */
+int z4c_check_finite(z4c_ctx *ctx, int reg);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* Z4C_B200_H */

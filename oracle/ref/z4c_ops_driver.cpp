@@ -1,0 +1,243 @@
+// Operator driver for the GR-Athena++ reference build that serves as the
+// parity oracle (test infrastructure only).
+//
+// It sets up the Mesh exactly as the reference main program does (steps 1-5
+// of src/main.cpp: parse inputs, construct Mesh, run the problem generator and
+// Mesh::Initialize), then calls the Z4c member functions directly and writes
+// every output to the record file named by <driver>/out:
+//
+//   u0                 state after initialisation (all points)
+//   rhs0               Z4cRHS(u0) after PrepareZ4cDerivatives(u0)
+//   alg0               AlgConstr applied to a copy of u0
+//   adm0               Z4cToADM(u0)
+//   con0               ADMConstraints(con, adm0, mat, u0)
+//   uadm0              ADMToZ4c(adm0) into a zeroed register
+//   gx_pre / gx_post   a block-dependent perturbation of u0 before and after
+//                      one ghost exchange + physical boundary conditions
+//   s<n>_rhs, s<n>_int, s<n>_exch, s<n>_alg
+//                      one full time step, stage by stage, following the
+//                      GR_Z4c task order (task_list/gr/task_list_gr_z4c.cpp:
+//                      CALC_Z4CRHS, INT_Z4C, SEND/RECV/SETB_Z4C, PHY_BVAL,
+//                      ALG_CONSTR); s<N>_adm and s<N>_con after the last stage
+//
+// usage: z4c_ops_ref -i <input deck> [block/name=value ...]
+#include <cstdint>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "main.hpp"
+#include "comm/comm_registry.hpp"
+#include "task_list/time_integrators.hpp"
+#include "z4c/z4c.hpp"
+
+#include "z4c_oracle_io.hpp"
+
+namespace z4c_oracle {
+void DumpGeometry(Mesh* pm, Writer& w);  // z4c_oracle_pgen.cpp
+}
+
+namespace {
+
+using z4c_oracle::Writer;
+
+struct Dumper {
+  Writer w;
+  std::vector<MeshBlock*> by_gid;
+  int nn1 = 0, nn2 = 0, nn3 = 0;
+  explicit Dumper(const std::string& path, Mesh* pm) : w(path) {
+    const auto& blocks = pm->GetMeshBlocksCached();
+    by_gid.assign(blocks.size(), nullptr);
+    for (auto* b : blocks) by_gid.at(b->gid) = b;
+    nn1 = by_gid[0]->pz4c->mbi.nn1;
+    nn2 = by_gid[0]->pz4c->mbi.nn2;
+    nn3 = by_gid[0]->pz4c->mbi.nn3;
+  }
+  template <class Get>
+  void dump(const std::string& name, int nvar, Get get) {
+    const std::int64_t nb = static_cast<std::int64_t>(by_gid.size());
+    const std::int64_t per = static_cast<std::int64_t>(nvar) * nn1 * nn2 * nn3;
+    std::vector<double> buf(nb * per);
+    for (std::int64_t g = 0; g < nb; ++g) {
+      AthenaArray<Real>& a = get(by_gid[g]);
+      std::int64_t p = g * per;
+      for (int n = 0; n < nvar; ++n)
+        for (int k = 0; k < nn3; ++k)
+          for (int j = 0; j < nn2; ++j)
+            for (int i = 0; i < nn1; ++i) buf[p++] = a(n, k, j, i);
+    }
+    w.f64(name, {nb, nvar, nn3, nn2, nn1}, buf.data());
+  }
+};
+
+void Copy(AthenaArray<Real>& dst, AthenaArray<Real>& src) {
+  dst.NewAthenaArray(src.GetDim4(), src.GetDim3(), src.GetDim2(), src.GetDim1());
+  for (int n = 0; n < src.GetDim4(); ++n)
+    for (int k = 0; k < src.GetDim3(); ++k)
+      for (int j = 0; j < src.GetDim2(); ++j)
+        for (int i = 0; i < src.GetDim1(); ++i) dst(n, k, j, i) = src(n, k, j, i);
+}
+
+// One ghost exchange of the Z4c group over all blocks, as the GR_Z4c task
+// list performs it (SEND_Z4C, RECV_Z4C, SETB_Z4C, PHY_BVAL, CLEAR_ALLBND).
+void ExchangeAndBC(const std::vector<MeshBlock*>& blocks, Real t, Real dt) {
+  for (auto* b : blocks) b->pcomm->StartReceiving(comm::CommGroup::Z4c);
+  for (auto* b : blocks) b->pcomm->SendBoundaryBuffers(comm::CommGroup::Z4c);
+  for (int it = 0; it < 1000; ++it) {
+    bool all = true;
+    for (auto* b : blocks)
+      all = b->pcomm->ReceiveBoundaryBuffers(comm::CommGroup::Z4c) && all;
+    if (all) break;
+  }
+  for (auto* b : blocks) b->pcomm->SetBoundaries(comm::CommGroup::Z4c);
+  for (auto* b : blocks) b->pcomm->ApplyPhysicalBCs(comm::CommGroup::Z4c, t, dt);
+  for (auto* b : blocks)
+    b->pcomm->ClearBoundary(comm::CommGroup::Z4c, comm::CommTarget::All, true);
+}
+
+}  // namespace
+
+int main(int argc, char* argv[]) {
+  gra::Pathing Pathing;
+  gra::Flags Flags;
+  Flags.res = 0; Flags.narg = 0; Flags.iarg = 0; Flags.mesh = 0; Flags.wtlim = 0;
+  gra::parallelism::Init(argc, argv);
+  gra::ParseCommandLine(argc, argv, &Pathing, &Flags);
+  ParameterInput* pin = new ParameterInput;
+  IOWrapper infile, restartfile;
+  gra::ParseInputs(argc, argv, &Pathing, &Flags, pin, infile, restartfile);
+  Mesh* pm = gra::InitMesh(&Flags, pin, restartfile);
+  gra::InitMeshData(&Flags, pin, pm);
+
+  const std::string out = pin->GetString("driver", "out");
+  Dumper d(out, pm);
+  std::vector<MeshBlock*>& blocks = d.by_gid;
+  const int NZ = Z4c::N_Z4c;
+
+  {
+    std::vector<double> t = {pm->time, pm->dt};
+    d.w.f64("time_dt", {2}, t.data());
+  }
+  z4c_oracle::DumpGeometry(pm, d.w);
+  d.dump("u0", NZ, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.u; });
+
+  // --- single operators on u0 -------------------------------------------
+  std::vector<AthenaArray<Real>> tmp(blocks.size());
+  for (size_t g = 0; g < blocks.size(); ++g) {
+    Z4c* z = blocks[g]->pz4c;
+    tmp[g].NewAthenaArray(NZ, d.nn3, d.nn2, d.nn1);
+    z->PrepareZ4cDerivatives(z->storage.u);
+    z->Z4cRHS(z->storage.u, z->storage.mat, tmp[g]);
+  }
+  d.dump("rhs0", NZ, [&](MeshBlock* b) -> AthenaArray<Real>& { return tmp[b->gid]; });
+
+  for (size_t g = 0; g < blocks.size(); ++g) {
+    Z4c* z = blocks[g]->pz4c;
+    Copy(tmp[g], z->storage.u);
+    z->AlgConstr(tmp[g]);
+  }
+  d.dump("alg0", NZ, [&](MeshBlock* b) -> AthenaArray<Real>& { return tmp[b->gid]; });
+
+  for (auto* b : blocks) {
+    Z4c* z = b->pz4c;
+    z->Z4cToADM(z->storage.u, z->storage.adm);
+    z->ADMConstraints(z->storage.con, z->storage.adm, z->storage.mat, z->storage.u);
+  }
+  d.dump("adm0", Z4c::N_ADM, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.adm; });
+  d.dump("con0", Z4c::N_CON, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.con; });
+  for (auto* b : blocks) {
+    Z4c* z = b->pz4c;
+    z->PrepareZ4cDerivatives(z->storage.u);
+    z->ADMConstraints(z->storage.con, z->storage.adm, z->storage.mat, z->storage.u);
+  }
+  d.dump("con0b", Z4c::N_CON, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.con; });
+
+  for (size_t g = 0; g < blocks.size(); ++g) {
+    Z4c* z = blocks[g]->pz4c;
+    tmp[g].NewAthenaArray(NZ, d.nn3, d.nn2, d.nn1);
+    z->ADMToZ4c(z->storage.adm, tmp[g]);
+  }
+  d.dump("uadm0", NZ, [&](MeshBlock* b) -> AthenaArray<Real>& { return tmp[b->gid]; });
+
+  // --- ghost exchange on data whose shared vertices disagree ----------
+  std::vector<AthenaArray<Real>> keep(blocks.size());
+  for (size_t g = 0; g < blocks.size(); ++g) {
+    Z4c* z = blocks[g]->pz4c;
+    Copy(keep[g], z->storage.u);
+    AthenaArray<Real>& u = z->storage.u;
+    for (int n = 0; n < NZ; ++n)
+      for (int k = 0; k < d.nn3; ++k)
+        for (int j = 0; j < d.nn2; ++j)
+          for (int i = 0; i < d.nn1; ++i)
+            u(n, k, j, i) += 1e-3 * (g + 1) * (1 + n) * std::sin(0.3 * i + 0.7 * j + 1.1 * k);
+  }
+  d.dump("gx_pre", NZ, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.u; });
+  ExchangeAndBC(blocks, pm->time, 0.0);
+  d.dump("gx_post", NZ, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.u; });
+  for (size_t g = 0; g < blocks.size(); ++g) Copy(blocks[g]->pz4c->storage.u, keep[g]);
+
+  // --- one full time step, stage by stage ------------------------------
+  using TaskLists::Integrators::LowStorage;
+  using TaskLists::Integrators::Butcher;
+  const std::string integ = pin->GetOrAddString("time", "integrator", "rk4");
+  const bool is_bt = integ.find("bt_") != std::string::npos;
+  const Real dt = pm->dt;
+  LowStorage* ls = nullptr;
+  Butcher* bt = nullptr;
+  int nstages;
+  if (is_bt) { bt = new Butcher(pin, pm); nstages = bt->nstages; }
+  else { ls = new LowStorage(pin, pm); nstages = ls->nstages; }
+
+  for (auto* b : blocks) {
+    Z4c* z = b->pz4c;
+    z->storage.u1.ZeroClear();
+    z->PrepareZ4cDerivatives(z->storage.u);
+  }
+  for (int stage = 1; stage <= nstages; ++stage) {
+    const std::string s = "s" + std::to_string(stage) + "_";
+    for (auto* b : blocks) {
+      Z4c* z = b->pz4c;
+      if (is_bt) {
+        bt->PrepareStageScratch(stage, b, z->bt_k, z->storage.u, z->storage.rhs);
+      }
+      z->Z4cRHS(z->storage.u, z->storage.mat, z->storage.rhs);
+      z->Z4cBoundaryRHS(z->storage.u, z->storage.mat, z->storage.rhs);
+    }
+    d.dump(s + "rhs", NZ, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.rhs; });
+    for (auto* b : blocks) {
+      Z4c* z = b->pz4c;
+      if (!is_bt) {
+        Real w[3] = {1.0, ls->stage_wghts[stage - 1].delta, 0.0};
+        z->WeightedAve(z->storage.u1, z->storage.u, z->storage.u2, w);
+        w[0] = ls->stage_wghts[stage - 1].gamma_1;
+        w[1] = ls->stage_wghts[stage - 1].gamma_2;
+        w[2] = ls->stage_wghts[stage - 1].gamma_3;
+        z->WeightedAve(z->storage.u, z->storage.u1, z->storage.u2, w);
+        z->AddZ4cRHS(z->storage.rhs, ls->stage_wghts[stage - 1].beta * dt, z->storage.u);
+      } else {
+        if (stage < nstages) bt->SumBT_ak(b, stage + 1, dt, z->bt_k, z->storage.u);
+        else bt->SumBT_bk(b, dt, z->bt_k, z->storage.u);
+      }
+    }
+    d.dump(s + "int", NZ, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.u; });
+    ExchangeAndBC(blocks, pm->time, dt);
+    d.dump(s + "exch", NZ, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.u; });
+    for (auto* b : blocks) {
+      Z4c* z = b->pz4c;
+      z->AlgConstr(z->storage.u);
+      z->PrepareZ4cDerivatives(z->storage.u);
+    }
+    d.dump(s + "alg", NZ, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.u; });
+    if (stage == nstages) {
+      for (auto* b : blocks) {
+        Z4c* z = b->pz4c;
+        z->Z4cToADM(z->storage.u, z->storage.adm);
+        z->ADMConstraints(z->storage.con, z->storage.adm, z->storage.mat, z->storage.u);
+      }
+      d.dump(s + "adm", Z4c::N_ADM, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.adm; });
+      d.dump(s + "con", Z4c::N_CON, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.con; });
+    }
+  }
+  std::cout << "z4c_ops_ref: wrote " << out << std::endl;
+  return 0;
+}

@@ -1,0 +1,1121 @@
+/* CPU restatement of the GR-Athena++ Z4c hot path: the parity oracle.
+ *
+ * TEST INFRASTRUCTURE ONLY (see z4c_oracle.h).  Parity of this file with the
+ * reference is pinned by tests/test_oracle_golden.py against record files
+ * produced by the reference CPU build itself (oracle/ref, tests/golden).
+ *
+ * Floating-point expressions keep the reference's evaluation order (the
+ * reference is built with -ffp-contract=off; so is this file).  Symmetric
+ * tensors are held as full 3x3 arrays whose lower triangle mirrors the upper
+ * one, which is how the reference's AthenaTensor SYM2 accessors read them.
+ */
+#define _GNU_SOURCE
+#include "z4c_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define NG ORC_NG
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+/* ---- finite differences, utils/finite_differencing.tpp with the
+ *      DBG_SYMMETRIZE_FD stencils (defs.hpp.in:18 defines it) -------------- */
+
+/* FDStencilCenteredDegreeOdd<1,3>, finite_differencing_stencils.tpp:266-272 */
+static const double C1[3] = {-1, 9, -45};
+static const double C1_LCM = 60;
+/* FDStencilCenteredDegreeEven<2,3>, :316-322 */
+static const double C2[4] = {2, -27, 270, -490};
+static const double C2_LCM = 180;
+/* FDStencilCenteredDegreeEven<8,4>, :372-378 */
+static const double CD[5] = {1, -8, 28, -56, 70};
+/* FDStencilBiasedLeft/Right<1,4,2>, :470-486 */
+static const double CL[7] = {1, -8, 30, -80, 35, 24, -2};
+static const double CR[7] = {2, -24, -35, 80, -30, 8, -1};
+static const double CLR_LCM = 60;
+
+typedef struct {
+  int nn1, nn2, nn3;
+  int64_t s[3];         /* strides */
+  double cidx1[3], cidx2[3], cidxd[3], lidx[3];
+  int il, iu, jl, ju, kl, ku; /* vertex interior range (ivs..ive) */
+} fd_t;
+
+static void fd_init(const orc_block_t *b, fd_t *f) {
+  f->nn1 = b->nx[0] + 1 + 2 * NG;
+  f->nn2 = b->nx[1] + 1 + 2 * NG;
+  f->nn3 = b->nx[2] + 1 + 2 * NG;
+  f->s[0] = 1;
+  f->s[1] = f->nn1;
+  f->s[2] = (int64_t)f->nn2 * f->nn1;
+  /* finite_differencing.tpp:24 */
+  const double diss_scaling = pow(2, -2 * NG) * (NG % 2 == 0 ? -1 : 1);
+  for (int a = 0; a < 3; ++a) {
+    const double dx = b->dx[a];
+    f->cidx1[a] = 1.0 / (dx * C1_LCM);                 /* .tpp:36-38 */
+    f->cidx2[a] = ((1.0 / dx) * (1.0 / dx)) / C2_LCM;  /* .tpp:40-42 */
+    f->cidxd[a] = diss_scaling / (dx * 1.0);           /* .tpp:48-50 */
+    f->lidx[a] = 1.0 / (dx * CLR_LCM);                 /* .tpp:53-55 */
+  }
+  f->il = NG; f->iu = NG + b->nx[0];
+  f->jl = NG; f->ju = NG + b->nx[1];
+  f->kl = NG; f->ku = NG + b->nx[2];
+}
+
+/* Uniform::Dx, finite_differencing.tpp:63-112 (symmetrized branch) */
+static inline double Dx(const fd_t *f, int dir, const double *u) {
+  const int64_t s = f->s[dir];
+  const double *pu = u - 3 * s;
+  double out = 0.;
+  for (int n1 = 0; n1 < 3; ++n1) {
+    const int n2 = 6 - n1;
+    out += C1[n1] * (pu[n1 * s] - pu[n2 * s]);
+  }
+  return out * f->cidx1[dir];
+}
+
+/* Uniform::Dxx, finite_differencing.tpp:196-236 */
+static inline double Dxx(const fd_t *f, int dir, const double *u) {
+  const int64_t s = f->s[dir];
+  const double *pu = u - 3 * s;
+  double out = 0.;
+  for (int n1 = 0; n1 < 3; ++n1) {
+    const int n2 = 6 - n1;
+    out += C2[n1] * (pu[n1 * s] + pu[n2 * s]);
+  }
+  out += C2[3] * pu[3 * s];
+  return out * f->cidx2[dir];
+}
+
+/* Uniform::Diss, finite_differencing.tpp:335-352 */
+static inline double Diss(const fd_t *f, int dir, const double *u, double diss) {
+  const int64_t s = f->s[dir];
+  const double *pu = u - 4 * s;
+  double out = 0.;
+  for (int n1 = 0; n1 < 4; ++n1) {
+    const int n2 = 8 - n1;
+    out += CD[n1] * (pu[n1 * s] + pu[n2 * s]);
+  }
+  out += CD[4] * pu[4 * s];
+  return out * f->cidxd[dir] * diss;
+}
+
+/* Uniform::Lx, finite_differencing.tpp:152-174 */
+static inline double Lx(const fd_t *f, int dir, double vx, const double *u) {
+  const int64_t s = f->s[dir];
+  double dl = 0.;
+  for (int n = 0; n < 7; ++n) dl += CL[n] * u[(n - 4) * s];
+  double dr = 0.;
+  for (int n = 6; n >= 0; --n) dr += CR[n] * u[(n - 2) * s];
+  return ((vx < 0) ? (vx * dl) : (vx * dr)) * f->lidx[dir];
+}
+
+/* ---- small linear algebra, utils/linear_algebra.hpp -------------------- */
+
+static const int SI[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+
+/* Det3Metric, linear_algebra.hpp:47-56 */
+static inline double det3(double gxx, double gxy, double gxz, double gyy,
+                          double gyz, double gzz) {
+  return (-(gxz * gxz) * gyy + 2 * gxy * gxz * gyz - gxx * (gyz * gyz) -
+          (gxy * gxy) * gzz + gxx * gyy * gzz);
+}
+
+/* Inv3Metric, linear_algebra.hpp:98-118 */
+static inline void inv3(double oodetg, double gxx, double gxy, double gxz,
+                        double gyy, double gyz, double gzz, double g_uu[3][3]) {
+  const double uxx = (-(gyz * gyz) + gyy * gzz) * oodetg;
+  const double uxy = (gxz * gyz - gxy * gzz) * oodetg;
+  const double uyy = (-(gxz * gxz) + gxx * gzz) * oodetg;
+  const double uxz = (-gxz * gyy + gxy * gyz) * oodetg;
+  const double uyz = (gxy * gxz - gxx * gyz) * oodetg;
+  const double uzz = (-(gxy * gxy) + gxx * gyy) * oodetg;
+  g_uu[0][0] = uxx; g_uu[0][1] = uxy; g_uu[0][2] = uxz;
+  g_uu[1][0] = uxy; g_uu[1][1] = uyy; g_uu[1][2] = uyz;
+  g_uu[2][0] = uxz; g_uu[2][1] = uyz; g_uu[2][2] = uzz;
+}
+
+/* TraceRank2, linear_algebra.hpp:271-290 */
+static inline double trace_rank2(double detginv, double gxx, double gxy,
+                                 double gxz, double gyy, double gyz, double gzz,
+                                 double Axx, double Axy, double Axz, double Ayy,
+                                 double Ayz, double Azz) {
+  return detginv * (-2. * Ayz * gxx * gyz + Axx * gyy * gzz +
+                    gxx * (Azz * gyy + Ayy * gzz) +
+                    2. * (gxz * (Ayz * gxy - Axz * gyy + Axy * gyz) +
+                          gxy * (Axz * gyz - Axy * gzz)) -
+                    Azz * (gxy * gxy) - Ayy * (gxz * gxz) - Axx * (gyz * gyz));
+}
+
+/* regularize_nth_root, utils/floating_point.hpp:120-131 */
+static inline double regularize_nth_root(double value, double value_reg,
+                                         double eps_floor, double npow) {
+  const double eps = value - value_reg;
+  return ((eps < eps_floor) ? (1.0 + eps_floor / npow) : pow(value, 1.0 / npow));
+}
+
+/* regularize_near_zero, floating_point.hpp:110-115 */
+static inline double regularize_near_zero(double value, double value_eps) {
+  return (value >= 0) ? ((value < value_eps) ? value_eps : value)
+                      : ((value > -value_eps) ? -value_eps : value);
+}
+
+static inline double dmax(double a, double b) { return (a < b) ? b : a; }
+
+/* ---- storage ------------------------------------------------------------ */
+
+int64_t orc_nvol(const orc_block_t *b) {
+  return (int64_t)(b->nx[0] + 1 + 2 * NG) * (b->nx[1] + 1 + 2 * NG) *
+         (b->nx[2] + 1 + 2 * NG);
+}
+
+int orc_derivs_alloc(const orc_block_t *b, orc_derivs_t *d) {
+  const int64_t n = orc_nvol(b);
+  memset(d, 0, sizeof(*d));
+  double **slots[3 + 3 + 9 + 18 + 6];
+  int ns = 0;
+  for (int a = 0; a < 3; ++a) slots[ns++] = &d->dalpha[a];
+  for (int a = 0; a < 3; ++a) slots[ns++] = &d->dchi[a];
+  for (int a = 0; a < 3; ++a)
+    for (int c = 0; c < 3; ++c) slots[ns++] = &d->dbeta[a][c];
+  for (int a = 0; a < 3; ++a)
+    for (int c = 0; c < 6; ++c) slots[ns++] = &d->dg[a][c];
+  for (int c = 0; c < 6; ++c) slots[ns++] = &d->ddchi[c];
+  for (int s = 0; s < ns; ++s) {
+    *slots[s] = (double *)calloc((size_t)n, sizeof(double));
+    if (!*slots[s]) { orc_derivs_free(d); return -1; }
+  }
+  return 0;
+}
+
+void orc_derivs_free(orc_derivs_t *d) {
+  for (int a = 0; a < 3; ++a) {
+    free(d->dalpha[a]); free(d->dchi[a]);
+    for (int c = 0; c < 3; ++c) free(d->dbeta[a][c]);
+    for (int c = 0; c < 6; ++c) free(d->dg[a][c]);
+  }
+  for (int c = 0; c < 6; ++c) free(d->ddchi[c]);
+  memset(d, 0, sizeof(*d));
+}
+
+#define V(u, n) ((u) + (int64_t)(n) * nvol)
+#define P(k, j, i) (((int64_t)(k) * f.nn2 + (j)) * f.nn1 + (i))
+
+/* ---- Z4c::PrepareZ4cDerivatives, adm_z4c.cpp:972-1037 ------------------ */
+void orc_prepare_derivs(const orc_block_t *b, const double *u, orc_derivs_t *d) {
+  fd_t f;
+  fd_init(b, &f);
+  const int64_t nvol = orc_nvol(b);
+  const int ng_ext = NG - 1;
+  for (int bd = 0; bd < 3; ++bd) {
+    const int klo = (bd == 2) ? f.kl : f.kl - ng_ext;
+    const int khi = (bd == 2) ? f.ku : f.ku + ng_ext;
+    const int jlo = (bd == 1) ? f.jl : f.jl - ng_ext;
+    const int jhi = (bd == 1) ? f.ju : f.ju + ng_ext;
+    const int ilo = (bd == 0) ? f.il : f.il - ng_ext;
+    const int ihi = (bd == 0) ? f.iu : f.iu + ng_ext;
+    for (int k = klo; k <= khi; ++k)
+      for (int j = jlo; j <= jhi; ++j)
+        for (int i = ilo; i <= ihi; ++i) {
+          const int64_t p = P(k, j, i);
+          d->dalpha[bd][p] = Dx(&f, bd, V(u, Z4C_ALPHA) + p);
+          d->dchi[bd][p] = Dx(&f, bd, V(u, Z4C_CHI) + p);
+          for (int c = 0; c < 3; ++c)
+            d->dbeta[bd][c][p] = Dx(&f, bd, V(u, Z4C_BETAX + c) + p);
+          for (int c = 0; c < 6; ++c)
+            d->dg[bd][c][p] = Dx(&f, bd, V(u, Z4C_GXX + c) + p);
+        }
+  }
+  for (int a = 0; a < 3; ++a) {
+    for (int k = f.kl; k <= f.ku; ++k)
+      for (int j = f.jl; j <= f.ju; ++j)
+        for (int i = f.il; i <= f.iu; ++i) {
+          const int64_t p = P(k, j, i);
+          d->ddchi[SI[a][a]][p] = Dxx(&f, a, V(u, Z4C_CHI) + p);
+        }
+    for (int bb = a + 1; bb < 3; ++bb)
+      for (int k = f.kl; k <= f.ku; ++k)
+        for (int j = f.jl; j <= f.ju; ++j)
+          for (int i = f.il; i <= f.iu; ++i) {
+            const int64_t p = P(k, j, i);
+            d->ddchi[SI[a][bb]][p] = Dx(&f, a, d->dchi[bb] + p);
+          }
+  }
+}
+
+/* ---- Z4c::Z4cRHS, calculate_z4c_rhs.cpp:29-916 -------------------------- */
+void orc_rhs(const orc_block_t *b, const z4c_params_t *opt, const double *u,
+             const orc_derivs_t *D, double *rhs) {
+  fd_t f;
+  fd_init(b, &f);
+  const int64_t nvol = orc_nvol(b);
+  const double oochi_psi_power = 1.0 / opt->chi_psi_power;
+  const double chi_pow_DA_u = -6.0 / opt->chi_psi_power;
+  const double rho = 0.0, S_d[3] = {0, 0, 0};  /* vacuum matter fields */
+
+  for (int k = f.kl; k <= f.ku; ++k)
+    for (int j = f.jl; j <= f.ju; ++j)
+      for (int i = f.il; i <= f.iu; ++i) {
+        const int64_t p = P(k, j, i);
+        double g_dd[3][3], A_dd[3][3], beta_u[3], Gam_u[3];
+        for (int a = 0; a < 3; ++a)
+          for (int c = 0; c < 3; ++c) {
+            g_dd[a][c] = V(u, Z4C_GXX + SI[a][c])[p];
+            A_dd[a][c] = V(u, Z4C_AXX + SI[a][c])[p];
+          }
+        for (int a = 0; a < 3; ++a) {
+          beta_u[a] = V(u, Z4C_BETAX + a)[p];
+          Gam_u[a] = V(u, Z4C_GAMX + a)[p];
+        }
+        const double chi = V(u, Z4C_CHI)[p], Khat = V(u, Z4C_KHAT)[p];
+        const double Theta = V(u, Z4C_THETA)[p], alpha = V(u, Z4C_ALPHA)[p];
+
+        /* 1st derivatives, :84-114 */
+        double dalpha_d[3], dchi_d[3], dKhat_d[3], dTheta_d[3];
+        double dbeta_du[3][3], dGam_du[3][3], dg_ddd[3][3][3], dA_ddd[3][3][3];
+        for (int a = 0; a < 3; ++a) {
+          dalpha_d[a] = D->dalpha[a][p];
+          dchi_d[a] = D->dchi[a][p];
+          dKhat_d[a] = Dx(&f, a, V(u, Z4C_KHAT) + p);
+          dTheta_d[a] = Dx(&f, a, V(u, Z4C_THETA) + p);
+        }
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb) {
+            dbeta_du[bb][a] = D->dbeta[bb][a][p];
+            dGam_du[bb][a] = Dx(&f, bb, V(u, Z4C_GAMX + a) + p);
+          }
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb)
+            for (int c = 0; c < 3; ++c) {
+              dg_ddd[c][a][bb] = dg_ddd[c][bb][a] = D->dg[c][SI[a][bb]][p];
+              dA_ddd[c][a][bb] = dA_ddd[c][bb][a] =
+                  Dx(&f, c, V(u, Z4C_AXX + SI[a][bb]) + p);
+            }
+
+        /* 2nd derivatives, :121-178 */
+        double ddalpha_dd[3][3], ddchi_dd[3][3], ddbeta_ddu[3][3][3];
+        double ddg_dddd[3][3][3][3];
+        for (int a = 0; a < 3; ++a) {
+          ddalpha_dd[a][a] = Dxx(&f, a, V(u, Z4C_ALPHA) + p);
+          ddchi_dd[a][a] = D->ddchi[SI[a][a]][p];
+          for (int bb = a + 1; bb < 3; ++bb) {
+            ddalpha_dd[a][bb] = ddalpha_dd[bb][a] = Dx(&f, a, D->dalpha[bb] + p);
+            ddchi_dd[a][bb] = ddchi_dd[bb][a] = D->ddchi[SI[a][bb]][p];
+          }
+        }
+        for (int c = 0; c < 3; ++c)
+          for (int a = 0; a < 3; ++a)
+            for (int bb = a; bb < 3; ++bb) {
+              double v;
+              if (a == bb) v = Dxx(&f, a, V(u, Z4C_BETAX + c) + p);
+              else v = Dx(&f, a, D->dbeta[bb][c] + p);
+              ddbeta_ddu[a][bb][c] = ddbeta_ddu[bb][a][c] = v;
+            }
+        for (int c = 0; c < 3; ++c)
+          for (int dd = c; dd < 3; ++dd)
+            for (int a = 0; a < 3; ++a)
+              for (int bb = a; bb < 3; ++bb) {
+                double v;
+                if (a == bb) v = Dxx(&f, a, V(u, Z4C_GXX + SI[c][dd]) + p);
+                else v = Dx(&f, a, D->dg[bb][SI[c][dd]] + p);
+                ddg_dddd[a][bb][c][dd] = ddg_dddd[bb][a][c][dd] =
+                    ddg_dddd[a][bb][dd][c] = ddg_dddd[bb][a][dd][c] = v;
+              }
+
+        /* advective derivatives, :184-226 */
+        double Lalpha = 0, Lchi = 0, LKhat = 0, LTheta = 0;
+        for (int a = 0; a < 3; ++a) {
+          Lalpha += Lx(&f, a, beta_u[a], V(u, Z4C_ALPHA) + p);
+          Lchi += Lx(&f, a, beta_u[a], V(u, Z4C_CHI) + p);
+          LKhat += Lx(&f, a, beta_u[a], V(u, Z4C_KHAT) + p);
+          LTheta += Lx(&f, a, beta_u[a], V(u, Z4C_THETA) + p);
+        }
+        double Lbeta_u[3] = {0, 0, 0}, LGam_u[3] = {0, 0, 0};
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb) {
+            Lbeta_u[bb] += Lx(&f, a, beta_u[a], V(u, Z4C_BETAX + bb) + p);
+            LGam_u[bb] += Lx(&f, a, beta_u[a], V(u, Z4C_GAMX + bb) + p);
+          }
+        double Lg_dd[3][3] = {{0}}, LA_dd[3][3] = {{0}};
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb)
+            for (int c = 0; c < 3; ++c) {
+              Lg_dd[a][bb] += Lx(&f, c, beta_u[c], V(u, Z4C_GXX + SI[a][bb]) + p);
+              LA_dd[a][bb] += Lx(&f, c, beta_u[c], V(u, Z4C_AXX + SI[a][bb]) + p);
+            }
+
+        /* :231-274 */
+        const double K = Khat + 2. * Theta;
+        const double chi_guarded = dmax(chi, opt->chi_div_floor);
+        const double oochi = 1.0 / chi_guarded;
+        double oopsi4;
+        if (opt->chi_psi_power == -4.) oopsi4 = chi_guarded;
+        else oopsi4 = pow(chi_guarded, -4. / opt->chi_psi_power);
+
+        /* inverse conformal metric, :295-311 */
+        double g_uu[3][3];
+        {
+          const double detg = det3(g_dd[0][0], g_dd[0][1], g_dd[0][2], g_dd[1][1],
+                                   g_dd[1][2], g_dd[2][2]);
+          inv3(1.0 / detg, g_dd[0][0], g_dd[0][1], g_dd[0][2], g_dd[1][1],
+               g_dd[1][2], g_dd[2][2], g_uu);
+        }
+
+        /* Christoffels, :317-352 */
+        double Gamma_ddd[3][3][3], Gamma_udd[3][3][3], Gamma_u[3];
+        for (int c = 0; c < 3; ++c)
+          for (int a = 0; a < 3; ++a)
+            for (int bb = a; bb < 3; ++bb)
+              Gamma_ddd[c][a][bb] = Gamma_ddd[c][bb][a] =
+                  0.5 * (dg_ddd[a][bb][c] + dg_ddd[bb][a][c] - dg_ddd[c][a][bb]);
+        for (int c = 0; c < 3; ++c)
+          for (int a = 0; a < 3; ++a)
+            for (int bb = a; bb < 3; ++bb) {
+              double s = 0;
+              for (int dd = 0; dd < 3; ++dd) s += g_uu[c][dd] * Gamma_ddd[dd][a][bb];
+              Gamma_udd[c][a][bb] = Gamma_udd[c][bb][a] = s;
+            }
+        for (int a = 0; a < 3; ++a) {
+          double s = 0;
+          for (int bb = 0; bb < 3; ++bb)
+            for (int c = bb; c < 3; ++c)
+              s += ((bb == c) ? 1.0 : 2.0) * g_uu[bb][c] * Gamma_udd[a][bb][c];
+          Gamma_u[a] = s;
+        }
+
+        /* Ricci of the conformal metric, :357-396 */
+        double R_dd[3][3];
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb) {
+            double s = 0;
+            for (int c = 0; c < 3; ++c)
+              s += 0.5 * (g_dd[c][a] * dGam_du[bb][c] + g_dd[c][bb] * dGam_du[a][c] +
+                          Gamma_u[c] * (Gamma_ddd[a][bb][c] + Gamma_ddd[bb][a][c]));
+            for (int c = 0; c < 3; ++c)
+              for (int dd = c; dd < 3; ++dd)
+                s -= ((c == dd) ? 0.5 : 1.0) * g_uu[c][dd] * ddg_dddd[c][dd][a][bb];
+            for (int c = 0; c < 3; ++c)
+              for (int dd = 0; dd < 3; ++dd)
+                for (int e = 0; e < 3; ++e)
+                  s += g_uu[c][dd] * (Gamma_udd[e][c][a] * Gamma_ddd[bb][e][dd] +
+                                      Gamma_udd[e][c][bb] * Gamma_ddd[a][e][dd] +
+                                      Gamma_udd[e][a][dd] * Gamma_ddd[e][c][bb]);
+            R_dd[a][bb] = R_dd[bb][a] = s;
+          }
+
+        /* conformal factor derivatives, :402-426 */
+        double dphi_d[3], Ddphi_dd[3][3];
+        for (int a = 0; a < 3; ++a) dphi_d[a] = dchi_d[a] * oochi * oochi_psi_power;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb) {
+            double v = ddchi_dd[a][bb] * oochi * oochi_psi_power -
+                       opt->chi_psi_power * dphi_d[a] * dphi_d[bb];
+            for (int c = 0; c < 3; ++c) v -= Gamma_udd[c][a][bb] * dphi_d[c];
+            Ddphi_dd[a][bb] = Ddphi_dd[bb][a] = v;
+          }
+
+        /* Rphi, :436-458 */
+        double Stmp = 0.0;
+        for (int c = 0; c < 3; ++c)
+          for (int dd = c; dd < 3; ++dd)
+            Stmp += ((c == dd) ? 1.0 : 2.0) * g_uu[c][dd] *
+                    (Ddphi_dd[c][dd] + 2. * dphi_d[c] * dphi_d[dd]);
+        double Rphi_dd[3][3];
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb)
+            Rphi_dd[a][bb] = Rphi_dd[bb][a] = 4. * dphi_d[a] * dphi_d[bb] -
+                                              2. * Ddphi_dd[a][bb] -
+                                              2. * g_dd[a][bb] * Stmp;
+
+        /* matter trace (zero matter), :465-474 */
+        double S = 0;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb)
+            S += ((a == bb) ? 1.0 : 2.0) * oopsi4 * g_uu[a][bb] * 0.0;
+
+        /* D D alpha, :482-521 */
+        double Ddalpha = 0;
+        for (int c = 0; c < 3; ++c)
+          for (int dd = 0; dd < 3; ++dd) Ddalpha += g_uu[c][dd] * dphi_d[c] * dalpha_d[dd];
+        double Ddalpha_dd[3][3];
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb) {
+            double v = ddalpha_dd[a][bb] -
+                       2. * (dphi_d[a] * dalpha_d[bb] + dphi_d[bb] * dalpha_d[a]) +
+                       2. * g_dd[a][bb] * Ddalpha;
+            for (int c = 0; c < 3; ++c) v -= Gamma_udd[c][a][bb] * dalpha_d[c];
+            Ddalpha_dd[a][bb] = Ddalpha_dd[bb][a] = v;
+          }
+        Ddalpha = 0;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb)
+            Ddalpha += ((a == bb) ? 1.0 : 2.0) * oopsi4 * g_uu[a][bb] * Ddalpha_dd[a][bb];
+
+        /* A contractions, :525-589 */
+        double A_ud[3][3], AA_dd[3][3], A_uu[3][3], DA_u[3];
+        for (int c = 0; c < 3; ++c)
+          for (int bb = 0; bb < 3; ++bb) {
+            double s = 0;
+            for (int dd = 0; dd < 3; ++dd) s += g_uu[c][dd] * A_dd[dd][bb];
+            A_ud[c][bb] = s;
+          }
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb) {
+            double s = 0;
+            for (int c = 0; c < 3; ++c) s += A_dd[a][c] * A_ud[c][bb];
+            AA_dd[a][bb] = AA_dd[bb][a] = s;
+          }
+        double trAA = 0;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb)
+            trAA += ((a == bb) ? 1.0 : 2.0) * g_uu[a][bb] * AA_dd[a][bb];
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb) {
+            double s = 0;
+            for (int c = 0; c < 3; ++c) s += g_uu[bb][c] * A_ud[a][c];
+            A_uu[a][bb] = A_uu[bb][a] = s;
+          }
+        for (int a = 0; a < 3; ++a) {
+          double s = 0;
+          for (int bb = 0; bb < 3; ++bb) {
+            s -= chi_pow_DA_u * A_uu[a][bb] * dchi_d[bb] * oochi;
+            s -= (1. / 3.) * g_uu[a][bb] * (2. * dKhat_d[bb] + dTheta_d[bb]);
+          }
+          for (int bb = 0; bb < 3; ++bb)
+            for (int c = bb; c < 3; ++c)
+              s += ((bb == c) ? 1.0 : 2.0) * Gamma_udd[a][bb][c] * A_uu[bb][c];
+          DA_u[a] = s;
+        }
+
+        /* Ricci scalar and Ht, :596-613 */
+        double R = 0;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb)
+            R += ((a == bb) ? 1.0 : 2.0) * oopsi4 * g_uu[a][bb] *
+                 (R_dd[a][bb] + Rphi_dd[a][bb]);
+        const double Ht = R + (2. / 3.) * (K * K) - trAA;
+
+        /* Lie derivatives, :619-687 */
+        double dbeta = 0;
+        for (int a = 0; a < 3; ++a) dbeta += dbeta_du[a][a];
+        double ddbeta_d[3] = {0, 0, 0};
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb) ddbeta_d[a] += (1. / 3.) * ddbeta_ddu[a][bb][bb];
+        Lchi += (1. / 6.) * opt->chi_psi_power * chi_guarded * dbeta;
+        for (int a = 0; a < 3; ++a) {
+          LGam_u[a] += (2. / 3.) * Gamma_u[a] * dbeta;
+          for (int bb = 0; bb < 3; ++bb) {
+            LGam_u[a] += g_uu[a][bb] * ddbeta_d[bb] - Gamma_u[bb] * dbeta_du[bb][a];
+            for (int c = bb; c < 3; ++c)
+              LGam_u[a] += ((bb == c) ? 1.0 : 2.0) * g_uu[bb][c] * ddbeta_ddu[bb][c][a];
+          }
+        }
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb) {
+            Lg_dd[a][bb] -= (2. / 3.) * g_dd[a][bb] * dbeta;
+            LA_dd[a][bb] -= (2. / 3.) * A_dd[a][bb] * dbeta;
+            for (int c = 0; c < 3; ++c) {
+              Lg_dd[a][bb] += dbeta_du[a][c] * g_dd[bb][c];
+              LA_dd[a][bb] += dbeta_du[bb][c] * A_dd[a][c];
+              Lg_dd[a][bb] += dbeta_du[bb][c] * g_dd[a][c];
+              LA_dd[a][bb] += dbeta_du[a][c] * A_dd[bb][c];
+            }
+          }
+
+        /* assemble, :694-902 */
+        double r_Khat = -Ddalpha + alpha * (trAA + (1. / 3.) * (K * K)) + LKhat +
+                        opt->damp_kappa1 * (1 - opt->damp_kappa2) * alpha * Theta;
+        r_Khat += 4 * M_PI * alpha * (S + rho);
+        const double r_chi = Lchi - (1. / 6.) * opt->chi_psi_power * chi_guarded * alpha * K;
+        double r_Theta = LTheta + alpha * (0.5 * Ht - (2. + opt->damp_kappa2) *
+                                                          opt->damp_kappa1 * Theta);
+        r_Theta -= 8. * M_PI * alpha * rho;
+        V(rhs, Z4C_KHAT)[p] = r_Khat;
+        V(rhs, Z4C_CHI)[p] = r_chi;
+        V(rhs, Z4C_THETA)[p] = r_Theta;
+        for (int a = 0; a < 3; ++a) {
+          double v = 2. * alpha * DA_u[a] + LGam_u[a];
+          v -= 2. * alpha * opt->damp_kappa1 * (Gam_u[a] - Gamma_u[a]);
+          for (int bb = 0; bb < 3; ++bb) {
+            v -= 2. * A_uu[a][bb] * dalpha_d[bb];
+            v -= 16. * M_PI * alpha * g_uu[a][bb] * S_d[bb];
+          }
+          V(rhs, Z4C_GAMX + a)[p] = v;
+        }
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb) {
+            V(rhs, Z4C_GXX + SI[a][bb])[p] = -2. * alpha * A_dd[a][bb] + Lg_dd[a][bb];
+            double v = oopsi4 * (-Ddalpha_dd[a][bb] + alpha * (R_dd[a][bb] + Rphi_dd[a][bb]));
+            v -= (1. / 3.) * g_dd[a][bb] * (-Ddalpha + alpha * R);
+            v += alpha * (K * A_dd[a][bb] - 2. * AA_dd[a][bb]);
+            v += LA_dd[a][bb];
+            v -= 8. * M_PI * alpha * (oopsi4 * 0.0 - (1. / 3.) * S * g_dd[a][bb]);
+            V(rhs, Z4C_AXX + SI[a][bb])[p] = v;
+          }
+        {
+          const double fl = opt->lapse_oplog * opt->lapse_harmonicf + opt->lapse_harmonic * alpha;
+          V(rhs, Z4C_ALPHA)[p] = (opt->lapse_advect * Lalpha -
+                                  fl * alpha * (Khat + 2 * opt->lapse_K * Theta));
+        }
+        for (int a = 0; a < 3; ++a) {
+          double v = opt->shift_Gamma * Gam_u[a] + opt->shift_advect * Lbeta_u[a];
+          if (fabs(opt->shift_alpha2Gamma) > 0.0)
+            v += opt->shift_alpha2Gamma * (alpha * alpha) * Gam_u[a];
+          if (fabs(opt->shift_H) > 0.0)
+            for (int bb = 0; bb < 3; ++bb)
+              v += opt->shift_H * alpha * chi_guarded *
+                   (0.5 * alpha * dchi_d[bb] - dalpha_d[bb]) * g_uu[a][bb];
+          v -= opt->shift_eta * beta_u[a];
+          V(rhs, Z4C_BETAX + a)[p] = v;
+        }
+      }
+
+  /* Kreiss-Oliger dissipation, :908-915 */
+  for (int n = 0; n < Z4C_NVAR; ++n)
+    for (int k = f.kl; k <= f.ku; ++k)
+      for (int j = f.jl; j <= f.ju; ++j)
+        for (int i = f.il; i <= f.iu; ++i) {
+          const int64_t p = P(k, j, i);
+          for (int a = 0; a < 3; ++a)
+            V(rhs, n)[p] += Diss(&f, a, V(u, n) + p, opt->diss);
+        }
+}
+
+/* ---- Z4c::AlgConstr, z4c.cpp:677-799 / 801-991 --------------------------- */
+static void algconstr_point(const z4c_params_t *opt, double *u, int64_t nvol,
+                            int64_t p) {
+  double *g[6], *A[6];
+  for (int c = 0; c < 6; ++c) {
+    g[c] = V(u, Z4C_GXX + c) + p;
+    A[c] = V(u, Z4C_AXX + c) + p;
+  }
+  if (opt->tf_force_regularization) {
+    double detg = det3(*g[0], *g[1], *g[2], *g[3], *g[4], *g[5]);
+    detg = detg > 0. ? detg : 1.;
+    const double oopsi4 = regularize_nth_root(detg, 1.0, opt->eps_floor, -3.0);
+    for (int c = 0; c < 6; ++c) *g[c] *= oopsi4;
+    const double tr = trace_rank2(1.0, *g[0], *g[1], *g[2], *g[3], *g[4], *g[5],
+                                  *A[0], *A[1], *A[2], *A[3], *A[4], *A[5]);
+    for (int c = 0; c < 6; ++c) *A[c] -= (1.0 / 3.0) * tr * *g[c];
+  } else {
+    const double detg = det3(*g[0], *g[1], *g[2], *g[3], *g[4], *g[5]);
+    if (detg > opt->eps_floor) {
+      const double oopsi4 = regularize_nth_root(detg, 1.0, opt->eps_floor, -3.0);
+      for (int c = 0; c < 6; ++c) *g[c] *= oopsi4;
+      const double tr = trace_rank2(1.0, *g[0], *g[1], *g[2], *g[3], *g[4], *g[5],
+                                    *A[0], *A[1], *A[2], *A[3], *A[4], *A[5]);
+      for (int c = 0; c < 6; ++c) *A[c] -= (1.0 / 3.0) * tr * *g[c];
+    }
+  }
+  if (opt->force_regularization) {
+    double *chi = V(u, Z4C_CHI) + p, *alpha = V(u, Z4C_ALPHA) + p;
+    *chi = dmax(*chi, opt->eps_floor);
+    *alpha = regularize_near_zero(*alpha, opt->eps_floor);
+  }
+}
+
+void orc_algconstr(const orc_block_t *b, const z4c_params_t *opt, double *u) {
+  const int64_t nvol = orc_nvol(b);
+  for (int64_t p = 0; p < nvol; ++p) algconstr_point(opt, u, nvol, p);
+}
+
+void orc_algconstr_ghosts(const orc_block_t *b, const z4c_params_t *opt, double *u) {
+  fd_t f;
+  fd_init(b, &f);
+  const int64_t nvol = orc_nvol(b);
+  for (int k = 0; k < f.nn3; ++k)
+    for (int j = 0; j < f.nn2; ++j)
+      for (int i = 0; i < f.nn1; ++i) {
+        const int interior = (k >= f.kl && k <= f.ku && j >= f.jl && j <= f.ju &&
+                              i >= f.il && i <= f.iu);
+        if (!interior) algconstr_point(opt, u, nvol, P(k, j, i));
+      }
+}
+
+/* ---- Z4c::Z4cToADM, adm_z4c.cpp:200-260 --------------------------------- */
+static void z4c_to_adm_point(const z4c_params_t *opt, const double *u, double *adm,
+                             int64_t nvol, int64_t p) {
+  V(adm, Z4C_ADM_ALPHA)[p] = V(u, Z4C_ALPHA)[p];
+  for (int a = 0; a < 3; ++a) V(adm, Z4C_ADM_BETAX + a)[p] = V(u, Z4C_BETAX + a)[p];
+  double psi4;
+  if (opt->chi_psi_power == -4.) psi4 = 1.0 / V(u, Z4C_CHI)[p];
+  else psi4 = pow(V(u, Z4C_CHI)[p], 4. / opt->chi_psi_power);
+  V(adm, Z4C_ADM_PSI4)[p] = psi4;
+  for (int c = 0; c < 6; ++c)
+    V(adm, Z4C_ADM_GXX + c)[p] = psi4 * V(u, Z4C_GXX + c)[p];
+  for (int c = 0; c < 6; ++c)
+    V(adm, Z4C_ADM_KXX + c)[p] =
+        psi4 * V(u, Z4C_AXX + c)[p] +
+        (1. / 3.) * (V(u, Z4C_KHAT)[p] + 2. * V(u, Z4C_THETA)[p]) * V(adm, Z4C_ADM_GXX + c)[p];
+}
+
+void orc_z4c_to_adm(const orc_block_t *b, const z4c_params_t *opt, const double *u,
+                    double *adm) {
+  const int64_t nvol = orc_nvol(b);
+  for (int64_t p = 0; p < nvol; ++p) z4c_to_adm_point(opt, u, adm, nvol, p);
+}
+
+void orc_z4c_to_adm_ghosts(const orc_block_t *b, const z4c_params_t *opt,
+                           const double *u, double *adm) {
+  fd_t f;
+  fd_init(b, &f);
+  const int64_t nvol = orc_nvol(b);
+  for (int k = 0; k < f.nn3; ++k)
+    for (int j = 0; j < f.nn2; ++j)
+      for (int i = 0; i < f.nn1; ++i) {
+        const int interior = (k >= f.kl && k <= f.ku && j >= f.jl && j <= f.ju &&
+                              i >= f.il && i <= f.iu);
+        if (!interior) z4c_to_adm_point(opt, u, adm, nvol, P(k, j, i));
+      }
+}
+
+/* ---- Z4c::ADMToZ4c, adm_z4c.cpp:46-192 ---------------------------------- */
+void orc_adm_to_z4c(const orc_block_t *b, const z4c_params_t *opt, const double *adm,
+                    double *u) {
+  fd_t f;
+  fd_init(b, &f);
+  const int64_t nvol = orc_nvol(b);
+  for (int64_t p = 0; p < nvol; ++p) {
+    V(u, Z4C_ALPHA)[p] = V(adm, Z4C_ADM_ALPHA)[p];
+    for (int a = 0; a < 3; ++a) V(u, Z4C_BETAX + a)[p] = V(adm, Z4C_ADM_BETAX + a)[p];
+    const double *G[6], *Kd[6];
+    for (int c = 0; c < 6; ++c) {
+      G[c] = V(adm, Z4C_ADM_GXX + c) + p;
+      Kd[c] = V(adm, Z4C_ADM_KXX + c) + p;
+    }
+    double detg = det3(*G[0], *G[1], *G[2], *G[3], *G[4], *G[5]);
+    double oopsi4;
+    if (opt->chi_psi_power == -4.) {
+      oopsi4 = cbrt(1.0 / detg);
+      V(u, Z4C_CHI)[p] = oopsi4;
+    } else {
+      oopsi4 = pow(detg, -1. / 3.);
+      V(u, Z4C_CHI)[p] = pow(detg, 1. / 12. * opt->chi_psi_power);
+    }
+    double Kt[6];
+    for (int c = 0; c < 6; ++c) {
+      V(u, Z4C_GXX + c)[p] = oopsi4 * *G[c];
+      Kt[c] = oopsi4 * *Kd[c];
+    }
+    double g[6];
+    for (int c = 0; c < 6; ++c) g[c] = V(u, Z4C_GXX + c)[p];
+    detg = det3(g[0], g[1], g[2], g[3], g[4], g[5]);
+    const double Khat = trace_rank2(1.0 / detg, g[0], g[1], g[2], g[3], g[4], g[5],
+                                    Kt[0], Kt[1], Kt[2], Kt[3], Kt[4], Kt[5]);
+    V(u, Z4C_KHAT)[p] = Khat;
+    for (int c = 0; c < 6; ++c) V(u, Z4C_AXX + c)[p] = Kt[c] - (1. / 3.) * Khat * g[c];
+  }
+  /* inverse conformal metric on all points, :146-163 */
+  double *guu = (double *)malloc(sizeof(double) * 6 * (size_t)nvol);
+  for (int64_t p = 0; p < nvol; ++p) {
+    double g[6], gu[3][3];
+    for (int c = 0; c < 6; ++c) g[c] = V(u, Z4C_GXX + c)[p];
+    const double detg = det3(g[0], g[1], g[2], g[3], g[4], g[5]);
+    inv3(1.0 / detg, g[0], g[1], g[2], g[3], g[4], g[5], gu);
+    for (int a = 0; a < 3; ++a)
+      for (int c = a; c < 3; ++c) guu[SI[a][c] * nvol + p] = gu[a][c];
+  }
+  /* Gammas, interior only, :166-176 */
+  for (int a = 0; a < 3; ++a) memset(V(u, Z4C_GAMX + a), 0, sizeof(double) * (size_t)nvol);
+  for (int k = f.kl; k <= f.ku; ++k)
+    for (int j = f.jl; j <= f.ju; ++j)
+      for (int a = 0; a < 3; ++a)
+        for (int bb = 0; bb < 3; ++bb)
+          for (int i = f.il; i <= f.iu; ++i) {
+            const int64_t p = P(k, j, i);
+            V(u, Z4C_GAMX + a)[p] -= Dx(&f, bb, guu + SI[bb][a] * nvol + p);
+          }
+  free(guu);
+  memset(V(u, Z4C_THETA), 0, sizeof(double) * (size_t)nvol);
+  orc_algconstr(b, opt, u);
+}
+
+/* ---- Z4c::ADMConstraints, adm_z4c.cpp:382-930 --------------------------- */
+void orc_adm_constraints(const orc_block_t *b, const z4c_params_t *opt,
+                         const double *adm, const double *u, const orc_derivs_t *D,
+                         double *con) {
+  fd_t f;
+  fd_init(b, &f);
+  const int64_t nvol = orc_nvol(b);
+  memset(con, 0, sizeof(double) * Z4C_NCON * (size_t)nvol);
+  const double pw = opt->chi_psi_power;
+  const double rho = 0.0, S_d[3] = {0, 0, 0};
+  const double r2_max = opt->r_max_con * opt->r_max_con;
+
+  for (int k = f.kl; k <= f.ku; ++k)
+    for (int j = f.jl; j <= f.ju; ++j)
+      for (int i = f.il; i <= f.iu; ++i) {
+        const int64_t p = P(k, j, i);
+        double ddchi_dd[3][3];
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb)
+            ddchi_dd[a][bb] = ddchi_dd[bb][a] = D->ddchi[SI[a][bb]][p];
+        const double chi = V(u, Z4C_CHI)[p];
+        const double chi_g = dmax(chi, opt->chi_div_floor);
+        const double oochi = 1.0 / chi_g;
+        double psi4c = 0.0;
+        if (pw != -4.) psi4c = pow(chi_g, 4.0 / pw);
+
+        double gt[3][3], Kd[3][3], gph[3][3];
+        for (int a = 0; a < 3; ++a)
+          for (int c = 0; c < 3; ++c) {
+            gt[a][c] = V(u, Z4C_GXX + SI[a][c])[p];
+            Kd[a][c] = V(adm, Z4C_ADM_KXX + SI[a][c])[p];
+            gph[a][c] = V(adm, Z4C_ADM_GXX + SI[a][c])[p];
+          }
+        double dg_ddd[3][3][3], dK_ddd[3][3][3], ddg_dddd[3][3][3][3];
+        /* pass 1, :446-460 / :532-546 */
+        for (int c = 0; c < 3; ++c)
+          for (int a = 0; a < 3; ++a)
+            for (int bb = a; bb < 3; ++bb) {
+              const double dg3 = D->dg[c][SI[a][bb]][p];
+              double v;
+              if (pw == -4.)
+                v = oochi * (dg3 - oochi * gt[a][bb] * D->dchi[c][p]);
+              else
+                v = psi4c * (dg3 + (4.0 / pw) * oochi * gt[a][bb] * D->dchi[c][p]);
+              dg_ddd[c][a][bb] = dg_ddd[c][bb][a] = v;
+              dK_ddd[c][a][bb] = dK_ddd[c][bb][a] =
+                  Dx(&f, c, V(adm, Z4C_ADM_KXX + SI[a][bb]) + p);
+            }
+        /* pass 2, :463-520 / :549-596 */
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb)
+            for (int c = 0; c < 3; ++c)
+              for (int dd = c; dd < 3; ++dd) {
+                const double dchi_a = D->dchi[a][p], dchi_b = D->dchi[bb][p];
+                const double gtil = gt[c][dd];
+                double v;
+                if (a == bb) {
+                  const double ddg_conf = Dxx(&f, a, V(u, Z4C_GXX + SI[c][dd]) + p);
+                  const double dg3 = D->dg[a][SI[c][dd]][p];
+                  if (pw == -4.)
+                    v = oochi * (ddg_conf - oochi * (2.0 * dchi_a * dg3 + ddchi_dd[a][a] * gtil) +
+                                 2.0 * oochi * oochi * dchi_a * dchi_a * gtil);
+                  else {
+                    const double fac = 4.0 / pw, fac2 = fac - 1.0;
+                    v = psi4c * (ddg_conf + fac * oochi * (2.0 * dchi_a * dg3 + ddchi_dd[a][a] * gtil) +
+                                 fac * fac2 * oochi * oochi * dchi_a * dchi_a * gtil);
+                  }
+                } else {
+                  const double ddg_conf = Dx(&f, a, D->dg[bb][SI[c][dd]] + p);
+                  const double dgb = D->dg[bb][SI[c][dd]][p], dga = D->dg[a][SI[c][dd]][p];
+                  if (pw == -4.)
+                    v = oochi * (ddg_conf -
+                                 oochi * (dchi_a * dgb + dchi_b * dga + ddchi_dd[a][bb] * gtil) +
+                                 2.0 * oochi * oochi * dchi_a * dchi_b * gtil);
+                  else {
+                    const double fac = 4.0 / pw, fac2 = fac - 1.0;
+                    v = psi4c * (ddg_conf +
+                                 fac * oochi * (dchi_a * dgb + dchi_b * dga + ddchi_dd[a][bb] * gtil) +
+                                 fac * fac2 * oochi * oochi * dchi_a * dchi_b * gtil);
+                  }
+                }
+                ddg_dddd[a][bb][c][dd] = ddg_dddd[bb][a][c][dd] =
+                    ddg_dddd[a][bb][dd][c] = ddg_dddd[bb][a][dd][c] = v;
+              }
+        /* inverse physical metric, :601-618 */
+        double g_uu[3][3];
+        {
+          const double detg = det3(gph[0][0], gph[0][1], gph[0][2], gph[1][1], gph[1][2], gph[2][2]);
+          inv3(1. / detg, gph[0][0], gph[0][1], gph[0][2], gph[1][1], gph[1][2], gph[2][2], g_uu);
+        }
+        double Gamma_ddd[3][3][3], Gamma_udd[3][3][3];
+        for (int c = 0; c < 3; ++c)
+          for (int a = 0; a < 3; ++a)
+            for (int bb = a; bb < 3; ++bb)
+              Gamma_ddd[c][a][bb] = Gamma_ddd[c][bb][a] =
+                  0.5 * (dg_ddd[a][bb][c] + dg_ddd[bb][a][c] - dg_ddd[c][a][bb]);
+        for (int c = 0; c < 3; ++c)
+          for (int a = 0; a < 3; ++a)
+            for (int bb = a; bb < 3; ++bb) {
+              double s = 0;
+              for (int dd = 0; dd < 3; ++dd) s += g_uu[c][dd] * Gamma_ddd[dd][a][bb];
+              Gamma_udd[c][a][bb] = Gamma_udd[c][bb][a] = s;
+            }
+        /* Ricci tensor and scalar, :655-689 */
+        double R = 0, R_dd[3][3];
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb) {
+            double s = 0;
+            for (int c = 0; c < 3; ++c)
+              for (int dd = 0; dd < 3; ++dd)
+                for (int ff = 0; ff < 3; ++ff)
+                  s += g_uu[dd][ff] * (Gamma_udd[c][a][ff] * Gamma_ddd[c][bb][dd] -
+                                       Gamma_udd[c][a][bb] * Gamma_ddd[c][ff][dd]);
+            for (int c = 0; c < 3; ++c)
+              for (int dd = 0; dd < 3; ++dd)
+                s += 0.5 * g_uu[c][dd] *
+                     (-ddg_dddd[bb][a][c][dd] + ddg_dddd[dd][a][bb][c] +
+                      ddg_dddd[dd][bb][a][c] - ddg_dddd[dd][c][a][bb]);
+            R_dd[a][bb] = R_dd[bb][a] = s;
+            R += ((a == bb) ? 1.0 : 2.0) * g_uu[a][bb] * R_dd[a][bb];
+          }
+        /* extrinsic curvature, :694-753 */
+        double K = 0, K_ud[3][3] = {{0}}, KK = 0;
+        for (int a = 0; a < 3; ++a) {
+          for (int bb = 0; bb < 3; ++bb)
+            for (int c = 0; c < 3; ++c) K_ud[a][bb] += g_uu[a][c] * Kd[c][bb];
+          K += K_ud[a][a];
+        }
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb) KK += K_ud[a][bb] * K_ud[bb][a];
+        double DK_ddd[3][3][3], DK_udd[3][3][3];
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb)
+            for (int c = bb; c < 3; ++c) {
+              double v = dK_ddd[a][bb][c];
+              for (int dd = 0; dd < 3; ++dd) {
+                v -= Gamma_udd[dd][a][bb] * Kd[dd][c];
+                v -= Gamma_udd[dd][a][c] * Kd[bb][dd];
+              }
+              DK_ddd[a][bb][c] = DK_ddd[a][c][bb] = v;
+            }
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb)
+            for (int c = bb; c < 3; ++c) {
+              double s = 0;
+              for (int dd = 0; dd < 3; ++dd) s += g_uu[a][dd] * DK_ddd[dd][bb][c];
+              DK_udd[a][bb][c] = DK_udd[a][c][bb] = s;
+            }
+        /* constraints, :760-814 */
+        const double H = R + (K * K) - KK - 16 * M_PI * rho;
+        double M_u[3] = {0, 0, 0};
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb) {
+            M_u[a] -= 8 * M_PI * g_uu[a][bb] * S_d[bb];
+            for (int c = 0; c < 3; ++c) {
+              M_u[a] += g_uu[a][bb] * DK_udd[c][bb][c];
+              M_u[a] -= g_uu[bb][c] * DK_udd[a][bb][c];
+            }
+          }
+        double M_d[3];
+        for (int a = 0; a < 3; ++a) {
+          M_d[a] = 0;
+          for (int bb = 0; bb < 3; ++bb) M_d[a] += gph[a][bb] * M_u[bb];
+        }
+        double M = 0.;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb)
+            M += ((a == bb) ? 1.0 : 2.0) * gph[a][bb] * M_u[a] * M_u[bb];
+        /* conformal connection functions for Z, :819-906 */
+        double gc_uu[3][3];
+        {
+          const double detg = det3(gt[0][0], gt[0][1], gt[0][2], gt[1][1], gt[1][2], gt[2][2]);
+          inv3(1. / detg, gt[0][0], gt[0][1], gt[0][2], gt[1][1], gt[1][2], gt[2][2], gc_uu);
+        }
+        double cG_ddd[3][3][3], cG_udd[3][3][3], cG_u[3];
+        for (int c = 0; c < 3; ++c)
+          for (int a = 0; a < 3; ++a)
+            for (int bb = a; bb < 3; ++bb) {
+              const double d1 = D->dg[a][SI[bb][c]][p], d2 = D->dg[bb][SI[a][c]][p],
+                           d3 = D->dg[c][SI[a][bb]][p];
+              cG_ddd[c][a][bb] = cG_ddd[c][bb][a] = 0.5 * (d1 + d2 - d3);
+            }
+        for (int c = 0; c < 3; ++c)
+          for (int a = 0; a < 3; ++a)
+            for (int bb = a; bb < 3; ++bb) {
+              double s = 0;
+              for (int dd = 0; dd < 3; ++dd) s += gc_uu[c][dd] * cG_ddd[dd][a][bb];
+              cG_udd[c][a][bb] = cG_udd[c][bb][a] = s;
+            }
+        for (int a = 0; a < 3; ++a) {
+          double s = 0;
+          for (int bb = 0; bb < 3; ++bb)
+            for (int c = bb; c < 3; ++c)
+              s += ((bb == c) ? 1.0 : 2.0) * gc_uu[bb][c] * cG_udd[a][bb][c];
+          cG_u[a] = s;
+        }
+        double Z = 0.;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb)
+            Z += ((a == bb) ? 0.25 : 0.5) * gph[a][bb] *
+                 (V(u, Z4C_GAMX + a)[p] - cG_u[a]) * (V(u, Z4C_GAMX + bb)[p] - cG_u[bb]);
+        /* radius cut + C, :908-928 */
+        const double x1 = b->x[0][i], x2 = b->x[1][j], x3 = b->x[2][k];
+        const double R2 = x1 * x1 + x2 * x2 + x3 * x3;
+        if (R2 > r2_max) {
+          /* all zero already */
+        } else {
+          const double Theta = V(u, Z4C_THETA)[p];
+          V(con, Z4C_CON_H)[p] = H;
+          V(con, Z4C_CON_M)[p] = M;
+          V(con, Z4C_CON_Z)[p] = Z;
+          for (int a = 0; a < 3; ++a) V(con, Z4C_CON_MX + a)[p] = M_d[a];
+          V(con, Z4C_CON_C)[p] = (H * H) + M + (Theta * Theta) + 4.0 * Z;
+        }
+      }
+}
+
+/* ---- uniform-mesh ghost exchange and physical BCs ------------------------ */
+
+/* Neighbour directions in the order MeshBlock::SearchAndSetNeighbors lists
+ * them (mesh/mesh_topology.cpp:329-960): x1, x2, x3 faces, then x1x2, x1x3,
+ * x2x3 edges, then corners, each with the first offset varying fastest.  The
+ * additive unpack (comm_channel.cpp:990+, comm_registry.cpp:1006+) adds the
+ * neighbours' contributions in this order. */
+static int neighbour_dirs(int dirs[26][3]) {
+  int n = 0;
+  for (int s = -1; s <= 1; s += 2) { dirs[n][0] = s; dirs[n][1] = 0; dirs[n][2] = 0; ++n; }
+  for (int s = -1; s <= 1; s += 2) { dirs[n][0] = 0; dirs[n][1] = s; dirs[n][2] = 0; ++n; }
+  for (int s = -1; s <= 1; s += 2) { dirs[n][0] = 0; dirs[n][1] = 0; dirs[n][2] = s; ++n; }
+  for (int m = -1; m <= 1; m += 2)
+    for (int s = -1; s <= 1; s += 2) { dirs[n][0] = s; dirs[n][1] = m; dirs[n][2] = 0; ++n; }
+  for (int m = -1; m <= 1; m += 2)
+    for (int s = -1; s <= 1; s += 2) { dirs[n][0] = s; dirs[n][1] = 0; dirs[n][2] = m; ++n; }
+  for (int m = -1; m <= 1; m += 2)
+    for (int s = -1; s <= 1; s += 2) { dirs[n][0] = 0; dirs[n][1] = s; dirs[n][2] = m; ++n; }
+  for (int l = -1; l <= 1; l += 2)
+    for (int m = -1; m <= 1; m += 2)
+      for (int s = -1; s <= 1; s += 2) { dirs[n][0] = s; dirs[n][1] = m; dirs[n][2] = l; ++n; }
+  return n;
+}
+
+void orc_mesh_exchange(const orc_mesh_t *m, int nvar, double *u_all) {
+  const int nn[3] = {m->nx[0] + 1 + 2 * NG, m->nx[1] + 1 + 2 * NG, m->nx[2] + 1 + 2 * NG};
+  const int64_t nvol = (int64_t)nn[0] * nn[1] * nn[2];
+  const int nblocks = m->nb[0] * m->nb[1] * m->nb[2];
+  const int64_t bstride = nvol * nvar;
+  int dirs[26][3];
+  neighbour_dirs(dirs);
+  /* every block unpacks from the pre-exchange state of its neighbours */
+  double *out = (double *)malloc(sizeof(double) * (size_t)bstride * nblocks);
+  memcpy(out, u_all, sizeof(double) * (size_t)bstride * nblocks);
+  for (int bl = 0; bl < nblocks; ++bl) {
+    const int loc[3] = {bl % m->nb[0], (bl / m->nb[0]) % m->nb[1], bl / (m->nb[0] * m->nb[1])};
+    /* neighbour block of each direction, -1 beyond a non-periodic face */
+    int nbr[26];
+    for (int d = 0; d < 26; ++d) {
+      int l[3], ok = 1;
+      for (int a = 0; a < 3; ++a) {
+        l[a] = loc[a] + dirs[d][a];
+        if (l[a] < 0 || l[a] >= m->nb[a]) {
+          if (m->bc[2 * a] == Z4C_BC_PERIODIC) l[a] = (l[a] + m->nb[a]) % m->nb[a];
+          else ok = 0;
+        }
+      }
+      nbr[d] = ok ? l[0] + m->nb[0] * (l[1] + m->nb[1] * l[2]) : -1;
+    }
+    for (int k = 0; k < nn[2]; ++k)
+      for (int j = 0; j < nn[1]; ++j)
+        for (int i = 0; i < nn[0]; ++i) {
+          const int idx[3] = {i, j, k};
+          int interior = 1, on_edge = 0;
+          for (int a = 0; a < 3; ++a) {
+            const int vs = NG, ve = NG + m->nx[a];
+            if (idx[a] < vs || idx[a] > ve) interior = 0;
+            if (idx[a] <= vs || idx[a] >= ve) on_edge = 1;
+          }
+          if (!on_edge) continue; /* strictly interior: untouched */
+          /* SetRangeVC (index_utilities.hpp:155-163) coverage per direction */
+          int cov[26], mult = interior ? 1 : 0;
+          for (int d = 0; d < 26; ++d) {
+            cov[d] = (nbr[d] >= 0);
+            for (int a = 0; a < 3 && cov[d]; ++a) {
+              const int vs = NG, ve = NG + m->nx[a], o = dirs[d][a];
+              if (o > 0) cov[d] = (idx[a] >= ve);
+              else if (o < 0) cov[d] = (idx[a] <= vs);
+              else cov[d] = (idx[a] >= vs && idx[a] <= ve);
+            }
+            mult += cov[d];
+          }
+          const int64_t p = ((int64_t)k * nn[1] + j) * nn[0] + i;
+          for (int n = 0; n < nvar; ++n) {
+            double s = interior ? u_all[bl * bstride + n * nvol + p] : 0.0;
+            for (int d = 0; d < 26; ++d) {
+              if (!cov[d]) continue;
+              const int64_t q = ((int64_t)(k - dirs[d][2] * m->nx[2]) * nn[1] +
+                                 (j - dirs[d][1] * m->nx[1])) * nn[0] +
+                                (i - dirs[d][0] * m->nx[0]);
+              s += u_all[(int64_t)nbr[d] * bstride + n * nvol + q];
+            }
+            if (mult > 1) s *= 1.0 / (double)mult;
+            out[bl * bstride + n * nvol + p] = s;
+          }
+        }
+  }
+  memcpy(u_all, out, sizeof(double) * (size_t)bstride * nblocks);
+  free(out);
+  for (int bl = 0; bl < nblocks; ++bl) {
+    const int loc[3] = {bl % m->nb[0], (bl / m->nb[0]) % m->nb[1], bl / (m->nb[0] * m->nb[1])};
+    orc_block_physical_bcs(m, loc, nvar, u_all + bl * bstride);
+  }
+}
+
+/* ExtrapolateOutflowBC with NEXTRAPOLATE=5 (physical_bcs.cpp:187-260); the
+ * index ranges follow ApplyPhysicalBCs (:506-670), which uses the
+ * cell-centred interior end ie = is + nx - 1 also for vertex data. */
+static const double CE[5] = {5., -10., 10., -5., 1.};
+
+void orc_block_physical_bcs(const orc_mesh_t *m, const int loc[3], int nvar, double *u) {
+  const int nn[3] = {m->nx[0] + 1 + 2 * NG, m->nx[1] + 1 + 2 * NG, m->nx[2] + 1 + 2 * NG};
+  const int64_t nvol = (int64_t)nn[0] * nn[1] * nn[2];
+  const int64_t st[3] = {1, nn[0], (int64_t)nn[0] * nn[1]};
+  int need[6];
+  for (int a = 0; a < 3; ++a) {
+    need[2 * a] = (m->bc[2 * a] == Z4C_BC_OUTFLOW) && loc[a] == 0;
+    need[2 * a + 1] = (m->bc[2 * a + 1] == Z4C_BC_OUTFLOW) && loc[a] == m->nb[a] - 1;
+  }
+  int is[3], ie[3];
+  for (int a = 0; a < 3; ++a) { is[a] = NG; ie[a] = NG + m->nx[a] - 1; }
+  /* transverse limits, :516-528 */
+  int bis = is[0] - NG, bie = ie[0] + NG;
+  int bjs = is[1], bje = ie[1], bks = is[2], bke = ie[2];
+  if (!need[2]) bjs = is[1] - NG;
+  if (!need[3]) bje = ie[1] + NG;
+  if (!need[4]) bks = is[2] - NG;
+  if (!need[5]) bke = ie[2] + NG;
+  for (int face = 0; face < 6; ++face) {
+    if (!need[face]) continue;
+    const int ax = face / 2, outer = face % 2;
+    int lo[3], hi[3];
+    if (ax == 0) { lo[1] = bjs; hi[1] = bje; lo[2] = bks; hi[2] = bke; }
+    else if (ax == 1) { lo[0] = bis; hi[0] = bie; lo[2] = bks; hi[2] = bke; }
+    else { lo[0] = bis; hi[0] = bie; lo[1] = is[1] - NG; hi[1] = ie[1] + NG; }
+    /* the x3 faces use the extended j range, :619-621 */
+    const int o1 = (ax + 1) % 3, o2 = (ax + 2) % 3;
+    for (int n = 0; n < nvar; ++n)
+      for (int t2 = lo[o2]; t2 <= hi[o2]; ++t2)
+        for (int t1 = lo[o1]; t1 <= hi[o1]; ++t1)
+          for (int g = 1; g <= NG; ++g) {
+            const int ia = outer ? ie[ax] + g : is[ax] - g;
+            const int dir = outer ? -1 : 1;
+            int64_t p = (int64_t)ia * st[ax] + (int64_t)t1 * st[o1] + (int64_t)t2 * st[o2];
+            double v = 0.0;
+            for (int q = 0; q < 5; ++q) v += CE[q] * u[n * nvol + p + dir * (q + 1) * st[ax]];
+            u[n * nvol + p] = v;
+          }
+  }
+}
+
+/* ---- history sums, outputs/history.cpp:168-200 --------------------------- */
+void orc_hst_accumulate(const orc_block_t *b, const z4c_params_t *opt,
+                        const double *con, const double *u, double out[8]) {
+  fd_t f;
+  fd_init(b, &f);
+  const int64_t nvol = orc_nvol(b);
+  const double r2_max = opt->r_max_con * opt->r_max_con;
+  for (int k = NG; k <= NG + b->nx[2] - 1; ++k)
+    for (int j = NG; j <= NG + b->nx[1] - 1; ++j)
+      for (int i = NG; i <= NG + b->nx[0] - 1; ++i) {
+        const double vol = b->dx[0] * b->dx[1] * b->dx[2];
+        const double x1 = b->xc[0][i], x2 = b->xc[1][j], x3 = b->xc[2][k];
+        const double R2 = x1 * x1 + x2 * x2 + x3 * x3;
+        if (!(R2 <= r2_max)) continue;
+        const int64_t p = P(k, j, i);
+        const double H = fabs(V(con, Z4C_CON_H)[p]);
+        out[0] += vol * (H * H);
+        out[1] += vol * fabs(V(con, Z4C_CON_M)[p]);
+        for (int a = 0; a < 3; ++a) {
+          const double m = fabs(V(con, Z4C_CON_MX + a)[p]);
+          out[2 + a] += vol * (m * m);
+        }
+        out[5] += vol * fabs(V(con, Z4C_CON_Z)[p]);
+        const double th = fabs(V(u, Z4C_THETA)[p]);
+        out[6] += vol * (th * th);
+        out[7] += vol * fabs(V(con, Z4C_CON_C)[p]);
+      }
+}

@@ -1,0 +1,108 @@
+/* CPU restatement of the GR-Athena++ Z4c hot path: the parity oracle.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / reference arms of bench.py may load this library, and only
+ * as the checker or the timed CPU baseline; the product path never calls it.
+ *
+ * Every function follows the reference file:line cited beside it, including
+ * its floating-point evaluation order, so that agreement with the reference
+ * CPU build is at the level of rounding (pinned by tests/golden, whose
+ * fixtures come from the reference itself built by oracle/ref).
+ *
+ * Layout (all arrays): one MeshBlock is [var][k][j][i], i fastest, with
+ * nn = nx + 1 + 2*ng vertices per axis (vertex-centred, ng = 4).
+ */
+#ifndef Z4C_ORACLE_H
+#define Z4C_ORACLE_H
+
+#include <stdint.h>
+
+#include "../include/z4c_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_NG 4
+
+/* Geometry of one vertex-centred MeshBlock. */
+typedef struct {
+  int nx[3];          /* interior cells per axis */
+  double dx[3];       /* grid spacing (the reference's dx?f(0)) */
+  const double *x[3]; /* vertex coordinates, nn[a] entries (the reference's x?f) */
+  const double *xc[3];/* cell-centre coordinates, nn[a]-1 entries (x?v) */
+} orc_block_t;
+
+/* Stored first derivatives used by the RHS and the constraints, computed by
+ * orc_prepare_derivs (adm_z4c.cpp:972-1037).  Each array holds nvol values. */
+typedef struct {
+  double *dalpha[3];      /* d_b alpha */
+  double *dchi[3];        /* d_b chi */
+  double *dbeta[3][3];    /* [b][c] d_b beta^c */
+  double *dg[3][6];       /* [b][cd] d_b g~_cd, cd in xx,xy,xz,yy,yz,zz order */
+  double *ddchi[6];       /* d_a d_b chi (interior only) */
+} orc_derivs_t;
+
+int64_t orc_nvol(const orc_block_t *b);
+/* Allocates / frees the stored-derivative arrays of one block. */
+int orc_derivs_alloc(const orc_block_t *b, orc_derivs_t *d);
+void orc_derivs_free(orc_derivs_t *d);
+
+/* Z4c::PrepareZ4cDerivatives, adm_z4c.cpp:972-1037. */
+void orc_prepare_derivs(const orc_block_t *b, const double *u, orc_derivs_t *d);
+/* Z4c::Z4cRHS, calculate_z4c_rhs.cpp:29-916 (constant-eta branch, vacuum:
+ * matter terms are evaluated with zero matter fields).  Writes the interior of
+ * rhs only.  Requires orc_prepare_derivs(u) first. */
+void orc_rhs(const orc_block_t *b, const z4c_params_t *p, const double *u,
+             const orc_derivs_t *d, double *rhs);
+/* Z4c::AlgConstr, z4c.cpp:677-799: all points, in place. */
+void orc_algconstr(const orc_block_t *b, const z4c_params_t *p, double *u);
+/* Z4c::AlgConstr ranged variant with skip_physical, z4c.cpp:801-991:
+ * every point outside the interior [vs..ve]^3. */
+void orc_algconstr_ghosts(const orc_block_t *b, const z4c_params_t *p, double *u);
+/* Z4c::Z4cToADM, adm_z4c.cpp:200-260: all points.  adm has 17 variables. */
+void orc_z4c_to_adm(const orc_block_t *b, const z4c_params_t *p, const double *u,
+                    double *adm);
+/* Z4c::Z4cToADM ranged variant with skip_physical (ghosts only), :262-365. */
+void orc_z4c_to_adm_ghosts(const orc_block_t *b, const z4c_params_t *p,
+                           const double *u, double *adm);
+/* Z4c::ADMToZ4c, adm_z4c.cpp:46-192 (then AlgConstr).  u is fully written
+ * (Gamma^i zero outside the interior). */
+void orc_adm_to_z4c(const orc_block_t *b, const z4c_params_t *p, const double *adm,
+                    double *u);
+/* Z4c::ADMConstraints, adm_z4c.cpp:382-930 (vacuum).  con (7 variables) is
+ * zeroed then written on the interior.  Requires orc_prepare_derivs(u). */
+void orc_adm_constraints(const orc_block_t *b, const z4c_params_t *p,
+                         const double *adm, const double *u, const orc_derivs_t *d,
+                         double *con);
+
+/* ---- uniform block grid (single level) ---------------------------------- */
+
+/* A uniform mesh of nb[0]*nb[1]*nb[2] blocks, block (l0,l1,l2) at index
+ * l0 + nb0*(l1 + nb1*l2) of the arrays.  bc[face] = Z4C_BC_PERIODIC or
+ * Z4C_BC_OUTFLOW for faces inner_x1, outer_x1, inner_x2, ... */
+typedef struct {
+  int nb[3];
+  int nx[3];
+  int bc[6];
+} orc_mesh_t;
+
+/* Same-level vertex-centred ghost exchange (comm_registry.cpp:336-382,
+ * node_multiplicity.cpp:102-430, index_utilities.hpp:124-170): every ghost
+ * and every block-boundary vertex becomes the mean over all blocks whose
+ * interior holds that vertex; then the physical boundary conditions
+ * (physical_bcs.cpp:187-260, 506-670).  nvar variables per block. */
+void orc_mesh_exchange(const orc_mesh_t *m, int nvar, double *u_all);
+/* Only the physical boundary conditions of one block (extrapolate_outflow). */
+void orc_block_physical_bcs(const orc_mesh_t *m, const int loc[3], int nvar,
+                            double *u);
+
+/* History-output sums (outputs/history.cpp:168-200) over the cell range of one
+ * block: out[8] += {H^2, M, Mx^2, My^2, Mz^2, Z, Theta^2, C} * vol. */
+void orc_hst_accumulate(const orc_block_t *b, const z4c_params_t *p,
+                        const double *con, const double *u, double out[8]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
