@@ -1,0 +1,733 @@
+// C ABI of the B200 Z4c path (include/z4c_b200.h): context, device registers,
+// operator launches, stage sequencing and the CUDA-graph-captured step.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/z4c_b200.h"
+#include "z4c_common.cuh"
+#include "z4c_kernels.cuh"
+
+using namespace z4c;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                         \
+  do {                                                                         \
+    cudaError_t e_ = (expr);                                                   \
+    if (e_ != cudaSuccess)                                                     \
+      return fail(Z4C_ECUDA, "%s: %s", #expr, cudaGetErrorString(e_));         \
+  } while (0)
+
+#define LAUNCH_CHECK(what)                                                     \
+  do {                                                                         \
+    cudaError_t e_ = cudaGetLastError();                                       \
+    if (e_ != cudaSuccess)                                                     \
+      return fail(Z4C_ECUDA, "%s launch: %s", what, cudaGetErrorString(e_));   \
+  } while (0)
+
+// Low-storage RK4()4[2S] (task_list_integrators_low_storage.cpp:112-142).
+const double kLsRk4[4][5] = {
+    {1.0, 0.0, 1.0, 0.0, 1.193743905974738},
+    {0.217683334308543, 0.121098479554482, 0.721781678111411, 0.0, 0.099279895495783},
+    {1.065841341361089, -3.843833699660025, 2.121209265338722, 0.0, 1.131678018054042},
+    {0.0, 0.546370891121863, 0.198653035682705, 0.0, 0.310665766509336}};
+// Classical RK4 tableau (task_list_integrators_butcher.cpp:37-48).
+const double kBtA[4][4] = {{0, 0, 0, 0}, {0.5, 0, 0, 0}, {0, 0.5, 0, 0}, {0, 0, 1, 0}};
+const double kBtB[4] = {1. / 6., 1. / 3., 1. / 3., 1. / 6.};
+
+// ComputeMeshGeneratorX with sym_interval (mesh/mesh.hpp:839-863) and
+// UniformMeshGeneratorX1 (mesh/mesh.hpp:939-945).
+double mesh_gen_x(int64_t index, int64_t nrange, double xmin, double xmax) {
+  const int64_t noffset = index - nrange / 2;
+  const int64_t noffset_ceil = index - (nrange + 1) / 2;
+  const double rx = static_cast<double>(noffset + noffset_ceil) / (2.0 * nrange);
+  return 0.5 * (xmin + xmax) + (rx * xmax - rx * xmin);
+}
+
+}  // namespace
+
+struct z4c_ctx {
+  Grid g{};
+  z4c_params_t params{};
+  int integrator = Z4C_INTEG_RK4;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  bool per_block = false;
+  int tile[3] = {128, 1, 1};
+  bool has_outflow = false;
+
+  // device buffers
+  double* reg[Z4C_NREG] = {};
+  double* un = nullptr;   // Butcher u_n scratch
+  double* guu = nullptr;  // ADMToZ4c inverse-metric scratch (6 vars)
+  double* xf = nullptr;   // [nblocks][nn0+nn1+nn2]
+  double* xv = nullptr;   // [nblocks][nn0+nn1+nn2-3]
+  FdScale* fd = nullptr;  // [nblocks]
+  int* nbr = nullptr;     // [nblocks][26]
+  double* partials = nullptr;
+  int* flag = nullptr;
+
+  // host copies
+  std::vector<double> h_xf, h_xv, h_dx;  // h_dx: [nblocks][3]
+
+  // captured step
+  cudaGraphExec_t graph = nullptr;
+  double graph_dt = 0.0;
+  bool graph_per_block = false;
+
+  DevParams dev() const {
+    DevParams P;
+    P.p = params;
+    P.fd = fd;
+    return P;
+  }
+};
+
+namespace {
+
+int reg_nvar_(int reg) {
+  switch (reg) {
+    case Z4C_REG_ADM: return Z4C_NADM;
+    case Z4C_REG_CON: return Z4C_NCON;
+    default: return (reg >= 0 && reg < Z4C_NREG) ? Z4C_NVAR : -1;
+  }
+}
+
+int check_reg(const z4c_ctx* c, int reg) {
+  if (reg < 0 || reg >= Z4C_NREG) return fail(Z4C_EINVAL, "register %d out of range", reg);
+  if (!c->reg[reg])
+    return fail(Z4C_ESTATE, "register %d is not allocated for this integrator", reg);
+  return Z4C_OK;
+}
+
+int check_block(const z4c_ctx* c, int block, int* b0, int* nb) {
+  if (block == -1) {
+    *b0 = 0;
+    *nb = c->g.nblocks;
+    return Z4C_OK;
+  }
+  if (block < 0 || block >= c->g.nblocks)
+    return fail(Z4C_EINVAL, "block %d out of range [0,%d)", block, c->g.nblocks);
+  *b0 = block;
+  *nb = 1;
+  return Z4C_OK;
+}
+
+int64_t reg_elems(const z4c_ctx* c, int reg) { return (int64_t)reg_nvar_(reg) * c->g.nvol * c->g.nblocks; }
+
+// Ghost exchange of a 22-variable register, then the physical BCs; the result
+// lands in `dst` (all points).  With fuse_alg the AlgConstr pass of the task
+// list is folded into the exchange when no physical BC intervenes.
+int exchange_into(z4c_ctx* c, const double* src, double* dst, bool alg) {
+  const DevParams P = c->dev();
+  const bool fuse = alg && !c->has_outflow;
+  launch_exchange(c->g, P, src, dst, Z4C_NVAR, c->nbr, fuse ? 1 : 0, c->stream);
+  LAUNCH_CHECK("exchange");
+  if (c->has_outflow) {
+    launch_physical_bcs(c->g, dst, Z4C_NVAR, c->stream);
+    LAUNCH_CHECK("physical_bcs");
+    if (alg) {
+      launch_alg_constr(c->g, P, dst, 0, c->g.nblocks, c->stream);
+      LAUNCH_CHECK("alg_constr");
+    }
+  }
+  return Z4C_OK;
+}
+
+// One GR_Z4c stage on all blocks.  Batched: fused RHS+KO+stage kernel
+// (u -> w interior), then exchange(+AlgConstr) w -> u.  Per-block: the plain
+// operator sequence with one RHS launch per block.
+int run_stage(z4c_ctx* c, int stage, double dt) {
+  const DevParams P = c->dev();
+  const Grid& g = c->g;
+  double* u = c->reg[Z4C_REG_U];
+  double* w = c->reg[Z4C_REG_W];
+  if (c->integrator == Z4C_INTEG_RK4) {
+    const double* wt = kLsRk4[stage - 1];
+    if (stage == 1) {
+      launch_zero_interior(g, c->reg[Z4C_REG_U1], Z4C_NVAR, c->stream);
+      LAUNCH_CHECK("zero u1");
+    }
+    if (!c->per_block) {
+      LsStage ls{wt[0], wt[1], wt[2], wt[3], wt[4] * dt};
+      launch_stage_ls(g, P, u, c->reg[Z4C_REG_U1], w, ls, 0, g.nblocks, c->stream);
+      LAUNCH_CHECK("stage_ls");
+      return exchange_into(c, w, u, true);
+    }
+    // plain path, every operator launched per block as the task list calls
+    // them: Z4cRHS, WeightedAve x2, AddZ4cRHS; then exchange, AlgConstr
+    const double w1[3] = {1.0, wt[0], 0.0};
+    const double w2[3] = {wt[1], wt[2], wt[3]};
+    for (int b = 0; b < g.nblocks; ++b) {
+      launch_rhs(g, P, u, c->reg[Z4C_REG_RHS], b, 1, c->stream);
+      launch_weighted_ave(g, c->reg[Z4C_REG_U1], u, nullptr, w1, b, 1, c->stream);
+      launch_weighted_ave(g, u, c->reg[Z4C_REG_U1], nullptr, w2, b, 1, c->stream);
+      launch_add_rhs(g, c->reg[Z4C_REG_RHS], wt[4] * dt, u, b, 1, c->stream);
+      LAUNCH_CHECK("per-block stage");
+    }
+    int rc = exchange_into(c, u, w, false);
+    if (rc) return rc;
+    std::swap(c->reg[Z4C_REG_U], c->reg[Z4C_REG_W]);
+    u = c->reg[Z4C_REG_U];
+    for (int b = 0; b < g.nblocks; ++b) {
+      launch_alg_constr(g, P, u, b, 1, c->stream);
+      LAUNCH_CHECK("alg_constr");
+    }
+    return Z4C_OK;
+  }
+  // classical Butcher RK4
+  if (stage == 1) {
+    CUDA_TRY(cudaMemcpyAsync(c->un, u, sizeof(double) * reg_elems(c, Z4C_REG_U),
+                             cudaMemcpyDeviceToDevice, c->stream));
+  }
+  BtStage bs{};
+  if (stage < 4) {
+    for (int q = 0; q < 4; ++q) bs.coef[q] = kBtA[stage][q] * dt;
+    bs.nq = stage + 1;
+  } else {
+    for (int q = 0; q < 4; ++q) bs.coef[q] = kBtB[q] * dt;
+    bs.nq = 4;
+  }
+  bs.kslot = stage - 1;
+  double* K[4] = {c->reg[Z4C_REG_K1], c->reg[Z4C_REG_K2], c->reg[Z4C_REG_K3],
+                  c->reg[Z4C_REG_K4]};
+  if (!c->per_block) {
+    launch_stage_bt(g, P, u, c->un, K, w, bs, 0, g.nblocks, c->stream);
+    LAUNCH_CHECK("stage_bt");
+    return exchange_into(c, w, u, true);
+  }
+  for (int b = 0; b < g.nblocks; ++b) {
+    launch_stage_bt(g, P, u, c->un, K, w, bs, b, 1, c->stream);
+    LAUNCH_CHECK("stage_bt");
+  }
+  int rc = exchange_into(c, w, u, false);
+  if (rc) return rc;
+  for (int b = 0; b < g.nblocks; ++b) {
+    launch_alg_constr(g, P, u, b, 1, c->stream);
+    LAUNCH_CHECK("alg_constr");
+  }
+  return Z4C_OK;
+}
+
+void free_ctx(z4c_ctx* c) {
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  for (auto& r : c->reg)
+    if (r) cudaFree(r);
+  for (void* p : {(void*)c->un, (void*)c->guu, (void*)c->xf, (void*)c->xv, (void*)c->fd,
+                  (void*)c->nbr, (void*)c->partials, (void*)c->flag})
+    if (p) cudaFree(p);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+}  // namespace
+
+extern "C" {
+
+void z4c_params_default(z4c_params_t* p) {
+  p->chi_psi_power = -4.0;
+  p->chi_div_floor = -1000.0;
+  p->diss = 0.0;
+  p->eps_floor = 1e-12;
+  p->damp_kappa1 = 0.0;
+  p->damp_kappa2 = 0.0;
+  p->lapse_oplog = 2.0;
+  p->lapse_harmonicf = 1.0;
+  p->lapse_harmonic = 0.0;
+  p->lapse_advect = 1.0;
+  p->lapse_K = 0.0;
+  p->shift_Gamma = 1.0;
+  p->shift_alpha2Gamma = 0.0;
+  p->shift_H = 0.0;
+  p->shift_advect = 1.0;
+  p->shift_eta = 2.0;
+  p->r_max_con = std::numeric_limits<double>::infinity();
+  p->tf_force_regularization = 1;
+  p->force_regularization = 0;
+}
+
+const char* z4c_last_error(void) { return g_err.c_str(); }
+
+int z4c_reg_nvar(int reg) { return reg_nvar_(reg); }
+
+int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int integrator,
+               z4c_ctx** out) {
+  if (!mesh || !params || !out) return fail(Z4C_EINVAL, "null argument");
+  *out = nullptr;
+  if (integrator != Z4C_INTEG_RK4 && integrator != Z4C_INTEG_BT_RK4)
+    return fail(Z4C_EINVAL, "unknown integrator %d", integrator);
+  for (int a = 0; a < 3; ++a) {
+    if (mesh->nb[a] < 1) return fail(Z4C_EINVAL, "nb[%d] = %d < 1", a, mesh->nb[a]);
+    if (mesh->nx[a] < 2 * Z4C_NG)
+      return fail(Z4C_EINVAL, "nx[%d] = %d below 2*ng = %d", a, mesh->nx[a], 2 * Z4C_NG);
+    if (!(mesh->xmax[a] > mesh->xmin[a])) return fail(Z4C_EINVAL, "empty extent on axis %d", a);
+    const int lo = mesh->bc[2 * a], hi = mesh->bc[2 * a + 1];
+    if ((lo != Z4C_BC_PERIODIC && lo != Z4C_BC_OUTFLOW) ||
+        (hi != Z4C_BC_PERIODIC && hi != Z4C_BC_OUTFLOW))
+      return fail(Z4C_EINVAL, "unknown boundary flag on axis %d", a);
+    if ((lo == Z4C_BC_PERIODIC) != (hi == Z4C_BC_PERIODIC))
+      return fail(Z4C_EINVAL, "axis %d: periodic on one face only", a);
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(Z4C_ENODEV, "no CUDA device");
+  z4c_ctx* c = new (std::nothrow) z4c_ctx();
+  if (!c) return fail(Z4C_ENOMEM, "host allocation");
+  cudaGetDevice(&c->device);
+  c->params = *params;
+  c->integrator = integrator;
+  Grid& g = c->g;
+  for (int a = 0; a < 3; ++a) {
+    g.nb[a] = mesh->nb[a];
+    g.nx[a] = mesh->nx[a];
+    g.nn[a] = mesh->nx[a] + 1 + 2 * Z4C_NG;
+  }
+  for (int f = 0; f < 6; ++f) {
+    g.bc[f] = mesh->bc[f];
+    if (g.bc[f] == Z4C_BC_OUTFLOW) c->has_outflow = true;
+  }
+  g.s[0] = 1;
+  g.s[1] = g.nn[0];
+  g.s[2] = (int64_t)g.nn[0] * g.nn[1];
+  g.nvol = (int64_t)g.nn[0] * g.nn[1] * g.nn[2];
+  g.nblocks = g.nb[0] * g.nb[1] * g.nb[2];
+
+  // block coordinates (coordinates/coordinates.cpp:170-198, cartesian.cpp:29)
+  const int nb = g.nblocks;
+  const int nsum = g.nn[0] + g.nn[1] + g.nn[2];
+  c->h_xf.assign((size_t)nb * nsum, 0.0);
+  c->h_xv.assign((size_t)nb * (nsum - 3), 0.0);
+  c->h_dx.assign((size_t)nb * 3, 0.0);
+  std::vector<FdScale> hfd(nb);
+  const double diss_scaling = std::pow(2, -2 * Z4C_NG) * (Z4C_NG % 2 == 0 ? -1 : 1);
+  for (int b = 0; b < nb; ++b) {
+    const int loc[3] = {b % g.nb[0], (b / g.nb[0]) % g.nb[1], b / (g.nb[0] * g.nb[1])};
+    int off = 0, offv = 0;
+    for (int a = 0; a < 3; ++a) {
+      const int64_t nroot = (int64_t)g.nx[a] * g.nb[a];
+      const double x0 = mesh->xmin[a], x1 = mesh->xmax[a];
+      const double bmin = (loc[a] == 0) ? x0 : mesh_gen_x((int64_t)loc[a] * g.nx[a], nroot, x0, x1);
+      const double bmax = (loc[a] == g.nb[a] - 1)
+                              ? x1 : mesh_gen_x((int64_t)(loc[a] + 1) * g.nx[a], nroot, x0, x1);
+      double* xf = &c->h_xf[(size_t)b * nsum + off];
+      for (int i = 0; i < g.nn[a]; ++i)
+        xf[i] = mesh_gen_x((int64_t)(i - Z4C_NG) + (int64_t)loc[a] * g.nx[a], nroot, x0, x1);
+      xf[Z4C_NG] = bmin;
+      xf[Z4C_NG + g.nx[a]] = bmax;
+      double* xv = &c->h_xv[(size_t)b * (nsum - 3) + offv];
+      for (int i = 0; i < g.nn[a] - 1; ++i) xv[i] = 0.5 * (xf[i + 1] + xf[i]);
+      const double dx = (bmax - bmin) / g.nx[a];
+      c->h_dx[(size_t)b * 3 + a] = dx;
+      hfd[b].cidx1[a] = 1.0 / (dx * 60.0);
+      hfd[b].cidx2[a] = ((1.0 / dx) * (1.0 / dx)) / 180.0;
+      hfd[b].cidxd[a] = diss_scaling / (dx * 1.0);
+      hfd[b].lidx[a] = 1.0 / (dx * 60.0);
+      off += g.nn[a];
+      offv += g.nn[a] - 1;
+    }
+  }
+  // neighbour table in the reference's search order (mesh_topology.cpp:329-960)
+  static const int dirs[26][3] = {
+      {-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1},
+      {-1, -1, 0}, {1, -1, 0}, {-1, 1, 0}, {1, 1, 0},
+      {-1, 0, -1}, {1, 0, -1}, {-1, 0, 1}, {1, 0, 1},
+      {0, -1, -1}, {0, 1, -1}, {0, -1, 1}, {0, 1, 1},
+      {-1, -1, -1}, {1, -1, -1}, {-1, 1, -1}, {1, 1, -1},
+      {-1, -1, 1}, {1, -1, 1}, {-1, 1, 1}, {1, 1, 1}};
+  std::vector<int> hnbr((size_t)nb * 26);
+  for (int b = 0; b < nb; ++b) {
+    const int loc[3] = {b % g.nb[0], (b / g.nb[0]) % g.nb[1], b / (g.nb[0] * g.nb[1])};
+    for (int d = 0; d < 26; ++d) {
+      int l[3];
+      bool ok = true;
+      for (int a = 0; a < 3; ++a) {
+        l[a] = loc[a] + dirs[d][a];
+        if (l[a] < 0 || l[a] >= g.nb[a]) {
+          if (g.bc[2 * a] == Z4C_BC_PERIODIC) l[a] = (l[a] + g.nb[a]) % g.nb[a];
+          else ok = false;
+        }
+      }
+      hnbr[(size_t)b * 26 + d] = ok ? l[0] + g.nb[0] * (l[1] + g.nb[1] * l[2]) : -1;
+    }
+  }
+
+  auto alloc = [&](void** p, size_t bytes) -> int {
+    if (cudaMalloc(p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(Z4C_ENOMEM, "cudaMalloc of %zu bytes failed", bytes);
+    }
+    return Z4C_OK;
+  };
+  int rc = Z4C_OK;
+  const size_t b22 = sizeof(double) * (size_t)Z4C_NVAR * g.nvol * nb;
+  int need[Z4C_NREG] = {};
+  need[Z4C_REG_U] = need[Z4C_REG_W] = need[Z4C_REG_RHS] = need[Z4C_REG_ADM] =
+      need[Z4C_REG_CON] = 1;
+  if (integrator == Z4C_INTEG_RK4) need[Z4C_REG_U1] = 1;
+  else need[Z4C_REG_K1] = need[Z4C_REG_K2] = need[Z4C_REG_K3] = need[Z4C_REG_K4] = 1;
+  for (int r = 0; r < Z4C_NREG && rc == Z4C_OK; ++r) {
+    if (!need[r]) continue;
+    const size_t bytes = sizeof(double) * (size_t)reg_nvar_(r) * g.nvol * nb;
+    rc = alloc((void**)&c->reg[r], bytes);
+    if (rc == Z4C_OK && cudaMemset(c->reg[r], 0, bytes) != cudaSuccess)
+      rc = fail(Z4C_ECUDA, "memset register %d", r);
+  }
+  if (rc == Z4C_OK && integrator == Z4C_INTEG_BT_RK4) rc = alloc((void**)&c->un, b22);
+  if (rc == Z4C_OK) rc = alloc((void**)&c->guu, sizeof(double) * 6 * (size_t)g.nvol * nb);
+  if (rc == Z4C_OK) rc = alloc((void**)&c->xf, sizeof(double) * c->h_xf.size());
+  if (rc == Z4C_OK) rc = alloc((void**)&c->xv, sizeof(double) * c->h_xv.size());
+  if (rc == Z4C_OK) rc = alloc((void**)&c->fd, sizeof(FdScale) * nb);
+  if (rc == Z4C_OK) rc = alloc((void**)&c->nbr, sizeof(int) * hnbr.size());
+  if (rc == Z4C_OK) rc = alloc((void**)&c->partials, sizeof(double) * 8 * nb);
+  if (rc == Z4C_OK) rc = alloc((void**)&c->flag, sizeof(int));
+  if (rc != Z4C_OK) {
+    free_ctx(c);
+    return rc;
+  }
+  if (cudaMemcpy(c->xf, c->h_xf.data(), sizeof(double) * c->h_xf.size(), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(c->xv, c->h_xv.data(), sizeof(double) * c->h_xv.size(), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(c->fd, hfd.data(), sizeof(FdScale) * nb, cudaMemcpyHostToDevice) ||
+      cudaMemcpy(c->nbr, hnbr.data(), sizeof(int) * hnbr.size(), cudaMemcpyHostToDevice)) {
+    free_ctx(c);
+    return fail(Z4C_ECUDA, "uploading mesh tables");
+  }
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    free_ctx(c);
+    return fail(Z4C_ECUDA, "stream creation");
+  }
+  c->own_stream = true;
+  *out = c;
+  return Z4C_OK;
+}
+
+int z4c_destroy(z4c_ctx* ctx) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  cudaStreamSynchronize(ctx->stream);
+  free_ctx(ctx);
+  return Z4C_OK;
+}
+
+int z4c_set_stream(z4c_ctx* ctx, void* stream) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  ctx->own_stream = false;
+  ctx->stream = static_cast<cudaStream_t>(stream);
+  if (ctx->graph) {
+    cudaGraphExecDestroy(ctx->graph);
+    ctx->graph = nullptr;
+  }
+  return Z4C_OK;
+}
+
+int z4c_sync(z4c_ctx* ctx) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return Z4C_OK;
+}
+
+int z4c_num_blocks(const z4c_ctx* ctx) { return ctx ? ctx->g.nblocks : fail(Z4C_EINVAL, "null context"); }
+
+int z4c_block_nn(const z4c_ctx* ctx, int axis) {
+  if (!ctx || axis < 0 || axis > 2) return fail(Z4C_EINVAL, "bad argument");
+  return ctx->g.nn[axis];
+}
+
+int z4c_dx(const z4c_ctx* ctx, double dx_out[3]) {
+  if (!ctx || !dx_out) return fail(Z4C_EINVAL, "null argument");
+  for (int a = 0; a < 3; ++a) dx_out[a] = ctx->h_dx[a];
+  return Z4C_OK;
+}
+
+int z4c_block_coords(const z4c_ctx* ctx, int block, int axis, double* x_out) {
+  if (!ctx || !x_out || axis < 0 || axis > 2) return fail(Z4C_EINVAL, "bad argument");
+  if (block < 0 || block >= ctx->g.nblocks) return fail(Z4C_EINVAL, "block out of range");
+  const int nsum = ctx->g.nn[0] + ctx->g.nn[1] + ctx->g.nn[2];
+  int off = 0;
+  for (int a = 0; a < axis; ++a) off += ctx->g.nn[a];
+  std::memcpy(x_out, &ctx->h_xf[(size_t)block * nsum + off], sizeof(double) * ctx->g.nn[axis]);
+  return Z4C_OK;
+}
+
+int z4c_upload(z4c_ctx* ctx, int reg, int block, const double* host) {
+  if (!ctx || !host) return fail(Z4C_EINVAL, "null argument");
+  int rc = check_reg(ctx, reg);
+  if (rc) return rc;
+  int b0, nb;
+  if ((rc = check_block(ctx, block, &b0, &nb))) return rc;
+  const size_t per = (size_t)reg_nvar_(reg) * ctx->g.nvol;
+  CUDA_TRY(cudaMemcpyAsync(ctx->reg[reg] + per * b0, host, sizeof(double) * per * nb,
+                           cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return Z4C_OK;
+}
+
+int z4c_download(z4c_ctx* ctx, int reg, int block, double* host) {
+  if (!ctx || !host) return fail(Z4C_EINVAL, "null argument");
+  int rc = check_reg(ctx, reg);
+  if (rc) return rc;
+  int b0, nb;
+  if ((rc = check_block(ctx, block, &b0, &nb))) return rc;
+  const size_t per = (size_t)reg_nvar_(reg) * ctx->g.nvol;
+  CUDA_TRY(cudaMemcpyAsync(host, ctx->reg[reg] + per * b0, sizeof(double) * per * nb,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return Z4C_OK;
+}
+
+int z4c_device_ptr(z4c_ctx* ctx, int reg, double** dptr) {
+  if (!ctx || !dptr) return fail(Z4C_EINVAL, "null argument");
+  int rc = check_reg(ctx, reg);
+  if (rc) return rc;
+  *dptr = ctx->reg[reg];
+  return Z4C_OK;
+}
+
+int z4c_rhs(z4c_ctx* ctx, int reg_u, int reg_rhs, int block) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  int rc, b0, nb;
+  if ((rc = check_reg(ctx, reg_u)) || (rc = check_reg(ctx, reg_rhs))) return rc;
+  if (reg_nvar_(reg_u) != Z4C_NVAR || reg_nvar_(reg_rhs) != Z4C_NVAR || reg_u == reg_rhs)
+    return fail(Z4C_EINVAL, "z4c_rhs needs two distinct 22-variable registers");
+  if ((rc = check_block(ctx, block, &b0, &nb))) return rc;
+  launch_rhs(ctx->g, ctx->dev(), ctx->reg[reg_u], ctx->reg[reg_rhs], b0, nb, ctx->stream);
+  LAUNCH_CHECK("rhs");
+  return Z4C_OK;
+}
+
+int z4c_add_rhs(z4c_ctx* ctx, int reg_rhs, double wght, int reg_out, int block) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  int rc, b0, nb;
+  if ((rc = check_reg(ctx, reg_rhs)) || (rc = check_reg(ctx, reg_out))) return rc;
+  if (reg_nvar_(reg_rhs) != Z4C_NVAR || reg_nvar_(reg_out) != Z4C_NVAR)
+    return fail(Z4C_EINVAL, "z4c_add_rhs needs 22-variable registers");
+  if ((rc = check_block(ctx, block, &b0, &nb))) return rc;
+  launch_add_rhs(ctx->g, ctx->reg[reg_rhs], wght, ctx->reg[reg_out], b0, nb, ctx->stream);
+  LAUNCH_CHECK("add_rhs");
+  return Z4C_OK;
+}
+
+int z4c_weighted_ave(z4c_ctx* ctx, int reg_out, int reg_in1, int reg_in2, const double w[3],
+                     int block) {
+  if (!ctx || !w) return fail(Z4C_EINVAL, "null argument");
+  int rc, b0, nb;
+  if ((rc = check_reg(ctx, reg_out)) || (rc = check_reg(ctx, reg_in1))) return rc;
+  const double* in2 = nullptr;
+  if (w[2] != 0.0) {
+    if ((rc = check_reg(ctx, reg_in2))) return rc;
+    in2 = ctx->reg[reg_in2];
+  }
+  if ((rc = check_block(ctx, block, &b0, &nb))) return rc;
+  launch_weighted_ave(ctx->g, ctx->reg[reg_out], ctx->reg[reg_in1], in2, w, b0, nb, ctx->stream);
+  LAUNCH_CHECK("weighted_ave");
+  return Z4C_OK;
+}
+
+int z4c_alg_constr(z4c_ctx* ctx, int reg_u, int block) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  int rc, b0, nb;
+  if ((rc = check_reg(ctx, reg_u))) return rc;
+  if (reg_nvar_(reg_u) != Z4C_NVAR) return fail(Z4C_EINVAL, "AlgConstr needs a Z4c register");
+  if ((rc = check_block(ctx, block, &b0, &nb))) return rc;
+  launch_alg_constr(ctx->g, ctx->dev(), ctx->reg[reg_u], b0, nb, ctx->stream);
+  LAUNCH_CHECK("alg_constr");
+  return Z4C_OK;
+}
+
+int z4c_adm_to_z4c(z4c_ctx* ctx, int reg_adm, int reg_u, int block) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  int rc, b0, nb;
+  if ((rc = check_reg(ctx, reg_adm)) || (rc = check_reg(ctx, reg_u))) return rc;
+  if (reg_nvar_(reg_adm) != Z4C_NADM || reg_nvar_(reg_u) != Z4C_NVAR)
+    return fail(Z4C_EINVAL, "ADMToZ4c needs the ADM and a Z4c register");
+  if ((rc = check_block(ctx, block, &b0, &nb))) return rc;
+  launch_adm_to_z4c(ctx->g, ctx->dev(), ctx->reg[reg_adm], ctx->reg[reg_u], ctx->guu, b0, nb,
+                    ctx->stream);
+  LAUNCH_CHECK("adm_to_z4c");
+  return Z4C_OK;
+}
+
+int z4c_z4c_to_adm(z4c_ctx* ctx, int reg_u, int reg_adm, int block) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  int rc, b0, nb;
+  if ((rc = check_reg(ctx, reg_adm)) || (rc = check_reg(ctx, reg_u))) return rc;
+  if (reg_nvar_(reg_adm) != Z4C_NADM || reg_nvar_(reg_u) != Z4C_NVAR)
+    return fail(Z4C_EINVAL, "Z4cToADM needs a Z4c and the ADM register");
+  if ((rc = check_block(ctx, block, &b0, &nb))) return rc;
+  launch_z4c_to_adm(ctx->g, ctx->dev(), ctx->reg[reg_u], ctx->reg[reg_adm], b0, nb, ctx->stream);
+  LAUNCH_CHECK("z4c_to_adm");
+  return Z4C_OK;
+}
+
+int z4c_adm_constraints(z4c_ctx* ctx, int reg_con, int reg_adm, int reg_u, int block) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  int rc, b0, nb;
+  if ((rc = check_reg(ctx, reg_con)) || (rc = check_reg(ctx, reg_adm)) ||
+      (rc = check_reg(ctx, reg_u)))
+    return rc;
+  if (reg_nvar_(reg_con) != Z4C_NCON || reg_nvar_(reg_adm) != Z4C_NADM ||
+      reg_nvar_(reg_u) != Z4C_NVAR)
+    return fail(Z4C_EINVAL, "ADMConstraints needs con, adm and a Z4c register");
+  if ((rc = check_block(ctx, block, &b0, &nb))) return rc;
+  launch_adm_constraints(ctx->g, ctx->dev(), ctx->reg[reg_adm], ctx->reg[reg_u],
+                         ctx->reg[reg_con], ctx->xf, b0, nb, ctx->stream);
+  LAUNCH_CHECK("adm_constraints");
+  return Z4C_OK;
+}
+
+int z4c_ghost_fill(z4c_ctx* ctx, int reg) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  int rc;
+  if ((rc = check_reg(ctx, reg))) return rc;
+  if (reg_nvar_(reg) != Z4C_NVAR) return fail(Z4C_EINVAL, "ghost fill needs a Z4c register");
+  if (reg == Z4C_REG_W) return fail(Z4C_EINVAL, "the work register cannot be ghost-filled");
+  if ((rc = exchange_into(ctx, ctx->reg[reg], ctx->reg[Z4C_REG_W], false))) return rc;
+  if (reg == Z4C_REG_U) {
+    std::swap(ctx->reg[Z4C_REG_U], ctx->reg[Z4C_REG_W]);
+    if (ctx->graph) {  // captured pointers are stale
+      cudaGraphExecDestroy(ctx->graph);
+      ctx->graph = nullptr;
+    }
+  } else {
+    CUDA_TRY(cudaMemcpyAsync(ctx->reg[reg], ctx->reg[Z4C_REG_W],
+                             sizeof(double) * reg_elems(ctx, reg), cudaMemcpyDeviceToDevice,
+                             ctx->stream));
+  }
+  return Z4C_OK;
+}
+
+int z4c_init_finalize(z4c_ctx* ctx) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  int rc;
+  if ((rc = z4c_ghost_fill(ctx, Z4C_REG_U))) return rc;
+  const DevParams P = ctx->dev();
+  launch_alg_constr(ctx->g, P, ctx->reg[Z4C_REG_U], 0, ctx->g.nblocks, ctx->stream, 1);
+  LAUNCH_CHECK("alg_constr ghosts");
+  launch_z4c_to_adm(ctx->g, P, ctx->reg[Z4C_REG_U], ctx->reg[Z4C_REG_ADM], 0, ctx->g.nblocks,
+                    ctx->stream, 1);
+  LAUNCH_CHECK("z4c_to_adm ghosts");
+  return Z4C_OK;
+}
+
+int z4c_hst_norms(z4c_ctx* ctx, double out[8]) {
+  if (!ctx || !out) return fail(Z4C_EINVAL, "null argument");
+  launch_hst(ctx->g, ctx->dev(), ctx->reg[Z4C_REG_CON], ctx->reg[Z4C_REG_U], ctx->xv,
+             ctx->partials, ctx->stream);
+  LAUNCH_CHECK("hst");
+  std::vector<double> h((size_t)8 * ctx->g.nblocks);
+  CUDA_TRY(cudaMemcpyAsync(h.data(), ctx->partials, sizeof(double) * h.size(),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  for (int q = 0; q < 8; ++q) out[q] = 0.0;
+  for (int b = 0; b < ctx->g.nblocks; ++b) {
+    const double* dx = &ctx->h_dx[(size_t)b * 3];
+    const double vol = dx[0] * dx[1] * dx[2];
+    for (int q = 0; q < 8; ++q) out[q] += vol * h[(size_t)b * 8 + q];
+  }
+  return Z4C_OK;
+}
+
+int z4c_stage(z4c_ctx* ctx, int stage, double dt) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  if (stage < 1 || stage > 4) return fail(Z4C_EINVAL, "stage %d outside 1..4", stage);
+  return run_stage(ctx, stage, dt);
+}
+
+int z4c_set_per_block(z4c_ctx* ctx, int per_block) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  ctx->per_block = per_block != 0;
+  return Z4C_OK;
+}
+
+int z4c_set_tile(z4c_ctx* ctx, int ti, int tj, int tk) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  if (ti != 128 || tj != 1 || tk != 1) return fail(Z4C_EINVAL, "unsupported tile");
+  ctx->tile[0] = ti;
+  ctx->tile[1] = tj;
+  ctx->tile[2] = tk;
+  return Z4C_OK;
+}
+
+int z4c_get_tile(const z4c_ctx* ctx, int tile_out[3]) {
+  if (!ctx || !tile_out) return fail(Z4C_EINVAL, "null argument");
+  for (int a = 0; a < 3; ++a) tile_out[a] = ctx->tile[a];
+  return Z4C_OK;
+}
+
+int z4c_evolve(z4c_ctx* ctx, double dt, int nsteps, int with_constraints) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  if (nsteps < 0) return fail(Z4C_EINVAL, "negative step count");
+  // The four stages of a step, captured once into a graph and replayed.  The
+  // register pointers inside the graph are fixed: a step leaves u in the same
+  // buffer it started from (exchange writes back into u), so replays are
+  // valid until a ghost fill swaps the registers (which drops the graph).
+  if (nsteps > 0 && (!ctx->graph || ctx->graph_dt != dt || ctx->graph_per_block != ctx->per_block)) {
+    if (ctx->graph) {
+      cudaGraphExecDestroy(ctx->graph);
+      ctx->graph = nullptr;
+    }
+    double* u_before = ctx->reg[Z4C_REG_U];
+    cudaGraph_t graph;
+    CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = Z4C_OK;
+    for (int s = 1; s <= 4 && rc == Z4C_OK; ++s) rc = run_stage(ctx, s, dt);
+    cudaError_t ec = cudaStreamEndCapture(ctx->stream, &graph);
+    if (rc) return rc;
+    if (ec != cudaSuccess) return fail(Z4C_ECUDA, "end capture: %s", cudaGetErrorString(ec));
+    if (ctx->reg[Z4C_REG_U] != u_before) {
+      // per-block path swaps u/w each stage: 4 swaps return to the start
+      cudaGraphDestroy(graph);
+      return fail(Z4C_ESTATE, "captured step does not return u to its buffer");
+    }
+    ec = cudaGraphInstantiate(&ctx->graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ec != cudaSuccess) return fail(Z4C_ECUDA, "graph instantiate: %s", cudaGetErrorString(ec));
+    ctx->graph_dt = dt;
+    ctx->graph_per_block = ctx->per_block;
+  }
+  for (int n = 0; n < nsteps; ++n) CUDA_TRY(cudaGraphLaunch(ctx->graph, ctx->stream));
+  if (with_constraints) {
+    const DevParams P = ctx->dev();
+    launch_z4c_to_adm(ctx->g, P, ctx->reg[Z4C_REG_U], ctx->reg[Z4C_REG_ADM], 0, ctx->g.nblocks,
+                      ctx->stream);
+    launch_adm_constraints(ctx->g, P, ctx->reg[Z4C_REG_ADM], ctx->reg[Z4C_REG_U],
+                           ctx->reg[Z4C_REG_CON], ctx->xf, 0, ctx->g.nblocks, ctx->stream);
+    LAUNCH_CHECK("constraints");
+  }
+  return Z4C_OK;
+}
+
+int z4c_check_finite(z4c_ctx* ctx, int reg) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  int rc;
+  if ((rc = check_reg(ctx, reg))) return rc;
+  CUDA_TRY(cudaMemsetAsync(ctx->flag, 0, sizeof(int), ctx->stream));
+  launch_check_finite(ctx->g, ctx->reg[reg], reg_nvar_(reg), ctx->flag, ctx->stream);
+  LAUNCH_CHECK("check_finite");
+  int h = 0;
+  CUDA_TRY(cudaMemcpyAsync(&h, ctx->flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return h ? fail(Z4C_ENONFINITE, "register %d holds NaN/Inf", reg) : Z4C_OK;
+}
+
+}  // extern "C"

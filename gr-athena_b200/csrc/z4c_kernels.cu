@@ -1,0 +1,589 @@
+// Z4c device kernels for sm_100a.  Compiled with -fmad=false so that every
+// floating-point expression rounds exactly as the reference's
+// -ffp-contract=off build does.
+#include <cuda_runtime.h>
+
+#include "z4c_adm.cuh"
+#include "z4c_common.cuh"
+#include "z4c_kernels.cuh"
+#include "z4c_rhs.cuh"
+
+namespace z4c {
+
+namespace {
+
+constexpr int kRhsThreads = 128;
+constexpr int kPointThreads = 256;
+
+inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// ---- Z4cRHS over the interior of blocks [block0, block0+nblk) -------------
+__global__ void __launch_bounds__(kRhsThreads, 1)
+k_rhs(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ rhs,
+      int block0, int nblk) {
+  const int64_t npts = interior_count(g);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * nblk) return;
+  const int b = block0 + (int)(t / npts);
+  int i, j, k;
+  interior_ijk(g, t % npts, i, j, k);
+  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  const double* ub = u + (int64_t)b * NVAR * g.nvol;
+  double out[NVAR];
+  rhs_point(ub, g.nvol, p, g.s, P, P.fd[b], out);
+  double* rb = rhs + (int64_t)b * NVAR * g.nvol + p;
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) rb[(int64_t)n * g.nvol] = out[n];
+}
+
+// ---- fused RHS + low-storage RK stage ---------------------------------------
+// IntegrateZ4c for 2S integrators (task_list_gr_z4c.cpp:176-195):
+//   WeightedAve(u1, u, u2, {1, delta, 0}); WeightedAve(u, u1, u2, {g1, g2, g3});
+//   AddZ4cRHS(rhs, beta*dt, u)        (mesh/weighted_ave.cpp:20-150)
+// u is read (all points, for the stencils); u_out, u1 are written (interior).
+__global__ void __launch_bounds__(kRhsThreads, 1)
+k_stage_ls(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ u1,
+           double* __restrict__ u_out, LsStage w, int block0, int nblk) {
+  const int64_t npts = interior_count(g);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * nblk) return;
+  const int b = block0 + (int)(t / npts);
+  int i, j, k;
+  interior_ijk(g, t % npts, i, j, k);
+  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  const int64_t off = (int64_t)b * NVAR * g.nvol + p;
+  double r[NVAR];
+  rhs_point(u + (int64_t)b * NVAR * g.nvol, g.nvol, p, g.s, P, P.fd[b], r);
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) {
+    const int64_t q = off + (int64_t)n * g.nvol;
+    const double un = __ldg(u + q);
+    double v1 = u1[q];
+    if (w.delta != 0.0) v1 += w.delta * un;  // w0 == 1, w2 == 0 branch
+    double v;
+    if (w.gamma1 == 1.0) {  // gamma3 == 0 for every 2S integrator accepted
+      v = un;
+      if (w.gamma2 != 0.0) v += w.gamma2 * v1;
+    } else if (w.gamma1 == 0.0) {
+      if (w.gamma2 == 1.0) v = v1;
+      else v = w.gamma2 * v1;
+    } else {
+      if (w.gamma2 != 0.0) v = w.gamma1 * un + w.gamma2 * v1;
+      else v = un * w.gamma1;
+    }
+    v += w.beta_dt * r[n];
+    u1[q] = v1;
+    u_out[q] = v;
+  }
+}
+
+// ---- fused RHS + Butcher stage (task_list_integrators_butcher.cpp:512-680) --
+// k_s = RHS(u); u_out = u_n + sum_q coef_q k_q in the reference's order.
+struct KPtrs {
+  double* k[4];
+};
+__global__ void __launch_bounds__(kRhsThreads, 1)
+k_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ un,
+           KPtrs K, double* __restrict__ u_out, BtStage w, int block0, int nblk) {
+  const int64_t npts = interior_count(g);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * nblk) return;
+  const int b = block0 + (int)(t / npts);
+  int i, j, k;
+  interior_ijk(g, t % npts, i, j, k);
+  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  const int64_t off = (int64_t)b * NVAR * g.nvol + p;
+  double r[NVAR];
+  rhs_point(u + (int64_t)b * NVAR * g.nvol, g.nvol, p, g.s, P, P.fd[b], r);
+#pragma unroll 1
+  for (int n = 0; n < NVAR; ++n) {
+    const int64_t q = off + (int64_t)n * g.nvol;
+    K.k[w.kslot][q] = r[n];
+    double v = __ldg(un + q);
+    for (int s = 0; s < w.nq; ++s) {
+      if (w.coef[s] != 0.0) {
+        const double ks = (s == w.kslot) ? r[n] : K.k[s][q];
+        v += w.coef[s] * ks;
+      }
+    }
+    u_out[q] = v;
+  }
+}
+
+// ---- same-level vertex-centred ghost exchange -------------------------------
+// CommRegistry::SetBoundaries (comm/comm_registry.cpp:336-382): ghosts are
+// zeroed, every neighbour whose set range (comm/index_utilities.hpp:155-163)
+// holds the vertex adds its value in neighbour-list order
+// (mesh/mesh_topology.cpp:329-960), and the sum is multiplied by
+// 1/multiplicity (comm/node_multiplicity.cpp:396-430).  Strictly interior
+// vertices are copied.  src and dst must differ.  With fuse_alg the
+// AlgConstr pass that follows in the task list is applied on the way out.
+__constant__ int c_dirs[26][3] = {
+    {-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1},
+    {-1, -1, 0}, {1, -1, 0}, {-1, 1, 0}, {1, 1, 0},
+    {-1, 0, -1}, {1, 0, -1}, {-1, 0, 1}, {1, 0, 1},
+    {0, -1, -1}, {0, 1, -1}, {0, -1, 1}, {0, 1, 1},
+    {-1, -1, -1}, {1, -1, -1}, {-1, 1, -1}, {1, 1, -1},
+    {-1, -1, 1}, {1, -1, 1}, {-1, 1, 1}, {1, 1, 1}};
+
+__global__ void __launch_bounds__(kPointThreads)
+k_exchange(Grid g, DevParams P, const double* __restrict__ src, double* __restrict__ dst,
+           int nvar, const int* __restrict__ nbr, int fuse_alg) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.nvol * g.nblocks) return;
+  const int b = (int)(t / g.nvol);
+  const int64_t p = t % g.nvol;
+  const int i = (int)(p % g.nn[0]);
+  const int j = (int)((p / g.nn[0]) % g.nn[1]);
+  const int k = (int)(p / ((int64_t)g.nn[0] * g.nn[1]));
+  const int idx[3] = {i, j, k};
+  bool interior = true, edge = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int vs = NG, ve = NG + g.nx[a];
+    if (idx[a] < vs || idx[a] > ve) interior = false;
+    if (idx[a] <= vs || idx[a] >= ve) edge = true;
+  }
+  const int64_t bstride = (int64_t)nvar * g.nvol;
+  const double* sb = src + b * bstride + p;
+  double* db = dst + b * bstride + p;
+  // neighbours covering this vertex, as 26-bit mask
+  unsigned mask = 0;
+  int mult = interior ? 1 : 0;
+  if (edge) {
+    for (int d = 0; d < 26; ++d) {
+      if (nbr[b * 26 + d] < 0) continue;
+      bool cov = true;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int vs = NG, ve = NG + g.nx[a], o = c_dirs[d][a];
+        if (o > 0) cov = cov && (idx[a] >= ve);
+        else if (o < 0) cov = cov && (idx[a] <= vs);
+        else cov = cov && (idx[a] >= vs && idx[a] <= ve);
+      }
+      if (cov) {
+        mask |= 1u << d;
+        ++mult;
+      }
+    }
+  }
+  const double inv = (mult > 1) ? 1.0 / (double)mult : 1.0;
+  auto value = [&](int n) -> double {
+    double s = interior ? __ldg(sb + (int64_t)n * g.nvol) : 0.0;
+    if (edge) {
+      for (int d = 0; d < 26; ++d) {
+        if (!(mask & (1u << d))) continue;
+        const int64_t q = ((int64_t)(k - c_dirs[d][2] * g.nx[2]) * g.nn[1] +
+                           (j - c_dirs[d][1] * g.nx[1])) * g.nn[0] +
+                          (i - c_dirs[d][0] * g.nx[0]);
+        s += __ldg(src + (int64_t)nbr[b * 26 + d] * bstride + (int64_t)n * g.nvol + q);
+      }
+      if (mult > 1) s *= inv;
+    }
+    return s;
+  };
+  if (!fuse_alg) {
+    for (int n = 0; n < nvar; ++n) db[(int64_t)n * g.nvol] = value(n);
+    return;
+  }
+  double gg[6], AA[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    gg[c] = value(Z4C_GXX + c);
+    AA[c] = value(Z4C_AXX + c);
+  }
+  double chi = value(Z4C_CHI), alpha = value(Z4C_ALPHA);
+  alg_constr_point(P.p, gg, AA, &chi, &alpha);
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    db[(int64_t)(Z4C_GXX + c) * g.nvol] = gg[c];
+    db[(int64_t)(Z4C_AXX + c) * g.nvol] = AA[c];
+  }
+  db[(int64_t)Z4C_CHI * g.nvol] = chi;
+  db[(int64_t)Z4C_ALPHA * g.nvol] = alpha;
+  const int rest[8] = {Z4C_KHAT, Z4C_GAMX, Z4C_GAMY, Z4C_GAMZ, Z4C_THETA,
+                       Z4C_BETAX, Z4C_BETAY, Z4C_BETAZ};
+#pragma unroll
+  for (int r = 0; r < 8; ++r) db[(int64_t)rest[r] * g.nvol] = value(rest[r]);
+}
+
+// ---- extrapolate_outflow boundary conditions --------------------------------
+// ExtrapolateOutflowBC with NEXTRAPOLATE = 5 (comm/physical_bcs.cpp:187-260)
+// over the ranges of ApplyPhysicalBCs (:506-670): the cell-centred interior
+// end ie = is + nx - 1 bounds the outer faces and the transverse ranges.
+// One thread per (block, variable, transverse pair, side) cascades outward.
+__global__ void k_bc_axis(Grid g, double* __restrict__ u, int nvar, int ax) {
+  const int o1 = (ax + 1) % 3, o2 = (ax + 2) % 3;
+  const int64_t nt = (int64_t)g.nn[o1] * g.nn[o2];
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt * nvar * 2 * g.nblocks) return;
+  const int side = (int)(t % 2);
+  int64_t r = t / 2;
+  const int64_t tr = r % nt;
+  r /= nt;
+  const int n = (int)(r % nvar);
+  const int b = (int)(r / nvar);
+  const int loc[3] = {b % g.nb[0], (b / g.nb[0]) % g.nb[1], b / (g.nb[0] * g.nb[1])};
+  bool need[6];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    need[2 * a] = (g.bc[2 * a] == Z4C_BC_OUTFLOW) && loc[a] == 0;
+    need[2 * a + 1] = (g.bc[2 * a + 1] == Z4C_BC_OUTFLOW) && loc[a] == g.nb[a] - 1;
+  }
+  if (!need[2 * ax + side]) return;
+  int is[3], ie[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    is[a] = NG;
+    ie[a] = NG + g.nx[a] - 1;
+  }
+  int lo[3], hi[3];
+  // transverse limits, physical_bcs.cpp:516-528, x3 faces :619-621
+  lo[0] = is[0] - NG; hi[0] = ie[0] + NG;
+  lo[1] = need[2] ? is[1] : is[1] - NG;
+  hi[1] = need[3] ? ie[1] : ie[1] + NG;
+  lo[2] = need[4] ? is[2] : is[2] - NG;
+  hi[2] = need[5] ? ie[2] : ie[2] + NG;
+  if (ax == 2) { lo[1] = is[1] - NG; hi[1] = ie[1] + NG; }
+  const int t1 = (int)(tr % g.nn[o1]), t2 = (int)(tr / g.nn[o1]);
+  if (t1 < lo[o1] || t1 > hi[o1] || t2 < lo[o2] || t2 > hi[o2]) return;
+  double* ub = u + ((int64_t)b * nvar + n) * g.nvol + (int64_t)t1 * g.s[o1] + (int64_t)t2 * g.s[o2];
+  const int64_t st = g.s[ax];
+  const double c[5] = {5., -10., 10., -5., 1.};
+  for (int gh = 1; gh <= NG; ++gh) {
+    const int ia = side ? ie[ax] + gh : is[ax] - gh;
+    const int dir = side ? -1 : 1;
+    double* pp = ub + (int64_t)ia * st;
+    double v = 0.0;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) v += c[q] * pp[dir * (q + 1) * st];
+    *pp = v;
+  }
+}
+
+// ---- AlgConstr over all points (z4c.cpp:677-799) ----------------------------
+// ghosts_only skips the interior vertices (ranged variant with
+// skip_physical, z4c.cpp:801-991).
+__device__ __forceinline__ bool is_interior_vertex(const Grid& g, int64_t p) {
+  const int i = (int)(p % g.nn[0]);
+  const int j = (int)((p / g.nn[0]) % g.nn[1]);
+  const int k = (int)(p / ((int64_t)g.nn[0] * g.nn[1]));
+  return i >= NG && i <= NG + g.nx[0] && j >= NG && j <= NG + g.nx[1] && k >= NG &&
+         k <= NG + g.nx[2];
+}
+
+__global__ void __launch_bounds__(kPointThreads)
+k_alg_constr(Grid g, DevParams P, double* __restrict__ u, int block0, int nblk,
+             int ghosts_only) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.nvol * nblk) return;
+  const int b = block0 + (int)(t / g.nvol);
+  if (ghosts_only && is_interior_vertex(g, t % g.nvol)) return;
+  double* ub = u + (int64_t)b * NVAR * g.nvol + t % g.nvol;
+  double gg[6], AA[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    gg[c] = ub[(int64_t)(Z4C_GXX + c) * g.nvol];
+    AA[c] = ub[(int64_t)(Z4C_AXX + c) * g.nvol];
+  }
+  double chi = ub[(int64_t)Z4C_CHI * g.nvol], alpha = ub[(int64_t)Z4C_ALPHA * g.nvol];
+  alg_constr_point(P.p, gg, AA, &chi, &alpha);
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    ub[(int64_t)(Z4C_GXX + c) * g.nvol] = gg[c];
+    ub[(int64_t)(Z4C_AXX + c) * g.nvol] = AA[c];
+  }
+  if (P.p.force_regularization) {
+    ub[(int64_t)Z4C_CHI * g.nvol] = chi;
+    ub[(int64_t)Z4C_ALPHA * g.nvol] = alpha;
+  }
+}
+
+// ---- WeightedAve / AddZ4cRHS on the interior (weighted_ave.cpp:20-167) --------
+__global__ void k_weighted_ave(Grid g, double* __restrict__ out, const double* __restrict__ in1,
+                               const double* __restrict__ in2, double w0, double w1, double w2,
+                               int block0, int nblk) {
+  const int64_t npts = interior_count(g);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * nblk * NVAR) return;
+  const int n = (int)(t % NVAR);
+  const int64_t r = t / NVAR;
+  const int b = block0 + (int)(r / npts);
+  int i, j, k;
+  interior_ijk(g, r % npts, i, j, k);
+  const int64_t q = ((int64_t)b * NVAR + n) * g.nvol + ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  if (w0 == 1.0) {
+    if (w2 != 0.0) out[q] += w1 * in1[q] + w2 * in2[q];
+    else if (w1 != 0.0) out[q] += w1 * in1[q];
+  } else if (w0 == 0.0) {
+    if (w2 != 0.0) out[q] = w1 * in1[q] + w2 * in2[q];
+    else if (w1 == 1.0) out[q] = in1[q];
+    else out[q] = w1 * in1[q];
+  } else {
+    if (w2 != 0.0) out[q] = w0 * out[q] + w1 * in1[q] + w2 * in2[q];
+    else if (w1 != 0.0) out[q] = w0 * out[q] + w1 * in1[q];
+    else out[q] *= w0;
+  }
+}
+
+__global__ void k_add_rhs(Grid g, const double* __restrict__ rhs, double wght,
+                          double* __restrict__ out, int block0, int nblk) {
+  const int64_t npts = interior_count(g);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * nblk * NVAR) return;
+  const int n = (int)(t % NVAR);
+  const int64_t r = t / NVAR;
+  const int b = block0 + (int)(r / npts);
+  int i, j, k;
+  interior_ijk(g, r % npts, i, j, k);
+  const int64_t q = ((int64_t)b * NVAR + n) * g.nvol + ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  out[q] += wght * rhs[q];
+}
+
+// ---- ADM maps ----------------------------------------------------------------
+__global__ void k_z4c_to_adm(Grid g, DevParams P, const double* __restrict__ u,
+                             double* __restrict__ adm, int block0, int nblk, int ghosts_only) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.nvol * nblk) return;
+  const int b = block0 + (int)(t / g.nvol);
+  const int64_t p = t % g.nvol;
+  if (ghosts_only && is_interior_vertex(g, p)) return;
+  z4c_to_adm_point(P.p, u + (int64_t)b * NVAR * g.nvol + p,
+                   adm + (int64_t)b * Z4C_NADM * g.nvol + p, g.nvol);
+}
+
+__global__ void k_adm_to_z4c_pt(Grid g, DevParams P, const double* __restrict__ adm,
+                                double* __restrict__ u, double* __restrict__ guu, int block0,
+                                int nblk) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.nvol * nblk) return;
+  const int b = block0 + (int)(t / g.nvol);
+  const int64_t p = t % g.nvol;
+  adm_to_z4c_point(P.p, adm + (int64_t)b * Z4C_NADM * g.nvol + p,
+                   u + (int64_t)b * NVAR * g.nvol + p, guu + (int64_t)b * 6 * g.nvol + p,
+                   g.nvol);
+}
+
+// Gamma^a = -sum_b Dx(b, g~^{ba}) on the interior, zero elsewhere (:165-176).
+__global__ void k_adm_to_z4c_gam(Grid g, DevParams P, const double* __restrict__ guu,
+                                 double* __restrict__ u, int block0, int nblk) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.nvol * nblk) return;
+  const int b = block0 + (int)(t / g.nvol);
+  const int64_t p = t % g.nvol;
+  const int i = (int)(p % g.nn[0]);
+  const int j = (int)((p / g.nn[0]) % g.nn[1]);
+  const int k = (int)(p / ((int64_t)g.nn[0] * g.nn[1]));
+  const bool in = i >= NG && i <= NG + g.nx[0] && j >= NG && j <= NG + g.nx[1] && k >= NG &&
+                  k <= NG + g.nx[2];
+  const double* gb = guu + (int64_t)b * 6 * g.nvol + p;
+  double* ub = u + (int64_t)b * NVAR * g.nvol + p;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    double v = 0.0;
+    if (in) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        v -= fd_dx(gb + (int64_t)sidx(c, a) * g.nvol, g.s[c], P.fd[b].cidx1[c]);
+    }
+    ub[(int64_t)(Z4C_GAMX + a) * g.nvol] = v;
+  }
+}
+
+__global__ void __launch_bounds__(kRhsThreads, 1)
+k_adm_constraints(Grid g, DevParams P, const double* __restrict__ adm,
+                  const double* __restrict__ u, double* __restrict__ con,
+                  const double* __restrict__ xf, int block0, int nblk) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.nvol * nblk) return;
+  const int b = block0 + (int)(t / g.nvol);
+  const int64_t p = t % g.nvol;
+  const int i = (int)(p % g.nn[0]);
+  const int j = (int)((p / g.nn[0]) % g.nn[1]);
+  const int k = (int)(p / ((int64_t)g.nn[0] * g.nn[1]));
+  double* cb = con + (int64_t)b * Z4C_NCON * g.nvol + p;
+  const bool in = i >= NG && i <= NG + g.nx[0] && j >= NG && j <= NG + g.nx[1] && k >= NG &&
+                  k <= NG + g.nx[2];
+  double c7[7] = {0, 0, 0, 0, 0, 0, 0};
+  if (in) {
+    const double* x = xf + (int64_t)b * (g.nn[0] + g.nn[1] + g.nn[2]);
+    adm_constraints_point(u + (int64_t)b * NVAR * g.nvol, adm + (int64_t)b * Z4C_NADM * g.nvol,
+                          g.nvol, p, g.s, P, P.fd[b], x[i], x[g.nn[0] + j],
+                          x[g.nn[0] + g.nn[1] + k], c7);
+  }
+#pragma unroll
+  for (int q = 0; q < 7; ++q) cb[(int64_t)q * g.nvol] = c7[q];
+}
+
+// ---- history sums (outputs/history.cpp:168-200): one CTA per block ---------
+__global__ void k_hst(Grid g, DevParams P, const double* __restrict__ con,
+                      const double* __restrict__ u, const double* __restrict__ xv,
+                      double* __restrict__ partials) {
+  const int b = blockIdx.x;
+  const int64_t ncell = (int64_t)g.nx[0] * g.nx[1] * g.nx[2];
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const double* x = xv + (int64_t)b * (g.nn[0] + g.nn[1] + g.nn[2] - 3);
+  for (int64_t c = threadIdx.x; c < ncell; c += blockDim.x) {
+    const int i = NG + (int)(c % g.nx[0]);
+    const int j = NG + (int)((c / g.nx[0]) % g.nx[1]);
+    const int k = NG + (int)(c / ((int64_t)g.nx[0] * g.nx[1]));
+    const double x1 = x[i], x2 = x[g.nn[0] - 1 + j], x3 = x[g.nn[0] + g.nn[1] - 2 + k];
+    const double R2 = x1 * x1 + x2 * x2 + x3 * x3;
+    if (!(R2 <= P.p.r_max_con * P.p.r_max_con)) continue;
+    const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+    const double* cb = con + (int64_t)b * Z4C_NCON * g.nvol + p;
+    const double H = fabs(cb[(int64_t)Z4C_CON_H * g.nvol]);
+    acc[0] += H * H;
+    acc[1] += fabs(cb[(int64_t)Z4C_CON_M * g.nvol]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double m = fabs(cb[(int64_t)(Z4C_CON_MX + a) * g.nvol]);
+      acc[2 + a] += m * m;
+    }
+    acc[5] += fabs(cb[(int64_t)Z4C_CON_Z * g.nvol]);
+    const double th = fabs(u[((int64_t)b * NVAR + Z4C_THETA) * g.nvol + p]);
+    acc[6] += th * th;
+    acc[7] += fabs(cb[(int64_t)Z4C_CON_C * g.nvol]);
+  }
+  __shared__ double sh[8][256];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) sh[q][threadIdx.x] = acc[q];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w)
+#pragma unroll
+      for (int q = 0; q < 8; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) partials[b * 8 + q] = sh[q][0];
+}
+
+__global__ void k_check_finite(int64_t n, const double* __restrict__ u, int* flag) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  bool bad = false;
+  for (; t < n; t += stride) bad |= !isfinite(u[t]);
+  if (bad) atomicOr(flag, 1);
+}
+
+__global__ void k_zero_interior(Grid g, double* __restrict__ u, int nvar) {
+  const int64_t npts = interior_count(g);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * g.nblocks * nvar) return;
+  const int n = (int)(t % nvar);
+  const int64_t r = t / nvar;
+  const int b = (int)(r / npts);
+  int i, j, k;
+  interior_ijk(g, r % npts, i, j, k);
+  u[((int64_t)b * nvar + n) * g.nvol + ((int64_t)k * g.nn[1] + j) * g.nn[0] + i] = 0.0;
+}
+
+}  // namespace
+
+// ---- launchers -----------------------------------------------------------------
+
+void launch_rhs(const Grid& g, const DevParams& P, const double* u, double* rhs, int block0,
+                int nblk, cudaStream_t st) {
+  const int64_t n = interior_count(g) * nblk;
+  k_rhs<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, rhs, block0, nblk);
+}
+
+void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, double* u1,
+                     double* u_out, const LsStage& w, int block0, int nblk, cudaStream_t st) {
+  const int64_t n = interior_count(g) * nblk;
+  k_stage_ls<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, u1, u_out, w, block0,
+                                                              nblk);
+}
+
+void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const double* un,
+                     double* const* k, double* u_out, const BtStage& w, int block0, int nblk,
+                     cudaStream_t st) {
+  KPtrs K;
+  for (int s = 0; s < 4; ++s) K.k[s] = k[s];
+  const int64_t n = interior_count(g) * nblk;
+  k_stage_bt<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, un, K, u_out, w, block0,
+                                                              nblk);
+}
+
+void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst, int nvar,
+                     const int* nbr, int fuse_alg, cudaStream_t st) {
+  const int64_t n = g.nvol * g.nblocks;
+  k_exchange<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, src, dst, nvar, nbr,
+                                                                  fuse_alg);
+}
+
+void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st) {
+  bool any = false;
+  for (int f = 0; f < 6; ++f) any |= (g.bc[f] == Z4C_BC_OUTFLOW);
+  if (!any) return;
+  for (int ax = 0; ax < 3; ++ax) {
+    const int o1 = (ax + 1) % 3, o2 = (ax + 2) % 3;
+    const int64_t n = (int64_t)g.nn[o1] * g.nn[o2] * nvar * 2 * g.nblocks;
+    k_bc_axis<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, u, nvar, ax);
+  }
+}
+
+void launch_alg_constr(const Grid& g, const DevParams& P, double* u, int block0, int nblk,
+                       cudaStream_t st, int ghosts_only) {
+  const int64_t n = g.nvol * nblk;
+  k_alg_constr<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, block0, nblk,
+                                                                    ghosts_only);
+}
+
+void launch_weighted_ave(const Grid& g, double* out, const double* in1, const double* in2,
+                         const double w[3], int block0, int nblk, cudaStream_t st) {
+  const int64_t n = interior_count(g) * nblk * NVAR;
+  k_weighted_ave<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(
+      g, out, in1, in2, w[0], w[1], w[2], block0, nblk);
+}
+
+void launch_add_rhs(const Grid& g, const double* rhs, double wght, double* out, int block0,
+                    int nblk, cudaStream_t st) {
+  const int64_t n = interior_count(g) * nblk * NVAR;
+  k_add_rhs<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, rhs, wght, out, block0, nblk);
+}
+
+void launch_z4c_to_adm(const Grid& g, const DevParams& P, const double* u, double* adm,
+                       int block0, int nblk, cudaStream_t st, int ghosts_only) {
+  const int64_t n = g.nvol * nblk;
+  k_z4c_to_adm<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, adm, block0, nblk,
+                                                                    ghosts_only);
+}
+
+void launch_adm_to_z4c(const Grid& g, const DevParams& P, const double* adm, double* u,
+                       double* guu_scratch, int block0, int nblk, cudaStream_t st) {
+  const int64_t n = g.nvol * nblk;
+  // guu_scratch is indexed by absolute block number
+  k_adm_to_z4c_pt<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, adm, u, guu_scratch,
+                                                                      block0, nblk);
+  k_adm_to_z4c_gam<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, guu_scratch, u,
+                                                                       block0, nblk);
+  k_alg_constr<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, block0, nblk, 0);
+}
+
+void launch_adm_constraints(const Grid& g, const DevParams& P, const double* adm,
+                            const double* u, double* con, const double* xf, int block0,
+                            int nblk, cudaStream_t st) {
+  const int64_t n = g.nvol * nblk;
+  k_adm_constraints<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, adm, u, con, xf,
+                                                                    block0, nblk);
+}
+
+void launch_hst(const Grid& g, const DevParams& P, const double* con, const double* u,
+                const double* xv, double* partials, cudaStream_t st) {
+  k_hst<<<g.nblocks, 256, 0, st>>>(g, P, con, u, xv, partials);
+}
+
+void launch_check_finite(const Grid& g, const double* u, int nvar, int* flag, cudaStream_t st) {
+  const int64_t n = g.nvol * g.nblocks * nvar;
+  k_check_finite<<<1184, 256, 0, st>>>(n, u, flag);
+}
+
+void launch_zero_interior(const Grid& g, double* u, int nvar, cudaStream_t st) {
+  const int64_t n = interior_count(g) * g.nblocks * nvar;
+  k_zero_interior<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, u, nvar);
+}
+
+}  // namespace z4c

@@ -1,0 +1,76 @@
+// Device kernels of the Z4c path.  Each kernel cites the reference routine it
+// replaces; the pointwise arithmetic lives in z4c_common.cuh / z4c_rhs.cuh /
+// z4c_adm.cuh.
+#pragma once
+
+#include "z4c_common.cuh"
+
+namespace z4c {
+
+// Register view: base pointer, variables per block.
+struct Reg {
+  double* p;
+  int nvar;
+  __device__ __forceinline__ double* block(const Grid& g, int b) const {
+    return p + (int64_t)b * nvar * g.nvol;
+  }
+};
+
+// LS stage weights (task_list_integrators_low_storage.cpp:112-142) with the
+// step already scaled: beta_dt = beta * dt (time_integrators.hpp:37-40).
+struct LsStage {
+  double delta, gamma1, gamma2, gamma3, beta_dt;
+};
+
+// Butcher stage: u_out = u_n + sum_{q < nq} coef[q] * k_q, coef = a*dt or b*dt
+// (task_list_integrators_butcher.cpp:580-680); zero coefficients skipped.
+struct BtStage {
+  double coef[4];
+  int nq;      // number of slopes summed (stage+1 for SumBT_ak, 4 for SumBT_bk)
+  int kslot;   // which K register receives this stage's RHS
+};
+
+// Interior vertex l of a block -> (i, j, k).
+__device__ __forceinline__ void interior_ijk(const Grid& g, int64_t l, int& i, int& j, int& k) {
+  const int n0 = g.nx[0] + 1, n1 = g.nx[1] + 1;
+  i = NG + (int)(l % n0);
+  j = NG + (int)((l / n0) % n1);
+  k = NG + (int)(l / ((int64_t)n0 * n1));
+}
+
+__host__ __device__ __forceinline__ int64_t interior_count(const Grid& g) {
+  return (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
+}
+
+// ---- launchers (host side) ----------------------------------------------
+
+// All launches return cudaGetLastError() mapped by the caller.
+void launch_rhs(const Grid& g, const DevParams& P, const double* u, double* rhs,
+                int block0, int nblk, cudaStream_t st);
+void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, double* u1,
+                     double* u_out, const LsStage& w, int block0, int nblk, cudaStream_t st);
+void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const double* un,
+                     double* const* k, double* u_out, const BtStage& w, int block0, int nblk,
+                     cudaStream_t st);
+void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst,
+                     int nvar, const int* nbr, int fuse_alg, cudaStream_t st);
+void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st);
+void launch_alg_constr(const Grid& g, const DevParams& P, double* u, int block0, int nblk,
+                       cudaStream_t st, int ghosts_only = 0);
+void launch_weighted_ave(const Grid& g, double* out, const double* in1, const double* in2,
+                         const double w[3], int block0, int nblk, cudaStream_t st);
+void launch_add_rhs(const Grid& g, const double* rhs, double wght, double* out, int block0,
+                    int nblk, cudaStream_t st);
+void launch_z4c_to_adm(const Grid& g, const DevParams& P, const double* u, double* adm,
+                       int block0, int nblk, cudaStream_t st, int ghosts_only = 0);
+void launch_adm_to_z4c(const Grid& g, const DevParams& P, const double* adm, double* u,
+                       double* guu_scratch, int block0, int nblk, cudaStream_t st);
+void launch_adm_constraints(const Grid& g, const DevParams& P, const double* adm,
+                            const double* u, double* con, const double* xf, int block0,
+                            int nblk, cudaStream_t st);
+void launch_hst(const Grid& g, const DevParams& P, const double* con, const double* u,
+                const double* xv, double* partials, cudaStream_t st);
+void launch_check_finite(const Grid& g, const double* u, int nvar, int* flag, cudaStream_t st);
+void launch_zero_interior(const Grid& g, double* u, int nvar, cudaStream_t st);
+
+}  // namespace z4c

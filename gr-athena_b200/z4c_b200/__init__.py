@@ -1,0 +1,302 @@
+"""Host-side mirror of the GR-Athena++ Z4c operator interface over the B200
+C ABI (include/z4c_b200.h, library gr-athena_b200/_build/libz4c_b200.so).
+
+The class :class:`Z4c` carries the reference member-function names
+(src/z4c/z4c.hpp:448-539): ``Z4cRHS``, ``AddZ4cRHS``, ``WeightedAve``,
+``ADMToZ4c``, ``Z4cToADM``, ``ADMConstraints``, ``AlgConstr``, plus the task
+list pieces (ghost fill, stages, whole steps).  Registers stay on the device;
+numpy arrays in the reference layout ``[block][var][k][j][i]`` move across
+the boundary only through ``upload``/``download``.
+
+There is no CPU fallback: constructing a context without the built library
+or without a CUDA device raises.
+"""
+import ctypes as C
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "_build", "libz4c_b200.so")
+
+NG = 4
+NVAR, NADM, NCON = 22, 17, 7
+(CHI, GXX, GXY, GXZ, GYY, GYZ, GZZ, KHAT, AXX, AXY, AXZ, AYY, AYZ, AZZ,
+ GAMX, GAMY, GAMZ, THETA, ALPHA, BETAX, BETAY, BETAZ) = range(22)
+(ADM_ALPHA, ADM_BETAX, ADM_BETAY, ADM_BETAZ, ADM_GXX, ADM_GXY, ADM_GXZ, ADM_GYY,
+ ADM_GYZ, ADM_GZZ, ADM_KXX, ADM_KXY, ADM_KXZ, ADM_KYY, ADM_KYZ, ADM_KZZ,
+ ADM_PSI4) = range(17)
+CON_C, CON_H, CON_M, CON_Z, CON_MX, CON_MY, CON_MZ = range(7)
+(REG_U, REG_U1, REG_RHS, REG_ADM, REG_CON, REG_W, REG_K1, REG_K2, REG_K3,
+ REG_K4) = range(10)
+BC_PERIODIC, BC_OUTFLOW = 0, 1
+INTEG = {"rk4": 0, "bt_rk4": 1}
+ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ENONFINITE", -5: "ETIMEOUT",
+          -6: "ESTATE", -7: "ENODEV"}
+HST_COLUMNS = ("H-norm2", "M-norm2", "Mx-norm2", "My-norm2", "Mz-norm2", "Z-norm2",
+               "Theta-norm2", "C-norm2")
+
+# symbols the library must export (one per declaration in include/z4c_b200.h)
+EXPORTS = (
+    "z4c_params_default", "z4c_last_error", "z4c_create", "z4c_destroy",
+    "z4c_set_stream", "z4c_sync", "z4c_num_blocks", "z4c_block_nn", "z4c_reg_nvar",
+    "z4c_dx", "z4c_block_coords", "z4c_upload", "z4c_download", "z4c_device_ptr",
+    "z4c_rhs", "z4c_add_rhs", "z4c_weighted_ave", "z4c_alg_constr", "z4c_adm_to_z4c",
+    "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_ghost_fill", "z4c_init_finalize",
+    "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
+    "z4c_get_tile", "z4c_check_finite")
+
+
+class Z4cError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    """z4c_params_t; defaults of the reference (z4c.cpp:318-410)."""
+
+    _fields_ = [(n, C.c_double) for n in (
+        "chi_psi_power", "chi_div_floor", "diss", "eps_floor", "damp_kappa1",
+        "damp_kappa2", "lapse_oplog", "lapse_harmonicf", "lapse_harmonic",
+        "lapse_advect", "lapse_K", "shift_Gamma", "shift_alpha2Gamma", "shift_H",
+        "shift_advect", "shift_eta", "r_max_con")] + [
+        ("tf_force_regularization", C.c_int), ("force_regularization", C.c_int)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("nb", C.c_int * 3), ("nx", C.c_int * 3), ("xmin", C.c_double * 3),
+                ("xmax", C.c_double * 3), ("bc", C.c_int * 6)]
+
+
+_lib = None
+
+
+def lib():
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"z4c_b200 library not built: {LIB_PATH} "
+                               "(run python gr-athena_b200/build.py)")
+        L = C.CDLL(LIB_PATH)
+        vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.c_int
+        L.z4c_last_error.restype = C.c_char_p
+        L.z4c_params_default.argtypes = [C.POINTER(Params)]
+        L.z4c_params_default.restype = None
+        L.z4c_create.argtypes = [C.POINTER(MeshDesc), C.POINTER(Params), ip, C.POINTER(vp)]
+        L.z4c_destroy.argtypes = [vp]
+        L.z4c_set_stream.argtypes = [vp, vp]
+        L.z4c_sync.argtypes = [vp]
+        L.z4c_num_blocks.argtypes = [vp]
+        L.z4c_block_nn.argtypes = [vp, ip]
+        L.z4c_reg_nvar.argtypes = [ip]
+        L.z4c_dx.argtypes = [vp, dp]
+        L.z4c_block_coords.argtypes = [vp, ip, ip, dp]
+        L.z4c_upload.argtypes = [vp, ip, ip, dp]
+        L.z4c_download.argtypes = [vp, ip, ip, dp]
+        L.z4c_device_ptr.argtypes = [vp, ip, C.POINTER(dp)]
+        L.z4c_rhs.argtypes = [vp, ip, ip, ip]
+        L.z4c_add_rhs.argtypes = [vp, ip, C.c_double, ip, ip]
+        L.z4c_weighted_ave.argtypes = [vp, ip, ip, ip, dp, ip]
+        L.z4c_alg_constr.argtypes = [vp, ip, ip]
+        L.z4c_adm_to_z4c.argtypes = [vp, ip, ip, ip]
+        L.z4c_z4c_to_adm.argtypes = [vp, ip, ip, ip]
+        L.z4c_adm_constraints.argtypes = [vp, ip, ip, ip, ip]
+        L.z4c_ghost_fill.argtypes = [vp, ip]
+        L.z4c_init_finalize.argtypes = [vp]
+        L.z4c_hst_norms.argtypes = [vp, dp]
+        L.z4c_stage.argtypes = [vp, ip, C.c_double]
+        L.z4c_evolve.argtypes = [vp, C.c_double, ip, ip]
+        L.z4c_set_per_block.argtypes = [vp, ip]
+        L.z4c_set_tile.argtypes = [vp, ip, ip, ip]
+        L.z4c_get_tile.argtypes = [vp, C.POINTER(C.c_int)]
+        L.z4c_check_finite.argtypes = [vp, ip]
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc < 0:
+        raise Z4cError(rc, lib().z4c_last_error().decode())
+    return rc
+
+
+def default_params(**overrides):
+    p = Params()
+    lib().z4c_params_default(C.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+class Mesh:
+    """Uniform single-level block grid (reference <mesh>/<meshblock> blocks)."""
+
+    def __init__(self, nb, nx, xmin, xmax, bc="periodic"):
+        self.nb = tuple(int(v) for v in nb)
+        self.nx = tuple(int(v) for v in nx)
+        self.xmin = tuple(float(v) for v in xmin)
+        self.xmax = tuple(float(v) for v in xmax)
+        if isinstance(bc, str):
+            bc = [BC_PERIODIC if bc == "periodic" else BC_OUTFLOW] * 6
+        self.bc = tuple(int(v) for v in bc)
+
+    @property
+    def nblocks(self):
+        return self.nb[0] * self.nb[1] * self.nb[2]
+
+    @property
+    def nn(self):
+        return tuple(n + 1 + 2 * NG for n in self.nx)
+
+    def desc(self):
+        d = MeshDesc()
+        for a in range(3):
+            d.nb[a], d.nx[a] = self.nb[a], self.nx[a]
+            d.xmin[a], d.xmax[a] = self.xmin[a], self.xmax[a]
+        for f in range(6):
+            d.bc[f] = self.bc[f]
+        return d
+
+    def zones(self):
+        """Cells of the mesh (the reference's zone count, mesh.hpp:289-292)."""
+        return self.nblocks * self.nx[0] * self.nx[1] * self.nx[2]
+
+
+class Z4c:
+    """A device context holding every MeshBlock of a mesh."""
+
+    def __init__(self, mesh, params=None, integrator="rk4"):
+        self.mesh = mesh
+        self.params = params if params is not None else default_params()
+        self.integrator = integrator
+        h = C.c_void_p()
+        _check(lib().z4c_create(C.byref(mesh.desc()), C.byref(self.params),
+                                INTEG[integrator], C.byref(h)))
+        self._h = h
+        self.nblocks = mesh.nblocks
+        self.nn = mesh.nn
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().z4c_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- data movement ----
+    def shape(self, reg, block=-1):
+        nv = lib().z4c_reg_nvar(reg)
+        s = (nv, self.nn[2], self.nn[1], self.nn[0])
+        return s if block >= 0 else (self.nblocks,) + s
+
+    def upload(self, reg, arr, block=-1):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.shape != self.shape(reg, block):
+            raise ValueError(f"shape {a.shape} != {self.shape(reg, block)}")
+        _check(lib().z4c_upload(self._h, reg, block, a.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def download(self, reg, block=-1):
+        a = np.empty(self.shape(reg, block))
+        _check(lib().z4c_download(self._h, reg, block, a.ctypes.data_as(C.POINTER(C.c_double))))
+        return a
+
+    def device_ptr(self, reg):
+        p = C.POINTER(C.c_double)()
+        _check(lib().z4c_device_ptr(self._h, reg, C.byref(p)))
+        return C.cast(p, C.c_void_p).value
+
+    def coords(self, block):
+        """Vertex coordinates (x, y, z) of one block, the reference's x?f."""
+        out = []
+        for a in range(3):
+            x = np.empty(self.nn[a])
+            _check(lib().z4c_block_coords(self._h, block, a,
+                                          x.ctypes.data_as(C.POINTER(C.c_double))))
+            out.append(x)
+        return out
+
+    def dx(self):
+        d = np.empty(3)
+        _check(lib().z4c_dx(self._h, d.ctypes.data_as(C.POINTER(C.c_double))))
+        return d
+
+    def sync(self):
+        _check(lib().z4c_sync(self._h))
+
+    def set_stream(self, stream_handle):
+        _check(lib().z4c_set_stream(self._h, C.c_void_p(stream_handle)))
+
+    # ---- reference operator names ----
+    def Z4cRHS(self, reg_u=REG_U, reg_rhs=REG_RHS, block=-1):
+        _check(lib().z4c_rhs(self._h, reg_u, reg_rhs, block))
+
+    def AddZ4cRHS(self, reg_rhs, wght, reg_out, block=-1):
+        _check(lib().z4c_add_rhs(self._h, reg_rhs, float(wght), reg_out, block))
+
+    def WeightedAve(self, reg_out, reg_in1, reg_in2, wght, block=-1):
+        w = (C.c_double * 3)(*[float(x) for x in wght])
+        _check(lib().z4c_weighted_ave(self._h, reg_out, reg_in1, reg_in2, w, block))
+
+    def AlgConstr(self, reg_u=REG_U, block=-1):
+        _check(lib().z4c_alg_constr(self._h, reg_u, block))
+
+    def ADMToZ4c(self, reg_adm=REG_ADM, reg_u=REG_U, block=-1):
+        _check(lib().z4c_adm_to_z4c(self._h, reg_adm, reg_u, block))
+
+    def Z4cToADM(self, reg_u=REG_U, reg_adm=REG_ADM, block=-1):
+        _check(lib().z4c_z4c_to_adm(self._h, reg_u, reg_adm, block))
+
+    def ADMConstraints(self, reg_con=REG_CON, reg_adm=REG_ADM, reg_u=REG_U, block=-1):
+        _check(lib().z4c_adm_constraints(self._h, reg_con, reg_adm, reg_u, block))
+
+    # ---- task-list pieces ----
+    def ghost_fill(self, reg=REG_U):
+        _check(lib().z4c_ghost_fill(self._h, reg))
+
+    def init_finalize(self):
+        _check(lib().z4c_init_finalize(self._h))
+
+    def stage(self, stage, dt):
+        _check(lib().z4c_stage(self._h, int(stage), float(dt)))
+
+    def evolve(self, dt, nsteps, with_constraints=False):
+        _check(lib().z4c_evolve(self._h, float(dt), int(nsteps), int(bool(with_constraints))))
+
+    def set_per_block(self, flag):
+        _check(lib().z4c_set_per_block(self._h, int(bool(flag))))
+
+    def hst_norms(self):
+        out = np.empty(8)
+        _check(lib().z4c_hst_norms(self._h, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def check_finite(self, reg=REG_U):
+        rc = lib().z4c_check_finite(self._h, reg)
+        if rc == -4:
+            return False
+        _check(rc)
+        return True
+
+    def constraints(self):
+        """Z4cToADM + ADMConstraints on the current state (last-stage tasks)."""
+        self.Z4cToADM()
+        self.ADMConstraints()

@@ -181,6 +181,11 @@ int z4c_adm_constraints(z4c_ctx *ctx, int reg_con, int reg_adm, int reg_u,
  * device copy, shared vertices averaged over their owners, then the
  * physical boundary conditions.  Whole mesh. */
 int z4c_ghost_fill(z4c_ctx *ctx, int reg);
+/* Mesh::FinalizeZ4cADMGhosts (mesh/mesh_communicate.cpp:100-167) for a
+ * single-level mesh: ghost fill of u, AlgConstr and Z4cToADM on the ghost
+ * vertices only.  Run once after the initial data is in place (after
+ * z4c_adm_to_z4c, or after uploading u and adm). */
+int z4c_init_finalize(z4c_ctx *ctx);
 /* History sums of outputs/history.cpp:168-200 over the whole mesh from the
  * con and u registers: H^2, M, Mx^2, My^2, Mz^2, Z, Theta^2, C (volume
  * weighted). */
