@@ -1,0 +1,418 @@
+"""Benchmark of the B200 Z4c path: FP64 Z4c zone-updates/s.
+
+Workload (one GPU): one Schwarzschild puncture (M = 1, precollapsed lapse) on
+a uniform mesh of 128^3 cells split into 512 MeshBlocks of 16^3 (nghost 4),
+domain [-16, 16]^3, extrapolate_outflow boundaries, 1+log slicing and
+Gamma-driver shift (eta = 2), kappa1 = 0.02, KO dissipation 0.02, low-storage
+RK4, Courant 0.25.  One step = one full RK4 step of the whole mesh (four
+stages: fused RHS+KO+stage update, ghost exchange, boundary conditions,
+AlgConstr), replayed from a captured CUDA graph.  A zone-update is one cell
+advanced one full step (the reference's zone-cycle, main.cpp:239).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank evolves its own replica of the mesh
+("replicas only": the path has no cross-GPU exchange on one-GPU meshes); the
+value is the total over ranks divided by the slowest rank's time.
+"""
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gr-athena_b200"))
+
+METRIC = "FP64 Z4c zone-updates/s"
+WORKLOAD = dict(workload="single puncture M=1, 128^3 cells as 512 MeshBlocks of 16^3, "
+                         "nghost=4, [-16,16]^3, extrapolate_outflow, 1+log + Gamma-driver "
+                         "(eta=2), kappa1=0.02, diss=0.02, rk4 (2S), cfl 0.25",
+                nb=[8, 8, 8], nx=[16, 16, 16], xmin=[-16.0] * 3, xmax=[16.0] * 3)
+PARAMS = dict(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02, damp_kappa2=0.0,
+              shift_eta=2.0, r_max_con=1e300)
+CFL = 0.25
+# Algorithmic HBM bytes of one fused stage per interior vertex: read u and u1,
+# write u' and u1' (22 FP64 variables each).
+STAGE_BYTES_PER_POINT = 4 * 22 * 8
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nb", type=int, default=8,
+                    help="MeshBlocks per axis (8 = the 128^3 workload; smaller for profiling)")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="graph-captured steps and the stage kernel only (for ncu)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines
+
+
+def reference_deck(nlim, threads):
+    nb, nx = WORKLOAD["nb"], WORKLOAD["nx"]
+    lines = ["<job>", "problem_id = bench", "<z4c>"]
+    lines += [f"{k} = {v!r}" for k, v in PARAMS.items()]
+    lines += ["<task_triggers>", "adjust_mesh_dt = false", "<time>", f"cfl_number = {CFL}",
+              "tlim = 1e10", f"nlim = {nlim}", "integrator = rk4", "ncycle_out = 1000000",
+              "<mesh>"]
+    for a in range(3):
+        d = a + 1
+        lines += [f"nx{d} = {nb[a] * nx[a]}", f"x{d}min = {WORKLOAD['xmin'][a]!r}",
+                  f"x{d}max = {WORKLOAD['xmax'][a]!r}", f"ix{d}_bc = extrapolate_outflow",
+                  f"ox{d}_bc = extrapolate_outflow"]
+    lines += ["refinement = none", f"num_threads = {threads}", "<meshblock>"]
+    lines += [f"nx{a + 1} = {nx[a]}" for a in range(3)]
+    lines += ["<problem>", "test = one_puncture", "punc_ADM_mass = 1.0"]
+    return "\n".join(lines) + "\n"
+
+
+def run_reference_cpu(nlim, threads):
+    """Times the reference's own OpenMP CPU build (oracle/_ref/athena_ref,
+    compiled from the reference sources) on the benchmark workload and returns
+    its printed zone-cycles/omp_wsecond (main.hpp:739-742)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "athena_ref")
+    if not os.path.exists(exe):
+        return None
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = os.path.join(tmp, "bench.inp")
+        with open(inp, "w") as f:
+            f.write(reference_deck(nlim, threads))
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        out = subprocess.run([exe, "-i", inp], cwd=tmp, capture_output=True, text=True,
+                             env=env, timeout=1800)
+    m = re.search(r"zone-cycles/omp_wsecond\s*=\s*([0-9.eE+-]+)", out.stdout)
+    if not m:
+        return None
+    return float(m.group(1))
+
+
+def run_oracle_cpu(max_seconds=20.0):
+    """Fallback CPU baseline: the C restatement (oracle/, single thread) on
+    whole MeshBlocks of the workload until max_seconds of work."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import z4c_oracle as O
+    from z4c_b200 import Mesh
+    from z4c_b200 import initial_data as ID
+    mesh = Mesh(WORKLOAD["nb"], WORKLOAD["nx"], WORKLOAD["xmin"], WORKLOAD["xmax"], "outflow")
+    p = O.default_params(**PARAMS)
+    xs, dxs = mesh.block_coords(0)
+    blk = O.Block(mesh.nx, dxs, xs)
+    u = np.ones((22,) + tuple(reversed(mesh.nn)))
+    t0 = time.perf_counter()
+    n = 0
+    while time.perf_counter() - t0 < max_seconds and n < 64:
+        O.rhs(blk, p, u)
+        n += 1
+    el = time.perf_counter() - t0
+    zones = 16 ** 3
+    # one zone-update = 4 RHS evaluations (the stage updates are negligible)
+    return n * zones / el / 4.0, n
+
+
+# ---------------------------------------------------------------------------
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return main_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    import z4c_b200 as Z
+    from z4c_b200 import initial_data as ID
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    nb = [args.nb] * 3
+    lim = 2.0 * args.nb
+    mesh = Z.Mesh(nb, WORKLOAD["nx"], [-lim] * 3, [lim] * 3, "outflow")
+    params = Z.default_params(**PARAMS)
+    ctx = Z.Z4c(mesh, params, "rk4")
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    adm = ID.punctures(mesh, params, masses=(1.0,), centres=((0.0, 0.0, 0.0),))
+    ID.load_adm(ctx, adm)
+    ctx.sync()
+    u_init = ctx.download(Z.REG_U)
+    dt = CFL * float(np.min(ctx.dx()))
+    zones = mesh.zones()
+    npts = mesh.nblocks * 17 ** 3
+    if args.nb != 8:
+        WORKLOAD["workload"] = WORKLOAD["workload"].replace(
+            "128^3 cells as 512", f"{16 * args.nb}^3 cells as {mesh.nblocks}").replace(
+            "[-16,16]^3", f"[-{lim:g},{lim:g}]^3")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident throughput: graph-captured steps -------------------
+    with torch.cuda.stream(stream):
+        ctx.evolve(dt, args.warmup)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    launches0 = Z.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    with torch.cuda.stream(stream):
+        ctx.evolve(dt, args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = Z.kernel_launches() - launches0
+    barrier()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = zones * args.steps * world / (ms * 1e-3)
+    finite = ctx.check_finite()
+
+    # ---- dominant kernel: the fused RHS+KO+stage kernel, timed alone -------
+    stage_ms = None
+    with torch.cuda.stream(stream):
+        ctx.upload(Z.REG_U, u_init)
+        ctx.init_finalize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 5
+        times = []
+        for _ in range(reps):
+            e0.record(stream)
+            ctx.rhs_stage(2, dt)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        stage_ms = sorted(times)[len(times) // 2]
+
+    if args.profile_run:
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "value": value, "stage_ms": stage_ms,
+                              "gpu_launches": launches}), flush=True)
+        ctx.close()
+        return
+
+    # ---- per-block plain path (one RHS launch per MeshBlock) ---------------
+    pb_steps = max(2, min(5, args.steps))
+    ctx.upload(Z.REG_U, u_init)
+    ctx.init_finalize()
+    ctx.set_per_block(True)
+    with torch.cuda.stream(stream):
+        ctx.evolve(dt, 1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.evolve(dt, pb_steps)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    pb_value = zones * pb_steps / (e0.elapsed_time(e1) * 1e-3)
+    ctx.set_per_block(False)
+
+    # ---- end to end through the public API with host buffers ----------------
+    # Every step: pinned host state -> device, one RK4 step, history norms
+    # (the step's result metric) and the state back to the host.
+    host = torch.from_numpy(u_init).pin_memory()
+    host_np = host.numpy()
+    out_host = torch.empty_like(host).pin_memory().numpy()
+    e2e_steps = max(2, min(args.steps, 5))
+    with torch.cuda.stream(stream):
+        ctx.upload(Z.REG_U, host_np)
+        ctx.evolve(dt, 1, with_constraints=True)
+        ctx.hst_norms()
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.upload(Z.REG_U, host_np)
+        ctx.evolve(dt, 1, with_constraints=True)
+        ctx.hst_norms()
+        ctx.download(Z.REG_U, out=out_host)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = zones * e2e_steps * world / e2e_s
+    state_bytes = host_np.nbytes
+
+    # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v = run_reference_cpu(2, threads)
+        if v is not None:
+            cpu = {"value": v, "unit": "zone-updates/s", "cores": threads, "kind": "reference",
+                   "sample": "reference OpenMP build (oracle/_ref/athena_ref) on the full "
+                             "workload, 2 RK4 steps, zone-cycles/omp_wsecond"}
+        else:
+            v, n = run_oracle_cpu()
+            cpu = {"value": v, "unit": "zone-updates/s", "cores": 1, "kind": "port",
+                   "sample": f"C oracle RHS on {n} MeshBlocks of 16^3, single thread"}
+
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    fp64_flops = 0.0  # FP64 operations per interior vertex per stage, from ncu
+    flops_file = os.path.join(ROOT, "profiles", "stage_kernel_fp64_ops.json")
+    if os.path.exists(flops_file):
+        with open(flops_file) as f:
+            fp64_flops = json.load(f).get("fp64_ops_per_point", 0.0)
+    fp64_peak_tf = ctx.fp64_probe()  # measured here: DFMA chains, 2 flops each
+    stage_s = stage_ms * 1e-3
+    achieved_gbs = STAGE_BYTES_PER_POINT * npts / stage_s / 1e9
+    if fp64_flops > 0:
+        achieved_tf = fp64_flops * npts / stage_s / 1e12
+        roof = {"bound": "fp64", "achieved": achieved_tf, "peak": fp64_peak_tf,
+                "unit": "TFLOP/s", "frac": achieved_tf / fp64_peak_tf, "traffic": None,
+                "hbm_achieved_gbs": achieved_gbs, "hbm_peak_gbs": hbm_peak,
+                "hbm_frac": achieved_gbs / hbm_peak, "kernel": "k_stage_ls",
+                "kernel_ms": stage_ms}
+    else:
+        roof = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved_gbs / hbm_peak, "traffic": None, "kernel": "k_stage_ls",
+                "kernel_ms": stage_ms}
+    traffic_file = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    if os.path.exists(traffic_file):
+        with open(traffic_file) as f:
+            roof["traffic"] = json.load(f).get("bytes_per_launch_full")
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (analytic puncture initial data)",
+        "config": dict(WORKLOAD, nb=nb, parallelism=f"replicas{world}",
+                       l2="inputs larger than L2 (1.4 GB per register)",
+                       per_block_value=pb_value, batched_over_per_block=value / world / pb_value,
+                       state_finite=finite),
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "zone-updates/s",
+                "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes + 64,
+                "note": "per step: pinned host state to device, one RK4 step, constraints "
+                        "and history norms to host, state back to host"},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main_reference(args, rank, world):
+    """The reference's own CPU implementation (the OpenMP build compiled from
+    the reference sources) on the same workload and metric; rank 0 only."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    nlim = max(1, args.steps)
+    v = run_reference_cpu(nlim, threads)
+    kind = "reference"
+    sample = f"reference OpenMP build, full workload, {nlim} RK4 steps"
+    if v is None:
+        v, n = run_oracle_cpu()
+        kind, threads = "port", 1
+        sample = f"C oracle RHS on {n} MeshBlocks of 16^3, single thread"
+    line = {"metric": METRIC, "value": v, "unit": "zone-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (analytic puncture initial data)",
+            "config": dict(WORKLOAD, parallelism="cpu"), "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": threads,
+                             "kind": kind, "sample": sample},
+            "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

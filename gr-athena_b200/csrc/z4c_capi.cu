@@ -2,6 +2,7 @@
 // operator launches, stage sequencing and the CUDA-graph-captured step.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -64,6 +65,22 @@ double mesh_gen_x(int64_t index, int64_t nrange, double xmin, double xmax) {
   return 0.5 * (xmin + xmax) + (rx * xmax - rx * xmin);
 }
 
+// Vertex coordinates x?f of one block along one axis (nn entries) and its
+// spacing, as Coordinates builds them for a uniform mesh
+// (coordinates/coordinates.cpp:170-198, mesh/mesh.cpp:2537-2556).
+double block_axis_coords(const z4c_mesh_desc_t* mesh, int loc, int axis, double* xf) {
+  const int nx = mesh->nx[axis], nb = mesh->nb[axis], nn = nx + 1 + 2 * Z4C_NG;
+  const int64_t nroot = (int64_t)nx * nb;
+  const double x0 = mesh->xmin[axis], x1 = mesh->xmax[axis];
+  const double bmin = (loc == 0) ? x0 : mesh_gen_x((int64_t)loc * nx, nroot, x0, x1);
+  const double bmax = (loc == nb - 1) ? x1 : mesh_gen_x((int64_t)(loc + 1) * nx, nroot, x0, x1);
+  for (int i = 0; i < nn; ++i)
+    xf[i] = mesh_gen_x((int64_t)(i - Z4C_NG) + (int64_t)loc * nx, nroot, x0, x1);
+  xf[Z4C_NG] = bmin;
+  xf[Z4C_NG + nx] = bmax;
+  return (bmax - bmin) / nx;
+}
+
 }  // namespace
 
 struct z4c_ctx {
@@ -90,6 +107,9 @@ struct z4c_ctx {
 
   // host copies
   std::vector<double> h_xf, h_xv, h_dx;  // h_dx: [nblocks][3]
+
+  // kernel nodes of the captured step (graph replays add this many launches)
+  long long graph_nodes = 0;
 
   // captured step
   cudaGraphExec_t graph = nullptr;
@@ -325,19 +345,10 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
     const int loc[3] = {b % g.nb[0], (b / g.nb[0]) % g.nb[1], b / (g.nb[0] * g.nb[1])};
     int off = 0, offv = 0;
     for (int a = 0; a < 3; ++a) {
-      const int64_t nroot = (int64_t)g.nx[a] * g.nb[a];
-      const double x0 = mesh->xmin[a], x1 = mesh->xmax[a];
-      const double bmin = (loc[a] == 0) ? x0 : mesh_gen_x((int64_t)loc[a] * g.nx[a], nroot, x0, x1);
-      const double bmax = (loc[a] == g.nb[a] - 1)
-                              ? x1 : mesh_gen_x((int64_t)(loc[a] + 1) * g.nx[a], nroot, x0, x1);
       double* xf = &c->h_xf[(size_t)b * nsum + off];
-      for (int i = 0; i < g.nn[a]; ++i)
-        xf[i] = mesh_gen_x((int64_t)(i - Z4C_NG) + (int64_t)loc[a] * g.nx[a], nroot, x0, x1);
-      xf[Z4C_NG] = bmin;
-      xf[Z4C_NG + g.nx[a]] = bmax;
+      const double dx = block_axis_coords(mesh, loc[a], a, xf);
       double* xv = &c->h_xv[(size_t)b * (nsum - 3) + offv];
       for (int i = 0; i < g.nn[a] - 1; ++i) xv[i] = 0.5 * (xf[i + 1] + xf[i]);
-      const double dx = (bmax - bmin) / g.nx[a];
       c->h_dx[(size_t)b * 3 + a] = dx;
       hfd[b].cidx1[a] = 1.0 / (dx * 60.0);
       hfd[b].cidx2[a] = ((1.0 / dx) * (1.0 / dx)) / 180.0;
@@ -466,6 +477,19 @@ int z4c_block_coords(const z4c_ctx* ctx, int block, int axis, double* x_out) {
   int off = 0;
   for (int a = 0; a < axis; ++a) off += ctx->g.nn[a];
   std::memcpy(x_out, &ctx->h_xf[(size_t)block * nsum + off], sizeof(double) * ctx->g.nn[axis]);
+  return Z4C_OK;
+}
+
+int z4c_mesh_block_coords(const z4c_mesh_desc_t* mesh, int block, int axis, double* x_out,
+                          double* dx_out) {
+  if (!mesh || !x_out || axis < 0 || axis > 2) return fail(Z4C_EINVAL, "bad argument");
+  const int nblocks = mesh->nb[0] * mesh->nb[1] * mesh->nb[2];
+  if (block < 0 || block >= nblocks || mesh->nx[axis] < 1)
+    return fail(Z4C_EINVAL, "block out of range");
+  const int loc[3] = {block % mesh->nb[0], (block / mesh->nb[0]) % mesh->nb[1],
+                      block / (mesh->nb[0] * mesh->nb[1])};
+  const double dx = block_axis_coords(mesh, loc[axis], axis, x_out);
+  if (dx_out) *dx_out = dx;
   return Z4C_OK;
 }
 
@@ -653,6 +677,45 @@ int z4c_stage(z4c_ctx* ctx, int stage, double dt) {
   return run_stage(ctx, stage, dt);
 }
 
+int z4c_rhs_stage(z4c_ctx* ctx, int stage, double dt) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  if (stage < 1 || stage > 4) return fail(Z4C_EINVAL, "stage %d outside 1..4", stage);
+  if (ctx->integrator != Z4C_INTEG_RK4)
+    return fail(Z4C_ESTATE, "z4c_rhs_stage runs the low-storage stage only");
+  const double* wt = kLsRk4[stage - 1];
+  LsStage ls{wt[0], wt[1], wt[2], wt[3], wt[4] * dt};
+  launch_stage_ls(ctx->g, ctx->dev(), ctx->reg[Z4C_REG_U], ctx->reg[Z4C_REG_U1],
+                  ctx->reg[Z4C_REG_W], ls, 0, ctx->g.nblocks, ctx->stream);
+  LAUNCH_CHECK("stage_ls");
+  return Z4C_OK;
+}
+
+int z4c_fp64_probe(z4c_ctx* ctx, double* tflops) {
+  if (!ctx || !tflops) return fail(Z4C_EINVAL, "null argument");
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+  const int iters = 4096;
+  double best = 0.0;
+  for (int rep = 0; rep < 3; ++rep) {
+    cudaEventRecord(e0, ctx->stream);
+    const long long flops = launch_fp64_probe(nsm, iters, ctx->partials, 8 * ctx->g.nblocks,
+                                              ctx->stream);
+    cudaEventRecord(e1, ctx->stream);
+    LAUNCH_CHECK("fp64_probe");
+    CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    best = std::max(best, flops / (ms * 1e-3) / 1e12);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *tflops = best;
+  return Z4C_OK;
+}
+
 int z4c_set_per_block(z4c_ctx* ctx, int per_block) {
   if (!ctx) return fail(Z4C_EINVAL, "null context");
   ctx->per_block = per_block != 0;
@@ -687,6 +750,7 @@ int z4c_evolve(z4c_ctx* ctx, double dt, int nsteps, int with_constraints) {
       ctx->graph = nullptr;
     }
     double* u_before = ctx->reg[Z4C_REG_U];
+    const long long count_before = kernel_launch_count();
     cudaGraph_t graph;
     CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     int rc = Z4C_OK;
@@ -699,13 +763,19 @@ int z4c_evolve(z4c_ctx* ctx, double dt, int nsteps, int with_constraints) {
       cudaGraphDestroy(graph);
       return fail(Z4C_ESTATE, "captured step does not return u to its buffer");
     }
+    // capture records kernels without running them
+    ctx->graph_nodes = kernel_launch_count() - count_before;
+    add_kernel_launches(-ctx->graph_nodes);
     ec = cudaGraphInstantiate(&ctx->graph, graph, 0);
     cudaGraphDestroy(graph);
     if (ec != cudaSuccess) return fail(Z4C_ECUDA, "graph instantiate: %s", cudaGetErrorString(ec));
     ctx->graph_dt = dt;
     ctx->graph_per_block = ctx->per_block;
   }
-  for (int n = 0; n < nsteps; ++n) CUDA_TRY(cudaGraphLaunch(ctx->graph, ctx->stream));
+  for (int n = 0; n < nsteps; ++n) {
+    CUDA_TRY(cudaGraphLaunch(ctx->graph, ctx->stream));
+    add_kernel_launches(ctx->graph_nodes);
+  }
   if (with_constraints) {
     const DevParams P = ctx->dev();
     launch_z4c_to_adm(ctx->g, P, ctx->reg[Z4C_REG_U], ctx->reg[Z4C_REG_ADM], 0, ctx->g.nblocks,
@@ -716,6 +786,8 @@ int z4c_evolve(z4c_ctx* ctx, double dt, int nsteps, int with_constraints) {
   }
   return Z4C_OK;
 }
+
+long long z4c_kernel_launches(void) { return kernel_launch_count(); }
 
 int z4c_check_finite(z4c_ctx* ctx, int reg) {
   if (!ctx) return fail(Z4C_EINVAL, "null context");

@@ -3,6 +3,8 @@
 // -ffp-contract=off build does.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "z4c_adm.cuh"
 #include "z4c_common.cuh"
 #include "z4c_kernels.cuh"
@@ -480,19 +482,45 @@ __global__ void k_zero_interior(Grid g, double* __restrict__ u, int nvar) {
   u[((int64_t)b * nvar + n) * g.nvol + ((int64_t)k * g.nn[1] + j) * g.nn[0] + i] = 0.0;
 }
 
+// 8 independent DFMA chains per thread; the result is stored so that the
+// compiler keeps the work.  Built with -fmad=false: the fma() intrinsic is an
+// explicit DFMA and is not affected.
+__global__ void __launch_bounds__(256) k_fp64_probe(int iters, double* sink, int nsink) {
+  double a[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) a[q] = 1.0 + 1e-9 * (threadIdx.x + q);
+  const double m = 0.999999999, c = 1e-9;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a[q] = fma(a[q], m, c);
+  }
+  double s = 0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) s += a[q];
+  // never true; keeps the chains live
+  if (s == 12345.6789 && (int)blockIdx.x < nsink) sink[blockIdx.x] = s;
+}
+
 }  // namespace
 
 // ---- launchers -----------------------------------------------------------------
 
+static std::atomic<long long> g_launches{0};
+long long kernel_launch_count() { return g_launches.load(); }
+void add_kernel_launches(long long n) { g_launches += n; }
+#define COUNTED ++g_launches;
+
 void launch_rhs(const Grid& g, const DevParams& P, const double* u, double* rhs, int block0,
                 int nblk, cudaStream_t st) {
   const int64_t n = interior_count(g) * nblk;
+  COUNTED
   k_rhs<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, rhs, block0, nblk);
 }
 
 void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, double* u1,
                      double* u_out, const LsStage& w, int block0, int nblk, cudaStream_t st) {
   const int64_t n = interior_count(g) * nblk;
+  COUNTED
   k_stage_ls<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, u1, u_out, w, block0,
                                                               nblk);
 }
@@ -503,6 +531,7 @@ void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const d
   KPtrs K;
   for (int s = 0; s < 4; ++s) K.k[s] = k[s];
   const int64_t n = interior_count(g) * nblk;
+  COUNTED
   k_stage_bt<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, un, K, u_out, w, block0,
                                                               nblk);
 }
@@ -510,6 +539,7 @@ void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const d
 void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst, int nvar,
                      const int* nbr, int fuse_alg, cudaStream_t st) {
   const int64_t n = g.nvol * g.nblocks;
+  COUNTED
   k_exchange<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, src, dst, nvar, nbr,
                                                                   fuse_alg);
 }
@@ -521,6 +551,7 @@ void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st) {
   for (int ax = 0; ax < 3; ++ax) {
     const int o1 = (ax + 1) % 3, o2 = (ax + 2) % 3;
     const int64_t n = (int64_t)g.nn[o1] * g.nn[o2] * nvar * 2 * g.nblocks;
+    COUNTED
     k_bc_axis<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, u, nvar, ax);
   }
 }
@@ -528,6 +559,7 @@ void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st) {
 void launch_alg_constr(const Grid& g, const DevParams& P, double* u, int block0, int nblk,
                        cudaStream_t st, int ghosts_only) {
   const int64_t n = g.nvol * nblk;
+  COUNTED
   k_alg_constr<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, block0, nblk,
                                                                     ghosts_only);
 }
@@ -535,6 +567,7 @@ void launch_alg_constr(const Grid& g, const DevParams& P, double* u, int block0,
 void launch_weighted_ave(const Grid& g, double* out, const double* in1, const double* in2,
                          const double w[3], int block0, int nblk, cudaStream_t st) {
   const int64_t n = interior_count(g) * nblk * NVAR;
+  COUNTED
   k_weighted_ave<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(
       g, out, in1, in2, w[0], w[1], w[2], block0, nblk);
 }
@@ -542,12 +575,14 @@ void launch_weighted_ave(const Grid& g, double* out, const double* in1, const do
 void launch_add_rhs(const Grid& g, const double* rhs, double wght, double* out, int block0,
                     int nblk, cudaStream_t st) {
   const int64_t n = interior_count(g) * nblk * NVAR;
+  COUNTED
   k_add_rhs<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, rhs, wght, out, block0, nblk);
 }
 
 void launch_z4c_to_adm(const Grid& g, const DevParams& P, const double* u, double* adm,
                        int block0, int nblk, cudaStream_t st, int ghosts_only) {
   const int64_t n = g.nvol * nblk;
+  COUNTED
   k_z4c_to_adm<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, adm, block0, nblk,
                                                                     ghosts_only);
 }
@@ -556,10 +591,13 @@ void launch_adm_to_z4c(const Grid& g, const DevParams& P, const double* adm, dou
                        double* guu_scratch, int block0, int nblk, cudaStream_t st) {
   const int64_t n = g.nvol * nblk;
   // guu_scratch is indexed by absolute block number
+  COUNTED
   k_adm_to_z4c_pt<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, adm, u, guu_scratch,
                                                                       block0, nblk);
+  COUNTED
   k_adm_to_z4c_gam<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, guu_scratch, u,
                                                                        block0, nblk);
+  COUNTED
   k_alg_constr<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, block0, nblk, 0);
 }
 
@@ -567,22 +605,33 @@ void launch_adm_constraints(const Grid& g, const DevParams& P, const double* adm
                             const double* u, double* con, const double* xf, int block0,
                             int nblk, cudaStream_t st) {
   const int64_t n = g.nvol * nblk;
+  COUNTED
   k_adm_constraints<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, adm, u, con, xf,
                                                                     block0, nblk);
 }
 
 void launch_hst(const Grid& g, const DevParams& P, const double* con, const double* u,
                 const double* xv, double* partials, cudaStream_t st) {
+  COUNTED
   k_hst<<<g.nblocks, 256, 0, st>>>(g, P, con, u, xv, partials);
 }
 
 void launch_check_finite(const Grid& g, const double* u, int nvar, int* flag, cudaStream_t st) {
   const int64_t n = g.nvol * g.nblocks * nvar;
+  COUNTED
   k_check_finite<<<1184, 256, 0, st>>>(n, u, flag);
+}
+
+long long launch_fp64_probe(int nsm, int iters, double* sink, int nsink, cudaStream_t st) {
+  const int blocks = nsm * 8;
+  COUNTED
+  k_fp64_probe<<<blocks, 256, 0, st>>>(iters, sink, nsink);
+  return 2LL * 8 * iters * 256LL * blocks;
 }
 
 void launch_zero_interior(const Grid& g, double* u, int nvar, cudaStream_t st) {
   const int64_t n = interior_count(g) * g.nblocks * nvar;
+  COUNTED
   k_zero_interior<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, u, nvar);
 }
 

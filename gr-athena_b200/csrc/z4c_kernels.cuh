@@ -44,6 +44,10 @@ __host__ __device__ __forceinline__ int64_t interior_count(const Grid& g) {
 
 // ---- launchers (host side) ----------------------------------------------
 
+// Process-wide count of kernels launched by the launchers below.
+long long kernel_launch_count();
+void add_kernel_launches(long long n);
+
 // All launches return cudaGetLastError() mapped by the caller.
 void launch_rhs(const Grid& g, const DevParams& P, const double* u, double* rhs,
                 int block0, int nblk, cudaStream_t st);
@@ -72,5 +76,8 @@ void launch_hst(const Grid& g, const DevParams& P, const double* con, const doub
                 const double* xv, double* partials, cudaStream_t st);
 void launch_check_finite(const Grid& g, const double* u, int nvar, int* flag, cudaStream_t st);
 void launch_zero_interior(const Grid& g, double* u, int nvar, cudaStream_t st);
+// FP64 throughput probe: dependent DFMA chains on every SM; returns the
+// flops issued (2 per DFMA).  sink receives one value per CTA.
+long long launch_fp64_probe(int nsm, int iters, double* sink, int nsink, cudaStream_t st);
 
 }  // namespace z4c

@@ -42,11 +42,12 @@ HST_COLUMNS = ("H-norm2", "M-norm2", "Mx-norm2", "My-norm2", "Mz-norm2", "Z-norm
 EXPORTS = (
     "z4c_params_default", "z4c_last_error", "z4c_create", "z4c_destroy",
     "z4c_set_stream", "z4c_sync", "z4c_num_blocks", "z4c_block_nn", "z4c_reg_nvar",
-    "z4c_dx", "z4c_block_coords", "z4c_upload", "z4c_download", "z4c_device_ptr",
+    "z4c_dx", "z4c_block_coords", "z4c_mesh_block_coords", "z4c_upload", "z4c_download", "z4c_device_ptr",
     "z4c_rhs", "z4c_add_rhs", "z4c_weighted_ave", "z4c_alg_constr", "z4c_adm_to_z4c",
     "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_ghost_fill", "z4c_init_finalize",
     "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
-    "z4c_get_tile", "z4c_check_finite")
+    "z4c_get_tile", "z4c_check_finite", "z4c_kernel_launches", "z4c_rhs_stage",
+    "z4c_fp64_probe")
 
 
 class Z4cError(RuntimeError):
@@ -98,6 +99,7 @@ def lib():
         L.z4c_reg_nvar.argtypes = [ip]
         L.z4c_dx.argtypes = [vp, dp]
         L.z4c_block_coords.argtypes = [vp, ip, ip, dp]
+        L.z4c_mesh_block_coords.argtypes = [C.POINTER(MeshDesc), ip, ip, dp, dp]
         L.z4c_upload.argtypes = [vp, ip, ip, dp]
         L.z4c_download.argtypes = [vp, ip, ip, dp]
         L.z4c_device_ptr.argtypes = [vp, ip, C.POINTER(dp)]
@@ -117,6 +119,10 @@ def lib():
         L.z4c_set_tile.argtypes = [vp, ip, ip, ip]
         L.z4c_get_tile.argtypes = [vp, C.POINTER(C.c_int)]
         L.z4c_check_finite.argtypes = [vp, ip]
+        L.z4c_rhs_stage.argtypes = [vp, ip, C.c_double]
+        L.z4c_fp64_probe.argtypes = [vp, dp]
+        L.z4c_kernel_launches.argtypes = []
+        L.z4c_kernel_launches.restype = C.c_longlong
         _lib = L
     return _lib
 
@@ -125,6 +131,12 @@ def _check(rc):
     if rc < 0:
         raise Z4cError(rc, lib().z4c_last_error().decode())
     return rc
+
+
+def kernel_launches():
+    """Kernels this library has launched in this process (graph replays
+    count every kernel node)."""
+    return int(lib().z4c_kernel_launches())
 
 
 def default_params(**overrides):
@@ -165,6 +177,21 @@ class Mesh:
         for f in range(6):
             d.bc[f] = self.bc[f]
         return d
+
+    def block_coords(self, block):
+        """Vertex coordinates (x, y, z) and spacing of one block, computed on
+        the host exactly as the reference's Coordinates constructor does."""
+        xs, dxs = [], []
+        d = self.desc()
+        for a in range(3):
+            x = np.empty(self.nn[a])
+            dx = C.c_double()
+            _check(lib().z4c_mesh_block_coords(C.byref(d), block, a,
+                                               x.ctypes.data_as(C.POINTER(C.c_double)),
+                                               C.byref(dx)))
+            xs.append(x)
+            dxs.append(dx.value)
+        return xs, dxs
 
     def zones(self):
         """Cells of the mesh (the reference's zone count, mesh.hpp:289-292)."""
@@ -214,8 +241,10 @@ class Z4c:
             raise ValueError(f"shape {a.shape} != {self.shape(reg, block)}")
         _check(lib().z4c_upload(self._h, reg, block, a.ctypes.data_as(C.POINTER(C.c_double))))
 
-    def download(self, reg, block=-1):
-        a = np.empty(self.shape(reg, block))
+    def download(self, reg, block=-1, out=None):
+        a = np.empty(self.shape(reg, block)) if out is None else out
+        if a.shape != self.shape(reg, block) or a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise ValueError("output array has the wrong shape, dtype or layout")
         _check(lib().z4c_download(self._h, reg, block, a.ctypes.data_as(C.POINTER(C.c_double))))
         return a
 
@@ -280,6 +309,15 @@ class Z4c:
 
     def evolve(self, dt, nsteps, with_constraints=False):
         _check(lib().z4c_evolve(self._h, float(dt), int(nsteps), int(bool(with_constraints))))
+
+    def rhs_stage(self, stage, dt):
+        """Fused RHS + low-storage stage update, without the ghost exchange."""
+        _check(lib().z4c_rhs_stage(self._h, int(stage), float(dt)))
+
+    def fp64_probe(self):
+        t = C.c_double()
+        _check(lib().z4c_fp64_probe(self._h, C.byref(t)))
+        return t.value
 
     def set_per_block(self, flag):
         _check(lib().z4c_set_per_block(self._h, int(bool(flag))))

@@ -145,6 +145,12 @@ int z4c_block_nn(const z4c_ctx *ctx, int axis);
 int z4c_reg_nvar(int reg);
 int z4c_dx(const z4c_ctx *ctx, double dx_out[3]);
 int z4c_block_coords(const z4c_ctx *ctx, int block, int axis, double *x_out);
+/* The same coordinates without a context (host only): vertex coordinates of
+ * one block along one axis (nx+1+2*Z4C_NG entries) and its spacing, built as
+ * the reference's Coordinates constructor does for a uniform mesh
+ * (coordinates/coordinates.cpp:170-198, mesh/mesh.hpp:839-945). */
+int z4c_mesh_block_coords(const z4c_mesh_desc_t *mesh, int block, int axis, double *x_out,
+                          double *dx_out);
 
 /* Host <-> device copies of a register; block = -1 for the whole mesh.  The
  * host buffer uses the reference layout (see above). */
@@ -202,6 +208,14 @@ int z4c_stage(z4c_ctx *ctx, int stage, double dt);
  * When with_constraints is non-zero the last stage of the last step also
  * runs Z4cToADM and ADMConstraints. */
 int z4c_evolve(z4c_ctx *ctx, double dt, int nsteps, int with_constraints);
+/* Z4c::Z4cRHS + GR_Z4c::IntegrateZ4c of one low-storage stage as a single
+ * fused launch over all blocks, without the ghost exchange that follows:
+ * reads u and u1, writes the updated interior into the work register and
+ * u1.  Used to time the dominant kernel in isolation. */
+int z4c_rhs_stage(z4c_ctx *ctx, int stage, double dt);
+/* Measured FP64 throughput of the device (dependent DFMA chains on every SM,
+ * 2 flops per DFMA), in TFLOP/s; the denominator of the FP64 roofline. */
+int z4c_fp64_probe(z4c_ctx *ctx, double *tflops);
 /* Selects the per-block launch loop (plain path, one RHS launch per block per
  * stage) instead of the batched launch inside z4c_stage/z4c_evolve. */
 int z4c_set_per_block(z4c_ctx *ctx, int per_block);
@@ -209,6 +223,9 @@ int z4c_set_per_block(z4c_ctx *ctx, int per_block);
  * i, j and k.  Returns Z4C_EINVAL for unsupported shapes. */
 int z4c_set_tile(z4c_ctx *ctx, int ti, int tj, int tk);
 int z4c_get_tile(const z4c_ctx *ctx, int tile_out[3]);
+/* Kernels launched by this library in this process so far (graph replays
+ * count every kernel node); a diagnostic with no reference counterpart. */
+long long z4c_kernel_launches(void);
 /* Scans a register for NaN/Inf (z4c/z4c_utils.cpp:18-150 is_finite_*):
  * Z4C_OK if all finite, Z4C_ENONFINITE otherwise. */
 int z4c_check_finite(z4c_ctx *ctx, int reg);

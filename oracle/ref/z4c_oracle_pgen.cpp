@@ -190,9 +190,13 @@ void MeshBlock::ProblemGenerator(ParameterInput* pin) {
   z->ADMToZ4c(z->storage.adm, z->storage.u);
 }
 
+// Called at the top of every main-loop iteration (main.cpp:167): only the
+// first call sees the initial state.
 void Mesh::UserWorkBeforeLoop(ParameterInput* pin) {
+  static bool dumped = false;
   const std::string path = pin->GetOrAddString("problem", "dump_initial", "");
-  if (!path.empty()) z4c_oracle::DumpMesh(this, path);
+  if (!path.empty() && !dumped) z4c_oracle::DumpMesh(this, path);
+  dumped = true;
 }
 
 void Mesh::UserWorkAfterLoop(ParameterInput* pin) {

@@ -1,0 +1,163 @@
+"""Generates the golden fixtures in tests/golden/ by running the GR-Athena++
+reference CPU build (oracle/ref, built from the reference sources) on small
+cases.  Run from the repository root:
+
+    make -C oracle/ref -j8          # needs the reference checkout
+    python tests/golden/make_golden.py
+
+Fixtures (numpy .npz, compressed):
+  ops_<case>.npz    one Mesh after initialisation ("u0") and the reference's
+                    output of every operator on it plus every stage of one
+                    time step (records written by oracle/ref/z4c_ops_driver.cpp)
+  evol_<case>.npz   a multi-step run of the stock reference driver: the
+                    history table (outputs/history.cpp columns) and the
+                    initial and final states
+Each fixture stores the input-deck parameters it was made with ("params",
+"mesh", "integrator" as JSON strings).
+"""
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF_BIN = os.path.join(ROOT, "oracle", "_ref")
+sys.path.insert(0, HERE)
+from z4cio import read_records  # noqa: E402
+
+OPS_KEEP = ["meta", "xf", "xv", "dx", "time_dt", "u0", "rhs0", "alg0", "adm0", "con0",
+            "uadm0", "gx_pre", "gx_post", "s1_rhs", "s1_alg", "s2_alg", "s3_alg", "s4_alg",
+            "s4_adm", "s4_con"]
+
+# run-time options of the cases (reference <z4c> block); r_max_con is always
+# given explicitly: the reference turns its +inf default into 0 on every
+# MeshBlock after the first (parameter_input.cpp:129-135, 732-752).
+GAUGE_WAVE = dict(lapse_harmonic=1.0, lapse_harmonicf=0.0, lapse_oplog=0.0,
+                  lapse_advect=0.0, shift_Gamma=0.0, shift_eta=0.0, shift_advect=0.0,
+                  diss=0.02, damp_kappa1=0.02, damp_kappa2=0.0, r_max_con=1e300)
+PUNCTURE = dict(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02, damp_kappa2=0.0,
+                shift_eta=2.0, r_max_con=1e300)
+
+CASES = {
+    # configs[0] physics on one 8^3 block (periodic)
+    "gw1": dict(test="gauge_wave1", z4c=GAUGE_WAVE, integ="rk4", bc="periodic",
+                mesh=[(8, -0.5, 0.5, 8)] * 3, extra={"AwA_amplitude": 0.01}),
+    # one puncture, two blocks along x, outflow faces (configs[1] gauge)
+    "punc2": dict(test="one_puncture", z4c=PUNCTURE, integ="rk4", bc="extrapolate_outflow",
+                  mesh=[(16, -4.0, 4.0, 8), (8, -2.0, 2.0, 8), (8, -2.0, 2.0, 8)],
+                  extra={}, problem={"punc_ADM_mass": 1.0}),
+    # the reference's robust-stability noise, two periodic blocks, Butcher RK4
+    "rs2": dict(test="robust_stability", z4c=PUNCTURE, integ="bt_rk4", bc="periodic",
+                mesh=[(16, -4.0, 4.0, 8), (8, -2.0, 2.0, 8), (8, -2.0, 2.0, 8)],
+                extra={"AwA_amplitude": 1e-10}),
+}
+
+EVOL = {
+    # configs[0] gauge wave, one 16^3 block, 40 steps, history every step
+    "gw16": dict(test="gauge_wave1", z4c=GAUGE_WAVE, integ="rk4", bc="periodic",
+                 mesh=[(16, -0.5, 0.5, 16)] * 3, extra={"AwA_amplitude": 0.01}, nlim=40),
+    # one puncture on 2x2x1 blocks with outflow boundaries, 12 steps
+    "punc4": dict(test="one_puncture", z4c=PUNCTURE, integ="rk4", bc="extrapolate_outflow",
+                  mesh=[(16, -4.0, 4.0, 8), (16, -4.0, 4.0, 8), (8, -2.0, 2.0, 8)], extra={},
+                  problem={"punc_ADM_mass": 1.0}, nlim=12),
+}
+
+
+def deck(case, out_file, nlim=1, dump_initial="", dump_final="", hst=False):
+    lines = ["<job>", "problem_id = golden", "<z4c>"]
+    for k, v in {**case["z4c"], **case.get("extra", {})}.items():
+        lines.append(f"{k} = {v!r}" if isinstance(v, float) else f"{k} = {v}")
+    lines += ["<task_triggers>", "adjust_mesh_dt = false",
+              "<time>", "cfl_number = 0.25", "tlim = 1e10", f"nlim = {nlim}",
+              f"integrator = {case['integ']}", "ncycle_out = 1000000", "<mesh>"]
+    for a, (nx, lo, hi, _) in enumerate(case["mesh"]):
+        d = a + 1
+        lines += [f"nx{d} = {nx}", f"x{d}min = {lo!r}", f"x{d}max = {hi!r}",
+                  f"ix{d}_bc = {case['bc']}", f"ox{d}_bc = {case['bc']}"]
+    lines += ["refinement = none", "num_threads = 1", "<meshblock>"]
+    for a, (_, _, _, nb) in enumerate(case["mesh"]):
+        lines.append(f"nx{a + 1} = {nb}")
+    lines += ["<problem>", f"test = {case['test']}"]
+    for k, v in case.get("problem", {}).items():
+        lines.append(f"{k} = {v}")
+    if dump_initial:
+        lines.append(f"dump_initial = {dump_initial}")
+    if dump_final:
+        lines.append(f"dump_final = {dump_final}")
+    lines += ["<driver>", f"out = {out_file}"]
+    if hst:
+        lines += ["<output1>", "file_type = hst", "dt = 1e-12", "data_format = %.17e"]
+    return "\n".join(lines) + "\n"
+
+
+def meta_json(case):
+    nb = [m[0] // m[3] for m in case["mesh"]]
+    nx = [m[3] for m in case["mesh"]]
+    bc = 0 if case["bc"] == "periodic" else 1
+    mesh = dict(nb=nb, nx=nx, xmin=[m[1] for m in case["mesh"]],
+                xmax=[m[2] for m in case["mesh"]], bc=[bc] * 6)
+    return dict(params=json.dumps(case["z4c"]), mesh=json.dumps(mesh),
+                integrator=json.dumps(case["integ"]))
+
+
+def make_ops(name, case, outdir):
+    with tempfile.TemporaryDirectory() as tmp:
+        rec_path = os.path.join(tmp, "ops.rec")
+        inp = os.path.join(tmp, "case.inp")
+        with open(inp, "w") as f:
+            f.write(deck(case, rec_path))
+        subprocess.run([os.path.join(REF_BIN, "z4c_ops_ref"), "-i", inp], cwd=tmp, check=True,
+                       stdout=subprocess.DEVNULL)
+        rec = read_records(rec_path)
+    out = {k: rec[k] for k in OPS_KEEP}
+    out.update(meta_json(case))
+    path = os.path.join(outdir, f"ops_{name}.npz")
+    np.savez_compressed(path, **out)
+    return path
+
+
+def parse_hst(path):
+    rows = []
+    with open(path) as f:
+        for line in f:
+            if line.startswith("#"):
+                continue
+            rows.append([float(x) for x in line.split()])
+    return np.array(rows)
+
+
+def make_evol(name, case, outdir):
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = os.path.join(tmp, "case.inp")
+        init, final = os.path.join(tmp, "init.rec"), os.path.join(tmp, "final.rec")
+        with open(inp, "w") as f:
+            f.write(deck(case, "unused", nlim=case["nlim"], dump_initial=init,
+                         dump_final=final, hst=True))
+        subprocess.run([os.path.join(REF_BIN, "athena_ref"), "-i", inp], cwd=tmp, check=True,
+                       stdout=subprocess.DEVNULL)
+        hst = parse_hst(os.path.join(tmp, "golden.hst"))
+        r0, r1 = read_records(init), read_records(final)
+    out = dict(hst=hst, meta=r0["meta"], xf=r0["xf"], xv=r0["xv"], dx=r0["dx"],
+               time_dt=r1["time_dt"], u_init=r0["u"], u_final=r1["u"],
+               con_final=r1["con"], nlim=np.array(case["nlim"]))
+    out.update(meta_json(case))
+    path = os.path.join(outdir, f"evol_{name}.npz")
+    np.savez_compressed(path, **out)
+    return path
+
+
+def main():
+    for name, case in CASES.items():
+        p = make_ops(name, case, HERE)
+        print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
+    for name, case in EVOL.items():
+        p = make_evol(name, case, HERE)
+        print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
+
+
+if __name__ == "__main__":
+    main()

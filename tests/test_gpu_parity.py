@@ -1,0 +1,110 @@
+"""B200 path against the reference's own outputs (golden fixtures produced by
+the reference CPU build).  Every operator is called through the C ABI.
+Tolerance: normwise relative 1e-12 per register (the reference's FP64 RHS
+agreement bound); most records agree bit for bit, the exceptions being values
+that pass through pow/cbrt, whose CUDA and glibc roundings may differ by an
+ulp."""
+import numpy as np
+import pytest
+
+from z4c_testlib import Case, rel_err
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+OPS = ["ops_gw1", "ops_punc2", "ops_rs2"]
+
+
+def make_ctx(c):
+    import z4c_b200 as Z
+    m = c.mesh
+    mesh = Z.Mesh(m["nb"], m["nx"], m["xmin"], m["xmax"], m["bc"])
+    return Z, Z.Z4c(mesh, Z.default_params(**c.params), c.integrator)
+
+
+@pytest.mark.parametrize("name", OPS)
+@pytest.mark.parametrize("per_block", [False, True])
+def test_operators(name, per_block):
+    c = Case(name)
+    Z, ctx = make_ctx(c)
+    blk = -1
+    I = c.interior()
+    u0 = c.to_grid(c.rec["u0"])
+    ctx.upload(Z.REG_U, u0)
+    if per_block:
+        for b in range(ctx.nblocks):
+            ctx.Z4cRHS(Z.REG_U, Z.REG_RHS, b)
+    else:
+        ctx.Z4cRHS(Z.REG_U, Z.REG_RHS, blk)
+    rhs = c.from_grid(ctx.download(Z.REG_RHS))
+    assert rel_err(rhs[I], c.rec["rhs0"][I]) <= TOL
+    ctx.AlgConstr(Z.REG_U)
+    assert rel_err(c.from_grid(ctx.download(Z.REG_U)), c.rec["alg0"]) <= TOL
+    ctx.upload(Z.REG_U, u0)
+    ctx.Z4cToADM()
+    assert rel_err(c.from_grid(ctx.download(Z.REG_ADM)), c.rec["adm0"]) <= TOL
+    ctx.ADMConstraints()
+    assert rel_err(c.from_grid(ctx.download(Z.REG_CON)), c.rec["con0"]) <= TOL
+    ctx.upload(Z.REG_ADM, c.to_grid(c.rec["adm0"]))
+    ctx.ADMToZ4c(Z.REG_ADM, Z.REG_RHS)
+    assert rel_err(c.from_grid(ctx.download(Z.REG_RHS)), c.rec["uadm0"]) <= TOL
+    ctx.upload(Z.REG_U, c.to_grid(c.rec["gx_pre"]))
+    ctx.ghost_fill(Z.REG_U)
+    assert np.array_equal(c.from_grid(ctx.download(Z.REG_U)), c.rec["gx_post"])
+    ctx.close()
+
+
+@pytest.mark.parametrize("name", OPS)
+@pytest.mark.parametrize("mode", ["batched", "per_block", "graph"])
+def test_one_step_stage_by_stage(name, mode):
+    c = Case(name)
+    Z, ctx = make_ctx(c)
+    dt = c.rec["time_dt"][1]
+    ctx.upload(Z.REG_U, c.to_grid(c.rec["u0"]))
+    ctx.set_per_block(mode == "per_block")
+    if mode == "graph":
+        ctx.evolve(dt, 1, with_constraints=True)
+    else:
+        for s in range(1, 5):
+            ctx.stage(s, dt)
+            u = c.from_grid(ctx.download(Z.REG_U))
+            assert rel_err(u, c.rec[f"s{s}_alg"]) <= TOL, f"stage {s}"
+        ctx.constraints()
+    assert rel_err(c.from_grid(ctx.download(Z.REG_U)), c.rec["s4_alg"]) <= TOL
+    assert rel_err(c.from_grid(ctx.download(Z.REG_ADM)), c.rec["s4_adm"]) <= TOL
+    assert rel_err(c.from_grid(ctx.download(Z.REG_CON)), c.rec["s4_con"]) <= TOL
+    ctx.close()
+
+
+@pytest.mark.parametrize("name", ["evol_gw16", "evol_punc4"])
+def test_evolution_history_and_final_state(name):
+    """Multi-step evolution from the reference's initial state (captured CUDA
+    graph) against the reference driver's final state and .hst norms."""
+    c = Case(name)
+    Z, ctx = make_ctx(c)
+    nlim = int(c.rec["nlim"])
+    dt = c.rec["time_dt"][1]
+    ctx.upload(Z.REG_U, c.to_grid(c.rec["u_init"]))
+    ctx.evolve(dt, nlim, with_constraints=True)
+    u = c.from_grid(ctx.download(Z.REG_U))
+    assert rel_err(u, c.rec["u_final"]) <= 1e-11
+    hst = ctx.hst_norms()
+    ref = c.rec["hst"][nlim, 3:11]
+    np.testing.assert_allclose(hst, ref, rtol=1e-9, atol=1e-30)
+    ctx.close()
+
+
+@pytest.mark.parametrize("name", ["evol_gw16", "evol_punc4"])
+def test_initial_data_on_device(name):
+    """Host initial data -> device ADMToZ4c -> ghost finalisation reproduces
+    the reference's initialised state."""
+    from z4c_b200 import initial_data as ID
+    c = Case(name)
+    Z, ctx = make_ctx(c)
+    if "gw" in name:
+        adm = ID.gauge_wave1(ctx.mesh, amplitude=0.01)
+    else:
+        adm = ID.punctures(ctx.mesh, ctx.params, masses=(1.0,), centres=((0.0, 0.0, 0.0),))
+    ID.load_adm(ctx, adm)
+    u = c.from_grid(ctx.download(Z.REG_U))
+    assert rel_err(u, c.rec["u_init"]) <= 1e-14
+    ctx.close()

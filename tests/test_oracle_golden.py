@@ -1,0 +1,106 @@
+"""The CPU oracle against the golden fixtures produced by the reference
+build itself (tests/golden/make_golden.py).  The oracle restates the
+reference's arithmetic in the same order, so agreement is bit for bit."""
+import numpy as np
+import pytest
+
+import z4c_oracle as O
+from z4c_testlib import Case, bitwise
+
+OPS = ["ops_gw1", "ops_punc2", "ops_rs2"]
+
+
+def _params(case):
+    return O.default_params(**case.params)
+
+
+@pytest.mark.parametrize("name", OPS)
+def test_single_operators(name):
+    c = Case(name)
+    p = _params(c)
+    blocks = c.blocks()
+    u0, adm0 = c.rec["u0"], c.rec["adm0"]
+    I = c.interior()
+    rhs = np.stack([O.rhs(b, p, u0[g]) for g, b in enumerate(blocks)])
+    assert bitwise(rhs[I], c.rec["rhs0"][I])
+    alg = np.stack([O.algconstr(b, p, u0[g]) for g, b in enumerate(blocks)])
+    assert bitwise(alg, c.rec["alg0"])
+    adm = np.stack([O.z4c_to_adm(b, p, u0[g]) for g, b in enumerate(blocks)])
+    assert bitwise(adm, adm0)
+    con = np.stack([O.adm_constraints(b, p, adm0[g], u0[g]) for g, b in enumerate(blocks)])
+    assert bitwise(con, c.rec["con0"])
+    uadm = np.stack([O.adm_to_z4c(b, p, adm0[g]) for g, b in enumerate(blocks)])
+    assert bitwise(uadm, c.rec["uadm0"])
+
+
+@pytest.mark.parametrize("name", OPS)
+def test_ghost_exchange(name):
+    c = Case(name)
+    bc = c.mesh["bc"]
+    out = c.from_grid(O.mesh_exchange(c.nb, c.nx, bc, c.to_grid(c.rec["gx_pre"])))
+    assert bitwise(out, c.rec["gx_post"])
+
+
+def oracle_step(c, p, blocks, u, dt):
+    """One full step of the GR_Z4c task list on the oracle (gid order)."""
+    nb = len(blocks)
+    u = u.copy()
+    if c.integrator == "rk4":
+        u1 = np.zeros_like(u)
+        for s in range(4):
+            w = O.LS_RK4[s]
+            r = np.stack([O.rhs(blocks[b], p, u[b]) for b in range(nb)])
+            for b in range(nb):
+                O.weighted_ave(u1[b], u[b], None, [1.0, w["delta"], 0.0], c.nn)
+                O.weighted_ave(u[b], u1[b], None, [w["gamma_1"], w["gamma_2"], w["gamma_3"]], c.nn)
+                O.add_rhs(r[b], w["beta"] * dt, u[b], c.nn)
+            u = c.from_grid(O.mesh_exchange(c.nb, c.nx, c.mesh["bc"], c.to_grid(u)))
+            u = np.stack([O.algconstr(blocks[b], p, u[b]) for b in range(nb)])
+            yield u
+    else:
+        un, ks = u.copy(), []
+        for s in range(4):
+            ks.append(np.stack([O.rhs(blocks[b], p, u[b]) for b in range(nb)]))
+            u = un.copy()
+            coefs = O.BT_RK4_A[s + 1][: s + 1] if s < 3 else O.BT_RK4_B
+            for q, a in enumerate(coefs):
+                if a != 0:
+                    u += (a * dt) * ks[q]
+            u = c.from_grid(O.mesh_exchange(c.nb, c.nx, c.mesh["bc"], c.to_grid(u)))
+            u = np.stack([O.algconstr(blocks[b], p, u[b]) for b in range(nb)])
+            yield u
+
+
+@pytest.mark.parametrize("name", OPS)
+def test_one_step_stage_by_stage(name):
+    c = Case(name)
+    p = _params(c)
+    blocks = c.blocks()
+    dt = c.rec["time_dt"][1]
+    for s, u in enumerate(oracle_step(c, p, blocks, c.rec["u0"], dt)):
+        assert bitwise(u, c.rec[f"s{s + 1}_alg"]), f"stage {s + 1}"
+    adm = np.stack([O.z4c_to_adm(b, p, u[g]) for g, b in enumerate(blocks)])
+    assert bitwise(adm, c.rec["s4_adm"])
+    con = np.stack([O.adm_constraints(b, p, adm[g], u[g]) for g, b in enumerate(blocks)])
+    assert bitwise(con, c.rec["s4_con"])
+
+
+@pytest.mark.parametrize("name", ["evol_gw16", "evol_punc4"])
+def test_evolution_and_history(name):
+    """Multi-step run of the stock reference driver: final state and the
+    history-output constraint norms (outputs/history.cpp:168-200)."""
+    c = Case(name)
+    p = _params(c)
+    blocks = c.blocks()
+    dt = c.rec["time_dt"][1]
+    u = c.rec["u_init"]
+    for _ in range(int(c.rec["nlim"])):
+        for u in oracle_step(c, p, blocks, u, dt):
+            pass
+    assert bitwise(u, c.rec["u_final"])
+    adm = np.stack([O.z4c_to_adm(b, p, u[g]) for g, b in enumerate(blocks)])
+    con = np.stack([O.adm_constraints(b, p, adm[g], u[g]) for g, b in enumerate(blocks)])
+    assert bitwise(con, c.rec["con_final"])
+    hst = O.hst_norms(blocks, p, con, u)
+    ref = c.rec["hst"][int(c.rec["nlim"]), 3:11]
+    np.testing.assert_allclose(hst, ref, rtol=1e-13, atol=0)
