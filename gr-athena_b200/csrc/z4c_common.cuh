@@ -47,6 +47,12 @@ struct Grid {
 
 // ---- stencils -----------------------------------------------------------
 
+#ifdef FD_BARRIER
+#define FD_FENCE() asm volatile("" ::: "memory")
+#else
+#define FD_FENCE()
+#endif
+
 // FDStencilCenteredDegreeOdd<1,3>: {-1, 9, -45} / 60
 __device__ __forceinline__ double fd_dx(const double* __restrict__ u, int64_t s,
                                         double cidx1) {
@@ -65,6 +71,7 @@ __device__ __forceinline__ double fd_dxx(const double* __restrict__ u, int64_t s
   out += -27. * (__ldg(u - 2 * s) + __ldg(u + 2 * s));
   out += 270. * (__ldg(u - s) + __ldg(u + s));
   out += -490. * __ldg(u);
+  FD_FENCE();
   return out * cidx2;
 }
 
@@ -77,6 +84,7 @@ __device__ __forceinline__ double fd_dxy(const double* __restrict__ u, int64_t s
   out += -1. * (fd_dx(u - 3 * sa, sb, cidx1b) - fd_dx(u + 3 * sa, sb, cidx1b));
   out += 9. * (fd_dx(u - 2 * sa, sb, cidx1b) - fd_dx(u + 2 * sa, sb, cidx1b));
   out += -45. * (fd_dx(u - sa, sb, cidx1b) - fd_dx(u + sa, sb, cidx1b));
+  FD_FENCE();
   return out * cidx1a;
 }
 

@@ -19,20 +19,56 @@ constexpr int kPointThreads = 256;
 
 inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
-// ---- Z4cRHS over the interior of blocks [block0, block0+nblk) -------------
+// Rsum scratch: [block][6][interior vertex], interior vertices in i-fastest
+// order.
+__device__ __forceinline__ double* rsum_at(const Grid& g, double* rsum, int b, int64_t l) {
+  return rsum + (int64_t)b * 6 * interior_count(g) + l;
+}
+
+// ---- first pass: Ricci tensor + conformal-factor part per interior vertex --
 __global__ void __launch_bounds__(kRhsThreads, 1)
-k_rhs(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ rhs,
-      int block0, int nblk) {
+k_ricci(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ rsum,
+        int block0, int nblk) {
   const int64_t npts = interior_count(g);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts * nblk) return;
   const int b = block0 + (int)(t / npts);
+  const int64_t l = t % npts;
   int i, j, k;
-  interior_ijk(g, t % npts, i, j, k);
+  interior_ijk(g, l, i, j, k);
+  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  double R[6];
+  ricci_point(u + (int64_t)b * NVAR * g.nvol, g.nvol, p, g.s, P, P.fd[b], R);
+  double* rs = rsum_at(g, rsum, b, l);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) rs[(int64_t)q * npts] = R[q];
+}
+
+__device__ __forceinline__ void load_rsum(const Grid& g, const double* __restrict__ rsum, int b,
+                                          int64_t l, double R[6]) {
+  const int64_t npts = interior_count(g);
+  const double* rs = rsum + (int64_t)b * 6 * npts + l;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) R[q] = __ldg(rs + (int64_t)q * npts);
+}
+
+// ---- Z4cRHS over the interior of blocks [block0, block0+nblk) -------------
+__global__ void __launch_bounds__(kRhsThreads, 1)
+k_rhs(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ rsum,
+      double* __restrict__ rhs, int block0, int nblk) {
+  const int64_t npts = interior_count(g);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * nblk) return;
+  const int b = block0 + (int)(t / npts);
+  const int64_t l = t % npts;
+  int i, j, k;
+  interior_ijk(g, l, i, j, k);
   const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
   const double* ub = u + (int64_t)b * NVAR * g.nvol;
+  double R[6];
+  load_rsum(g, rsum, b, l, R);
   double out[NVAR];
-  rhs_point(ub, g.nvol, p, g.s, P, P.fd[b], out);
+  rhs_point(ub, g.nvol, p, g.s, P, P.fd[b], R, out);
   double* rb = rhs + (int64_t)b * NVAR * g.nvol + p;
 #pragma unroll
   for (int n = 0; n < NVAR; ++n) rb[(int64_t)n * g.nvol] = out[n];
@@ -44,18 +80,22 @@ k_rhs(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ rh
 //   AddZ4cRHS(rhs, beta*dt, u)        (mesh/weighted_ave.cpp:20-150)
 // u is read (all points, for the stencils); u_out, u1 are written (interior).
 __global__ void __launch_bounds__(kRhsThreads, 1)
-k_stage_ls(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ u1,
-           double* __restrict__ u_out, LsStage w, int block0, int nblk) {
+k_stage_ls(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ rsum,
+           double* __restrict__ u1, double* __restrict__ u_out, LsStage w, int block0,
+           int nblk) {
   const int64_t npts = interior_count(g);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts * nblk) return;
   const int b = block0 + (int)(t / npts);
+  const int64_t l = t % npts;
   int i, j, k;
-  interior_ijk(g, t % npts, i, j, k);
+  interior_ijk(g, l, i, j, k);
   const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
   const int64_t off = (int64_t)b * NVAR * g.nvol + p;
+  double R[6];
+  load_rsum(g, rsum, b, l, R);
   double r[NVAR];
-  rhs_point(u + (int64_t)b * NVAR * g.nvol, g.nvol, p, g.s, P, P.fd[b], r);
+  rhs_point(u + (int64_t)b * NVAR * g.nvol, g.nvol, p, g.s, P, P.fd[b], R, r);
 #pragma unroll
   for (int n = 0; n < NVAR; ++n) {
     const int64_t q = off + (int64_t)n * g.nvol;
@@ -85,18 +125,22 @@ struct KPtrs {
   double* k[4];
 };
 __global__ void __launch_bounds__(kRhsThreads, 1)
-k_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ un,
-           KPtrs K, double* __restrict__ u_out, BtStage w, int block0, int nblk) {
+k_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ rsum,
+           const double* __restrict__ un, KPtrs K, double* __restrict__ u_out, BtStage w,
+           int block0, int nblk) {
   const int64_t npts = interior_count(g);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts * nblk) return;
   const int b = block0 + (int)(t / npts);
+  const int64_t l = t % npts;
   int i, j, k;
-  interior_ijk(g, t % npts, i, j, k);
+  interior_ijk(g, l, i, j, k);
   const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
   const int64_t off = (int64_t)b * NVAR * g.nvol + p;
+  double R[6];
+  load_rsum(g, rsum, b, l, R);
   double r[NVAR];
-  rhs_point(u + (int64_t)b * NVAR * g.nvol, g.nvol, p, g.s, P, P.fd[b], r);
+  rhs_point(u + (int64_t)b * NVAR * g.nvol, g.nvol, p, g.s, P, P.fd[b], R, r);
 #pragma unroll 1
   for (int n = 0; n < NVAR; ++n) {
     const int64_t q = off + (int64_t)n * g.nvol;
@@ -510,30 +554,41 @@ long long kernel_launch_count() { return g_launches.load(); }
 void add_kernel_launches(long long n) { g_launches += n; }
 #define COUNTED ++g_launches;
 
-void launch_rhs(const Grid& g, const DevParams& P, const double* u, double* rhs, int block0,
-                int nblk, cudaStream_t st) {
+static void launch_ricci(const Grid& g, const DevParams& P, const double* u, double* rsum,
+                         int block0, int nblk, cudaStream_t st) {
   const int64_t n = interior_count(g) * nblk;
   COUNTED
-  k_rhs<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, rhs, block0, nblk);
+  k_ricci<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, rsum, block0, nblk);
 }
 
-void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, double* u1,
-                     double* u_out, const LsStage& w, int block0, int nblk, cudaStream_t st) {
+void launch_rhs(const Grid& g, const DevParams& P, const double* u, double* rsum, double* rhs,
+                int block0, int nblk, cudaStream_t st) {
+  launch_ricci(g, P, u, rsum, block0, nblk, st);
   const int64_t n = interior_count(g) * nblk;
   COUNTED
-  k_stage_ls<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, u1, u_out, w, block0,
-                                                              nblk);
+  k_rhs<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, rsum, rhs, block0, nblk);
 }
 
-void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const double* un,
-                     double* const* k, double* u_out, const BtStage& w, int block0, int nblk,
+void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, double* rsum,
+                     double* u1, double* u_out, const LsStage& w, int block0, int nblk,
                      cudaStream_t st) {
+  launch_ricci(g, P, u, rsum, block0, nblk, st);
+  const int64_t n = interior_count(g) * nblk;
+  COUNTED
+  k_stage_ls<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, rsum, u1, u_out, w,
+                                                              block0, nblk);
+}
+
+void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, double* rsum,
+                     const double* un, double* const* k, double* u_out, const BtStage& w,
+                     int block0, int nblk, cudaStream_t st) {
+  launch_ricci(g, P, u, rsum, block0, nblk, st);
   KPtrs K;
   for (int s = 0; s < 4; ++s) K.k[s] = k[s];
   const int64_t n = interior_count(g) * nblk;
   COUNTED
-  k_stage_bt<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, un, K, u_out, w, block0,
-                                                              nblk);
+  k_stage_bt<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, rsum, un, K, u_out, w,
+                                                              block0, nblk);
 }
 
 void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst, int nvar,

@@ -49,13 +49,16 @@ long long kernel_launch_count();
 void add_kernel_launches(long long n);
 
 // All launches return cudaGetLastError() mapped by the caller.
-void launch_rhs(const Grid& g, const DevParams& P, const double* u, double* rhs,
+// The RHS launches run two kernels: the Ricci pass into the rsum scratch
+// ([block][6][interior vertex]) and the main pass that reads it.
+void launch_rhs(const Grid& g, const DevParams& P, const double* u, double* rsum, double* rhs,
                 int block0, int nblk, cudaStream_t st);
-void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, double* u1,
-                     double* u_out, const LsStage& w, int block0, int nblk, cudaStream_t st);
-void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const double* un,
-                     double* const* k, double* u_out, const BtStage& w, int block0, int nblk,
+void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, double* rsum,
+                     double* u1, double* u_out, const LsStage& w, int block0, int nblk,
                      cudaStream_t st);
+void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, double* rsum,
+                     const double* un, double* const* k, double* u_out, const BtStage& w,
+                     int block0, int nblk, cudaStream_t st);
 void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst,
                      int nvar, const int* nbr, int fuse_alg, cudaStream_t st);
 void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st);

@@ -3,79 +3,71 @@
 // (z4c/adm_z4c.cpp:972-1037) evaluated in place from the state, constant-eta
 // branch, vacuum (matter terms vanish), Kreiss-Oliger dissipation included.
 //
-// One call computes the 22 right-hand-side values of one interior vertex.
-// The operation order follows the reference line by line; line numbers in
-// the comments refer to calculate_z4c_rhs.cpp.
+// The work per vertex is split in two passes so that each keeps its live
+// values in registers:
+//   ricci_point  the Ricci tensor of the conformal metric and its
+//                conformal-factor part, stored as Rsum_ab = R_ab + Rphi_ab
+//                (the reference only ever uses the sum, :603, :745);
+//   rhs_point    everything else, reading Rsum_ab.
+// The operation order of every quantity follows the reference line by line;
+// line numbers in the comments refer to calculate_z4c_rhs.cpp.
 #pragma once
 
 #include "z4c_common.cuh"
 
 namespace z4c {
 
-// u: base of one block register ([var][k][j][i]); p: vertex offset.
-__device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t nvol,
-                                          int64_t p, const int64_t s[3],
-                                          const DevParams& P, const FdScale& F,
-                                          double out[NVAR]) {
-  const z4c_params_t& opt = P.p;
-  const double* U = u + p;
 #define UV(n) (U + (int64_t)(n) * nvol)
+#define GUU(a, b) g_uu[sidx(a, b)]
 
-  double g_dd[6], A_dd[6], beta_u[3], Gam_u[3];
-#pragma unroll
-  for (int c = 0; c < 6; ++c) {
-    g_dd[c] = __ldg(UV(Z4C_GXX + c));
-    A_dd[c] = __ldg(UV(Z4C_AXX + c));
-  }
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    beta_u[a] = __ldg(UV(Z4C_BETAX + a));
-    Gam_u[a] = __ldg(UV(Z4C_GAMX + a));
-  }
-  const double chi = __ldg(UV(Z4C_CHI)), Khat = __ldg(UV(Z4C_KHAT));
-  const double Theta = __ldg(UV(Z4C_THETA)), alpha = __ldg(UV(Z4C_ALPHA));
+// (a,b) of the symmetric pair q in xx,xy,xz,yy,yz,zz order
+__device__ __forceinline__ int pair_a(int q) { return q < 3 ? 0 : (q < 5 ? 1 : 2); }
+__device__ __forceinline__ int pair_b(int q) { return q < 3 ? q : (q < 5 ? q - 2 : 2); }
 
-  // --- first derivatives, :84-114 (dA_ddd of :112 is never read) ---
-  double dalpha_d[3], dchi_d[3], dKhat_d[3], dTheta_d[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    dalpha_d[a] = fd_dx(UV(Z4C_ALPHA), s[a], F.cidx1[a]);
-    dchi_d[a] = fd_dx(UV(Z4C_CHI), s[a], F.cidx1[a]);
-    dKhat_d[a] = fd_dx(UV(Z4C_KHAT), s[a], F.cidx1[a]);
-    dTheta_d[a] = fd_dx(UV(Z4C_THETA), s[a], F.cidx1[a]);
-  }
-  double dbeta_du[3][3];  // [b][a] = d_b beta^a
-#pragma unroll
-  for (int b = 0; b < 3; ++b)
-#pragma unroll
-    for (int a = 0; a < 3; ++a) dbeta_du[b][a] = fd_dx(UV(Z4C_BETAX + a), s[b], F.cidx1[b]);
+// Second derivative of f along the pair q: Dxx on the diagonal, otherwise Dx
+// along the first index of the stored Dx along the second (a < b).
+__device__ __forceinline__ double fd_d2(const double* __restrict__ f, int q, const int64_t s[3],
+                                        const FdScale& F) {
+  const int a = pair_a(q), b = pair_b(q);
+  if (a == b) return fd_dxx(f, s[a], F.cidx2[a]);
+  return fd_dxy(f, s[a], s[b], F.cidx1[a], F.cidx1[b]);
+}
 
-  // --- Christoffel symbols, :317-352 (needs d g only here) ---
-  double g_uu[6];
+// The heavy derivative gathers below run as rolled loops (#pragma unroll 1)
+// writing small per-thread arrays; the tensor algebra that consumes them is
+// fully unrolled.  Unrolled gathers let the compiler hoist hundreds of
+// stencil loads at once and spill.
+#define GDD(a, b) g_dd[sidx(a, b)]
+#define ADD(a, b) A_dd[sidx(a, b)]
+
+// Inverse conformal metric (:295-311) and Christoffel symbols (:317-352).
+// Gamma_ddd is written only when the caller passes storage for it.
+__device__ __forceinline__ void christoffel(const double* __restrict__ U, int64_t nvol,
+                                            const int64_t s[3], const FdScale& F,
+                                            const double g_dd[6], double g_uu[6],
+                                            double Gamma_ddd[3][6], double Gamma_udd[3][6],
+                                            double Gamma_u[3]) {
   {
     const double detg = det3(g_dd[0], g_dd[1], g_dd[2], g_dd[3], g_dd[4], g_dd[5]);
     inv3(1.0 / detg, g_dd, g_uu);
   }
-#define GUU(a, b) g_uu[sidx(a, b)]
-#define GDD(a, b) g_dd[sidx(a, b)]
-#define ADD(a, b) A_dd[sidx(a, b)]
-  double Gamma_ddd[3][6];  // [c][ab]
+  double Gd[3][6];
   {
-    double dg[3][6];       // [c][ab] = d_c g_ab
+    double dg[3][6];  // [c][ab] = d_c g_ab (stored dg_ddd_3d)
+#pragma unroll 1
+    for (int q = 0; q < 6; ++q) {
+      const double* f = UV(Z4C_GXX + q);
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int q = 0; q < 6; ++q) dg[c][q] = fd_dx(UV(Z4C_GXX + q), s[c], F.cidx1[c]);
+      for (int c = 0; c < 3; ++c) dg[c][q] = fd_dx(f, s[c], F.cidx1[c]);
+    }
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int b = a; b < 3; ++b)
-          Gamma_ddd[c][sidx(a, b)] =
-              0.5 * (dg[a][sidx(b, c)] + dg[b][sidx(a, c)] - dg[c][sidx(a, b)]);
+          Gd[c][sidx(a, b)] = 0.5 * (dg[a][sidx(b, c)] + dg[b][sidx(a, c)] - dg[c][sidx(a, b)]);
   }
-  double Gamma_udd[3][6];
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -84,10 +76,9 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
       for (int b = a; b < 3; ++b) {
         double sacc = 0;
 #pragma unroll
-        for (int d = 0; d < 3; ++d) sacc += GUU(c, d) * Gamma_ddd[d][sidx(a, b)];
+        for (int d = 0; d < 3; ++d) sacc += GUU(c, d) * Gd[d][sidx(a, b)];
         Gamma_udd[c][sidx(a, b)] = sacc;
       }
-  double Gamma_u[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     double sacc = 0;
@@ -98,10 +89,38 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
         sacc += ((b == c) ? 1.0 : 2.0) * GUU(b, c) * Gamma_udd[a][sidx(b, c)];
     Gamma_u[a] = sacc;
   }
+  if (Gamma_ddd) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) Gamma_ddd[c][q] = Gd[c][q];
+  }
+}
+
+// Rsum_ab = R_ab + Rphi_ab at one interior vertex (:357-458).
+__device__ __forceinline__ void ricci_point(const double* __restrict__ u, int64_t nvol,
+                                            int64_t p, const int64_t s[3],
+                                            const DevParams& P, const FdScale& F,
+                                            double Rsum[6]) {
+  const z4c_params_t& opt = P.p;
+  const double* U = u + p;
+  double g_dd[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) g_dd[c] = __ldg(UV(Z4C_GXX + c));
+  double g_uu[6], Gamma_ddd[3][6], Gamma_udd[3][6], Gamma_u[3];
+  christoffel(U, nvol, s, F, g_dd, g_uu, Gamma_ddd, Gamma_udd, Gamma_u);
 #define GDDD(c, a, b) Gamma_ddd[c][sidx(a, b)]
 #define GUDD(c, a, b) Gamma_udd[c][sidx(a, b)]
 
-  // --- Ricci tensor of the conformal metric, :357-396 ---
+  // Ricci tensor of the conformal metric, :357-396; each R_ab accumulates
+  // its three groups of terms in the reference's order
+  double dGam[3][3];  // [b][c] = d_b Gamma^c
+#pragma unroll 1
+  for (int c = 0; c < 3; ++c) {
+    const double* f = UV(Z4C_GAMX + c);
+#pragma unroll
+    for (int b = 0; b < 3; ++b) dGam[b][c] = fd_dx(f, s[b], F.cidx1[b]);
+  }
   double R_dd[6];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
@@ -109,22 +128,28 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
     for (int b = a; b < 3; ++b) {
       double sacc = 0;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const double dGam_bc = fd_dx(UV(Z4C_GAMX + c), s[b], F.cidx1[b]);
-        const double dGam_ac = fd_dx(UV(Z4C_GAMX + c), s[a], F.cidx1[a]);
-        sacc += 0.5 * (GDD(c, a) * dGam_bc + GDD(c, b) * dGam_ac +
-                       Gamma_u[c] * (GDDD(a, b, c) + GDDD(b, a, c)));
-      }
-#pragma unroll
       for (int c = 0; c < 3; ++c)
+        sacc += 0.5 * (GDD(c, a) * dGam[b][c] + GDD(c, b) * dGam[a][c] +
+                       Gamma_u[c] * (GDDD(a, b, c) + GDDD(b, a, c)));
+      R_dd[sidx(a, b)] = sacc;
+    }
+  // ddg_dddd(c,d,a,b): second derivative along c,d of g_ab, :158-178
+#pragma unroll 1
+  for (int q = 0; q < 6; ++q) {
+    const double* f = UV(Z4C_GXX + q);
+    double sacc = R_dd[q];
 #pragma unroll
-        for (int d = c; d < 3; ++d) {
-          // ddg_dddd(c,d,a,b): second derivative along c,d of g_ab, :158-178
-          const double* f = UV(Z4C_GXX + sidx(a, b));
-          const double dd = (c == d) ? fd_dxx(f, s[c], F.cidx2[c])
-                                     : fd_dxy(f, s[c], s[d], F.cidx1[c], F.cidx1[d]);
-          sacc -= ((c == d) ? 0.5 : 1.0) * GUU(c, d) * dd;
-        }
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int d = c; d < 3; ++d)
+        sacc -= ((c == d) ? 0.5 : 1.0) * GUU(c, d) * fd_d2(f, sidx(c, d), s, F);
+    R_dd[q] = sacc;
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = a; b < 3; ++b) {
+      double sacc = R_dd[sidx(a, b)];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -136,31 +161,29 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
       R_dd[sidx(a, b)] = sacc;
     }
 
-  // --- conformal factor, :231-274, :402-426 ---
-  const double K = Khat + 2. * Theta;
+  // conformal-factor part, :241-245, :402-458
+  const double chi = __ldg(UV(Z4C_CHI));
   const double chi_guarded = dmax(chi, opt.chi_div_floor);
   const double oochi = 1.0 / chi_guarded;
-  double oopsi4;
-  if (opt.chi_psi_power == -4.) oopsi4 = chi_guarded;
-  else oopsi4 = pow(chi_guarded, -4. / opt.chi_psi_power);
   const double oochi_psi_power = 1.0 / opt.chi_psi_power;
   double dphi_d[3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) dphi_d[a] = dchi_d[a] * oochi * oochi_psi_power;
+  for (int a = 0; a < 3; ++a)
+    dphi_d[a] = fd_dx(UV(Z4C_CHI), s[a], F.cidx1[a]) * oochi * oochi_psi_power;
+  double ddchi[6];  // stored ddchi_dd_3d
+#pragma unroll 1
+  for (int q = 0; q < 6; ++q) ddchi[q] = fd_d2(UV(Z4C_CHI), q, s, F);
   double Ddphi_dd[6];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
     for (int b = a; b < 3; ++b) {
-      const double* f = UV(Z4C_CHI);
-      const double ddchi = (a == b) ? fd_dxx(f, s[a], F.cidx2[a])
-                                    : fd_dxy(f, s[a], s[b], F.cidx1[a], F.cidx1[b]);
-      double v = ddchi * oochi * oochi_psi_power - opt.chi_psi_power * dphi_d[a] * dphi_d[b];
+      double v = ddchi[sidx(a, b)] * oochi * oochi_psi_power -
+                 opt.chi_psi_power * dphi_d[a] * dphi_d[b];
 #pragma unroll
       for (int c = 0; c < 3; ++c) v -= GUDD(c, a, b) * dphi_d[c];
       Ddphi_dd[sidx(a, b)] = v;
     }
-  // Rphi, :436-458
   double Stmp = 0.0;
 #pragma unroll
   for (int c = 0; c < 3; ++c)
@@ -168,28 +191,69 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
     for (int d = c; d < 3; ++d)
       Stmp += ((c == d) ? 1.0 : 2.0) * GUU(c, d) *
               (Ddphi_dd[sidx(c, d)] + 2. * dphi_d[c] * dphi_d[d]);
-  double Rphi_dd[6];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
-    for (int b = a; b < 3; ++b)
-      Rphi_dd[sidx(a, b)] = 4. * dphi_d[a] * dphi_d[b] - 2. * Ddphi_dd[sidx(a, b)] -
-                            2. * GDD(a, b) * Stmp;
+    for (int b = a; b < 3; ++b) {
+      const double rphi = 4. * dphi_d[a] * dphi_d[b] - 2. * Ddphi_dd[sidx(a, b)] -
+                          2. * GDD(a, b) * Stmp;
+      Rsum[sidx(a, b)] = R_dd[sidx(a, b)] + rphi;
+    }
+#undef GDDD
+#undef GUDD
+}
 
-  // --- D D alpha, :482-521 ---
+// All 22 right-hand-side values at one interior vertex, given Rsum_ab.
+__device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t nvol,
+                                          int64_t p, const int64_t s[3],
+                                          const DevParams& P, const FdScale& F,
+                                          const double Rsum[6], double out[NVAR]) {
+  const z4c_params_t& opt = P.p;
+  const double* U = u + p;
+  double g_dd[6], A_dd[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    g_dd[c] = __ldg(UV(Z4C_GXX + c));
+    A_dd[c] = __ldg(UV(Z4C_AXX + c));
+  }
+  const double chi = __ldg(UV(Z4C_CHI)), Khat = __ldg(UV(Z4C_KHAT));
+  const double Theta = __ldg(UV(Z4C_THETA)), alpha = __ldg(UV(Z4C_ALPHA));
+
+  double g_uu[6], Gamma_udd[3][6], Gamma_u[3];
+  christoffel(U, nvol, s, F, g_dd, g_uu, nullptr, Gamma_udd, Gamma_u);
+#define GUDD(c, a, b) Gamma_udd[c][sidx(a, b)]
+
+  // :231-274
+  const double K = Khat + 2. * Theta;
+  const double chi_guarded = dmax(chi, opt.chi_div_floor);
+  const double oochi = 1.0 / chi_guarded;
+  double oopsi4;
+  if (opt.chi_psi_power == -4.) oopsi4 = chi_guarded;
+  else oopsi4 = pow(chi_guarded, -4. / opt.chi_psi_power);
+  const double oochi_psi_power = 1.0 / opt.chi_psi_power;
+  double dchi_d[3], dphi_d[3], dalpha_d[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    dchi_d[a] = fd_dx(UV(Z4C_CHI), s[a], F.cidx1[a]);
+    dphi_d[a] = dchi_d[a] * oochi * oochi_psi_power;
+    dalpha_d[a] = fd_dx(UV(Z4C_ALPHA), s[a], F.cidx1[a]);
+  }
+
+  // D D alpha, :482-521
   double Ddalpha = 0;
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
     for (int d = 0; d < 3; ++d) Ddalpha += GUU(c, d) * dphi_d[c] * dalpha_d[d];
+  double ddalpha[6];
+#pragma unroll 1
+  for (int q = 0; q < 6; ++q) ddalpha[q] = fd_d2(UV(Z4C_ALPHA), q, s, F);
   double Ddalpha_dd[6];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
     for (int b = a; b < 3; ++b) {
-      const double* f = UV(Z4C_ALPHA);
-      const double ddal = (a == b) ? fd_dxx(f, s[a], F.cidx2[a])
-                                   : fd_dxy(f, s[a], s[b], F.cidx1[a], F.cidx1[b]);
+      const double ddal = ddalpha[sidx(a, b)];
       double v = ddal - 2. * (dphi_d[a] * dalpha_d[b] + dphi_d[b] * dalpha_d[a]) +
                  2. * GDD(a, b) * Ddalpha;
 #pragma unroll
@@ -203,7 +267,7 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
     for (int b = a; b < 3; ++b)
       Ddalpha += ((a == b) ? 1.0 : 2.0) * oopsi4 * GUU(a, b) * Ddalpha_dd[sidx(a, b)];
 
-  // --- A contractions, :525-589 ---
+  // A contractions, :525-589
   double A_ud[3][3];
 #pragma unroll
   for (int c = 0; c < 3; ++c)
@@ -246,8 +310,10 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
     double sacc = 0;
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
+      const double dKhat_b = fd_dx(UV(Z4C_KHAT), s[b], F.cidx1[b]);
+      const double dTheta_b = fd_dx(UV(Z4C_THETA), s[b], F.cidx1[b]);
       sacc -= chi_pow_DA_u * A_uu[sidx(a, b)] * dchi_d[b] * oochi;
-      sacc -= (1. / 3.) * GUU(a, b) * (2. * dKhat_d[b] + dTheta_d[b]);
+      sacc -= (1. / 3.) * GUU(a, b) * (2. * dKhat_b + dTheta_b);
     }
 #pragma unroll
     for (int b = 0; b < 3; ++b)
@@ -256,56 +322,67 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
         sacc += ((b == c) ? 1.0 : 2.0) * GUDD(a, b, c) * A_uu[sidx(b, c)];
     DA_u[a] = sacc;
   }
+#undef GUDD
 
-  // --- Ricci scalar, Ht, :596-613 ---
+  // Ricci scalar, Ht, :596-613
   double R = 0;
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
     for (int b = a; b < 3; ++b)
-      R += ((a == b) ? 1.0 : 2.0) * oopsi4 * GUU(a, b) * (R_dd[sidx(a, b)] + Rphi_dd[sidx(a, b)]);
+      R += ((a == b) ? 1.0 : 2.0) * oopsi4 * GUU(a, b) * Rsum[sidx(a, b)];
   const double Ht = R + (2. / 3.) * (K * K) - trAA;
 
-  // --- advective derivatives, :184-226 ---
-  double Lsc[4] = {0, 0, 0, 0};  // alpha, chi, Khat, Theta
-  double Lbeta_u[3] = {0, 0, 0}, LGam_u[3] = {0, 0, 0};
-  double Lg_dd[6] = {0, 0, 0, 0, 0, 0}, LA_dd[6] = {0, 0, 0, 0, 0, 0};
+  // advective derivatives, :184-226
+  double beta_u[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) beta_u[a] = __ldg(UV(Z4C_BETAX + a));
+  // Lx of every variable summed over the three directions in order
+  double Lv[NVAR];
+#pragma unroll 1
+  for (int n = 0; n < NVAR; ++n) {
+    double acc = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) acc += fd_lx(load9(UV(n), s[a]), beta_u[a], F.lidx[a]);
+    Lv[n] = acc;
+  }
+  double Lsc[4] = {Lv[Z4C_ALPHA], Lv[Z4C_CHI], Lv[Z4C_KHAT], Lv[Z4C_THETA]};
+  double Lbeta_u[3], LGam_u[3], Lg_dd[6], LA_dd[6];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const int64_t sa = s[a];
-    const double la = F.lidx[a];
+    Lbeta_u[a] = Lv[Z4C_BETAX + a];
+    LGam_u[a] = Lv[Z4C_GAMX + a];
+  }
 #pragma unroll
-    for (int n = 0; n < NVAR; ++n) {
-      const Line9 L = load9(UV(n), sa);
-      const double lx = fd_lx(L, beta_u[a], la);
-      if (n == Z4C_ALPHA) Lsc[0] += lx;
-      else if (n == Z4C_CHI) Lsc[1] += lx;
-      else if (n == Z4C_KHAT) Lsc[2] += lx;
-      else if (n == Z4C_THETA) Lsc[3] += lx;
-      else if (n >= Z4C_BETAX) Lbeta_u[n - Z4C_BETAX] += lx;
-      else if (n >= Z4C_GAMX && n <= Z4C_GAMZ) LGam_u[n - Z4C_GAMX] += lx;
-      else if (n >= Z4C_GXX && n <= Z4C_GZZ) Lg_dd[n - Z4C_GXX] += lx;
-      else if (n >= Z4C_AXX && n <= Z4C_AZZ) LA_dd[n - Z4C_AXX] += lx;
-    }
+  for (int q = 0; q < 6; ++q) {
+    Lg_dd[q] = Lv[Z4C_GXX + q];
+    LA_dd[q] = Lv[Z4C_AXX + q];
   }
 
-  // --- finalize Lie derivatives, :619-687 ---
+  // finalize Lie derivatives, :619-687
+  double dbeta_du[3][3];  // [b][a] = d_b beta^a
+#pragma unroll 1
+  for (int a = 0; a < 3; ++a) {
+    const double* f = UV(Z4C_BETAX + a);
+#pragma unroll
+    for (int b = 0; b < 3; ++b) dbeta_du[b][a] = fd_dx(f, s[b], F.cidx1[b]);
+  }
   double dbeta = 0;
 #pragma unroll
   for (int a = 0; a < 3; ++a) dbeta += dbeta_du[a][a];
-  double ddbeta_d[3] = {0, 0, 0};
   // ddbeta_ddu(a,b,c): second derivative along a,b of beta^c, :138-156
+  double ddbeta[3][6];  // [c][pair(a,b)]
+#pragma unroll 1
+  for (int i = 0; i < 18; ++i) {
+    const int c = i / 6, q = i % 6;
+    ddbeta[c][q] = fd_d2(UV(Z4C_BETAX + c), q, s, F);
+  }
+  double ddbeta_d[3] = {0, 0, 0};
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      const double* f = UV(Z4C_BETAX + b);
-      const double v = (a == b) ? fd_dxx(f, s[a], F.cidx2[a])
-                                : fd_dxy(f, s[a < b ? a : b], s[a < b ? b : a],
-                                         F.cidx1[a < b ? a : b], F.cidx1[a < b ? b : a]);
-      ddbeta_d[a] += (1. / 3.) * v;
-    }
-  double Lchi = Lsc[1] + (1. / 6.) * opt.chi_psi_power * chi_guarded * dbeta;
+    for (int b = 0; b < 3; ++b) ddbeta_d[a] += (1. / 3.) * ddbeta[b][sidx(a, b)];
+  const double Lchi = Lsc[1] + (1. / 6.) * opt.chi_psi_power * chi_guarded * dbeta;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     LGam_u[a] += (2. / 3.) * Gamma_u[a] * dbeta;
@@ -313,12 +390,8 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
     for (int b = 0; b < 3; ++b) {
       LGam_u[a] += GUU(a, b) * ddbeta_d[b] - Gamma_u[b] * dbeta_du[b][a];
 #pragma unroll
-      for (int c = b; c < 3; ++c) {
-        const double* f = UV(Z4C_BETAX + a);
-        const double v = (b == c) ? fd_dxx(f, s[b], F.cidx2[b])
-                                  : fd_dxy(f, s[b], s[c], F.cidx1[b], F.cidx1[c]);
-        LGam_u[a] += ((b == c) ? 1.0 : 2.0) * GUU(b, c) * v;
-      }
+      for (int c = b; c < 3; ++c)
+        LGam_u[a] += ((b == c) ? 1.0 : 2.0) * GUU(b, c) * ddbeta[a][sidx(b, c)];
     }
   }
 #pragma unroll
@@ -339,8 +412,7 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
       LA_dd[sidx(a, b)] = la;
     }
 
-  // --- assemble, :694-902 (matter fields are zero: S = rho = S_i = S_ij = 0) ---
-  const double S = 0.0;
+  // assemble, :694-902 (matter fields are zero, so their terms vanish exactly)
   out[Z4C_KHAT] = -Ddalpha + alpha * (trAA + (1. / 3.) * (K * K)) + Lsc[2] +
                   opt.damp_kappa1 * (1 - opt.damp_kappa2) * alpha * Theta;
   out[Z4C_CHI] = Lchi - (1. / 6.) * opt.chi_psi_power * chi_guarded * alpha * K;
@@ -348,7 +420,7 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     double v = 2. * alpha * DA_u[a] + LGam_u[a];
-    v -= 2. * alpha * opt.damp_kappa1 * (Gam_u[a] - Gamma_u[a]);
+    v -= 2. * alpha * opt.damp_kappa1 * (__ldg(UV(Z4C_GAMX + a)) - Gamma_u[a]);
 #pragma unroll
     for (int b = 0; b < 3; ++b) v -= 2. * A_uu[sidx(a, b)] * dalpha_d[b];
     out[Z4C_GAMX + a] = v;
@@ -359,11 +431,10 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
     for (int b = a; b < 3; ++b) {
       const int q = sidx(a, b);
       out[Z4C_GXX + q] = -2. * alpha * A_dd[q] + Lg_dd[q];
-      double v = oopsi4 * (-Ddalpha_dd[q] + alpha * (R_dd[q] + Rphi_dd[q]));
+      double v = oopsi4 * (-Ddalpha_dd[q] + alpha * Rsum[q]);
       v -= (1. / 3.) * g_dd[q] * (-Ddalpha + alpha * R);
       v += alpha * (K * A_dd[q] - 2. * AA_dd[q]);
       v += LA_dd[q];
-      (void)S;
       out[Z4C_AXX + q] = v;
     }
   {
@@ -372,8 +443,9 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
   }
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    double v = opt.shift_Gamma * Gam_u[a] + opt.shift_advect * Lbeta_u[a];
-    if (fabs(opt.shift_alpha2Gamma) > 0.0) v += opt.shift_alpha2Gamma * (alpha * alpha) * Gam_u[a];
+    const double gam_a = __ldg(UV(Z4C_GAMX + a));
+    double v = opt.shift_Gamma * gam_a + opt.shift_advect * Lbeta_u[a];
+    if (fabs(opt.shift_alpha2Gamma) > 0.0) v += opt.shift_alpha2Gamma * (alpha * alpha) * gam_a;
     if (fabs(opt.shift_H) > 0.0) {
 #pragma unroll
       for (int b = 0; b < 3; ++b)
@@ -383,18 +455,18 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
     out[Z4C_BETAX + a] = v;
   }
   // Kreiss-Oliger, :908-915: rhs += Diss_x; rhs += Diss_y; rhs += Diss_z
+#pragma unroll 1
+  for (int n = 0; n < NVAR; ++n) {
+    double v = out[n];
 #pragma unroll
-  for (int n = 0; n < NVAR; ++n)
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-      out[n] += fd_diss(load9(UV(n), s[a]), F.cidxd[a], opt.diss);
+    for (int a = 0; a < 3; ++a) v += fd_diss(load9(UV(n), s[a]), F.cidxd[a], opt.diss);
+    out[n] = v;
+  }
+}
 
 #undef UV
 #undef GUU
 #undef GDD
 #undef ADD
-#undef GDDD
-#undef GUDD
-}
 
 }  // namespace z4c
