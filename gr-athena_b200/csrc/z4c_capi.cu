@@ -99,6 +99,7 @@ struct z4c_ctx {
   double* un = nullptr;   // Butcher u_n scratch
   double* guu = nullptr;  // ADMToZ4c inverse-metric scratch (6 vars)
   double* rsum = nullptr; // Ricci-pass scratch, 6 values per interior vertex
+  double* lv = nullptr;   // advection sums, 22 values per interior vertex
   double* xf = nullptr;   // [nblocks][nn0+nn1+nn2]
   double* xv = nullptr;   // [nblocks][nn0+nn1+nn2-3]
   FdScale* fd = nullptr;  // [nblocks]
@@ -116,6 +117,8 @@ struct z4c_ctx {
   cudaGraphExec_t graph = nullptr;
   double graph_dt = 0.0;
   bool graph_per_block = false;
+
+  RhsScratch scratch() const { return RhsScratch{rsum, lv}; }
 
   DevParams dev() const {
     DevParams P;
@@ -192,7 +195,8 @@ int run_stage(z4c_ctx* c, int stage, double dt) {
     }
     if (!c->per_block) {
       LsStage ls{wt[0], wt[1], wt[2], wt[3], wt[4] * dt};
-      launch_stage_ls(g, P, u, c->rsum, c->reg[Z4C_REG_U1], w, ls, 0, g.nblocks, c->stream);
+      launch_stage_ls(g, P, u, c->scratch(), c->reg[Z4C_REG_RHS], c->reg[Z4C_REG_U1], w, ls, 0,
+                      g.nblocks, c->stream);
       LAUNCH_CHECK("stage_ls");
       return exchange_into(c, w, u, true);
     }
@@ -201,7 +205,7 @@ int run_stage(z4c_ctx* c, int stage, double dt) {
     const double w1[3] = {1.0, wt[0], 0.0};
     const double w2[3] = {wt[1], wt[2], wt[3]};
     for (int b = 0; b < g.nblocks; ++b) {
-      launch_rhs(g, P, u, c->rsum, c->reg[Z4C_REG_RHS], b, 1, c->stream);
+      launch_rhs(g, P, u, c->scratch(), c->reg[Z4C_REG_RHS], b, 1, c->stream);
       launch_weighted_ave(g, c->reg[Z4C_REG_U1], u, nullptr, w1, b, 1, c->stream);
       launch_weighted_ave(g, u, c->reg[Z4C_REG_U1], nullptr, w2, b, 1, c->stream);
       launch_add_rhs(g, c->reg[Z4C_REG_RHS], wt[4] * dt, u, b, 1, c->stream);
@@ -234,12 +238,14 @@ int run_stage(z4c_ctx* c, int stage, double dt) {
   double* K[4] = {c->reg[Z4C_REG_K1], c->reg[Z4C_REG_K2], c->reg[Z4C_REG_K3],
                   c->reg[Z4C_REG_K4]};
   if (!c->per_block) {
-    launch_stage_bt(g, P, u, c->rsum, c->un, K, w, bs, 0, g.nblocks, c->stream);
+    launch_stage_bt(g, P, u, c->scratch(), c->reg[Z4C_REG_RHS], c->un, K, w, bs, 0, g.nblocks,
+                    c->stream);
     LAUNCH_CHECK("stage_bt");
     return exchange_into(c, w, u, true);
   }
   for (int b = 0; b < g.nblocks; ++b) {
-    launch_stage_bt(g, P, u, c->rsum, c->un, K, w, bs, b, 1, c->stream);
+    launch_stage_bt(g, P, u, c->scratch(), c->reg[Z4C_REG_RHS], c->un, K, w, bs, b, 1,
+                    c->stream);
     LAUNCH_CHECK("stage_bt");
   }
   int rc = exchange_into(c, w, u, false);
@@ -255,7 +261,7 @@ void free_ctx(z4c_ctx* c) {
   if (c->graph) cudaGraphExecDestroy(c->graph);
   for (auto& r : c->reg)
     if (r) cudaFree(r);
-  for (void* p : {(void*)c->un, (void*)c->guu, (void*)c->rsum, (void*)c->xf, (void*)c->xv, (void*)c->fd,
+  for (void* p : {(void*)c->un, (void*)c->guu, (void*)c->rsum, (void*)c->lv, (void*)c->xf, (void*)c->xv, (void*)c->fd,
                   (void*)c->nbr, (void*)c->partials, (void*)c->flag})
     if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -409,6 +415,8 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
   if (rc == Z4C_OK) rc = alloc((void**)&c->guu, sizeof(double) * 6 * (size_t)g.nvol * nb);
   if (rc == Z4C_OK)
     rc = alloc((void**)&c->rsum, sizeof(double) * 6 * (size_t)interior_count(g) * nb);
+  if (rc == Z4C_OK)
+    rc = alloc((void**)&c->lv, sizeof(double) * Z4C_NVAR * (size_t)interior_count(g) * nb);
   if (rc == Z4C_OK) rc = alloc((void**)&c->xf, sizeof(double) * c->h_xf.size());
   if (rc == Z4C_OK) rc = alloc((void**)&c->xv, sizeof(double) * c->h_xv.size());
   if (rc == Z4C_OK) rc = alloc((void**)&c->fd, sizeof(FdScale) * nb);
@@ -537,7 +545,7 @@ int z4c_rhs(z4c_ctx* ctx, int reg_u, int reg_rhs, int block) {
   if (reg_nvar_(reg_u) != Z4C_NVAR || reg_nvar_(reg_rhs) != Z4C_NVAR || reg_u == reg_rhs)
     return fail(Z4C_EINVAL, "z4c_rhs needs two distinct 22-variable registers");
   if ((rc = check_block(ctx, block, &b0, &nb))) return rc;
-  launch_rhs(ctx->g, ctx->dev(), ctx->reg[reg_u], ctx->rsum, ctx->reg[reg_rhs], b0, nb,
+  launch_rhs(ctx->g, ctx->dev(), ctx->reg[reg_u], ctx->scratch(), ctx->reg[reg_rhs], b0, nb,
              ctx->stream);
   LAUNCH_CHECK("rhs");
   return Z4C_OK;
@@ -688,8 +696,9 @@ int z4c_rhs_stage(z4c_ctx* ctx, int stage, double dt) {
     return fail(Z4C_ESTATE, "z4c_rhs_stage runs the low-storage stage only");
   const double* wt = kLsRk4[stage - 1];
   LsStage ls{wt[0], wt[1], wt[2], wt[3], wt[4] * dt};
-  launch_stage_ls(ctx->g, ctx->dev(), ctx->reg[Z4C_REG_U], ctx->rsum, ctx->reg[Z4C_REG_U1],
-                  ctx->reg[Z4C_REG_W], ls, 0, ctx->g.nblocks, ctx->stream);
+  launch_stage_ls(ctx->g, ctx->dev(), ctx->reg[Z4C_REG_U], ctx->scratch(),
+                  ctx->reg[Z4C_REG_RHS], ctx->reg[Z4C_REG_U1], ctx->reg[Z4C_REG_W], ls, 0,
+                  ctx->g.nblocks, ctx->stream);
   LAUNCH_CHECK("stage_ls");
   return Z4C_OK;
 }

@@ -52,10 +52,31 @@ __device__ __forceinline__ void load_rsum(const Grid& g, const double* __restric
   for (int q = 0; q < 6; ++q) R[q] = __ldg(rs + (int64_t)q * npts);
 }
 
-// ---- Z4cRHS over the interior of blocks [block0, block0+nblk) -------------
+// ---- advection sums: one thread per (interior vertex, variable) ----------
+// lv: [block][22][interior vertex]
+__global__ void __launch_bounds__(kPointThreads)
+k_adv(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ lv, int block0,
+      int nblk) {
+  const int64_t npts = interior_count(g);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * NVAR * nblk) return;
+  const int64_t l = t % npts;
+  const int n = (int)((t / npts) % NVAR);
+  const int b = block0 + (int)(t / (npts * NVAR));
+  int i, j, k;
+  interior_ijk(g, l, i, j, k);
+  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  const double* U = u + (int64_t)b * NVAR * g.nvol + p;
+  double beta[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) beta[a] = __ldg(U + (int64_t)(Z4C_BETAX + a) * g.nvol);
+  lv[((int64_t)b * NVAR + n) * npts + l] = advect_point(U, g.nvol, n, g.s, P.fd[b], beta);
+}
+
+// ---- main pass: the right-hand side without the Kreiss-Oliger terms -------
 __global__ void __launch_bounds__(kRhsThreads, 1)
-k_rhs(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ rsum,
-      double* __restrict__ rhs, int block0, int nblk) {
+k_main(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ rsum,
+       const double* __restrict__ lv, double* __restrict__ rhs, int block0, int nblk) {
   const int64_t npts = interior_count(g);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts * nblk) return;
@@ -64,96 +85,101 @@ k_rhs(Grid g, DevParams P, const double* __restrict__ u, const double* __restric
   int i, j, k;
   interior_ijk(g, l, i, j, k);
   const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
-  const double* ub = u + (int64_t)b * NVAR * g.nvol;
   double R[6];
   load_rsum(g, rsum, b, l, R);
+  double L[NVAR];
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) L[n] = __ldg(lv + ((int64_t)b * NVAR + n) * npts + l);
   double out[NVAR];
-  rhs_point(ub, g.nvol, p, g.s, P, P.fd[b], R, out);
+  rhs_point(u + (int64_t)b * NVAR * g.nvol, g.nvol, p, g.s, P, P.fd[b], R, L, out);
   double* rb = rhs + (int64_t)b * NVAR * g.nvol + p;
 #pragma unroll
   for (int n = 0; n < NVAR; ++n) rb[(int64_t)n * g.nvol] = out[n];
 }
 
-// ---- fused RHS + low-storage RK stage ---------------------------------------
+// (interior vertex, variable) of thread t in the KO passes, l fastest
+struct PointVar {
+  int b, n;
+  int64_t p;  // vertex offset in the block
+  int64_t q;  // offset of (b, n, p) in a 22-variable register
+};
+__device__ __forceinline__ bool point_var(const Grid& g, int block0, int nblk, PointVar& pv) {
+  const int64_t npts = interior_count(g);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * NVAR * nblk) return false;
+  const int64_t l = t % npts;
+  pv.n = (int)((t / npts) % NVAR);
+  pv.b = block0 + (int)(t / (npts * NVAR));
+  int i, j, k;
+  interior_ijk(g, l, i, j, k);
+  pv.p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  pv.q = ((int64_t)pv.b * NVAR + pv.n) * g.nvol + pv.p;
+  return true;
+}
+
+// Z4cRHS tail: rhs += KO, in place.
+__global__ void __launch_bounds__(kPointThreads)
+k_ko_rhs(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ rhs,
+         int block0, int nblk) {
+  PointVar pv;
+  if (!point_var(g, block0, nblk, pv)) return;
+  rhs[pv.q] = add_ko(rhs[pv.q], u + pv.q, g.s, P.fd[pv.b], P.p.diss);
+}
+
+// ---- KO + low-storage RK stage ----------------------------------------------
 // IntegrateZ4c for 2S integrators (task_list_gr_z4c.cpp:176-195):
 //   WeightedAve(u1, u, u2, {1, delta, 0}); WeightedAve(u, u1, u2, {g1, g2, g3});
 //   AddZ4cRHS(rhs, beta*dt, u)        (mesh/weighted_ave.cpp:20-150)
 // u is read (all points, for the stencils); u_out, u1 are written (interior).
-__global__ void __launch_bounds__(kRhsThreads, 1)
-k_stage_ls(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ rsum,
-           double* __restrict__ u1, double* __restrict__ u_out, LsStage w, int block0,
-           int nblk) {
-  const int64_t npts = interior_count(g);
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= npts * nblk) return;
-  const int b = block0 + (int)(t / npts);
-  const int64_t l = t % npts;
-  int i, j, k;
-  interior_ijk(g, l, i, j, k);
-  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
-  const int64_t off = (int64_t)b * NVAR * g.nvol + p;
-  double R[6];
-  load_rsum(g, rsum, b, l, R);
-  double r[NVAR];
-  rhs_point(u + (int64_t)b * NVAR * g.nvol, g.nvol, p, g.s, P, P.fd[b], R, r);
-#pragma unroll
-  for (int n = 0; n < NVAR; ++n) {
-    const int64_t q = off + (int64_t)n * g.nvol;
-    const double un = __ldg(u + q);
-    double v1 = u1[q];
-    if (w.delta != 0.0) v1 += w.delta * un;  // w0 == 1, w2 == 0 branch
-    double v;
-    if (w.gamma1 == 1.0) {  // gamma3 == 0 for every 2S integrator accepted
-      v = un;
-      if (w.gamma2 != 0.0) v += w.gamma2 * v1;
-    } else if (w.gamma1 == 0.0) {
-      if (w.gamma2 == 1.0) v = v1;
-      else v = w.gamma2 * v1;
-    } else {
-      if (w.gamma2 != 0.0) v = w.gamma1 * un + w.gamma2 * v1;
-      else v = un * w.gamma1;
-    }
-    v += w.beta_dt * r[n];
-    u1[q] = v1;
-    u_out[q] = v;
+__global__ void __launch_bounds__(kPointThreads)
+k_ko_stage_ls(Grid g, DevParams P, const double* __restrict__ u,
+              const double* __restrict__ rhs, double* __restrict__ u1,
+              double* __restrict__ u_out, LsStage w, int block0, int nblk) {
+  PointVar pv;
+  if (!point_var(g, block0, nblk, pv)) return;
+  const int64_t q = pv.q;
+  const double r = add_ko(__ldg(rhs + q), u + q, g.s, P.fd[pv.b], P.p.diss);
+  const double un = __ldg(u + q);
+  double v1 = u1[q];
+  if (w.delta != 0.0) v1 += w.delta * un;  // w0 == 1, w2 == 0 branch
+  double v;
+  if (w.gamma1 == 1.0) {  // gamma3 == 0 for every 2S integrator accepted
+    v = un;
+    if (w.gamma2 != 0.0) v += w.gamma2 * v1;
+  } else if (w.gamma1 == 0.0) {
+    if (w.gamma2 == 1.0) v = v1;
+    else v = w.gamma2 * v1;
+  } else {
+    if (w.gamma2 != 0.0) v = w.gamma1 * un + w.gamma2 * v1;
+    else v = un * w.gamma1;
   }
+  v += w.beta_dt * r;
+  u1[q] = v1;
+  u_out[q] = v;
 }
 
-// ---- fused RHS + Butcher stage (task_list_integrators_butcher.cpp:512-680) --
+// ---- KO + Butcher stage (task_list_integrators_butcher.cpp:512-680) ---------
 // k_s = RHS(u); u_out = u_n + sum_q coef_q k_q in the reference's order.
 struct KPtrs {
   double* k[4];
 };
-__global__ void __launch_bounds__(kRhsThreads, 1)
-k_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ rsum,
-           const double* __restrict__ un, KPtrs K, double* __restrict__ u_out, BtStage w,
-           int block0, int nblk) {
-  const int64_t npts = interior_count(g);
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= npts * nblk) return;
-  const int b = block0 + (int)(t / npts);
-  const int64_t l = t % npts;
-  int i, j, k;
-  interior_ijk(g, l, i, j, k);
-  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
-  const int64_t off = (int64_t)b * NVAR * g.nvol + p;
-  double R[6];
-  load_rsum(g, rsum, b, l, R);
-  double r[NVAR];
-  rhs_point(u + (int64_t)b * NVAR * g.nvol, g.nvol, p, g.s, P, P.fd[b], R, r);
-#pragma unroll 1
-  for (int n = 0; n < NVAR; ++n) {
-    const int64_t q = off + (int64_t)n * g.nvol;
-    K.k[w.kslot][q] = r[n];
-    double v = __ldg(un + q);
-    for (int s = 0; s < w.nq; ++s) {
-      if (w.coef[s] != 0.0) {
-        const double ks = (s == w.kslot) ? r[n] : K.k[s][q];
-        v += w.coef[s] * ks;
-      }
+__global__ void __launch_bounds__(kPointThreads)
+k_ko_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ rhs,
+              const double* __restrict__ un, KPtrs K, double* __restrict__ u_out, BtStage w,
+              int block0, int nblk) {
+  PointVar pv;
+  if (!point_var(g, block0, nblk, pv)) return;
+  const int64_t q = pv.q;
+  const double r = add_ko(__ldg(rhs + q), u + q, g.s, P.fd[pv.b], P.p.diss);
+  K.k[w.kslot][q] = r;
+  double v = __ldg(un + q);
+  for (int s = 0; s < w.nq; ++s) {
+    if (w.coef[s] != 0.0) {
+      const double ks = (s == w.kslot) ? r : K.k[s][q];
+      v += w.coef[s] * ks;
     }
-    u_out[q] = v;
   }
+  u_out[q] = v;
 }
 
 // ---- same-level vertex-centred ghost exchange -------------------------------
@@ -554,41 +580,49 @@ long long kernel_launch_count() { return g_launches.load(); }
 void add_kernel_launches(long long n) { g_launches += n; }
 #define COUNTED ++g_launches;
 
-static void launch_ricci(const Grid& g, const DevParams& P, const double* u, double* rsum,
-                         int block0, int nblk, cudaStream_t st) {
+// The right-hand side passes shared by every RHS launch: Ricci (rsum),
+// advection sums (lv) and the main pass into rhs (without KO).
+static void launch_rhs_passes(const Grid& g, const DevParams& P, const double* u,
+                              const RhsScratch& sc, double* rhs, int block0, int nblk,
+                              cudaStream_t st) {
   const int64_t n = interior_count(g) * nblk;
   COUNTED
-  k_ricci<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, rsum, block0, nblk);
-}
-
-void launch_rhs(const Grid& g, const DevParams& P, const double* u, double* rsum, double* rhs,
-                int block0, int nblk, cudaStream_t st) {
-  launch_ricci(g, P, u, rsum, block0, nblk, st);
-  const int64_t n = interior_count(g) * nblk;
+  k_ricci<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, sc.rsum, block0, nblk);
   COUNTED
-  k_rhs<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, rsum, rhs, block0, nblk);
-}
-
-void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, double* rsum,
-                     double* u1, double* u_out, const LsStage& w, int block0, int nblk,
-                     cudaStream_t st) {
-  launch_ricci(g, P, u, rsum, block0, nblk, st);
-  const int64_t n = interior_count(g) * nblk;
+  k_adv<<<div_up(n * NVAR, kPointThreads), kPointThreads, 0, st>>>(g, P, u, sc.lv, block0, nblk);
   COUNTED
-  k_stage_ls<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, rsum, u1, u_out, w,
-                                                              block0, nblk);
+  k_main<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, sc.rsum, sc.lv, rhs, block0,
+                                                          nblk);
 }
 
-void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, double* rsum,
-                     const double* un, double* const* k, double* u_out, const BtStage& w,
-                     int block0, int nblk, cudaStream_t st) {
-  launch_ricci(g, P, u, rsum, block0, nblk, st);
+void launch_rhs(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
+                double* rhs, int block0, int nblk, cudaStream_t st) {
+  launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, st);
+  const int64_t n = interior_count(g) * nblk * NVAR;
+  COUNTED
+  k_ko_rhs<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, rhs, block0, nblk);
+}
+
+void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
+                     double* rhs, double* u1, double* u_out, const LsStage& w, int block0,
+                     int nblk, cudaStream_t st) {
+  launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, st);
+  const int64_t n = interior_count(g) * nblk * NVAR;
+  COUNTED
+  k_ko_stage_ls<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, rhs, u1, u_out, w,
+                                                                     block0, nblk);
+}
+
+void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
+                     double* rhs, const double* un, double* const* k, double* u_out,
+                     const BtStage& w, int block0, int nblk, cudaStream_t st) {
+  launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, st);
   KPtrs K;
   for (int s = 0; s < 4; ++s) K.k[s] = k[s];
-  const int64_t n = interior_count(g) * nblk;
+  const int64_t n = interior_count(g) * nblk * NVAR;
   COUNTED
-  k_stage_bt<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, rsum, un, K, u_out, w,
-                                                              block0, nblk);
+  k_ko_stage_bt<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, rhs, un, K, u_out,
+                                                                     w, block0, nblk);
 }
 
 void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst, int nvar,

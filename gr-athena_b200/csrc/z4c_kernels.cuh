@@ -49,16 +49,26 @@ long long kernel_launch_count();
 void add_kernel_launches(long long n);
 
 // All launches return cudaGetLastError() mapped by the caller.
-// The RHS launches run two kernels: the Ricci pass into the rsum scratch
-// ([block][6][interior vertex]) and the main pass that reads it.
-void launch_rhs(const Grid& g, const DevParams& P, const double* u, double* rsum, double* rhs,
-                int block0, int nblk, cudaStream_t st);
-void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, double* rsum,
-                     double* u1, double* u_out, const LsStage& w, int block0, int nblk,
-                     cudaStream_t st);
-void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, double* rsum,
-                     const double* un, double* const* k, double* u_out, const BtStage& w,
-                     int block0, int nblk, cudaStream_t st);
+// Scratch of the right-hand-side passes, indexed by absolute block:
+// rsum [block][6][interior vertex] (R_ab + Rphi_ab), lv [block][22][interior
+// vertex] (advection sums).
+struct RhsScratch {
+  double* rsum;
+  double* lv;
+};
+
+// Every RHS launch runs four kernels: Ricci pass, advection sums, main pass
+// (into rhs, without Kreiss-Oliger), then Kreiss-Oliger fused with the
+// consumer: in place for launch_rhs, with the stage update for the stage
+// launches (rhs then holds the pre-dissipation right-hand side).
+void launch_rhs(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
+                double* rhs, int block0, int nblk, cudaStream_t st);
+void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
+                     double* rhs, double* u1, double* u_out, const LsStage& w, int block0,
+                     int nblk, cudaStream_t st);
+void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
+                     double* rhs, const double* un, double* const* k, double* u_out,
+                     const BtStage& w, int block0, int nblk, cudaStream_t st);
 void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst,
                      int nvar, const int* nbr, int fuse_alg, cudaStream_t st);
 void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st);

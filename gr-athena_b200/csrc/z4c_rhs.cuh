@@ -8,7 +8,9 @@
 //   ricci_point  the Ricci tensor of the conformal metric and its
 //                conformal-factor part, stored as Rsum_ab = R_ab + Rphi_ab
 //                (the reference only ever uses the sum, :603, :745);
-//   rhs_point    everything else, reading Rsum_ab.
+//   rhs_point    everything else, reading Rsum_ab and the advection sums;
+// the advection sums (advect_point) and the Kreiss-Oliger terms (add_ko) run
+// in separate light kernels, one thread per vertex and variable.
 // The operation order of every quantity follows the reference line by line;
 // line numbers in the comments refer to calculate_z4c_rhs.cpp.
 #pragma once
@@ -203,11 +205,33 @@ __device__ __forceinline__ void ricci_point(const double* __restrict__ u, int64_
 #undef GUDD
 }
 
-// All 22 right-hand-side values at one interior vertex, given Rsum_ab.
+// Sum over the three directions, in order, of the lop-sided advection
+// operator of variable n (:184-226).
+__device__ __forceinline__ double advect_point(const double* __restrict__ U, int64_t nvol, int n,
+                                               const int64_t s[3], const FdScale& F,
+                                               const double beta_u[3]) {
+  double acc = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) acc += fd_lx(load9(UV(n), s[a]), beta_u[a], F.lidx[a]);
+  return acc;
+}
+
+// Kreiss-Oliger dissipation added to one right-hand-side value in the
+// reference's order, rhs += Diss_x; rhs += Diss_y; rhs += Diss_z (:908-915).
+__device__ __forceinline__ double add_ko(double r, const double* __restrict__ Un,
+                                        const int64_t s[3], const FdScale& F, double diss) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) r += fd_diss(load9(Un, s[a]), F.cidxd[a], diss);
+  return r;
+}
+
+// The 22 right-hand-side values at one interior vertex without the
+// Kreiss-Oliger terms, given Rsum_ab and the advection sums Lv.
 __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t nvol,
                                           int64_t p, const int64_t s[3],
                                           const DevParams& P, const FdScale& F,
-                                          const double Rsum[6], double out[NVAR]) {
+                                          const double Rsum[6], const double Lv[NVAR],
+                                          double out[NVAR]) {
   const z4c_params_t& opt = P.p;
   const double* U = u + p;
   double g_dd[6], A_dd[6];
@@ -337,15 +361,6 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
   double beta_u[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) beta_u[a] = __ldg(UV(Z4C_BETAX + a));
-  // Lx of every variable summed over the three directions in order
-  double Lv[NVAR];
-#pragma unroll 1
-  for (int n = 0; n < NVAR; ++n) {
-    double acc = 0;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) acc += fd_lx(load9(UV(n), s[a]), beta_u[a], F.lidx[a]);
-    Lv[n] = acc;
-  }
   double Lsc[4] = {Lv[Z4C_ALPHA], Lv[Z4C_CHI], Lv[Z4C_KHAT], Lv[Z4C_THETA]};
   double Lbeta_u[3], LGam_u[3], Lg_dd[6], LA_dd[6];
 #pragma unroll
@@ -453,14 +468,6 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
     }
     v -= opt.shift_eta * beta_u[a];
     out[Z4C_BETAX + a] = v;
-  }
-  // Kreiss-Oliger, :908-915: rhs += Diss_x; rhs += Diss_y; rhs += Diss_z
-#pragma unroll 1
-  for (int n = 0; n < NVAR; ++n) {
-    double v = out[n];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) v += fd_diss(load9(UV(n), s[a]), F.cidxd[a], opt.diss);
-    out[n] = v;
   }
 }
 

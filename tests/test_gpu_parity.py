@@ -96,7 +96,14 @@ def test_evolution_history_and_final_state(name):
 @pytest.mark.parametrize("name", ["evol_gw16", "evol_punc4"])
 def test_initial_data_on_device(name):
     """Host initial data -> device ADMToZ4c -> ghost finalisation reproduces
-    the reference's initialised state."""
+    the reference's initialised state.
+
+    Interior vertices agree to round-off.  On an outflow mesh the ghost
+    vertices are filled by repeated fifth-order extrapolation (u_g = 5u_1 -
+    10u_2 + 10u_3 - 5u_4 + u_5, each layer from the ones inside it, axis after
+    axis), which multiplies a 1-ulp difference in a cube root of the puncture
+    data by up to ~10^3 per axis in the outermost corner ghosts; the whole
+    register is therefore held to a looser bound than the interior."""
     from z4c_b200 import initial_data as ID
     c = Case(name)
     Z, ctx = make_ctx(c)
@@ -106,5 +113,8 @@ def test_initial_data_on_device(name):
         adm = ID.punctures(ctx.mesh, ctx.params, masses=(1.0,), centres=((0.0, 0.0, 0.0),))
     ID.load_adm(ctx, adm)
     u = c.from_grid(ctx.download(Z.REG_U))
-    assert rel_err(u, c.rec["u_init"]) <= 1e-14
+    ref = c.rec["u_init"]
+    I = c.interior()
+    assert rel_err(u[I], ref[I]) <= 1e-14
+    assert rel_err(u, ref) <= (1e-14 if "gw" in name else 1e-7)
     ctx.close()
