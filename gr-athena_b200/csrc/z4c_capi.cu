@@ -83,6 +83,15 @@ double block_axis_coords(const z4c_mesh_desc_t* mesh, int loc, int axis, double*
 
 }  // namespace
 
+namespace z4c {
+// Records the message z4c_last_error() returns on this thread (used by the
+// entry points defined in other translation units).
+int set_error(int code, const char* msg) {
+  g_err = msg;
+  return code;
+}
+}  // namespace z4c
+
 struct z4c_ctx {
   Grid g{};
   z4c_params_t params{};

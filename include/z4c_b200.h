@@ -230,6 +230,40 @@ long long z4c_kernel_launches(void);
  * Z4C_OK if all finite, Z4C_ENONFINITE otherwise. */
 int z4c_check_finite(z4c_ctx *ctx, int reg);
 
+/* ---- allocation-free variant ----------------------------------------------
+ *
+ * No counterpart in the reference: an addition for callers that cannot call
+ * cudaMalloc.  Some host programs own all device memory through their own
+ * allocator (a framework's caching allocator, or a pool reserved at start-up)
+ * and may not allocate behind its back; others run the right-hand side inside
+ * a time-stepping loop that cannot take the device-wide synchronisation a
+ * cudaMalloc/cudaFree pair implies.  z4c_rhs needs a context, and creating one
+ * allocates, so those callers use this instead.
+ *
+ * z4c_rhs_noalloc computes what z4c_rhs computes (Z4c::Z4cRHS with the
+ * derivative precompute fused, Kreiss-Oliger included) for nblocks MeshBlocks
+ * of nx[0] x nx[1] x nx[2] cells and vertex spacing dx, all with the same
+ * spacing.  u and rhs are caller-owned DEVICE buffers in the register layout
+ * [block][22][nn2][nn1][nn0], nn = nx + 1 + 2*Z4C_NG; only the interior
+ * vertices of rhs are written, and u must already carry filled ghosts.  Work is
+ * enqueued on `stream` (a cudaStream_t; NULL = the legacy default stream).
+ *
+ * The scratch of the right-hand-side passes lives in one fixed array of
+ * Z4C_NOALLOC_SCRATCH_MIB MiB compiled into the library; every GPU that loads
+ * the library holds it until the process exits.  The first call on a device
+ * looks the array's device address up (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  Blocks are
+ * processed in chunks that fit the array; a MeshBlock whose scratch alone
+ * (224 bytes per interior vertex) exceeds it -- above roughly 64^3 cells --
+ * is rejected with Z4C_EINVAL before any work is enqueued.  Every call shares
+ * the array and it keeps the previous call's contents (nothing in it needs to
+ * start at zero); calls whose work overlaps on the GPU race on it, so
+ * serialise them (one stream, or events between streams).  No cudaMalloc,
+ * cudaFree or allocating library routine is called. */
+#define Z4C_NOALLOC_SCRATCH_MIB 64
+int z4c_rhs_noalloc(const double *u, double *rhs, int nblocks, const int nx[3],
+                    const double dx[3], const z4c_params_t *params, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
