@@ -43,6 +43,16 @@ CFL = 0.25
 # Algorithmic HBM bytes of one fused stage per interior vertex: read u and u1,
 # write u' and u1' (22 FP64 variables each).
 STAGE_BYTES_PER_POINT = 4 * 22 * 8
+# FP64 operations of the reference algorithm per interior vertex per stage on
+# 16^3 MeshBlocks: 7697 for PrepareZ4cDerivatives + Z4cRHS with KO, counted by
+# running the oracle with a counting number type (oracle/opcount), plus 154
+# for the low-storage stage update (7 per variable).
+FP64_OPS_PER_POINT_STAGE = 7697 + 154
+# The launches of one fused stage and their measured DRAM traffic per interior
+# vertex (ncu dram__bytes_read.sum + dram__bytes_write.sum summed over them,
+# 64-block capture scaled by the vertex count; see profiles/).
+STAGE_KERNELS = "k_ricci, k_adv, k_main, k_ko_stage_ls"
+STAGE_TRAFFIC_PER_POINT = 930.8e6 / (64 * 17 ** 3)
 
 
 def parse():
@@ -339,29 +349,22 @@ def main():
     except OSError:
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    fp64_flops = 0.0  # FP64 operations per interior vertex per stage, from ncu
-    flops_file = os.path.join(ROOT, "profiles", "stage_kernel_fp64_ops.json")
-    if os.path.exists(flops_file):
-        with open(flops_file) as f:
-            fp64_flops = json.load(f).get("fp64_ops_per_point", 0.0)
     fp64_peak_tf = ctx.fp64_probe()  # measured here: DFMA chains, 2 flops each
     stage_s = stage_ms * 1e-3
     achieved_gbs = STAGE_BYTES_PER_POINT * npts / stage_s / 1e9
-    if fp64_flops > 0:
-        achieved_tf = fp64_flops * npts / stage_s / 1e12
-        roof = {"bound": "fp64", "achieved": achieved_tf, "peak": fp64_peak_tf,
-                "unit": "TFLOP/s", "frac": achieved_tf / fp64_peak_tf, "traffic": None,
-                "hbm_achieved_gbs": achieved_gbs, "hbm_peak_gbs": hbm_peak,
-                "hbm_frac": achieved_gbs / hbm_peak, "kernel": "k_stage_ls",
-                "kernel_ms": stage_ms}
-    else:
-        roof = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved_gbs / hbm_peak, "traffic": None, "kernel": "k_stage_ls",
-                "kernel_ms": stage_ms}
-    traffic_file = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
-    if os.path.exists(traffic_file):
-        with open(traffic_file) as f:
-            roof["traffic"] = json.load(f).get("bytes_per_launch_full")
+    achieved_tf = FP64_OPS_PER_POINT_STAGE * npts / stage_s / 1e12
+    roof = {"bound": "fp64", "achieved": achieved_tf, "peak": fp64_peak_tf, "unit": "TFLOP/s",
+            "frac": achieved_tf / fp64_peak_tf,
+            "peak_source": "measured in this run: dependent DFMA chains on every SM "
+                           "(2 flops per DFMA); MEASURED_PEAKS.json has no FP64 figure",
+            "frac_of_unfused_ceiling": achieved_tf / (0.5 * fp64_peak_tf),
+            "traffic": STAGE_TRAFFIC_PER_POINT * npts,
+            "algorithmic_bytes": STAGE_BYTES_PER_POINT * npts,
+            "hbm_achieved_gbs": achieved_gbs, "hbm_peak_gbs": hbm_peak,
+            "hbm_frac": achieved_gbs / hbm_peak, "hbm_peak_source": "MEASURED_PEAKS.json",
+            "kernel": "RHS+KO+stage launch sequence (" + STAGE_KERNELS + "), one stage, "
+                      "all 512 MeshBlocks",
+            "kernel_ms": stage_ms, "fp64_ops_per_vertex": FP64_OPS_PER_POINT_STAGE}
 
     line = {
         "metric": METRIC, "value": value, "unit": "zone-updates/s", "n_gpus": world,

@@ -198,19 +198,22 @@ int run_stage(z4c_ctx* c, int stage, double dt) {
   double* w = c->reg[Z4C_REG_W];
   if (c->integrator == Z4C_INTEG_RK4) {
     const double* wt = kLsRk4[stage - 1];
-    if (stage == 1) {
-      launch_zero_interior(g, c->reg[Z4C_REG_U1], Z4C_NVAR, c->stream);
-      LAUNCH_CHECK("zero u1");
-    }
     if (!c->per_block) {
-      LsStage ls{wt[0], wt[1], wt[2], wt[3], wt[4] * dt};
+      // stage 1 treats u1 as the zero register the task list starts from
+      // instead of clearing it first
+      LsStage ls{wt[0], wt[1], wt[2], wt[3], wt[4] * dt, stage == 1 ? 1 : 0};
       launch_stage_ls(g, P, u, c->scratch(), c->reg[Z4C_REG_RHS], c->reg[Z4C_REG_U1], w, ls, 0,
                       g.nblocks, c->stream);
       LAUNCH_CHECK("stage_ls");
       return exchange_into(c, w, u, true);
     }
     // plain path, every operator launched per block as the task list calls
-    // them: Z4cRHS, WeightedAve x2, AddZ4cRHS; then exchange, AlgConstr
+    // them: u1 = 0 at stage 1, then Z4cRHS, WeightedAve x2, AddZ4cRHS; then
+    // exchange, AlgConstr
+    if (stage == 1) {
+      launch_zero_interior(g, c->reg[Z4C_REG_U1], Z4C_NVAR, c->stream);
+      LAUNCH_CHECK("zero u1");
+    }
     const double w1[3] = {1.0, wt[0], 0.0};
     const double w2[3] = {wt[1], wt[2], wt[3]};
     for (int b = 0; b < g.nblocks; ++b) {
@@ -704,7 +707,7 @@ int z4c_rhs_stage(z4c_ctx* ctx, int stage, double dt) {
   if (ctx->integrator != Z4C_INTEG_RK4)
     return fail(Z4C_ESTATE, "z4c_rhs_stage runs the low-storage stage only");
   const double* wt = kLsRk4[stage - 1];
-  LsStage ls{wt[0], wt[1], wt[2], wt[3], wt[4] * dt};
+  LsStage ls{wt[0], wt[1], wt[2], wt[3], wt[4] * dt, 0};
   launch_stage_ls(ctx->g, ctx->dev(), ctx->reg[Z4C_REG_U], ctx->scratch(),
                   ctx->reg[Z4C_REG_RHS], ctx->reg[Z4C_REG_U1], ctx->reg[Z4C_REG_W], ls, 0,
                   ctx->g.nblocks, ctx->stream);

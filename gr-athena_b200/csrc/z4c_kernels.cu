@@ -140,7 +140,7 @@ k_ko_stage_ls(Grid g, DevParams P, const double* __restrict__ u,
   const int64_t q = pv.q;
   const double r = add_ko(__ldg(rhs + q), u + q, g.s, P.fd[pv.b], P.p.diss);
   const double un = __ldg(u + q);
-  double v1 = u1[q];
+  double v1 = w.u1_zero ? 0.0 : u1[q];
   if (w.delta != 0.0) v1 += w.delta * un;  // w0 == 1, w2 == 0 branch
   double v;
   if (w.gamma1 == 1.0) {  // gamma3 == 0 for every 2S integrator accepted
@@ -190,13 +190,18 @@ k_ko_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* _
 // 1/multiplicity (comm/node_multiplicity.cpp:396-430).  Strictly interior
 // vertices are copied.  src and dst must differ.  With fuse_alg the
 // AlgConstr pass that follows in the task list is applied on the way out.
-__constant__ int c_dirs[26][3] = {
-    {-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1},
-    {-1, -1, 0}, {1, -1, 0}, {-1, 1, 0}, {1, 1, 0},
-    {-1, 0, -1}, {1, 0, -1}, {-1, 0, 1}, {1, 0, 1},
-    {0, -1, -1}, {0, 1, -1}, {0, -1, 1}, {0, 1, 1},
-    {-1, -1, -1}, {1, -1, -1}, {-1, 1, -1}, {1, 1, -1},
-    {-1, -1, 1}, {1, -1, 1}, {-1, 1, 1}, {1, 1, 1}};
+//
+// Per axis a vertex is a ghost (below vs or above ve: owned by the neighbour
+// on that side only), on a shared plane (vs or ve: owned by this block and
+// the neighbour on that side) or inside.  The owners of a vertex are the
+// directions whose support U contains every ghost axis and otherwise only
+// shared axes; U = {} is the block itself.  The neighbour list orders
+// directions by the size of their support and then by the support's axis
+// set as a bit mask (x=1, y=2, z=4): faces x, y, z, then edges xy, xz, yz,
+// then the corner.  u_order walks the supports in that order.
+__constant__ int c_dir_index[27];  // (o0+1) + 3(o1+1) + 9(o2+1) -> neighbour slot
+// supports in list order: 0, 1, 2, 4, 3, 5, 6, 7
+__device__ __forceinline__ constexpr int u_order(int q) { return (q == 3) ? 4 : (q == 4) ? 3 : q; }
 
 __global__ void __launch_bounds__(kPointThreads)
 k_exchange(Grid g, DevParams P, const double* __restrict__ src, double* __restrict__ dst,
@@ -205,53 +210,49 @@ k_exchange(Grid g, DevParams P, const double* __restrict__ src, double* __restri
   if (t >= g.nvol * g.nblocks) return;
   const int b = (int)(t / g.nvol);
   const int64_t p = t % g.nvol;
-  const int i = (int)(p % g.nn[0]);
-  const int j = (int)((p / g.nn[0]) % g.nn[1]);
-  const int k = (int)(p / ((int64_t)g.nn[0] * g.nn[1]));
-  const int idx[3] = {i, j, k};
-  bool interior = true, edge = false;
+  const int idx[3] = {(int)(p % g.nn[0]), (int)((p / g.nn[0]) % g.nn[1]),
+                      (int)(p / ((int64_t)g.nn[0] * g.nn[1]))};
+  int gmask = 0, smask = 0, side[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const int vs = NG, ve = NG + g.nx[a];
-    if (idx[a] < vs || idx[a] > ve) interior = false;
-    if (idx[a] <= vs || idx[a] >= ve) edge = true;
+    const int vs = NG, ve = NG + g.nx[a], x = idx[a];
+    side[a] = (x <= vs) ? -1 : 1;
+    if (x < vs || x > ve) gmask |= 1 << a;
+    else if (x == vs || x == ve) smask |= 1 << a;
   }
   const int64_t bstride = (int64_t)nvar * g.nvol;
-  const double* sb = src + b * bstride + p;
-  double* db = dst + b * bstride + p;
-  // neighbours covering this vertex, as 26-bit mask
-  unsigned mask = 0;
-  int mult = interior ? 1 : 0;
-  if (edge) {
-    for (int d = 0; d < 26; ++d) {
-      if (nbr[b * 26 + d] < 0) continue;
-      bool cov = true;
+  // source offset of every owner in list order (-1: not an owner)
+  int64_t off[8];
+  int mult = 0;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const int vs = NG, ve = NG + g.nx[a], o = c_dirs[d][a];
-        if (o > 0) cov = cov && (idx[a] >= ve);
-        else if (o < 0) cov = cov && (idx[a] <= vs);
-        else cov = cov && (idx[a] >= vs && idx[a] <= ve);
-      }
-      if (cov) {
-        mask |= 1u << d;
-        ++mult;
-      }
+  for (int q = 0; q < 8; ++q) {
+    const int U = u_order(q);
+    off[q] = -1;
+    if ((U & gmask) != gmask || (U & ~(gmask | smask)) != 0) continue;
+    if (U == 0) {
+      off[q] = (int64_t)b * bstride + p;
+      ++mult;
+      continue;
     }
+    int o[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) o[a] = (U >> a & 1) ? side[a] : 0;
+    const int nb = __ldg(nbr + b * 26 + c_dir_index[(o[0] + 1) + 3 * (o[1] + 1) + 9 * (o[2] + 1)]);
+    if (nb < 0) continue;
+    off[q] = (int64_t)nb * bstride + p -
+             (((int64_t)o[2] * g.nx[2] * g.nn[1] + (int64_t)o[1] * g.nx[1]) * g.nn[0] +
+              (int64_t)o[0] * g.nx[0]);
+    ++mult;
   }
   const double inv = (mult > 1) ? 1.0 / (double)mult : 1.0;
+  double* db = dst + (int64_t)b * bstride + p;
   auto value = [&](int n) -> double {
-    double s = interior ? __ldg(sb + (int64_t)n * g.nvol) : 0.0;
-    if (edge) {
-      for (int d = 0; d < 26; ++d) {
-        if (!(mask & (1u << d))) continue;
-        const int64_t q = ((int64_t)(k - c_dirs[d][2] * g.nx[2]) * g.nn[1] +
-                           (j - c_dirs[d][1] * g.nx[1])) * g.nn[0] +
-                          (i - c_dirs[d][0] * g.nx[0]);
-        s += __ldg(src + (int64_t)nbr[b * 26 + d] * bstride + (int64_t)n * g.nvol + q);
-      }
-      if (mult > 1) s *= inv;
-    }
+    const int64_t vo = (int64_t)n * g.nvol;
+    double s = (off[0] >= 0) ? __ldg(src + off[0] + vo) : 0.0;
+#pragma unroll
+    for (int q = 1; q < 8; ++q)
+      if (off[q] >= 0) s += __ldg(src + off[q] + vo);
+    if (mult > 1) s *= inv;
     return s;
   };
   if (!fuse_alg) {
@@ -283,26 +284,35 @@ k_exchange(Grid g, DevParams P, const double* __restrict__ src, double* __restri
 // ExtrapolateOutflowBC with NEXTRAPOLATE = 5 (comm/physical_bcs.cpp:187-260)
 // over the ranges of ApplyPhysicalBCs (:506-670): the cell-centred interior
 // end ie = is + nx - 1 bounds the outer faces and the transverse ranges.
-// One thread per (block, variable, transverse pair, side) cascades outward.
-__global__ void k_bc_axis(Grid g, double* __restrict__ u, int nvar, int ax) {
-  const int o1 = (ax + 1) % 3, o2 = (ax + 2) % 3;
+// Only the blocks on the two faces of axis ax are visited.  One thread per
+// (face block, variable, side, transverse pair) cascades outward; the
+// fastest thread index runs along the transverse axis of smallest stride.
+__global__ void __launch_bounds__(kPointThreads)
+k_bc_axis(Grid g, double* __restrict__ u, int nvar, int ax) {
+  const int o1 = (ax == 0) ? 1 : 0;       // fastest transverse axis
+  const int o2 = (ax == 2) ? 1 : 2;       // slowest transverse axis
   const int64_t nt = (int64_t)g.nn[o1] * g.nn[o2];
+  const int nfb = g.nb[o1] * g.nb[o2];    // blocks on one face
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nt * nvar * 2 * g.nblocks) return;
-  const int side = (int)(t % 2);
-  int64_t r = t / 2;
-  const int64_t tr = r % nt;
-  r /= nt;
+  if (t >= nt * 2 * nvar * nfb) return;
+  const int64_t tr = t % nt;
+  int64_t r = t / nt;
+  const int side = (int)(r % 2);
+  r /= 2;
   const int n = (int)(r % nvar);
-  const int b = (int)(r / nvar);
-  const int loc[3] = {b % g.nb[0], (b / g.nb[0]) % g.nb[1], b / (g.nb[0] * g.nb[1])};
+  const int fb = (int)(r / nvar);
+  int loc[3];
+  loc[ax] = side ? g.nb[ax] - 1 : 0;
+  loc[o1] = fb % g.nb[o1];
+  loc[o2] = fb / g.nb[o1];
+  if (g.bc[2 * ax + side] != Z4C_BC_OUTFLOW) return;
+  const int b = loc[0] + g.nb[0] * (loc[1] + g.nb[1] * loc[2]);
   bool need[6];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     need[2 * a] = (g.bc[2 * a] == Z4C_BC_OUTFLOW) && loc[a] == 0;
     need[2 * a + 1] = (g.bc[2 * a + 1] == Z4C_BC_OUTFLOW) && loc[a] == g.nb[a] - 1;
   }
-  if (!need[2 * ax + side]) return;
   int is[3], ie[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -625,8 +635,27 @@ void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const R
                                                                      w, block0, nblk);
 }
 
+// Slot of every direction in the neighbour list (mesh_topology.cpp:329-960
+// order, the c_dirs table of the context), indexed (o0+1) + 3(o1+1) + 9(o2+1).
+static int upload_dir_index() {
+  static const int dirs[26][3] = {
+      {-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1},
+      {-1, -1, 0}, {1, -1, 0}, {-1, 1, 0}, {1, 1, 0},
+      {-1, 0, -1}, {1, 0, -1}, {-1, 0, 1}, {1, 0, 1},
+      {0, -1, -1}, {0, 1, -1}, {0, -1, 1}, {0, 1, 1},
+      {-1, -1, -1}, {1, -1, -1}, {-1, 1, -1}, {1, 1, -1},
+      {-1, -1, 1}, {1, -1, 1}, {-1, 1, 1}, {1, 1, 1}};
+  int h[27];
+  for (int q = 0; q < 27; ++q) h[q] = 0;  // slot 13 (no offset) is never read
+  for (int d = 0; d < 26; ++d)
+    h[(dirs[d][0] + 1) + 3 * (dirs[d][1] + 1) + 9 * (dirs[d][2] + 1)] = d;
+  return (int)cudaMemcpyToSymbol(c_dir_index, h, sizeof(h));
+}
+
 void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst, int nvar,
                      const int* nbr, int fuse_alg, cudaStream_t st) {
+  static const int dir_rc = upload_dir_index();  // once per process
+  (void)dir_rc;
   const int64_t n = g.nvol * g.nblocks;
   COUNTED
   k_exchange<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, src, dst, nvar, nbr,
@@ -638,8 +667,9 @@ void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st) {
   for (int f = 0; f < 6; ++f) any |= (g.bc[f] == Z4C_BC_OUTFLOW);
   if (!any) return;
   for (int ax = 0; ax < 3; ++ax) {
-    const int o1 = (ax + 1) % 3, o2 = (ax + 2) % 3;
-    const int64_t n = (int64_t)g.nn[o1] * g.nn[o2] * nvar * 2 * g.nblocks;
+    if (g.bc[2 * ax] != Z4C_BC_OUTFLOW && g.bc[2 * ax + 1] != Z4C_BC_OUTFLOW) continue;
+    const int o1 = (ax == 0) ? 1 : 0, o2 = (ax == 2) ? 1 : 2;
+    const int64_t n = (int64_t)g.nn[o1] * g.nn[o2] * 2 * nvar * g.nb[o1] * g.nb[o2];
     COUNTED
     k_bc_axis<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, u, nvar, ax);
   }

@@ -18,8 +18,11 @@ struct Reg {
 
 // LS stage weights (task_list_integrators_low_storage.cpp:112-142) with the
 // step already scaled: beta_dt = beta * dt (time_integrators.hpp:37-40).
+// u1_zero: u1 is known to be zero (stage 1 after the task list's u1 = 0,
+// task_list_gr_z4c.cpp:115-119), so the kernel does not read it.
 struct LsStage {
   double delta, gamma1, gamma2, gamma3, beta_dt;
+  int u1_zero;
 };
 
 // Butcher stage: u_out = u_n + sum_{q < nq} coef[q] * k_q, coef = a*dt or b*dt
