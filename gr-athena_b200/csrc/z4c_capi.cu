@@ -107,6 +107,7 @@ struct z4c_ctx {
   double* reg[Z4C_NREG] = {};
   double* un = nullptr;   // Butcher u_n scratch
   double* guu = nullptr;  // ADMToZ4c inverse-metric scratch (6 vars)
+  double* sd = nullptr;   // stored first derivatives, 33 values per vertex
   double* rsum = nullptr; // Ricci-pass scratch, 6 values per interior vertex
   double* lv = nullptr;   // advection sums, 22 values per interior vertex
   double* xf = nullptr;   // [nblocks][nn0+nn1+nn2]
@@ -127,7 +128,7 @@ struct z4c_ctx {
   double graph_dt = 0.0;
   bool graph_per_block = false;
 
-  RhsScratch scratch() const { return RhsScratch{rsum, lv}; }
+  RhsScratch scratch() const { return RhsScratch{sd, rsum, lv}; }
 
   DevParams dev() const {
     DevParams P;
@@ -175,7 +176,7 @@ int64_t reg_elems(const z4c_ctx* c, int reg) { return (int64_t)reg_nvar_(reg) * 
 int exchange_into(z4c_ctx* c, const double* src, double* dst, bool alg) {
   const DevParams P = c->dev();
   const bool fuse = alg && !c->has_outflow;
-  launch_exchange(c->g, P, src, dst, Z4C_NVAR, c->nbr, fuse ? 1 : 0, c->stream);
+  launch_exchange(c->g, P, src, dst, c->nbr, fuse ? 1 : 0, c->stream);
   LAUNCH_CHECK("exchange");
   if (c->has_outflow) {
     launch_physical_bcs(c->g, dst, Z4C_NVAR, c->stream);
@@ -273,7 +274,7 @@ void free_ctx(z4c_ctx* c) {
   if (c->graph) cudaGraphExecDestroy(c->graph);
   for (auto& r : c->reg)
     if (r) cudaFree(r);
-  for (void* p : {(void*)c->un, (void*)c->guu, (void*)c->rsum, (void*)c->lv, (void*)c->xf, (void*)c->xv, (void*)c->fd,
+  for (void* p : {(void*)c->un, (void*)c->guu, (void*)c->sd, (void*)c->rsum, (void*)c->lv, (void*)c->xf, (void*)c->xv, (void*)c->fd,
                   (void*)c->nbr, (void*)c->partials, (void*)c->flag})
     if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -327,6 +328,13 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
       return fail(Z4C_EINVAL, "unknown boundary flag on axis %d", a);
     if ((lo == Z4C_BC_PERIODIC) != (hi == Z4C_BC_PERIODIC))
       return fail(Z4C_EINVAL, "axis %d: periodic on one face only", a);
+  }
+  {
+    // the column passes index (block, variable, interior column) in 32 bits
+    const int64_t cols = (int64_t)(mesh->nx[0] + 1) * (mesh->nx[1] + 1) * Z4C_NVAR *
+                         mesh->nb[0] * mesh->nb[1] * mesh->nb[2];
+    if (cols >= (int64_t)std::numeric_limits<int>::max())
+      return fail(Z4C_EINVAL, "mesh too large: %lld interior columns x variables", (long long)cols);
   }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -425,6 +433,8 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
   }
   if (rc == Z4C_OK && integrator == Z4C_INTEG_BT_RK4) rc = alloc((void**)&c->un, b22);
   if (rc == Z4C_OK) rc = alloc((void**)&c->guu, sizeof(double) * 6 * (size_t)g.nvol * nb);
+  if (rc == Z4C_OK)
+    rc = alloc((void**)&c->sd, sizeof(double) * kSdComponents * (size_t)g.nvol * nb);
   if (rc == Z4C_OK)
     rc = alloc((void**)&c->rsum, sizeof(double) * 6 * (size_t)interior_count(g) * nb);
   if (rc == Z4C_OK)

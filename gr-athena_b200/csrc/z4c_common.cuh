@@ -88,47 +88,6 @@ __device__ __forceinline__ double fd_dxy(const double* __restrict__ u, int64_t s
   return out * cidx1a;
 }
 
-// Lop-sided advection Lx (FDStencilBiased{Left,Right}<1,4,2>) and the
-// Kreiss-Oliger operator (FDStencilCenteredDegreeEven<8,4>) share the nine
-// points -4..4 along one axis.
-struct Line9 {
-  double v[9];
-};
-__device__ __forceinline__ Line9 load9(const double* __restrict__ u, int64_t s) {
-  Line9 l;
-#pragma unroll
-  for (int q = 0; q < 9; ++q) l.v[q] = __ldg(u + (q - 4) * s);
-  return l;
-}
-__device__ __forceinline__ double fd_lx(const Line9& l, double vx, double lidx) {
-  double dl = 0.;
-  dl += 1. * l.v[0];
-  dl += -8. * l.v[1];
-  dl += 30. * l.v[2];
-  dl += -80. * l.v[3];
-  dl += 35. * l.v[4];
-  dl += 24. * l.v[5];
-  dl += -2. * l.v[6];
-  double dr = 0.;
-  dr += -1. * l.v[8];
-  dr += 8. * l.v[7];
-  dr += -30. * l.v[6];
-  dr += 80. * l.v[5];
-  dr += -35. * l.v[4];
-  dr += -24. * l.v[3];
-  dr += 2. * l.v[2];
-  return ((vx < 0) ? (vx * dl) : (vx * dr)) * lidx;
-}
-__device__ __forceinline__ double fd_diss(const Line9& l, double cidxd, double diss) {
-  double out = 0.;
-  out += 1. * (l.v[0] + l.v[8]);
-  out += -8. * (l.v[1] + l.v[7]);
-  out += 28. * (l.v[2] + l.v[6]);
-  out += -56. * (l.v[3] + l.v[5]);
-  out += 70. * l.v[4];
-  return out * cidxd * diss;
-}
-
 // ---- linear algebra -------------------------------------------------------
 
 // index of the symmetric pair (a,b) in xx,xy,xz,yy,yz,zz order

@@ -14,7 +14,19 @@ namespace z4c {
 
 namespace {
 
-constexpr int kRhsThreads = 128;
+// Launch shape of the two heavy right-hand-side passes: threads per CTA and
+// the CTAs per SM the register allocation must allow (compile-time
+// candidates of the launch-shape sweep).
+#ifndef Z4C_RHS_THREADS
+#define Z4C_RHS_THREADS 128
+#endif
+#ifndef Z4C_RICCI_MINB
+#define Z4C_RICCI_MINB 1
+#endif
+#ifndef Z4C_MAIN_MINB
+#define Z4C_MAIN_MINB 1
+#endif
+constexpr int kRhsThreads = Z4C_RHS_THREADS;
 constexpr int kPointThreads = 256;
 
 inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
@@ -25,10 +37,64 @@ __device__ __forceinline__ double* rsum_at(const Grid& g, double* rsum, int b, i
   return rsum + (int64_t)b * 6 * interior_count(g) + l;
 }
 
+// ---- stored first derivatives (Z4c::PrepareZ4cDerivatives) ----------------
+// adm_z4c.cpp:972-1037: D_b f for f in chi, g~_ab, alpha, beta^a.  The
+// reference fills the interior extended by 3 vertices along both directions
+// other than b (:977-985); the passes that read them need D_b f off the
+// interior only along the directions a < b of the mixed derivatives
+// (Dx_a of the stored Dx_b), so D_x f is computed on the interior, D_y f on
+// the interior extended along x, D_z f extended along x and y.  Values are
+// the reference's wherever they are computed.
+//
+// One thread per (i, j) column of a component's region, looping over the
+// interior k; D_z keeps the seven-vertex window along k in registers.
+// blockIdx.y is the component slot*3 + b, blockIdx.z the block.
+__device__ __forceinline__ double fd_dx7(double m3, double m2, double m1, double p1, double p2,
+                                         double p3, double cidx1) {
+  double out = 0.;
+  out += -1. * (m3 - p3);
+  out += 9. * (m2 - p2);
+  out += -45. * (m1 - p1);
+  return out * cidx1;
+}
+
+__global__ void __launch_bounds__(kPointThreads)
+k_prep(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ sd, int block0) {
+  const int comp = blockIdx.y;
+  const int slot = comp / 3, dir = comp % 3;
+  const int b = block0 + (int)blockIdx.z;
+  const int ex = (dir >= 1) ? 3 : 0, ey = (dir == 2) ? 3 : 0;
+  const int e0 = g.nx[0] + 1 + 2 * ex, e1 = g.nx[1] + 1 + 2 * ey;
+  const int c = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (c >= e0 * e1) return;
+  const int i = NG - ex + c % e0, j = NG - ey + c / e0;
+  const int nn0 = g.nn[0];
+  const int sk = nn0 * g.nn[1];
+  const int k0 = NG, k1 = NG + g.nx[2];
+  const double* f = u + ((int64_t)b * NVAR + sd_field_var(slot)) * g.nvol + j * nn0 + i;
+  double* out = sd + ((int64_t)b * kSdComponents + comp) * g.nvol + j * nn0 + i;
+  const FdScale& F = P.fd[b];
+  if (dir == 2) {
+    const double cz = F.cidx1[2];
+    double w0 = __ldg(f + (k0 - 3) * sk), w1 = __ldg(f + (k0 - 2) * sk),
+           w2 = __ldg(f + (k0 - 1) * sk), w3 = __ldg(f + k0 * sk),
+           w4 = __ldg(f + (k0 + 1) * sk), w5 = __ldg(f + (k0 + 2) * sk);
+    for (int k = k0; k <= k1; ++k) {
+      const double w6 = __ldg(f + (k + 3) * sk);
+      out[k * sk] = fd_dx7(w0, w1, w2, w4, w5, w6, cz);
+      w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = w6;
+    }
+  } else {
+    const int st = (dir == 0) ? 1 : nn0;
+    const double ca = (dir == 0) ? F.cidx1[0] : F.cidx1[1];
+    for (int k = k0; k <= k1; ++k) out[k * sk] = fd_dx(f + k * sk, st, ca);
+  }
+}
+
 // ---- first pass: Ricci tensor + conformal-factor part per interior vertex --
-__global__ void __launch_bounds__(kRhsThreads, 1)
-k_ricci(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ rsum,
-        int block0, int nblk) {
+__global__ void __launch_bounds__(kRhsThreads, Z4C_RICCI_MINB)
+k_ricci(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
+        double* __restrict__ rsum, int block0, int nblk) {
   const int64_t npts = interior_count(g);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts * nblk) return;
@@ -38,7 +104,8 @@ k_ricci(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ 
   interior_ijk(g, l, i, j, k);
   const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
   double R[6];
-  ricci_point(u + (int64_t)b * NVAR * g.nvol, g.nvol, p, g.s, P, P.fd[b], R);
+  ricci_point(u + (int64_t)b * NVAR * g.nvol, sd + (int64_t)b * kSdComponents * g.nvol, g.nvol,
+              p, g.s, P, P.fd[b], R);
   double* rs = rsum_at(g, rsum, b, l);
 #pragma unroll
   for (int q = 0; q < 6; ++q) rs[(int64_t)q * npts] = R[q];
@@ -52,31 +119,257 @@ __device__ __forceinline__ void load_rsum(const Grid& g, const double* __restric
   for (int q = 0; q < 6; ++q) R[q] = __ldg(rs + (int64_t)q * npts);
 }
 
-// ---- advection sums: one thread per (interior vertex, variable) ----------
-// lv: [block][22][interior vertex]
+// ---- per-variable passes: advection sums and Kreiss-Oliger -------------------
+// One thread per (block, variable, interior (i, j)) column, looping over the
+// interior k.  Stencils along x and y read their lines directly; along z the
+// nine-vertex window slides in registers.  Index arithmetic is 32-bit (the
+// launcher checks that the thread count fits).
+struct Column {
+  int b, n, i, j;
+};
+__device__ __forceinline__ bool column_index(const Grid& g, int block0, int nblk, Column& c) {
+  const int n0 = g.nx[0] + 1, per = n0 * (g.nx[1] + 1);
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= per * NVAR * nblk) return false;
+  const int ij = t % per, rest = t / per;
+  c.n = rest % NVAR;
+  c.b = block0 + rest / NVAR;
+  c.i = NG + ij % n0;
+  c.j = NG + ij / n0;
+  return true;
+}
+
+// Lop-sided advection along one direction (FDStencilBiased{Left,Right}<1,4,2>,
+// finite_differencing.tpp:175-191): only the side the sign of vx selects is
+// evaluated; its value is the reference's, which evaluates both and keeps one.
+__device__ __forceinline__ double fd_lx_side(const double* __restrict__ u, int st, double vx,
+                                             double lidx) {
+  if (vx < 0) {
+    double dl = 0.;
+    dl += 1. * __ldg(u - 4 * st);
+    dl += -8. * __ldg(u - 3 * st);
+    dl += 30. * __ldg(u - 2 * st);
+    dl += -80. * __ldg(u - st);
+    dl += 35. * __ldg(u);
+    dl += 24. * __ldg(u + st);
+    dl += -2. * __ldg(u + 2 * st);
+    return (vx * dl) * lidx;
+  }
+  double dr = 0.;
+  dr += -1. * __ldg(u + 4 * st);
+  dr += 8. * __ldg(u + 3 * st);
+  dr += -30. * __ldg(u + 2 * st);
+  dr += 80. * __ldg(u + st);
+  dr += -35. * __ldg(u);
+  dr += -24. * __ldg(u - st);
+  dr += 2. * __ldg(u - 2 * st);
+  return (vx * dr) * lidx;
+}
+// The same along z from the window w[0..8] = f(k-4..k+4).
+__device__ __forceinline__ double fd_lx_window(const double w[9], double vx, double lidx) {
+  if (vx < 0) {
+    double dl = 0.;
+    dl += 1. * w[0];
+    dl += -8. * w[1];
+    dl += 30. * w[2];
+    dl += -80. * w[3];
+    dl += 35. * w[4];
+    dl += 24. * w[5];
+    dl += -2. * w[6];
+    return (vx * dl) * lidx;
+  }
+  double dr = 0.;
+  dr += -1. * w[8];
+  dr += 8. * w[7];
+  dr += -30. * w[6];
+  dr += 80. * w[5];
+  dr += -35. * w[4];
+  dr += -24. * w[3];
+  dr += 2. * w[2];
+  return (vx * dr) * lidx;
+}
+
+// Kreiss-Oliger along one direction (FDStencilCenteredDegreeEven<8,4>,
+// finite_differencing.tpp:335-368) from a line pointer or from the window.
+__device__ __forceinline__ double fd_diss_line(const double* __restrict__ u, int st, double cidxd,
+                                               double diss) {
+  double out = 0.;
+  out += 1. * (__ldg(u - 4 * st) + __ldg(u + 4 * st));
+  out += -8. * (__ldg(u - 3 * st) + __ldg(u + 3 * st));
+  out += 28. * (__ldg(u - 2 * st) + __ldg(u + 2 * st));
+  out += -56. * (__ldg(u - st) + __ldg(u + st));
+  out += 70. * __ldg(u);
+  return out * cidxd * diss;
+}
+__device__ __forceinline__ double fd_diss_window(const double w[9], double cidxd, double diss) {
+  double out = 0.;
+  out += 1. * (w[0] + w[8]);
+  out += -8. * (w[1] + w[7]);
+  out += 28. * (w[2] + w[6]);
+  out += -56. * (w[3] + w[5]);
+  out += 70. * w[4];
+  return out * cidxd * diss;
+}
+
+// Fills the z window of column c at the first interior k.
+__device__ __forceinline__ void window_init(const double* __restrict__ f, int sk, int k0,
+                                            double w[9]) {
+#pragma unroll
+  for (int q = 0; q < 8; ++q) w[q] = __ldg(f + (k0 - 4 + q) * sk);
+}
+__device__ __forceinline__ void window_advance(const double* __restrict__ f, int sk, int k,
+                                               double w[9]) {
+  w[8] = __ldg(f + (k + 4) * sk);
+}
+__device__ __forceinline__ void window_shift(double w[9]) {
+#pragma unroll
+  for (int q = 0; q < 8; ++q) w[q] = w[q + 1];
+}
+
+// Advection sums (calculate_z4c_rhs.cpp:184-226): lv [block][22][interior vertex]
 __global__ void __launch_bounds__(kPointThreads)
 k_adv(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ lv, int block0,
       int nblk) {
+  Column c;
+  if (!column_index(g, block0, nblk, c)) return;
+  const int nn0 = g.nn[0], sk = nn0 * g.nn[1];
+  const int n0 = g.nx[0] + 1, n1 = g.nx[1] + 1;
   const int64_t npts = interior_count(g);
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= npts * NVAR * nblk) return;
-  const int64_t l = t % npts;
-  const int n = (int)((t / npts) % NVAR);
-  const int b = block0 + (int)(t / (npts * NVAR));
-  int i, j, k;
-  interior_ijk(g, l, i, j, k);
-  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
-  const double* U = u + (int64_t)b * NVAR * g.nvol + p;
-  double beta[3];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) beta[a] = __ldg(U + (int64_t)(Z4C_BETAX + a) * g.nvol);
-  lv[((int64_t)b * NVAR + n) * npts + l] = advect_point(U, g.nvol, n, g.s, P.fd[b], beta);
+  const double* U = u + (int64_t)c.b * NVAR * g.nvol + c.j * nn0 + c.i;
+  const double* f = U + (int64_t)c.n * g.nvol;
+  const double* bx = U + (int64_t)Z4C_BETAX * g.nvol;
+  const double* by = U + (int64_t)Z4C_BETAY * g.nvol;
+  const double* bz = U + (int64_t)Z4C_BETAZ * g.nvol;
+  double* out = lv + ((int64_t)c.b * NVAR + c.n) * npts + (c.j - NG) * n0 + (c.i - NG);
+  const FdScale& F = P.fd[c.b];
+  double w[9];
+  window_init(f, sk, NG, w);
+  for (int k = NG; k <= NG + g.nx[2]; ++k) {
+    window_advance(f, sk, k, w);
+    const int o = k * sk;
+    double acc = 0;
+    acc += fd_lx_side(f + o, 1, __ldg(bx + o), F.lidx[0]);
+    acc += fd_lx_side(f + o, nn0, __ldg(by + o), F.lidx[1]);
+    acc += fd_lx_window(w, __ldg(bz + o), F.lidx[2]);
+    out[(k - NG) * n0 * n1] = acc;
+    window_shift(w);
+  }
+}
+
+// Kreiss-Oliger added to one right-hand-side value in the reference's
+// order, rhs += Diss_x; rhs += Diss_y; rhs += Diss_z (:908-915).
+__device__ __forceinline__ double add_ko_column(double r, const double* __restrict__ fo, int nn0,
+                                                const double w[9], const FdScale& F,
+                                                double diss) {
+  r += fd_diss_line(fo, 1, F.cidxd[0], diss);
+  r += fd_diss_line(fo, nn0, F.cidxd[1], diss);
+  r += fd_diss_window(w, F.cidxd[2], diss);
+  return r;
+}
+
+// Z4cRHS tail: rhs += KO, in place.
+__global__ void __launch_bounds__(kPointThreads)
+k_ko_rhs(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ rhs,
+         int block0, int nblk) {
+  Column c;
+  if (!column_index(g, block0, nblk, c)) return;
+  const int nn0 = g.nn[0], sk = nn0 * g.nn[1];
+  const int64_t base = ((int64_t)c.b * NVAR + c.n) * g.nvol + c.j * nn0 + c.i;
+  const double* f = u + base;
+  const FdScale& F = P.fd[c.b];
+  double w[9];
+  window_init(f, sk, NG, w);
+  for (int k = NG; k <= NG + g.nx[2]; ++k) {
+    window_advance(f, sk, k, w);
+    const int o = k * sk;
+    rhs[base + o] = add_ko_column(rhs[base + o], f + o, nn0, w, F, P.p.diss);
+    window_shift(w);
+  }
+}
+
+// ---- KO + low-storage RK stage ----------------------------------------------
+// IntegrateZ4c for 2S integrators (task_list_gr_z4c.cpp:176-195):
+//   WeightedAve(u1, u, u2, {1, delta, 0}); WeightedAve(u, u1, u2, {g1, g2, g3});
+//   AddZ4cRHS(rhs, beta*dt, u)        (mesh/weighted_ave.cpp:20-150)
+// u is read (all points, for the stencils); u_out, u1 are written (interior).
+__global__ void __launch_bounds__(kPointThreads)
+k_ko_stage_ls(Grid g, DevParams P, const double* __restrict__ u,
+              const double* __restrict__ rhs, double* __restrict__ u1,
+              double* __restrict__ u_out, LsStage w, int block0, int nblk) {
+  Column c;
+  if (!column_index(g, block0, nblk, c)) return;
+  const int nn0 = g.nn[0], sk = nn0 * g.nn[1];
+  const int64_t base = ((int64_t)c.b * NVAR + c.n) * g.nvol + c.j * nn0 + c.i;
+  const double* f = u + base;
+  const FdScale& F = P.fd[c.b];
+  double win[9];
+  window_init(f, sk, NG, win);
+  for (int k = NG; k <= NG + g.nx[2]; ++k) {
+    window_advance(f, sk, k, win);
+    const int o = k * sk;
+    const int64_t q = base + o;
+    const double r = add_ko_column(__ldg(rhs + q), f + o, nn0, win, F, P.p.diss);
+    const double un = win[4];
+    double v1 = w.u1_zero ? 0.0 : u1[q];
+    if (w.delta != 0.0) v1 += w.delta * un;  // w0 == 1, w2 == 0 branch
+    double v;
+    if (w.gamma1 == 1.0) {  // gamma3 == 0 for every 2S integrator accepted
+      v = un;
+      if (w.gamma2 != 0.0) v += w.gamma2 * v1;
+    } else if (w.gamma1 == 0.0) {
+      if (w.gamma2 == 1.0) v = v1;
+      else v = w.gamma2 * v1;
+    } else {
+      if (w.gamma2 != 0.0) v = w.gamma1 * un + w.gamma2 * v1;
+      else v = un * w.gamma1;
+    }
+    v += w.beta_dt * r;
+    u1[q] = v1;
+    u_out[q] = v;
+    window_shift(win);
+  }
+}
+
+// ---- KO + Butcher stage (task_list_integrators_butcher.cpp:512-680) ---------
+// k_s = RHS(u); u_out = u_n + sum_q coef_q k_q in the reference's order.
+struct KPtrs {
+  double* k[4];
+};
+__global__ void __launch_bounds__(kPointThreads)
+k_ko_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ rhs,
+              const double* __restrict__ un, KPtrs K, double* __restrict__ u_out, BtStage w,
+              int block0, int nblk) {
+  Column c;
+  if (!column_index(g, block0, nblk, c)) return;
+  const int nn0 = g.nn[0], sk = nn0 * g.nn[1];
+  const int64_t base = ((int64_t)c.b * NVAR + c.n) * g.nvol + c.j * nn0 + c.i;
+  const double* f = u + base;
+  const FdScale& F = P.fd[c.b];
+  double win[9];
+  window_init(f, sk, NG, win);
+  for (int k = NG; k <= NG + g.nx[2]; ++k) {
+    window_advance(f, sk, k, win);
+    const int o = k * sk;
+    const int64_t q = base + o;
+    const double r = add_ko_column(__ldg(rhs + q), f + o, nn0, win, F, P.p.diss);
+    K.k[w.kslot][q] = r;
+    double v = __ldg(un + q);
+    for (int s = 0; s < w.nq; ++s) {
+      if (w.coef[s] != 0.0) {
+        const double ks = (s == w.kslot) ? r : K.k[s][q];
+        v += w.coef[s] * ks;
+      }
+    }
+    u_out[q] = v;
+    window_shift(win);
+  }
 }
 
 // ---- main pass: the right-hand side without the Kreiss-Oliger terms -------
-__global__ void __launch_bounds__(kRhsThreads, 1)
-k_main(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ rsum,
-       const double* __restrict__ lv, double* __restrict__ rhs, int block0, int nblk) {
+__global__ void __launch_bounds__(kRhsThreads, Z4C_MAIN_MINB)
+k_main(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
+       const double* __restrict__ rsum, const double* __restrict__ lv, double* __restrict__ rhs,
+       int block0, int nblk) {
   const int64_t npts = interior_count(g);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts * nblk) return;
@@ -91,95 +384,11 @@ k_main(Grid g, DevParams P, const double* __restrict__ u, const double* __restri
 #pragma unroll
   for (int n = 0; n < NVAR; ++n) L[n] = __ldg(lv + ((int64_t)b * NVAR + n) * npts + l);
   double out[NVAR];
-  rhs_point(u + (int64_t)b * NVAR * g.nvol, g.nvol, p, g.s, P, P.fd[b], R, L, out);
+  rhs_point(u + (int64_t)b * NVAR * g.nvol, sd + (int64_t)b * kSdComponents * g.nvol, g.nvol, p,
+            g.s, P, P.fd[b], R, L, out);
   double* rb = rhs + (int64_t)b * NVAR * g.nvol + p;
 #pragma unroll
   for (int n = 0; n < NVAR; ++n) rb[(int64_t)n * g.nvol] = out[n];
-}
-
-// (interior vertex, variable) of thread t in the KO passes, l fastest
-struct PointVar {
-  int b, n;
-  int64_t p;  // vertex offset in the block
-  int64_t q;  // offset of (b, n, p) in a 22-variable register
-};
-__device__ __forceinline__ bool point_var(const Grid& g, int block0, int nblk, PointVar& pv) {
-  const int64_t npts = interior_count(g);
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= npts * NVAR * nblk) return false;
-  const int64_t l = t % npts;
-  pv.n = (int)((t / npts) % NVAR);
-  pv.b = block0 + (int)(t / (npts * NVAR));
-  int i, j, k;
-  interior_ijk(g, l, i, j, k);
-  pv.p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
-  pv.q = ((int64_t)pv.b * NVAR + pv.n) * g.nvol + pv.p;
-  return true;
-}
-
-// Z4cRHS tail: rhs += KO, in place.
-__global__ void __launch_bounds__(kPointThreads)
-k_ko_rhs(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ rhs,
-         int block0, int nblk) {
-  PointVar pv;
-  if (!point_var(g, block0, nblk, pv)) return;
-  rhs[pv.q] = add_ko(rhs[pv.q], u + pv.q, g.s, P.fd[pv.b], P.p.diss);
-}
-
-// ---- KO + low-storage RK stage ----------------------------------------------
-// IntegrateZ4c for 2S integrators (task_list_gr_z4c.cpp:176-195):
-//   WeightedAve(u1, u, u2, {1, delta, 0}); WeightedAve(u, u1, u2, {g1, g2, g3});
-//   AddZ4cRHS(rhs, beta*dt, u)        (mesh/weighted_ave.cpp:20-150)
-// u is read (all points, for the stencils); u_out, u1 are written (interior).
-__global__ void __launch_bounds__(kPointThreads)
-k_ko_stage_ls(Grid g, DevParams P, const double* __restrict__ u,
-              const double* __restrict__ rhs, double* __restrict__ u1,
-              double* __restrict__ u_out, LsStage w, int block0, int nblk) {
-  PointVar pv;
-  if (!point_var(g, block0, nblk, pv)) return;
-  const int64_t q = pv.q;
-  const double r = add_ko(__ldg(rhs + q), u + q, g.s, P.fd[pv.b], P.p.diss);
-  const double un = __ldg(u + q);
-  double v1 = w.u1_zero ? 0.0 : u1[q];
-  if (w.delta != 0.0) v1 += w.delta * un;  // w0 == 1, w2 == 0 branch
-  double v;
-  if (w.gamma1 == 1.0) {  // gamma3 == 0 for every 2S integrator accepted
-    v = un;
-    if (w.gamma2 != 0.0) v += w.gamma2 * v1;
-  } else if (w.gamma1 == 0.0) {
-    if (w.gamma2 == 1.0) v = v1;
-    else v = w.gamma2 * v1;
-  } else {
-    if (w.gamma2 != 0.0) v = w.gamma1 * un + w.gamma2 * v1;
-    else v = un * w.gamma1;
-  }
-  v += w.beta_dt * r;
-  u1[q] = v1;
-  u_out[q] = v;
-}
-
-// ---- KO + Butcher stage (task_list_integrators_butcher.cpp:512-680) ---------
-// k_s = RHS(u); u_out = u_n + sum_q coef_q k_q in the reference's order.
-struct KPtrs {
-  double* k[4];
-};
-__global__ void __launch_bounds__(kPointThreads)
-k_ko_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ rhs,
-              const double* __restrict__ un, KPtrs K, double* __restrict__ u_out, BtStage w,
-              int block0, int nblk) {
-  PointVar pv;
-  if (!point_var(g, block0, nblk, pv)) return;
-  const int64_t q = pv.q;
-  const double r = add_ko(__ldg(rhs + q), u + q, g.s, P.fd[pv.b], P.p.diss);
-  K.k[w.kslot][q] = r;
-  double v = __ldg(un + q);
-  for (int s = 0; s < w.nq; ++s) {
-    if (w.coef[s] != 0.0) {
-      const double ks = (s == w.kslot) ? r : K.k[s][q];
-      v += w.coef[s] * ks;
-    }
-  }
-  u_out[q] = v;
 }
 
 // ---- same-level vertex-centred ghost exchange -------------------------------
@@ -188,8 +397,7 @@ k_ko_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* _
 // holds the vertex adds its value in neighbour-list order
 // (mesh/mesh_topology.cpp:329-960), and the sum is multiplied by
 // 1/multiplicity (comm/node_multiplicity.cpp:396-430).  Strictly interior
-// vertices are copied.  src and dst must differ.  With fuse_alg the
-// AlgConstr pass that follows in the task list is applied on the way out.
+// vertices keep their value.
 //
 // Per axis a vertex is a ghost (below vs or above ve: owned by the neighbour
 // on that side only), on a shared plane (vs or ve: owned by this block and
@@ -199,41 +407,46 @@ k_ko_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* _
 // directions by the size of their support and then by the support's axis
 // set as a bit mask (x=1, y=2, z=4): faces x, y, z, then edges xy, xz, yz,
 // then the corner.  u_order walks the supports in that order.
+//
+// Two passes.  k_exchange_interior forms every block's own vertices
+// [vs, ve]^3 from the owners' pre-exchange copies (src).  For a ghost
+// vertex, the owners seen from this block are the ones seen from its
+// primary owner (the neighbour across the ghost axes only) plus the ghost
+// axes, in the same order, so the reference's sum for the ghost equals the
+// primary owner's result for that vertex: k_exchange_ghosts copies it from
+// there.  With fuse_alg the AlgConstr pass that follows in the task list is
+// applied to the interior results, and the ghosts copy those.
 __constant__ int c_dir_index[27];  // (o0+1) + 3(o1+1) + 9(o2+1) -> neighbour slot
 // supports in list order: 0, 1, 2, 4, 3, 5, 6, 7
 __device__ __forceinline__ constexpr int u_order(int q) { return (q == 3) ? 4 : (q == 4) ? 3 : q; }
 
 __global__ void __launch_bounds__(kPointThreads)
-k_exchange(Grid g, DevParams P, const double* __restrict__ src, double* __restrict__ dst,
-           int nvar, const int* __restrict__ nbr, int fuse_alg) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= g.nvol * g.nblocks) return;
-  const int b = (int)(t / g.nvol);
-  const int64_t p = t % g.nvol;
-  const int idx[3] = {(int)(p % g.nn[0]), (int)((p / g.nn[0]) % g.nn[1]),
-                      (int)(p / ((int64_t)g.nn[0] * g.nn[1]))};
-  int gmask = 0, smask = 0, side[3];
+k_exchange_interior(Grid g, DevParams P, const double* __restrict__ src,
+                    double* __restrict__ dst, const int* __restrict__ nbr, int fuse_alg) {
+  const int n0 = g.nx[0] + 1, n1 = g.nx[1] + 1, n2 = g.nx[2] + 1;
+  const int per = n0 * n1 * n2;
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= per * g.nblocks) return;
+  const int b = t / per, l = t % per;
+  const int idx[3] = {NG + l % n0, NG + (l / n0) % n1, NG + l / (n0 * n1)};
+  const int p = (idx[2] * g.nn[1] + idx[1]) * g.nn[0] + idx[0];
+  int smask = 0, side[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const int vs = NG, ve = NG + g.nx[a], x = idx[a];
-    side[a] = (x <= vs) ? -1 : 1;
-    if (x < vs || x > ve) gmask |= 1 << a;
-    else if (x == vs || x == ve) smask |= 1 << a;
+    side[a] = (x == vs) ? -1 : 1;
+    if (x == vs || x == ve) smask |= 1 << a;
   }
-  const int64_t bstride = (int64_t)nvar * g.nvol;
+  const int64_t bstride = (int64_t)NVAR * g.nvol;
   // source offset of every owner in list order (-1: not an owner)
   int64_t off[8];
-  int mult = 0;
+  int mult = 1;
+  off[0] = (int64_t)b * bstride + p;
 #pragma unroll
-  for (int q = 0; q < 8; ++q) {
+  for (int q = 1; q < 8; ++q) {
     const int U = u_order(q);
     off[q] = -1;
-    if ((U & gmask) != gmask || (U & ~(gmask | smask)) != 0) continue;
-    if (U == 0) {
-      off[q] = (int64_t)b * bstride + p;
-      ++mult;
-      continue;
-    }
+    if (smask == 0 || (U & ~smask) != 0) continue;
     int o[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) o[a] = (U >> a & 1) ? side[a] : 0;
@@ -245,39 +458,72 @@ k_exchange(Grid g, DevParams P, const double* __restrict__ src, double* __restri
     ++mult;
   }
   const double inv = (mult > 1) ? 1.0 / (double)mult : 1.0;
-  double* db = dst + (int64_t)b * bstride + p;
-  auto value = [&](int n) -> double {
-    const int64_t vo = (int64_t)n * g.nvol;
-    double s = (off[0] >= 0) ? __ldg(src + off[0] + vo) : 0.0;
+  double v[NVAR];
 #pragma unroll
-    for (int q = 1; q < 8; ++q)
-      if (off[q] >= 0) s += __ldg(src + off[q] + vo);
-    if (mult > 1) s *= inv;
-    return s;
-  };
-  if (!fuse_alg) {
-    for (int n = 0; n < nvar; ++n) db[(int64_t)n * g.nvol] = value(n);
+  for (int n = 0; n < NVAR; ++n) v[n] = __ldg(src + off[0] + (int64_t)n * g.nvol);
+  if (mult > 1) {
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) {
+      const int64_t vo = (int64_t)n * g.nvol;
+      double s = v[n];
+#pragma unroll
+      for (int q = 1; q < 8; ++q)
+        if (off[q] >= 0) s += __ldg(src + off[q] + vo);
+      v[n] = s * inv;
+    }
+  }
+  if (fuse_alg) {
+    double gg[6], AA[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      gg[c] = v[Z4C_GXX + c];
+      AA[c] = v[Z4C_AXX + c];
+    }
+    alg_constr_point(P.p, gg, AA, &v[Z4C_CHI], &v[Z4C_ALPHA]);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      v[Z4C_GXX + c] = gg[c];
+      v[Z4C_AXX + c] = AA[c];
+    }
+  }
+  double* db = dst + off[0];
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) db[(int64_t)n * g.nvol] = v[n];
+}
+
+// Ghost vertices: copy of the primary owner's result (zero where the primary
+// owner lies beyond a physical face; the boundary conditions overwrite those).
+__global__ void __launch_bounds__(kPointThreads)
+k_exchange_ghosts(Grid g, double* __restrict__ u, const int* __restrict__ nbr) {
+  const int per = (int)g.nvol;
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= per * g.nblocks) return;
+  const int b = t / per, p = t % per;
+  const int idx[3] = {p % g.nn[0], (p / g.nn[0]) % g.nn[1], p / (g.nn[0] * g.nn[1])};
+  int o[3];
+  bool ghost = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    o[a] = (idx[a] < NG) ? -1 : (idx[a] > NG + g.nx[a] ? 1 : 0);
+    ghost |= (o[a] != 0);
+  }
+  if (!ghost) return;
+  const int64_t bstride = (int64_t)NVAR * g.nvol;
+  double* db = u + (int64_t)b * bstride + p;
+  const int nb = __ldg(nbr + b * 26 + c_dir_index[(o[0] + 1) + 3 * (o[1] + 1) + 9 * (o[2] + 1)]);
+  if (nb < 0) {
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) db[(int64_t)n * g.nvol] = 0.0;
     return;
   }
-  double gg[6], AA[6];
+  const double* sb = u + (int64_t)nb * bstride + p -
+                     (((int64_t)o[2] * g.nx[2] * g.nn[1] + (int64_t)o[1] * g.nx[1]) * g.nn[0] +
+                      (int64_t)o[0] * g.nx[0]);
+  double v[NVAR];
 #pragma unroll
-  for (int c = 0; c < 6; ++c) {
-    gg[c] = value(Z4C_GXX + c);
-    AA[c] = value(Z4C_AXX + c);
-  }
-  double chi = value(Z4C_CHI), alpha = value(Z4C_ALPHA);
-  alg_constr_point(P.p, gg, AA, &chi, &alpha);
+  for (int n = 0; n < NVAR; ++n) v[n] = sb[(int64_t)n * g.nvol];
 #pragma unroll
-  for (int c = 0; c < 6; ++c) {
-    db[(int64_t)(Z4C_GXX + c) * g.nvol] = gg[c];
-    db[(int64_t)(Z4C_AXX + c) * g.nvol] = AA[c];
-  }
-  db[(int64_t)Z4C_CHI * g.nvol] = chi;
-  db[(int64_t)Z4C_ALPHA * g.nvol] = alpha;
-  const int rest[8] = {Z4C_KHAT, Z4C_GAMX, Z4C_GAMY, Z4C_GAMZ, Z4C_THETA,
-                       Z4C_BETAX, Z4C_BETAY, Z4C_BETAZ};
-#pragma unroll
-  for (int r = 0; r < 8; ++r) db[(int64_t)rest[r] * g.nvol] = value(rest[r]);
+  for (int n = 0; n < NVAR; ++n) db[(int64_t)n * g.nvol] = v[n];
 }
 
 // ---- extrapolate_outflow boundary conditions --------------------------------
@@ -590,37 +836,46 @@ long long kernel_launch_count() { return g_launches.load(); }
 void add_kernel_launches(long long n) { g_launches += n; }
 #define COUNTED ++g_launches;
 
+// Threads of the column passes (one per block, variable and interior (i, j)).
+static int64_t columns(const Grid& g, int nblk) {
+  return (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * NVAR * nblk;
+}
+
 // The right-hand side passes shared by every RHS launch: Ricci (rsum),
 // advection sums (lv) and the main pass into rhs (without KO).
 static void launch_rhs_passes(const Grid& g, const DevParams& P, const double* u,
                               const RhsScratch& sc, double* rhs, int block0, int nblk,
                               cudaStream_t st) {
   const int64_t n = interior_count(g) * nblk;
+  const int64_t cprep = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7);  // widest component region
   COUNTED
-  k_ricci<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, sc.rsum, block0, nblk);
+  k_prep<<<dim3(div_up(cprep, kPointThreads), kSdComponents, nblk), kPointThreads, 0, st>>>(
+      g, P, u, sc.sd, block0);
   COUNTED
-  k_adv<<<div_up(n * NVAR, kPointThreads), kPointThreads, 0, st>>>(g, P, u, sc.lv, block0, nblk);
+  k_ricci<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, sc.sd, sc.rsum, block0, nblk);
   COUNTED
-  k_main<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, sc.rsum, sc.lv, rhs, block0,
-                                                          nblk);
+  k_adv<<<div_up(columns(g, nblk), kPointThreads), kPointThreads, 0, st>>>(g, P, u, sc.lv, block0,
+                                                                           nblk);
+  COUNTED
+  k_main<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, sc.sd, sc.rsum, sc.lv, rhs,
+                                                          block0, nblk);
 }
 
 void launch_rhs(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                 double* rhs, int block0, int nblk, cudaStream_t st) {
   launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, st);
-  const int64_t n = interior_count(g) * nblk * NVAR;
   COUNTED
-  k_ko_rhs<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, rhs, block0, nblk);
+  k_ko_rhs<<<div_up(columns(g, nblk), kPointThreads), kPointThreads, 0, st>>>(g, P, u, rhs, block0,
+                                                                              nblk);
 }
 
 void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                      double* rhs, double* u1, double* u_out, const LsStage& w, int block0,
                      int nblk, cudaStream_t st) {
   launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, st);
-  const int64_t n = interior_count(g) * nblk * NVAR;
   COUNTED
-  k_ko_stage_ls<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, rhs, u1, u_out, w,
-                                                                     block0, nblk);
+  k_ko_stage_ls<<<div_up(columns(g, nblk), kPointThreads), kPointThreads, 0, st>>>(
+      g, P, u, rhs, u1, u_out, w, block0, nblk);
 }
 
 void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
@@ -629,10 +884,9 @@ void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const R
   launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, st);
   KPtrs K;
   for (int s = 0; s < 4; ++s) K.k[s] = k[s];
-  const int64_t n = interior_count(g) * nblk * NVAR;
   COUNTED
-  k_ko_stage_bt<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, rhs, un, K, u_out,
-                                                                     w, block0, nblk);
+  k_ko_stage_bt<<<div_up(columns(g, nblk), kPointThreads), kPointThreads, 0, st>>>(
+      g, P, u, rhs, un, K, u_out, w, block0, nblk);
 }
 
 // Slot of every direction in the neighbour list (mesh_topology.cpp:329-960
@@ -652,14 +906,16 @@ static int upload_dir_index() {
   return (int)cudaMemcpyToSymbol(c_dir_index, h, sizeof(h));
 }
 
-void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst, int nvar,
+void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst,
                      const int* nbr, int fuse_alg, cudaStream_t st) {
   static const int dir_rc = upload_dir_index();  // once per process
   (void)dir_rc;
-  const int64_t n = g.nvol * g.nblocks;
   COUNTED
-  k_exchange<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, src, dst, nvar, nbr,
-                                                                  fuse_alg);
+  k_exchange_interior<<<div_up(interior_count(g) * g.nblocks, kPointThreads), kPointThreads, 0,
+                        st>>>(g, P, src, dst, nbr, fuse_alg);
+  COUNTED
+  k_exchange_ghosts<<<div_up(g.nvol * g.nblocks, kPointThreads), kPointThreads, 0, st>>>(g, dst,
+                                                                                        nbr);
 }
 
 void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st) {

@@ -53,17 +53,21 @@ void add_kernel_launches(long long n);
 
 // All launches return cudaGetLastError() mapped by the caller.
 // Scratch of the right-hand-side passes, indexed by absolute block:
-// rsum [block][6][interior vertex] (R_ab + Rphi_ab), lv [block][22][interior
-// vertex] (advection sums).
+// sd [block][33][vertex] (stored first derivatives of chi, g~, alpha, beta
+// along x, y, z), rsum [block][6][interior vertex] (R_ab + Rphi_ab),
+// lv [block][22][interior vertex] (advection sums).
 struct RhsScratch {
+  double* sd;
   double* rsum;
   double* lv;
 };
+constexpr int kSdComponents = 33;
 
-// Every RHS launch runs four kernels: Ricci pass, advection sums, main pass
-// (into rhs, without Kreiss-Oliger), then Kreiss-Oliger fused with the
-// consumer: in place for launch_rhs, with the stage update for the stage
-// launches (rhs then holds the pre-dissipation right-hand side).
+// Every RHS launch runs five kernels: stored first derivatives, Ricci pass,
+// advection sums, main pass (into rhs, without Kreiss-Oliger), then
+// Kreiss-Oliger fused with the consumer: in place for launch_rhs, with the
+// stage update for the stage launches (rhs then holds the pre-dissipation
+// right-hand side).
 void launch_rhs(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                 double* rhs, int block0, int nblk, cudaStream_t st);
 void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
@@ -72,8 +76,10 @@ void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, const R
 void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                      double* rhs, const double* un, double* const* k, double* u_out,
                      const BtStage& w, int block0, int nblk, cudaStream_t st);
+// Ghost exchange of a 22-variable register: src (pre-exchange) -> dst (all
+// vertices); src and dst must differ.
 void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst,
-                     int nvar, const int* nbr, int fuse_alg, cudaStream_t st);
+                     const int* nbr, int fuse_alg, cudaStream_t st);
 void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st);
 void launch_alg_constr(const Grid& g, const DevParams& P, double* u, int block0, int nblk,
                        cudaStream_t st, int ghosts_only = 0);

@@ -8,8 +8,9 @@
 // device-wide synchronisation that cudaMalloc/cudaFree bring.  z4c_rhs needs a
 // context, and a context allocates its registers and scratch.  This entry
 // point takes the state and the output as plain device pointers and keeps the
-// scratch of the right-hand-side passes (the Ricci sums and the advection
-// sums) in a fixed array compiled into the library.
+// scratch of the right-hand-side passes (the stored first derivatives, the
+// Ricci sums and the advection sums) in a fixed array compiled into the
+// library.
 //
 // The array: kScratchBytes = 64 MiB, a file-scope __device__ array.  Every GPU
 // that loads the library holds it until the process exits.  All calls share
@@ -103,8 +104,9 @@ extern "C" int z4c_rhs_noalloc(const double* u, double* rhs, int nblocks, const 
   g.s[2] = (int64_t)g.nn[0] * g.nn[1];
   g.nvol = (int64_t)g.nn[0] * g.nn[1] * g.nn[2];
   const int64_t npts = interior_count(g);
-  // scratch per block: 6 Ricci sums + 22 advection sums per interior vertex
-  const size_t per_block = sizeof(double) * 28 * (size_t)npts;
+  // scratch per block: 33 stored first derivatives per vertex, 6 Ricci sums
+  // and 22 advection sums per interior vertex
+  const size_t per_block = sizeof(double) * (kSdComponents * (size_t)g.nvol + 28 * (size_t)npts);
   const size_t room = kScratchBytes - kFdBytes;
   if (per_block > room) {
     char buf[256];
@@ -123,7 +125,8 @@ extern "C" int z4c_rhs_noalloc(const double* u, double* rhs, int nblocks, const 
   if (rc) return rc;
   FdScale* fd = reinterpret_cast<FdScale*>(base);
   RhsScratch sc;
-  sc.rsum = base + kFdBytes / sizeof(double);
+  sc.sd = base + kFdBytes / sizeof(double);
+  sc.rsum = sc.sd + (size_t)kSdComponents * g.nvol * chunk;
   sc.lv = sc.rsum + (size_t)6 * npts * chunk;
 
   // FD scalings of finite_differencing.tpp:20-56, as z4c_create computes them

@@ -3,6 +3,13 @@
 // (z4c/adm_z4c.cpp:972-1037) evaluated in place from the state, constant-eta
 // branch, vacuum (matter terms vanish), Kreiss-Oliger dissipation included.
 //
+// The first derivatives that the reference stores in PrepareZ4cDerivatives
+// (chi, g~_ab, alpha, beta^a along every direction, on the interior extended
+// by 3 vertices across) are computed by a separate pass into the `sd`
+// scratch, exactly as the reference computes them; the passes below read
+// them there, both as first derivatives and as the inputs of the mixed
+// second derivatives (Dx_a of the stored Dx_b, Q1 of the reference).
+//
 // The work per vertex is split in two passes so that each keeps its live
 // values in registers:
 //   ricci_point  the Ricci tensor of the conformal metric and its
@@ -26,26 +33,45 @@ namespace z4c {
 __device__ __forceinline__ int pair_a(int q) { return q < 3 ? 0 : (q < 5 ? 1 : 2); }
 __device__ __forceinline__ int pair_b(int q) { return q < 3 ? q : (q < 5 ? q - 2 : 2); }
 
-// Second derivative of f along the pair q: Dxx on the diagonal, otherwise Dx
-// along the first index of the stored Dx along the second (a < b).
-__device__ __forceinline__ double fd_d2(const double* __restrict__ f, int q, const int64_t s[3],
-                                        const FdScale& F) {
-  const int a = pair_a(q), b = pair_b(q);
-  if (a == b) return fd_dxx(f, s[a], F.cidx2[a]);
-  return fd_dxy(f, s[a], s[b], F.cidx1[a], F.cidx1[b]);
+// Slots of the fields with stored first derivatives; component
+// slot*3 + direction of the sd scratch ([block][33][vertex]).
+constexpr int kSdChi = 0, kSdG = 1, kSdAlpha = 7, kSdBeta = 8, kSdFields = 11;
+__host__ __device__ __forceinline__ constexpr int sd_field_var(int slot) {
+  return slot == 0 ? Z4C_CHI : (slot <= 6 ? Z4C_GXX + slot - 1 : (slot == 7 ? Z4C_ALPHA
+                                                                        : Z4C_BETAX + slot - 8));
 }
 
-// The heavy derivative gathers below run as rolled loops (#pragma unroll 1)
+// Second derivative of f along the pair q: Dxx on the diagonal, otherwise Dx
+// along the first index of the stored Dx along the second (a < b); sdf points
+// at the three stored first derivatives of f (stride nvol).
+__device__ __forceinline__ double fd_d2(const double* __restrict__ f,
+                                        const double* __restrict__ sdf, int64_t nvol, int q,
+                                        const int64_t s[3], const FdScale& F) {
+  const int a = pair_a(q), b = pair_b(q);
+  if (a == b) return fd_dxx(f, s[a], F.cidx2[a]);
+  return fd_dx(sdf + b * nvol, s[a], F.cidx1[a]);
+}
+#define SDF(slot) (SD + (int64_t)(slot) * 3 * nvol)
+#define SDV(slot, dir) __ldg(SD + ((int64_t)(slot) * 3 + (dir)) * nvol)
+
+// The heavy derivative gathers below run as rolled loops (GATHER_LOOP)
 // writing small per-thread arrays; the tensor algebra that consumes them is
 // fully unrolled.  Unrolled gathers let the compiler hoist hundreds of
 // stencil loads at once and spill.
+#ifndef Z4C_ROLLED_GATHERS
+#define Z4C_ROLLED_GATHERS 0
+#endif
+#if Z4C_ROLLED_GATHERS
+#define GATHER_LOOP _Pragma("unroll 1")
+#else
+#define GATHER_LOOP _Pragma("unroll")
+#endif
 #define GDD(a, b) g_dd[sidx(a, b)]
 #define ADD(a, b) A_dd[sidx(a, b)]
 
 // Inverse conformal metric (:295-311) and Christoffel symbols (:317-352).
 // Gamma_ddd is written only when the caller passes storage for it.
-__device__ __forceinline__ void christoffel(const double* __restrict__ U, int64_t nvol,
-                                            const int64_t s[3], const FdScale& F,
+__device__ __forceinline__ void christoffel(const double* __restrict__ SD, int64_t nvol,
                                             const double g_dd[6], double g_uu[6],
                                             double Gamma_ddd[3][6], double Gamma_udd[3][6],
                                             double Gamma_u[3]) {
@@ -56,12 +82,10 @@ __device__ __forceinline__ void christoffel(const double* __restrict__ U, int64_
   double Gd[3][6];
   {
     double dg[3][6];  // [c][ab] = d_c g_ab (stored dg_ddd_3d)
-#pragma unroll 1
-    for (int q = 0; q < 6; ++q) {
-      const double* f = UV(Z4C_GXX + q);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) dg[c][q] = fd_dx(f, s[c], F.cidx1[c]);
-    }
+    for (int q = 0; q < 6; ++q)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) dg[c][q] = SDV(kSdG + q, c);
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -100,24 +124,26 @@ __device__ __forceinline__ void christoffel(const double* __restrict__ U, int64_
 }
 
 // Rsum_ab = R_ab + Rphi_ab at one interior vertex (:357-458).
-__device__ __forceinline__ void ricci_point(const double* __restrict__ u, int64_t nvol,
+__device__ __forceinline__ void ricci_point(const double* __restrict__ u,
+                                            const double* __restrict__ sd, int64_t nvol,
                                             int64_t p, const int64_t s[3],
                                             const DevParams& P, const FdScale& F,
                                             double Rsum[6]) {
   const z4c_params_t& opt = P.p;
   const double* U = u + p;
+  const double* SD = sd + p;
   double g_dd[6];
 #pragma unroll
   for (int c = 0; c < 6; ++c) g_dd[c] = __ldg(UV(Z4C_GXX + c));
   double g_uu[6], Gamma_ddd[3][6], Gamma_udd[3][6], Gamma_u[3];
-  christoffel(U, nvol, s, F, g_dd, g_uu, Gamma_ddd, Gamma_udd, Gamma_u);
+  christoffel(SD, nvol, g_dd, g_uu, Gamma_ddd, Gamma_udd, Gamma_u);
 #define GDDD(c, a, b) Gamma_ddd[c][sidx(a, b)]
 #define GUDD(c, a, b) Gamma_udd[c][sidx(a, b)]
 
   // Ricci tensor of the conformal metric, :357-396; each R_ab accumulates
   // its three groups of terms in the reference's order
   double dGam[3][3];  // [b][c] = d_b Gamma^c
-#pragma unroll 1
+GATHER_LOOP
   for (int c = 0; c < 3; ++c) {
     const double* f = UV(Z4C_GAMX + c);
 #pragma unroll
@@ -136,15 +162,16 @@ __device__ __forceinline__ void ricci_point(const double* __restrict__ u, int64_
       R_dd[sidx(a, b)] = sacc;
     }
   // ddg_dddd(c,d,a,b): second derivative along c,d of g_ab, :158-178
-#pragma unroll 1
+GATHER_LOOP
   for (int q = 0; q < 6; ++q) {
     const double* f = UV(Z4C_GXX + q);
+    const double* sdf = SDF(kSdG + q);
     double sacc = R_dd[q];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int d = c; d < 3; ++d)
-        sacc -= ((c == d) ? 0.5 : 1.0) * GUU(c, d) * fd_d2(f, sidx(c, d), s, F);
+        sacc -= ((c == d) ? 0.5 : 1.0) * GUU(c, d) * fd_d2(f, sdf, nvol, sidx(c, d), s, F);
     R_dd[q] = sacc;
   }
 #pragma unroll
@@ -170,11 +197,10 @@ __device__ __forceinline__ void ricci_point(const double* __restrict__ u, int64_
   const double oochi_psi_power = 1.0 / opt.chi_psi_power;
   double dphi_d[3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a)
-    dphi_d[a] = fd_dx(UV(Z4C_CHI), s[a], F.cidx1[a]) * oochi * oochi_psi_power;
+  for (int a = 0; a < 3; ++a) dphi_d[a] = SDV(kSdChi, a) * oochi * oochi_psi_power;
   double ddchi[6];  // stored ddchi_dd_3d
-#pragma unroll 1
-  for (int q = 0; q < 6; ++q) ddchi[q] = fd_d2(UV(Z4C_CHI), q, s, F);
+GATHER_LOOP
+  for (int q = 0; q < 6; ++q) ddchi[q] = fd_d2(UV(Z4C_CHI), SDF(kSdChi), nvol, q, s, F);
   double Ddphi_dd[6];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
@@ -205,35 +231,17 @@ __device__ __forceinline__ void ricci_point(const double* __restrict__ u, int64_
 #undef GUDD
 }
 
-// Sum over the three directions, in order, of the lop-sided advection
-// operator of variable n (:184-226).
-__device__ __forceinline__ double advect_point(const double* __restrict__ U, int64_t nvol, int n,
-                                               const int64_t s[3], const FdScale& F,
-                                               const double beta_u[3]) {
-  double acc = 0;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) acc += fd_lx(load9(UV(n), s[a]), beta_u[a], F.lidx[a]);
-  return acc;
-}
-
-// Kreiss-Oliger dissipation added to one right-hand-side value in the
-// reference's order, rhs += Diss_x; rhs += Diss_y; rhs += Diss_z (:908-915).
-__device__ __forceinline__ double add_ko(double r, const double* __restrict__ Un,
-                                        const int64_t s[3], const FdScale& F, double diss) {
-#pragma unroll
-  for (int a = 0; a < 3; ++a) r += fd_diss(load9(Un, s[a]), F.cidxd[a], diss);
-  return r;
-}
-
 // The 22 right-hand-side values at one interior vertex without the
 // Kreiss-Oliger terms, given Rsum_ab and the advection sums Lv.
-__device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t nvol,
+__device__ __forceinline__ void rhs_point(const double* __restrict__ u,
+                                          const double* __restrict__ sd, int64_t nvol,
                                           int64_t p, const int64_t s[3],
                                           const DevParams& P, const FdScale& F,
                                           const double Rsum[6], const double Lv[NVAR],
                                           double out[NVAR]) {
   const z4c_params_t& opt = P.p;
   const double* U = u + p;
+  const double* SD = sd + p;
   double g_dd[6], A_dd[6];
 #pragma unroll
   for (int c = 0; c < 6; ++c) {
@@ -244,7 +252,7 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
   const double Theta = __ldg(UV(Z4C_THETA)), alpha = __ldg(UV(Z4C_ALPHA));
 
   double g_uu[6], Gamma_udd[3][6], Gamma_u[3];
-  christoffel(U, nvol, s, F, g_dd, g_uu, nullptr, Gamma_udd, Gamma_u);
+  christoffel(SD, nvol, g_dd, g_uu, nullptr, Gamma_udd, Gamma_u);
 #define GUDD(c, a, b) Gamma_udd[c][sidx(a, b)]
 
   // :231-274
@@ -258,9 +266,9 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
   double dchi_d[3], dphi_d[3], dalpha_d[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    dchi_d[a] = fd_dx(UV(Z4C_CHI), s[a], F.cidx1[a]);
+    dchi_d[a] = SDV(kSdChi, a);
     dphi_d[a] = dchi_d[a] * oochi * oochi_psi_power;
-    dalpha_d[a] = fd_dx(UV(Z4C_ALPHA), s[a], F.cidx1[a]);
+    dalpha_d[a] = SDV(kSdAlpha, a);
   }
 
   // D D alpha, :482-521
@@ -270,8 +278,8 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
 #pragma unroll
     for (int d = 0; d < 3; ++d) Ddalpha += GUU(c, d) * dphi_d[c] * dalpha_d[d];
   double ddalpha[6];
-#pragma unroll 1
-  for (int q = 0; q < 6; ++q) ddalpha[q] = fd_d2(UV(Z4C_ALPHA), q, s, F);
+GATHER_LOOP
+  for (int q = 0; q < 6; ++q) ddalpha[q] = fd_d2(UV(Z4C_ALPHA), SDF(kSdAlpha), nvol, q, s, F);
   double Ddalpha_dd[6];
 #pragma unroll
   for (int a = 0; a < 3; ++a)
@@ -376,21 +384,19 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
 
   // finalize Lie derivatives, :619-687
   double dbeta_du[3][3];  // [b][a] = d_b beta^a
-#pragma unroll 1
-  for (int a = 0; a < 3; ++a) {
-    const double* f = UV(Z4C_BETAX + a);
 #pragma unroll
-    for (int b = 0; b < 3; ++b) dbeta_du[b][a] = fd_dx(f, s[b], F.cidx1[b]);
-  }
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) dbeta_du[b][a] = SDV(kSdBeta + a, b);
   double dbeta = 0;
 #pragma unroll
   for (int a = 0; a < 3; ++a) dbeta += dbeta_du[a][a];
   // ddbeta_ddu(a,b,c): second derivative along a,b of beta^c, :138-156
   double ddbeta[3][6];  // [c][pair(a,b)]
-#pragma unroll 1
+GATHER_LOOP
   for (int i = 0; i < 18; ++i) {
     const int c = i / 6, q = i % 6;
-    ddbeta[c][q] = fd_d2(UV(Z4C_BETAX + c), q, s, F);
+    ddbeta[c][q] = fd_d2(UV(Z4C_BETAX + c), SDF(kSdBeta + c), nvol, q, s, F);
   }
   double ddbeta_d[3] = {0, 0, 0};
 #pragma unroll
@@ -472,6 +478,8 @@ __device__ __forceinline__ void rhs_point(const double* __restrict__ u, int64_t 
 }
 
 #undef UV
+#undef SDF
+#undef SDV
 #undef GUU
 #undef GDD
 #undef ADD

@@ -254,8 +254,9 @@ int z4c_check_finite(z4c_ctx *ctx, int reg);
  * looks the array's device address up (cudaGetSymbolAddress) with that device
  * current; make that first call before any stream capture.  Blocks are
  * processed in chunks that fit the array; a MeshBlock whose scratch alone
- * (224 bytes per interior vertex) exceeds it -- above roughly 64^3 cells --
- * is rejected with Z4C_EINVAL before any work is enqueued.  Every call shares
+ * (33 doubles per vertex, ghosts included, plus 28 per interior vertex)
+ * exceeds it -- above roughly 45^3 cells -- is rejected with Z4C_EINVAL
+ * before any work is enqueued.  Every call shares
  * the array and it keeps the previous call's contents (nothing in it needs to
  * start at zero); calls whose work overlaps on the GPU race on it, so
  * serialise them (one stream, or events between streams).  No cudaMalloc,

@@ -49,8 +49,9 @@ def test_noalloc_rhs_matches_context_rhs_on_two_calls():
     from z4c_b200 import initial_data as ID
     params = Z.default_params(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02,
                               shift_eta=2.0, r_max_con=1e300)
-    # 8 blocks of 40^3 cells: 41^3 interior vertices x 224 B = 15.4 MB of
-    # scratch per block, so the 64 MiB array takes 4 blocks per chunk
+    # 8 blocks of 40^3 cells: 46.5 MB of scratch per block (33 doubles per
+    # vertex, 28 per interior vertex), so the 64 MiB array takes one block
+    # per chunk
     mesh = Z.Mesh((2, 2, 2), (40, 40, 40), (-8.0,) * 3, (8.0,) * 3, "outflow")
     ctx = Z.Z4c(mesh, params, "rk4")
     # one stream for the context and the allocation-free call, so that the
