@@ -112,6 +112,7 @@ struct z4c_ctx {
   double* lv = nullptr;   // advection sums, 22 values per interior vertex
   double* xf = nullptr;   // [nblocks][nn0+nn1+nn2]
   double* xv = nullptr;   // [nblocks][nn0+nn1+nn2-3]
+  double* dxd = nullptr;  // [nblocks][3] vertex spacing
   FdScale* fd = nullptr;  // [nblocks]
   int* nbr = nullptr;     // [nblocks][26]
   double* partials = nullptr;
@@ -134,6 +135,8 @@ struct z4c_ctx {
     DevParams P;
     P.p = params;
     P.fd = fd;
+    P.xf = xf;
+    P.dx = dxd;
     return P;
   }
 };
@@ -219,6 +222,7 @@ int run_stage(z4c_ctx* c, int stage, double dt) {
     const double w2[3] = {wt[1], wt[2], wt[3]};
     for (int b = 0; b < g.nblocks; ++b) {
       launch_rhs(g, P, u, c->scratch(), c->reg[Z4C_REG_RHS], b, 1, c->stream);
+      launch_boundary_rhs(g, P, u, c->reg[Z4C_REG_RHS], b, 1, c->stream);
       launch_weighted_ave(g, c->reg[Z4C_REG_U1], u, nullptr, w1, b, 1, c->stream);
       launch_weighted_ave(g, u, c->reg[Z4C_REG_U1], nullptr, w2, b, 1, c->stream);
       launch_add_rhs(g, c->reg[Z4C_REG_RHS], wt[4] * dt, u, b, 1, c->stream);
@@ -274,7 +278,7 @@ void free_ctx(z4c_ctx* c) {
   if (c->graph) cudaGraphExecDestroy(c->graph);
   for (auto& r : c->reg)
     if (r) cudaFree(r);
-  for (void* p : {(void*)c->un, (void*)c->guu, (void*)c->sd, (void*)c->rsum, (void*)c->lv, (void*)c->xf, (void*)c->xv, (void*)c->fd,
+  for (void* p : {(void*)c->un, (void*)c->guu, (void*)c->sd, (void*)c->rsum, (void*)c->lv, (void*)c->xf, (void*)c->xv, (void*)c->dxd, (void*)c->fd,
                   (void*)c->nbr, (void*)c->partials, (void*)c->flag})
     if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -323,8 +327,10 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
       return fail(Z4C_EINVAL, "nx[%d] = %d below 2*ng = %d", a, mesh->nx[a], 2 * Z4C_NG);
     if (!(mesh->xmax[a] > mesh->xmin[a])) return fail(Z4C_EINVAL, "empty extent on axis %d", a);
     const int lo = mesh->bc[2 * a], hi = mesh->bc[2 * a + 1];
-    if ((lo != Z4C_BC_PERIODIC && lo != Z4C_BC_OUTFLOW) ||
-        (hi != Z4C_BC_PERIODIC && hi != Z4C_BC_OUTFLOW))
+    auto known = [](int f) {
+      return f == Z4C_BC_PERIODIC || f == Z4C_BC_OUTFLOW || f == Z4C_BC_SOMMERFELD;
+    };
+    if (!known(lo) || !known(hi))
       return fail(Z4C_EINVAL, "unknown boundary flag on axis %d", a);
     if ((lo == Z4C_BC_PERIODIC) != (hi == Z4C_BC_PERIODIC))
       return fail(Z4C_EINVAL, "axis %d: periodic on one face only", a);
@@ -352,7 +358,8 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
   }
   for (int f = 0; f < 6; ++f) {
     g.bc[f] = mesh->bc[f];
-    if (g.bc[f] == Z4C_BC_OUTFLOW) c->has_outflow = true;
+    if (g.bc[f] != Z4C_BC_PERIODIC) c->has_outflow = true;
+    if (g.bc[f] == Z4C_BC_SOMMERFELD) g.has_sommerfeld = 1;
   }
   g.s[0] = 1;
   g.s[1] = g.nn[0];
@@ -441,6 +448,7 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
     rc = alloc((void**)&c->lv, sizeof(double) * Z4C_NVAR * (size_t)interior_count(g) * nb);
   if (rc == Z4C_OK) rc = alloc((void**)&c->xf, sizeof(double) * c->h_xf.size());
   if (rc == Z4C_OK) rc = alloc((void**)&c->xv, sizeof(double) * c->h_xv.size());
+  if (rc == Z4C_OK) rc = alloc((void**)&c->dxd, sizeof(double) * c->h_dx.size());
   if (rc == Z4C_OK) rc = alloc((void**)&c->fd, sizeof(FdScale) * nb);
   if (rc == Z4C_OK) rc = alloc((void**)&c->nbr, sizeof(int) * hnbr.size());
   if (rc == Z4C_OK) rc = alloc((void**)&c->partials, sizeof(double) * 8 * nb);
@@ -451,6 +459,7 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
   }
   if (cudaMemcpy(c->xf, c->h_xf.data(), sizeof(double) * c->h_xf.size(), cudaMemcpyHostToDevice) ||
       cudaMemcpy(c->xv, c->h_xv.data(), sizeof(double) * c->h_xv.size(), cudaMemcpyHostToDevice) ||
+      cudaMemcpy(c->dxd, c->h_dx.data(), sizeof(double) * c->h_dx.size(), cudaMemcpyHostToDevice) ||
       cudaMemcpy(c->fd, hfd.data(), sizeof(FdScale) * nb, cudaMemcpyHostToDevice) ||
       cudaMemcpy(c->nbr, hnbr.data(), sizeof(int) * hnbr.size(), cudaMemcpyHostToDevice)) {
     free_ctx(c);
@@ -570,6 +579,18 @@ int z4c_rhs(z4c_ctx* ctx, int reg_u, int reg_rhs, int block) {
   launch_rhs(ctx->g, ctx->dev(), ctx->reg[reg_u], ctx->scratch(), ctx->reg[reg_rhs], b0, nb,
              ctx->stream);
   LAUNCH_CHECK("rhs");
+  return Z4C_OK;
+}
+
+int z4c_boundary_rhs(z4c_ctx* ctx, int reg_u, int reg_rhs, int block) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  int rc, b0, nb;
+  if ((rc = check_reg(ctx, reg_u)) || (rc = check_reg(ctx, reg_rhs))) return rc;
+  if (reg_nvar_(reg_u) != Z4C_NVAR || reg_nvar_(reg_rhs) != Z4C_NVAR || reg_u == reg_rhs)
+    return fail(Z4C_EINVAL, "z4c_boundary_rhs needs two distinct 22-variable registers");
+  if ((rc = check_block(ctx, block, &b0, &nb))) return rc;
+  launch_boundary_rhs(ctx->g, ctx->dev(), ctx->reg[reg_u], ctx->reg[reg_rhs], b0, nb, ctx->stream);
+  LAUNCH_CHECK("boundary_rhs");
   return Z4C_OK;
 }
 

@@ -32,6 +32,8 @@ struct FdScale {
 struct DevParams {
   z4c_params_t p;
   const FdScale* fd;  // [nblocks]
+  const double* xf;   // [nblocks][nn0+nn1+nn2] vertex coordinates (Sommerfeld faces)
+  const double* dx;   // [nblocks][3] vertex spacing (Sommerfeld faces)
 };
 
 // Geometry of the uniform block grid.
@@ -43,6 +45,7 @@ struct Grid {
   int64_t nvol;     // vertices per block
   int nblocks;
   int bc[6];
+  int has_sommerfeld;  // some face is Z4C_BC_SOMMERFELD
 };
 
 // ---- stencils -----------------------------------------------------------

@@ -27,6 +27,12 @@ namespace {
 #define Z4C_MAIN_MINB 1
 #endif
 constexpr int kRhsThreads = Z4C_RHS_THREADS;
+// Unroll factor of the k loops of the column passes (loads of several k in
+// flight per thread).
+#ifndef Z4C_KUNROLL
+#define Z4C_KUNROLL 4
+#endif
+constexpr int kKUnroll = Z4C_KUNROLL;
 constexpr int kPointThreads = 256;
 
 inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
@@ -79,6 +85,7 @@ k_prep(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ s
     double w0 = __ldg(f + (k0 - 3) * sk), w1 = __ldg(f + (k0 - 2) * sk),
            w2 = __ldg(f + (k0 - 1) * sk), w3 = __ldg(f + k0 * sk),
            w4 = __ldg(f + (k0 + 1) * sk), w5 = __ldg(f + (k0 + 2) * sk);
+#pragma unroll kKUnroll
     for (int k = k0; k <= k1; ++k) {
       const double w6 = __ldg(f + (k + 3) * sk);
       out[k * sk] = fd_dx7(w0, w1, w2, w4, w5, w6, cz);
@@ -87,6 +94,7 @@ k_prep(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ s
   } else {
     const int st = (dir == 0) ? 1 : nn0;
     const double ca = (dir == 0) ? F.cidx1[0] : F.cidx1[1];
+#pragma unroll kKUnroll
     for (int k = k0; k <= k1; ++k) out[k * sk] = fd_dx(f + k * sk, st, ca);
   }
 }
@@ -211,6 +219,75 @@ __device__ __forceinline__ double fd_diss_window(const double w[9], double cidxd
   return out * cidxd * diss;
 }
 
+// ---- Sommerfeld boundary right-hand side (Z4c::Z4cBoundaryRHS) -----------
+// z4c/boundary_conditions.cpp:16-174.  On a gr_sommerfeld face's vertex
+// plane the right-hand side of Theta, Khat, Gamma^a and A_ab is replaced by
+//   rhs = -c u / r - sum_a c s^a Ds_a(u),  s^a = x^a / r,  c = sqrt(2) for
+// Khat and 1 otherwise, with the second-order Ds (finite_differencing.tpp:
+// 132-150, DBG_SYMMETRIZE_FD branch).  The value depends only on the vertex
+// and the variable, so a vertex on several Sommerfeld faces gets it once.
+__device__ __forceinline__ bool sommerfeld_var(int n) {
+  return n == Z4C_KHAT || n == Z4C_THETA || (n >= Z4C_AXX && n <= Z4C_GAMZ);
+}
+// Whether vertex (i, j, k) of block b lies on one of its gr_sommerfeld faces.
+__device__ __forceinline__ bool on_sommerfeld_face(const Grid& g, int b, int i, int j, int k) {
+  const int l0 = b % g.nb[0], l1 = (b / g.nb[0]) % g.nb[1], l2 = b / (g.nb[0] * g.nb[1]);
+  return (g.bc[0] == Z4C_BC_SOMMERFELD && l0 == 0 && i == NG) ||
+         (g.bc[1] == Z4C_BC_SOMMERFELD && l0 == g.nb[0] - 1 && i == NG + g.nx[0]) ||
+         (g.bc[2] == Z4C_BC_SOMMERFELD && l1 == 0 && j == NG) ||
+         (g.bc[3] == Z4C_BC_SOMMERFELD && l1 == g.nb[1] - 1 && j == NG + g.nx[1]) ||
+         (g.bc[4] == Z4C_BC_SOMMERFELD && l2 == 0 && k == NG) ||
+         (g.bc[5] == Z4C_BC_SOMMERFELD && l2 == g.nb[2] - 1 && k == NG + g.nx[2]);
+}
+__device__ __forceinline__ double fd_ds(const double* __restrict__ f, int64_t st, double dx) {
+  double out = 0.;
+  out += -1. * (__ldg(f - st) - __ldg(f + st));
+  return out * (1.0 / (dx * 2));
+}
+// Sommerfeld value of variable n at vertex (i, j, k) of block b; f points at
+// that variable's value there.
+__device__ __forceinline__ double sommerfeld_value(const Grid& g, const DevParams& P, int b,
+                                                  int n, const double* __restrict__ f, int i,
+                                                  int j, int k) {
+  const double* x = P.xf + (int64_t)b * (g.nn[0] + g.nn[1] + g.nn[2]);
+  const double x1 = x[i], x2 = x[g.nn[0] + j], x3 = x[g.nn[0] + g.nn[1] + k];
+  double d[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) d[a] = fd_ds(f, g.s[a], P.dx[(int64_t)b * 3 + a]);
+  const double r = sqrt(x1 * x1 + x2 * x2 + x3 * x3);
+  const double s_u[3] = {x1 / r, x2 / r, x3 / r};
+  const double sqrt2 = sqrt(2.);
+  double v;
+  if (n == Z4C_KHAT) {
+    v = -sqrt2 * __ldg(f) / r;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) v -= sqrt2 * s_u[a] * d[a];
+  } else {
+    v = -__ldg(f) / r;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) v -= s_u[a] * d[a];
+  }
+  return v;
+}
+
+// Z4c::Z4cBoundaryRHS on its own: one thread per (block, interior vertex,
+// Sommerfeld variable); rhs is overwritten where the vertex lies on a
+// gr_sommerfeld face.
+__global__ void __launch_bounds__(kPointThreads)
+k_sommerfeld(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ rhs,
+             int block0, int nblk) {
+  const int n0 = g.nx[0] + 1, n1 = g.nx[1] + 1, per = n0 * n1 * (g.nx[2] + 1);
+  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (t >= per * 11 * nblk) return;
+  const int l = t % per, rest = t / per;
+  const int v = rest % 11, b = block0 + rest / 11;
+  const int n = (v < 2) ? (v == 0 ? Z4C_KHAT : Z4C_THETA) : Z4C_AXX + (v - 2);  // A, Gamma
+  const int i = NG + l % n0, j = NG + (l / n0) % n1, k = NG + l / (n0 * n1);
+  if (!on_sommerfeld_face(g, b, i, j, k)) return;
+  const int64_t q = ((int64_t)b * NVAR + n) * g.nvol + ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  rhs[q] = sommerfeld_value(g, P, b, n, u + q, i, j, k);
+}
+
 // Fills the z window of column c at the first interior k.
 __device__ __forceinline__ void window_init(const double* __restrict__ f, int sk, int k0,
                                             double w[9]) {
@@ -244,6 +321,7 @@ k_adv(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ lv
   const FdScale& F = P.fd[c.b];
   double w[9];
   window_init(f, sk, NG, w);
+#pragma unroll kKUnroll
   for (int k = NG; k <= NG + g.nx[2]; ++k) {
     window_advance(f, sk, k, w);
     const int o = k * sk;
@@ -279,6 +357,7 @@ k_ko_rhs(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__
   const FdScale& F = P.fd[c.b];
   double w[9];
   window_init(f, sk, NG, w);
+#pragma unroll kKUnroll
   for (int k = NG; k <= NG + g.nx[2]; ++k) {
     window_advance(f, sk, k, w);
     const int o = k * sk;
@@ -288,10 +367,13 @@ k_ko_rhs(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__
 }
 
 // ---- KO + low-storage RK stage ----------------------------------------------
+// The right-hand side used is Z4cRHS (main pass + KO) followed by
+// Z4cBoundaryRHS, as CALC_Z4CRHS runs them (task_list_gr_z4c.cpp:142-166).
 // IntegrateZ4c for 2S integrators (task_list_gr_z4c.cpp:176-195):
 //   WeightedAve(u1, u, u2, {1, delta, 0}); WeightedAve(u, u1, u2, {g1, g2, g3});
 //   AddZ4cRHS(rhs, beta*dt, u)        (mesh/weighted_ave.cpp:20-150)
 // u is read (all points, for the stencils); u_out, u1 are written (interior).
+template <bool SOM>
 __global__ void __launch_bounds__(kPointThreads)
 k_ko_stage_ls(Grid g, DevParams P, const double* __restrict__ u,
               const double* __restrict__ rhs, double* __restrict__ u1,
@@ -302,13 +384,18 @@ k_ko_stage_ls(Grid g, DevParams P, const double* __restrict__ u,
   const int64_t base = ((int64_t)c.b * NVAR + c.n) * g.nvol + c.j * nn0 + c.i;
   const double* f = u + base;
   const FdScale& F = P.fd[c.b];
+  // Z4cBoundaryRHS replaces this variable's right-hand side on Sommerfeld faces
+  const bool som = SOM && sommerfeld_var(c.n);
   double win[9];
   window_init(f, sk, NG, win);
+#pragma unroll kKUnroll
   for (int k = NG; k <= NG + g.nx[2]; ++k) {
     window_advance(f, sk, k, win);
     const int o = k * sk;
     const int64_t q = base + o;
-    const double r = add_ko_column(__ldg(rhs + q), f + o, nn0, win, F, P.p.diss);
+    const double r = (som && on_sommerfeld_face(g, c.b, c.i, c.j, k))
+                         ? sommerfeld_value(g, P, c.b, c.n, f + o, c.i, c.j, k)
+                         : add_ko_column(__ldg(rhs + q), f + o, nn0, win, F, P.p.diss);
     const double un = win[4];
     double v1 = w.u1_zero ? 0.0 : u1[q];
     if (w.delta != 0.0) v1 += w.delta * un;  // w0 == 1, w2 == 0 branch
@@ -335,6 +422,7 @@ k_ko_stage_ls(Grid g, DevParams P, const double* __restrict__ u,
 struct KPtrs {
   double* k[4];
 };
+template <bool SOM>
 __global__ void __launch_bounds__(kPointThreads)
 k_ko_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ rhs,
               const double* __restrict__ un, KPtrs K, double* __restrict__ u_out, BtStage w,
@@ -345,13 +433,18 @@ k_ko_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* _
   const int64_t base = ((int64_t)c.b * NVAR + c.n) * g.nvol + c.j * nn0 + c.i;
   const double* f = u + base;
   const FdScale& F = P.fd[c.b];
+  // Z4cBoundaryRHS replaces this variable's right-hand side on Sommerfeld faces
+  const bool som = SOM && sommerfeld_var(c.n);
   double win[9];
   window_init(f, sk, NG, win);
+#pragma unroll kKUnroll
   for (int k = NG; k <= NG + g.nx[2]; ++k) {
     window_advance(f, sk, k, win);
     const int o = k * sk;
     const int64_t q = base + o;
-    const double r = add_ko_column(__ldg(rhs + q), f + o, nn0, win, F, P.p.diss);
+    const double r = (som && on_sommerfeld_face(g, c.b, c.i, c.j, k))
+                         ? sommerfeld_value(g, P, c.b, c.n, f + o, c.i, c.j, k)
+                         : add_ko_column(__ldg(rhs + q), f + o, nn0, win, F, P.p.diss);
     K.k[w.kslot][q] = r;
     double v = __ldg(un + q);
     for (int s = 0; s < w.nq; ++s) {
@@ -527,7 +620,8 @@ k_exchange_ghosts(Grid g, double* __restrict__ u, const int* __restrict__ nbr) {
 }
 
 // ---- extrapolate_outflow boundary conditions --------------------------------
-// ExtrapolateOutflowBC with NEXTRAPOLATE = 5 (comm/physical_bcs.cpp:187-260)
+// ExtrapolateOutflowBC with NEXTRAPOLATE = 5 (comm/physical_bcs.cpp:187-260),
+// also the ghost fill of gr_sommerfeld faces for vertex-centred data (:445-453)
 // over the ranges of ApplyPhysicalBCs (:506-670): the cell-centred interior
 // end ie = is + nx - 1 bounds the outer faces and the transverse ranges.
 // Only the blocks on the two faces of axis ax are visited.  One thread per
@@ -551,13 +645,13 @@ k_bc_axis(Grid g, double* __restrict__ u, int nvar, int ax) {
   loc[ax] = side ? g.nb[ax] - 1 : 0;
   loc[o1] = fb % g.nb[o1];
   loc[o2] = fb / g.nb[o1];
-  if (g.bc[2 * ax + side] != Z4C_BC_OUTFLOW) return;
+  if (g.bc[2 * ax + side] == Z4C_BC_PERIODIC) return;
   const int b = loc[0] + g.nb[0] * (loc[1] + g.nb[1] * loc[2]);
   bool need[6];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    need[2 * a] = (g.bc[2 * a] == Z4C_BC_OUTFLOW) && loc[a] == 0;
-    need[2 * a + 1] = (g.bc[2 * a + 1] == Z4C_BC_OUTFLOW) && loc[a] == g.nb[a] - 1;
+    need[2 * a] = (g.bc[2 * a] != Z4C_BC_PERIODIC) && loc[a] == 0;
+    need[2 * a + 1] = (g.bc[2 * a + 1] != Z4C_BC_PERIODIC) && loc[a] == g.nb[a] - 1;
   }
   int is[3], ie[3];
 #pragma unroll
@@ -874,8 +968,9 @@ void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, const R
                      int nblk, cudaStream_t st) {
   launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, st);
   COUNTED
-  k_ko_stage_ls<<<div_up(columns(g, nblk), kPointThreads), kPointThreads, 0, st>>>(
-      g, P, u, rhs, u1, u_out, w, block0, nblk);
+  auto kern = g.has_sommerfeld ? k_ko_stage_ls<true> : k_ko_stage_ls<false>;
+  kern<<<div_up(columns(g, nblk), kPointThreads), kPointThreads, 0, st>>>(g, P, u, rhs, u1, u_out,
+                                                                          w, block0, nblk);
 }
 
 void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
@@ -885,8 +980,9 @@ void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const R
   KPtrs K;
   for (int s = 0; s < 4; ++s) K.k[s] = k[s];
   COUNTED
-  k_ko_stage_bt<<<div_up(columns(g, nblk), kPointThreads), kPointThreads, 0, st>>>(
-      g, P, u, rhs, un, K, u_out, w, block0, nblk);
+  auto kern = g.has_sommerfeld ? k_ko_stage_bt<true> : k_ko_stage_bt<false>;
+  kern<<<div_up(columns(g, nblk), kPointThreads), kPointThreads, 0, st>>>(g, P, u, rhs, un, K,
+                                                                          u_out, w, block0, nblk);
 }
 
 // Slot of every direction in the neighbour list (mesh_topology.cpp:329-960
@@ -906,6 +1002,14 @@ static int upload_dir_index() {
   return (int)cudaMemcpyToSymbol(c_dir_index, h, sizeof(h));
 }
 
+void launch_boundary_rhs(const Grid& g, const DevParams& P, const double* u, double* rhs,
+                         int block0, int nblk, cudaStream_t st) {
+  if (!g.has_sommerfeld) return;
+  COUNTED
+  k_sommerfeld<<<div_up(interior_count(g) * 11 * nblk, kPointThreads), kPointThreads, 0, st>>>(
+      g, P, u, rhs, block0, nblk);
+}
+
 void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst,
                      const int* nbr, int fuse_alg, cudaStream_t st) {
   static const int dir_rc = upload_dir_index();  // once per process
@@ -920,10 +1024,10 @@ void launch_exchange(const Grid& g, const DevParams& P, const double* src, doubl
 
 void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st) {
   bool any = false;
-  for (int f = 0; f < 6; ++f) any |= (g.bc[f] == Z4C_BC_OUTFLOW);
+  for (int f = 0; f < 6; ++f) any |= (g.bc[f] != Z4C_BC_PERIODIC);
   if (!any) return;
   for (int ax = 0; ax < 3; ++ax) {
-    if (g.bc[2 * ax] != Z4C_BC_OUTFLOW && g.bc[2 * ax + 1] != Z4C_BC_OUTFLOW) continue;
+    if (g.bc[2 * ax] == Z4C_BC_PERIODIC && g.bc[2 * ax + 1] == Z4C_BC_PERIODIC) continue;
     const int o1 = (ax == 0) ? 1 : 0, o2 = (ax == 2) ? 1 : 2;
     const int64_t n = (int64_t)g.nn[o1] * g.nn[o2] * 2 * nvar * g.nb[o1] * g.nb[o2];
     COUNTED

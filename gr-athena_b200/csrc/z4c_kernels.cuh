@@ -78,6 +78,9 @@ void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const R
                      const BtStage& w, int block0, int nblk, cudaStream_t st);
 // Ghost exchange of a 22-variable register: src (pre-exchange) -> dst (all
 // vertices); src and dst must differ.
+// Z4c::Z4cBoundaryRHS: Sommerfeld right-hand side on gr_sommerfeld faces.
+void launch_boundary_rhs(const Grid& g, const DevParams& P, const double* u, double* rhs,
+                         int block0, int nblk, cudaStream_t st);
 void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst,
                      const int* nbr, int fuse_alg, cudaStream_t st);
 void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st);

@@ -31,7 +31,9 @@ NVAR, NADM, NCON = 22, 17, 7
 CON_C, CON_H, CON_M, CON_Z, CON_MX, CON_MY, CON_MZ = range(7)
 (REG_U, REG_U1, REG_RHS, REG_ADM, REG_CON, REG_W, REG_K1, REG_K2, REG_K3,
  REG_K4) = range(10)
-BC_PERIODIC, BC_OUTFLOW = 0, 1
+BC_PERIODIC, BC_OUTFLOW, BC_SOMMERFELD = 0, 1, 2
+BC_NAMES = {"periodic": BC_PERIODIC, "outflow": BC_OUTFLOW, "extrapolate_outflow": BC_OUTFLOW,
+            "sommerfeld": BC_SOMMERFELD, "gr_sommerfeld": BC_SOMMERFELD}
 INTEG = {"rk4": 0, "bt_rk4": 1}
 ERRORS = {-1: "EINVAL", -2: "ENOMEM", -3: "ECUDA", -4: "ENONFINITE", -5: "ETIMEOUT",
           -6: "ESTATE", -7: "ENODEV"}
@@ -43,7 +45,7 @@ EXPORTS = (
     "z4c_params_default", "z4c_last_error", "z4c_create", "z4c_destroy",
     "z4c_set_stream", "z4c_sync", "z4c_num_blocks", "z4c_block_nn", "z4c_reg_nvar",
     "z4c_dx", "z4c_block_coords", "z4c_mesh_block_coords", "z4c_upload", "z4c_download", "z4c_device_ptr",
-    "z4c_rhs", "z4c_add_rhs", "z4c_weighted_ave", "z4c_alg_constr", "z4c_adm_to_z4c",
+    "z4c_rhs", "z4c_boundary_rhs", "z4c_add_rhs", "z4c_weighted_ave", "z4c_alg_constr", "z4c_adm_to_z4c",
     "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_ghost_fill", "z4c_init_finalize",
     "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
     "z4c_get_tile", "z4c_check_finite", "z4c_kernel_launches", "z4c_rhs_stage",
@@ -104,6 +106,7 @@ def lib():
         L.z4c_download.argtypes = [vp, ip, ip, dp]
         L.z4c_device_ptr.argtypes = [vp, ip, C.POINTER(dp)]
         L.z4c_rhs.argtypes = [vp, ip, ip, ip]
+        L.z4c_boundary_rhs.argtypes = [vp, ip, ip, ip]
         L.z4c_add_rhs.argtypes = [vp, ip, C.c_double, ip, ip]
         L.z4c_weighted_ave.argtypes = [vp, ip, ip, ip, dp, ip]
         L.z4c_alg_constr.argtypes = [vp, ip, ip]
@@ -160,7 +163,7 @@ class Mesh:
         self.xmin = tuple(float(v) for v in xmin)
         self.xmax = tuple(float(v) for v in xmax)
         if isinstance(bc, str):
-            bc = [BC_PERIODIC if bc == "periodic" else BC_OUTFLOW] * 6
+            bc = [BC_NAMES[bc]] * 6
         self.bc = tuple(int(v) for v in bc)
 
     @property
@@ -279,6 +282,9 @@ class Z4c:
     # ---- reference operator names ----
     def Z4cRHS(self, reg_u=REG_U, reg_rhs=REG_RHS, block=-1):
         _check(lib().z4c_rhs(self._h, reg_u, reg_rhs, block))
+
+    def Z4cBoundaryRHS(self, reg_u=REG_U, reg_rhs=REG_RHS, block=-1):
+        _check(lib().z4c_boundary_rhs(self._h, reg_u, reg_rhs, block))
 
     def AddZ4cRHS(self, reg_rhs, wght, reg_out, block=-1):
         _check(lib().z4c_add_rhs(self._h, reg_rhs, float(wght), reg_out, block))

@@ -64,9 +64,13 @@ enum {
 
 /* Physical boundary flags per face (inner_x1, outer_x1, inner_x2, ...). */
 #define Z4C_BC_PERIODIC 0
-/* extrapolate_outflow; gr_sommerfeld maps to the same ghost fill for
- * vertex-centred data (comm/physical_bcs.cpp:445-453). */
+/* extrapolate_outflow: polynomial extrapolation of the ghosts
+ * (comm/physical_bcs.cpp:187-260). */
 #define Z4C_BC_OUTFLOW 1
+/* gr_sommerfeld: the same ghost fill for vertex-centred data
+ * (comm/physical_bcs.cpp:445-453), plus the Sommerfeld right-hand side of
+ * Z4c::Z4cBoundaryRHS on the face's vertex plane (z4c/boundary_conditions.cpp). */
+#define Z4C_BC_SOMMERFELD 2
 
 /* Registers held by a context (one value per variable per vertex per block). */
 enum {
@@ -166,6 +170,12 @@ int z4c_device_ptr(z4c_ctx *ctx, int reg, double **dptr);
  * precompute of Z4c::PrepareZ4cDerivatives (z4c/adm_z4c.cpp:972-1037) fused
  * in.  Writes the interior of reg_rhs. */
 int z4c_rhs(z4c_ctx *ctx, int reg_u, int reg_rhs, int block);
+/* Z4c::Z4cBoundaryRHS (z4c/boundary_conditions.cpp:16-174): on the vertex
+ * planes of gr_sommerfeld faces (Z4C_BC_SOMMERFELD), replaces the right-hand
+ * side of Theta, Khat, Gamma^a and A_ab in reg_rhs by the Sommerfeld
+ * condition evaluated from reg_u.  z4c_stage and z4c_evolve apply it after
+ * z4c_rhs, as the CALC_Z4CRHS task does. */
+int z4c_boundary_rhs(z4c_ctx *ctx, int reg_u, int reg_rhs, int block);
 /* Z4c::AddZ4cRHS (z4c/add_z4c_rhs.cpp:24-35): u_out += wght * rhs, interior. */
 int z4c_add_rhs(z4c_ctx *ctx, int reg_rhs, double wght, int reg_out, int block);
 /* Z4c::WeightedAve (mesh/weighted_ave.cpp:20-167, VC range):

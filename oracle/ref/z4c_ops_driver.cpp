@@ -8,6 +8,7 @@
 //
 //   u0                 state after initialisation (all points)
 //   rhs0               Z4cRHS(u0) after PrepareZ4cDerivatives(u0)
+//   brhs0              rhs0 followed by Z4cBoundaryRHS (Sommerfeld faces)
 //   alg0               AlgConstr applied to a copy of u0
 //   adm0               Z4cToADM(u0)
 //   con0               ADMConstraints(con, adm0, mat, u0)
@@ -130,6 +131,11 @@ int main(int argc, char* argv[]) {
     z->Z4cRHS(z->storage.u, z->storage.mat, tmp[g]);
   }
   d.dump("rhs0", NZ, [&](MeshBlock* b) -> AthenaArray<Real>& { return tmp[b->gid]; });
+  for (size_t g = 0; g < blocks.size(); ++g) {
+    Z4c* z = blocks[g]->pz4c;
+    z->Z4cBoundaryRHS(z->storage.u, z->storage.mat, tmp[g]);
+  }
+  d.dump("brhs0", NZ, [&](MeshBlock* b) -> AthenaArray<Real>& { return tmp[b->gid]; });
 
   for (size_t g = 0; g < blocks.size(); ++g) {
     Z4c* z = blocks[g]->pz4c;

@@ -584,6 +584,70 @@ void orc_rhs(const orc_block_t *b, const z4c_params_t *opt, const double *u,
         }
 }
 
+/* ---- Z4c::Z4cBoundaryRHS, z4c/boundary_conditions.cpp:16-174 ------------ */
+
+/* Uniform::Ds with DBG_SYMMETRIZE_FD (finite_differencing.tpp:132-150):
+ * FDStencilCenteredDegreeOdd<1,1> = {-1} / 2. */
+static inline double Ds(const fd_t *f, int dir, const double *u, double cidx1_lo) {
+  const int64_t s = f->s[dir];
+  double out = 0.;
+  out += -1. * (u[-s] - u[s]);
+  return out * cidx1_lo;
+}
+
+/* Z4c::Z4cSommerfeld_ (:66-174) at one vertex p with coordinates x, y, z. */
+static void sommerfeld_point(const fd_t *f, const double cl[3], const double *u, double *rhs,
+                             int64_t p, double x, double y, double z) {
+  const int64_t nvol = (int64_t)f->nn1 * f->nn2 * f->nn3;
+  double dKhat[3], dTheta[3], dGam[3][3], dA[3][6];
+  for (int a = 0; a < 3; ++a) {
+    dKhat[a] = Ds(f, a, u + Z4C_KHAT * nvol + p, cl[a]);
+    dTheta[a] = Ds(f, a, u + Z4C_THETA * nvol + p, cl[a]);
+  }
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) dGam[b][a] = Ds(f, b, u + (Z4C_GAMX + a) * nvol + p, cl[b]);
+  for (int q = 0; q < 6; ++q)
+    for (int c = 0; c < 3; ++c) dA[c][q] = Ds(f, c, u + (Z4C_AXX + q) * nvol + p, cl[c]);
+  const double r = sqrt(x * x + y * y + z * z);
+  const double s_u[3] = {x / r, y / r, z / r};
+  double th = -u[Z4C_THETA * nvol + p] / r;
+  double kh = -sqrt(2.) * u[Z4C_KHAT * nvol + p] / r;
+  for (int a = 0; a < 3; ++a) {
+    th -= s_u[a] * dTheta[a];
+    kh -= sqrt(2.) * s_u[a] * dKhat[a];
+  }
+  rhs[Z4C_THETA * nvol + p] = th;
+  rhs[Z4C_KHAT * nvol + p] = kh;
+  for (int a = 0; a < 3; ++a) {
+    double v = -u[(Z4C_GAMX + a) * nvol + p] / r;
+    for (int b = 0; b < 3; ++b) v -= s_u[b] * dGam[b][a];
+    rhs[(Z4C_GAMX + a) * nvol + p] = v;
+  }
+  for (int q = 0; q < 6; ++q) {
+    double v = -u[(Z4C_AXX + q) * nvol + p] / r;
+    for (int c = 0; c < 3; ++c) v -= s_u[c] * dA[c][q];
+    rhs[(Z4C_AXX + q) * nvol + p] = v;
+  }
+}
+
+void orc_boundary_rhs(const orc_block_t *b, const double *u, double *rhs, const int som[6]) {
+  fd_t f;
+  fd_init(b, &f);
+  /* cidx1_lo, finite_differencing.tpp:43-45 */
+  const double cl[3] = {1.0 / (b->dx[0] * 2), 1.0 / (b->dx[1] * 2), 1.0 / (b->dx[2] * 2)};
+  for (int face = 0; face < 6; ++face) {
+    if (!som[face]) continue;
+    const int ax = face / 2;
+    int lo[3] = {f.il, f.jl, f.kl}, hi[3] = {f.iu, f.ju, f.ku};
+    if (face % 2 == 0) hi[ax] = lo[ax];
+    else lo[ax] = hi[ax];
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j)
+        for (int i = lo[0]; i <= hi[0]; ++i)
+          sommerfeld_point(&f, cl, u, rhs, P(k, j, i), b->x[0][i], b->x[1][j], b->x[2][k]);
+  }
+}
+
 /* ---- Z4c::AlgConstr, z4c.cpp:677-799 / 801-991 --------------------------- */
 static void algconstr_point(const z4c_params_t *opt, double *u, int64_t nvol,
                             int64_t p) {
@@ -1056,8 +1120,8 @@ void orc_block_physical_bcs(const orc_mesh_t *m, const int loc[3], int nvar, dou
   const int64_t st[3] = {1, nn[0], (int64_t)nn[0] * nn[1]};
   int need[6];
   for (int a = 0; a < 3; ++a) {
-    need[2 * a] = (m->bc[2 * a] == Z4C_BC_OUTFLOW) && loc[a] == 0;
-    need[2 * a + 1] = (m->bc[2 * a + 1] == Z4C_BC_OUTFLOW) && loc[a] == m->nb[a] - 1;
+    need[2 * a] = (m->bc[2 * a] != Z4C_BC_PERIODIC) && loc[a] == 0;
+    need[2 * a + 1] = (m->bc[2 * a + 1] != Z4C_BC_PERIODIC) && loc[a] == m->nb[a] - 1;
   }
   int is[3], ie[3];
   for (int a = 0; a < 3; ++a) { is[a] = NG; ie[a] = NG + m->nx[a] - 1; }

@@ -55,6 +55,11 @@ void orc_prepare_derivs(const orc_block_t *b, const double *u, orc_derivs_t *d);
  * rhs only.  Requires orc_prepare_derivs(u) first. */
 void orc_rhs(const orc_block_t *b, const z4c_params_t *p, const double *u,
              const orc_derivs_t *d, double *rhs);
+/* Z4c::Z4cBoundaryRHS, z4c/boundary_conditions.cpp:16-174: on every face
+ * with som[face] != 0 (inner_x1, outer_x1, inner_x2, ...) the Sommerfeld
+ * right-hand side of Theta, Khat, Gamma^a and A_ab replaces rhs on that
+ * face's vertex plane (the interior vertex range of the other axes). */
+void orc_boundary_rhs(const orc_block_t *b, const double *u, double *rhs, const int som[6]);
 /* Z4c::AlgConstr, z4c.cpp:677-799: all points, in place. */
 void orc_algconstr(const orc_block_t *b, const z4c_params_t *p, double *u);
 /* Z4c::AlgConstr ranged variant with skip_physical, z4c.cpp:801-991:
@@ -79,8 +84,9 @@ void orc_adm_constraints(const orc_block_t *b, const z4c_params_t *p,
 /* ---- uniform block grid (single level) ---------------------------------- */
 
 /* A uniform mesh of nb[0]*nb[1]*nb[2] blocks, block (l0,l1,l2) at index
- * l0 + nb0*(l1 + nb1*l2) of the arrays.  bc[face] = Z4C_BC_PERIODIC or
- * Z4C_BC_OUTFLOW for faces inner_x1, outer_x1, inner_x2, ... */
+ * l0 + nb0*(l1 + nb1*l2) of the arrays.  bc[face] = Z4C_BC_PERIODIC,
+ * Z4C_BC_OUTFLOW or Z4C_BC_SOMMERFELD for faces inner_x1, outer_x1, inner_x2,
+ * ... (the last two fill ghosts alike). */
 typedef struct {
   int nb[3];
   int nx[3];

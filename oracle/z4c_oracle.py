@@ -76,6 +76,7 @@ def lib():
         L.orc_derivs_free.argtypes = [Dp]
         L.orc_prepare_derivs.argtypes = [bp, dp, Dp]
         L.orc_rhs.argtypes = [bp, pp, dp, Dp, dp]
+        L.orc_boundary_rhs.argtypes = [bp, dp, dp, C.POINTER(C.c_int)]
         L.orc_algconstr.argtypes = [bp, pp, dp]
         L.orc_algconstr_ghosts.argtypes = [bp, pp, dp]
         L.orc_z4c_to_adm.argtypes = [bp, pp, dp, dp]
@@ -138,6 +139,24 @@ def rhs(blk, p, u):
     d = _DerivsHolder(blk, u)
     lib().orc_rhs(C.byref(blk._s), C.byref(p), _ptr(u), C.byref(d.d), _ptr(out))
     return out
+
+
+def sommerfeld_faces(nb, bc, block):
+    """Faces (inner_x1, outer_x1, ...) of block `block` of an nb block grid
+    that carry gr_sommerfeld (Z4C_BC_SOMMERFELD = 2)."""
+    loc = (block % nb[0], (block // nb[0]) % nb[1], block // (nb[0] * nb[1]))
+    return [int(bc[2 * a + side] == 2 and loc[a] == (0 if side == 0 else nb[a] - 1))
+            for a in range(3) for side in range(2)]
+
+
+def boundary_rhs(blk, u, rhs, som):
+    """Z4c::Z4cBoundaryRHS on the faces flagged in som, in place on rhs."""
+    if not any(som):
+        return rhs
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    assert rhs.flags.c_contiguous and rhs.dtype == np.float64
+    lib().orc_boundary_rhs(C.byref(blk._s), _ptr(u), _ptr(rhs), (C.c_int * 6)(*som))
+    return rhs
 
 
 def algconstr(blk, p, u, ghosts_only=False):

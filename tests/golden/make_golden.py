@@ -3,7 +3,7 @@ reference CPU build (oracle/ref, built from the reference sources) on small
 cases.  Run from the repository root:
 
     make -C oracle/ref -j8          # needs the reference checkout
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [ops_<case> evol_<case> ...]
 
 Fixtures (numpy .npz, compressed):
   ops_<case>.npz    one Mesh after initialisation ("u0") and the reference's
@@ -54,7 +54,13 @@ CASES = {
     "rs2": dict(test="robust_stability", z4c=PUNCTURE, integ="bt_rk4", bc="periodic",
                 mesh=[(16, -4.0, 4.0, 8), (8, -2.0, 2.0, 8), (8, -2.0, 2.0, 8)],
                 extra={"AwA_amplitude": 1e-10}),
+    # one puncture, two blocks along x, gr_sommerfeld faces (Z4cBoundaryRHS)
+    "somm2": dict(test="one_puncture", z4c=PUNCTURE, integ="rk4", bc="gr_sommerfeld",
+                  mesh=[(16, -4.0, 4.0, 8), (8, -2.0, 2.0, 8), (8, -2.0, 2.0, 8)],
+                  extra={}, problem={"punc_ADM_mass": 1.0}),
 }
+# records every ops fixture keeps when the driver wrote them
+OPS_OPTIONAL = ["brhs0"]
 
 EVOL = {
     # configs[0] gauge wave, one 16^3 block, 40 steps, history every step
@@ -64,7 +70,12 @@ EVOL = {
     "punc4": dict(test="one_puncture", z4c=PUNCTURE, integ="rk4", bc="extrapolate_outflow",
                   mesh=[(16, -4.0, 4.0, 8), (16, -4.0, 4.0, 8), (8, -2.0, 2.0, 8)], extra={},
                   problem={"punc_ADM_mass": 1.0}, nlim=12),
+    # the same puncture with gr_sommerfeld faces, 8 steps
+    "somm4": dict(test="one_puncture", z4c=PUNCTURE, integ="rk4", bc="gr_sommerfeld",
+                  mesh=[(16, -4.0, 4.0, 8), (16, -4.0, 4.0, 8), (8, -2.0, 2.0, 8)], extra={},
+                  problem={"punc_ADM_mass": 1.0}, nlim=8),
 }
+BC_CODES = {"periodic": 0, "extrapolate_outflow": 1, "gr_sommerfeld": 2}
 
 
 def deck(case, out_file, nlim=1, dump_initial="", dump_final="", hst=False):
@@ -97,7 +108,7 @@ def deck(case, out_file, nlim=1, dump_initial="", dump_final="", hst=False):
 def meta_json(case):
     nb = [m[0] // m[3] for m in case["mesh"]]
     nx = [m[3] for m in case["mesh"]]
-    bc = 0 if case["bc"] == "periodic" else 1
+    bc = BC_CODES[case["bc"]]
     mesh = dict(nb=nb, nx=nx, xmin=[m[1] for m in case["mesh"]],
                 xmax=[m[2] for m in case["mesh"]], bc=[bc] * 6)
     return dict(params=json.dumps(case["z4c"]), mesh=json.dumps(mesh),
@@ -114,6 +125,7 @@ def make_ops(name, case, outdir):
                        stdout=subprocess.DEVNULL)
         rec = read_records(rec_path)
     out = {k: rec[k] for k in OPS_KEEP}
+    out.update({k: rec[k] for k in OPS_OPTIONAL if k in rec})
     out.update(meta_json(case))
     path = os.path.join(outdir, f"ops_{name}.npz")
     np.savez_compressed(path, **out)
@@ -151,10 +163,15 @@ def make_evol(name, case, outdir):
 
 
 def main():
+    only = set(sys.argv[1:])  # fixture names to (re)make; all when empty
     for name, case in CASES.items():
+        if only and f"ops_{name}" not in only:
+            continue
         p = make_ops(name, case, HERE)
         print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
     for name, case in EVOL.items():
+        if only and f"evol_{name}" not in only:
+            continue
         p = make_evol(name, case, HERE)
         print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
 

@@ -40,8 +40,8 @@ def test_defaults_match_reference():
     assert p.r_max_con == float("inf")
 
 
-@pytest.mark.parametrize("name", ["ops_gw1", "ops_punc2", "ops_rs2", "evol_gw16",
-                                  "evol_punc4"])
+@pytest.mark.parametrize("name", ["ops_gw1", "ops_punc2", "ops_rs2", "ops_somm2", "evol_gw16",
+                                  "evol_punc4", "evol_somm4"])
 def test_block_coordinates_bitwise(name):
     c = Case(name)
     m = c.mesh
@@ -66,7 +66,7 @@ def test_create_errors_without_device_or_with_bad_mesh():
     assert e.value.code == -7
 
 
-@pytest.mark.parametrize("name", ["evol_gw16", "evol_punc4"])
+@pytest.mark.parametrize("name", ["evol_gw16", "evol_punc4", "evol_somm4"])
 def test_initial_data_pipeline_matches_reference(name):
     """Host initial data (restated problem generators) taken through the
     oracle's ADMToZ4c, ghost exchange and ghost-only AlgConstr reproduces the

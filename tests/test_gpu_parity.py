@@ -11,7 +11,7 @@ from z4c_testlib import NG, Case, rel_err
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
-OPS = ["ops_gw1", "ops_punc2", "ops_rs2"]
+OPS = ["ops_gw1", "ops_punc2", "ops_rs2", "ops_somm2"]
 
 
 def make_ctx(c):
@@ -37,6 +37,10 @@ def test_operators(name, per_block):
         ctx.Z4cRHS(Z.REG_U, Z.REG_RHS, blk)
     rhs = c.from_grid(ctx.download(Z.REG_RHS))
     assert rel_err(rhs[I], c.rec["rhs0"][I]) <= TOL
+    if "brhs0" in c.rec:  # Z4cBoundaryRHS on the gr_sommerfeld faces
+        ctx.Z4cBoundaryRHS(Z.REG_U, Z.REG_RHS, blk)
+        brhs = c.from_grid(ctx.download(Z.REG_RHS))
+        assert rel_err(brhs[I], c.rec["brhs0"][I]) <= TOL
     ctx.AlgConstr(Z.REG_U)
     assert rel_err(c.from_grid(ctx.download(Z.REG_U)), c.rec["alg0"]) <= TOL
     ctx.upload(Z.REG_U, u0)
@@ -75,7 +79,7 @@ def test_one_step_stage_by_stage(name, mode):
     ctx.close()
 
 
-@pytest.mark.parametrize("name", ["evol_gw16", "evol_punc4"])
+@pytest.mark.parametrize("name", ["evol_gw16", "evol_punc4", "evol_somm4"])
 def test_evolution_history_and_final_state(name):
     """Multi-step evolution from the reference's initial state (captured CUDA
     graph) against the reference driver's final state and .hst norms."""
@@ -93,7 +97,7 @@ def test_evolution_history_and_final_state(name):
     ctx.close()
 
 
-@pytest.mark.parametrize("name", ["evol_gw16", "evol_punc4"])
+@pytest.mark.parametrize("name", ["evol_gw16", "evol_punc4", "evol_somm4"])
 def test_initial_data_on_device(name):
     """Host initial data -> device ADMToZ4c -> ghost finalisation reproduces
     the reference's initialised state.

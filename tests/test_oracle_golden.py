@@ -7,11 +7,16 @@ import pytest
 import z4c_oracle as O
 from z4c_testlib import Case, bitwise
 
-OPS = ["ops_gw1", "ops_punc2", "ops_rs2"]
+OPS = ["ops_gw1", "ops_punc2", "ops_rs2", "ops_somm2"]
 
 
 def _params(case):
     return O.default_params(**case.params)
+
+
+def _som(case, g):
+    """Sommerfeld faces of the block with reference gid g."""
+    return O.sommerfeld_faces(case.nb, case.mesh["bc"], case.order[g])
 
 
 @pytest.mark.parametrize("name", OPS)
@@ -23,6 +28,10 @@ def test_single_operators(name):
     I = c.interior()
     rhs = np.stack([O.rhs(b, p, u0[g]) for g, b in enumerate(blocks)])
     assert bitwise(rhs[I], c.rec["rhs0"][I])
+    if "brhs0" in c.rec:  # Z4cBoundaryRHS on the gr_sommerfeld faces
+        for g, b in enumerate(blocks):
+            O.boundary_rhs(b, u0[g], rhs[g], _som(c, g))
+        assert bitwise(rhs[I], c.rec["brhs0"][I])
     alg = np.stack([O.algconstr(b, p, u0[g]) for g, b in enumerate(blocks)])
     assert bitwise(alg, c.rec["alg0"])
     adm = np.stack([O.z4c_to_adm(b, p, u0[g]) for g, b in enumerate(blocks)])
@@ -51,6 +60,8 @@ def oracle_step(c, p, blocks, u, dt):
             w = O.LS_RK4[s]
             r = np.stack([O.rhs(blocks[b], p, u[b]) for b in range(nb)])
             for b in range(nb):
+                O.boundary_rhs(blocks[b], u[b], r[b], _som(c, b))
+            for b in range(nb):
                 O.weighted_ave(u1[b], u[b], None, [1.0, w["delta"], 0.0], c.nn)
                 O.weighted_ave(u[b], u1[b], None, [w["gamma_1"], w["gamma_2"], w["gamma_3"]], c.nn)
                 O.add_rhs(r[b], w["beta"] * dt, u[b], c.nn)
@@ -61,6 +72,8 @@ def oracle_step(c, p, blocks, u, dt):
         un, ks = u.copy(), []
         for s in range(4):
             ks.append(np.stack([O.rhs(blocks[b], p, u[b]) for b in range(nb)]))
+            for b in range(nb):
+                O.boundary_rhs(blocks[b], u[b], ks[-1][b], _som(c, b))
             u = un.copy()
             coefs = O.BT_RK4_A[s + 1][: s + 1] if s < 3 else O.BT_RK4_B
             for q, a in enumerate(coefs):
@@ -85,7 +98,7 @@ def test_one_step_stage_by_stage(name):
     assert bitwise(con, c.rec["s4_con"])
 
 
-@pytest.mark.parametrize("name", ["evol_gw16", "evol_punc4"])
+@pytest.mark.parametrize("name", ["evol_gw16", "evol_punc4", "evol_somm4"])
 def test_evolution_and_history(name):
     """Multi-step run of the stock reference driver: final state and the
     history-output constraint norms (outputs/history.cpp:168-200)."""
