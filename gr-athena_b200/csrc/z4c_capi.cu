@@ -535,6 +535,31 @@ int z4c_mesh_block_coords(const z4c_mesh_desc_t* mesh, int block, int axis, doub
   return Z4C_OK;
 }
 
+int z4c_mesh_new_dt(const z4c_mesh_desc_t* mesh, double cfl, double* dt_out) {
+  if (!mesh || !dt_out) return fail(Z4C_EINVAL, "null argument");
+  if (!(cfl > 0.0)) return fail(Z4C_EINVAL, "cfl must be positive");
+  const int nblocks = mesh->nb[0] * mesh->nb[1] * mesh->nb[2];
+  if (nblocks < 1) return fail(Z4C_EINVAL, "empty mesh");
+  std::vector<double> x;
+  double dt = std::numeric_limits<double>::max();
+  for (int b = 0; b < nblocks; ++b) {
+    const int loc[3] = {b % mesh->nb[0], (b / mesh->nb[0]) % mesh->nb[1],
+                        b / (mesh->nb[0] * mesh->nb[1])};
+    // NewBlockTimeStep: the minimum cell width of the block (uniform: dx per
+    // axis), times the Courant number; the mesh step is the minimum over
+    // blocks (Mesh::NewTimeStep)
+    double min_dt = std::numeric_limits<float>::max();
+    for (int a = 0; a < 3; ++a) {
+      x.resize(mesh->nx[a] + 1 + 2 * Z4C_NG);
+      min_dt = std::min(min_dt, block_axis_coords(mesh, loc[a], a, x.data()));
+    }
+    min_dt *= cfl;
+    dt = std::min(dt, min_dt);
+  }
+  *dt_out = dt;
+  return Z4C_OK;
+}
+
 int z4c_upload(z4c_ctx* ctx, int reg, int block, const double* host) {
   if (!ctx || !host) return fail(Z4C_EINVAL, "null argument");
   int rc = check_reg(ctx, reg);

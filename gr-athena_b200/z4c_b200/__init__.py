@@ -44,7 +44,7 @@ HST_COLUMNS = ("H-norm2", "M-norm2", "Mx-norm2", "My-norm2", "Mz-norm2", "Z-norm
 EXPORTS = (
     "z4c_params_default", "z4c_last_error", "z4c_create", "z4c_destroy",
     "z4c_set_stream", "z4c_sync", "z4c_num_blocks", "z4c_block_nn", "z4c_reg_nvar",
-    "z4c_dx", "z4c_block_coords", "z4c_mesh_block_coords", "z4c_upload", "z4c_download", "z4c_device_ptr",
+    "z4c_dx", "z4c_block_coords", "z4c_mesh_block_coords", "z4c_mesh_new_dt", "z4c_upload", "z4c_download", "z4c_device_ptr",
     "z4c_rhs", "z4c_boundary_rhs", "z4c_add_rhs", "z4c_weighted_ave", "z4c_alg_constr", "z4c_adm_to_z4c",
     "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_ghost_fill", "z4c_init_finalize",
     "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
@@ -102,6 +102,7 @@ def lib():
         L.z4c_dx.argtypes = [vp, dp]
         L.z4c_block_coords.argtypes = [vp, ip, ip, dp]
         L.z4c_mesh_block_coords.argtypes = [C.POINTER(MeshDesc), ip, ip, dp, dp]
+        L.z4c_mesh_new_dt.argtypes = [C.POINTER(MeshDesc), C.c_double, dp]
         L.z4c_upload.argtypes = [vp, ip, ip, dp]
         L.z4c_download.argtypes = [vp, ip, ip, dp]
         L.z4c_device_ptr.argtypes = [vp, ip, C.POINTER(dp)]
@@ -197,6 +198,13 @@ class Mesh:
             xs.append(x)
             dxs.append(dx.value)
         return xs, dxs
+
+    def new_dt(self, cfl):
+        """Time step of the mesh: NewBlockTimeStep on every block, minimum
+        over blocks (cfl times the smallest cell width)."""
+        dt = C.c_double()
+        _check(lib().z4c_mesh_new_dt(C.byref(self.desc()), float(cfl), C.byref(dt)))
+        return dt.value
 
     def zones(self):
         """Cells of the mesh (the reference's zone count, mesh.hpp:289-292)."""

@@ -156,6 +156,11 @@ int z4c_block_coords(const z4c_ctx *ctx, int block, int axis, double *x_out);
 int z4c_mesh_block_coords(const z4c_mesh_desc_t *mesh, int block, int axis, double *x_out,
                           double *dx_out);
 
+/* Z4c::NewBlockTimeStep (z4c/new_blockdt_z4c.cpp:24-70) over every block and
+ * the minimum over blocks of Mesh::NewTimeStep (mesh/mesh.cpp:1753-1803):
+ * cfl times the smallest cell width (host only, no context needed). */
+int z4c_mesh_new_dt(const z4c_mesh_desc_t *mesh, double cfl, double *dt_out);
+
 /* Host <-> device copies of a register; block = -1 for the whole mesh.  The
  * host buffer uses the reference layout (see above). */
 int z4c_upload(z4c_ctx *ctx, int reg, int block, const double *host);

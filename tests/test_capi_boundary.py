@@ -52,6 +52,17 @@ def test_block_coordinates_bitwise(name):
         assert np.array_equal(np.array(dxs), c.rec["dx"][g])
 
 
+@pytest.mark.parametrize("name", ["ops_gw1", "ops_punc2", "ops_rs2", "ops_somm2", "evol_gw16",
+                                  "evol_punc4", "evol_somm4"])
+def test_time_step_matches_reference(name):
+    """NewBlockTimeStep + Mesh::NewTimeStep with the decks' Courant number 0.25
+    give the reference's dt bit for bit."""
+    c = Case(name)
+    m = c.mesh
+    mesh = Z.Mesh(m["nb"], m["nx"], m["xmin"], m["xmax"], m["bc"])
+    assert mesh.new_dt(0.25) == c.rec["time_dt"][1]
+
+
 def test_create_errors_without_device_or_with_bad_mesh():
     bad = Z.Mesh((1, 1, 1), (4, 8, 8), (0, 0, 0), (1, 1, 1))
     with pytest.raises(Z.Z4cError) as e:
