@@ -49,7 +49,7 @@ EXPORTS = (
     "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_ghost_fill", "z4c_init_finalize",
     "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
     "z4c_get_tile", "z4c_check_finite", "z4c_kernel_launches", "z4c_rhs_stage",
-    "z4c_fp64_probe", "z4c_rhs_noalloc")
+    "z4c_fp64_probe", "z4c_vc_restrict", "z4c_vc_prolongate", "z4c_rhs_noalloc")
 
 
 class Z4cError(RuntimeError):
@@ -125,6 +125,9 @@ def lib():
         L.z4c_check_finite.argtypes = [vp, ip]
         L.z4c_rhs_stage.argtypes = [vp, ip, C.c_double]
         L.z4c_fp64_probe.argtypes = [vp, dp]
+        ipp = C.POINTER(C.c_int)
+        L.z4c_vc_restrict.argtypes = [vp, vp, ip, ip, ipp, ipp, vp]
+        L.z4c_vc_prolongate.argtypes = [vp, vp, ip, ip, ipp, ipp, vp]
         L.z4c_rhs_noalloc.argtypes = [vp, vp, ip, C.POINTER(C.c_int), dp,
                                       C.POINTER(Params), vp]
         L.z4c_kernel_launches.argtypes = []

@@ -245,6 +245,27 @@ long long z4c_kernel_launches(void);
  * Z4C_OK if all finite, Z4C_ENONFINITE otherwise. */
 int z4c_check_finite(z4c_ctx *ctx, int reg);
 
+/* ---- vertex-centred refinement operators ----------------------------------
+ *
+ * MeshRefinement's vertex-centred operators (mesh/mesh_refinement_vc.cpp) on
+ * nblocks MeshBlocks of nx[0] x nx[1] x nx[2] cells held in caller-owned
+ * DEVICE arrays: fine [block][nvar][nn3][nn2][nn1] with nn = nx + 1 +
+ * 2*Z4C_NG, coarse [block][nvar][cn3][cn2][cn1] with cn = nx/2 + 1 + 2*Z4C_NCG
+ * (the reference's coarse_u_ layout, z4c.cpp:78-84).  box = {si, ei, sj, ej,
+ * sk, ek} is an inclusive range of coarse vertex indices, the arguments
+ * csi..cek / si..ek of the reference functions.  A box whose reads or writes
+ * would leave the arrays is rejected with Z4C_EINVAL before any launch.
+ * Work is enqueued on `stream` (a cudaStream_t; NULL = legacy default). */
+#define Z4C_NCG 4  /* coarse ghost vertices (reference NCGHOST for NGHOST=4) */
+/* MeshRefinement::RestrictVertexCenteredValues (:56-134): injection. */
+int z4c_vc_restrict(const double *fine, double *coarse, int nblocks, int nvar,
+                    const int nx[3], const int box[6], void *stream);
+/* MeshRefinement::ProlongateVertexCenteredValues (:283-775, 3-D): injection at
+ * coincident vertices, tensor-product 6-point Lagrange interpolation
+ * elsewhere (InterpolateLagrangeUniform<3>, utils/interp_univariate.hpp:43). */
+int z4c_vc_prolongate(const double *coarse, double *fine, int nblocks, int nvar,
+                      const int nx[3], const int box[6], void *stream);
+
 /* ---- allocation-free variant ----------------------------------------------
  *
  * No counterpart in the reference: an addition for callers that cannot call

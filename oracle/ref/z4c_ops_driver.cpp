@@ -15,6 +15,9 @@
 //   uadm0              ADMToZ4c(adm0) into a zeroed register
 //   gx_pre / gx_post   a block-dependent perturbation of u0 before and after
 //                      one ghost exchange + physical boundary conditions
+//   rf_*               with <driver> refine_ops_only = true, only the
+//                      vertex-centred refinement operators of one block of a
+//                      multilevel mesh (see RefinementOperators)
 //   s<n>_rhs, s<n>_int, s<n>_exch, s<n>_alg
 //                      one full time step, stage by stage, following the
 //                      GR_Z4c task order (task_list/gr/task_list_gr_z4c.cpp:
@@ -29,6 +32,7 @@
 
 #include "main.hpp"
 #include "comm/comm_registry.hpp"
+#include "mesh/mesh_refinement.hpp"
 #include "task_list/time_integrators.hpp"
 #include "z4c/z4c.hpp"
 
@@ -96,6 +100,73 @@ void ExchangeAndBC(const std::vector<MeshBlock*>& blocks, Real t, Real dt) {
     b->pcomm->ClearBoundary(comm::CommGroup::Z4c, comm::CommTarget::All, true);
 }
 
+// Vertex-centred refinement operators of one MeshBlock of a multilevel mesh
+// (mesh/mesh_refinement_vc.cpp): a fine array and a coarse array with
+// deterministic contents, MeshRefinement::RestrictVertexCenteredValues over
+// the coarse range whose fine image lies inside the block, and
+// MeshRefinement::ProlongateVertexCenteredValues over four coarse boxes (the
+// block interior, a face, an edge and a corner ghost region).  Records:
+//   rf_fine, rf_coarse      inputs
+//   rf_rbox, rf_restrict    restriction box {si,ei,sj,ej,sk,ek} and result
+//   rf_pbox<q>, rf_prolong<q>  prolongation boxes and results (fine array,
+//                           starting from rf_fine)
+void RefinementOperators(MeshBlock* b, Writer& w) {
+  const int NZ = Z4c::N_Z4c;
+  const int nn1 = b->nverts1, nn2 = b->nverts2, nn3 = b->nverts3;
+  const int cn1 = b->ncv1, cn2 = b->ncv2, cn3 = b->ncv3;
+  AthenaArray<Real> fine(NZ, nn3, nn2, nn1), coarse(NZ, cn3, cn2, cn1);
+  for (int n = 0; n < NZ; ++n) {
+    for (int k = 0; k < nn3; ++k)
+      for (int j = 0; j < nn2; ++j)
+        for (int i = 0; i < nn1; ++i)
+          fine(n, k, j, i) = std::sin(0.37 * n + 0.21 * i + 0.13 * j + 0.07 * k) +
+                             1e-3 * (i * j + k);
+    for (int k = 0; k < cn3; ++k)
+      for (int j = 0; j < cn2; ++j)
+        for (int i = 0; i < cn1; ++i)
+          coarse(n, k, j, i) = std::cos(0.29 * n + 0.43 * i + 0.31 * j + 0.17 * k) +
+                               1e-3 * (i + j * k);
+  }
+  auto dump = [&](const std::string& name, AthenaArray<Real>& a) {
+    std::vector<double> buf;
+    for (int n = 0; n < a.GetDim4(); ++n)
+      for (int k = 0; k < a.GetDim3(); ++k)
+        for (int j = 0; j < a.GetDim2(); ++j)
+          for (int i = 0; i < a.GetDim1(); ++i) buf.push_back(a(n, k, j, i));
+    w.f64(name, {a.GetDim4(), a.GetDim3(), a.GetDim2(), a.GetDim1()}, buf.data());
+  };
+  auto dump_box = [&](const std::string& name, const int* box) {
+    std::vector<std::int32_t> v(box, box + 6);
+    w.i32(name, {6}, v.data());
+  };
+  dump("rf_fine", fine);
+  dump("rf_coarse", coarse);
+  MeshRefinement* pmr = b->pmr;
+  {
+    AthenaArray<Real> out(NZ, cn3, cn2, cn1);
+    const int box[6] = {b->civs - 2, b->cive + 2, b->cjvs - 2, b->cjve + 2,
+                        b->ckvs - 2, b->ckve + 2};
+    pmr->RestrictVertexCenteredValues(fine, out, 0, NZ - 1, box[0], box[1], box[2], box[3],
+                                      box[4], box[5]);
+    dump_box("rf_rbox", box);
+    dump("rf_restrict", out);
+  }
+  const int lo = b->civs - 2, hi = b->cive + 2;  // coarse ghost slabs of width 2
+  const int boxes[4][6] = {
+      {b->civs, b->cive, b->cjvs, b->cjve, b->ckvs, b->ckve},            // interior
+      {lo, b->civs - 1, b->cjvs, b->cjve, b->ckvs, b->ckve},             // -x face
+      {b->cive + 1, hi, b->cjve + 1, hi, b->ckvs, b->ckve},              // +x+y edge
+      {lo, b->civs - 1, lo, b->cjvs - 1, b->ckve + 1, hi}};              // corner
+  for (int q = 0; q < 4; ++q) {
+    AthenaArray<Real> out;
+    Copy(out, fine);
+    pmr->ProlongateVertexCenteredValues(coarse, out, 0, NZ - 1, boxes[q][0], boxes[q][1],
+                                        boxes[q][2], boxes[q][3], boxes[q][4], boxes[q][5]);
+    dump_box("rf_pbox" + std::to_string(q), boxes[q]);
+    dump("rf_prolong" + std::to_string(q), out);
+  }
+}
+
 }  // namespace
 
 int main(int argc, char* argv[]) {
@@ -121,6 +192,12 @@ int main(int argc, char* argv[]) {
   }
   z4c_oracle::DumpGeometry(pm, d.w);
   d.dump("u0", NZ, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.u; });
+
+  if (pin->GetOrAddBoolean("driver", "refine_ops_only", false)) {
+    RefinementOperators(blocks[0], d.w);
+    std::cout << "z4c_ops_ref: wrote " << out << std::endl;
+    return 0;
+  }
 
   // --- single operators on u0 -------------------------------------------
   std::vector<AthenaArray<Real>> tmp(blocks.size());

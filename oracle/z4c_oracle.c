@@ -1155,6 +1155,160 @@ void orc_block_physical_bcs(const orc_mesh_t *m, const int loc[3], int nvar, dou
   }
 }
 
+/* ---- vertex-centred refinement operators, mesh/mesh_refinement_vc.cpp ---- */
+
+/* InterpolateLagrangeUniform<3>::coeff, utils/interp_univariate_stencils.tpp:99-101 */
+static const double LAG3[3] = {3. / 256., -25. / 256., 75. / 128.};
+
+void orc_vc_restrict(const int nx[3], int nvar, const double *fine, double *coarse,
+                     const int box[6]) {
+  const int nn[3] = {nx[0] + 1 + 2 * NG, nx[1] + 1 + 2 * NG, nx[2] + 1 + 2 * NG};
+  const int cn[3] = {nx[0] / 2 + 1 + 2 * ORC_NCG, nx[1] / 2 + 1 + 2 * ORC_NCG,
+                     nx[2] / 2 + 1 + 2 * ORC_NCG};
+  const int64_t fvol = (int64_t)nn[0] * nn[1] * nn[2], cvol = (int64_t)cn[0] * cn[1] * cn[2];
+  /* RestrictVertexCenteredIndicialHelper (:24-46): every branch maps a
+   * coarse index c to the fine index 2 (c - cvs) + vs */
+  for (int n = 0; n < nvar; ++n)
+    for (int ck = box[4]; ck <= box[5]; ++ck) {
+      const int k = 2 * (ck - ORC_NCG) + NG;
+      for (int cj = box[2]; cj <= box[3]; ++cj) {
+        const int j = 2 * (cj - ORC_NCG) + NG;
+        for (int ci = box[0]; ci <= box[1]; ++ci) {
+          const int i = 2 * (ci - ORC_NCG) + NG;
+          coarse[n * cvol + ((int64_t)ck * cn[1] + cj) * cn[0] + ci] =
+              fine[n * fvol + ((int64_t)k * nn[1] + j) * nn[0] + i];
+        }
+      }
+    }
+}
+
+void orc_vc_prolongate(const int nx[3], int nvar, const double *coarse, double *fine,
+                       const int box[6]) {
+  const int H = 3, HNC = (2 * ORC_NCG - NG) / 2; /* H_SZ, H_NCGHOST */
+  const int nn[3] = {nx[0] + 1 + 2 * NG, nx[1] + 1 + 2 * NG, nx[2] + 1 + 2 * NG};
+  const int cn[3] = {nx[0] / 2 + 1 + 2 * ORC_NCG, nx[1] / 2 + 1 + 2 * ORC_NCG,
+                     nx[2] / 2 + 1 + 2 * ORC_NCG};
+  const int cmp[3] = {ORC_NCG + nx[0] / 4, ORC_NCG + nx[1] / 4, ORC_NCG + nx[2] / 4};
+  const int64_t fvol = (int64_t)nn[0] * nn[1] * nn[2], cvol = (int64_t)cn[0] * cn[1] * cn[2];
+  const int si = box[0], ei = box[1], sj = box[2], ej = box[3], sk = box[4], ek = box[5];
+  /* bias offsets, :351-356 */
+  const int si_p = (si > cmp[0]) ? si - 1 : si, ei_p = (ei < cmp[0]) ? ei + 1 : ei;
+  const int sj_p = (sj > cmp[1]) ? sj - 1 : sj, ej_p = (ej < cmp[1]) ? ej + 1 : ej;
+  const int sk_p = (sk > cmp[2]) ? sk - 1 : sk, ek_p = (ek < cmp[2]) ? ek + 1 : ek;
+#define CO(k, j, i) c[((int64_t)(k) * cn[1] + (j)) * cn[0] + (i)]
+#define FI(k, j, i) f[((int64_t)(k) * nn[1] + (j)) * nn[0] + (i)]
+  for (int n = 0; n < nvar; ++n) {
+    const double *c = coarse + n * cvol;
+    double *f = fine + n * fvol;
+    /* (prl, prl, prl) */
+    for (int k = sk_p; k < ek_p; ++k)
+      for (int j = sj_p; j < ej_p; ++j)
+        for (int i = si_p; i < ei_p; ++i) {
+          double *o = &FI(2 * (k - HNC) + 1, 2 * (j - HNC) + 1, 2 * (i - HNC) + 1);
+          *o = 0.;
+          for (int dk = 0; dk < H; ++dk) {
+            const int ku = k + dk + 1, kl = k - dk;
+            const double lck = LAG3[H - dk - 1];
+            for (int dj = 0; dj < H; ++dj) {
+              const int ju = j + dj + 1, jl = j - dj;
+              const double lckj = lck * LAG3[H - dj - 1];
+              for (int di = 0; di < H; ++di) {
+                const int iu = i + di + 1, il = i - di;
+                const double lckji = lckj * LAG3[H - di - 1];
+                /* FloatingPoint::sum_corners (utils/floating_point.hpp:50-55) */
+                *o += lckji * (((CO(ku, ju, iu) + CO(kl, jl, il)) +
+                                (CO(ku, ju, il) + CO(kl, jl, iu))) +
+                               ((CO(kl, ju, il) + CO(ku, jl, iu)) +
+                                (CO(kl, ju, iu) + CO(ku, jl, il))));
+              }
+            }
+          }
+        }
+    /* (inj, prl, prl) */
+    for (int k = sk; k <= ek; ++k)
+      for (int j = sj_p; j < ej_p; ++j)
+        for (int i = si_p; i < ei_p; ++i) {
+          double *o = &FI(2 * (k - HNC), 2 * (j - HNC) + 1, 2 * (i - HNC) + 1);
+          *o = 0.;
+          for (int dj = 0; dj < H; ++dj) {
+            const int ju = j + dj + 1, jl = j - dj;
+            const double lcj = LAG3[H - dj - 1];
+            for (int di = 0; di < H; ++di) {
+              const int iu = i + di + 1, il = i - di;
+              const double lcji = lcj * LAG3[H - di - 1];
+              *o += lcji * ((CO(k, ju, iu) + CO(k, jl, il)) + (CO(k, jl, iu) + CO(k, ju, il)));
+            }
+          }
+        }
+    /* (prl, inj, prl) */
+    for (int k = sk_p; k < ek_p; ++k)
+      for (int j = sj; j <= ej; ++j)
+        for (int i = si_p; i < ei_p; ++i) {
+          double *o = &FI(2 * (k - HNC) + 1, 2 * (j - HNC), 2 * (i - HNC) + 1);
+          *o = 0.;
+          for (int dk = 0; dk < H; ++dk) {
+            const int ku = k + dk + 1, kl = k - dk;
+            const double lck = LAG3[H - dk - 1];
+            for (int di = 0; di < H; ++di) {
+              const int iu = i + di + 1, il = i - di;
+              const double lcki = lck * LAG3[H - di - 1];
+              *o += lcki * ((CO(kl, j, iu) + CO(ku, j, il)) + (CO(ku, j, iu) + CO(kl, j, il)));
+            }
+          }
+        }
+    /* (prl, prl, inj) */
+    for (int k = sk_p; k < ek_p; ++k)
+      for (int j = sj_p; j < ej_p; ++j)
+        for (int i = si; i <= ei; ++i) {
+          double *o = &FI(2 * (k - HNC) + 1, 2 * (j - HNC) + 1, 2 * (i - HNC));
+          *o = 0.;
+          for (int dk = 0; dk < H; ++dk) {
+            const int ku = k + dk + 1, kl = k - dk;
+            const double lck = LAG3[H - dk - 1];
+            for (int dj = 0; dj < H; ++dj) {
+              const int ju = j + dj + 1, jl = j - dj;
+              const double lckj = lck * LAG3[H - dj - 1];
+              *o += lckj * ((CO(ku, ju, i) + CO(kl, jl, i)) + (CO(kl, ju, i) + CO(ku, jl, i)));
+            }
+          }
+        }
+    /* (inj, inj, prl) */
+    for (int k = sk; k <= ek; ++k)
+      for (int j = sj; j <= ej; ++j)
+        for (int i = si_p; i < ei_p; ++i) {
+          double *o = &FI(2 * (k - HNC), 2 * (j - HNC), 2 * (i - HNC) + 1);
+          *o = 0.;
+          for (int di = 0; di < H; ++di)
+            *o += LAG3[H - di - 1] * (CO(k, j, i - di) + CO(k, j, i + di + 1));
+        }
+    /* (inj, prl, inj) */
+    for (int k = sk; k <= ek; ++k)
+      for (int j = sj_p; j < ej_p; ++j)
+        for (int i = si; i <= ei; ++i) {
+          double *o = &FI(2 * (k - HNC), 2 * (j - HNC) + 1, 2 * (i - HNC));
+          *o = 0.;
+          for (int dj = 0; dj < H; ++dj)
+            *o += LAG3[H - dj - 1] * (CO(k, j - dj, i) + CO(k, j + dj + 1, i));
+        }
+    /* (prl, inj, inj) */
+    for (int k = sk_p; k < ek_p; ++k)
+      for (int j = sj; j <= ej; ++j)
+        for (int i = si; i <= ei; ++i) {
+          double *o = &FI(2 * (k - HNC) + 1, 2 * (j - HNC), 2 * (i - HNC));
+          *o = 0.;
+          for (int dk = 0; dk < H; ++dk)
+            *o += LAG3[H - dk - 1] * (CO(k - dk, j, i) + CO(k + dk + 1, j, i));
+        }
+    /* (inj, inj, inj) */
+    for (int k = sk; k <= ek; ++k)
+      for (int j = sj; j <= ej; ++j)
+        for (int i = si; i <= ei; ++i)
+          FI(2 * (k - HNC), 2 * (j - HNC), 2 * (i - HNC)) = CO(k, j, i);
+  }
+#undef CO
+#undef FI
+}
+
 /* ---- history sums, outputs/history.cpp:168-200 --------------------------- */
 void orc_hst_accumulate(const orc_block_t *b, const z4c_params_t *opt,
                         const double *con, const double *u, double out[8]) {

@@ -81,6 +81,23 @@ void orc_adm_constraints(const orc_block_t *b, const z4c_params_t *p,
                          const double *adm, const double *u, const orc_derivs_t *d,
                          double *con);
 
+/* ---- vertex-centred refinement operators (mesh/mesh_refinement_vc.cpp) ---
+ *
+ * One MeshBlock of nx[3] cells: fine arrays are [nvar][nn3][nn2][nn1] with
+ * nn = nx + 1 + 2*ORC_NG, coarse arrays [nvar][cn3][cn2][cn1] with
+ * cn = nx/2 + 1 + 2*ORC_NCG.  Boxes are coarse index ranges
+ * {si, ei, sj, ej, sk, ek}, inclusive. */
+#define ORC_NCG 4
+/* MeshRefinement::RestrictVertexCenteredValues (:56-134), 3-D: injection. */
+void orc_vc_restrict(const int nx[3], int nvar, const double *fine, double *coarse,
+                     const int box[6]);
+/* MeshRefinement::ProlongateVertexCenteredValues (:283-775), 3-D branch with
+ * DBG_SYMMETRIZE_P_OP and DBG_SYMMETRIZE_CHEAP (defs.hpp.in:17-20):
+ * injection at coincident vertices, tensor-product 6-point Lagrange
+ * interpolation (H_SZ = 3) elsewhere. */
+void orc_vc_prolongate(const int nx[3], int nvar, const double *coarse, double *fine,
+                       const int box[6]);
+
 /* ---- uniform block grid (single level) ---------------------------------- */
 
 /* A uniform mesh of nb[0]*nb[1]*nb[2] blocks, block (l0,l1,l2) at index

@@ -78,6 +78,9 @@ def lib():
         L.orc_rhs.argtypes = [bp, pp, dp, Dp, dp]
         L.orc_boundary_rhs.argtypes = [bp, dp, dp, C.POINTER(C.c_int)]
         L.orc_algconstr.argtypes = [bp, pp, dp]
+        ip6 = C.POINTER(C.c_int)
+        L.orc_vc_restrict.argtypes = [ip6, C.c_int, dp, dp, ip6]
+        L.orc_vc_prolongate.argtypes = [ip6, C.c_int, dp, dp, ip6]
         L.orc_algconstr_ghosts.argtypes = [bp, pp, dp]
         L.orc_z4c_to_adm.argtypes = [bp, pp, dp, dp]
         L.orc_z4c_to_adm_ghosts.argtypes = [bp, pp, dp, dp]
@@ -263,3 +266,23 @@ LS_RK4 = [
 # classical Butcher RK4, task_list_integrators_butcher.cpp:37-48
 BT_RK4_A = [[0, 0, 0, 0], [0.5, 0, 0, 0], [0, 0.5, 0, 0], [0, 0, 1, 0]]
 BT_RK4_B = [1. / 6., 1. / 3., 1. / 3., 1. / 6.]
+
+
+# ---- vertex-centred refinement operators (mesh/mesh_refinement_vc.cpp) ----
+
+def vc_restrict(nx, fine, coarse, box):
+    """MeshRefinement::RestrictVertexCenteredValues over the coarse box, in
+    place on coarse ([nvar][cn3][cn2][cn1])."""
+    assert fine.flags.c_contiguous and coarse.flags.c_contiguous
+    lib().orc_vc_restrict((C.c_int * 3)(*nx), fine.shape[0], _ptr(fine), _ptr(coarse),
+                          (C.c_int * 6)(*[int(b) for b in box]))
+    return coarse
+
+
+def vc_prolongate(nx, coarse, fine, box):
+    """MeshRefinement::ProlongateVertexCenteredValues (3-D) over the coarse
+    box, in place on fine ([nvar][nn3][nn2][nn1])."""
+    assert fine.flags.c_contiguous and coarse.flags.c_contiguous
+    lib().orc_vc_prolongate((C.c_int * 3)(*nx), coarse.shape[0], _ptr(coarse), _ptr(fine),
+                            (C.c_int * 6)(*[int(b) for b in box]))
+    return fine

@@ -12,6 +12,8 @@ Fixtures (numpy .npz, compressed):
   evol_<case>.npz   a multi-step run of the stock reference driver: the
                     history table (outputs/history.cpp columns) and the
                     initial and final states
+  refine_vc.npz     the vertex-centred restriction and prolongation operators
+                    of one MeshBlock of a statically refined mesh
 Each fixture stores the input-deck parameters it was made with ("params",
 "mesh", "integrator" as JSON strings).
 """
@@ -162,8 +164,39 @@ def make_evol(name, case, outdir):
     return path
 
 
+# vertex-centred refinement operators (mesh/mesh_refinement_vc.cpp) on one
+# MeshBlock of a statically refined mesh: 16^3 cells as 2^3 blocks of 8^3 at
+# the root level, the centre refined once
+REFINE = dict(test="one_puncture", z4c=PUNCTURE, integ="rk4", bc="extrapolate_outflow",
+              mesh=[(16, -4.0, 4.0, 8)] * 3, extra={}, problem={"punc_ADM_mass": 1.0})
+
+
+def make_refine(outdir):
+    with tempfile.TemporaryDirectory() as tmp:
+        rec_path = os.path.join(tmp, "refine.rec")
+        inp = os.path.join(tmp, "case.inp")
+        text = deck(REFINE, rec_path).replace("refinement = none", "refinement = static")
+        text += "refine_ops_only = true\n<refinement1>\n" + "".join(
+            f"x{d}min = -0.5\nx{d}max = 0.5\n" for d in (1, 2, 3)) + "level = 1\n"
+        with open(inp, "w") as f:
+            f.write(text)
+        subprocess.run([os.path.join(REF_BIN, "z4c_ops_ref"), "-i", inp], cwd=tmp, check=True,
+                       stdout=subprocess.DEVNULL)
+        rec = read_records(rec_path)
+    # the operators act on every variable alike: keep three of them
+    keep = [0, 7, 21]
+    out = {k: (v if v.ndim == 1 else v[keep]) for k, v in rec.items() if k.startswith("rf_")}
+    out["nx"] = np.array([8, 8, 8])
+    path = os.path.join(outdir, "refine_vc.npz")
+    np.savez_compressed(path, **out)
+    return path
+
+
 def main():
     only = set(sys.argv[1:])  # fixture names to (re)make; all when empty
+    if not only or "refine_vc" in only:
+        p = make_refine(HERE)
+        print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
     for name, case in CASES.items():
         if only and f"ops_{name}" not in only:
             continue

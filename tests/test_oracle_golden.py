@@ -1,11 +1,13 @@
 """The CPU oracle against the golden fixtures produced by the reference
 build itself (tests/golden/make_golden.py).  The oracle restates the
 reference's arithmetic in the same order, so agreement is bit for bit."""
+import os
+
 import numpy as np
 import pytest
 
 import z4c_oracle as O
-from z4c_testlib import Case, bitwise
+from z4c_testlib import GOLDEN, Case, bitwise
 
 OPS = ["ops_gw1", "ops_punc2", "ops_rs2", "ops_somm2"]
 
@@ -117,3 +119,17 @@ def test_evolution_and_history(name):
     hst = O.hst_norms(blocks, p, con, u)
     ref = c.rec["hst"][int(c.rec["nlim"]), 3:11]
     np.testing.assert_allclose(hst, ref, rtol=1e-13, atol=0)
+
+
+def test_vc_refinement_operators():
+    """Restriction (injection) and prolongation (injection + tensor-product
+    Lagrange) of one MeshBlock of a statically refined mesh, bit for bit
+    against MeshRefinement's own operators."""
+    z = np.load(os.path.join(GOLDEN, "refine_vc.npz"))
+    nx = [int(v) for v in z["nx"]]
+    fine, coarse = z["rf_fine"], z["rf_coarse"]
+    out = O.vc_restrict(nx, fine.copy(), np.zeros_like(coarse), z["rf_rbox"])
+    assert bitwise(out, z["rf_restrict"])
+    for q in range(4):
+        out = O.vc_prolongate(nx, coarse.copy(), fine.copy(), z[f"rf_pbox{q}"])
+        assert bitwise(out, z[f"rf_prolong{q}"]), q
