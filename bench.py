@@ -193,6 +193,33 @@ def run_oracle_cpu(max_seconds=20.0):
 # ---------------------------------------------------------------------------
 
 
+class Ranks:
+    """Rank bookkeeping of the replica benchmark: every rank evolves its own
+    copy of the mesh, and the timed region ends at the slowest rank.  dist is
+    torch.distributed with an initialised process group (NCCL on the GPUs;
+    the tests use gloo on the CPU), or None for one rank."""
+
+    def __init__(self, dist, world, device):
+        self.dist, self.world, self.device = dist, world, device
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, x):
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, max_seconds):
+    """Units processed by all ranks divided by the slowest rank's time."""
+    return units_per_rank * world / max_seconds
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -231,16 +258,8 @@ def main():
             "128^3 cells as 512", f"{16 * args.nb}^3 cells as {mesh.nblocks}").replace(
             "[-16,16]^3", f"[-{lim:g},{lim:g}]^3")
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks(dist if world > 1 else None, world, "cuda")
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     # ---- device-resident throughput: graph-captured steps -------------------
     with torch.cuda.stream(stream):
@@ -262,7 +281,7 @@ def main():
     torch.cuda.synchronize()
     clocks = sampler.stop()
     ms = max_over_ranks(ev0.elapsed_time(ev1))
-    value = zones * args.steps * world / (ms * 1e-3)
+    value = whole_job_rate(zones * args.steps, world, ms * 1e-3)
     finite = ctx.check_finite()
 
     # ---- dominant kernel: the fused RHS+KO+stage kernel, timed alone -------
@@ -325,7 +344,7 @@ def main():
         ctx.download(Z.REG_U, out=out_host)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = zones * e2e_steps * world / e2e_s
+    e2e_value = whole_job_rate(zones * e2e_steps, world, e2e_s)
     state_bytes = host_np.nbytes
 
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
