@@ -100,7 +100,7 @@ struct z4c_ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   bool per_block = false;
-  int tile[3] = {128, 1, 1};
+  LaunchShape shape;  // launch shape of the RHS passes (autotuner output)
   bool has_outflow = false;
 
   // device buffers
@@ -207,7 +207,7 @@ int run_stage(z4c_ctx* c, int stage, double dt) {
       // instead of clearing it first
       LsStage ls{wt[0], wt[1], wt[2], wt[3], wt[4] * dt, stage == 1 ? 1 : 0};
       launch_stage_ls(g, P, u, c->scratch(), c->reg[Z4C_REG_RHS], c->reg[Z4C_REG_U1], w, ls, 0,
-                      g.nblocks, c->stream);
+                      g.nblocks, c->shape, c->stream);
       LAUNCH_CHECK("stage_ls");
       return exchange_into(c, w, u, true);
     }
@@ -221,7 +221,7 @@ int run_stage(z4c_ctx* c, int stage, double dt) {
     const double w1[3] = {1.0, wt[0], 0.0};
     const double w2[3] = {wt[1], wt[2], wt[3]};
     for (int b = 0; b < g.nblocks; ++b) {
-      launch_rhs(g, P, u, c->scratch(), c->reg[Z4C_REG_RHS], b, 1, c->stream);
+      launch_rhs(g, P, u, c->scratch(), c->reg[Z4C_REG_RHS], b, 1, c->shape, c->stream);
       launch_boundary_rhs(g, P, u, c->reg[Z4C_REG_RHS], b, 1, c->stream);
       launch_weighted_ave(g, c->reg[Z4C_REG_U1], u, nullptr, w1, b, 1, c->stream);
       launch_weighted_ave(g, u, c->reg[Z4C_REG_U1], nullptr, w2, b, 1, c->stream);
@@ -256,13 +256,13 @@ int run_stage(z4c_ctx* c, int stage, double dt) {
                   c->reg[Z4C_REG_K4]};
   if (!c->per_block) {
     launch_stage_bt(g, P, u, c->scratch(), c->reg[Z4C_REG_RHS], c->un, K, w, bs, 0, g.nblocks,
-                    c->stream);
+                    c->shape, c->stream);
     LAUNCH_CHECK("stage_bt");
     return exchange_into(c, w, u, true);
   }
   for (int b = 0; b < g.nblocks; ++b) {
     launch_stage_bt(g, P, u, c->scratch(), c->reg[Z4C_REG_RHS], c->un, K, w, bs, b, 1,
-                    c->stream);
+                    c->shape, c->stream);
     LAUNCH_CHECK("stage_bt");
   }
   int rc = exchange_into(c, w, u, false);
@@ -602,7 +602,7 @@ int z4c_rhs(z4c_ctx* ctx, int reg_u, int reg_rhs, int block) {
     return fail(Z4C_EINVAL, "z4c_rhs needs two distinct 22-variable registers");
   if ((rc = check_block(ctx, block, &b0, &nb))) return rc;
   launch_rhs(ctx->g, ctx->dev(), ctx->reg[reg_u], ctx->scratch(), ctx->reg[reg_rhs], b0, nb,
-             ctx->stream);
+             ctx->shape, ctx->stream);
   LAUNCH_CHECK("rhs");
   return Z4C_OK;
 }
@@ -766,7 +766,7 @@ int z4c_rhs_stage(z4c_ctx* ctx, int stage, double dt) {
   LsStage ls{wt[0], wt[1], wt[2], wt[3], wt[4] * dt, 0};
   launch_stage_ls(ctx->g, ctx->dev(), ctx->reg[Z4C_REG_U], ctx->scratch(),
                   ctx->reg[Z4C_REG_RHS], ctx->reg[Z4C_REG_U1], ctx->reg[Z4C_REG_W], ls, 0,
-                  ctx->g.nblocks, ctx->stream);
+                  ctx->g.nblocks, ctx->shape, ctx->stream);
   LAUNCH_CHECK("stage_ls");
   return Z4C_OK;
 }
@@ -803,18 +803,104 @@ int z4c_set_per_block(z4c_ctx* ctx, int per_block) {
   return Z4C_OK;
 }
 
+namespace {
+void drop_graph(z4c_ctx* ctx) {
+  if (ctx->graph) {
+    cudaGraphExecDestroy(ctx->graph);
+    ctx->graph = nullptr;
+  }
+}
+
+// Device time of one fused low-storage stage (u -> w, u1) with the given
+// shape: the minimum over reps launches after one warm-up launch.
+int time_stage(z4c_ctx* ctx, const LaunchShape& sh, int reps, float* best_ms) {
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  const double* wt = kLsRk4[0];
+  const LsStage ls{wt[0], wt[1], wt[2], wt[3], wt[4] * 1e-3, 1};
+  const DevParams P = ctx->dev();
+  float best = 1e30f;
+  int rc = Z4C_OK;
+  for (int r = 0; r <= reps && rc == Z4C_OK; ++r) {
+    cudaEventRecord(e0, ctx->stream);
+    launch_stage_ls(ctx->g, P, ctx->reg[Z4C_REG_U], ctx->scratch(), ctx->reg[Z4C_REG_RHS],
+                    ctx->reg[Z4C_REG_U1], ctx->reg[Z4C_REG_W], ls, 0, ctx->g.nblocks, sh,
+                    ctx->stream);
+    cudaEventRecord(e1, ctx->stream);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      rc = fail(Z4C_ECUDA, "autotune launch: %s", cudaGetErrorString(e));
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r > 0 && ms < best) best = ms;  // launch 0 is the warm-up
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *best_ms = best;
+  return rc;
+}
+}  // namespace
+
 int z4c_set_tile(z4c_ctx* ctx, int ti, int tj, int tk) {
   if (!ctx) return fail(Z4C_EINVAL, "null context");
-  if (ti != 128 || tj != 1 || tk != 1) return fail(Z4C_EINVAL, "unsupported tile");
-  ctx->tile[0] = ti;
-  ctx->tile[1] = tj;
-  ctx->tile[2] = tk;
+  LaunchShape sh;
+  sh.point_threads = ti;
+  sh.column_threads = tj;
+  sh.column_unroll = tk;
+  if (!valid_shape(sh))
+    return fail(Z4C_EINVAL, "unsupported launch shape (%d, %d, %d): point threads 64/128/256, "
+                "column threads 128/256/512, column unroll 2/4", ti, tj, tk);
+  ctx->shape = sh;
+  drop_graph(ctx);
   return Z4C_OK;
 }
 
 int z4c_get_tile(const z4c_ctx* ctx, int tile_out[3]) {
   if (!ctx || !tile_out) return fail(Z4C_EINVAL, "null argument");
-  for (int a = 0; a < 3; ++a) tile_out[a] = ctx->tile[a];
+  tile_out[0] = ctx->shape.point_threads;
+  tile_out[1] = ctx->shape.column_threads;
+  tile_out[2] = ctx->shape.column_unroll;
+  return Z4C_OK;
+}
+
+int z4c_autotune(z4c_ctx* ctx, int reps, float* best_ms_out) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  if (ctx->integrator != Z4C_INTEG_RK4)
+    return fail(Z4C_ESTATE, "the autotuner times the low-storage stage");
+  if (reps < 1) reps = 1;
+  // greedy: the heavy passes' CTA size first, then the column passes' shape;
+  // the stage writes only the work register, u1 and rhs, so u is untouched
+  LaunchShape best = ctx->shape;
+  float best_ms = 1e30f, ms = 0.f;
+  int rc;
+  for (int pt : {64, 128, 256}) {
+    LaunchShape sh = best;
+    sh.point_threads = pt;
+    if ((rc = time_stage(ctx, sh, reps, &ms))) return rc;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best.point_threads = pt;
+    }
+  }
+  for (int ct : {128, 256, 512})
+    for (int un : {2, 4}) {
+      LaunchShape sh = best;
+      sh.column_threads = ct;
+      sh.column_unroll = un;
+      if ((rc = time_stage(ctx, sh, reps, &ms))) return rc;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best.column_threads = ct;
+        best.column_unroll = un;
+      }
+    }
+  ctx->shape = best;
+  drop_graph(ctx);
+  if (best_ms_out) *best_ms_out = best_ms;
   return Z4C_OK;
 }
 

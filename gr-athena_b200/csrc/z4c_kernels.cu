@@ -14,26 +14,13 @@ namespace z4c {
 
 namespace {
 
-// Launch shape of the two heavy right-hand-side passes: threads per CTA and
-// the CTAs per SM the register allocation must allow (compile-time
-// candidates of the launch-shape sweep).
-#ifndef Z4C_RHS_THREADS
-#define Z4C_RHS_THREADS 128
-#endif
-#ifndef Z4C_RICCI_MINB
-#define Z4C_RICCI_MINB 1
-#endif
-#ifndef Z4C_MAIN_MINB
-#define Z4C_MAIN_MINB 1
-#endif
-constexpr int kRhsThreads = Z4C_RHS_THREADS;
-// Unroll factor of the k loops of the column passes (loads of several k in
-// flight per thread).
-#ifndef Z4C_KUNROLL
-#define Z4C_KUNROLL 4
-#endif
-constexpr int kKUnroll = Z4C_KUNROLL;
+// Launch shapes.  The heavy per-vertex passes (k_ricci, k_main) are compiled
+// for 64, 128 and 256 threads per CTA (all at the full register file of
+// 255 registers per thread); the column passes for k-loop unrolls of 2 and 4
+// and up to 512 threads per CTA.  A context's shape comes from the
+// autotuner (z4c_autotune) or from z4c_set_tile.
 constexpr int kPointThreads = 256;
+constexpr int kColumnMaxThreads = 512;
 
 inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
@@ -85,7 +72,7 @@ k_prep(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ s
     double w0 = __ldg(f + (k0 - 3) * sk), w1 = __ldg(f + (k0 - 2) * sk),
            w2 = __ldg(f + (k0 - 1) * sk), w3 = __ldg(f + k0 * sk),
            w4 = __ldg(f + (k0 + 1) * sk), w5 = __ldg(f + (k0 + 2) * sk);
-#pragma unroll kKUnroll
+#pragma unroll 4
     for (int k = k0; k <= k1; ++k) {
       const double w6 = __ldg(f + (k + 3) * sk);
       out[k * sk] = fd_dx7(w0, w1, w2, w4, w5, w6, cz);
@@ -94,13 +81,14 @@ k_prep(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ s
   } else {
     const int st = (dir == 0) ? 1 : nn0;
     const double ca = (dir == 0) ? F.cidx1[0] : F.cidx1[1];
-#pragma unroll kKUnroll
+#pragma unroll 4
     for (int k = k0; k <= k1; ++k) out[k * sk] = fd_dx(f + k * sk, st, ca);
   }
 }
 
 // ---- first pass: Ricci tensor + conformal-factor part per interior vertex --
-__global__ void __launch_bounds__(kRhsThreads, Z4C_RICCI_MINB)
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 1)
 k_ricci(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
         double* __restrict__ rsum, int block0, int nblk) {
   const int64_t npts = interior_count(g);
@@ -304,7 +292,8 @@ __device__ __forceinline__ void window_shift(double w[9]) {
 }
 
 // Advection sums (calculate_z4c_rhs.cpp:184-226): lv [block][22][interior vertex]
-__global__ void __launch_bounds__(kPointThreads)
+template <int UNROLL>
+__global__ void __launch_bounds__(kColumnMaxThreads)
 k_adv(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ lv, int block0,
       int nblk) {
   Column c;
@@ -321,7 +310,7 @@ k_adv(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ lv
   const FdScale& F = P.fd[c.b];
   double w[9];
   window_init(f, sk, NG, w);
-#pragma unroll kKUnroll
+#pragma unroll UNROLL
   for (int k = NG; k <= NG + g.nx[2]; ++k) {
     window_advance(f, sk, k, w);
     const int o = k * sk;
@@ -346,7 +335,8 @@ __device__ __forceinline__ double add_ko_column(double r, const double* __restri
 }
 
 // Z4cRHS tail: rhs += KO, in place.
-__global__ void __launch_bounds__(kPointThreads)
+template <int UNROLL>
+__global__ void __launch_bounds__(kColumnMaxThreads)
 k_ko_rhs(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ rhs,
          int block0, int nblk) {
   Column c;
@@ -357,7 +347,7 @@ k_ko_rhs(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__
   const FdScale& F = P.fd[c.b];
   double w[9];
   window_init(f, sk, NG, w);
-#pragma unroll kKUnroll
+#pragma unroll UNROLL
   for (int k = NG; k <= NG + g.nx[2]; ++k) {
     window_advance(f, sk, k, w);
     const int o = k * sk;
@@ -373,8 +363,8 @@ k_ko_rhs(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__
 //   WeightedAve(u1, u, u2, {1, delta, 0}); WeightedAve(u, u1, u2, {g1, g2, g3});
 //   AddZ4cRHS(rhs, beta*dt, u)        (mesh/weighted_ave.cpp:20-150)
 // u is read (all points, for the stencils); u_out, u1 are written (interior).
-template <bool SOM>
-__global__ void __launch_bounds__(kPointThreads)
+template <int UNROLL, bool SOM>
+__global__ void __launch_bounds__(kColumnMaxThreads)
 k_ko_stage_ls(Grid g, DevParams P, const double* __restrict__ u,
               const double* __restrict__ rhs, double* __restrict__ u1,
               double* __restrict__ u_out, LsStage w, int block0, int nblk) {
@@ -388,7 +378,7 @@ k_ko_stage_ls(Grid g, DevParams P, const double* __restrict__ u,
   const bool som = SOM && sommerfeld_var(c.n);
   double win[9];
   window_init(f, sk, NG, win);
-#pragma unroll kKUnroll
+#pragma unroll UNROLL
   for (int k = NG; k <= NG + g.nx[2]; ++k) {
     window_advance(f, sk, k, win);
     const int o = k * sk;
@@ -422,8 +412,8 @@ k_ko_stage_ls(Grid g, DevParams P, const double* __restrict__ u,
 struct KPtrs {
   double* k[4];
 };
-template <bool SOM>
-__global__ void __launch_bounds__(kPointThreads)
+template <int UNROLL, bool SOM>
+__global__ void __launch_bounds__(kColumnMaxThreads)
 k_ko_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ rhs,
               const double* __restrict__ un, KPtrs K, double* __restrict__ u_out, BtStage w,
               int block0, int nblk) {
@@ -437,7 +427,7 @@ k_ko_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* _
   const bool som = SOM && sommerfeld_var(c.n);
   double win[9];
   window_init(f, sk, NG, win);
-#pragma unroll kKUnroll
+#pragma unroll UNROLL
   for (int k = NG; k <= NG + g.nx[2]; ++k) {
     window_advance(f, sk, k, win);
     const int o = k * sk;
@@ -459,7 +449,8 @@ k_ko_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* _
 }
 
 // ---- main pass: the right-hand side without the Kreiss-Oliger terms -------
-__global__ void __launch_bounds__(kRhsThreads, Z4C_MAIN_MINB)
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 1)
 k_main(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
        const double* __restrict__ rsum, const double* __restrict__ lv, double* __restrict__ rhs,
        int block0, int nblk) {
@@ -812,7 +803,7 @@ __global__ void k_adm_to_z4c_gam(Grid g, DevParams P, const double* __restrict__
   }
 }
 
-__global__ void __launch_bounds__(kRhsThreads, 1)
+__global__ void __launch_bounds__(128, 1)
 k_adm_constraints(Grid g, DevParams P, const double* __restrict__ adm,
                   const double* __restrict__ u, double* __restrict__ con,
                   const double* __restrict__ xf, int block0, int nblk) {
@@ -935,54 +926,86 @@ static int64_t columns(const Grid& g, int nblk) {
   return (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * NVAR * nblk;
 }
 
-// The right-hand side passes shared by every RHS launch: Ricci (rsum),
-// advection sums (lv) and the main pass into rhs (without KO).
+bool valid_shape(const LaunchShape& sh) {
+  return (sh.point_threads == 64 || sh.point_threads == 128 || sh.point_threads == 256) &&
+         (sh.column_threads == 128 || sh.column_threads == 256 ||
+          sh.column_threads == 512) &&
+         (sh.column_unroll == 2 || sh.column_unroll == 4);
+}
+
+template <int T>
+static void launch_point_passes_t(const Grid& g, const DevParams& P, const double* u,
+                                  const RhsScratch& sc, double* rhs, int block0, int nblk,
+                                  int which, cudaStream_t st) {
+  const int64_t n = interior_count(g) * nblk;
+  COUNTED
+  if (which == 0)
+    k_ricci<T><<<div_up(n, T), T, 0, st>>>(g, P, u, sc.sd, sc.rsum, block0, nblk);
+  else
+    k_main<T><<<div_up(n, T), T, 0, st>>>(g, P, u, sc.sd, sc.rsum, sc.lv, rhs, block0, nblk);
+}
+static void launch_point_pass(const Grid& g, const DevParams& P, const double* u,
+                              const RhsScratch& sc, double* rhs, int block0, int nblk, int which,
+                              const LaunchShape& sh, cudaStream_t st) {
+  switch (sh.point_threads) {
+    case 64: launch_point_passes_t<64>(g, P, u, sc, rhs, block0, nblk, which, st); break;
+    case 256: launch_point_passes_t<256>(g, P, u, sc, rhs, block0, nblk, which, st); break;
+    default: launch_point_passes_t<128>(g, P, u, sc, rhs, block0, nblk, which, st); break;
+  }
+}
+
+// The right-hand side passes shared by every RHS launch: stored first
+// derivatives (sd), Ricci (rsum), advection sums (lv) and the main pass into
+// rhs (without KO).
 static void launch_rhs_passes(const Grid& g, const DevParams& P, const double* u,
                               const RhsScratch& sc, double* rhs, int block0, int nblk,
-                              cudaStream_t st) {
-  const int64_t n = interior_count(g) * nblk;
+                              const LaunchShape& sh, cudaStream_t st) {
   const int64_t cprep = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7);  // widest component region
   COUNTED
   k_prep<<<dim3(div_up(cprep, kPointThreads), kSdComponents, nblk), kPointThreads, 0, st>>>(
       g, P, u, sc.sd, block0);
+  launch_point_pass(g, P, u, sc, rhs, block0, nblk, 0, sh, st);
+  const int ct = sh.column_threads, cb = div_up(columns(g, nblk), ct);
   COUNTED
-  k_ricci<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, sc.sd, sc.rsum, block0, nblk);
-  COUNTED
-  k_adv<<<div_up(columns(g, nblk), kPointThreads), kPointThreads, 0, st>>>(g, P, u, sc.lv, block0,
-                                                                           nblk);
-  COUNTED
-  k_main<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, u, sc.sd, sc.rsum, sc.lv, rhs,
-                                                          block0, nblk);
+  if (sh.column_unroll == 2) k_adv<2><<<cb, ct, 0, st>>>(g, P, u, sc.lv, block0, nblk);
+  else k_adv<4><<<cb, ct, 0, st>>>(g, P, u, sc.lv, block0, nblk);
+  launch_point_pass(g, P, u, sc, rhs, block0, nblk, 1, sh, st);
 }
 
 void launch_rhs(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
-                double* rhs, int block0, int nblk, cudaStream_t st) {
-  launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, st);
+                double* rhs, int block0, int nblk, const LaunchShape& sh, cudaStream_t st) {
+  launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, sh, st);
+  const int ct = sh.column_threads, cb = div_up(columns(g, nblk), ct);
   COUNTED
-  k_ko_rhs<<<div_up(columns(g, nblk), kPointThreads), kPointThreads, 0, st>>>(g, P, u, rhs, block0,
-                                                                              nblk);
+  if (sh.column_unroll == 2) k_ko_rhs<2><<<cb, ct, 0, st>>>(g, P, u, rhs, block0, nblk);
+  else k_ko_rhs<4><<<cb, ct, 0, st>>>(g, P, u, rhs, block0, nblk);
 }
 
 void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                      double* rhs, double* u1, double* u_out, const LsStage& w, int block0,
-                     int nblk, cudaStream_t st) {
-  launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, st);
+                     int nblk, const LaunchShape& sh, cudaStream_t st) {
+  launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, sh, st);
   COUNTED
-  auto kern = g.has_sommerfeld ? k_ko_stage_ls<true> : k_ko_stage_ls<false>;
-  kern<<<div_up(columns(g, nblk), kPointThreads), kPointThreads, 0, st>>>(g, P, u, rhs, u1, u_out,
-                                                                          w, block0, nblk);
+  auto kern = (sh.column_unroll == 2)
+                  ? (g.has_sommerfeld ? k_ko_stage_ls<2, true> : k_ko_stage_ls<2, false>)
+                  : (g.has_sommerfeld ? k_ko_stage_ls<4, true> : k_ko_stage_ls<4, false>);
+  const int ct = sh.column_threads;
+  kern<<<div_up(columns(g, nblk), ct), ct, 0, st>>>(g, P, u, rhs, u1, u_out, w, block0, nblk);
 }
 
 void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                      double* rhs, const double* un, double* const* k, double* u_out,
-                     const BtStage& w, int block0, int nblk, cudaStream_t st) {
-  launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, st);
+                     const BtStage& w, int block0, int nblk, const LaunchShape& sh,
+                     cudaStream_t st) {
+  launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, sh, st);
   KPtrs K;
   for (int s = 0; s < 4; ++s) K.k[s] = k[s];
   COUNTED
-  auto kern = g.has_sommerfeld ? k_ko_stage_bt<true> : k_ko_stage_bt<false>;
-  kern<<<div_up(columns(g, nblk), kPointThreads), kPointThreads, 0, st>>>(g, P, u, rhs, un, K,
-                                                                          u_out, w, block0, nblk);
+  auto kern = (sh.column_unroll == 2)
+                  ? (g.has_sommerfeld ? k_ko_stage_bt<2, true> : k_ko_stage_bt<2, false>)
+                  : (g.has_sommerfeld ? k_ko_stage_bt<4, true> : k_ko_stage_bt<4, false>);
+  const int ct = sh.column_threads;
+  kern<<<div_up(columns(g, nblk), ct), ct, 0, st>>>(g, P, u, rhs, un, K, u_out, w, block0, nblk);
 }
 
 // Slot of every direction in the neighbour list (mesh_topology.cpp:329-960
@@ -1085,7 +1108,7 @@ void launch_adm_constraints(const Grid& g, const DevParams& P, const double* adm
                             int nblk, cudaStream_t st) {
   const int64_t n = g.nvol * nblk;
   COUNTED
-  k_adm_constraints<<<div_up(n, kRhsThreads), kRhsThreads, 0, st>>>(g, P, adm, u, con, xf,
+  k_adm_constraints<<<div_up(n, 128), 128, 0, st>>>(g, P, adm, u, con, xf,
                                                                     block0, nblk);
 }
 

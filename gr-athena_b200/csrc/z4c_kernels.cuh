@@ -63,19 +63,30 @@ struct RhsScratch {
 };
 constexpr int kSdComponents = 33;
 
+// Launch shape of the right-hand-side passes: threads per CTA of the heavy
+// per-vertex passes (64, 128, 256), threads per CTA of the column passes
+// (128, 256, 512) and the k-loop unroll of the column passes (2, 4).
+struct LaunchShape {
+  int point_threads = 128;
+  int column_threads = 256;
+  int column_unroll = 4;
+};
+bool valid_shape(const LaunchShape& sh);
+
 // Every RHS launch runs five kernels: stored first derivatives, Ricci pass,
 // advection sums, main pass (into rhs, without Kreiss-Oliger), then
 // Kreiss-Oliger fused with the consumer: in place for launch_rhs, with the
 // stage update for the stage launches (rhs then holds the pre-dissipation
 // right-hand side).
 void launch_rhs(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
-                double* rhs, int block0, int nblk, cudaStream_t st);
+                double* rhs, int block0, int nblk, const LaunchShape& sh, cudaStream_t st);
 void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                      double* rhs, double* u1, double* u_out, const LsStage& w, int block0,
-                     int nblk, cudaStream_t st);
+                     int nblk, const LaunchShape& sh, cudaStream_t st);
 void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                      double* rhs, const double* un, double* const* k, double* u_out,
-                     const BtStage& w, int block0, int nblk, cudaStream_t st);
+                     const BtStage& w, int block0, int nblk, const LaunchShape& sh,
+                     cudaStream_t st);
 // Ghost exchange of a 22-variable register: src (pre-exchange) -> dst (all
 // vertices); src and dst must differ.
 // Z4c::Z4cBoundaryRHS: Sommerfeld right-hand side on gr_sommerfeld faces.

@@ -152,7 +152,7 @@ extern "C" int z4c_rhs_noalloc(const double* u, double* rhs, int nblocks, const 
     g.nb[0] = nb;
     g.nb[1] = g.nb[2] = 1;
     g.nblocks = nb;
-    launch_rhs(g, P, u + bstride * b0, sc, rhs + bstride * b0, 0, nb, st);
+    launch_rhs(g, P, u + bstride * b0, sc, rhs + bstride * b0, 0, nb, LaunchShape(), st);
   }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

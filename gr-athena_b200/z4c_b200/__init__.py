@@ -48,7 +48,7 @@ EXPORTS = (
     "z4c_rhs", "z4c_boundary_rhs", "z4c_add_rhs", "z4c_weighted_ave", "z4c_alg_constr", "z4c_adm_to_z4c",
     "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_ghost_fill", "z4c_init_finalize",
     "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
-    "z4c_get_tile", "z4c_check_finite", "z4c_kernel_launches", "z4c_rhs_stage",
+    "z4c_get_tile", "z4c_autotune", "z4c_check_finite", "z4c_kernel_launches", "z4c_rhs_stage",
     "z4c_fp64_probe", "z4c_vc_restrict", "z4c_vc_prolongate", "z4c_rhs_noalloc")
 
 
@@ -122,6 +122,7 @@ def lib():
         L.z4c_set_per_block.argtypes = [vp, ip]
         L.z4c_set_tile.argtypes = [vp, ip, ip, ip]
         L.z4c_get_tile.argtypes = [vp, C.POINTER(C.c_int)]
+        L.z4c_autotune.argtypes = [vp, ip, C.POINTER(C.c_float)]
         L.z4c_check_finite.argtypes = [vp, ip]
         L.z4c_rhs_stage.argtypes = [vp, ip, C.c_double]
         L.z4c_fp64_probe.argtypes = [vp, dp]
@@ -340,6 +341,22 @@ class Z4c:
 
     def set_per_block(self, flag):
         _check(lib().z4c_set_per_block(self._h, int(bool(flag))))
+
+    def set_tile(self, point_threads, column_threads, column_unroll):
+        _check(lib().z4c_set_tile(self._h, int(point_threads), int(column_threads),
+                                  int(column_unroll)))
+
+    def get_tile(self):
+        t = (C.c_int * 3)()
+        _check(lib().z4c_get_tile(self._h, t))
+        return tuple(t)
+
+    def autotune(self, reps=3):
+        """Picks the fastest launch shape of the RHS passes on this mesh;
+        returns (shape, stage milliseconds)."""
+        ms = C.c_float()
+        _check(lib().z4c_autotune(self._h, int(reps), C.byref(ms)))
+        return self.get_tile(), ms.value
 
     def hst_norms(self):
         out = np.empty(8)

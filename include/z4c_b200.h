@@ -234,10 +234,20 @@ int z4c_fp64_probe(z4c_ctx *ctx, double *tflops);
 /* Selects the per-block launch loop (plain path, one RHS launch per block per
  * stage) instead of the batched launch inside z4c_stage/z4c_evolve. */
 int z4c_set_per_block(z4c_ctx *ctx, int per_block);
-/* Tile shape of the RHS kernel (autotuner output): threads per CTA along
- * i, j and k.  Returns Z4C_EINVAL for unsupported shapes. */
+/* Launch shape of the right-hand-side passes (no reference counterpart):
+ * tile = {threads per CTA of the per-vertex Ricci and main passes (64, 128,
+ * 256), threads per CTA of the per-variable column passes (128, 256, 512),
+ * k-loop unroll of the column passes (2, 4)}.  The default is {128, 256, 4};
+ * unsupported shapes return Z4C_EINVAL.  Results do not depend on the shape. */
 int z4c_set_tile(z4c_ctx *ctx, int ti, int tj, int tk);
 int z4c_get_tile(const z4c_ctx *ctx, int tile_out[3]);
+/* Autotuner (no reference counterpart): times one fused low-storage stage on
+ * the context's current state for each candidate shape (the Ricci/main CTA
+ * size first, then the column-pass shape; reps timed launches each after a
+ * warm-up), keeps the fastest and drops the captured step graph.  Writes the
+ * work register, u1 and rhs (u is untouched); call it between steps.
+ * *best_ms (may be NULL) receives the stage time of the chosen shape. */
+int z4c_autotune(z4c_ctx *ctx, int reps, float *best_ms);
 /* Kernels launched by this library in this process so far (graph replays
  * count every kernel node); a diagnostic with no reference counterpart. */
 long long z4c_kernel_launches(void);

@@ -115,3 +115,31 @@ def test_gauge_wave_convergence_order():
         ctx.close()
     order = np.log2(errs[0] / errs[1])
     assert order > 3.5, (errs, order)
+
+
+def test_launch_shapes_and_autotuner_leave_results_unchanged():
+    """Every launch shape the autotuner can pick gives the same bits; the
+    autotuner leaves u untouched and picks a supported shape."""
+    Z, ctx = mesh_ctx("outflow", nb=(4, 4, 4))
+    u0 = puncture_state(Z, ctx)
+    dt = 0.25 * float(ctx.dx().min())
+    ref = None
+    for shape in [(128, 256, 4), (64, 128, 2), (256, 512, 4), (128, 512, 2)]:
+        ctx.set_tile(*shape)
+        assert ctx.get_tile() == shape
+        ctx.upload(Z.REG_U, u0)
+        ctx.evolve(dt, 1)
+        out = ctx.download(Z.REG_U)
+        if ref is None:
+            ref = out
+        assert np.array_equal(out, ref), shape
+    ctx.upload(Z.REG_U, u0)
+    shape, ms = ctx.autotune(reps=2)
+    assert shape[0] in (64, 128, 256) and shape[1] in (128, 256, 512) and shape[2] in (2, 4)
+    assert ms > 0
+    assert np.array_equal(ctx.download(Z.REG_U), u0)
+    ctx.evolve(dt, 1)
+    assert np.array_equal(ctx.download(Z.REG_U), ref)
+    with pytest.raises(Z.Z4cError):
+        ctx.set_tile(100, 256, 4)
+    ctx.close()
