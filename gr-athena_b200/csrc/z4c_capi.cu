@@ -465,6 +465,10 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
     free_ctx(c);
     return fail(Z4C_ECUDA, "uploading mesh tables");
   }
+  if (allow_slab_smem() != 0) {
+    free_ctx(c);
+    return fail(Z4C_ECUDA, "raising the shared-memory limit of the slab kernels");
+  }
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
     free_ctx(c);
     return fail(Z4C_ECUDA, "stream creation");
@@ -850,10 +854,10 @@ int z4c_set_tile(z4c_ctx* ctx, int ti, int tj, int tk) {
   LaunchShape sh;
   sh.point_threads = ti;
   sh.column_threads = tj;
-  sh.column_unroll = tk;
+  sh.column_slabs = tk;
   if (!valid_shape(sh))
     return fail(Z4C_EINVAL, "unsupported launch shape (%d, %d, %d): point threads 64/128/256, "
-                "column threads 128/256/512, column unroll 2/4", ti, tj, tk);
+                "column threads 128/256/512, column slabs 0-4", ti, tj, tk);
   ctx->shape = sh;
   drop_graph(ctx);
   return Z4C_OK;
@@ -863,7 +867,7 @@ int z4c_get_tile(const z4c_ctx* ctx, int tile_out[3]) {
   if (!ctx || !tile_out) return fail(Z4C_EINVAL, "null argument");
   tile_out[0] = ctx->shape.point_threads;
   tile_out[1] = ctx->shape.column_threads;
-  tile_out[2] = ctx->shape.column_unroll;
+  tile_out[2] = ctx->shape.column_slabs;
   return Z4C_OK;
 }
 
@@ -887,15 +891,16 @@ int z4c_autotune(z4c_ctx* ctx, int reps, float* best_ms_out) {
     }
   }
   for (int ct : {128, 256, 512})
-    for (int un : {2, 4}) {
+    for (int ns : {0, 1, 2, 3, 4}) {
       LaunchShape sh = best;
       sh.column_threads = ct;
-      sh.column_unroll = un;
+      sh.column_slabs = ns;
+      if (ns > 0 && !slabs_fit(ctx->g, sh)) continue;
       if ((rc = time_stage(ctx, sh, reps, &ms))) return rc;
       if (ms < best_ms) {
         best_ms = ms;
         best.column_threads = ct;
-        best.column_unroll = un;
+        best.column_slabs = ns;
       }
     }
   ctx->shape = best;

@@ -135,30 +135,39 @@ __device__ __forceinline__ bool column_index(const Grid& g, int block0, int nblk
   return true;
 }
 
+// Loads for the stencil helpers below: read-only cache path for global
+// memory (GL = true), plain loads for shared memory.
+template <bool GL>
+__device__ __forceinline__ double ld(const double* p) {
+  if (GL) return __ldg(p);
+  return *p;
+}
+
 // Lop-sided advection along one direction (FDStencilBiased{Left,Right}<1,4,2>,
 // finite_differencing.tpp:175-191): only the side the sign of vx selects is
 // evaluated; its value is the reference's, which evaluates both and keeps one.
+template <bool GL = true>
 __device__ __forceinline__ double fd_lx_side(const double* __restrict__ u, int st, double vx,
                                              double lidx) {
   if (vx < 0) {
     double dl = 0.;
-    dl += 1. * __ldg(u - 4 * st);
-    dl += -8. * __ldg(u - 3 * st);
-    dl += 30. * __ldg(u - 2 * st);
-    dl += -80. * __ldg(u - st);
-    dl += 35. * __ldg(u);
-    dl += 24. * __ldg(u + st);
-    dl += -2. * __ldg(u + 2 * st);
+    dl += 1. * ld<GL>(u - 4 * st);
+    dl += -8. * ld<GL>(u - 3 * st);
+    dl += 30. * ld<GL>(u - 2 * st);
+    dl += -80. * ld<GL>(u - st);
+    dl += 35. * ld<GL>(u);
+    dl += 24. * ld<GL>(u + st);
+    dl += -2. * ld<GL>(u + 2 * st);
     return (vx * dl) * lidx;
   }
   double dr = 0.;
-  dr += -1. * __ldg(u + 4 * st);
-  dr += 8. * __ldg(u + 3 * st);
-  dr += -30. * __ldg(u + 2 * st);
-  dr += 80. * __ldg(u + st);
-  dr += -35. * __ldg(u);
-  dr += -24. * __ldg(u - st);
-  dr += 2. * __ldg(u - 2 * st);
+  dr += -1. * ld<GL>(u + 4 * st);
+  dr += 8. * ld<GL>(u + 3 * st);
+  dr += -30. * ld<GL>(u + 2 * st);
+  dr += 80. * ld<GL>(u + st);
+  dr += -35. * ld<GL>(u);
+  dr += -24. * ld<GL>(u - st);
+  dr += 2. * ld<GL>(u - 2 * st);
   return (vx * dr) * lidx;
 }
 // The same along z from the window w[0..8] = f(k-4..k+4).
@@ -187,14 +196,15 @@ __device__ __forceinline__ double fd_lx_window(const double w[9], double vx, dou
 
 // Kreiss-Oliger along one direction (FDStencilCenteredDegreeEven<8,4>,
 // finite_differencing.tpp:335-368) from a line pointer or from the window.
+template <bool GL = true>
 __device__ __forceinline__ double fd_diss_line(const double* __restrict__ u, int st, double cidxd,
                                                double diss) {
   double out = 0.;
-  out += 1. * (__ldg(u - 4 * st) + __ldg(u + 4 * st));
-  out += -8. * (__ldg(u - 3 * st) + __ldg(u + 3 * st));
-  out += 28. * (__ldg(u - 2 * st) + __ldg(u + 2 * st));
-  out += -56. * (__ldg(u - st) + __ldg(u + st));
-  out += 70. * __ldg(u);
+  out += 1. * (ld<GL>(u - 4 * st) + ld<GL>(u + 4 * st));
+  out += -8. * (ld<GL>(u - 3 * st) + ld<GL>(u + 3 * st));
+  out += 28. * (ld<GL>(u - 2 * st) + ld<GL>(u + 2 * st));
+  out += -56. * (ld<GL>(u - st) + ld<GL>(u + st));
+  out += 70. * ld<GL>(u);
   return out * cidxd * diss;
 }
 __device__ __forceinline__ double fd_diss_window(const double w[9], double cidxd, double diss) {
@@ -227,31 +237,33 @@ __device__ __forceinline__ bool on_sommerfeld_face(const Grid& g, int b, int i, 
          (g.bc[4] == Z4C_BC_SOMMERFELD && l2 == 0 && k == NG) ||
          (g.bc[5] == Z4C_BC_SOMMERFELD && l2 == g.nb[2] - 1 && k == NG + g.nx[2]);
 }
+template <bool GL = true>
 __device__ __forceinline__ double fd_ds(const double* __restrict__ f, int64_t st, double dx) {
   double out = 0.;
-  out += -1. * (__ldg(f - st) - __ldg(f + st));
+  out += -1. * (ld<GL>(f - st) - ld<GL>(f + st));
   return out * (1.0 / (dx * 2));
 }
 // Sommerfeld value of variable n at vertex (i, j, k) of block b; f points at
-// that variable's value there.
+// that variable's value there, st holds the strides of f's array.
+template <bool GL = true>
 __device__ __forceinline__ double sommerfeld_value(const Grid& g, const DevParams& P, int b,
                                                   int n, const double* __restrict__ f, int i,
-                                                  int j, int k) {
+                                                  int j, int k, const int64_t* st) {
   const double* x = P.xf + (int64_t)b * (g.nn[0] + g.nn[1] + g.nn[2]);
   const double x1 = x[i], x2 = x[g.nn[0] + j], x3 = x[g.nn[0] + g.nn[1] + k];
   double d[3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) d[a] = fd_ds(f, g.s[a], P.dx[(int64_t)b * 3 + a]);
+  for (int a = 0; a < 3; ++a) d[a] = fd_ds<GL>(f, st[a], P.dx[(int64_t)b * 3 + a]);
   const double r = sqrt(x1 * x1 + x2 * x2 + x3 * x3);
   const double s_u[3] = {x1 / r, x2 / r, x3 / r};
   const double sqrt2 = sqrt(2.);
   double v;
   if (n == Z4C_KHAT) {
-    v = -sqrt2 * __ldg(f) / r;
+    v = -sqrt2 * ld<GL>(f) / r;
 #pragma unroll
     for (int a = 0; a < 3; ++a) v -= sqrt2 * s_u[a] * d[a];
   } else {
-    v = -__ldg(f) / r;
+    v = -ld<GL>(f) / r;
 #pragma unroll
     for (int a = 0; a < 3; ++a) v -= s_u[a] * d[a];
   }
@@ -273,7 +285,7 @@ k_sommerfeld(Grid g, DevParams P, const double* __restrict__ u, double* __restri
   const int i = NG + l % n0, j = NG + (l / n0) % n1, k = NG + l / (n0 * n1);
   if (!on_sommerfeld_face(g, b, i, j, k)) return;
   const int64_t q = ((int64_t)b * NVAR + n) * g.nvol + ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
-  rhs[q] = sommerfeld_value(g, P, b, n, u + q, i, j, k);
+  rhs[q] = sommerfeld_value(g, P, b, n, u + q, i, j, k, g.s);
 }
 
 // Fills the z window of column c at the first interior k.
@@ -384,7 +396,7 @@ k_ko_stage_ls(Grid g, DevParams P, const double* __restrict__ u,
     const int o = k * sk;
     const int64_t q = base + o;
     const double r = (som && on_sommerfeld_face(g, c.b, c.i, c.j, k))
-                         ? sommerfeld_value(g, P, c.b, c.n, f + o, c.i, c.j, k)
+                         ? sommerfeld_value(g, P, c.b, c.n, f + o, c.i, c.j, k, g.s)
                          : add_ko_column(__ldg(rhs + q), f + o, nn0, win, F, P.p.diss);
     const double un = win[4];
     double v1 = w.u1_zero ? 0.0 : u1[q];
@@ -433,7 +445,7 @@ k_ko_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* _
     const int o = k * sk;
     const int64_t q = base + o;
     const double r = (som && on_sommerfeld_face(g, c.b, c.i, c.j, k))
-                         ? sommerfeld_value(g, P, c.b, c.n, f + o, c.i, c.j, k)
+                         ? sommerfeld_value(g, P, c.b, c.n, f + o, c.i, c.j, k, g.s)
                          : add_ko_column(__ldg(rhs + q), f + o, nn0, win, F, P.p.diss);
     K.k[w.kslot][q] = r;
     double v = __ldg(un + q);
@@ -445,6 +457,207 @@ k_ko_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* _
     }
     u_out[q] = v;
     window_shift(win);
+  }
+}
+
+// ---- slab passes: one CTA per (block, variable, z-slab) --------------------
+// The per-variable passes read one variable's stencils only, so a CTA takes
+// one (block, variable) pair and a slab of its interior planes kl..kh,
+// copies the vertex planes kl-4..kh+4 (a contiguous range of the register)
+// into shared memory with coalesced loads, and evaluates every stencil of
+// the slab's interior vertices from there.  The arithmetic is that of the
+// pencil kernels above, vertex by vertex.  Used when the planes fit in
+// shared memory (16^3 blocks: 5 kB per plane).
+struct SlabGeom {
+  int kper;   // interior planes per slab
+  int plane;  // vertices per plane, nn0*nn1
+};
+__device__ __forceinline__ void slab_range(const Grid& g, const SlabGeom& S, int& kl, int& kh) {
+  kl = NG + (int)blockIdx.x * S.kper;
+  kh = min(NG + g.nx[2], kl + S.kper - 1);
+}
+// Copies planes kl-4..kh+4 of the variable block f into sm with
+// asynchronous global-to-shared copies (cp.async, 8 bytes each): every
+// thread issues all of its copies before waiting, so the whole slab is in
+// flight at once.
+__device__ __forceinline__ void slab_load(double* __restrict__ sm, const double* __restrict__ f,
+                                          int kl, int kh, int plane) {
+  const double* src = f + (int64_t)(kl - NG) * plane;
+  const int n = (kh - kl + 1 + 2 * NG) * plane;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sm + q);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src + q) : "memory");
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+}
+
+// Advection sums, and for chi, g~, alpha, beta the stored first derivatives
+// (the work of k_adv and k_prep on one variable).
+__global__ void __launch_bounds__(kColumnMaxThreads)
+k_adv_prep_slab(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ lv,
+                double* __restrict__ sd, SlabGeom S, int block0) {
+  extern __shared__ double sm[];
+  const int n = (int)blockIdx.y, b = block0 + (int)blockIdx.z;
+  int kl, kh;
+  slab_range(g, S, kl, kh);
+  if (kl > kh) return;
+  const int nn0 = g.nn[0], pl = S.plane;
+  const double* U = u + (int64_t)b * NVAR * g.nvol;
+  slab_load(sm, U + (int64_t)n * g.nvol, kl, kh, pl);
+  // vertex (i, j, k) of the block in shared memory
+  const double* s0 = sm - (int64_t)(kl - NG) * pl;
+  const FdScale& F = P.fd[b];
+  const int n0 = g.nx[0] + 1, n1 = g.nx[1] + 1, nk = kh - kl + 1;
+  const int64_t npts = interior_count(g);
+  double* out = lv + ((int64_t)b * NVAR + n) * npts;
+  for (int q = threadIdx.x; q < n0 * n1 * nk; q += blockDim.x) {
+    const int i = NG + q % n0, j = NG + (q / n0) % n1, k = kl + q / (n0 * n1);
+    const int o = k * pl + j * nn0 + i;
+    double acc = 0;
+    acc += fd_lx_side<false>(s0 + o, 1, __ldg(U + (int64_t)Z4C_BETAX * g.nvol + o), F.lidx[0]);
+    acc += fd_lx_side<false>(s0 + o, nn0, __ldg(U + (int64_t)Z4C_BETAY * g.nvol + o), F.lidx[1]);
+    acc += fd_lx_side<false>(s0 + o, pl, __ldg(U + (int64_t)Z4C_BETAZ * g.nvol + o), F.lidx[2]);
+    out[((k - NG) * n1 + (j - NG)) * n0 + (i - NG)] = acc;
+  }
+  // stored first derivatives (k_prep's regions): D_x on the interior, D_y
+  // extended by 3 along x, D_z extended by 3 along x and y
+  int slot = -1;
+#pragma unroll
+  for (int q = 0; q < kSdFields; ++q)
+    if (sd_field_var(q) == n) slot = q;
+  if (slot < 0) return;
+  double* sdb = sd + ((int64_t)b * kSdComponents + slot * 3) * g.nvol;
+  for (int dir = 0; dir < 3; ++dir) {
+    const int ex = (dir >= 1) ? 3 : 0, ey = (dir == 2) ? 3 : 0;
+    const int e0 = n0 + 2 * ex, e1 = n1 + 2 * ey;
+    const int st = (dir == 0) ? 1 : (dir == 1 ? nn0 : pl);
+    const double c1 = F.cidx1[dir];
+    double* o_dir = sdb + (int64_t)dir * g.nvol;
+    for (int q = threadIdx.x; q < e0 * e1 * nk; q += blockDim.x) {
+      const int i = NG - ex + q % e0, j = NG - ey + (q / e0) % e1, k = kl + q / (e0 * e1);
+      const int o = k * pl + j * nn0 + i;
+      const double* v = s0 + o;
+      o_dir[o] = fd_dx7(v[-3 * st], v[-2 * st], v[-st], v[st], v[2 * st], v[3 * st], c1);
+    }
+  }
+}
+
+// Kreiss-Oliger from shared memory, rhs += Diss_x; += Diss_y; += Diss_z.
+__device__ __forceinline__ double add_ko_slab(double r, const double* v, int nn0, int pl,
+                                              const FdScale& F, double diss) {
+  r += fd_diss_line<false>(v, 1, F.cidxd[0], diss);
+  r += fd_diss_line<false>(v, nn0, F.cidxd[1], diss);
+  r += fd_diss_line<false>(v, pl, F.cidxd[2], diss);
+  return r;
+}
+
+// KO + low-storage stage (k_ko_stage_ls) with Z4cBoundaryRHS on
+// Sommerfeld faces, from a shared-memory slab.
+template <bool SOM>
+__global__ void __launch_bounds__(kColumnMaxThreads)
+k_ko_stage_ls_slab(Grid g, DevParams P, const double* __restrict__ u,
+                   const double* __restrict__ rhs, double* __restrict__ u1,
+                   double* __restrict__ u_out, LsStage w, SlabGeom S, int block0) {
+  extern __shared__ double sm[];
+  const int n = (int)blockIdx.y, b = block0 + (int)blockIdx.z;
+  int kl, kh;
+  slab_range(g, S, kl, kh);
+  if (kl > kh) return;
+  const int nn0 = g.nn[0], pl = S.plane;
+  const int64_t base = ((int64_t)b * NVAR + n) * g.nvol;
+  slab_load(sm, u + base, kl, kh, pl);
+  const double* s0 = sm - (int64_t)(kl - NG) * pl;
+  const FdScale& F = P.fd[b];
+  const bool som = SOM && sommerfeld_var(n);
+  const int64_t sst[3] = {1, nn0, pl};
+  const int n0 = g.nx[0] + 1, n1 = g.nx[1] + 1, nk = kh - kl + 1;
+  for (int q = threadIdx.x; q < n0 * n1 * nk; q += blockDim.x) {
+    const int i = NG + q % n0, j = NG + (q / n0) % n1, k = kl + q / (n0 * n1);
+    const int o = k * pl + j * nn0 + i;
+    const int64_t qq = base + o;
+    const double* v = s0 + o;
+    const double r = (som && on_sommerfeld_face(g, b, i, j, k))
+                         ? sommerfeld_value<false>(g, P, b, n, v, i, j, k, sst)
+                         : add_ko_slab(__ldg(rhs + qq), v, nn0, pl, F, P.p.diss);
+    const double un = *v;
+    double v1 = w.u1_zero ? 0.0 : u1[qq];
+    if (w.delta != 0.0) v1 += w.delta * un;  // w0 == 1, w2 == 0 branch
+    double x;
+    if (w.gamma1 == 1.0) {  // gamma3 == 0 for every 2S integrator accepted
+      x = un;
+      if (w.gamma2 != 0.0) x += w.gamma2 * v1;
+    } else if (w.gamma1 == 0.0) {
+      if (w.gamma2 == 1.0) x = v1;
+      else x = w.gamma2 * v1;
+    } else {
+      if (w.gamma2 != 0.0) x = w.gamma1 * un + w.gamma2 * v1;
+      else x = un * w.gamma1;
+    }
+    x += w.beta_dt * r;
+    u1[qq] = v1;
+    u_out[qq] = x;
+  }
+}
+
+// KO + Butcher stage (k_ko_stage_bt) from a shared-memory slab.
+template <bool SOM>
+__global__ void __launch_bounds__(kColumnMaxThreads)
+k_ko_stage_bt_slab(Grid g, DevParams P, const double* __restrict__ u,
+                   const double* __restrict__ rhs, const double* __restrict__ un_reg, KPtrs K,
+                   double* __restrict__ u_out, BtStage w, SlabGeom S, int block0) {
+  extern __shared__ double sm[];
+  const int n = (int)blockIdx.y, b = block0 + (int)blockIdx.z;
+  int kl, kh;
+  slab_range(g, S, kl, kh);
+  if (kl > kh) return;
+  const int nn0 = g.nn[0], pl = S.plane;
+  const int64_t base = ((int64_t)b * NVAR + n) * g.nvol;
+  slab_load(sm, u + base, kl, kh, pl);
+  const double* s0 = sm - (int64_t)(kl - NG) * pl;
+  const FdScale& F = P.fd[b];
+  const bool som = SOM && sommerfeld_var(n);
+  const int64_t sst[3] = {1, nn0, pl};
+  const int n0 = g.nx[0] + 1, n1 = g.nx[1] + 1, nk = kh - kl + 1;
+  for (int q = threadIdx.x; q < n0 * n1 * nk; q += blockDim.x) {
+    const int i = NG + q % n0, j = NG + (q / n0) % n1, k = kl + q / (n0 * n1);
+    const int o = k * pl + j * nn0 + i;
+    const int64_t qq = base + o;
+    const double* v = s0 + o;
+    const double r = (som && on_sommerfeld_face(g, b, i, j, k))
+                         ? sommerfeld_value<false>(g, P, b, n, v, i, j, k, sst)
+                         : add_ko_slab(__ldg(rhs + qq), v, nn0, pl, F, P.p.diss);
+    K.k[w.kslot][qq] = r;
+    double x = __ldg(un_reg + qq);
+    for (int sidx_ = 0; sidx_ < w.nq; ++sidx_) {
+      if (w.coef[sidx_] != 0.0) {
+        const double ks = (sidx_ == w.kslot) ? r : K.k[sidx_][qq];
+        x += w.coef[sidx_] * ks;
+      }
+    }
+    u_out[qq] = x;
+  }
+}
+
+// Z4cRHS tail (k_ko_rhs) from a shared-memory slab: rhs += KO, in place.
+__global__ void __launch_bounds__(kColumnMaxThreads)
+k_ko_rhs_slab(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ rhs,
+              SlabGeom S, int block0) {
+  extern __shared__ double sm[];
+  const int n = (int)blockIdx.y, b = block0 + (int)blockIdx.z;
+  int kl, kh;
+  slab_range(g, S, kl, kh);
+  if (kl > kh) return;
+  const int nn0 = g.nn[0], pl = S.plane;
+  const int64_t base = ((int64_t)b * NVAR + n) * g.nvol;
+  slab_load(sm, u + base, kl, kh, pl);
+  const double* s0 = sm - (int64_t)(kl - NG) * pl;
+  const FdScale& F = P.fd[b];
+  const int n0 = g.nx[0] + 1, n1 = g.nx[1] + 1, nk = kh - kl + 1;
+  for (int q = threadIdx.x; q < n0 * n1 * nk; q += blockDim.x) {
+    const int i = NG + q % n0, j = NG + (q / n0) % n1, k = kl + q / (n0 * n1);
+    const int o = k * pl + j * nn0 + i;
+    rhs[base + o] = add_ko_slab(rhs[base + o], s0 + o, nn0, pl, F, P.p.diss);
   }
 }
 
@@ -930,7 +1143,45 @@ bool valid_shape(const LaunchShape& sh) {
   return (sh.point_threads == 64 || sh.point_threads == 128 || sh.point_threads == 256) &&
          (sh.column_threads == 128 || sh.column_threads == 256 ||
           sh.column_threads == 512) &&
-         (sh.column_unroll == 2 || sh.column_unroll == 4);
+         (sh.column_slabs >= 0 && sh.column_slabs <= 4);
+}
+
+// Shared-memory slab geometry of a shape, or kper = 0 when the per-variable
+// passes run as pencils (column_slabs = 0, or planes that do not fit).
+constexpr int kSlabMaxBytes = 200 * 1024;
+static SlabGeom slab_geom(const Grid& g, const LaunchShape& sh, size_t* bytes) {
+  SlabGeom S{0, g.nn[0] * g.nn[1]};
+  *bytes = 0;
+  if (sh.column_slabs <= 0) return S;
+  const int nk = g.nx[2] + 1;
+  const int kper = (nk + sh.column_slabs - 1) / sh.column_slabs;
+  const size_t b = sizeof(double) * (size_t)(kper + 2 * NG) * S.plane;
+  if (b > (size_t)kSlabMaxBytes) return S;
+  S.kper = kper;
+  *bytes = b;
+  return S;
+}
+bool slabs_fit(const Grid& g, const LaunchShape& sh) {
+  size_t b;
+  return slab_geom(g, sh, &b).kper > 0;
+}
+// Lets every slab kernel take up to kSlabMaxBytes of dynamic shared memory.
+// Runs before any launch (at context creation), never inside a captured
+// stream.
+int allow_slab_smem() {
+  cudaError_t e = cudaSuccess;
+  auto set = [&](const void* k) {
+    const cudaError_t r =
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kSlabMaxBytes);
+    if (e == cudaSuccess) e = r;
+  };
+  set((const void*)k_adv_prep_slab);
+  set((const void*)k_ko_rhs_slab);
+  set((const void*)k_ko_stage_ls_slab<true>);
+  set((const void*)k_ko_stage_ls_slab<false>);
+  set((const void*)k_ko_stage_bt_slab<true>);
+  set((const void*)k_ko_stage_bt_slab<false>);
+  return (int)e;
 }
 
 template <int T>
@@ -960,37 +1211,58 @@ static void launch_point_pass(const Grid& g, const DevParams& P, const double* u
 static void launch_rhs_passes(const Grid& g, const DevParams& P, const double* u,
                               const RhsScratch& sc, double* rhs, int block0, int nblk,
                               const LaunchShape& sh, cudaStream_t st) {
-  const int64_t cprep = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7);  // widest component region
-  COUNTED
-  k_prep<<<dim3(div_up(cprep, kPointThreads), kSdComponents, nblk), kPointThreads, 0, st>>>(
-      g, P, u, sc.sd, block0);
-  launch_point_pass(g, P, u, sc, rhs, block0, nblk, 0, sh, st);
-  const int ct = sh.column_threads, cb = div_up(columns(g, nblk), ct);
-  COUNTED
-  if (sh.column_unroll == 2) k_adv<2><<<cb, ct, 0, st>>>(g, P, u, sc.lv, block0, nblk);
-  else k_adv<4><<<cb, ct, 0, st>>>(g, P, u, sc.lv, block0, nblk);
+  size_t smem;
+  const SlabGeom S = slab_geom(g, sh, &smem);
+  const int ct = sh.column_threads;
+  if (S.kper > 0) {
+    // advection sums and stored first derivatives from shared-memory slabs
+    const dim3 grid((g.nx[2] + S.kper) / S.kper, NVAR, nblk);
+    COUNTED
+    k_adv_prep_slab<<<grid, ct, smem, st>>>(g, P, u, sc.lv, sc.sd, S, block0);
+    launch_point_pass(g, P, u, sc, rhs, block0, nblk, 0, sh, st);
+  } else {
+    const int64_t cprep = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7);  // widest component region
+    COUNTED
+    k_prep<<<dim3(div_up(cprep, kPointThreads), kSdComponents, nblk), kPointThreads, 0, st>>>(
+        g, P, u, sc.sd, block0);
+    launch_point_pass(g, P, u, sc, rhs, block0, nblk, 0, sh, st);
+    COUNTED
+    k_adv<4><<<div_up(columns(g, nblk), ct), ct, 0, st>>>(g, P, u, sc.lv, block0, nblk);
+  }
   launch_point_pass(g, P, u, sc, rhs, block0, nblk, 1, sh, st);
 }
 
 void launch_rhs(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                 double* rhs, int block0, int nblk, const LaunchShape& sh, cudaStream_t st) {
   launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, sh, st);
-  const int ct = sh.column_threads, cb = div_up(columns(g, nblk), ct);
+  size_t smem;
+  const SlabGeom S = slab_geom(g, sh, &smem);
+  const int ct = sh.column_threads;
   COUNTED
-  if (sh.column_unroll == 2) k_ko_rhs<2><<<cb, ct, 0, st>>>(g, P, u, rhs, block0, nblk);
-  else k_ko_rhs<4><<<cb, ct, 0, st>>>(g, P, u, rhs, block0, nblk);
+  if (S.kper > 0) {
+    k_ko_rhs_slab<<<dim3((g.nx[2] + S.kper) / S.kper, NVAR, nblk), ct, smem, st>>>(g, P, u, rhs,
+                                                                                 S, block0);
+  } else {
+    k_ko_rhs<4><<<div_up(columns(g, nblk), ct), ct, 0, st>>>(g, P, u, rhs, block0, nblk);
+  }
 }
 
 void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                      double* rhs, double* u1, double* u_out, const LsStage& w, int block0,
                      int nblk, const LaunchShape& sh, cudaStream_t st) {
   launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, sh, st);
-  COUNTED
-  auto kern = (sh.column_unroll == 2)
-                  ? (g.has_sommerfeld ? k_ko_stage_ls<2, true> : k_ko_stage_ls<2, false>)
-                  : (g.has_sommerfeld ? k_ko_stage_ls<4, true> : k_ko_stage_ls<4, false>);
+  size_t smem;
+  const SlabGeom S = slab_geom(g, sh, &smem);
   const int ct = sh.column_threads;
-  kern<<<div_up(columns(g, nblk), ct), ct, 0, st>>>(g, P, u, rhs, u1, u_out, w, block0, nblk);
+  COUNTED
+  if (S.kper > 0) {
+    auto kern = g.has_sommerfeld ? k_ko_stage_ls_slab<true> : k_ko_stage_ls_slab<false>;
+    kern<<<dim3((g.nx[2] + S.kper) / S.kper, NVAR, nblk), ct, smem, st>>>(g, P, u, rhs, u1, u_out,
+                                                                        w, S, block0);
+  } else {
+    auto kern = g.has_sommerfeld ? k_ko_stage_ls<4, true> : k_ko_stage_ls<4, false>;
+    kern<<<div_up(columns(g, nblk), ct), ct, 0, st>>>(g, P, u, rhs, u1, u_out, w, block0, nblk);
+  }
 }
 
 void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
@@ -1000,12 +1272,19 @@ void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const R
   launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, sh, st);
   KPtrs K;
   for (int s = 0; s < 4; ++s) K.k[s] = k[s];
-  COUNTED
-  auto kern = (sh.column_unroll == 2)
-                  ? (g.has_sommerfeld ? k_ko_stage_bt<2, true> : k_ko_stage_bt<2, false>)
-                  : (g.has_sommerfeld ? k_ko_stage_bt<4, true> : k_ko_stage_bt<4, false>);
+  size_t smem;
+  const SlabGeom S = slab_geom(g, sh, &smem);
   const int ct = sh.column_threads;
-  kern<<<div_up(columns(g, nblk), ct), ct, 0, st>>>(g, P, u, rhs, un, K, u_out, w, block0, nblk);
+  COUNTED
+  if (S.kper > 0) {
+    auto kern = g.has_sommerfeld ? k_ko_stage_bt_slab<true> : k_ko_stage_bt_slab<false>;
+    kern<<<dim3((g.nx[2] + S.kper) / S.kper, NVAR, nblk), ct, smem, st>>>(g, P, u, rhs, un, K,
+                                                                        u_out, w, S, block0);
+  } else {
+    auto kern = g.has_sommerfeld ? k_ko_stage_bt<4, true> : k_ko_stage_bt<4, false>;
+    kern<<<div_up(columns(g, nblk), ct), ct, 0, st>>>(g, P, u, rhs, un, K, u_out, w, block0,
+                                                      nblk);
+  }
 }
 
 // Slot of every direction in the neighbour list (mesh_topology.cpp:329-960

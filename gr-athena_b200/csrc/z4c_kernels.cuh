@@ -64,14 +64,22 @@ struct RhsScratch {
 constexpr int kSdComponents = 33;
 
 // Launch shape of the right-hand-side passes: threads per CTA of the heavy
-// per-vertex passes (64, 128, 256), threads per CTA of the column passes
-// (128, 256, 512) and the k-loop unroll of the column passes (2, 4).
+// per-vertex passes (64, 128, 256), threads per CTA of the per-variable
+// passes (128, 256, 512) and the number of z-slabs per block in which those
+// passes stage a variable in shared memory (1-4; 0 or a slab whose planes do
+// not fit: global-memory pencils instead).
 struct LaunchShape {
   int point_threads = 128;
-  int column_threads = 256;
-  int column_unroll = 4;
+  int column_threads = 128;
+  int column_slabs = 0;
 };
 bool valid_shape(const LaunchShape& sh);
+// Whether the shape's slabs fit in shared memory on this grid.
+bool slabs_fit(const Grid& g, const LaunchShape& sh);
+// Raises the dynamic shared-memory limit of the slab kernels (call once per
+// device before the first launch, outside stream capture); returns a
+// cudaError_t value.
+int allow_slab_smem();
 
 // Every RHS launch runs five kernels: stored first derivatives, Ricci pass,
 // advection sums, main pass (into rhs, without Kreiss-Oliger), then

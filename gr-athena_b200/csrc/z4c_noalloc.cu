@@ -71,6 +71,16 @@ int scratch_for_current_device(double** out) {
       return set_error(Z4C_ECUDA, buf);
     }
     g_scratch_addr[dev] = static_cast<double*>(p);
+    // the slab kernels launched by the right-hand side take more than the
+    // default 48 kB of dynamic shared memory
+    e = static_cast<cudaError_t>(allow_slab_smem());
+    if (e != cudaSuccess) {
+      char buf[160];
+      snprintf(buf, sizeof(buf), "z4c_rhs_noalloc: shared-memory limit: %s",
+               cudaGetErrorString(e));
+      g_scratch_addr[dev] = nullptr;
+      return set_error(Z4C_ECUDA, buf);
+    }
   }
   *out = g_scratch_addr[dev];
   return Z4C_OK;

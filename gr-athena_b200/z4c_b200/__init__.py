@@ -342,9 +342,10 @@ class Z4c:
     def set_per_block(self, flag):
         _check(lib().z4c_set_per_block(self._h, int(bool(flag))))
 
-    def set_tile(self, point_threads, column_threads, column_unroll):
+    def set_tile(self, point_threads, column_threads, column_slabs):
+        """Launch shape of the RHS passes (see z4c_set_tile)."""
         _check(lib().z4c_set_tile(self._h, int(point_threads), int(column_threads),
-                                  int(column_unroll)))
+                                  int(column_slabs)))
 
     def get_tile(self):
         t = (C.c_int * 3)()

@@ -236,9 +236,12 @@ int z4c_fp64_probe(z4c_ctx *ctx, double *tflops);
 int z4c_set_per_block(z4c_ctx *ctx, int per_block);
 /* Launch shape of the right-hand-side passes (no reference counterpart):
  * tile = {threads per CTA of the per-vertex Ricci and main passes (64, 128,
- * 256), threads per CTA of the per-variable column passes (128, 256, 512),
- * k-loop unroll of the column passes (2, 4)}.  The default is {128, 256, 4};
- * unsupported shapes return Z4C_EINVAL.  Results do not depend on the shape. */
+ * 256), threads per CTA of the per-variable passes (advection, stored first
+ * derivatives, Kreiss-Oliger + stage update: 128, 256, 512), z-slabs per
+ * MeshBlock in which those passes stage one variable in shared memory (1-4;
+ * 0, or slabs whose vertex planes do not fit, selects global-memory
+ * pencils)}.  The default is {128, 128, 0}; unsupported shapes return
+ * Z4C_EINVAL.  Results do not depend on the shape. */
 int z4c_set_tile(z4c_ctx *ctx, int ti, int tj, int tk);
 int z4c_get_tile(const z4c_ctx *ctx, int tile_out[3]);
 /* Autotuner (no reference counterpart): times one fused low-storage stage on

@@ -124,7 +124,7 @@ def test_launch_shapes_and_autotuner_leave_results_unchanged():
     u0 = puncture_state(Z, ctx)
     dt = 0.25 * float(ctx.dx().min())
     ref = None
-    for shape in [(128, 256, 4), (64, 128, 2), (256, 512, 4), (128, 512, 2)]:
+    for shape in [(128, 256, 2), (64, 128, 0), (256, 512, 1), (128, 512, 3), (128, 128, 4)]:
         ctx.set_tile(*shape)
         assert ctx.get_tile() == shape
         ctx.upload(Z.REG_U, u0)
@@ -135,11 +135,11 @@ def test_launch_shapes_and_autotuner_leave_results_unchanged():
         assert np.array_equal(out, ref), shape
     ctx.upload(Z.REG_U, u0)
     shape, ms = ctx.autotune(reps=2)
-    assert shape[0] in (64, 128, 256) and shape[1] in (128, 256, 512) and shape[2] in (2, 4)
+    assert shape[0] in (64, 128, 256) and shape[1] in (128, 256, 512) and 0 <= shape[2] <= 4
     assert ms > 0
     assert np.array_equal(ctx.download(Z.REG_U), u0)
     ctx.evolve(dt, 1)
     assert np.array_equal(ctx.download(Z.REG_U), ref)
     with pytest.raises(Z.Z4cError):
-        ctx.set_tile(100, 256, 4)
+        ctx.set_tile(100, 256, 2)
     ctx.close()
