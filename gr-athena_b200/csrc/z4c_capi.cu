@@ -116,6 +116,8 @@ struct z4c_ctx {
   FdScale* fd = nullptr;  // [nblocks]
   int* nbr = nullptr;     // [nblocks][26]
   double* partials = nullptr;
+  double* trk = nullptr;  // puncture trackers [kMaxTrackers][8]
+  int ntrk = 0;
   int* flag = nullptr;
 
   // host copies
@@ -195,7 +197,27 @@ int exchange_into(z4c_ctx* c, const double* src, double* dst, bool alg) {
 // One GR_Z4c stage on all blocks.  Batched: fused RHS+KO+stage kernel
 // (u -> w interior), then exchange(+AlgConstr) w -> u.  Per-block: the plain
 // operator sequence with one RHS launch per block.
+int run_stage_body(z4c_ctx* c, int stage, double dt);
+
+// One stage with the puncture trackers around it: the shift is interpolated
+// from the state at the start of the step (CalculateZ4cRHS, stage 1,
+// task_list_gr_z4c.cpp:147-153) and the positions move after the last stage
+// (EvolveTracker, main.hpp:1079-1082).
 int run_stage(z4c_ctx* c, int stage, double dt) {
+  if (c->ntrk > 0 && stage == 1) {
+    launch_track_interp(c->g, c->dev(), c->reg[Z4C_REG_U], c->trk, c->ntrk, c->stream);
+    LAUNCH_CHECK("tracker interpolation");
+  }
+  int rc = run_stage_body(c, stage, dt);
+  if (rc) return rc;
+  if (c->ntrk > 0 && stage == 4) {
+    launch_track_update(c->trk, c->ntrk, dt, c->stream);
+    LAUNCH_CHECK("tracker update");
+  }
+  return Z4C_OK;
+}
+
+int run_stage_body(z4c_ctx* c, int stage, double dt) {
   const DevParams P = c->dev();
   const Grid& g = c->g;
   double* u = c->reg[Z4C_REG_U];
@@ -279,7 +301,7 @@ void free_ctx(z4c_ctx* c) {
   for (auto& r : c->reg)
     if (r) cudaFree(r);
   for (void* p : {(void*)c->un, (void*)c->guu, (void*)c->sd, (void*)c->rsum, (void*)c->lv, (void*)c->xf, (void*)c->xv, (void*)c->dxd, (void*)c->fd,
-                  (void*)c->nbr, (void*)c->partials, (void*)c->flag})
+                  (void*)c->nbr, (void*)c->partials, (void*)c->flag, (void*)c->trk})
     if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -453,6 +475,7 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
   if (rc == Z4C_OK) rc = alloc((void**)&c->nbr, sizeof(int) * hnbr.size());
   if (rc == Z4C_OK) rc = alloc((void**)&c->partials, sizeof(double) * 8 * nb);
   if (rc == Z4C_OK) rc = alloc((void**)&c->flag, sizeof(int));
+  if (rc == Z4C_OK) rc = alloc((void**)&c->trk, sizeof(double) * 8 * kMaxTrackers);
   if (rc != Z4C_OK) {
     free_ctx(c);
     return rc;
@@ -960,6 +983,30 @@ int z4c_evolve(z4c_ctx* ctx, double dt, int nsteps, int with_constraints) {
 }
 
 long long z4c_kernel_launches(void) { return kernel_launch_count(); }
+
+int z4c_tracker_add(z4c_ctx* ctx, const double pos[3], int* id) {
+  if (!ctx || !pos || !id) return fail(Z4C_EINVAL, "null argument");
+  if (ctx->ntrk >= kMaxTrackers) return fail(Z4C_EINVAL, "at most %d trackers", kMaxTrackers);
+  const double rec[8] = {pos[0], pos[1], pos[2], NAN, NAN, NAN, 0.0, 0.0};
+  CUDA_TRY(cudaMemcpyAsync(ctx->trk + 8 * ctx->ntrk, rec, sizeof(rec), cudaMemcpyHostToDevice,
+                           ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  *id = ctx->ntrk++;
+  drop_graph(ctx);  // the captured step must include the new tracker
+  return Z4C_OK;
+}
+
+int z4c_tracker_get(z4c_ctx* ctx, int id, double out[6]) {
+  if (!ctx || !out) return fail(Z4C_EINVAL, "null argument");
+  if (id < 0 || id >= ctx->ntrk) return fail(Z4C_EINVAL, "no tracker %d", id);
+  double rec[8];
+  CUDA_TRY(cudaMemcpyAsync(rec, ctx->trk + 8 * id, sizeof(rec), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  for (int q = 0; q < 6; ++q) out[q] = rec[q];
+  if (rec[6] != 0.0) return fail(Z4C_ESTATE, "puncture %d has left the grid", id);
+  return Z4C_OK;
+}
 
 int z4c_check_finite(z4c_ctx* ctx, int reg) {
   if (!ctx) return fail(Z4C_EINVAL, "null context");

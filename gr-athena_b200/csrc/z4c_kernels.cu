@@ -688,6 +688,95 @@ k_main(Grid g, DevParams P, const double* __restrict__ u, const double* __restri
   for (int n = 0; n < NVAR; ++n) rb[(int64_t)n * g.nvol] = out[n];
 }
 
+// ---- puncture tracker (z4c/puncture_tracker.cpp) ----------------------------
+// Tracker record: pos[3], betap[3], lost flag, padding (8 doubles).
+// LagrangeInterp1D<2*NGHOST-1> (utils/lagrange_interp.hpp:33-146): first
+// stencil point and the 8 coefficients, in the reference's operation order.
+constexpr int kTrkOrder = 2 * NG - 1;
+__device__ int trk_lagrange1d(double origin, double delta, int siz, double coord,
+                              double coeff[kTrkOrder + 1]) {
+  const double delta_inv = 1.0 / delta;
+  int point = __double2int_rn(floor((coord - origin) * delta_inv - 0.5 * (kTrkOrder - 1)));
+  int shift = point;
+  if (shift < 0) point -= shift;
+  shift = point + kTrkOrder - (siz - 1);
+  if (shift > 0) point -= shift;
+  double xp[kTrkOrder + 1];
+  for (int i = 0; i <= kTrkOrder; ++i) xp[i] = (point + i) * delta + origin;
+  for (int j = 0; j <= kTrkOrder; ++j) {
+    double num = 1.0, den = 1.0;
+    for (int i = 0; i <= kTrkOrder; ++i) {
+      if (i == j) continue;
+      num = num * (coord - xp[i]);
+      den = den * (xp[j] - xp[i]);
+    }
+    coeff[j] = num / den;
+  }
+  return point;
+}
+
+// PunctureTracker::InterpolateShift (:95-129): one thread per tracker finds
+// the block that holds the puncture exclusively (MeshBlock::
+// PointContainedExclusive, mesh/meshblock.cpp:1186-1201) and interpolates
+// the shift there (LagrangeInterpND: x innermost, then y, then z).
+__global__ void k_track_interp(Grid g, DevParams P, const double* __restrict__ u,
+                               double* __restrict__ trk, int ntrk) {
+  const int t = (int)threadIdx.x;
+  if (t >= ntrk) return;
+  double* T = trk + 8 * t;
+  const double pos[3] = {T[0], T[1], T[2]};
+  const int nsum = g.nn[0] + g.nn[1] + g.nn[2];
+  int owner = -1;
+  for (int b = 0; b < g.nblocks && owner < 0; ++b) {
+    const double* x = P.xf + (int64_t)b * nsum;
+    bool in = true;
+    int off = 0;
+    for (int a = 0; a < 3; ++a) {
+      in = in && (x[off + NG] <= pos[a]) && (pos[a] < x[off + NG + g.nx[a]]);
+      off += g.nn[a];
+    }
+    if (in) owner = b;
+  }
+  if (owner < 0) {  // the puncture has left the grid
+    T[6] = 1.0;
+    return;
+  }
+  const double* x = P.xf + (int64_t)owner * nsum;
+  double c[3][kTrkOrder + 1];
+  int pt[3], off = 0;
+  for (int a = 0; a < 3; ++a) {
+    pt[a] = trk_lagrange1d(x[off], P.dx[(int64_t)owner * 3 + a], g.nn[a], pos[a], c[a]);
+    off += g.nn[a];
+  }
+  for (int v = 0; v < 3; ++v) {
+    const double* f = u + ((int64_t)owner * NVAR + Z4C_BETAX + v) * g.nvol;
+    double vz[kTrkOrder + 1];
+    for (int ez = 0; ez <= kTrkOrder; ++ez) {
+      double vy[kTrkOrder + 1];
+      for (int ey = 0; ey <= kTrkOrder; ++ey) {
+        const double* row = f + ((int64_t)(pt[2] + ez) * g.nn[1] + (pt[1] + ey)) * g.nn[0] + pt[0];
+        double o = 0;
+        for (int i = 0; i <= kTrkOrder; ++i) o += c[0][i] * row[i];
+        vy[ey] = o;
+      }
+      double o = 0;
+      for (int i = 0; i <= kTrkOrder; ++i) o += c[1][i] * vy[i];
+      vz[ez] = o;
+    }
+    double o = 0;
+    for (int i = 0; i <= kTrkOrder; ++i) o += c[2][i] * vz[i];
+    T[3 + v] = o;
+  }
+}
+
+// PunctureTracker::EvolveTracker (:132-186): pos -= dt * betap.
+__global__ void k_track_update(double* __restrict__ trk, int ntrk, double dt) {
+  const int t = (int)threadIdx.x;
+  if (t >= ntrk) return;
+  double* T = trk + 8 * t;
+  for (int a = 0; a < 3; ++a) T[a] -= dt * T[3 + a];
+}
+
 // ---- same-level vertex-centred ghost exchange -------------------------------
 // CommRegistry::SetBoundaries (comm/comm_registry.cpp:336-382): ghosts are
 // zeroed, every neighbour whose set range (comm/index_utilities.hpp:155-163)
@@ -1302,6 +1391,16 @@ static int upload_dir_index() {
   for (int d = 0; d < 26; ++d)
     h[(dirs[d][0] + 1) + 3 * (dirs[d][1] + 1) + 9 * (dirs[d][2] + 1)] = d;
   return (int)cudaMemcpyToSymbol(c_dir_index, h, sizeof(h));
+}
+
+void launch_track_interp(const Grid& g, const DevParams& P, const double* u, double* trk,
+                         int ntrk, cudaStream_t st) {
+  COUNTED
+  k_track_interp<<<1, 32, 0, st>>>(g, P, u, trk, ntrk);
+}
+void launch_track_update(double* trk, int ntrk, double dt, cudaStream_t st) {
+  COUNTED
+  k_track_update<<<1, 32, 0, st>>>(trk, ntrk, dt);
 }
 
 void launch_boundary_rhs(const Grid& g, const DevParams& P, const double* u, double* rhs,

@@ -97,6 +97,12 @@ void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const R
                      cudaStream_t st);
 // Ghost exchange of a 22-variable register: src (pre-exchange) -> dst (all
 // vertices); src and dst must differ.
+// Puncture trackers (records of 8 doubles: pos, betap, lost flag): the
+// shift interpolated at each puncture, and pos -= dt * betap.
+constexpr int kMaxTrackers = 8;
+void launch_track_interp(const Grid& g, const DevParams& P, const double* u, double* trk,
+                         int ntrk, cudaStream_t st);
+void launch_track_update(double* trk, int ntrk, double dt, cudaStream_t st);
 // Z4c::Z4cBoundaryRHS: Sommerfeld right-hand side on gr_sommerfeld faces.
 void launch_boundary_rhs(const Grid& g, const DevParams& P, const double* u, double* rhs,
                          int block0, int nblk, cudaStream_t st);

@@ -49,7 +49,7 @@ EXPORTS = (
     "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_ghost_fill", "z4c_init_finalize",
     "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
     "z4c_get_tile", "z4c_autotune", "z4c_check_finite", "z4c_kernel_launches", "z4c_rhs_stage",
-    "z4c_fp64_probe", "z4c_vc_restrict", "z4c_vc_prolongate", "z4c_rhs_noalloc")
+    "z4c_fp64_probe", "z4c_tracker_add", "z4c_tracker_get", "z4c_vc_restrict", "z4c_vc_prolongate", "z4c_rhs_noalloc")
 
 
 class Z4cError(RuntimeError):
@@ -127,6 +127,8 @@ def lib():
         L.z4c_rhs_stage.argtypes = [vp, ip, C.c_double]
         L.z4c_fp64_probe.argtypes = [vp, dp]
         ipp = C.POINTER(C.c_int)
+        L.z4c_tracker_add.argtypes = [vp, dp, ipp]
+        L.z4c_tracker_get.argtypes = [vp, ip, dp]
         L.z4c_vc_restrict.argtypes = [vp, vp, ip, ip, ipp, ipp, vp]
         L.z4c_vc_prolongate.argtypes = [vp, vp, ip, ip, ipp, ipp, vp]
         L.z4c_rhs_noalloc.argtypes = [vp, vp, ip, C.POINTER(C.c_int), dp,
@@ -358,6 +360,19 @@ class Z4c:
         ms = C.c_float()
         _check(lib().z4c_autotune(self._h, int(reps), C.byref(ms)))
         return self.get_tile(), ms.value
+
+    def add_tracker(self, pos):
+        """PunctureTracker at pos; returns its id."""
+        p = (C.c_double * 3)(*[float(v) for v in pos])
+        i = C.c_int()
+        _check(lib().z4c_tracker_add(self._h, p, C.byref(i)))
+        return i.value
+
+    def tracker(self, tid):
+        """(position, interpolated shift) of a tracker."""
+        out = np.empty(6)
+        _check(lib().z4c_tracker_get(self._h, int(tid), out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out[:3], out[3:]
 
     def hst_norms(self):
         out = np.empty(8)

@@ -251,6 +251,16 @@ int z4c_get_tile(const z4c_ctx *ctx, int tile_out[3]);
  * work register, u1 and rhs (u is untouched); call it between steps.
  * *best_ms (may be NULL) receives the stage time of the chosen shape. */
 int z4c_autotune(z4c_ctx *ctx, int reps, float *best_ms);
+/* PunctureTracker (z4c/puncture_tracker.cpp): adds a tracker at pos; every
+ * following step interpolates the shift at the tracker from the state at the
+ * start of the step (InterpolateShift, :95-129, 8-point Lagrange stencils)
+ * and moves it, pos -= dt * shift (EvolveTracker, :132-186).  At most 8
+ * trackers; adding one drops the captured step graph. */
+int z4c_tracker_add(z4c_ctx *ctx, const double pos[3], int *id);
+/* Position and interpolated shift of tracker id: out = {x, y, z, beta^x,
+ * beta^y, beta^z} (the columns of WriteTracker, :189-203).  Z4C_ESTATE when
+ * the puncture has left every MeshBlock. */
+int z4c_tracker_get(z4c_ctx *ctx, int id, double out[6]);
 /* Kernels launched by this library in this process so far (graph replays
  * count every kernel node); a diagnostic with no reference counterpart. */
 long long z4c_kernel_launches(void);

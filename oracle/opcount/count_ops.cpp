@@ -59,6 +59,8 @@ inline CReal cbrt(CReal a) { ++opcount::fn; return CReal(std::cbrt(a.v)); }
 inline CReal pow(CReal a, CReal b) { ++opcount::fn; return CReal(std::pow(a.v, b.v)); }
 inline CReal pow(int a, int b) { return CReal(std::pow((double)a, (double)b)); }
 inline int isfinite(CReal a) { return std::isfinite(a.v); }
+inline CReal floor(CReal a) { return CReal(std::floor(a.v)); }
+inline long lrint(CReal a) { return std::lrint(a.v); }
 
 #define double CReal
 #include "../z4c_oracle.c"

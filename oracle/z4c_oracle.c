@@ -1309,6 +1309,61 @@ void orc_vc_prolongate(const int nx[3], int nvar, const double *coarse, double *
 #undef FI
 }
 
+/* ---- puncture tracker, z4c/puncture_tracker.cpp:95-129 ------------------ */
+
+/* LagrangeInterp1D<7> (utils/lagrange_interp.hpp:33-146), odd order: first
+ * stencil point and the coefficients of the 8-point stencil. */
+#define TRK_ORDER (2 * NG - 1)
+static int lagrange1d(double origin, double delta, int siz, double coord, double coeff[]) {
+  const double delta_inv = 1.0 / delta;
+  int point = (int)lrint(floor((coord - origin) * delta_inv - 0.5 * (TRK_ORDER - 1)));
+  int shift = point;
+  if (shift < 0) point -= shift;
+  shift = point + TRK_ORDER - (siz - 1);
+  if (shift > 0) point -= shift;
+  double xp[TRK_ORDER + 1];
+  for (int i = 0; i <= TRK_ORDER; ++i) xp[i] = (point + i) * delta + origin;
+  for (int j = 0; j <= TRK_ORDER; ++j) {
+    double num = 1.0, den = 1.0;
+    for (int i = 0; i <= TRK_ORDER; ++i) {
+      if (i == j) continue;
+      num = num * (coord - xp[i]);
+      den = den * (xp[j] - xp[i]);
+    }
+    coeff[j] = num / den;
+  }
+  return point;
+}
+
+void orc_tracker_interp(const orc_block_t *b, const double *u, const double pos[3],
+                        double beta[3]) {
+  const int nn[3] = {b->nx[0] + 1 + 2 * NG, b->nx[1] + 1 + 2 * NG, b->nx[2] + 1 + 2 * NG};
+  const int64_t nvol = (int64_t)nn[0] * nn[1] * nn[2];
+  double c[3][TRK_ORDER + 1];
+  int pt[3];
+  for (int a = 0; a < 3; ++a) pt[a] = lagrange1d(b->x[a][0], b->dx[a], nn[a], pos[a], c[a]);
+  for (int v = 0; v < 3; ++v) {
+    const double *f = u + (Z4C_BETAX + v) * nvol;
+    /* LagrangeInterpND::m_fill_stencil: x innermost, then y, then z */
+    double vz[TRK_ORDER + 1];
+    for (int ez = 0; ez <= TRK_ORDER; ++ez) {
+      double vy[TRK_ORDER + 1];
+      for (int ey = 0; ey <= TRK_ORDER; ++ey) {
+        const double *row = f + ((int64_t)(pt[2] + ez) * nn[1] + (pt[1] + ey)) * nn[0] + pt[0];
+        double o = 0;
+        for (int i = 0; i <= TRK_ORDER; ++i) o += c[0][i] * row[i];
+        vy[ey] = o;
+      }
+      double o = 0;
+      for (int i = 0; i <= TRK_ORDER; ++i) o += c[1][i] * vy[i];
+      vz[ez] = o;
+    }
+    double o = 0;
+    for (int i = 0; i <= TRK_ORDER; ++i) o += c[2][i] * vz[i];
+    beta[v] = o;
+  }
+}
+
 /* ---- history sums, outputs/history.cpp:168-200 --------------------------- */
 void orc_hst_accumulate(const orc_block_t *b, const z4c_params_t *opt,
                         const double *con, const double *u, double out[8]) {

@@ -98,6 +98,14 @@ void orc_vc_restrict(const int nx[3], int nvar, const double *fine, double *coar
 void orc_vc_prolongate(const int nx[3], int nvar, const double *coarse, double *fine,
                        const int box[6]);
 
+/* ---- puncture tracker (z4c/puncture_tracker.cpp) ------------------------ */
+
+/* PunctureTracker::InterpolateShift (:95-129): the shift of block b at pos
+ * by LagrangeInterpND<2*NGHOST-1, 3> (utils/lagrange_interp.hpp), origin the
+ * block's first vertex, spacing dx.  pos must lie in the block. */
+void orc_tracker_interp(const orc_block_t *b, const double *u, const double pos[3],
+                        double beta[3]);
+
 /* ---- uniform block grid (single level) ---------------------------------- */
 
 /* A uniform mesh of nb[0]*nb[1]*nb[2] blocks, block (l0,l1,l2) at index

@@ -78,6 +78,7 @@ def lib():
         L.orc_rhs.argtypes = [bp, pp, dp, Dp, dp]
         L.orc_boundary_rhs.argtypes = [bp, dp, dp, C.POINTER(C.c_int)]
         L.orc_algconstr.argtypes = [bp, pp, dp]
+        L.orc_tracker_interp.argtypes = [bp, dp, dp, dp]
         ip6 = C.POINTER(C.c_int)
         L.orc_vc_restrict.argtypes = [ip6, C.c_int, dp, dp, ip6]
         L.orc_vc_prolongate.argtypes = [ip6, C.c_int, dp, dp, ip6]
@@ -286,3 +287,19 @@ def vc_prolongate(nx, coarse, fine, box):
     lib().orc_vc_prolongate((C.c_int * 3)(*nx), coarse.shape[0], _ptr(coarse), _ptr(fine),
                             (C.c_int * 6)(*[int(b) for b in box]))
     return fine
+
+
+# ---- puncture tracker (z4c/puncture_tracker.cpp) ----
+
+def tracker_interp(blk, u, pos):
+    """PunctureTracker::InterpolateShift in the block blk (pos inside it)."""
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    p = np.ascontiguousarray(pos, dtype=np.float64)
+    out = np.zeros(3)
+    lib().orc_tracker_interp(C.byref(blk._s), _ptr(u), _ptr(p), _ptr(out))
+    return out
+
+
+def contains_exclusive(blk, pos):
+    """MeshBlock::PointContainedExclusive (mesh/meshblock.cpp:1186-1201)."""
+    return all(blk.xf[a][NG] <= pos[a] < blk.xf[a][NG + blk.nx[a]] for a in range(3))

@@ -76,6 +76,12 @@ EVOL = {
     "somm4": dict(test="one_puncture", z4c=PUNCTURE, integ="rk4", bc="gr_sommerfeld",
                   mesh=[(16, -4.0, 4.0, 8), (16, -4.0, 4.0, 8), (8, -2.0, 2.0, 8)], extra={},
                   problem={"punc_ADM_mass": 1.0}, nlim=8),
+    # the puncture of punc4 with a puncture tracker started off the origin
+    # (z4c/puncture_tracker.cpp), 10 steps; the tracker file is recorded
+    "track4": dict(test="one_puncture", z4c=PUNCTURE, integ="rk4", bc="extrapolate_outflow",
+                   mesh=[(16, -4.0, 4.0, 8), (16, -4.0, 4.0, 8), (8, -2.0, 2.0, 8)],
+                   extra={"npunct": 1, "bh_0_x": 0.37, "bh_0_y": -0.21, "bh_0_z": 0.13},
+                   problem={"punc_ADM_mass": 1.0}, nlim=10, tracker=True),
 }
 BC_CODES = {"periodic": 0, "extrapolate_outflow": 1, "gr_sommerfeld": 2}
 
@@ -104,6 +110,9 @@ def deck(case, out_file, nlim=1, dump_initial="", dump_final="", hst=False):
     lines += ["<driver>", f"out = {out_file}"]
     if hst:
         lines += ["<output1>", "file_type = hst", "dt = 1e-12", "data_format = %.17e"]
+    if case.get("tracker"):
+        lines[lines.index("<task_triggers>") + 1:lines.index("<task_triggers>") + 1] = [
+            "dt_Z4c_tracker_punctures = 1e-12"]
     return "\n".join(lines) + "\n"
 
 
@@ -155,9 +164,15 @@ def make_evol(name, case, outdir):
                        stdout=subprocess.DEVNULL)
         hst = parse_hst(os.path.join(tmp, "golden.hst"))
         r0, r1 = read_records(init), read_records(final)
+        track = None
+        if case.get("tracker"):  # 1:iter 2:time 3:x 4:y 5:z 6:betax 7:betay 8:betaz
+            track = np.loadtxt(os.path.join(tmp, "golden.puncture_0.txt"), ndmin=2)
     out = dict(hst=hst, meta=r0["meta"], xf=r0["xf"], xv=r0["xv"], dx=r0["dx"],
                time_dt=r1["time_dt"], u_init=r0["u"], u_final=r1["u"],
                con_final=r1["con"], nlim=np.array(case["nlim"]))
+    if track is not None:
+        out["tracker"] = track
+        out["tracker_start"] = np.array([case["extra"][f"bh_0_{c}"] for c in "xyz"])
     out.update(meta_json(case))
     path = os.path.join(outdir, f"evol_{name}.npz")
     np.savez_compressed(path, **out)

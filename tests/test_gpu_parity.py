@@ -128,3 +128,19 @@ def test_initial_data_on_device(name):
     assert rel_err(u[I], ref[I]) <= 1e-14
     assert rel_err(u, ref) <= (1e-14 if "gw" in name else 1e-7)
     ctx.close()
+
+
+def test_puncture_tracker_matches_reference():
+    """PunctureTracker on the device (interpolation inside the captured step)
+    against the reference's tracker file, step by step."""
+    c = Case("evol_track4")
+    Z, ctx = make_ctx(c)
+    dt = c.rec["time_dt"][1]
+    ctx.upload(Z.REG_U, c.to_grid(c.rec["u_init"]))
+    tid = ctx.add_tracker(c.rec["tracker_start"])
+    for row in c.rec["tracker"]:
+        ctx.evolve(dt, 1)
+        pos, beta = ctx.tracker(tid)
+        np.testing.assert_allclose(pos, row[2:5], rtol=1e-12, atol=0)
+        np.testing.assert_allclose(beta, row[5:8], rtol=1e-9, atol=1e-15)
+    ctx.close()

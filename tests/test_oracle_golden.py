@@ -133,3 +133,24 @@ def test_vc_refinement_operators():
     for q in range(4):
         out = O.vc_prolongate(nx, coarse.copy(), fine.copy(), z[f"rf_pbox{q}"])
         assert bitwise(out, z[f"rf_prolong{q}"]), q
+
+
+def test_puncture_tracker():
+    """PunctureTracker: the shift interpolated at the puncture at the start of
+    every step, then pos -= dt * beta; matches the reference's tracker file
+    (printed with 16 significant digits) on every step."""
+    c = Case("evol_track4")
+    p = _params(c)
+    blocks = c.blocks()
+    dt = c.rec["time_dt"][1]
+    u = c.rec["u_init"]
+    pos = c.rec["tracker_start"].astype(np.float64).copy()
+    for row in c.rec["tracker"]:
+        owner = [g for g, b in enumerate(blocks) if O.contains_exclusive(b, pos)]
+        assert len(owner) == 1
+        beta = O.tracker_interp(blocks[owner[0]], u[owner[0]], pos)
+        for u in oracle_step(c, p, blocks, u, dt):
+            pass
+        pos = pos - dt * beta
+        got = [float("%.15e" % v) for v in (*pos, *beta)]
+        assert got == [float(v) for v in row[2:8]], row[0]
