@@ -9,6 +9,8 @@
 //   u0                 state after initialisation (all points)
 //   rhs0               Z4cRHS(u0) after PrepareZ4cDerivatives(u0)
 //   brhs0              rhs0 followed by Z4cBoundaryRHS (Sommerfeld faces)
+//   weyl0              with <driver> weyl = true: Z4cWeyl(adm0) (Re, Im psi4)
+//   s<N>_weyl          with <driver> weyl = true: Z4cWeyl after the last stage
 //   alg0               AlgConstr applied to a copy of u0
 //   adm0               Z4cToADM(u0)
 //   con0               ADMConstraints(con, adm0, mat, u0)
@@ -234,6 +236,13 @@ int main(int argc, char* argv[]) {
     z->ADMConstraints(z->storage.con, z->storage.adm, z->storage.mat, z->storage.u);
   }
   d.dump("con0b", Z4c::N_CON, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.con; });
+  if (pin->GetOrAddBoolean("driver", "weyl", false)) {
+    for (auto* b : blocks) {
+      Z4c* z = b->pz4c;
+      z->Z4cWeyl(z->storage.adm, z->storage.mat, z->storage.weyl);
+    }
+    d.dump("weyl0", Z4c::N_WEY, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.weyl; });
+  }
 
   for (size_t g = 0; g < blocks.size(); ++g) {
     Z4c* z = blocks[g]->pz4c;
@@ -319,6 +328,13 @@ int main(int argc, char* argv[]) {
       }
       d.dump(s + "adm", Z4c::N_ADM, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.adm; });
       d.dump(s + "con", Z4c::N_CON, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.con; });
+      if (pin->GetOrAddBoolean("driver", "weyl", false)) {
+        for (auto* b : blocks) {
+          Z4c* z = b->pz4c;
+          z->Z4cWeyl(z->storage.adm, z->storage.mat, z->storage.weyl);
+        }
+        d.dump(s + "weyl", Z4c::N_WEY, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.weyl; });
+      }
     }
   }
   std::cout << "z4c_ops_ref: wrote " << out << std::endl;

@@ -1309,6 +1309,221 @@ void orc_vc_prolongate(const int nx[3], int nvar, const double *coarse, double *
 #undef FI
 }
 
+/* ---- Z4c::Z4cWeyl, z4c/calculate_weyl_scalars.cpp:44-630 ----------------- */
+void orc_weyl(const orc_block_t *b, const z4c_params_t *opt, const double *adm, const double *u,
+              const orc_derivs_t *d, double *weyl) {
+  fd_t f;
+  fd_init(b, &f);
+  const int64_t nvol = orc_nvol(b);
+  for (int64_t q = 0; q < 2 * nvol; ++q) weyl[q] = NAN;
+  const double FR4 = 0.25;
+  const double pw = opt->chi_psi_power;
+#define G3(a, b) V(adm, Z4C_ADM_GXX + SI[a][b])[p]
+#define K3(a, b) V(adm, Z4C_ADM_KXX + SI[a][b])[p]
+#define GT(a, b) V(u, Z4C_GXX + SI[a][b])[p]
+  for (int k = f.kl; k <= f.ku; ++k)
+    for (int j = f.jl; j <= f.ju; ++j)
+      for (int i = f.il; i <= f.iu; ++i) {
+        const int64_t p = P(k, j, i);
+        double ddchi[3][3];
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb) ddchi[a][bb] = d->ddchi[SI[a][bb]][p];
+        const double chi_g = dmax(V(u, Z4C_CHI)[p], opt->chi_div_floor);
+        /* pass 1: physical first derivatives and dK, :150-166 / :224-239 */
+        double dg[3][3][3], dK[3][3][3];
+        for (int c = 0; c < 3; ++c)
+          for (int a = 0; a < 3; ++a)
+            for (int bb = a; bb < 3; ++bb) {
+              double v;
+              if (pw == -4.) {
+                const double oochi = 1.0 / chi_g;
+                v = oochi * (d->dg[c][SI[a][bb]][p] - oochi * GT(a, bb) * d->dchi[c][p]);
+              } else {
+                const double fac = 4.0 / pw;
+                const double psi4 = pow(chi_g, fac);
+                const double oochi = 1.0 / chi_g;
+                v = psi4 * (d->dg[c][SI[a][bb]][p] + fac * oochi * GT(a, bb) * d->dchi[c][p]);
+              }
+              dg[c][a][bb] = dg[c][bb][a] = v;
+              const double dk = Dx(&f, c, V(adm, Z4C_ADM_KXX + SI[a][bb]) + p);
+              dK[c][a][bb] = dK[c][bb][a] = dk;
+            }
+        /* pass 2: physical second derivatives, :169-206 / :242-288 */
+        double ddg[3][3][3][3];
+        for (int c = 0; c < 3; ++c)
+          for (int dd = c; dd < 3; ++dd)
+            for (int a = 0; a < 3; ++a)
+              for (int bb = a; bb < 3; ++bb) {
+                const double dchi_a = d->dchi[a][p], dchi_b = d->dchi[bb][p];
+                const double gtil = GT(c, dd);
+                double v;
+                if (a == bb) {
+                  const double ddg_conf = Dxx(&f, a, V(u, Z4C_GXX + SI[c][dd]) + p);
+                  const double d3 = d->dg[a][SI[c][dd]][p];
+                  if (pw == -4.) {
+                    const double oochi = 1.0 / chi_g;
+                    v = oochi * (ddg_conf - oochi * (2.0 * dchi_a * d3 + ddchi[a][a] * gtil) +
+                                 2.0 * oochi * oochi * dchi_a * dchi_a * gtil);
+                  } else {
+                    const double fac = 4.0 / pw, fac2 = fac - 1.0;
+                    const double psi4 = pow(chi_g, fac);
+                    const double oochi = 1.0 / chi_g;
+                    v = psi4 * (ddg_conf + fac * oochi * (2.0 * dchi_a * d3 + ddchi[a][a] * gtil) +
+                                fac * fac2 * oochi * oochi * dchi_a * dchi_a * gtil);
+                  }
+                } else {
+                  const double ddg_conf = Dx(&f, a, d->dg[bb][SI[c][dd]] + p);
+                  const double db3 = d->dg[bb][SI[c][dd]][p], da3 = d->dg[a][SI[c][dd]][p];
+                  if (pw == -4.) {
+                    const double oochi = 1.0 / chi_g;
+                    v = oochi * (ddg_conf - oochi * (dchi_a * db3 + dchi_b * da3 +
+                                                     ddchi[a][bb] * gtil) +
+                                 2.0 * oochi * oochi * dchi_a * dchi_b * gtil);
+                  } else {
+                    const double fac = 4.0 / pw, fac2 = fac - 1.0;
+                    const double psi4 = pow(chi_g, fac);
+                    const double oochi = 1.0 / chi_g;
+                    v = psi4 * (ddg_conf + fac * oochi * (dchi_a * db3 + dchi_b * da3 +
+                                                          ddchi[a][bb] * gtil) +
+                                fac * fac2 * oochi * oochi * dchi_a * dchi_b * gtil);
+                  }
+                }
+                ddg[a][bb][c][dd] = ddg[bb][a][c][dd] = ddg[a][bb][dd][c] = ddg[bb][a][dd][c] = v;
+              }
+        /* inverse metric, :293-309 */
+        double gu[3][3];
+        {
+          const double detg = det3(G3(0, 0), G3(0, 1), G3(0, 2), G3(1, 1), G3(1, 2), G3(2, 2));
+          inv3(1. / detg, G3(0, 0), G3(0, 1), G3(0, 2), G3(1, 1), G3(1, 2), G3(2, 2), gu);
+        }
+        /* Christoffels, :314-337 */
+        double Gd[3][3][3], Gu[3][3][3];
+        for (int c = 0; c < 3; ++c)
+          for (int a = 0; a < 3; ++a)
+            for (int bb = a; bb < 3; ++bb)
+              Gd[c][a][bb] = Gd[c][bb][a] =
+                  0.5 * (dg[a][bb][c] + dg[bb][a][c] - dg[c][a][bb]);
+        for (int c = 0; c < 3; ++c)
+          for (int a = 0; a < 3; ++a)
+            for (int bb = a; bb < 3; ++bb) {
+              double acc = 0.0;
+              for (int dd = 0; dd < 3; ++dd) acc += gu[c][dd] * Gd[dd][a][bb];
+              Gu[c][a][bb] = Gu[c][bb][a] = acc;
+            }
+        /* Ricci tensor and scalar, :342-378 */
+        double R = 0.0, Rd[3][3];
+        for (int a = 0; a < 3; ++a)
+          for (int bb = a; bb < 3; ++bb) {
+            double acc = 0.0;
+            for (int c = 0; c < 3; ++c)
+              for (int dd = 0; dd < 3; ++dd) {
+                for (int e = 0; e < 3; ++e) {
+                  acc += gu[c][dd] * Gu[e][a][c] * Gd[e][bb][dd];
+                  acc -= gu[c][dd] * Gu[e][a][bb] * Gd[e][c][dd];
+                }
+                acc += 0.5 * gu[c][dd] *
+                       (-ddg[c][dd][a][bb] - ddg[a][bb][c][dd] + ddg[a][c][bb][dd] +
+                        ddg[bb][c][a][dd]);
+              }
+            Rd[a][bb] = Rd[bb][a] = acc;
+            R += ((a == bb) ? 1.0 : 2.0) * gu[a][bb] * acc;
+          }
+        /* extrinsic curvature, :383-420 */
+        double Kt = 0.0, Kud[3][3];
+        for (int a = 0; a < 3; ++a) {
+          for (int bb = 0; bb < 3; ++bb) {
+            double acc = 0.0;
+            for (int c = 0; c < 3; ++c) acc += gu[a][c] * K3(c, bb);
+            Kud[a][bb] = acc;
+          }
+          Kt += Kud[a][a];
+        }
+        /* DK_ddd is stored symmetric in its last two indices and the loop
+         * runs over all (b, c): for b < c the (c, b) pass comes later and its
+         * value, with the two subtractions in the other order, is kept */
+        double DK[3][3][3];
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb)
+            for (int c = 0; c < 3; ++c) {
+              double v = dK[a][bb][c];
+              for (int dd = 0; dd < 3; ++dd) {
+                v -= Gu[dd][a][bb] * K3(dd, c);
+                v -= Gu[dd][a][c] * K3(bb, dd);
+              }
+              DK[a][bb][c] = DK[a][c][bb] = v;
+            }
+        /* tetrad and Gram-Schmidt, :426-524 */
+        const double x1 = b->x[0][i], x2 = b->x[1][j], x3 = b->x[2][k];
+        double xx = x1;
+        if (x1 * x1 + x2 * x2 < 1e-10) xx = xx + 1e-8;
+        double uv[3] = {xx, x2, x3};
+        double vv[3] = {xx * x3, x2 * x3, -(xx * xx) - (x2 * x2)};
+        double wv[3] = {x2 * -1.0, xx, 0.0};
+        double dot = 0.0, dot2;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb) dot += G3(a, bb) * wv[a] * wv[bb];
+        for (int a = 0; a < 3; ++a) wv[a] = wv[a] / sqrt(dot);
+        dot = 0.0;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb) dot += G3(a, bb) * wv[a] * uv[bb];
+        for (int a = 0; a < 3; ++a) uv[a] -= dot * wv[a];
+        dot = 0.0;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb) dot += G3(a, bb) * uv[a] * uv[bb];
+        for (int a = 0; a < 3; ++a) uv[a] = uv[a] / sqrt(dot);
+        dot = 0.0;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb) dot += G3(a, bb) * wv[a] * vv[bb];
+        dot2 = 0.0;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb) dot2 += G3(a, bb) * uv[a] * vv[bb];
+        for (int a = 0; a < 3; ++a) vv[a] -= dot * wv[a] + dot2 * uv[a];
+        dot = 0.0;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb) dot += G3(a, bb) * vv[a] * vv[bb];
+        for (int a = 0; a < 3; ++a) vv[a] = vv[a] / sqrt(dot);
+        /* psi4, :532-630 */
+        double rp = 0, ip = 0;
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb) {
+            double R4 = Rd[a][bb] + Kt * K3(a, bb);
+            for (int c = 0; c < 3; ++c)
+              for (int dd = 0; dd < 3; ++dd) R4 -= gu[c][dd] * K3(a, c) * K3(dd, bb);
+            const double Tr = vv[a] * vv[bb] - wv[a] * wv[bb];
+            const double Ti = -vv[a] * wv[bb] - wv[a] * vv[bb];
+            rp += -FR4 * R4 * Tr;
+            ip += -FR4 * R4 * Ti;
+          }
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb)
+            for (int c = 0; c < 3; ++c) {
+              const double R4 = -(DK[bb][a][c] - DK[c][a][bb]);
+              const double Tr = vv[a] * vv[bb] - wv[a] * wv[bb];
+              const double Ti = -vv[a] * wv[bb] - wv[a] * vv[bb];
+              rp += 0.5 * R4 * uv[c] * Tr;
+              ip += 0.5 * R4 * uv[c] * Ti;
+            }
+        for (int a = 0; a < 3; ++a)
+          for (int bb = 0; bb < 3; ++bb)
+            for (int c = 0; c < 3; ++c)
+              for (int dd = 0; dd < 3; ++dd) {
+                const double R4 = G3(dd, c) * Rd[a][bb] + G3(a, bb) * Rd[dd][c] -
+                                  G3(dd, bb) * Rd[a][c] - G3(a, c) * Rd[dd][bb] -
+                                  0.5 * R * (G3(dd, c) * G3(a, bb) - G3(dd, bb) * G3(a, c)) +
+                                  K3(dd, c) * K3(a, bb) - K3(dd, bb) * K3(a, c);
+                const double Tr = vv[a] * vv[bb] - wv[a] * wv[bb];
+                const double Ti = -vv[a] * wv[bb] - wv[a] * vv[bb];
+                rp += -FR4 * R4 * uv[dd] * uv[c] * Tr;
+                ip += -FR4 * R4 * uv[dd] * uv[c] * Ti;
+              }
+        weyl[p] = rp;
+        weyl[nvol + p] = ip;
+      }
+#undef G3
+#undef K3
+#undef GT
+}
+
 /* ---- puncture tracker, z4c/puncture_tracker.cpp:95-129 ------------------ */
 
 /* LagrangeInterp1D<7> (utils/lagrange_interp.hpp:33-146), odd order: first

@@ -98,6 +98,13 @@ void orc_vc_restrict(const int nx[3], int nvar, const double *fine, double *coar
 void orc_vc_prolongate(const int nx[3], int nvar, const double *coarse, double *fine,
                        const int box[6]);
 
+/* Z4c::Z4cWeyl, z4c/calculate_weyl_scalars.cpp:44-630 (vacuum): the real
+ * and imaginary parts of psi4 on the interior from the ADM variables, the Z4c
+ * state and the stored derivatives; weyl (2 variables) is NaN elsewhere.
+ * Requires orc_prepare_derivs(u). */
+void orc_weyl(const orc_block_t *b, const z4c_params_t *p, const double *adm, const double *u,
+              const orc_derivs_t *d, double *weyl);
+
 /* ---- puncture tracker (z4c/puncture_tracker.cpp) ------------------------ */
 
 /* PunctureTracker::InterpolateShift (:95-129): the shift of block b at pos

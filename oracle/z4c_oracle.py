@@ -87,6 +87,7 @@ def lib():
         L.orc_z4c_to_adm_ghosts.argtypes = [bp, pp, dp, dp]
         L.orc_adm_to_z4c.argtypes = [bp, pp, dp, dp]
         L.orc_adm_constraints.argtypes = [bp, pp, dp, dp, Dp, dp]
+        L.orc_weyl.argtypes = [bp, pp, dp, dp, Dp, dp]
         L.orc_mesh_exchange.argtypes = [mp, C.c_int, dp]
         L.orc_hst_accumulate.argtypes = [bp, pp, dp, dp, dp]
         _lib = L
@@ -192,6 +193,16 @@ def adm_constraints(blk, p, adm, u):
     d = _DerivsHolder(blk, u)
     lib().orc_adm_constraints(C.byref(blk._s), C.byref(p), _ptr(adm), _ptr(u),
                               C.byref(d.d), _ptr(out))
+    return out
+
+
+def weyl(blk, p, adm, u):
+    """Z4c::Z4cWeyl: Re and Im psi4 on the interior, NaN elsewhere."""
+    adm = np.ascontiguousarray(adm, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    out = np.zeros(blk.shape(2))
+    d = _DerivsHolder(blk, u)
+    lib().orc_weyl(C.byref(blk._s), C.byref(p), _ptr(adm), _ptr(u), C.byref(d.d), _ptr(out))
     return out
 
 

@@ -12,6 +12,8 @@ Fixtures (numpy .npz, compressed):
   evol_<case>.npz   a multi-step run of the stock reference driver: the
                     history table (outputs/history.cpp columns) and the
                     initial and final states
+  weyl_punc2.npz    Z4cWeyl (Re, Im psi4) on the initial state of ops_punc2
+                    and after its one RK4 step
   refine_vc.npz     the vertex-centred restriction and prolongation operators
                     of one MeshBlock of a statically refined mesh
 Each fixture stores the input-deck parameters it was made with ("params",
@@ -186,6 +188,27 @@ REFINE = dict(test="one_puncture", z4c=PUNCTURE, integ="rk4", bc="extrapolate_ou
               mesh=[(16, -4.0, 4.0, 8)] * 3, extra={}, problem={"punc_ADM_mass": 1.0})
 
 
+def make_weyl(outdir):
+    """Z4cWeyl on the initial state of the ops_punc2 case and after its one
+    RK4 step (the inputs, u0/adm0 and s4_alg/s4_adm, are in ops_punc2.npz);
+    only the Weyl records are stored."""
+    with tempfile.TemporaryDirectory() as tmp:
+        rec_path = os.path.join(tmp, "ops.rec")
+        inp = os.path.join(tmp, "case.inp")
+        with open(inp, "w") as f:
+            f.write(deck(CASES["punc2"], rec_path) + "weyl = true\n")
+        subprocess.run([os.path.join(REF_BIN, "z4c_ops_ref"), "-i", inp], cwd=tmp, check=True,
+                       stdout=subprocess.DEVNULL)
+        rec = read_records(rec_path)
+    path = os.path.join(outdir, "weyl_punc2.npz")
+    # weyl0 on the initial data (K_ab = 0), weyl1 after one RK4 step (K_ab
+    # nonzero); a corner of each input state ties them to ops_punc2
+    np.savez_compressed(path, weyl0=rec["weyl0"], weyl1=rec["s4_weyl"],
+                        u0=rec["u0"][:, :1, :1, :1, :1],
+                        s4_alg=rec["s4_alg"][:, :1, :1, :1, :1])
+    return path
+
+
 def make_refine(outdir):
     with tempfile.TemporaryDirectory() as tmp:
         rec_path = os.path.join(tmp, "refine.rec")
@@ -209,6 +232,9 @@ def make_refine(outdir):
 
 def main():
     only = set(sys.argv[1:])  # fixture names to (re)make; all when empty
+    if not only or "weyl_punc2" in only:
+        p = make_weyl(HERE)
+        print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
     if not only or "refine_vc" in only:
         p = make_refine(HERE)
         print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")

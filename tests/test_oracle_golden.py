@@ -121,6 +121,31 @@ def test_evolution_and_history(name):
     np.testing.assert_allclose(hst, ref, rtol=1e-13, atol=0)
 
 
+@pytest.mark.parametrize("when", ["initial", "one_step"])
+def test_weyl_psi4(when):
+    """Z4cWeyl (Re, Im psi4) on the puncture of ops_punc2, bit for bit on the
+    interior and NaN elsewhere, as the reference fills it: on the initial data
+    (K_ab = 0) and after one RK4 step (K_ab nonzero, so the Codazzi and K K
+    terms take part)."""
+    c = Case("ops_punc2")
+    z = np.load(os.path.join(GOLDEN, "weyl_punc2.npz"))
+    ukey, akey, wkey = {"initial": ("u0", "adm0", "weyl0"),
+                        "one_step": ("s4_alg", "s4_adm", "weyl1")}[when]
+    u, adm = c.rec[ukey], c.rec[akey]
+    assert bitwise(z[ukey], u[:, :1, :1, :1, :1])  # the same input state
+    if when == "one_step":
+        kdd = adm[:, 10:16][c.interior()]  # K_ab, the ADM variables 10..15
+        assert np.abs(kdd).max() > 1e-3
+    p = _params(c)
+    blocks = c.blocks()
+    w = np.stack([O.weyl(b, p, adm[g], u[g]) for g, b in enumerate(blocks)])
+    ref = z[wkey]
+    assert (np.isnan(w) == np.isnan(ref)).all()
+    fin = ~np.isnan(ref)
+    assert fin.sum() == 2 * 2 * 9 ** 3
+    assert bitwise(w[fin], ref[fin])
+
+
 def test_vc_refinement_operators():
     """Restriction (injection) and prolongation (injection + tensor-product
     Lagrange) of one MeshBlock of a statically refined mesh, bit for bit
