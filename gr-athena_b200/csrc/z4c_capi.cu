@@ -149,6 +149,7 @@ int reg_nvar_(int reg) {
   switch (reg) {
     case Z4C_REG_ADM: return Z4C_NADM;
     case Z4C_REG_CON: return Z4C_NCON;
+    case Z4C_REG_WEYL: return Z4C_NWEYL;
     default: return (reg >= 0 && reg < Z4C_NREG) ? Z4C_NVAR : -1;
   }
 }
@@ -450,7 +451,7 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
   const size_t b22 = sizeof(double) * (size_t)Z4C_NVAR * g.nvol * nb;
   int need[Z4C_NREG] = {};
   need[Z4C_REG_U] = need[Z4C_REG_W] = need[Z4C_REG_RHS] = need[Z4C_REG_ADM] =
-      need[Z4C_REG_CON] = 1;
+      need[Z4C_REG_CON] = need[Z4C_REG_WEYL] = 1;
   if (integrator == Z4C_INTEG_RK4) need[Z4C_REG_U1] = 1;
   else need[Z4C_REG_K1] = need[Z4C_REG_K2] = need[Z4C_REG_K3] = need[Z4C_REG_K4] = 1;
   for (int r = 0; r < Z4C_NREG && rc == Z4C_OK; ++r) {
@@ -723,6 +724,22 @@ int z4c_adm_constraints(z4c_ctx* ctx, int reg_con, int reg_adm, int reg_u, int b
   launch_adm_constraints(ctx->g, ctx->dev(), ctx->reg[reg_adm], ctx->reg[reg_u],
                          ctx->reg[reg_con], ctx->xf, b0, nb, ctx->stream);
   LAUNCH_CHECK("adm_constraints");
+  return Z4C_OK;
+}
+
+int z4c_weyl(z4c_ctx* ctx, int reg_adm, int reg_u, int reg_weyl, int block) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  int rc, b0, nb;
+  if ((rc = check_reg(ctx, reg_adm)) || (rc = check_reg(ctx, reg_u)) ||
+      (rc = check_reg(ctx, reg_weyl)))
+    return rc;
+  if (reg_nvar_(reg_adm) != Z4C_NADM || reg_nvar_(reg_u) != Z4C_NVAR ||
+      reg_nvar_(reg_weyl) != Z4C_NWEYL)
+    return fail(Z4C_EINVAL, "Z4cWeyl needs the ADM, a Z4c and the Weyl register");
+  if ((rc = check_block(ctx, block, &b0, &nb))) return rc;
+  launch_weyl(ctx->g, ctx->dev(), ctx->reg[reg_adm], ctx->reg[reg_u], ctx->sd,
+              ctx->reg[reg_weyl], ctx->xf, b0, nb, ctx->stream);
+  LAUNCH_CHECK("weyl");
   return Z4C_OK;
 }
 

@@ -9,6 +9,7 @@
 #include "z4c_common.cuh"
 #include "z4c_kernels.cuh"
 #include "z4c_rhs.cuh"
+#include "z4c_weyl.cuh"
 
 namespace z4c {
 
@@ -1130,6 +1131,34 @@ k_adm_constraints(Grid g, DevParams P, const double* __restrict__ adm,
   for (int q = 0; q < 7; ++q) cb[(int64_t)q * g.nvol] = c7[q];
 }
 
+// ---- Weyl scalar psi4 (z4c/calculate_weyl_scalars.cpp:44-630) --------------
+// One thread per vertex of the requested blocks; interior vertices get psi4,
+// every other vertex NaN (the reference fills the register with NaN first).
+__global__ void __launch_bounds__(128, 1)
+k_weyl(Grid g, DevParams P, const double* __restrict__ adm, const double* __restrict__ u,
+       const double* __restrict__ sd, double* __restrict__ weyl, const double* __restrict__ xf,
+       int block0, int nblk) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.nvol * nblk) return;
+  const int b = block0 + (int)(t / g.nvol);
+  const int64_t p = t % g.nvol;
+  const int i = (int)(p % g.nn[0]);
+  const int j = (int)((p / g.nn[0]) % g.nn[1]);
+  const int k = (int)(p / ((int64_t)g.nn[0] * g.nn[1]));
+  double* wb = weyl + (int64_t)b * 2 * g.nvol + p;
+  const bool in = i >= NG && i <= NG + g.nx[0] && j >= NG && j <= NG + g.nx[1] && k >= NG &&
+                  k <= NG + g.nx[2];
+  double rp = __longlong_as_double(0x7ff8000000000000LL), ip = rp;
+  if (in) {
+    const double* x = xf + (int64_t)b * (g.nn[0] + g.nn[1] + g.nn[2]);
+    weyl_point(u + (int64_t)b * NVAR * g.nvol, adm + (int64_t)b * Z4C_NADM * g.nvol,
+               sd + (int64_t)b * kSdComponents * g.nvol, g.nvol, p, g.s, P, P.fd[b], x[i],
+               x[g.nn[0] + j], x[g.nn[0] + g.nn[1] + k], &rp, &ip);
+  }
+  wb[0] = rp;
+  wb[g.nvol] = ip;
+}
+
 // ---- history sums (outputs/history.cpp:168-200): one CTA per block ---------
 __global__ void k_hst(Grid g, DevParams P, const double* __restrict__ con,
                       const double* __restrict__ u, const double* __restrict__ xv,
@@ -1488,6 +1517,18 @@ void launch_adm_constraints(const Grid& g, const DevParams& P, const double* adm
   COUNTED
   k_adm_constraints<<<div_up(n, 128), 128, 0, st>>>(g, P, adm, u, con, xf,
                                                                     block0, nblk);
+}
+
+void launch_weyl(const Grid& g, const DevParams& P, const double* adm, const double* u,
+                 double* sd, double* weyl, const double* xf, int block0, int nblk,
+                 cudaStream_t st) {
+  const int64_t cprep = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7);  // widest component region
+  COUNTED
+  k_prep<<<dim3(div_up(cprep, kPointThreads), kSdComponents, nblk), kPointThreads, 0, st>>>(
+      g, P, u, sd, block0);
+  const int64_t n = g.nvol * nblk;
+  COUNTED
+  k_weyl<<<div_up(n, 128), 128, 0, st>>>(g, P, adm, u, sd, weyl, xf, block0, nblk);
 }
 
 void launch_hst(const Grid& g, const DevParams& P, const double* con, const double* u,

@@ -22,7 +22,7 @@ PKG = os.path.dirname(HERE)
 LIB_PATH = os.path.join(PKG, "_build", "libz4c_b200.so")
 
 NG = 4
-NVAR, NADM, NCON = 22, 17, 7
+NVAR, NADM, NCON, NWEYL = 22, 17, 7, 2
 (CHI, GXX, GXY, GXZ, GYY, GYZ, GZZ, KHAT, AXX, AXY, AXZ, AYY, AYZ, AZZ,
  GAMX, GAMY, GAMZ, THETA, ALPHA, BETAX, BETAY, BETAZ) = range(22)
 (ADM_ALPHA, ADM_BETAX, ADM_BETAY, ADM_BETAZ, ADM_GXX, ADM_GXY, ADM_GXZ, ADM_GYY,
@@ -30,7 +30,7 @@ NVAR, NADM, NCON = 22, 17, 7
  ADM_PSI4) = range(17)
 CON_C, CON_H, CON_M, CON_Z, CON_MX, CON_MY, CON_MZ = range(7)
 (REG_U, REG_U1, REG_RHS, REG_ADM, REG_CON, REG_W, REG_K1, REG_K2, REG_K3,
- REG_K4) = range(10)
+ REG_K4, REG_WEYL) = range(11)
 BC_PERIODIC, BC_OUTFLOW, BC_SOMMERFELD = 0, 1, 2
 BC_NAMES = {"periodic": BC_PERIODIC, "outflow": BC_OUTFLOW, "extrapolate_outflow": BC_OUTFLOW,
             "sommerfeld": BC_SOMMERFELD, "gr_sommerfeld": BC_SOMMERFELD}
@@ -46,7 +46,7 @@ EXPORTS = (
     "z4c_set_stream", "z4c_sync", "z4c_num_blocks", "z4c_block_nn", "z4c_reg_nvar",
     "z4c_dx", "z4c_block_coords", "z4c_mesh_block_coords", "z4c_mesh_new_dt", "z4c_upload", "z4c_download", "z4c_device_ptr",
     "z4c_rhs", "z4c_boundary_rhs", "z4c_add_rhs", "z4c_weighted_ave", "z4c_alg_constr", "z4c_adm_to_z4c",
-    "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_ghost_fill", "z4c_init_finalize",
+    "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_weyl", "z4c_ghost_fill", "z4c_init_finalize",
     "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
     "z4c_get_tile", "z4c_autotune", "z4c_check_finite", "z4c_kernel_launches", "z4c_rhs_stage",
     "z4c_fp64_probe", "z4c_tracker_add", "z4c_tracker_get", "z4c_vc_restrict", "z4c_vc_prolongate", "z4c_rhs_noalloc")
@@ -114,6 +114,7 @@ def lib():
         L.z4c_adm_to_z4c.argtypes = [vp, ip, ip, ip]
         L.z4c_z4c_to_adm.argtypes = [vp, ip, ip, ip]
         L.z4c_adm_constraints.argtypes = [vp, ip, ip, ip, ip]
+        L.z4c_weyl.argtypes = [vp, ip, ip, ip, ip]
         L.z4c_ghost_fill.argtypes = [vp, ip]
         L.z4c_init_finalize.argtypes = [vp]
         L.z4c_hst_norms.argtypes = [vp, dp]
@@ -320,6 +321,10 @@ class Z4c:
         _check(lib().z4c_adm_constraints(self._h, reg_con, reg_adm, reg_u, block))
 
     # ---- task-list pieces ----
+    def Z4cWeyl(self, reg_adm=REG_ADM, reg_weyl=REG_WEYL, block=-1, reg_u=REG_U):
+        """Z4c::Z4cWeyl: Re and Im psi4 on the interior, NaN elsewhere."""
+        _check(lib().z4c_weyl(self._h, reg_adm, reg_u, reg_weyl, block))
+
     def ghost_fill(self, reg=REG_U):
         _check(lib().z4c_ghost_fill(self._h, reg))
 

@@ -31,6 +31,7 @@ extern "C" {
 #define Z4C_NVAR 22        /* evolved variables (z4c.hpp:63-88)             */
 #define Z4C_NADM 17        /* ADM variables (z4c.hpp:100-118)               */
 #define Z4C_NCON 7         /* constraint variables (z4c.hpp:128-137)        */
+#define Z4C_NWEYL 2        /* Weyl variables: Re, Im psi4 (z4c.hpp:163-171) */
 
 /* Evolved-variable indices, z4c.hpp:63-88. */
 enum {
@@ -85,6 +86,7 @@ enum {
   Z4C_REG_K2,
   Z4C_REG_K3,
   Z4C_REG_K4,
+  Z4C_REG_WEYL,    /* storage.weyl (2 vars: Re psi4, Im psi4)       */
   Z4C_NREG
 };
 
@@ -197,6 +199,13 @@ int z4c_z4c_to_adm(z4c_ctx *ctx, int reg_u, int reg_adm, int block);
 /* Z4c::ADMConstraints (z4c/adm_z4c.cpp:382-930), vacuum. */
 int z4c_adm_constraints(z4c_ctx *ctx, int reg_con, int reg_adm, int reg_u,
                         int block);
+/* Z4c::Z4cWeyl (z4c/calculate_weyl_scalars.cpp:44-630), vacuum: Re and Im of
+ * psi4 into reg_weyl (a Z4C_NWEYL register) on the interior vertices and NaN
+ * on every other vertex, from the ADM register (metric and extrinsic
+ * curvature) and the Z4c register reg_u (the reference's storage.u, whose
+ * first derivatives PrepareZ4cDerivatives stores: this call recomputes
+ * them). */
+int z4c_weyl(z4c_ctx *ctx, int reg_adm, int reg_u, int reg_weyl, int block);
 /* GR_Z4c SEND/RECV/SETB_Z4C + PHY_BVAL (comm/comm_registry.cpp:336-382,
  * comm/physical_bcs.cpp:506-670): same-level vertex-centred ghost fill by
  * device copy, shared vertices averaged over their owners, then the

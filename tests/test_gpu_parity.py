@@ -144,3 +144,58 @@ def test_puncture_tracker_matches_reference():
         np.testing.assert_allclose(pos, row[2:5], rtol=1e-12, atol=0)
         np.testing.assert_allclose(beta, row[5:8], rtol=1e-9, atol=1e-15)
     ctx.close()
+
+
+@pytest.mark.parametrize("when", ["initial", "one_step"])
+@pytest.mark.parametrize("per_block", [False, True])
+def test_weyl_psi4(when, per_block):
+    """Z4cWeyl through the C ABI against the reference's psi4 on the puncture
+    of ops_punc2: on the initial data and after one RK4 step (nonzero K_ab).
+    NaN outside the interior, as the reference fills the register."""
+    import os
+    from z4c_testlib import GOLDEN
+    c = Case("ops_punc2")
+    z = np.load(os.path.join(GOLDEN, "weyl_punc2.npz"))
+    ukey, akey, wkey = {"initial": ("u0", "adm0", "weyl0"),
+                        "one_step": ("s4_alg", "s4_adm", "weyl1")}[when]
+    Z, ctx = make_ctx(c)
+    ctx.upload(Z.REG_U, c.to_grid(c.rec[ukey]))
+    ctx.upload(Z.REG_ADM, c.to_grid(c.rec[akey]))
+    if per_block:
+        for b in range(ctx.nblocks):
+            ctx.Z4cWeyl(Z.REG_ADM, Z.REG_WEYL, b)
+    else:
+        ctx.Z4cWeyl()
+    w = c.from_grid(ctx.download(Z.REG_WEYL))
+    ref = z[wkey]
+    assert np.array_equal(np.isnan(w), np.isnan(ref))
+    assert rel_err(w, ref) <= TOL
+    ctx.close()
+
+
+def test_weyl_on_evolved_binary_matches_oracle():
+    """Two punctures on 4^3 MeshBlocks of 16^3, two RK4 steps on the device,
+    then Z4cToADM and Z4cWeyl on the device against the oracle's psi4 on the
+    same downloaded state, block by block."""
+    import z4c_b200 as Z
+    import z4c_oracle as O
+    from z4c_b200 import initial_data as ID
+    params = dict(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02, damp_kappa2=0.0,
+                  shift_eta=2.0, r_max_con=1e300)
+    mesh = Z.Mesh((4, 4, 4), (16, 16, 16), (-6.0,) * 3, (6.0,) * 3, "outflow")
+    ctx = Z.Z4c(mesh, Z.default_params(**params), "rk4")
+    ID.load_adm(ctx, ID.punctures(mesh, ctx.params, masses=(0.5, 0.5),
+                                  centres=((1.3, 0.2, 0.1), (-1.3, -0.25, 0.0))))
+    ctx.evolve(0.25 * float(ctx.dx().min()), 2)
+    ctx.Z4cToADM()
+    ctx.Z4cWeyl()
+    w = ctx.download(Z.REG_WEYL)
+    u, adm = ctx.download(Z.REG_U), ctx.download(Z.REG_ADM)
+    p = O.default_params(**params)
+    for b in (0, 21, 42, 63):
+        xs, dxs = mesh.block_coords(b)
+        ref = O.weyl(O.Block(mesh.nx, dxs, xs), p, adm[b], u[b])
+        assert np.array_equal(np.isnan(w[b]), np.isnan(ref)), b
+        assert rel_err(w[b], ref) <= TOL, b
+        assert np.nanmax(np.abs(ref)) > 1e-6
+    ctx.close()
