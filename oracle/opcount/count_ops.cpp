@@ -60,6 +60,12 @@ inline CReal pow(CReal a, CReal b) { ++opcount::fn; return CReal(std::pow(a.v, b
 inline CReal pow(int a, int b) { return CReal(std::pow((double)a, (double)b)); }
 inline int isfinite(CReal a) { return std::isfinite(a.v); }
 inline CReal floor(CReal a) { return CReal(std::floor(a.v)); }
+// trigonometry of the extraction-sphere set-up (not on the counted path)
+inline CReal sin(CReal a) { ++opcount::fn; return CReal(std::sin(a.v)); }
+inline CReal cos(CReal a) { ++opcount::fn; return CReal(std::cos(a.v)); }
+inline CReal acos(CReal a) { ++opcount::fn; return CReal(std::acos(a.v)); }
+inline CReal atan(CReal a) { ++opcount::fn; return CReal(std::atan(a.v)); }
+inline CReal atan2(CReal a, CReal b) { ++opcount::fn; return CReal(std::atan2(a.v, b.v)); }
 inline long lrint(CReal a) { return std::lrint(a.v); }
 
 #define double CReal

@@ -11,6 +11,8 @@
 //   brhs0              rhs0 followed by Z4cBoundaryRHS (Sommerfeld faces)
 //   weyl0              with <driver> weyl = true: Z4cWeyl(adm0) (Re, Im psi4)
 //   s<N>_weyl          with <driver> weyl = true: Z4cWeyl after the last stage
+//   s<N>_wave_*        with <driver> weyl = true and <psi4_extraction>
+//                      spheres: the psi4 multipoles of s<N>_weyl (WaveRecords)
 //   alg0               AlgConstr applied to a copy of u0
 //   adm0               Z4cToADM(u0)
 //   con0               ADMConstraints(con, adm0, mat, u0)
@@ -36,7 +38,9 @@
 #include "comm/comm_registry.hpp"
 #include "mesh/mesh_refinement.hpp"
 #include "task_list/time_integrators.hpp"
+#include "z4c/wave_extract.hpp"
 #include "z4c/z4c.hpp"
+#include "mesh/spherical_grid.hpp"
 
 #include "z4c_oracle_io.hpp"
 
@@ -76,6 +80,70 @@ struct Dumper {
     w.f64(name, {nb, nvar, nn3, nn2, nn1}, buf.data());
   }
 };
+
+// psi4 extraction on the <psi4_extraction> spheres, as the main loop runs it
+// after the Weyl task (main.hpp Z4c_DerivedQuantities): the Aux group ghost
+// exchange of the Weyl register (Mesh::CommunicateAuxZ4c), the per-block
+// multipole projection (Aux_Z4c::WeylDecompose) and the reduction over blocks
+// (WaveExtract::ReduceMultipole).  Records, for radius n:
+//   <p>weylx      the Weyl register after the exchange and physical BCs
+//   <p>geo<n>     per sphere vertex: theta, phi, x, y, z, SphericalGrid weight
+//   <p>patch<n>   per (block in gid order, patch point): gid, vertex index
+//   <p>loc<n>     per block: the local (l, m) projections
+//   <p>psi<n>     the reduced projections, psi(l-2, m+l, re/im)
+void WaveRecords(Mesh* pm, const std::vector<MeshBlock*>& blocks, Writer& w, const std::string& p,
+                 int nn1, int nn2, int nn3) {
+  pm->CommunicateAuxZ4c();
+  {
+    const std::int64_t per = 2LL * nn1 * nn2 * nn3;
+    std::vector<double> buf(blocks.size() * per);
+    std::int64_t q = 0;
+    for (auto* b : blocks) {
+      AthenaArray<Real>& a = b->pz4c->storage.weyl;
+      for (int n = 0; n < 2; ++n)
+        for (int k = 0; k < nn3; ++k)
+          for (int j = 0; j < nn2; ++j)
+            for (int i = 0; i < nn1; ++i) buf[q++] = a(n, k, j, i);
+    }
+    w.f64(p + "weylx", {(std::int64_t)blocks.size(), 2, nn3, nn2, nn1}, buf.data());
+  }
+  for (auto* b : blocks) {
+    AthenaArray<Real> u_R, u_I;
+    u_R.InitWithShallowSlice(b->pz4c->storage.weyl, Z4c::I_WEY_rpsi4, 1);
+    u_I.InitWithShallowSlice(b->pz4c->storage.weyl, Z4c::I_WEY_ipsi4, 1);
+    for (auto* loc : b->pwave_extr_loc) loc->Decompose_multipole(u_R, u_I);
+  }
+  for (size_t n = 0; n < pm->pwave_extr.size(); ++n) {
+    WaveExtract* we = pm->pwave_extr[n];
+    we->ReduceMultipole();
+    const std::string sn = std::to_string(n);
+    SphericalGrid* sg = we->psphere;
+    const int np = sg->NumVertices();
+    std::vector<double> geo(6 * (size_t)np);
+    for (int ic = 0; ic < np; ++ic) {
+      Real th, ph, x, y, z;
+      sg->GeodesicGrid::PositionPolar(ic, &th, &ph);
+      sg->Position(ic, &x, &y, &z);
+      double* g = &geo[6 * (size_t)ic];
+      g[0] = th; g[1] = ph; g[2] = x; g[3] = y; g[4] = z;
+      g[5] = sg->ComputeWeight(ic);
+    }
+    w.f64(p + "geo" + sn, {np, 6}, geo.data());
+    std::vector<double> patch, loc;
+    for (auto* b : blocks) {
+      WaveExtractLocal* l = b->pwave_extr_loc[n];
+      for (int ip = 0; ip < l->ppatch->NumPoints(); ++ip) {
+        patch.push_back(b->gid);
+        patch.push_back(l->ppatch->idxMap(ip));
+      }
+      for (std::int64_t q = 0; q < l->psi.GetSize(); ++q) loc.push_back(l->psi(q));
+    }
+    w.f64(p + "patch" + sn, {(std::int64_t)patch.size() / 2, 2}, patch.data());
+    const std::int64_t d3 = we->psi.GetDim3(), d2 = we->psi.GetDim2(), d1 = we->psi.GetDim1();
+    w.f64(p + "loc" + sn, {(std::int64_t)blocks.size(), d3, d2, d1}, loc.data());
+    w.f64(p + "psi" + sn, {d3, d2, d1}, we->psi.data());
+  }
+}
 
 void Copy(AthenaArray<Real>& dst, AthenaArray<Real>& src) {
   dst.NewAthenaArray(src.GetDim4(), src.GetDim3(), src.GetDim2(), src.GetDim1());
@@ -334,6 +402,7 @@ int main(int argc, char* argv[]) {
           z->Z4cWeyl(z->storage.adm, z->storage.mat, z->storage.weyl);
         }
         d.dump(s + "weyl", Z4c::N_WEY, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.weyl; });
+        if (!pm->pwave_extr.empty()) WaveRecords(pm, blocks, d.w, s + "wave_", d.nn1, d.nn2, d.nn3);
       }
     }
   }

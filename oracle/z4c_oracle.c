@@ -1579,6 +1579,320 @@ void orc_tracker_interp(const orc_block_t *b, const double *u, const double pos[
   }
 }
 
+/* ---- psi4 extraction -------------------------------------------------------
+ * GeodesicGrid (mesh/geodesic_grid.cpp:21-160, geodesic_grid.hpp:145-160):
+ * five blocks of nlev x 2 nlev vertices plus the two poles, each block held
+ * with one ghost row/column; vertex ic = bl 2 nlev^2 + l 2 nlev + m. */
+#define GEO_PI 3.1415926535897932 /* PI of the reference's defs.hpp.in:250 */
+typedef struct {
+  int nlev;
+  double *c[3]; /* [5][nlev+2][2 nlev+2] unit-vector components */
+  int *idx;     /* [5][nlev+2][2 nlev+2] vertex indices */
+  double pol[3][2];
+  int poli[2];
+} geo_t;
+
+static inline int64_t geo_at(const geo_t *g, int bl, int l, int m) {
+  return ((int64_t)bl * (g->nlev + 2) + l) * (2 * g->nlev + 2) + m;
+}
+
+static void geo_fill_ghosts_d(const geo_t *g, double *a, const double *pole) {
+  const int n = g->nlev;
+  for (int bl = 0; bl < 5; ++bl) {
+    for (int k = 0; k < n; ++k) {
+      a[geo_at(g, bl, 0, k + 1)] = a[geo_at(g, (bl + 4) % 5, k + 1, 1)];
+      a[geo_at(g, bl, 0, k + n + 1)] = a[geo_at(g, (bl + 4) % 5, n, k + 1)];
+      a[geo_at(g, bl, k + 1, 2 * n + 1)] = a[geo_at(g, (bl + 4) % 5, n, k + n + 1)];
+      a[geo_at(g, bl, k + 2, 0)] = a[geo_at(g, (bl + 1) % 5, 1, k + 1)];
+      a[geo_at(g, bl, n + 1, k + 1)] = a[geo_at(g, (bl + 1) % 5, 1, k + n + 1)];
+      a[geo_at(g, bl, n + 1, k + n + 1)] = a[geo_at(g, (bl + 1) % 5, k + 2, 2 * n)];
+    }
+    a[geo_at(g, bl, 1, 0)] = pole[0];
+    a[geo_at(g, bl, n + 1, 2 * n)] = pole[1];
+    a[geo_at(g, bl, 0, 2 * n + 1)] = a[geo_at(g, bl, 0, 2 * n)];
+  }
+}
+
+static void geo_fill_ghosts_i(const geo_t *g, int *a, const int *pole) {
+  const int n = g->nlev;
+  for (int bl = 0; bl < 5; ++bl) {
+    for (int k = 0; k < n; ++k) {
+      a[geo_at(g, bl, 0, k + 1)] = a[geo_at(g, (bl + 4) % 5, k + 1, 1)];
+      a[geo_at(g, bl, 0, k + n + 1)] = a[geo_at(g, (bl + 4) % 5, n, k + 1)];
+      a[geo_at(g, bl, k + 1, 2 * n + 1)] = a[geo_at(g, (bl + 4) % 5, n, k + n + 1)];
+      a[geo_at(g, bl, k + 2, 0)] = a[geo_at(g, (bl + 1) % 5, 1, k + 1)];
+      a[geo_at(g, bl, n + 1, k + 1)] = a[geo_at(g, (bl + 1) % 5, 1, k + n + 1)];
+      a[geo_at(g, bl, n + 1, k + n + 1)] = a[geo_at(g, (bl + 1) % 5, k + 2, 2 * n)];
+    }
+    a[geo_at(g, bl, 1, 0)] = pole[0];
+    a[geo_at(g, bl, n + 1, 2 * n)] = pole[1];
+    a[geo_at(g, bl, 0, 2 * n + 1)] = a[geo_at(g, bl, 0, 2 * n)];
+  }
+}
+
+/* one vertex of row l of block 0: the normalised (wa A + wb B + wc C) / nlev */
+static void geo_put(geo_t *g, int row, int col, int wa, const double *A, int wb, const double *B,
+                    int wc, const double *C) {
+  const double n = (double)g->nlev;
+  const double x = (wa * A[0] + wb * B[0] + wc * C[0]) / n;
+  const double y = (wa * A[1] + wb * B[1] + wc * C[1]) / n;
+  const double z = (wa * A[2] + wb * B[2] + wc * C[2]) / n;
+  const double norm = sqrt(x * x + y * y + z * z);
+  const int64_t q = geo_at(g, 0, row, col);
+  g->c[0][q] = x / norm;
+  g->c[1][q] = y / norm;
+  g->c[2][q] = z / norm;
+}
+
+static int geo_init(geo_t *g, int nlev) {
+  g->nlev = nlev;
+  const int64_t sz = (int64_t)5 * (nlev + 2) * (2 * nlev + 2);
+  for (int a = 0; a < 3; ++a) g->c[a] = (double *)calloc((size_t)sz, sizeof(double));
+  g->idx = (int *)calloc((size_t)sz, sizeof(int));
+  if (!g->c[0] || !g->c[1] || !g->c[2] || !g->idx) return -1;
+  const double sa = 2.0 / sqrt(5.0), ca = 1.0 / sqrt(5.0);
+  const double P1[3] = {0.0, 0.0, 1.0};
+  const double P2[3] = {sa, 0.0, ca};
+  const double P3[3] = {sa * cos(0.2 * GEO_PI), sa * sin(0.2 * GEO_PI), -ca};
+  const double P4[3] = {sa * cos(-0.4 * GEO_PI), sa * sin(-0.4 * GEO_PI), ca};
+  const double P5[3] = {sa * cos(-0.2 * GEO_PI), sa * sin(-0.2 * GEO_PI), -ca};
+  const double P6[3] = {0.0, 0.0, -1.0};
+  for (int l = 0; l < nlev; ++l) {
+    int col = 1;
+    for (int m = l; m < nlev; ++m) geo_put(g, l + 1, col++, m - l + 1, P2, nlev - m - 1, P1, l, P4);
+    for (int m = nlev - l; m < nlev; ++m)
+      geo_put(g, l + 1, col++, nlev - l, P2, m - nlev + l + 1, P5, nlev - m - 1, P4);
+    for (int m = l; m < nlev; ++m) geo_put(g, l + 1, col++, m - l + 1, P3, nlev - m - 1, P2, l, P5);
+    for (int m = nlev - l; m < nlev; ++m)
+      geo_put(g, l + 1, col++, nlev - l, P3, m - nlev + l + 1, P6, nlev - m - 1, P5);
+  }
+  for (int bl = 1; bl < 5; ++bl)
+    for (int l = 1; l < nlev + 1; ++l)
+      for (int m = 1; m < 2 * nlev + 1; ++m) {
+        const int64_t q0 = geo_at(g, 0, l, m), q = geo_at(g, bl, l, m);
+        const double x0 = g->c[0][q0], y0 = g->c[1][q0];
+        g->c[0][q] = x0 * cos(bl * 0.4 * GEO_PI) + y0 * sin(bl * 0.4 * GEO_PI);
+        g->c[1][q] = y0 * cos(bl * 0.4 * GEO_PI) - x0 * sin(bl * 0.4 * GEO_PI);
+        g->c[2][q] = g->c[2][q0];
+      }
+  g->pol[0][0] = 0.0; g->pol[1][0] = 0.0; g->pol[2][0] = 1.0;
+  g->pol[0][1] = 0.0; g->pol[1][1] = 0.0; g->pol[2][1] = -1.0;
+  for (int a = 0; a < 3; ++a) geo_fill_ghosts_d(g, g->c[a], g->pol[a]);
+  for (int bl = 0; bl < 5; ++bl)
+    for (int l = 0; l < nlev; ++l)
+      for (int m = 0; m < 2 * nlev; ++m)
+        g->idx[geo_at(g, bl, l + 1, m + 1)] = bl * 2 * nlev * nlev + l * 2 * nlev + m;
+  g->poli[0] = 10 * nlev * nlev;
+  g->poli[1] = 10 * nlev * nlev + 1;
+  geo_fill_ghosts_i(g, g->idx, g->poli);
+  return 0;
+}
+
+static void geo_free(geo_t *g) {
+  for (int a = 0; a < 3; ++a) free(g->c[a]);
+  free(g->idx);
+}
+
+/* GeodesicGrid::Position (:219-236) */
+static void geo_position(const geo_t *g, int ic, double out[3]) {
+  const int n = g->nlev;
+  const int b0 = ic / (2 * n * n), b1 = (ic % (2 * n * n)) / (2 * n), b2 = (ic % (2 * n * n)) % (2 * n);
+  for (int a = 0; a < 3; ++a)
+    out[a] = (b0 == 5) ? g->pol[a][b2] : g->c[a][geo_at(g, b0, b1 + 1, b2 + 1)];
+}
+
+/* GeodesicGrid::NumNeighbors (:168-206) */
+static int geo_neighbours(const geo_t *g, int ic, int nb[6]) {
+  const int n = g->nlev;
+  if (ic == 10 * n * n) {
+    for (int bl = 0; bl < 5; ++bl) nb[bl] = g->idx[geo_at(g, bl, 1, 1)];
+    return 5;
+  }
+  if (ic == 10 * n * n + 1) {
+    for (int bl = 0; bl < 5; ++bl) nb[bl] = g->idx[geo_at(g, bl, n, 2 * n)];
+    return 5;
+  }
+  const int b0 = ic / (2 * n * n), b1 = (ic % (2 * n * n)) / (2 * n), b2 = (ic % (2 * n * n)) % (2 * n);
+  nb[0] = g->idx[geo_at(g, b0, b1 + 1, b2 + 2)];
+  nb[1] = g->idx[geo_at(g, b0, b1 + 2, b2 + 1)];
+  nb[2] = g->idx[geo_at(g, b0, b1 + 2, b2)];
+  nb[3] = g->idx[geo_at(g, b0, b1 + 1, b2)];
+  nb[4] = g->idx[geo_at(g, b0, b1, b2 + 1)];
+  if (ic % (2 * n * n) == n - 1 || ic % (2 * n * n) == 2 * n - 1) return 5;
+  nb[5] = g->idx[geo_at(g, b0, b1, b2 + 2)];
+  return 6;
+}
+
+/* GeodesicGrid::CircumcenterNormalized (:463-475) */
+static void geo_circumcentre(const double p1[3], const double p2[3], const double p3[3],
+                             double out[3]) {
+  const double x1 = p1[0], x2 = p2[0], x3 = p3[0];
+  const double y1 = p1[1], y2 = p2[1], y3 = p3[1];
+  const double z1 = p1[2], z2 = p2[2], z3 = p3[2];
+  const double a = sqrt((x3 - x2) * (x3 - x2) + (y3 - y2) * (y3 - y2) + (z3 - z2) * (z3 - z2));
+  const double b = sqrt((x1 - x3) * (x1 - x3) + (y1 - y3) * (y1 - y3) + (z1 - z3) * (z1 - z3));
+  const double c = sqrt((x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1) + (z2 - z1) * (z2 - z1));
+  const double den = 1.0 / ((a + c + b) * (a + c - b) * (a + b - c) * (b + c - a));
+  const double xc = (x1 * a * a * (b * b + c * c - a * a) + x2 * b * b * (c * c + a * a - b * b) +
+                     x3 * c * c * (a * a + b * b - c * c)) * den;
+  const double yc = (y1 * a * a * (b * b + c * c - a * a) + y2 * b * b * (c * c + a * a - b * b) +
+                     y3 * c * c * (a * a + b * b - c * c)) * den;
+  const double zc = (z1 * a * a * (b * b + c * c - a * a) + z2 * b * b * (c * c + a * a - b * b) +
+                     z3 * c * c * (a * a + b * b - c * c)) * den;
+  const double nc = sqrt(xc * xc + yc * yc + zc * zc);
+  out[0] = xc / nc;
+  out[1] = yc / nc;
+  out[2] = zc / nc;
+}
+
+/* GeodesicGrid::ComputeWeightAndDualEdges (:312-360): the dual-cell area */
+static double geo_weight(const geo_t *g, int ic) {
+  int nv[6];
+  const int nn = geo_neighbours(g, ic, nv);
+  double p0[3];
+  geo_position(g, ic, p0);
+  double w = 0.0;
+  for (int q = 0; q < nn; ++q) {
+    double n1[3], n2[3], n3[3], c1[3], c2[3];
+    geo_position(g, nv[(q + nn - 1) % nn], n1);
+    geo_position(g, nv[q], n2);
+    geo_position(g, nv[(q + 1) % nn], n3);
+    geo_circumcentre(p0, n1, n2, c1);
+    geo_circumcentre(p0, n2, n3, c2);
+    const double s1 = p0[0] * c1[0] + p0[1] * c1[1] + p0[2] * c1[2];
+    const double s2 = p0[0] * c2[0] + p0[1] * c2[1] + p0[2] * c2[2];
+    const double s12 = c1[0] * c2[0] + c1[1] * c2[1] + c1[2] * c2[2];
+    const double num = fabs(p0[0] * (c1[1] * c2[2] - c2[1] * c1[2]) +
+                            p0[1] * (c2[0] * c1[2] - c1[0] * c2[2]) +
+                            p0[2] * (c1[0] * c2[1] - c1[1] * c2[0]));
+    const double den = 1.0 + s1 + s2 + s12;
+    w += 2.0 * atan(num / den);
+  }
+  return w;
+}
+
+/* SphericalGrid (mesh/spherical_grid.cpp:17-36) over GeodesicGrid */
+int orc_sphere_grid(int nlev, double rad, int bitant, double *geo) {
+  geo_t g;
+  if (geo_init(&g, nlev)) {
+    geo_free(&g);
+    return -1;
+  }
+  const int np = 10 * nlev * nlev + 2;
+  for (int ic = 0; ic < np; ++ic) {
+    double p[3];
+    geo_position(&g, ic, p);
+    const double th = acos(p[2]), ph = atan2(p[1], p[0]);
+    double *o = geo + 6 * (int64_t)ic;
+    o[0] = th;
+    o[1] = ph;
+    o[2] = rad * sin(th) * cos(ph);
+    o[3] = rad * sin(th) * sin(ph);
+    o[4] = rad * cos(th);
+    if (bitant) o[4] = fabs(o[4]);
+    o[5] = rad * rad * geo_weight(&g, ic);
+  }
+  geo_free(&g);
+  return np;
+}
+
+/* gra::sph_harm::Factorial over its table (spherical_harmonics.hpp:20-60) */
+static double sph_fact(int n) {
+  double t = 1.0;
+  for (int i = 1; i <= n; ++i) t = t * (double)i;
+  return t;
+}
+
+void orc_sylm(int s, int l, int m, double theta, double phi, double *re, double *im) {
+  double wd = 0;
+  const int k1 = (0 > m + s) ? 0 : m + s;
+  const int k2 = (l + m < l + s) ? l + m : l + s;
+  for (int k = k1; k <= k2; ++k) {
+    wd += ((k % 2 == 0) ? 1.0 : -1.0) *
+          sqrt(sph_fact(l + m) * sph_fact(l - m) * sph_fact(l - s) * sph_fact(l + s)) *
+          pow(cos(theta / 2.0), (double)(2 * l + m + s - 2 * k)) *
+          pow(sin(theta / 2.0), (double)(2 * k - m - s)) /
+          (sph_fact(l + m - k) * sph_fact(l + s - k) * sph_fact(k) * sph_fact(k - m - s));
+  }
+  const double norm = sqrt((2 * l + 1) / (4.0 * GEO_PI));
+  *re = norm * wd * cos(m * phi);
+  *im = norm * wd * sin(m * phi);
+}
+
+/* LagrangeInterpND<7, 3>::eval of one variable: x innermost, then y, then z */
+static double lagrange_eval3(const double *f, const int nn[3], const int pt[3],
+                             double c[3][TRK_ORDER + 1]) {
+  double vz[TRK_ORDER + 1];
+  for (int ez = 0; ez <= TRK_ORDER; ++ez) {
+    double vy[TRK_ORDER + 1];
+    for (int ey = 0; ey <= TRK_ORDER; ++ey) {
+      const double *row = f + ((int64_t)(pt[2] + ez) * nn[1] + (pt[1] + ey)) * nn[0] + pt[0];
+      double o = 0;
+      for (int i = 0; i <= TRK_ORDER; ++i) o += c[0][i] * row[i];
+      vy[ey] = o;
+    }
+    double o = 0;
+    for (int i = 0; i <= TRK_ORDER; ++i) o += c[1][i] * vy[i];
+    vz[ez] = o;
+  }
+  double o = 0;
+  for (int i = 0; i <= TRK_ORDER; ++i) o += c[2][i] * vz[i];
+  return o;
+}
+
+/* SphericalPatch (spherical_grid.cpp:44-116, vertex collocation) and
+ * WaveExtractLocal::Decompose_multipole (wave_extract.cpp:160-234) */
+int orc_wave_block(const orc_block_t *b, const double *weyl, int np, const double *geo,
+                   double rad, int lmax, int bitant, int *owned, double *psi) {
+  const int nn[3] = {b->nx[0] + 1 + 2 * NG, b->nx[1] + 1 + 2 * NG, b->nx[2] + 1 + 2 * NG};
+  const int64_t nvol = (int64_t)nn[0] * nn[1] * nn[2];
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = b->x[a][NG];
+    hi[a] = b->x[a][NG + b->nx[a]];
+  }
+  int n = 0;
+  for (int ic = 0; ic < np; ++ic) {
+    const double *o = geo + 6 * (int64_t)ic;
+    if (o[2] >= lo[0] && o[2] < hi[0] && o[3] >= lo[1] && o[3] < hi[1] && o[4] >= lo[2] &&
+        o[4] < hi[2])
+      owned[n++] = ic;
+  }
+  double *dr = (double *)malloc(sizeof(double) * (n ? n : 1));
+  double *di = (double *)malloc(sizeof(double) * (n ? n : 1));
+  double *wt = (double *)malloc(sizeof(double) * (n ? n : 1));
+  for (int q = 0; q < n; ++q) {
+    const double *o = geo + 6 * (int64_t)owned[q];
+    double c[3][TRK_ORDER + 1];
+    int pt[3];
+    for (int a = 0; a < 3; ++a) pt[a] = lagrange1d(b->x[a][0], b->dx[a], nn[a], o[2 + a], c[a]);
+    dr[q] = lagrange_eval3(weyl, nn, pt, c);
+    di[q] = lagrange_eval3(weyl + nvol, nn, pt, c);
+    wt[q] = o[5];
+    wt[q] /= rad * rad;
+  }
+  const int nm = 2 * lmax + 1;
+  for (int q = 0; q < (lmax - 1) * nm * 2; ++q) psi[q] = 0.0;
+  for (int l = 2; l < lmax + 1; ++l)
+    for (int m = -l; m < l + 1; ++m) {
+      double pr = 0.0, pi = 0.0;
+      for (int q = 0; q < n; ++q) {
+        const double *o = geo + 6 * (int64_t)owned[q];
+        double yr, yi;
+        orc_sylm(-2, l, m, o[0], o[1], &yr, &yi);
+        const double bz = (bitant && o[0] > GEO_PI / 2) ? -1 : 1;
+        pr += dr[q] * wt[q] * yr + bz * di[q] * wt[q] * yi;
+        pi += bz * di[q] * wt[q] * yr - dr[q] * wt[q] * yi;
+      }
+      psi[((l - 2) * nm + (m + l)) * 2 + 0] = pr;
+      psi[((l - 2) * nm + (m + l)) * 2 + 1] = pi;
+    }
+  free(dr);
+  free(di);
+  free(wt);
+  return n;
+}
+
 /* ---- history sums, outputs/history.cpp:168-200 --------------------------- */
 void orc_hst_accumulate(const orc_block_t *b, const z4c_params_t *opt,
                         const double *con, const double *u, double out[8]) {

@@ -105,6 +105,23 @@ void orc_vc_prolongate(const int nx[3], int nvar, const double *coarse, double *
 void orc_weyl(const orc_block_t *b, const z4c_params_t *p, const double *adm, const double *u,
               const orc_derivs_t *d, double *weyl);
 
+/* ---- psi4 extraction (z4c/wave_extract.cpp, mesh/spherical_grid.cpp,
+ * mesh/geodesic_grid.cpp, utils/spherical_harmonics.hpp) ------------------- */
+/* Vertices of SphericalGrid(nlev, rad, bitant): 10 nlev^2 + 2 rows of
+ * (theta, phi, x, y, z, weight), theta/phi from GeodesicGrid::PositionPolar,
+ * x/y/z from SphericalGrid::Position and weight from
+ * SphericalGrid::ComputeWeight (rad^2 times the dual-cell area). */
+int orc_sphere_grid(int nlev, double rad, int bitant, double *geo);
+/* gra::sph_harm::sYlm (spherical_harmonics.hpp:231-255). */
+void orc_sylm(int s, int l, int m, double theta, double phi, double *re, double *im);
+/* WaveExtractLocal::Decompose_multipole of one MeshBlock on the sphere whose
+ * vertices orc_sphere_grid wrote: the SphericalPatch points of the block
+ * (their vertex indices into owned, their count returned) and the (l, m)
+ * projections of weyl (2 variables, ghosts filled) into psi, laid out
+ * psi[l-2][m+l][re/im] with 2 lmax + 1 entries per l. */
+int orc_wave_block(const orc_block_t *b, const double *weyl, int np, const double *geo,
+                   double rad, int lmax, int bitant, int *owned, double *psi);
+
 /* ---- puncture tracker (z4c/puncture_tracker.cpp) ------------------------ */
 
 /* PunctureTracker::InterpolateShift (:95-129): the shift of block b at pos

@@ -88,6 +88,10 @@ def lib():
         L.orc_adm_to_z4c.argtypes = [bp, pp, dp, dp]
         L.orc_adm_constraints.argtypes = [bp, pp, dp, dp, Dp, dp]
         L.orc_weyl.argtypes = [bp, pp, dp, dp, Dp, dp]
+        L.orc_sphere_grid.argtypes = [C.c_int, C.c_double, C.c_int, dp]
+        L.orc_sylm.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, dp, dp]
+        L.orc_wave_block.argtypes = [bp, dp, C.c_int, dp, C.c_double, C.c_int, C.c_int,
+                                     C.POINTER(C.c_int), dp]
         L.orc_mesh_exchange.argtypes = [mp, C.c_int, dp]
         L.orc_hst_accumulate.argtypes = [bp, pp, dp, dp, dp]
         _lib = L
@@ -204,6 +208,32 @@ def weyl(blk, p, adm, u):
     d = _DerivsHolder(blk, u)
     lib().orc_weyl(C.byref(blk._s), C.byref(p), _ptr(adm), _ptr(u), C.byref(d.d), _ptr(out))
     return out
+
+
+def sphere_grid(nlev, rad, bitant=False):
+    """SphericalGrid(nlev, rad, bitant): rows (theta, phi, x, y, z, weight)."""
+    np_ = 10 * nlev * nlev + 2
+    out = np.zeros((np_, 6))
+    assert lib().orc_sphere_grid(int(nlev), float(rad), int(bitant), _ptr(out)) == np_
+    return out
+
+
+def sylm(s, l, m, theta, phi):
+    re, im = C.c_double(), C.c_double()
+    lib().orc_sylm(s, l, m, float(theta), float(phi), C.byref(re), C.byref(im))
+    return re.value, im.value
+
+
+def wave_block(blk, weyl, geo, rad, lmax, bitant=False):
+    """WaveExtractLocal::Decompose_multipole of one block: (the sphere
+    vertices it owns, psi[l-2][m+l][re/im])."""
+    weyl = np.ascontiguousarray(weyl, dtype=np.float64)
+    geo = np.ascontiguousarray(geo, dtype=np.float64)
+    owned = (C.c_int * len(geo))()
+    psi = np.zeros((lmax - 1, 2 * lmax + 1, 2))
+    n = lib().orc_wave_block(C.byref(blk._s), _ptr(weyl), len(geo), _ptr(geo), float(rad),
+                             int(lmax), int(bitant), owned, _ptr(psi))
+    return np.array(owned[:n], dtype=np.int64), psi
 
 
 def mesh_exchange(nb, nx, bc, u_all):

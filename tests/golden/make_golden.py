@@ -13,7 +13,9 @@ Fixtures (numpy .npz, compressed):
                     history table (outputs/history.cpp columns) and the
                     initial and final states
   weyl_punc2.npz    Z4cWeyl (Re, Im psi4) on the initial state of ops_punc2
-                    and after its one RK4 step
+                    and after its one RK4 step; psi4 extraction (ghost
+                    exchange of the Weyl register, sphere interpolation and
+                    (l, m) projection) of the latter
   refine_vc.npz     the vertex-centred restriction and prolongation operators
                     of one MeshBlock of a statically refined mesh
 Each fixture stores the input-deck parameters it was made with ("params",
@@ -188,24 +190,34 @@ REFINE = dict(test="one_puncture", z4c=PUNCTURE, integ="rk4", bc="extrapolate_ou
               mesh=[(16, -4.0, 4.0, 8)] * 3, extra={}, problem={"punc_ADM_mass": 1.0})
 
 
+# psi4 extraction spheres of the Weyl fixture (<psi4_extraction> block): one
+# sphere inside the domain of ops_punc2 and one that leaves it through the y
+# and z faces
+WAVE = dict(num_radii=2, radius_0=1.5, radius_1=3.0, nlev=6, lmax=4)
+WAVE_DECK = "<psi4_extraction>\n" + "".join(f"{k} = {v}\n" for k, v in WAVE.items())
+
+
 def make_weyl(outdir):
     """Z4cWeyl on the initial state of the ops_punc2 case and after its one
-    RK4 step (the inputs, u0/adm0 and s4_alg/s4_adm, are in ops_punc2.npz);
-    only the Weyl records are stored."""
+    RK4 step (the inputs, u0/adm0 and s4_alg/s4_adm, are in ops_punc2.npz),
+    and the psi4 multipoles of the second on the WAVE spheres; only the Weyl
+    and extraction records are stored."""
     with tempfile.TemporaryDirectory() as tmp:
         rec_path = os.path.join(tmp, "ops.rec")
         inp = os.path.join(tmp, "case.inp")
         with open(inp, "w") as f:
-            f.write(deck(CASES["punc2"], rec_path) + "weyl = true\n")
+            f.write(deck(CASES["punc2"], rec_path) + "weyl = true\n" + WAVE_DECK)
         subprocess.run([os.path.join(REF_BIN, "z4c_ops_ref"), "-i", inp], cwd=tmp, check=True,
                        stdout=subprocess.DEVNULL)
         rec = read_records(rec_path)
     path = os.path.join(outdir, "weyl_punc2.npz")
     # weyl0 on the initial data (K_ab = 0), weyl1 after one RK4 step (K_ab
     # nonzero); a corner of each input state ties them to ops_punc2
+    wave = {k[len("s4_wave_"):]: v for k, v in rec.items() if k.startswith("s4_wave_")}
     np.savez_compressed(path, weyl0=rec["weyl0"], weyl1=rec["s4_weyl"],
                         u0=rec["u0"][:, :1, :1, :1, :1],
-                        s4_alg=rec["s4_alg"][:, :1, :1, :1, :1])
+                        s4_alg=rec["s4_alg"][:, :1, :1, :1, :1],
+                        wave=json.dumps(WAVE), **{"wave_" + k: v for k, v in wave.items()})
     return path
 
 

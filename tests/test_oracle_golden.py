@@ -146,6 +146,36 @@ def test_weyl_psi4(when):
     assert bitwise(w[fin], ref[fin])
 
 
+def test_psi4_extraction():
+    """psi4 extraction after the one RK4 step of ops_punc2, piece by piece
+    against the reference: the SphericalGrid vertices and weights, the ghost
+    exchange of the Weyl register, the SphericalPatch ownership, each block's
+    (l, m) projections and their sum over blocks; two spheres, one of which
+    leaves the domain."""
+    import json
+    c = Case("ops_punc2")
+    z = np.load(os.path.join(GOLDEN, "weyl_punc2.npz"))
+    W = json.loads(str(z["wave"]))
+    wx = c.from_grid(O.mesh_exchange(c.nb, c.nx, c.mesh["bc"], c.to_grid(z["weyl1"])))
+    assert bitwise(wx, z["wave_weylx"])
+    blocks = c.blocks()
+    for n in range(W["num_radii"]):
+        rad = W[f"radius_{n}"]
+        geo = O.sphere_grid(W["nlev"], rad)
+        assert bitwise(geo, z[f"wave_geo{n}"])
+        total = np.zeros_like(z[f"wave_psi{n}"])
+        owned = []
+        for g, b in enumerate(blocks):
+            own, psi = O.wave_block(b, wx[g], geo, rad, W["lmax"])
+            owned += [(g, i) for i in own]
+            assert bitwise(psi, z[f"wave_loc{n}"][g]), (n, g)
+            total = total + psi
+        assert np.array_equal(np.array(owned), z[f"wave_patch{n}"].astype(np.int64))
+        assert bitwise(total, z[f"wave_psi{n}"])
+    assert len(z["wave_patch0"]) == 10 * W["nlev"] ** 2 + 2  # the inner sphere is whole
+    assert 0 < len(z["wave_patch1"]) < 10 * W["nlev"] ** 2 + 2
+
+
 def test_vc_refinement_operators():
     """Restriction (injection) and prolongation (injection + tensor-product
     Lagrange) of one MeshBlock of a statically refined mesh, bit for bit
