@@ -1,8 +1,9 @@
 """Builds the in-tree shared library gr-athena_b200/_build/libz4c_b200.so.
 
 The CUDA sources are compiled for sm_100a only (B200).  -fmad=false keeps
-every multiply and add separately rounded, as the reference CPU build
-(-ffp-contract=off) does.
+every multiply and add of the device code separately rounded, as the
+reference CPU build (-ffp-contract=off) does; the host code (the extraction
+spheres' tables) gets -ffp-contract=off itself.
 """
 import os
 import subprocess
@@ -12,10 +13,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libz4c_b200.so")
-SOURCES = ["z4c_kernels.cu", "z4c_capi.cu", "z4c_refine.cu", "z4c_noalloc.cu"]
+SOURCES = ["z4c_kernels.cu", "z4c_capi.cu", "z4c_refine.cu", "z4c_noalloc.cu", "z4c_wave.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-         "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
+         "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+         "-Xcompiler", "-ffp-contract=off"]
 
 
 def _stale():

@@ -15,6 +15,7 @@
 #include "../../include/z4c_b200.h"
 #include "z4c_common.cuh"
 #include "z4c_kernels.cuh"
+#include "z4c_wave.cuh"
 
 using namespace z4c;
 
@@ -119,6 +120,7 @@ struct z4c_ctx {
   double* trk = nullptr;  // puncture trackers [kMaxTrackers][8]
   int ntrk = 0;
   int* flag = nullptr;
+  std::vector<WaveSphere> waves;  // psi4 extraction spheres
 
   // host copies
   std::vector<double> h_xf, h_xv, h_dx;  // h_dx: [nblocks][3]
@@ -304,6 +306,7 @@ void free_ctx(z4c_ctx* c) {
   for (void* p : {(void*)c->un, (void*)c->guu, (void*)c->sd, (void*)c->rsum, (void*)c->lv, (void*)c->xf, (void*)c->xv, (void*)c->dxd, (void*)c->fd,
                   (void*)c->nbr, (void*)c->partials, (void*)c->flag, (void*)c->trk})
     if (p) cudaFree(p);
+  for (auto& w : c->waves) wave_free(&w);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -747,6 +750,20 @@ int z4c_ghost_fill(z4c_ctx* ctx, int reg) {
   if (!ctx) return fail(Z4C_EINVAL, "null context");
   int rc;
   if ((rc = check_reg(ctx, reg))) return rc;
+  if (reg == Z4C_REG_WEYL) {
+    // Mesh::CommunicateAuxZ4c: the Aux group exchange and physical BCs of the
+    // Weyl register, through the work register
+    double* w = ctx->reg[Z4C_REG_W];
+    launch_exchange(ctx->g, ctx->dev(), ctx->reg[reg], w, ctx->nbr, 0, ctx->stream, Z4C_NWEYL);
+    LAUNCH_CHECK("exchange");
+    if (ctx->has_outflow) {
+      launch_physical_bcs(ctx->g, w, Z4C_NWEYL, ctx->stream);
+      LAUNCH_CHECK("physical_bcs");
+    }
+    CUDA_TRY(cudaMemcpyAsync(ctx->reg[reg], w, sizeof(double) * reg_elems(ctx, reg),
+                             cudaMemcpyDeviceToDevice, ctx->stream));
+    return Z4C_OK;
+  }
   if (reg_nvar_(reg) != Z4C_NVAR) return fail(Z4C_EINVAL, "ghost fill needs a Z4c register");
   if (reg == Z4C_REG_W) return fail(Z4C_EINVAL, "the work register cannot be ghost-filled");
   if ((rc = exchange_into(ctx, ctx->reg[reg], ctx->reg[Z4C_REG_W], false))) return rc;
@@ -761,6 +778,51 @@ int z4c_ghost_fill(z4c_ctx* ctx, int reg) {
                              sizeof(double) * reg_elems(ctx, reg), cudaMemcpyDeviceToDevice,
                              ctx->stream));
   }
+  return Z4C_OK;
+}
+
+int z4c_sphere_grid(int nlev, double rad, int bitant, double* geo) {
+  if (nlev < 1 || nlev > 2000) return fail(Z4C_EINVAL, "nlev %d out of range [1, 2000]", nlev);
+  if (!(rad > 0.0)) return fail(Z4C_EINVAL, "sphere radius must be positive");
+  if (!geo) return fail(Z4C_EINVAL, "null output");
+  const std::vector<double> g = sphere_grid(nlev, rad, bitant != 0);
+  std::memcpy(geo, g.data(), sizeof(double) * g.size());
+  return (int)(g.size() / 6);
+}
+
+int z4c_wave_add(z4c_ctx* ctx, double rad, int nlev, int lmax, int bitant, int* id) {
+  if (!ctx || !id) return fail(Z4C_EINVAL, "null argument");
+  if (nlev < 1 || nlev > 2000) return fail(Z4C_EINVAL, "nlev %d out of range [1, 2000]", nlev);
+  if (lmax < 2 || lmax > 16) return fail(Z4C_EINVAL, "lmax %d out of range [2, 16]", lmax);
+  if (!(rad > 0.0)) return fail(Z4C_EINVAL, "sphere radius must be positive");
+  WaveSphere w;
+  char msg[256] = {0};
+  const int rc = wave_build(ctx->g, ctx->h_xf, ctx->h_dx, rad, nlev, lmax, bitant != 0, &w, msg,
+                            (int)sizeof(msg));
+  if (rc) return fail(rc, "%s", msg);
+  ctx->waves.push_back(w);
+  *id = (int)ctx->waves.size() - 1;
+  return Z4C_OK;
+}
+
+int z4c_wave_points(const z4c_ctx* ctx, int id) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  if (id < 0 || id >= (int)ctx->waves.size()) return fail(Z4C_EINVAL, "no sphere %d", id);
+  return ctx->waves[id].npts;
+}
+
+int z4c_wave_decompose(z4c_ctx* ctx, int id, int reg_weyl, double* psi) {
+  if (!ctx || !psi) return fail(Z4C_EINVAL, "null argument");
+  if (id < 0 || id >= (int)ctx->waves.size()) return fail(Z4C_EINVAL, "no sphere %d", id);
+  int rc;
+  if ((rc = check_reg(ctx, reg_weyl))) return rc;
+  if (reg_nvar_(reg_weyl) != Z4C_NWEYL) return fail(Z4C_EINVAL, "decomposition needs the Weyl register");
+  const WaveSphere& w = ctx->waves[id];
+  launch_wave(ctx->g, w, ctx->reg[reg_weyl], ctx->stream);
+  LAUNCH_CHECK("wave");
+  CUDA_TRY(cudaMemcpyAsync(psi, w.psi, sizeof(double) * 2 * w.nslot, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return Z4C_OK;
 }
 

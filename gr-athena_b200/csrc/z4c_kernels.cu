@@ -807,6 +807,7 @@ __constant__ int c_dir_index[27];  // (o0+1) + 3(o1+1) + 9(o2+1) -> neighbour sl
 // supports in list order: 0, 1, 2, 4, 3, 5, 6, 7
 __device__ __forceinline__ constexpr int u_order(int q) { return (q == 3) ? 4 : (q == 4) ? 3 : q; }
 
+template <int NV>
 __global__ void __launch_bounds__(kPointThreads)
 k_exchange_interior(Grid g, DevParams P, const double* __restrict__ src,
                     double* __restrict__ dst, const int* __restrict__ nbr, int fuse_alg) {
@@ -824,7 +825,7 @@ k_exchange_interior(Grid g, DevParams P, const double* __restrict__ src,
     side[a] = (x == vs) ? -1 : 1;
     if (x == vs || x == ve) smask |= 1 << a;
   }
-  const int64_t bstride = (int64_t)NVAR * g.nvol;
+  const int64_t bstride = (int64_t)NV * g.nvol;
   // source offset of every owner in list order (-1: not an owner)
   int64_t off[8];
   int mult = 1;
@@ -845,12 +846,12 @@ k_exchange_interior(Grid g, DevParams P, const double* __restrict__ src,
     ++mult;
   }
   const double inv = (mult > 1) ? 1.0 / (double)mult : 1.0;
-  double v[NVAR];
+  double v[NV];
 #pragma unroll
-  for (int n = 0; n < NVAR; ++n) v[n] = __ldg(src + off[0] + (int64_t)n * g.nvol);
+  for (int n = 0; n < NV; ++n) v[n] = __ldg(src + off[0] + (int64_t)n * g.nvol);
   if (mult > 1) {
 #pragma unroll
-    for (int n = 0; n < NVAR; ++n) {
+    for (int n = 0; n < NV; ++n) {
       const int64_t vo = (int64_t)n * g.nvol;
       double s = v[n];
 #pragma unroll
@@ -859,7 +860,8 @@ k_exchange_interior(Grid g, DevParams P, const double* __restrict__ src,
       v[n] = s * inv;
     }
   }
-  if (fuse_alg) {
+  if constexpr (NV == NVAR) {
+    if (fuse_alg) {
     double gg[6], AA[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
@@ -872,14 +874,16 @@ k_exchange_interior(Grid g, DevParams P, const double* __restrict__ src,
       v[Z4C_GXX + c] = gg[c];
       v[Z4C_AXX + c] = AA[c];
     }
+    }
   }
   double* db = dst + off[0];
 #pragma unroll
-  for (int n = 0; n < NVAR; ++n) db[(int64_t)n * g.nvol] = v[n];
+  for (int n = 0; n < NV; ++n) db[(int64_t)n * g.nvol] = v[n];
 }
 
 // Ghost vertices: copy of the primary owner's result (zero where the primary
 // owner lies beyond a physical face; the boundary conditions overwrite those).
+template <int NV>
 __global__ void __launch_bounds__(kPointThreads)
 k_exchange_ghosts(Grid g, double* __restrict__ u, const int* __restrict__ nbr) {
   const int per = (int)g.nvol;
@@ -895,22 +899,22 @@ k_exchange_ghosts(Grid g, double* __restrict__ u, const int* __restrict__ nbr) {
     ghost |= (o[a] != 0);
   }
   if (!ghost) return;
-  const int64_t bstride = (int64_t)NVAR * g.nvol;
+  const int64_t bstride = (int64_t)NV * g.nvol;
   double* db = u + (int64_t)b * bstride + p;
   const int nb = __ldg(nbr + b * 26 + c_dir_index[(o[0] + 1) + 3 * (o[1] + 1) + 9 * (o[2] + 1)]);
   if (nb < 0) {
 #pragma unroll
-    for (int n = 0; n < NVAR; ++n) db[(int64_t)n * g.nvol] = 0.0;
+    for (int n = 0; n < NV; ++n) db[(int64_t)n * g.nvol] = 0.0;
     return;
   }
   const double* sb = u + (int64_t)nb * bstride + p -
                      (((int64_t)o[2] * g.nx[2] * g.nn[1] + (int64_t)o[1] * g.nx[1]) * g.nn[0] +
                       (int64_t)o[0] * g.nx[0]);
-  double v[NVAR];
+  double v[NV];
 #pragma unroll
-  for (int n = 0; n < NVAR; ++n) v[n] = sb[(int64_t)n * g.nvol];
+  for (int n = 0; n < NV; ++n) v[n] = sb[(int64_t)n * g.nvol];
 #pragma unroll
-  for (int n = 0; n < NVAR; ++n) db[(int64_t)n * g.nvol] = v[n];
+  for (int n = 0; n < NV; ++n) db[(int64_t)n * g.nvol] = v[n];
 }
 
 // ---- extrapolate_outflow boundary conditions --------------------------------
@@ -1441,15 +1445,23 @@ void launch_boundary_rhs(const Grid& g, const DevParams& P, const double* u, dou
 }
 
 void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst,
-                     const int* nbr, int fuse_alg, cudaStream_t st) {
+                     const int* nbr, int fuse_alg, cudaStream_t st, int nvar) {
   static const int dir_rc = upload_dir_index();  // once per process
   (void)dir_rc;
+  const int64_t ni = div_up(interior_count(g) * g.nblocks, kPointThreads);
+  const int64_t ng = div_up(g.nvol * g.nblocks, kPointThreads);
   COUNTED
-  k_exchange_interior<<<div_up(interior_count(g) * g.nblocks, kPointThreads), kPointThreads, 0,
-                        st>>>(g, P, src, dst, nbr, fuse_alg);
+  if (nvar == Z4C_NWEYL) {
+    k_exchange_interior<Z4C_NWEYL><<<ni, kPointThreads, 0, st>>>(g, P, src, dst, nbr, 0);
+  } else {
+    k_exchange_interior<NVAR><<<ni, kPointThreads, 0, st>>>(g, P, src, dst, nbr, fuse_alg);
+  }
   COUNTED
-  k_exchange_ghosts<<<div_up(g.nvol * g.nblocks, kPointThreads), kPointThreads, 0, st>>>(g, dst,
-                                                                                        nbr);
+  if (nvar == Z4C_NWEYL) {
+    k_exchange_ghosts<Z4C_NWEYL><<<ng, kPointThreads, 0, st>>>(g, dst, nbr);
+  } else {
+    k_exchange_ghosts<NVAR><<<ng, kPointThreads, 0, st>>>(g, dst, nbr);
+  }
 }
 
 void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st) {

@@ -107,7 +107,7 @@ void launch_track_update(double* trk, int ntrk, double dt, cudaStream_t st);
 void launch_boundary_rhs(const Grid& g, const DevParams& P, const double* u, double* rhs,
                          int block0, int nblk, cudaStream_t st);
 void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst,
-                     const int* nbr, int fuse_alg, cudaStream_t st);
+                     const int* nbr, int fuse_alg, cudaStream_t st, int nvar = NVAR);
 void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st);
 void launch_alg_constr(const Grid& g, const DevParams& P, double* u, int block0, int nblk,
                        cudaStream_t st, int ghosts_only = 0);

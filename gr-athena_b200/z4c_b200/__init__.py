@@ -49,7 +49,8 @@ EXPORTS = (
     "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_weyl", "z4c_ghost_fill", "z4c_init_finalize",
     "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
     "z4c_get_tile", "z4c_autotune", "z4c_check_finite", "z4c_kernel_launches", "z4c_rhs_stage",
-    "z4c_fp64_probe", "z4c_tracker_add", "z4c_tracker_get", "z4c_vc_restrict", "z4c_vc_prolongate", "z4c_rhs_noalloc")
+    "z4c_fp64_probe", "z4c_tracker_add", "z4c_tracker_get", "z4c_vc_restrict", "z4c_vc_prolongate", "z4c_rhs_noalloc",
+    "z4c_sphere_grid", "z4c_wave_add", "z4c_wave_points", "z4c_wave_decompose")
 
 
 class Z4cError(RuntimeError):
@@ -134,6 +135,10 @@ def lib():
         L.z4c_vc_prolongate.argtypes = [vp, vp, ip, ip, ipp, ipp, vp]
         L.z4c_rhs_noalloc.argtypes = [vp, vp, ip, C.POINTER(C.c_int), dp,
                                       C.POINTER(Params), vp]
+        L.z4c_sphere_grid.argtypes = [ip, C.c_double, ip, dp]
+        L.z4c_wave_add.argtypes = [vp, C.c_double, ip, ip, ip, ipp]
+        L.z4c_wave_points.argtypes = [vp, ip]
+        L.z4c_wave_decompose.argtypes = [vp, ip, ip, dp]
         L.z4c_kernel_launches.argtypes = []
         L.z4c_kernel_launches.restype = C.c_longlong
         _lib = L
@@ -144,6 +149,62 @@ def _check(rc):
     if rc < 0:
         raise Z4cError(rc, lib().z4c_last_error().decode())
     return rc
+
+
+def sphere_grid(nlev, rad, bitant=False):
+    """SphericalGrid(nlev, rad, bitant) on the host: one row (theta, phi, x,
+    y, z, weight) per geodesic vertex."""
+    out = np.empty((10 * nlev * nlev + 2, 6))
+    _check(lib().z4c_sphere_grid(int(nlev), float(rad), int(bool(bitant)),
+                                 out.ctypes.data_as(C.POINTER(C.c_double))))
+    return out
+
+
+class WaveExtract:
+    """WaveExtract (z4c/wave_extract.cpp): the (l, m) multipoles of psi4 on
+    one coordinate sphere, 2 <= l <= lmax, as psi[l-2, m+l, re/im]; the
+    <psi4_extraction> parameters nlev (default 3), radius_n (10.0), lmax (2),
+    filename ("wave") and <mesh> bitant."""
+
+    def __init__(self, ctx, radius=10.0, nlev=3, lmax=2, bitant=False, filename="wave"):
+        self.ctx, self.radius, self.nlev, self.lmax = ctx, float(radius), int(nlev), int(lmax)
+        i = C.c_int()
+        _check(lib().z4c_wave_add(ctx._h, self.radius, self.nlev, self.lmax, int(bool(bitant)),
+                                  C.byref(i)))
+        self.id = i.value
+        self.psi = np.zeros((self.lmax - 1, 2 * self.lmax + 1, 2))
+        self.ofname = f"{filename}_r{self.radius:05.2f}.txt"
+
+    def num_points(self):
+        """Sphere vertices owned by some MeshBlock."""
+        return _check(lib().z4c_wave_points(self.ctx._h, self.id))
+
+    def ReduceMultipole(self, reg_weyl=REG_WEYL):
+        """Decompose_multipole on every block plus the sum over blocks, from
+        the Weyl register (ghosts filled)."""
+        out = np.zeros_like(self.psi)
+        _check(lib().z4c_wave_decompose(self.ctx._h, self.id, reg_weyl,
+                                        out.ctypes.data_as(C.POINTER(C.c_double))))
+        self.psi = out
+        return out
+
+    def Write(self, iteration, time):
+        """Appends one line to the reference's wave_r<radius>.txt format,
+        writing the column header first when the file is new."""
+        new = not os.path.exists(self.ofname)
+        with open(self.ofname, "a") as f:
+            if new:
+                cols, idx = ["# 1:iter 2:time"], 3
+                for l in range(2, self.lmax + 1):
+                    for m in range(-l, l + 1):
+                        cols.append(f" {idx}:l={l}-m={m}-Re {idx + 1}:l={l}-m={m}-Im")
+                        idx += 2
+                f.write("".join(cols) + "\n")
+            line = [f"{int(iteration)} {time:.17g} "]
+            for l in range(2, self.lmax + 1):
+                for m in range(-l, l + 1):
+                    line.append(f"{self.psi[l - 2, m + l, 0]:.17g} {self.psi[l - 2, m + l, 1]:.17g} ")
+            f.write("".join(line) + "\n")
 
 
 def kernel_launches():
@@ -378,6 +439,17 @@ class Z4c:
         out = np.empty(6)
         _check(lib().z4c_tracker_get(self._h, int(tid), out.ctypes.data_as(C.POINTER(C.c_double))))
         return out[:3], out[3:]
+
+    def psi4_multipoles(self, spheres):
+        """The extraction of the main loop after a step (main.hpp
+        Z4c_DerivedQuantities): Z4cToADM, Z4cWeyl, the Weyl ghost exchange
+        (Mesh::CommunicateAuxZ4c), then ReduceMultipole on every sphere."""
+        self.Z4cToADM()
+        self.Z4cWeyl()
+        self.ghost_fill(REG_WEYL)
+        for w in spheres:
+            w.ReduceMultipole()
+        return [w.psi for w in spheres]
 
     def hst_norms(self):
         out = np.empty(8)

@@ -206,6 +206,30 @@ int z4c_adm_constraints(z4c_ctx *ctx, int reg_con, int reg_adm, int reg_u,
  * first derivatives PrepareZ4cDerivatives stores: this call recomputes
  * them). */
 int z4c_weyl(z4c_ctx *ctx, int reg_adm, int reg_u, int reg_weyl, int block);
+
+/* ---- psi4 extraction (z4c/wave_extract.cpp, mesh/spherical_grid.cpp,
+ * mesh/geodesic_grid.cpp) ---------------------------------------------------
+ * A sphere of radius rad carries the geodesic grid of nlev levels
+ * (10 nlev^2 + 2 vertices); its multipoles psi(l, m), 2 <= l <= lmax, are
+ * laid out as WaveExtract::psi, psi[l-2][m+l][re/im] with 2 lmax + 1 slots
+ * per l (slots m + l > 2 l stay 0).  The extraction sequence of the main
+ * loop (main.hpp Z4c_DerivedQuantities) is z4c_weyl, then
+ * z4c_ghost_fill(Z4C_REG_WEYL) (Mesh::CommunicateAuxZ4c), then
+ * z4c_wave_decompose per sphere (Decompose_multipole + ReduceMultipole). */
+/* SphericalGrid(nlev, rad, bitant): writes (theta, phi, x, y, z, weight) per
+ * vertex into geo (6 (10 nlev^2 + 2) doubles); returns the vertex count.
+ * Host only, no context. */
+int z4c_sphere_grid(int nlev, double rad, int bitant, double *geo);
+/* WaveExtract(pmesh, pin, n) + WaveExtractLocal on every block: sets up a
+ * sphere on the context's mesh (vertex ownership, interpolation stencils,
+ * spin-weight -2 harmonics); *id numbers the context's spheres from 0. */
+int z4c_wave_add(z4c_ctx *ctx, double rad, int nlev, int lmax, int bitant, int *id);
+/* Number of sphere vertices owned by some MeshBlock (SphericalPatch sizes). */
+int z4c_wave_points(const z4c_ctx *ctx, int id);
+/* Decompose_multipole on every block and ReduceMultipole: the multipoles of
+ * reg_weyl (ghosts filled) into the host array psi, (lmax-1)(2 lmax+1) 2
+ * doubles; returns when psi is written. */
+int z4c_wave_decompose(z4c_ctx *ctx, int id, int reg_weyl, double *psi);
 /* GR_Z4c SEND/RECV/SETB_Z4C + PHY_BVAL (comm/comm_registry.cpp:336-382,
  * comm/physical_bcs.cpp:506-670): same-level vertex-centred ghost fill by
  * device copy, shared vertices averaged over their owners, then the
