@@ -52,6 +52,12 @@ FP64_OPS_PER_POINT_STAGE = 7697 + 154
 # vertex (ncu dram__bytes_read.sum + dram__bytes_write.sum summed over them,
 # 64-block capture scaled by the vertex count; see profiles/).
 STAGE_KERNELS = "k_prep, k_ricci, k_adv, k_main, k_ko_stage_ls"
+# FP64 operations of PrepareZ4cDerivatives + Z4cWeyl per interior vertex
+# (oracle/opcount), for the psi4 diagnostics line.
+FP64_OPS_PER_POINT_WEYL = 7409
+# psi4 extraction spheres of the diagnostics: (radius, nlev, lmax) inside
+# the [-16,16]^3 domain
+WAVE_SPHERES = ((6.0, 30, 8), (12.0, 30, 8))
 STAGE_TRAFFIC_PER_POINT = 1278.0e6 / (64 * 17 ** 3)
 
 
@@ -188,6 +194,56 @@ def run_oracle_cpu(max_seconds=20.0):
     zones = 16 ** 3
     # one zone-update = 4 RHS evaluations (the stage updates are negligible)
     return n * zones / el / 4.0, n
+
+
+def psi4_diagnostics(Z, ctx, stream, npts, nblocks, with_cpu):
+    """Times Z4cWeyl alone (k_prep + k_weyl on every block) and the whole
+    extraction sequence of the main loop (Z4cToADM, Z4cWeyl, Weyl ghost
+    exchange, interpolation and (l, m) projection on WAVE_SPHERES, psi on
+    the host) with CUDA events, median of 5; the oracle's Z4cWeyl on one
+    MeshBlock, single thread, as the CPU figure."""
+    import torch
+    spheres = [Z.WaveExtract(ctx, r, nlev, lmax) for r, nlev, lmax in WAVE_SPHERES]
+
+    def timed(fn, reps=5):
+        out = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+            torch.cuda.synchronize()
+            out.append(e0.elapsed_time(e1))
+        return sorted(out)[len(out) // 2]
+
+    with torch.cuda.stream(stream):
+        ctx.psi4_multipoles(spheres)  # warm-up
+    torch.cuda.synchronize()
+    weyl_ms = timed(lambda: ctx.Z4cWeyl())
+    extract_ms = timed(lambda: ctx.psi4_multipoles(spheres))
+    tf = FP64_OPS_PER_POINT_WEYL * npts / (weyl_ms * 1e-3) / 1e12
+    out = {"weyl_ms": weyl_ms, "extraction_ms": extract_ms,
+           "weyl_tflops": tf, "fp64_ops_per_vertex": FP64_OPS_PER_POINT_WEYL,
+           "spheres": [{"radius": w.radius, "nlev": w.nlev, "lmax": w.lmax,
+                        "points": w.num_points()} for w in spheres],
+           "psi22_re_r6": float(spheres[0].psi[0, 4, 0]),
+           "note": "weyl_ms: k_prep + k_weyl on all MeshBlocks; extraction_ms: Z4cToADM, "
+                   "Z4cWeyl, Weyl ghost exchange and both spheres' multipoles to the host"}
+    if with_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import z4c_oracle as O
+        mesh = ctx.mesh
+        xs, dxs = mesh.block_coords(0)
+        blk = O.Block(mesh.nx, dxs, xs)
+        u = ctx.download(Z.REG_U, block=0)
+        adm = ctx.download(Z.REG_ADM, block=0)
+        t0 = time.perf_counter()
+        O.weyl(blk, O.default_params(**PARAMS), adm, u)
+        per_block = time.perf_counter() - t0
+        out["cpu_port_ms_all_blocks"] = per_block * nblocks * 1e3
+        out["cpu_sample"] = "C oracle Z4cWeyl on one MeshBlock, single thread, times the block count"
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -350,6 +406,10 @@ def main():
     e2e_value = whole_job_rate(zones * e2e_steps, world, e2e_s)
     state_bytes = host_np.nbytes
 
+    # ---- psi4 diagnostics: Z4cWeyl, then the extraction sequence ------------
+    psi4 = psi4_diagnostics(Z, ctx, stream, npts, mesh.nblocks, rank == 0 and world == 1
+                            and not args.no_cpu_baseline)
+
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -405,6 +465,7 @@ def main():
                         "and history norms to host, state back to host"},
         "gpu_launches": launches,
         "clocks": clocks,
+        "psi4": psi4,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

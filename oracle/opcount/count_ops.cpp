@@ -110,12 +110,23 @@ int main(int argc, char** argv) {
   orc_rhs(&b, &opt, u, &d, rhs);
   const unsigned long long r_add = opcount::add, r_mul = opcount::mul, r_div = opcount::div,
                            r_fn = opcount::fn;
+  // Z4cWeyl after PrepareZ4cDerivatives on the ADM image of the same state
+  CReal* adm = (CReal*)calloc((size_t)Z4C_NADM * nvol, sizeof(CReal));
+  CReal* weyl = (CReal*)calloc((size_t)2 * nvol, sizeof(CReal));
+  orc_z4c_to_adm(&b, &opt, u, adm);
+  opcount::add = opcount::mul = opcount::div = opcount::fn = opcount::cmp = 0;
+  orc_prepare_derivs(&b, u, &d);
+  orc_weyl(&b, &opt, adm, u, &d, weyl);
+  const unsigned long long w_all = opcount::add + opcount::mul + opcount::div + opcount::fn;
+  const unsigned long long w_div = opcount::div, w_fn = opcount::fn;
   const double P = (double)npts;
   printf("{\"nx\": %d, \"interior_vertices\": %lld, "
          "\"rhs\": {\"add\": %.3f, \"mul\": %.3f, \"div\": %.3f, \"fn\": %.3f, \"total\": %.3f}, "
-         "\"stage\": {\"total\": %d}}\n",
+         "\"stage\": {\"total\": %d}, "
+         "\"weyl\": {\"div\": %.3f, \"fn\": %.3f, \"total\": %.3f}}\n",
          nx, (long long)npts, r_add / P, r_mul / P, r_div / P, r_fn / P,
-         (r_add + r_mul + r_div + r_fn) / P, 7 * Z4C_NVAR);
+         (r_add + r_mul + r_div + r_fn) / P, 7 * Z4C_NVAR, w_div / P, w_fn / P, w_all / P);
+  free(adm); free(weyl);
   orc_derivs_free(&d);
   free(u); free(rhs); free(x);
   return 0;

@@ -20,3 +20,5 @@ def test_fp64_operation_count_matches_bench_constant():
     # nearly all of it is separately rounded adds and multiplies: the FP64
     # pipe sees one instruction per operation
     assert out["rhs"]["div"] < 3 and out["rhs"]["fn"] < 10
+    # PrepareZ4cDerivatives + Z4cWeyl, the psi4 diagnostics figure
+    assert round(out["weyl"]["total"]) == bench.FP64_OPS_PER_POINT_WEYL
