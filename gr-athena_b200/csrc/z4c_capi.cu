@@ -15,6 +15,7 @@
 #include "../../include/z4c_b200.h"
 #include "z4c_common.cuh"
 #include "z4c_kernels.cuh"
+#include "z4c_restart.cuh"
 #include "z4c_wave.cuh"
 
 using namespace z4c;
@@ -95,6 +96,7 @@ int set_error(int code, const char* msg) {
 
 struct z4c_ctx {
   Grid g{};
+  z4c_mesh_desc_t desc{};
   z4c_params_t params{};
   int integrator = Z4C_INTEG_RK4;
   int device = 0;
@@ -374,6 +376,7 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
   z4c_ctx* c = new (std::nothrow) z4c_ctx();
   if (!c) return fail(Z4C_ENOMEM, "host allocation");
   cudaGetDevice(&c->device);
+  c->desc = *mesh;
   c->params = *params;
   c->integrator = integrator;
   Grid& g = c->g;
@@ -1072,6 +1075,56 @@ int z4c_tracker_add(z4c_ctx* ctx, const double pos[3], int* id) {
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   *id = ctx->ntrk++;
   drop_graph(ctx);  // the captured step must include the new tracker
+  return Z4C_OK;
+}
+
+int z4c_restart_load(z4c_ctx* ctx, const char* path, z4c_restart_info_t* info_out) {
+  if (!ctx || !path) return fail(Z4C_EINVAL, "null argument");
+  z4c_restart_info_t info;
+  std::string text, err;
+  std::vector<double> u;
+  int rc = restart_read_file(path, &info, &text, &u, &err);
+  if (rc) return fail(rc, "%s", err.c_str());
+  for (int a = 0; a < 3; ++a)
+    if (info.nb[a] != ctx->g.nb[a] || info.block_nx[a] != ctx->g.nx[a] ||
+        info.xmin[a] != ctx->desc.xmin[a] || info.xmax[a] != ctx->desc.xmax[a])
+      return fail(Z4C_EINVAL, "restart file %s holds another mesh than this context's", path);
+  if (ctx->ntrk != 0 && ctx->ntrk != info.ntrackers)
+    return fail(Z4C_ESTATE, "the context has %d trackers, the restart file %d", ctx->ntrk,
+                info.ntrackers);
+  CUDA_TRY(cudaMemcpyAsync(ctx->reg[Z4C_REG_U], u.data(), sizeof(double) * u.size(),
+                           cudaMemcpyHostToDevice, ctx->stream));
+  for (int t = 0; t < info.ntrackers; ++t) {
+    const double* r = info.trackers[t];
+    const double rec[8] = {r[0], r[1], r[2], r[3], r[4], r[5], 0.0, 0.0};
+    CUDA_TRY(cudaMemcpyAsync(ctx->trk + 8 * t, rec, sizeof(rec), cudaMemcpyHostToDevice,
+                             ctx->stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  ctx->ntrk = info.ntrackers;
+  drop_graph(ctx);
+  if (info_out) *info_out = info;
+  return Z4C_OK;
+}
+
+int z4c_restart_save(z4c_ctx* ctx, const char* path, const char* par_text, double time,
+                     double dt, int ncycle) {
+  if (!ctx || !path) return fail(Z4C_EINVAL, "null argument");
+  std::vector<double> u((size_t)reg_elems(ctx, Z4C_REG_U));
+  std::vector<double> trk((size_t)8 * (ctx->ntrk > 0 ? ctx->ntrk : 1));
+  CUDA_TRY(cudaMemcpyAsync(u.data(), ctx->reg[Z4C_REG_U], sizeof(double) * u.size(),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  if (ctx->ntrk > 0)
+    CUDA_TRY(cudaMemcpyAsync(trk.data(), ctx->trk, sizeof(double) * 8 * ctx->ntrk,
+                             cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  std::vector<double> t6((size_t)6 * (ctx->ntrk > 0 ? ctx->ntrk : 1));
+  for (int t = 0; t < ctx->ntrk; ++t)
+    for (int q = 0; q < 6; ++q) t6[6 * t + q] = trk[8 * t + q];
+  std::string err;
+  const int rc = restart_write_file(path, par_text ? par_text : "", ctx->desc, u.data(), time, dt,
+                                    ncycle, ctx->ntrk, t6.data(), &err);
+  if (rc) return fail(rc, "%s", err.c_str());
   return Z4C_OK;
 }
 

@@ -50,7 +50,9 @@ EXPORTS = (
     "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
     "z4c_get_tile", "z4c_autotune", "z4c_check_finite", "z4c_kernel_launches", "z4c_rhs_stage",
     "z4c_fp64_probe", "z4c_tracker_add", "z4c_tracker_get", "z4c_vc_restrict", "z4c_vc_prolongate", "z4c_rhs_noalloc",
-    "z4c_sphere_grid", "z4c_wave_add", "z4c_wave_points", "z4c_wave_decompose")
+    "z4c_sphere_grid", "z4c_wave_add", "z4c_wave_points", "z4c_wave_decompose",
+    "z4c_restart_info", "z4c_restart_text", "z4c_restart_read", "z4c_restart_write_host",
+    "z4c_restart_load", "z4c_restart_save")
 
 
 class Z4cError(RuntimeError):
@@ -71,6 +73,15 @@ class Params(C.Structure):
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class RestartInfo(C.Structure):
+    _fields_ = [("nbtotal", C.c_int), ("root_level", C.c_int), ("xmin", C.c_double * 3),
+                ("xmax", C.c_double * 3), ("xrat", C.c_double * 3), ("mesh_nx", C.c_int * 3),
+                ("time", C.c_double), ("dt", C.c_double), ("ncycle", C.c_int),
+                ("datasize", C.c_ulonglong), ("nb", C.c_int * 3), ("block_nx", C.c_int * 3),
+                ("ntrackers", C.c_int), ("trackers", (C.c_double * 6) * 8),
+                ("text_bytes", C.c_longlong)]
 
 
 class MeshDesc(C.Structure):
@@ -139,6 +150,15 @@ def lib():
         L.z4c_wave_add.argtypes = [vp, C.c_double, ip, ip, ip, ipp]
         L.z4c_wave_points.argtypes = [vp, ip]
         L.z4c_wave_decompose.argtypes = [vp, ip, ip, dp]
+        cp = C.c_char_p
+        L.z4c_restart_info.argtypes = [cp, C.POINTER(RestartInfo)]
+        L.z4c_restart_text.argtypes = [cp, C.c_char_p, C.c_longlong]
+        L.z4c_restart_text.restype = C.c_longlong
+        L.z4c_restart_read.argtypes = [cp, dp]
+        L.z4c_restart_write_host.argtypes = [cp, cp, C.POINTER(MeshDesc), dp, C.c_double,
+                                             C.c_double, ip, ip, dp]
+        L.z4c_restart_load.argtypes = [vp, cp, C.POINTER(RestartInfo)]
+        L.z4c_restart_save.argtypes = [vp, cp, cp, C.c_double, C.c_double, ip]
         L.z4c_kernel_launches.argtypes = []
         L.z4c_kernel_launches.restype = C.c_longlong
         _lib = L
@@ -277,6 +297,79 @@ class Mesh:
     def zones(self):
         """Cells of the mesh (the reference's zone count, mesh.hpp:289-292)."""
         return self.nblocks * self.nx[0] * self.nx[1] * self.nx[2]
+
+    @classmethod
+    def from_restart(cls, path):
+        """The mesh of a reference restart file: block grid and bounds from
+        its header, boundary conditions from its <mesh> block."""
+        info = restart_info(path)
+        text = restart_text(path)
+        bc = []
+        for a in (1, 2, 3):
+            for side in ("i", "o"):
+                v = _param(text, "mesh", f"{side}x{a}_bc")
+                bc.append(BC_NAMES[v or "periodic"])
+        return cls(info["nb"], info["block_nx"], info["xmin"], info["xmax"], bc)
+
+
+def _param(text, block, key):
+    """Value of key in <block> of an input or restart parameter text."""
+    inside = False
+    for line in text.splitlines():
+        s = line.split("#", 1)[0].strip()
+        if s.startswith("<"):
+            inside = s.startswith(f"<{block}>")
+            continue
+        if inside and "=" in s:
+            k, v = s.split("=", 1)
+            if k.strip() == key:
+                return v.strip()
+    return None
+
+
+def _info_dict(I):
+    return dict(nbtotal=I.nbtotal, root_level=I.root_level, xmin=tuple(I.xmin),
+                xmax=tuple(I.xmax), xrat=tuple(I.xrat), mesh_nx=tuple(I.mesh_nx), time=I.time,
+                dt=I.dt, ncycle=I.ncycle, datasize=I.datasize, nb=tuple(I.nb),
+                block_nx=tuple(I.block_nx),
+                trackers=[tuple(I.trackers[t]) for t in range(I.ntrackers)])
+
+
+def restart_info(path):
+    """Header of a reference restart file (outputs/restart.cpp layout)."""
+    I = RestartInfo()
+    _check(lib().z4c_restart_info(os.fsencode(path), C.byref(I)))
+    return _info_dict(I)
+
+
+def restart_text(path):
+    """Parameter text of a restart file, through the byte after <par_end>."""
+    n = _check(lib().z4c_restart_text(os.fsencode(path), None, 0))
+    buf = C.create_string_buffer(n + 1)
+    lib().z4c_restart_text(os.fsencode(path), buf, n + 1)
+    return buf.raw[:n].decode()
+
+
+def restart_read(path):
+    """(header, state): the Z4c state of every MeshBlock of a restart file,
+    [block][var][k][j][i] with blocks in grid order."""
+    info = restart_info(path)
+    nn = [n + 1 + 2 * NG for n in info["block_nx"]]
+    u = np.empty((info["nbtotal"], NVAR, nn[2], nn[1], nn[0]))
+    _check(lib().z4c_restart_read(os.fsencode(path), u.ctypes.data_as(C.POINTER(C.c_double))))
+    return info, u
+
+
+def restart_write(path, par_text, mesh, u, time, dt, ncycle, trackers=()):
+    """RestartOutput::WriteOutputFile from host data: u in grid order,
+    trackers as (x, y, z, betax, betay, betaz) rows."""
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    assert u.shape == (mesh.nblocks, NVAR) + tuple(reversed(mesh.nn))
+    t = np.ascontiguousarray(np.asarray(trackers, dtype=np.float64).reshape(-1, 6))
+    _check(lib().z4c_restart_write_host(
+        os.fsencode(path), par_text.encode(), C.byref(mesh.desc()),
+        u.ctypes.data_as(C.POINTER(C.c_double)), float(time), float(dt), int(ncycle), len(t),
+        t.ctypes.data_as(C.POINTER(C.c_double)) if len(t) else None))
 
 
 class Z4c:
@@ -439,6 +532,20 @@ class Z4c:
         out = np.empty(6)
         _check(lib().z4c_tracker_get(self._h, int(tid), out.ctypes.data_as(C.POINTER(C.c_double))))
         return out[:3], out[3:]
+
+    def restart_load(self, path):
+        """Mesh restart constructor: state and puncture trackers of a reference
+        restart file into this context; returns the header (time, dt,
+        ncycle, ...)."""
+        I = RestartInfo()
+        _check(lib().z4c_restart_load(self._h, os.fsencode(path), C.byref(I)))
+        return _info_dict(I)
+
+    def restart_save(self, path, par_text, time, dt, ncycle):
+        """RestartOutput::WriteOutputFile for this context's state and
+        trackers; par_text is the parameter text the reference re-reads."""
+        _check(lib().z4c_restart_save(self._h, os.fsencode(path), par_text.encode(),
+                                      float(time), float(dt), int(ncycle)))
 
     def psi4_multipoles(self, spheres):
         """The extraction of the main loop after a step (main.hpp

@@ -207,6 +207,50 @@ int z4c_adm_constraints(z4c_ctx *ctx, int reg_con, int reg_adm, int reg_u,
  * them). */
 int z4c_weyl(z4c_ctx *ctx, int reg_adm, int reg_u, int reg_weyl, int block);
 
+/* ---- restart files (outputs/restart.cpp:43-352; read back by the Mesh
+ * restart constructor, mesh/mesh.cpp:775-1420) -------------------------------
+ * The Z4c vacuum build on a uniform mesh: the parameter text, the header,
+ * the puncture trackers as the only user Mesh data, the ID list and each
+ * MeshBlock's storage.u, blocks in gid order. */
+#define Z4C_MAX_TRACKERS 8
+typedef struct z4c_restart_info {
+  int nbtotal;           /* MeshBlocks */
+  int root_level;
+  double xmin[3], xmax[3], xrat[3];  /* Mesh::mesh_size */
+  int mesh_nx[3];        /* cells of the whole mesh per axis */
+  double time, dt;
+  int ncycle;
+  unsigned long long datasize;  /* bytes per MeshBlock */
+  int nb[3];             /* MeshBlocks per axis */
+  int block_nx[3];       /* cells per MeshBlock axis */
+  int ntrackers;         /* puncture trackers (<z4c> npunct) */
+  double trackers[Z4C_MAX_TRACKERS][6];  /* position, shift there (pos, betap) */
+  long long text_bytes;  /* parameter text through the byte after <par_end> */
+} z4c_restart_info_t;
+/* Reads the header of a restart file (no context). */
+int z4c_restart_info(const char *path, z4c_restart_info_t *info);
+/* Copies the parameter text (NUL-terminated, at most cap - 1 bytes) into
+ * buf; returns its full length.  buf may be null to ask for the length. */
+long long z4c_restart_text(const char *path, char *buf, long long cap);
+/* The state of every MeshBlock into the host array u, [block][var][k][j][i]
+ * with blocks in context order l0 + nb0 (l1 + nb1 l2) (no context). */
+int z4c_restart_read(const char *path, double *u);
+/* Writes a restart file from host data (no context): par_text is the
+ * parameter text the reference re-reads (an input deck or the text of
+ * another restart file; "<par_end>" is appended when missing), u as for
+ * z4c_restart_read, trackers[n][6] = position, shift there. */
+int z4c_restart_write_host(const char *path, const char *par_text,
+                           const z4c_mesh_desc_t *mesh, const double *u, double time,
+                           double dt, int ncycle, int ntrackers, const double *trackers);
+/* The Mesh restart constructor for this context: checks that the file's mesh
+ * is the context's, loads storage.u into Z4C_REG_U and the puncture trackers
+ * (added when the context has none); *info receives the header (may be
+ * null).  Ghosts are loaded as stored, as the reference does. */
+int z4c_restart_load(z4c_ctx *ctx, const char *path, z4c_restart_info_t *info);
+/* RestartOutput::WriteOutputFile for this context's Z4C_REG_U and trackers. */
+int z4c_restart_save(z4c_ctx *ctx, const char *path, const char *par_text, double time,
+                     double dt, int ncycle);
+
 /* ---- psi4 extraction (z4c/wave_extract.cpp, mesh/spherical_grid.cpp,
  * mesh/geodesic_grid.cpp) ---------------------------------------------------
  * A sphere of radius rad carries the geodesic grid of nlev levels

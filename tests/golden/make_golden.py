@@ -16,6 +16,9 @@ Fixtures (numpy .npz, compressed):
                     and after its one RK4 step; psi4 extraction (ghost
                     exchange of the Weyl register, sphere interpolation and
                     (l, m) projection) of the latter
+  restart_track4.npz  the reference's restart file of the evol_track4 run
+                    without its MeshBlock data (that is evol_track4's final
+                    state)
   refine_vc.npz     the vertex-centred restriction and prolongation operators
                     of one MeshBlock of a statically refined mesh
 Each fixture stores the input-deck parameters it was made with ("params",
@@ -242,6 +245,36 @@ def make_refine(outdir):
     return path
 
 
+RST_DECK = "<output2>\nfile_type = rst\ndt = 1e10\n"
+
+
+def make_restart(outdir):
+    """The restart file the stock reference driver writes at the end of the
+    evol_track4 run (<output2> file_type = rst): everything before the
+    MeshBlock data (parameter text, header, the tracker record, ID list) is
+    stored; the data section is the run's final state, which evol_track4.npz
+    already holds (checked here), so the test rebuilds the file byte for
+    byte."""
+    case = EVOL["track4"]
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = os.path.join(tmp, "case.inp")
+        final = os.path.join(tmp, "final.rec")
+        with open(inp, "w") as f:
+            f.write(deck(case, "unused", nlim=case["nlim"], dump_final=final) + RST_DECK)
+        subprocess.run([os.path.join(REF_BIN, "athena_ref"), "-i", inp], cwd=tmp, check=True,
+                       stdout=subprocess.DEVNULL)
+        raw = open(os.path.join(tmp, "golden.final.rst"), "rb").read()
+        u = read_records(final)["u"]
+    data = u.astype("<f8").tobytes()
+    assert raw.endswith(data), "restart data section is not the final state in gid order"
+    ev = np.load(os.path.join(outdir, "evol_track4.npz"))
+    assert np.array_equal(ev["u_final"], u), "evol_track4 fixture is stale"
+    prefix = np.frombuffer(raw[:len(raw) - len(data)], dtype=np.uint8)
+    path = os.path.join(outdir, "restart_track4.npz")
+    np.savez_compressed(path, prefix=prefix, rst_deck=RST_DECK)
+    return path
+
+
 def main():
     only = set(sys.argv[1:])  # fixture names to (re)make; all when empty
     if not only or "weyl_punc2" in only:
@@ -259,6 +292,9 @@ def main():
         if only and f"evol_{name}" not in only:
             continue
         p = make_evol(name, case, HERE)
+        print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
+    if not only or "restart_track4" in only:  # needs evol_track4
+        p = make_restart(HERE)
         print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
 
 
