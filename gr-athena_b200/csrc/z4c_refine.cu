@@ -183,6 +183,24 @@ int setup(const int nx[3], int nvar, int nblocks, const int box[6], RefGeom& G, 
   return Z4C_OK;
 }
 
+// Regrid transfer copies between a MeshBlock and the coarse buffer, one
+// thread per (variable, coarse vertex) of the box lo..hi (inclusive):
+// to_coarse: coarse(c) = fine(f0 + c - lo); otherwise fine(f0 + c - lo) = coarse(c).
+__global__ void k_regrid_copy(int nvar, int3 nn, int3 cn, int3 lo, int3 hi, int3 f0,
+                              const double* __restrict__ src, double* __restrict__ dst,
+                              int to_coarse) {
+  const int ex = hi.x - lo.x + 1, ey = hi.y - lo.y + 1, ez = hi.z - lo.z + 1;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)ex * ey * ez * nvar) return;
+  const int i = (int)(t % ex), j = (int)((t / ex) % ey), k = (int)((t / ((int64_t)ex * ey)) % ez);
+  const int n = (int)(t / ((int64_t)ex * ey * ez));
+  const int64_t fv = (int64_t)nn.x * nn.y * nn.z, cv = (int64_t)cn.x * cn.y * cn.z;
+  const int64_t c = n * cv + ((int64_t)(lo.z + k) * cn.y + (lo.y + j)) * cn.x + (lo.x + i);
+  const int64_t f = n * fv + ((int64_t)(f0.z + k) * nn.y + (f0.y + j)) * nn.x + (f0.x + i);
+  if (to_coarse) dst[c] = src[f];
+  else dst[f] = src[c];
+}
+
 int launched(const char* what) {
   const cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) return Z4C_OK;
@@ -219,4 +237,67 @@ extern "C" int z4c_vc_prolongate(const double* coarse, double* fine, int nblocks
       G, coarse, fine, nblocks);
   add_kernel_launches(1);
   return launched("z4c_vc_prolongate");
+}
+
+namespace {
+
+int regrid_geom(const int nx[3], int nvar, const int oct[3], int3* nn, int3* cn) {
+  if (!nx || !oct) return set_error(Z4C_EINVAL, "regrid transfer: null argument");
+  if (nvar < 1) return set_error(Z4C_EINVAL, "regrid transfer: nvar < 1");
+  for (int a = 0; a < 3; ++a) {
+    if (nx[a] < 2 * NG || nx[a] % 2)
+      return set_error(Z4C_EINVAL, "regrid transfer: nx must be even and >= 2*ng");
+    if (oct[a] != 0 && oct[a] != 1) return set_error(Z4C_EINVAL, "regrid transfer: octant is 0 or 1 per axis");
+  }
+  *nn = make_int3(nx[0] + 1 + 2 * NG, nx[1] + 1 + 2 * NG, nx[2] + 1 + 2 * NG);
+  *cn = make_int3(nx[0] / 2 + 1 + 2 * NCG, nx[1] / 2 + 1 + 2 * NCG, nx[2] / 2 + 1 + 2 * NCG);
+  return Z4C_OK;
+}
+
+}  // namespace
+
+// AMRRegistry::FillSameRankCoarseToFine (comm/amr_registry.cpp:1015-1233),
+// vertex-centred branch: the parent's vertices around the child octant, NCG
+// coarse ghosts included, into the coarse buffer, then the prolongation over
+// the child's interior vertices.
+extern "C" int z4c_regrid_refine(const double* parent, double* child, double* coarse, int nvar,
+                                 const int nx[3], const int oct[3], void* stream) {
+  if (!parent || !child || !coarse) return set_error(Z4C_EINVAL, "z4c_regrid_refine: null array");
+  int3 nn, cn;
+  int rc = regrid_geom(nx, nvar, oct, &nn, &cn);
+  if (rc) return rc;
+  constexpr int ndg = NCG < NG ? NCG : NG;
+  const int3 lo = make_int3(NCG - ndg, NCG - ndg, NCG - ndg);
+  const int3 hi = make_int3(NCG + nx[0] / 2 + ndg, NCG + nx[1] / 2 + ndg, NCG + nx[2] / 2 + ndg);
+  const int3 f0 = make_int3(oct[0] * (nx[0] / 2) + NG - ndg, oct[1] * (nx[1] / 2) + NG - ndg,
+                            oct[2] * (nx[2] / 2) + NG - ndg);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t n = (int64_t)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1) * nvar;
+  k_regrid_copy<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(nvar, nn, cn, lo, hi, f0, parent,
+                                                             coarse, 1);
+  add_kernel_launches(1);
+  if ((rc = launched("z4c_regrid_refine"))) return rc;
+  const int box[6] = {NCG, NCG + nx[0] / 2, NCG, NCG + nx[1] / 2, NCG, NCG + nx[2] / 2};
+  return z4c_vc_prolongate(coarse, child, 1, nvar, nx, box, stream);
+}
+
+// AMRRegistry::FillSameRankFineToCoarse (:814-1012), vertex-centred branch:
+// the child's interior restricted (injection) into the coarse buffer, then
+// copied into the parent's octant.
+extern "C" int z4c_regrid_derefine(const double* child, double* parent, double* coarse, int nvar,
+                                   const int nx[3], const int oct[3], void* stream) {
+  if (!parent || !child || !coarse) return set_error(Z4C_EINVAL, "z4c_regrid_derefine: null array");
+  int3 nn, cn;
+  int rc = regrid_geom(nx, nvar, oct, &nn, &cn);
+  if (rc) return rc;
+  const int box[6] = {NCG, NCG + nx[0] / 2, NCG, NCG + nx[1] / 2, NCG, NCG + nx[2] / 2};
+  if ((rc = z4c_vc_restrict(child, coarse, 1, nvar, nx, box, stream))) return rc;
+  const int3 lo = make_int3(box[0], box[2], box[4]), hi = make_int3(box[1], box[3], box[5]);
+  const int3 f0 = make_int3(NG + oct[0] * (nx[0] / 2), NG + oct[1] * (nx[1] / 2),
+                            NG + oct[2] * (nx[2] / 2));
+  const int64_t n = (int64_t)(hi.x - lo.x + 1) * (hi.y - lo.y + 1) * (hi.z - lo.z + 1) * nvar;
+  k_regrid_copy<<<(unsigned)((n + 255) / 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      nvar, nn, cn, lo, hi, f0, coarse, parent, 0);
+  add_kernel_launches(1);
+  return launched("z4c_regrid_derefine");
 }

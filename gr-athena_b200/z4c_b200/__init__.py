@@ -49,7 +49,8 @@ EXPORTS = (
     "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_weyl", "z4c_ghost_fill", "z4c_init_finalize",
     "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
     "z4c_get_tile", "z4c_autotune", "z4c_check_finite", "z4c_kernel_launches", "z4c_rhs_stage",
-    "z4c_fp64_probe", "z4c_tracker_add", "z4c_tracker_get", "z4c_vc_restrict", "z4c_vc_prolongate", "z4c_rhs_noalloc",
+    "z4c_fp64_probe", "z4c_tracker_add", "z4c_tracker_get", "z4c_vc_restrict", "z4c_vc_prolongate",
+    "z4c_regrid_refine", "z4c_regrid_derefine", "z4c_rhs_noalloc",
     "z4c_sphere_grid", "z4c_wave_add", "z4c_wave_points", "z4c_wave_decompose",
     "z4c_restart_info", "z4c_restart_text", "z4c_restart_read", "z4c_restart_write_host",
     "z4c_restart_load", "z4c_restart_save")
@@ -144,6 +145,8 @@ def lib():
         L.z4c_tracker_get.argtypes = [vp, ip, dp]
         L.z4c_vc_restrict.argtypes = [vp, vp, ip, ip, ipp, ipp, vp]
         L.z4c_vc_prolongate.argtypes = [vp, vp, ip, ip, ipp, ipp, vp]
+        L.z4c_regrid_refine.argtypes = [vp, vp, vp, ip, ipp, ipp, vp]
+        L.z4c_regrid_derefine.argtypes = [vp, vp, vp, ip, ipp, ipp, vp]
         L.z4c_rhs_noalloc.argtypes = [vp, vp, ip, C.POINTER(C.c_int), dp,
                                       C.POINTER(Params), vp]
         L.z4c_sphere_grid.argtypes = [ip, C.c_double, ip, dp]

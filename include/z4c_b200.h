@@ -365,6 +365,19 @@ int z4c_vc_restrict(const double *fine, double *coarse, int nblocks, int nvar,
  * elsewhere (InterpolateLagrangeUniform<3>, utils/interp_univariate.hpp:43). */
 int z4c_vc_prolongate(const double *coarse, double *fine, int nblocks, int nvar,
                       const int nx[3], const int box[6], void *stream);
+/* Regrid-time state transfer between one parent MeshBlock and its child in
+ * octant oct[3] (0 or 1 per axis), one block each in the fine layout above;
+ * coarse is a caller-owned device scratch of one coarse block (nvar cn^3).
+ * AMRRegistry::FillSameRankCoarseToFine (comm/amr_registry.cpp:1015-1233,
+ * vertex-centred): the child's interior vertices prolongated from the
+ * parent's vertices around the octant; ghosts are left to the next ghost
+ * exchange, as in the reference. */
+int z4c_regrid_refine(const double *parent, double *child, double *coarse, int nvar,
+                      const int nx[3], const int oct[3], void *stream);
+/* AMRRegistry::FillSameRankFineToCoarse (:814-1012, vertex-centred): the
+ * child's interior vertices restricted (injection) into the parent's octant. */
+int z4c_regrid_derefine(const double *child, double *parent, double *coarse, int nvar,
+                        const int nx[3], const int oct[3], void *stream);
 
 /* ---- allocation-free variant ----------------------------------------------
  *

@@ -21,7 +21,9 @@
 //                      one ghost exchange + physical boundary conditions
 //   rf_*               with <driver> refine_ops_only = true, only the
 //                      vertex-centred refinement operators of one block of a
-//                      multilevel mesh (see RefinementOperators)
+//                      multilevel mesh (see RefinementOperators) and the
+//                      regrid-time transfer between two of its blocks
+//                      (rg_*, see RegridTransfer)
 //   s<n>_rhs, s<n>_int, s<n>_exch, s<n>_alg
 //                      one full time step, stage by stage, following the
 //                      GR_Z4c task order (task_list/gr/task_list_gr_z4c.cpp:
@@ -35,6 +37,7 @@
 #include <vector>
 
 #include "main.hpp"
+#include "comm/amr_registry.hpp"
 #include "comm/comm_registry.hpp"
 #include "mesh/mesh_refinement.hpp"
 #include "task_list/time_integrators.hpp"
@@ -237,6 +240,62 @@ void RefinementOperators(MeshBlock* b, Writer& w) {
   }
 }
 
+// Regrid-time state transfer of the Main AMR group (Z4c storage.u) between two
+// blocks C and F of a multilevel mesh, used as parent and child: AMRRegistry::FillSameRankCoarseToFine (F's interior from
+// C's vertices around the child octant) and FillSameRankFineToCoarse (C's
+// octant from F's interior).  Only the parity of the location passed decides
+// the octant, so every octant can be exercised on one pair of blocks.
+//   rg_parent, rg_child      the synthetic states before the transfer
+//   rg_c2f<q>, rg_f2c<q>     F after refinement / C after derefinement into
+//                            octant rg_oct<q>
+void RegridTransfer(const std::vector<MeshBlock*>& blocks, Writer& w) {
+  // the transfer reads only the blocks' index geometry (equal for all blocks
+  // of the mesh) and their refinement objects, so any two blocks serve
+  if (blocks.size() < 2) return;
+  MeshBlock* C = blocks.front();
+  MeshBlock* F = blocks.back();
+  const int NZ = Z4c::N_Z4c;
+  AthenaArray<Real>& uc = C->pz4c->storage.u;
+  AthenaArray<Real>& uf = F->pz4c->storage.u;
+  const int nn1 = C->nverts1, nn2 = C->nverts2, nn3 = C->nverts3;
+  for (int n = 0; n < NZ; ++n)
+    for (int k = 0; k < nn3; ++k)
+      for (int j = 0; j < nn2; ++j)
+        for (int i = 0; i < nn1; ++i) {
+          uc(n, k, j, i) = std::sin(0.31 * n + 0.23 * i + 0.17 * j + 0.11 * k) + 2e-3 * (i + 2 * j + 3 * k);
+          uf(n, k, j, i) = std::cos(0.41 * n + 0.19 * i + 0.29 * j + 0.07 * k) - 1e-3 * (i * k + j);
+        }
+  auto dump = [&](const std::string& name, AthenaArray<Real>& a) {
+    std::vector<double> buf;
+    for (int n = 0; n < NZ; ++n)
+      for (int k = 0; k < nn3; ++k)
+        for (int j = 0; j < nn2; ++j)
+          for (int i = 0; i < nn1; ++i) buf.push_back(a(n, k, j, i));
+    w.f64(name, {NZ, nn3, nn2, nn1}, buf.data());
+  };
+  dump("rg_parent", uc);
+  dump("rg_child", uf);
+  AthenaArray<Real> keep_c, keep_f;
+  Copy(keep_c, uc);
+  Copy(keep_f, uf);
+  const int octs[3][3] = {{0, 0, 0}, {1, 0, 1}, {1, 1, 1}};
+  for (int q = 0; q < 3; ++q) {
+    LogicalLocation loc = C->loc;
+    loc.level += 1;
+    loc.lx1 = 2 * C->loc.lx1 + octs[q][0];
+    loc.lx2 = 2 * C->loc.lx2 + octs[q][1];
+    loc.lx3 = 2 * C->loc.lx3 + octs[q][2];
+    std::vector<std::int32_t> o(octs[q], octs[q] + 3);
+    w.i32("rg_oct" + std::to_string(q), {3}, o.data());
+    C->pamr->FillSameRankCoarseToFine(C, F, loc, comm::AMRGroup::Main, C->pamr, F->pamr);
+    dump("rg_c2f" + std::to_string(q), uf);
+    Copy(uf, keep_f);
+    F->pamr->FillSameRankFineToCoarse(F, C, loc, comm::AMRGroup::Main, C->pamr);
+    dump("rg_f2c" + std::to_string(q), uc);
+    Copy(uc, keep_c);
+  }
+}
+
 }  // namespace
 
 int main(int argc, char* argv[]) {
@@ -265,6 +324,7 @@ int main(int argc, char* argv[]) {
 
   if (pin->GetOrAddBoolean("driver", "refine_ops_only", false)) {
     RefinementOperators(blocks[0], d.w);
+    RegridTransfer(blocks, d.w);
     std::cout << "z4c_ops_ref: wrote " << out << std::endl;
     return 0;
   }

@@ -1524,6 +1524,61 @@ void orc_weyl(const orc_block_t *b, const z4c_params_t *opt, const double *adm, 
 #undef GT
 }
 
+/* ---- regrid-time transfer, comm/amr_registry.cpp:814-1233 (VC) ----------- */
+void orc_regrid_refine(const int nx[3], int nvar, const double *parent, double *child,
+                       const int oct[3]) {
+  const int NCG = Z4C_NCG, ndg = NCG < NG ? NCG : NG;
+  int nn[3], cn[3], box[6];
+  for (int a = 0; a < 3; ++a) {
+    nn[a] = nx[a] + 1 + 2 * NG;
+    cn[a] = nx[a] / 2 + 1 + 2 * NCG;
+    box[2 * a] = NCG;                 /* civs */
+    box[2 * a + 1] = NCG + nx[a] / 2; /* cive */
+  }
+  const int64_t fvol = (int64_t)nn[0] * nn[1] * nn[2], cvol = (int64_t)cn[0] * cn[1] * cn[2];
+  double *coarse = (double *)calloc((size_t)(nvar * cvol), sizeof(double));
+  /* coarse [civs - ndg, cive + ndg] <- parent from oct*nx/2 + ivs - ndg */
+  int c0[3], s0[3];
+  for (int a = 0; a < 3; ++a) {
+    c0[a] = NCG - ndg;
+    s0[a] = oct[a] * (nx[a] / 2) + NG - ndg;
+  }
+  for (int n = 0; n < nvar; ++n)
+    for (int k = c0[2]; k <= NCG + nx[2] / 2 + ndg; ++k)
+      for (int j = c0[1]; j <= NCG + nx[1] / 2 + ndg; ++j)
+        for (int i = c0[0]; i <= NCG + nx[0] / 2 + ndg; ++i)
+          coarse[n * cvol + ((int64_t)k * cn[1] + j) * cn[0] + i] =
+              parent[n * fvol + ((int64_t)(s0[2] + k - c0[2]) * nn[1] + (s0[1] + j - c0[1])) * nn[0] +
+                     (s0[0] + i - c0[0])];
+  orc_vc_prolongate(nx, nvar, coarse, child, box);
+  free(coarse);
+}
+
+void orc_regrid_derefine(const int nx[3], int nvar, const double *child, double *parent,
+                         const int oct[3]) {
+  const int NCG = Z4C_NCG;
+  int nn[3], cn[3], box[6];
+  for (int a = 0; a < 3; ++a) {
+    nn[a] = nx[a] + 1 + 2 * NG;
+    cn[a] = nx[a] / 2 + 1 + 2 * NCG;
+    box[2 * a] = NCG;
+    box[2 * a + 1] = NCG + nx[a] / 2;
+  }
+  const int64_t fvol = (int64_t)nn[0] * nn[1] * nn[2], cvol = (int64_t)cn[0] * cn[1] * cn[2];
+  double *coarse = (double *)calloc((size_t)(nvar * cvol), sizeof(double));
+  orc_vc_restrict(nx, nvar, child, coarse, box);
+  for (int n = 0; n < nvar; ++n)
+    for (int k = box[4]; k <= box[5]; ++k)
+      for (int j = box[2]; j <= box[3]; ++j)
+        for (int i = box[0]; i <= box[1]; ++i)
+          parent[n * fvol +
+                 ((int64_t)(NG + oct[2] * (nx[2] / 2) + k - box[4]) * nn[1] +
+                  (NG + oct[1] * (nx[1] / 2) + j - box[2])) * nn[0] +
+                 (NG + oct[0] * (nx[0] / 2) + i - box[0])] =
+              coarse[n * cvol + ((int64_t)k * cn[1] + j) * cn[0] + i];
+  free(coarse);
+}
+
 /* ---- puncture tracker, z4c/puncture_tracker.cpp:95-129 ------------------ */
 
 /* LagrangeInterp1D<7> (utils/lagrange_interp.hpp:33-146), odd order: first

@@ -122,6 +122,19 @@ void orc_sylm(int s, int l, int m, double theta, double phi, double *re, double 
 int orc_wave_block(const orc_block_t *b, const double *weyl, int np, const double *geo,
                    double rad, int lmax, int bitant, int *owned, double *psi);
 
+/* Regrid-time state transfer between a parent block and one child octant
+ * oct[3] (0/1 per axis), one MeshBlock each ([nvar][nn3][nn2][nn1]):
+ * AMRRegistry::FillSameRankCoarseToFine, comm/amr_registry.cpp:1015-1233
+ * (VC branch: the parent's vertices around the octant, with NCG coarse
+ * ghosts, into a coarse buffer, then ProlongateVertexCenteredValues over the
+ * child's interior vertices), and FillSameRankFineToCoarse, :814-1012
+ * (RestrictVertexCenteredValues of the child's interior, copied into the
+ * parent's octant). */
+void orc_regrid_refine(const int nx[3], int nvar, const double *parent, double *child,
+                       const int oct[3]);
+void orc_regrid_derefine(const int nx[3], int nvar, const double *child, double *parent,
+                         const int oct[3]);
+
 /* ---- puncture tracker (z4c/puncture_tracker.cpp) ------------------------ */
 
 /* PunctureTracker::InterpolateShift (:95-129): the shift of block b at pos

@@ -82,6 +82,8 @@ def lib():
         ip6 = C.POINTER(C.c_int)
         L.orc_vc_restrict.argtypes = [ip6, C.c_int, dp, dp, ip6]
         L.orc_vc_prolongate.argtypes = [ip6, C.c_int, dp, dp, ip6]
+        L.orc_regrid_refine.argtypes = [ip6, C.c_int, dp, dp, ip6]
+        L.orc_regrid_derefine.argtypes = [ip6, C.c_int, dp, dp, ip6]
         L.orc_algconstr_ghosts.argtypes = [bp, pp, dp]
         L.orc_z4c_to_adm.argtypes = [bp, pp, dp, dp]
         L.orc_z4c_to_adm_ghosts.argtypes = [bp, pp, dp, dp]
@@ -207,6 +209,24 @@ def weyl(blk, p, adm, u):
     out = np.zeros(blk.shape(2))
     d = _DerivsHolder(blk, u)
     lib().orc_weyl(C.byref(blk._s), C.byref(p), _ptr(adm), _ptr(u), C.byref(d.d), _ptr(out))
+    return out
+
+
+def regrid_refine(nx, parent, child, oct):
+    """FillSameRankCoarseToFine: child's interior from the parent's octant."""
+    parent = np.ascontiguousarray(parent, dtype=np.float64)
+    out = np.array(child, dtype=np.float64, copy=True, order="C")
+    lib().orc_regrid_refine((C.c_int * 3)(*nx), out.shape[0], _ptr(parent), _ptr(out),
+                            (C.c_int * 3)(*[int(v) for v in oct]))
+    return out
+
+
+def regrid_derefine(nx, child, parent, oct):
+    """FillSameRankFineToCoarse: the parent's octant from the child."""
+    child = np.ascontiguousarray(child, dtype=np.float64)
+    out = np.array(parent, dtype=np.float64, copy=True, order="C")
+    lib().orc_regrid_derefine((C.c_int * 3)(*nx), out.shape[0], _ptr(child), _ptr(out),
+                              (C.c_int * 3)(*[int(v) for v in oct]))
     return out
 
 

@@ -20,7 +20,9 @@ Fixtures (numpy .npz, compressed):
                     without its MeshBlock data (that is evol_track4's final
                     state)
   refine_vc.npz     the vertex-centred restriction and prolongation operators
-                    of one MeshBlock of a statically refined mesh
+                    of one MeshBlock of a statically refined mesh, and the
+                    regrid-time state transfer (coarse to fine, fine to
+                    coarse) between two of its blocks
 Each fixture stores the input-deck parameters it was made with ("params",
 "mesh", "integrator" as JSON strings).
 """
@@ -238,7 +240,8 @@ def make_refine(outdir):
         rec = read_records(rec_path)
     # the operators act on every variable alike: keep three of them
     keep = [0, 7, 21]
-    out = {k: (v if v.ndim == 1 else v[keep]) for k, v in rec.items() if k.startswith("rf_")}
+    out = {k: (v if v.ndim == 1 else v[keep]) for k, v in rec.items()
+           if k.startswith("rf_") or k.startswith("rg_")}
     out["nx"] = np.array([8, 8, 8])
     path = os.path.join(outdir, "refine_vc.npz")
     np.savez_compressed(path, **out)

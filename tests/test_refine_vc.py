@@ -68,3 +68,65 @@ def test_restrict_and_prolongate_match_reference():
         assert bitwise(got[0], z[f"rf_prolong{q}"]), q
         ref1 = O.vc_prolongate(nx, coarse2[1].copy(), fine2[1].copy(), box)
         assert bitwise(got[1], ref1), q
+
+
+def test_regrid_oracle_matches_reference():
+    """The oracle's regrid transfer (both directions, three octants) bit for
+    bit against AMRRegistry::FillSameRank{CoarseToFine,FineToCoarse}."""
+    z = _fixture()
+    nx = [int(v) for v in z["nx"]]
+    for q in range(3):
+        oct_ = z[f"rg_oct{q}"]
+        assert bitwise(O.regrid_refine(nx, z["rg_parent"], z["rg_child"], oct_), z[f"rg_c2f{q}"])
+        assert bitwise(O.regrid_derefine(nx, z["rg_child"], z["rg_parent"], oct_),
+                       z[f"rg_f2c{q}"])
+
+
+def test_regrid_rejects_bad_octants():
+    L = Z.lib()
+    nx = (8, 8, 8)
+    args = (C.c_void_p(0x100), C.c_void_p(0x200), C.c_void_p(0x300), 3, (C.c_int * 3)(*nx))
+    assert L.z4c_regrid_refine(*args, (C.c_int * 3)(0, 2, 0), None) == -1
+    assert L.z4c_regrid_derefine(*args, (C.c_int * 3)(0, 0, -1), None) == -1
+
+
+@pytest.mark.gpu
+def test_regrid_transfer_matches_reference():
+    """Refinement of a parent into each recorded octant and derefinement of a
+    child into it, on the device, against the reference; then all eight
+    octants against the oracle."""
+    import torch
+    z = _fixture()
+    nx = [int(v) for v in z["nx"]]
+    dev = torch.device("cuda:0")
+    L = Z.lib()
+    s = torch.cuda.current_stream().cuda_stream
+    parent, child = z["rg_parent"], z["rg_child"]
+    nvar = parent.shape[0]
+    cn = [n // 2 + 1 + 2 * Z4C_NCG for n in nx]
+    scratch = torch.zeros((nvar, cn[2], cn[1], cn[0]), dtype=torch.float64, device=dev)
+    p_d = torch.from_numpy(parent).to(dev)
+    c_d = torch.from_numpy(child).to(dev)
+
+    def run(fn, src, dst, oct_):
+        out = dst.clone()
+        rc = fn(C.c_void_p(src.data_ptr()), C.c_void_p(out.data_ptr()),
+                C.c_void_p(scratch.data_ptr()), nvar, (C.c_int * 3)(*nx),
+                (C.c_int * 3)(*[int(v) for v in oct_]), C.c_void_p(s))
+        assert rc == 0, L.z4c_last_error()
+        torch.cuda.synchronize()
+        return out.cpu().numpy()
+
+    for q in range(3):
+        oct_ = z[f"rg_oct{q}"]
+        assert bitwise(run(L.z4c_regrid_refine, p_d, c_d, oct_), z[f"rg_c2f{q}"])
+        assert bitwise(run(L.z4c_regrid_derefine, c_d, p_d, oct_), z[f"rg_f2c{q}"])
+    for o in range(8):
+        oct_ = (o & 1, o >> 1 & 1, o >> 2 & 1)
+        assert bitwise(run(L.z4c_regrid_refine, p_d, c_d, oct_),
+                       O.regrid_refine(nx, parent, child, oct_))
+        assert bitwise(run(L.z4c_regrid_derefine, c_d, p_d, oct_),
+                       O.regrid_derefine(nx, child, parent, oct_))
+
+
+Z4C_NCG = 4  # coarse ghost vertices, include/z4c_b200.h
