@@ -48,6 +48,37 @@ struct Grid {
   int has_sommerfeld;  // some face is Z4C_BC_SOMMERFELD
 };
 
+// Block geometry fixed at compile time.  Kernels instantiated with NX > 0 run
+// on NX^3 MeshBlocks and see constant vertex counts and strides, so every
+// stencil offset folds into the load instruction; NX = 0 reads the geometry
+// from the Grid.  kFixedNX is the MeshBlock size that gets the fixed
+// instances (0 disables them).
+#ifndef Z4C_FIXED_NX
+#define Z4C_FIXED_NX 16
+#endif
+constexpr int kFixedNX = Z4C_FIXED_NX;
+template <int NX>
+__host__ __device__ __forceinline__ Grid fixed_geometry(const Grid& g) {
+  if constexpr (NX == 0) {
+    return g;
+  } else {
+    constexpr int nn = NX + 1 + 2 * NG;
+    Grid r = g;
+    for (int a = 0; a < 3; ++a) {
+      r.nx[a] = NX;
+      r.nn[a] = nn;
+    }
+    r.s[0] = 1;
+    r.s[1] = nn;
+    r.s[2] = (int64_t)nn * nn;
+    r.nvol = (int64_t)nn * nn * nn;
+    return r;
+  }
+}
+__host__ __forceinline__ bool has_fixed_geometry(const Grid& g) {
+  return kFixedNX > 0 && g.nx[0] == kFixedNX && g.nx[1] == kFixedNX && g.nx[2] == kFixedNX;
+}
+
 // ---- stencils -----------------------------------------------------------
 
 #ifdef FD_BARRIER

@@ -52,8 +52,10 @@ __device__ __forceinline__ double fd_dx7(double m3, double m2, double m1, double
   return out * cidx1;
 }
 
+template <int NX>
 __global__ void __launch_bounds__(kPointThreads)
-k_prep(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ sd, int block0) {
+k_prep(Grid gin, DevParams P, const double* __restrict__ u, double* __restrict__ sd, int block0) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int comp = blockIdx.y;
   const int slot = comp / 3, dir = comp % 3;
   const int b = block0 + (int)blockIdx.z;
@@ -88,10 +90,11 @@ k_prep(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ s
 }
 
 // ---- first pass: Ricci tensor + conformal-factor part per interior vertex --
-template <int THREADS>
+template <int THREADS, int NX>
 __global__ void __launch_bounds__(THREADS, 1)
-k_ricci(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
+k_ricci(Grid gin, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
         double* __restrict__ rsum, int block0, int nblk) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int64_t npts = interior_count(g);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts * nblk) return;
@@ -305,10 +308,11 @@ __device__ __forceinline__ void window_shift(double w[9]) {
 }
 
 // Advection sums (calculate_z4c_rhs.cpp:184-226): lv [block][22][interior vertex]
-template <int UNROLL>
+template <int UNROLL, int NX>
 __global__ void __launch_bounds__(kColumnMaxThreads)
-k_adv(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ lv, int block0,
+k_adv(Grid gin, DevParams P, const double* __restrict__ u, double* __restrict__ lv, int block0,
       int nblk) {
+  const Grid g = fixed_geometry<NX>(gin);
   Column c;
   if (!column_index(g, block0, nblk, c)) return;
   const int nn0 = g.nn[0], sk = nn0 * g.nn[1];
@@ -348,10 +352,11 @@ __device__ __forceinline__ double add_ko_column(double r, const double* __restri
 }
 
 // Z4cRHS tail: rhs += KO, in place.
-template <int UNROLL>
+template <int UNROLL, int NX>
 __global__ void __launch_bounds__(kColumnMaxThreads)
-k_ko_rhs(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__ rhs,
+k_ko_rhs(Grid gin, DevParams P, const double* __restrict__ u, double* __restrict__ rhs,
          int block0, int nblk) {
+  const Grid g = fixed_geometry<NX>(gin);
   Column c;
   if (!column_index(g, block0, nblk, c)) return;
   const int nn0 = g.nn[0], sk = nn0 * g.nn[1];
@@ -376,11 +381,12 @@ k_ko_rhs(Grid g, DevParams P, const double* __restrict__ u, double* __restrict__
 //   WeightedAve(u1, u, u2, {1, delta, 0}); WeightedAve(u, u1, u2, {g1, g2, g3});
 //   AddZ4cRHS(rhs, beta*dt, u)        (mesh/weighted_ave.cpp:20-150)
 // u is read (all points, for the stencils); u_out, u1 are written (interior).
-template <int UNROLL, bool SOM>
+template <int UNROLL, bool SOM, int NX>
 __global__ void __launch_bounds__(kColumnMaxThreads)
-k_ko_stage_ls(Grid g, DevParams P, const double* __restrict__ u,
+k_ko_stage_ls(Grid gin, DevParams P, const double* __restrict__ u,
               const double* __restrict__ rhs, double* __restrict__ u1,
               double* __restrict__ u_out, LsStage w, int block0, int nblk) {
+  const Grid g = fixed_geometry<NX>(gin);
   Column c;
   if (!column_index(g, block0, nblk, c)) return;
   const int nn0 = g.nn[0], sk = nn0 * g.nn[1];
@@ -425,11 +431,12 @@ k_ko_stage_ls(Grid g, DevParams P, const double* __restrict__ u,
 struct KPtrs {
   double* k[4];
 };
-template <int UNROLL, bool SOM>
+template <int UNROLL, bool SOM, int NX>
 __global__ void __launch_bounds__(kColumnMaxThreads)
-k_ko_stage_bt(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ rhs,
+k_ko_stage_bt(Grid gin, DevParams P, const double* __restrict__ u, const double* __restrict__ rhs,
               const double* __restrict__ un, KPtrs K, double* __restrict__ u_out, BtStage w,
               int block0, int nblk) {
+  const Grid g = fixed_geometry<NX>(gin);
   Column c;
   if (!column_index(g, block0, nblk, c)) return;
   const int nn0 = g.nn[0], sk = nn0 * g.nn[1];
@@ -663,11 +670,12 @@ k_ko_rhs_slab(Grid g, DevParams P, const double* __restrict__ u, double* __restr
 }
 
 // ---- main pass: the right-hand side without the Kreiss-Oliger terms -------
-template <int THREADS>
+template <int THREADS, int NX>
 __global__ void __launch_bounds__(THREADS, 1)
-k_main(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
+k_main(Grid gin, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
        const double* __restrict__ rsum, const double* __restrict__ lv, double* __restrict__ rhs,
        int block0, int nblk) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int64_t npts = interior_count(g);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts * nblk) return;
@@ -1313,9 +1321,11 @@ static void launch_point_passes_t(const Grid& g, const DevParams& P, const doubl
   const int64_t n = interior_count(g) * nblk;
   COUNTED
   if (which == 0)
-    k_ricci<T><<<div_up(n, T), T, 0, st>>>(g, P, u, sc.sd, sc.rsum, block0, nblk);
+    (has_fixed_geometry(g) ? k_ricci<T, kFixedNX> : k_ricci<T, 0>)<<<div_up(n, T), T, 0, st>>>(
+        g, P, u, sc.sd, sc.rsum, block0, nblk);
   else
-    k_main<T><<<div_up(n, T), T, 0, st>>>(g, P, u, sc.sd, sc.rsum, sc.lv, rhs, block0, nblk);
+    (has_fixed_geometry(g) ? k_main<T, kFixedNX> : k_main<T, 0>)<<<div_up(n, T), T, 0, st>>>(
+        g, P, u, sc.sd, sc.rsum, sc.lv, rhs, block0, nblk);
 }
 static void launch_point_pass(const Grid& g, const DevParams& P, const double* u,
                               const RhsScratch& sc, double* rhs, int block0, int nblk, int which,
@@ -1345,11 +1355,15 @@ static void launch_rhs_passes(const Grid& g, const DevParams& P, const double* u
   } else {
     const int64_t cprep = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7);  // widest component region
     COUNTED
-    k_prep<<<dim3(div_up(cprep, kPointThreads), kSdComponents, nblk), kPointThreads, 0, st>>>(
+    (has_fixed_geometry(g) ? k_prep<kFixedNX> : k_prep<0>)<<<dim3(div_up(cprep, kPointThreads),
+                                                                 kSdComponents, nblk),
+                                                            kPointThreads, 0, st>>>(
         g, P, u, sc.sd, block0);
     launch_point_pass(g, P, u, sc, rhs, block0, nblk, 0, sh, st);
     COUNTED
-    k_adv<4><<<div_up(columns(g, nblk), ct), ct, 0, st>>>(g, P, u, sc.lv, block0, nblk);
+    (has_fixed_geometry(g) ? k_adv<4, kFixedNX> : k_adv<4, 0>)<<<div_up(columns(g, nblk), ct), ct,
+                                                                   0, st>>>(g, P, u, sc.lv, block0,
+                                                                            nblk);
   }
   launch_point_pass(g, P, u, sc, rhs, block0, nblk, 1, sh, st);
 }
@@ -1365,7 +1379,9 @@ void launch_rhs(const Grid& g, const DevParams& P, const double* u, const RhsScr
     k_ko_rhs_slab<<<dim3((g.nx[2] + S.kper) / S.kper, NVAR, nblk), ct, smem, st>>>(g, P, u, rhs,
                                                                                  S, block0);
   } else {
-    k_ko_rhs<4><<<div_up(columns(g, nblk), ct), ct, 0, st>>>(g, P, u, rhs, block0, nblk);
+    (has_fixed_geometry(g) ? k_ko_rhs<4, kFixedNX> : k_ko_rhs<4, 0>)<<<div_up(columns(g, nblk), ct),
+                                                                        ct, 0, st>>>(g, P, u, rhs,
+                                                                                     block0, nblk);
   }
 }
 
@@ -1382,7 +1398,10 @@ void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, const R
     kern<<<dim3((g.nx[2] + S.kper) / S.kper, NVAR, nblk), ct, smem, st>>>(g, P, u, rhs, u1, u_out,
                                                                         w, S, block0);
   } else {
-    auto kern = g.has_sommerfeld ? k_ko_stage_ls<4, true> : k_ko_stage_ls<4, false>;
+    auto kern = has_fixed_geometry(g)
+                    ? (g.has_sommerfeld ? k_ko_stage_ls<4, true, kFixedNX>
+                                        : k_ko_stage_ls<4, false, kFixedNX>)
+                    : (g.has_sommerfeld ? k_ko_stage_ls<4, true, 0> : k_ko_stage_ls<4, false, 0>);
     kern<<<div_up(columns(g, nblk), ct), ct, 0, st>>>(g, P, u, rhs, u1, u_out, w, block0, nblk);
   }
 }
@@ -1403,7 +1422,10 @@ void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const R
     kern<<<dim3((g.nx[2] + S.kper) / S.kper, NVAR, nblk), ct, smem, st>>>(g, P, u, rhs, un, K,
                                                                         u_out, w, S, block0);
   } else {
-    auto kern = g.has_sommerfeld ? k_ko_stage_bt<4, true> : k_ko_stage_bt<4, false>;
+    auto kern = has_fixed_geometry(g)
+                    ? (g.has_sommerfeld ? k_ko_stage_bt<4, true, kFixedNX>
+                                        : k_ko_stage_bt<4, false, kFixedNX>)
+                    : (g.has_sommerfeld ? k_ko_stage_bt<4, true, 0> : k_ko_stage_bt<4, false, 0>);
     kern<<<div_up(columns(g, nblk), ct), ct, 0, st>>>(g, P, u, rhs, un, K, u_out, w, block0,
                                                       nblk);
   }
@@ -1536,7 +1558,9 @@ void launch_weyl(const Grid& g, const DevParams& P, const double* adm, const dou
                  cudaStream_t st) {
   const int64_t cprep = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7);  // widest component region
   COUNTED
-  k_prep<<<dim3(div_up(cprep, kPointThreads), kSdComponents, nblk), kPointThreads, 0, st>>>(
+  (has_fixed_geometry(g) ? k_prep<kFixedNX> : k_prep<0>)<<<dim3(div_up(cprep, kPointThreads),
+                                                               kSdComponents, nblk),
+                                                          kPointThreads, 0, st>>>(
       g, P, u, sd, block0);
   const int64_t n = g.nvol * nblk;
   COUNTED
