@@ -815,10 +815,11 @@ __constant__ int c_dir_index[27];  // (o0+1) + 3(o1+1) + 9(o2+1) -> neighbour sl
 // supports in list order: 0, 1, 2, 4, 3, 5, 6, 7
 __device__ __forceinline__ constexpr int u_order(int q) { return (q == 3) ? 4 : (q == 4) ? 3 : q; }
 
-template <int NV>
+template <int NV, int NX>
 __global__ void __launch_bounds__(kPointThreads)
-k_exchange_interior(Grid g, DevParams P, const double* __restrict__ src,
+k_exchange_interior(Grid gin, DevParams P, const double* __restrict__ src,
                     double* __restrict__ dst, const int* __restrict__ nbr, int fuse_alg) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int n0 = g.nx[0] + 1, n1 = g.nx[1] + 1, n2 = g.nx[2] + 1;
   const int per = n0 * n1 * n2;
   const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
@@ -891,9 +892,10 @@ k_exchange_interior(Grid g, DevParams P, const double* __restrict__ src,
 
 // Ghost vertices: copy of the primary owner's result (zero where the primary
 // owner lies beyond a physical face; the boundary conditions overwrite those).
-template <int NV>
+template <int NV, int NX>
 __global__ void __launch_bounds__(kPointThreads)
-k_exchange_ghosts(Grid g, double* __restrict__ u, const int* __restrict__ nbr) {
+k_exchange_ghosts(Grid gin, double* __restrict__ u, const int* __restrict__ nbr) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int per = (int)g.nvol;
   const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (t >= per * g.nblocks) return;
@@ -933,8 +935,10 @@ k_exchange_ghosts(Grid g, double* __restrict__ u, const int* __restrict__ nbr) {
 // Only the blocks on the two faces of axis ax are visited.  One thread per
 // (face block, variable, side, transverse pair) cascades outward; the
 // fastest thread index runs along the transverse axis of smallest stride.
+template <int NX>
 __global__ void __launch_bounds__(kPointThreads)
-k_bc_axis(Grid g, double* __restrict__ u, int nvar, int ax) {
+k_bc_axis(Grid gin, double* __restrict__ u, int nvar, int ax) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int o1 = (ax == 0) ? 1 : 0;       // fastest transverse axis
   const int o2 = (ax == 2) ? 1 : 2;       // slowest transverse axis
   const int64_t nt = (int64_t)g.nn[o1] * g.nn[o2];
@@ -1000,9 +1004,11 @@ __device__ __forceinline__ bool is_interior_vertex(const Grid& g, int64_t p) {
          k <= NG + g.nx[2];
 }
 
+template <int NX>
 __global__ void __launch_bounds__(kPointThreads)
-k_alg_constr(Grid g, DevParams P, double* __restrict__ u, int block0, int nblk,
+k_alg_constr(Grid gin, DevParams P, double* __restrict__ u, int block0, int nblk,
              int ghosts_only) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.nvol * nblk) return;
   const int b = block0 + (int)(t / g.nvol);
@@ -1472,17 +1478,22 @@ void launch_exchange(const Grid& g, const DevParams& P, const double* src, doubl
   (void)dir_rc;
   const int64_t ni = div_up(interior_count(g) * g.nblocks, kPointThreads);
   const int64_t ng = div_up(g.nvol * g.nblocks, kPointThreads);
+  const bool fx = has_fixed_geometry(g);
   COUNTED
   if (nvar == Z4C_NWEYL) {
-    k_exchange_interior<Z4C_NWEYL><<<ni, kPointThreads, 0, st>>>(g, P, src, dst, nbr, 0);
+    (fx ? k_exchange_interior<Z4C_NWEYL, kFixedNX> : k_exchange_interior<Z4C_NWEYL, 0>)<<<
+        ni, kPointThreads, 0, st>>>(g, P, src, dst, nbr, 0);
   } else {
-    k_exchange_interior<NVAR><<<ni, kPointThreads, 0, st>>>(g, P, src, dst, nbr, fuse_alg);
+    (fx ? k_exchange_interior<NVAR, kFixedNX> : k_exchange_interior<NVAR, 0>)<<<
+        ni, kPointThreads, 0, st>>>(g, P, src, dst, nbr, fuse_alg);
   }
   COUNTED
   if (nvar == Z4C_NWEYL) {
-    k_exchange_ghosts<Z4C_NWEYL><<<ng, kPointThreads, 0, st>>>(g, dst, nbr);
+    (fx ? k_exchange_ghosts<Z4C_NWEYL, kFixedNX> : k_exchange_ghosts<Z4C_NWEYL, 0>)<<<
+        ng, kPointThreads, 0, st>>>(g, dst, nbr);
   } else {
-    k_exchange_ghosts<NVAR><<<ng, kPointThreads, 0, st>>>(g, dst, nbr);
+    (fx ? k_exchange_ghosts<NVAR, kFixedNX> : k_exchange_ghosts<NVAR, 0>)<<<
+        ng, kPointThreads, 0, st>>>(g, dst, nbr);
   }
 }
 
@@ -1495,7 +1506,8 @@ void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st) {
     const int o1 = (ax == 0) ? 1 : 0, o2 = (ax == 2) ? 1 : 2;
     const int64_t n = (int64_t)g.nn[o1] * g.nn[o2] * 2 * nvar * g.nb[o1] * g.nb[o2];
     COUNTED
-    k_bc_axis<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, u, nvar, ax);
+    (has_fixed_geometry(g) ? k_bc_axis<kFixedNX> : k_bc_axis<0>)<<<
+        div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, u, nvar, ax);
   }
 }
 
@@ -1503,8 +1515,8 @@ void launch_alg_constr(const Grid& g, const DevParams& P, double* u, int block0,
                        cudaStream_t st, int ghosts_only) {
   const int64_t n = g.nvol * nblk;
   COUNTED
-  k_alg_constr<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, block0, nblk,
-                                                                    ghosts_only);
+  (has_fixed_geometry(g) ? k_alg_constr<kFixedNX> : k_alg_constr<0>)<<<
+      div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, block0, nblk, ghosts_only);
 }
 
 void launch_weighted_ave(const Grid& g, double* out, const double* in1, const double* in2,
@@ -1541,7 +1553,8 @@ void launch_adm_to_z4c(const Grid& g, const DevParams& P, const double* adm, dou
   k_adm_to_z4c_gam<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, guu_scratch, u,
                                                                        block0, nblk);
   COUNTED
-  k_alg_constr<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, block0, nblk, 0);
+  (has_fixed_geometry(g) ? k_alg_constr<kFixedNX> : k_alg_constr<0>)<<<
+      div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, block0, nblk, 0);
 }
 
 void launch_adm_constraints(const Grid& g, const DevParams& P, const double* adm,
