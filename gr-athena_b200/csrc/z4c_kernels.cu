@@ -56,6 +56,7 @@ template <int NX>
 __global__ void __launch_bounds__(kPointThreads)
 k_prep(Grid gin, DevParams P, const double* __restrict__ u, double* __restrict__ sd, int block0) {
   const Grid g = fixed_geometry<NX>(gin);
+  constexpr int kUnroll = NX > 0 ? NX + 1 : 4;  // the whole z loop when fixed
   const int comp = blockIdx.y;
   const int slot = comp / 3, dir = comp % 3;
   const int b = block0 + (int)blockIdx.z;
@@ -75,7 +76,7 @@ k_prep(Grid gin, DevParams P, const double* __restrict__ u, double* __restrict__
     double w0 = __ldg(f + (k0 - 3) * sk), w1 = __ldg(f + (k0 - 2) * sk),
            w2 = __ldg(f + (k0 - 1) * sk), w3 = __ldg(f + k0 * sk),
            w4 = __ldg(f + (k0 + 1) * sk), w5 = __ldg(f + (k0 + 2) * sk);
-#pragma unroll 4
+#pragma unroll kUnroll
     for (int k = k0; k <= k1; ++k) {
       const double w6 = __ldg(f + (k + 3) * sk);
       out[k * sk] = fd_dx7(w0, w1, w2, w4, w5, w6, cz);
@@ -84,7 +85,7 @@ k_prep(Grid gin, DevParams P, const double* __restrict__ u, double* __restrict__
   } else {
     const int st = (dir == 0) ? 1 : nn0;
     const double ca = (dir == 0) ? F.cidx1[0] : F.cidx1[1];
-#pragma unroll 4
+#pragma unroll kUnroll
     for (int k = k0; k <= k1; ++k) out[k * sk] = fd_dx(f + k * sk, st, ca);
   }
 }
@@ -1124,10 +1125,12 @@ __global__ void k_adm_to_z4c_gam(Grid g, DevParams P, const double* __restrict__
   }
 }
 
+template <int NX>
 __global__ void __launch_bounds__(128, 1)
-k_adm_constraints(Grid g, DevParams P, const double* __restrict__ adm,
+k_adm_constraints(Grid gin, DevParams P, const double* __restrict__ adm,
                   const double* __restrict__ u, double* __restrict__ con,
                   const double* __restrict__ xf, int block0, int nblk) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.nvol * nblk) return;
   const int b = block0 + (int)(t / g.nvol);
@@ -1152,10 +1155,12 @@ k_adm_constraints(Grid g, DevParams P, const double* __restrict__ adm,
 // ---- Weyl scalar psi4 (z4c/calculate_weyl_scalars.cpp:44-630) --------------
 // One thread per vertex of the requested blocks; interior vertices get psi4,
 // every other vertex NaN (the reference fills the register with NaN first).
+template <int NX>
 __global__ void __launch_bounds__(128, 1)
-k_weyl(Grid g, DevParams P, const double* __restrict__ adm, const double* __restrict__ u,
+k_weyl(Grid gin, DevParams P, const double* __restrict__ adm, const double* __restrict__ u,
        const double* __restrict__ sd, double* __restrict__ weyl, const double* __restrict__ xf,
        int block0, int nblk) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.nvol * nblk) return;
   const int b = block0 + (int)(t / g.nvol);
@@ -1270,6 +1275,11 @@ long long kernel_launch_count() { return g_launches.load(); }
 void add_kernel_launches(long long n) { g_launches += n; }
 #define COUNTED ++g_launches;
 
+// Unroll of the column passes' z loops (loads in flight per thread): the
+// fixed-geometry instances unroll their nx + 1 iterations completely, the
+// generic ones by kColUnroll.
+constexpr int kColUnroll = 4;
+
 // Threads of the column passes (one per block, variable and interior (i, j)).
 static int64_t columns(const Grid& g, int nblk) {
   return (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * NVAR * nblk;
@@ -1367,7 +1377,7 @@ static void launch_rhs_passes(const Grid& g, const DevParams& P, const double* u
         g, P, u, sc.sd, block0);
     launch_point_pass(g, P, u, sc, rhs, block0, nblk, 0, sh, st);
     COUNTED
-    (has_fixed_geometry(g) ? k_adv<4, kFixedNX> : k_adv<4, 0>)<<<div_up(columns(g, nblk), ct), ct,
+    (has_fixed_geometry(g) ? k_adv<kFixedNX + 1, kFixedNX> : k_adv<kColUnroll, 0>)<<<div_up(columns(g, nblk), ct), ct,
                                                                    0, st>>>(g, P, u, sc.lv, block0,
                                                                             nblk);
   }
@@ -1385,7 +1395,7 @@ void launch_rhs(const Grid& g, const DevParams& P, const double* u, const RhsScr
     k_ko_rhs_slab<<<dim3((g.nx[2] + S.kper) / S.kper, NVAR, nblk), ct, smem, st>>>(g, P, u, rhs,
                                                                                  S, block0);
   } else {
-    (has_fixed_geometry(g) ? k_ko_rhs<4, kFixedNX> : k_ko_rhs<4, 0>)<<<div_up(columns(g, nblk), ct),
+    (has_fixed_geometry(g) ? k_ko_rhs<kFixedNX + 1, kFixedNX> : k_ko_rhs<kColUnroll, 0>)<<<div_up(columns(g, nblk), ct),
                                                                         ct, 0, st>>>(g, P, u, rhs,
                                                                                      block0, nblk);
   }
@@ -1405,9 +1415,9 @@ void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, const R
                                                                         w, S, block0);
   } else {
     auto kern = has_fixed_geometry(g)
-                    ? (g.has_sommerfeld ? k_ko_stage_ls<4, true, kFixedNX>
-                                        : k_ko_stage_ls<4, false, kFixedNX>)
-                    : (g.has_sommerfeld ? k_ko_stage_ls<4, true, 0> : k_ko_stage_ls<4, false, 0>);
+                    ? (g.has_sommerfeld ? k_ko_stage_ls<kFixedNX + 1, true, kFixedNX>
+                                        : k_ko_stage_ls<kFixedNX + 1, false, kFixedNX>)
+                    : (g.has_sommerfeld ? k_ko_stage_ls<kColUnroll, true, 0> : k_ko_stage_ls<kColUnroll, false, 0>);
     kern<<<div_up(columns(g, nblk), ct), ct, 0, st>>>(g, P, u, rhs, u1, u_out, w, block0, nblk);
   }
 }
@@ -1429,9 +1439,9 @@ void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const R
                                                                         u_out, w, S, block0);
   } else {
     auto kern = has_fixed_geometry(g)
-                    ? (g.has_sommerfeld ? k_ko_stage_bt<4, true, kFixedNX>
-                                        : k_ko_stage_bt<4, false, kFixedNX>)
-                    : (g.has_sommerfeld ? k_ko_stage_bt<4, true, 0> : k_ko_stage_bt<4, false, 0>);
+                    ? (g.has_sommerfeld ? k_ko_stage_bt<kFixedNX + 1, true, kFixedNX>
+                                        : k_ko_stage_bt<kFixedNX + 1, false, kFixedNX>)
+                    : (g.has_sommerfeld ? k_ko_stage_bt<kColUnroll, true, 0> : k_ko_stage_bt<kColUnroll, false, 0>);
     kern<<<div_up(columns(g, nblk), ct), ct, 0, st>>>(g, P, u, rhs, un, K, u_out, w, block0,
                                                       nblk);
   }
@@ -1562,8 +1572,8 @@ void launch_adm_constraints(const Grid& g, const DevParams& P, const double* adm
                             int nblk, cudaStream_t st) {
   const int64_t n = g.nvol * nblk;
   COUNTED
-  k_adm_constraints<<<div_up(n, 128), 128, 0, st>>>(g, P, adm, u, con, xf,
-                                                                    block0, nblk);
+  (has_fixed_geometry(g) ? k_adm_constraints<kFixedNX> : k_adm_constraints<0>)<<<
+      div_up(n, 128), 128, 0, st>>>(g, P, adm, u, con, xf, block0, nblk);
 }
 
 void launch_weyl(const Grid& g, const DevParams& P, const double* adm, const double* u,
@@ -1577,7 +1587,8 @@ void launch_weyl(const Grid& g, const DevParams& P, const double* adm, const dou
       g, P, u, sd, block0);
   const int64_t n = g.nvol * nblk;
   COUNTED
-  k_weyl<<<div_up(n, 128), 128, 0, st>>>(g, P, adm, u, sd, weyl, xf, block0, nblk);
+  (has_fixed_geometry(g) ? k_weyl<kFixedNX> : k_weyl<0>)<<<div_up(n, 128), 128, 0, st>>>(
+      g, P, adm, u, sd, weyl, xf, block0, nblk);
 }
 
 void launch_hst(const Grid& g, const DevParams& P, const double* con, const double* u,
