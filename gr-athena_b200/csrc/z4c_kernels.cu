@@ -983,14 +983,23 @@ k_bc_axis(Grid gin, double* __restrict__ u, int nvar, int ax) {
   double* ub = u + ((int64_t)b * nvar + n) * g.nvol + (int64_t)t1 * g.s[o1] + (int64_t)t2 * g.s[o2];
   const int64_t st = g.s[ax];
   const double c[5] = {5., -10., 10., -5., 1.};
+  // w[q] = the value q + 1 vertices inward of the ghost being filled; each
+  // new ghost enters the window, so the cascade stays in registers
+  const int dir = side ? -1 : 1;
+  const int ia0 = side ? ie[ax] + 1 : is[ax] - 1;
+  double w[5];
+#pragma unroll
+  for (int q = 0; q < 5; ++q) w[q] = ub[(int64_t)(ia0 + dir * (q + 1)) * st];
+#pragma unroll
   for (int gh = 1; gh <= NG; ++gh) {
     const int ia = side ? ie[ax] + gh : is[ax] - gh;
-    const int dir = side ? -1 : 1;
-    double* pp = ub + (int64_t)ia * st;
     double v = 0.0;
 #pragma unroll
-    for (int q = 0; q < 5; ++q) v += c[q] * pp[dir * (q + 1) * st];
-    *pp = v;
+    for (int q = 0; q < 5; ++q) v += c[q] * w[q];
+    ub[(int64_t)ia * st] = v;
+#pragma unroll
+    for (int q = 4; q > 0; --q) w[q] = w[q - 1];
+    w[0] = v;
   }
 }
 
