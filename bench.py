@@ -72,6 +72,10 @@ def parse():
                     help="MeshBlocks per axis (8 = the 128^3 workload; smaller for profiling)")
     ap.add_argument("--profile-run", action="store_true",
                     help="graph-captured steps and the stage kernel only (for ncu)")
+    ap.add_argument("--shape", default=None,
+                    help="launch shape point_threads,column_threads,column_slabs instead of "
+                         "the autotuner's pick (profiling under ncu, whose serialised launches "
+                         "would mislead the autotuner)")
     return ap.parse_args()
 
 
@@ -307,8 +311,12 @@ def main():
     ctx.sync()
     u_init = ctx.download(Z.REG_U)
     # launch shape of the right-hand-side passes, picked on this mesh
-    with torch.cuda.stream(stream):
-        tile, _ = ctx.autotune(reps=3)
+    if args.shape:
+        tile = tuple(int(v) for v in args.shape.split(","))
+        ctx.set_tile(*tile)
+    else:
+        with torch.cuda.stream(stream):
+            tile, _ = ctx.autotune(reps=3)
     dt = CFL * float(np.min(ctx.dx()))
     zones = mesh.zones()
     npts = mesh.nblocks * 17 ** 3
