@@ -58,7 +58,7 @@ FP64_OPS_PER_POINT_WEYL = 7409
 # psi4 extraction spheres of the diagnostics: (radius, nlev, lmax) inside
 # the [-16,16]^3 domain
 WAVE_SPHERES = ((6.0, 30, 8), (12.0, 30, 8))
-STAGE_TRAFFIC_PER_POINT = 1278.0e6 / (64 * 17 ** 3)
+STAGE_TRAFFIC_PER_POINT = 1350.0e6 / (64 * 17 ** 3)
 
 
 def parse():
