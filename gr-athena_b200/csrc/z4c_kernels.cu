@@ -112,13 +112,6 @@ k_ricci(Grid gin, DevParams P, const double* __restrict__ u, const double* __res
   for (int q = 0; q < 6; ++q) rs[(int64_t)q * npts] = R[q];
 }
 
-__device__ __forceinline__ void load_rsum(const Grid& g, const double* __restrict__ rsum, int b,
-                                          int64_t l, double R[6]) {
-  const int64_t npts = interior_count(g);
-  const double* rs = rsum + (int64_t)b * 6 * npts + l;
-#pragma unroll
-  for (int q = 0; q < 6; ++q) R[q] = __ldg(rs + (int64_t)q * npts);
-}
 
 // ---- per-variable passes: advection sums and Kreiss-Oliger -------------------
 // One thread per (block, variable, interior (i, j)) column, looping over the
@@ -685,14 +678,10 @@ k_main(Grid gin, DevParams P, const double* __restrict__ u, const double* __rest
   int i, j, k;
   interior_ijk(g, l, i, j, k);
   const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
-  double R[6];
-  load_rsum(g, rsum, b, l, R);
-  double L[NVAR];
-#pragma unroll
-  for (int n = 0; n < NVAR; ++n) L[n] = __ldg(lv + ((int64_t)b * NVAR + n) * npts + l);
   double out[NVAR];
   rhs_point(u + (int64_t)b * NVAR * g.nvol, sd + (int64_t)b * kSdComponents * g.nvol, g.nvol, p,
-            g.s, P, P.fd[b], R, L, out);
+            g.s, P, P.fd[b], rsum + (int64_t)b * 6 * npts + l, lv + (int64_t)b * NVAR * npts + l,
+            npts, out);
   double* rb = rhs + (int64_t)b * NVAR * g.nvol + p;
 #pragma unroll
   for (int n = 0; n < NVAR; ++n) rb[(int64_t)n * g.nvol] = out[n];

@@ -232,12 +232,14 @@ GATHER_LOOP
 }
 
 // The 22 right-hand-side values at one interior vertex without the
-// Kreiss-Oliger terms, given Rsum_ab and the advection sums Lv.
+// Kreiss-Oliger terms, given Rsum_ab (rsum[q * stride]) and the advection sums
+// (lv[n * stride]).
 __device__ __forceinline__ void rhs_point(const double* __restrict__ u,
                                           const double* __restrict__ sd, int64_t nvol,
                                           int64_t p, const int64_t s[3],
                                           const DevParams& P, const FdScale& F,
-                                          const double Rsum[6], const double Lv[NVAR],
+                                          const double* __restrict__ rsum,
+                                          const double* __restrict__ lv, int64_t stride,
                                           double out[NVAR]) {
   const z4c_params_t& opt = P.p;
   const double* U = u + p;
@@ -362,24 +364,26 @@ GATHER_LOOP
   for (int a = 0; a < 3; ++a)
 #pragma unroll
     for (int b = a; b < 3; ++b)
-      R += ((a == b) ? 1.0 : 2.0) * oopsi4 * GUU(a, b) * Rsum[sidx(a, b)];
+      R += ((a == b) ? 1.0 : 2.0) * oopsi4 * GUU(a, b) * __ldg(rsum + sidx(a, b) * stride);
   const double Ht = R + (2. / 3.) * (K * K) - trAA;
 
   // advective derivatives, :184-226
   double beta_u[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) beta_u[a] = __ldg(UV(Z4C_BETAX + a));
-  double Lsc[4] = {Lv[Z4C_ALPHA], Lv[Z4C_CHI], Lv[Z4C_KHAT], Lv[Z4C_THETA]};
+  // the advection sums, read where they enter (lv[n * stride])
+  auto Lv = [&](int n) { return __ldg(lv + (int64_t)n * stride); };
+  double Lsc[4] = {Lv(Z4C_ALPHA), Lv(Z4C_CHI), Lv(Z4C_KHAT), Lv(Z4C_THETA)};
   double Lbeta_u[3], LGam_u[3], Lg_dd[6], LA_dd[6];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    Lbeta_u[a] = Lv[Z4C_BETAX + a];
-    LGam_u[a] = Lv[Z4C_GAMX + a];
+    Lbeta_u[a] = Lv(Z4C_BETAX + a);
+    LGam_u[a] = Lv(Z4C_GAMX + a);
   }
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
-    Lg_dd[q] = Lv[Z4C_GXX + q];
-    LA_dd[q] = Lv[Z4C_AXX + q];
+    Lg_dd[q] = Lv(Z4C_GXX + q);
+    LA_dd[q] = Lv(Z4C_AXX + q);
   }
 
   // finalize Lie derivatives, :619-687
@@ -452,7 +456,7 @@ GATHER_LOOP
     for (int b = a; b < 3; ++b) {
       const int q = sidx(a, b);
       out[Z4C_GXX + q] = -2. * alpha * A_dd[q] + Lg_dd[q];
-      double v = oopsi4 * (-Ddalpha_dd[q] + alpha * Rsum[q]);
+      double v = oopsi4 * (-Ddalpha_dd[q] + alpha * __ldg(rsum + q * stride));
       v -= (1. / 3.) * g_dd[q] * (-Ddalpha + alpha * R);
       v += alpha * (K * A_dd[q] - 2. * AA_dd[q]);
       v += LA_dd[q];
