@@ -371,20 +371,9 @@ GATHER_LOOP
   double beta_u[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) beta_u[a] = __ldg(UV(Z4C_BETAX + a));
-  // the advection sums, read where they enter (lv[n * stride])
+  // the advection sums, each read where it enters (lv[n * stride])
   auto Lv = [&](int n) { return __ldg(lv + (int64_t)n * stride); };
-  double Lsc[4] = {Lv(Z4C_ALPHA), Lv(Z4C_CHI), Lv(Z4C_KHAT), Lv(Z4C_THETA)};
-  double Lbeta_u[3], LGam_u[3], Lg_dd[6], LA_dd[6];
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    Lbeta_u[a] = Lv(Z4C_BETAX + a);
-    LGam_u[a] = Lv(Z4C_GAMX + a);
-  }
-#pragma unroll
-  for (int q = 0; q < 6; ++q) {
-    Lg_dd[q] = Lv(Z4C_GXX + q);
-    LA_dd[q] = Lv(Z4C_AXX + q);
-  }
+  double LGam_u[3], Lg_dd[6], LA_dd[6];
 
   // finalize Lie derivatives, :619-687
   double dbeta_du[3][3];  // [b][a] = d_b beta^a
@@ -407,9 +396,10 @@ GATHER_LOOP
   for (int a = 0; a < 3; ++a)
 #pragma unroll
     for (int b = 0; b < 3; ++b) ddbeta_d[a] += (1. / 3.) * ddbeta[b][sidx(a, b)];
-  const double Lchi = Lsc[1] + (1. / 6.) * opt.chi_psi_power * chi_guarded * dbeta;
+  const double Lchi = Lv(Z4C_CHI) + (1. / 6.) * opt.chi_psi_power * chi_guarded * dbeta;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
+    LGam_u[a] = Lv(Z4C_GAMX + a);
     LGam_u[a] += (2. / 3.) * Gamma_u[a] * dbeta;
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
@@ -423,7 +413,7 @@ GATHER_LOOP
   for (int a = 0; a < 3; ++a)
 #pragma unroll
     for (int b = a; b < 3; ++b) {
-      double lg = Lg_dd[sidx(a, b)], la = LA_dd[sidx(a, b)];
+      double lg = Lv(Z4C_GXX + sidx(a, b)), la = Lv(Z4C_AXX + sidx(a, b));
       lg -= (2. / 3.) * GDD(a, b) * dbeta;
       la -= (2. / 3.) * ADD(a, b) * dbeta;
 #pragma unroll
@@ -438,10 +428,10 @@ GATHER_LOOP
     }
 
   // assemble, :694-902 (matter fields are zero, so their terms vanish exactly)
-  out[Z4C_KHAT] = -Ddalpha + alpha * (trAA + (1. / 3.) * (K * K)) + Lsc[2] +
+  out[Z4C_KHAT] = -Ddalpha + alpha * (trAA + (1. / 3.) * (K * K)) + Lv(Z4C_KHAT) +
                   opt.damp_kappa1 * (1 - opt.damp_kappa2) * alpha * Theta;
   out[Z4C_CHI] = Lchi - (1. / 6.) * opt.chi_psi_power * chi_guarded * alpha * K;
-  out[Z4C_THETA] = Lsc[3] + alpha * (0.5 * Ht - (2. + opt.damp_kappa2) * opt.damp_kappa1 * Theta);
+  out[Z4C_THETA] = Lv(Z4C_THETA) + alpha * (0.5 * Ht - (2. + opt.damp_kappa2) * opt.damp_kappa1 * Theta);
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     double v = 2. * alpha * DA_u[a] + LGam_u[a];
@@ -464,12 +454,12 @@ GATHER_LOOP
     }
   {
     const double fl = opt.lapse_oplog * opt.lapse_harmonicf + opt.lapse_harmonic * alpha;
-    out[Z4C_ALPHA] = (opt.lapse_advect * Lsc[0] - fl * alpha * (Khat + 2 * opt.lapse_K * Theta));
+    out[Z4C_ALPHA] = (opt.lapse_advect * Lv(Z4C_ALPHA) - fl * alpha * (Khat + 2 * opt.lapse_K * Theta));
   }
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const double gam_a = __ldg(UV(Z4C_GAMX + a));
-    double v = opt.shift_Gamma * gam_a + opt.shift_advect * Lbeta_u[a];
+    double v = opt.shift_Gamma * gam_a + opt.shift_advect * Lv(Z4C_BETAX + a);
     if (fabs(opt.shift_alpha2Gamma) > 0.0) v += opt.shift_alpha2Gamma * (alpha * alpha) * gam_a;
     if (fabs(opt.shift_H) > 0.0) {
 #pragma unroll
