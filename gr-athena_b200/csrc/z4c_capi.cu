@@ -181,18 +181,20 @@ int check_block(const z4c_ctx* c, int block, int* b0, int* nb) {
 int64_t reg_elems(const z4c_ctx* c, int reg) { return (int64_t)reg_nvar_(reg) * c->g.nvol * c->g.nblocks; }
 
 // Ghost exchange of a 22-variable register, then the physical BCs; the result
-// lands in `dst` (all points).  With fuse_alg the AlgConstr pass of the task
-// list is folded into the exchange when no physical BC intervenes.
+// lands in `dst` (all points).  With alg the AlgConstr pass of the task list
+// follows; it is folded into the exchange wherever no boundary condition
+// reads the values: everywhere on periodic meshes, else on the blocks that
+// touch no physical face, the others being constrained after their BCs.
 int exchange_into(z4c_ctx* c, const double* src, double* dst, bool alg) {
   const DevParams P = c->dev();
-  const bool fuse = alg && !c->has_outflow;
-  launch_exchange(c->g, P, src, dst, c->nbr, fuse ? 1 : 0, c->stream);
+  const int fuse = !alg ? 0 : (c->has_outflow ? 2 : 1);
+  launch_exchange(c->g, P, src, dst, c->nbr, fuse, c->stream);
   LAUNCH_CHECK("exchange");
   if (c->has_outflow) {
     launch_physical_bcs(c->g, dst, Z4C_NVAR, c->stream);
     LAUNCH_CHECK("physical_bcs");
     if (alg) {
-      launch_alg_constr(c->g, P, dst, 0, c->g.nblocks, c->stream);
+      launch_alg_constr_boundary(c->g, P, dst, c->nbr, c->stream);
       LAUNCH_CHECK("alg_constr");
     }
   }

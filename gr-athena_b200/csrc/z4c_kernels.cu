@@ -801,6 +801,26 @@ __global__ void k_track_update(double* __restrict__ trk, int ntrk, double dt) {
 // primary owner's result for that vertex: k_exchange_ghosts copies it from
 // there.  With fuse_alg the AlgConstr pass that follows in the task list is
 // applied to the interior results, and the ghosts copy those.
+// Whether block b (context order) touches a physical (non-periodic) face.
+// Every vertex a boundary condition reads or writes belongs to such a block:
+// the extrapolation reads the block's own vertices near the face and its
+// ghosts across the faces transverse to it, whose owners sit at the same
+// position along the face normal and so touch the same face.
+__device__ __forceinline__ bool touches_physical_face(const Grid& g, int b) {
+  const int l[3] = {b % g.nb[0], (b / g.nb[0]) % g.nb[1], b / (g.nb[0] * g.nb[1])};
+  bool t = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    t |= (l[a] == 0 && g.bc[2 * a] != Z4C_BC_PERIODIC) ||
+         (l[a] == g.nb[a] - 1 && g.bc[2 * a + 1] != Z4C_BC_PERIODIC);
+  return t;
+}
+// AlgConstr in the exchange: kAlgNone, kAlgAll (no physical faces: every
+// vertex constrained in the exchange), kAlgInner (the blocks that touch no
+// physical face constrained in the exchange, the others by
+// k_alg_constr_boundary after their boundary conditions).
+constexpr int kAlgNone = 0, kAlgAll = 1, kAlgInner = 2;
+
 __constant__ int c_dir_index[27];  // (o0+1) + 3(o1+1) + 9(o2+1) -> neighbour slot
 // supports in list order: 0, 1, 2, 4, 3, 5, 6, 7
 __device__ __forceinline__ constexpr int u_order(int q) { return (q == 3) ? 4 : (q == 4) ? 3 : q; }
@@ -860,7 +880,7 @@ k_exchange_interior(Grid gin, DevParams P, const double* __restrict__ src,
     }
   }
   if constexpr (NV == NVAR) {
-    if (fuse_alg) {
+    if (fuse_alg == kAlgAll || (fuse_alg == kAlgInner && !touches_physical_face(g, b))) {
     double gg[6], AA[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c) {
@@ -884,7 +904,8 @@ k_exchange_interior(Grid gin, DevParams P, const double* __restrict__ src,
 // owner lies beyond a physical face; the boundary conditions overwrite those).
 template <int NV, int NX>
 __global__ void __launch_bounds__(kPointThreads)
-k_exchange_ghosts(Grid gin, double* __restrict__ u, const int* __restrict__ nbr) {
+k_exchange_ghosts(Grid gin, DevParams P, double* __restrict__ u, const int* __restrict__ nbr,
+                  int fuse_alg) {
   const Grid g = fixed_geometry<NX>(gin);
   const int per = (int)g.nvol;
   const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
@@ -913,8 +934,70 @@ k_exchange_ghosts(Grid gin, double* __restrict__ u, const int* __restrict__ nbr)
   double v[NV];
 #pragma unroll
   for (int n = 0; n < NV; ++n) v[n] = sb[(int64_t)n * g.nvol];
+  if constexpr (NV == NVAR) {
+    // a block constrained in the exchange receives from an owner constrained
+    // only after its boundary conditions: constrain the copy
+    if (fuse_alg == kAlgInner && !touches_physical_face(g, b) && touches_physical_face(g, nb)) {
+      double gg[6], AA[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        gg[c] = v[Z4C_GXX + c];
+        AA[c] = v[Z4C_AXX + c];
+      }
+      alg_constr_point(P.p, gg, AA, &v[Z4C_CHI], &v[Z4C_ALPHA]);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        v[Z4C_GXX + c] = gg[c];
+        v[Z4C_AXX + c] = AA[c];
+      }
+    }
+  }
 #pragma unroll
   for (int n = 0; n < NV; ++n) db[(int64_t)n * g.nvol] = v[n];
+}
+
+// AlgConstr after the boundary conditions on the blocks that touch a physical
+// face, except their ghosts copied from blocks constrained in the exchange
+// (those copies already carry the constrained value).
+template <int NX>
+__global__ void __launch_bounds__(kPointThreads)
+k_alg_constr_boundary(Grid gin, DevParams P, double* __restrict__ u, const int* __restrict__ nbr) {
+  const Grid g = fixed_geometry<NX>(gin);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= g.nvol * g.nblocks) return;
+  const int b = (int)(t / g.nvol);
+  if (!touches_physical_face(g, b)) return;
+  const int p = (int)(t % g.nvol);
+  const int idx[3] = {p % g.nn[0], (p / g.nn[0]) % g.nn[1], p / (g.nn[0] * g.nn[1])};
+  int o[3];
+  bool ghost = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    o[a] = (idx[a] < NG) ? -1 : (idx[a] > NG + g.nx[a] ? 1 : 0);
+    ghost |= (o[a] != 0);
+  }
+  if (ghost) {
+    const int nb = __ldg(nbr + b * 26 + c_dir_index[(o[0] + 1) + 3 * (o[1] + 1) + 9 * (o[2] + 1)]);
+    if (nb >= 0 && !touches_physical_face(g, nb)) return;
+  }
+  double* ub = u + (int64_t)b * NVAR * g.nvol + p;
+  double gg[6], AA[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    gg[c] = ub[(int64_t)(Z4C_GXX + c) * g.nvol];
+    AA[c] = ub[(int64_t)(Z4C_AXX + c) * g.nvol];
+  }
+  double chi = ub[(int64_t)Z4C_CHI * g.nvol], alpha = ub[(int64_t)Z4C_ALPHA * g.nvol];
+  alg_constr_point(P.p, gg, AA, &chi, &alpha);
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    ub[(int64_t)(Z4C_GXX + c) * g.nvol] = gg[c];
+    ub[(int64_t)(Z4C_AXX + c) * g.nvol] = AA[c];
+  }
+  if (P.p.force_regularization) {
+    ub[(int64_t)Z4C_CHI * g.nvol] = chi;
+    ub[(int64_t)Z4C_ALPHA * g.nvol] = alpha;
+  }
 }
 
 // ---- extrapolate_outflow boundary conditions --------------------------------
@@ -1498,11 +1581,19 @@ void launch_exchange(const Grid& g, const DevParams& P, const double* src, doubl
   COUNTED
   if (nvar == Z4C_NWEYL) {
     (fx ? k_exchange_ghosts<Z4C_NWEYL, kFixedNX> : k_exchange_ghosts<Z4C_NWEYL, 0>)<<<
-        ng, kPointThreads, 0, st>>>(g, dst, nbr);
+        ng, kPointThreads, 0, st>>>(g, P, dst, nbr, kAlgNone);
   } else {
     (fx ? k_exchange_ghosts<NVAR, kFixedNX> : k_exchange_ghosts<NVAR, 0>)<<<
-        ng, kPointThreads, 0, st>>>(g, dst, nbr);
+        ng, kPointThreads, 0, st>>>(g, P, dst, nbr, fuse_alg);
   }
+}
+
+void launch_alg_constr_boundary(const Grid& g, const DevParams& P, double* u, const int* nbr,
+                                cudaStream_t st) {
+  const int64_t n = g.nvol * g.nblocks;
+  COUNTED
+  (has_fixed_geometry(g) ? k_alg_constr_boundary<kFixedNX> : k_alg_constr_boundary<0>)<<<
+      div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, nbr);
 }
 
 void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st) {

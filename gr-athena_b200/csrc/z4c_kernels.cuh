@@ -106,6 +106,11 @@ void launch_track_update(double* trk, int ntrk, double dt, cudaStream_t st);
 // Z4c::Z4cBoundaryRHS: Sommerfeld right-hand side on gr_sommerfeld faces.
 void launch_boundary_rhs(const Grid& g, const DevParams& P, const double* u, double* rhs,
                          int block0, int nblk, cudaStream_t st);
+// AlgConstr after the boundary conditions for an exchange run with
+// fuse_alg = 2: the blocks that touch a physical face, except the ghosts
+// they copied from blocks constrained in the exchange.
+void launch_alg_constr_boundary(const Grid& g, const DevParams& P, double* u, const int* nbr,
+                                cudaStream_t st);
 void launch_exchange(const Grid& g, const DevParams& P, const double* src, double* dst,
                      const int* nbr, int fuse_alg, cudaStream_t st, int nvar = NVAR);
 void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st);

@@ -2,10 +2,10 @@
 
 The golden fixtures use 8^3 MeshBlocks, which run the generic kernels; every
 kernel of the step also exists in a form specialised for 16^3 MeshBlocks
-(constant strides, whole-loop unrolling).  Here a 2x2x2 mesh of 16^3 blocks
-takes one full step through the captured graph for each integrator and
-boundary condition, including the Sommerfeld and Butcher stage kernels, and
-is compared with the same step on the oracle."""
+(constant strides, whole-loop unrolling).  Here meshes of 2^3 and 3^3
+MeshBlocks of 16^3 take one full step through the captured graph for each
+integrator and boundary condition, including the Sommerfeld and Butcher
+stage kernels, and are compared with the same step on the oracle."""
 import numpy as np
 import pytest
 
@@ -62,13 +62,16 @@ def oracle_step(mesh, p, u, dt, integ):
     return u
 
 
-@pytest.mark.parametrize("integ,bc", [("rk4", "outflow"), ("rk4", "sommerfeld"),
-                                      ("rk4", "periodic"), ("bt_rk4", "outflow"),
-                                      ("bt_rk4", "sommerfeld")])
-def test_one_step_on_16cubed_blocks_matches_oracle(integ, bc):
+@pytest.mark.parametrize("integ,bc,nb", [("rk4", "outflow", 2), ("rk4", "sommerfeld", 2),
+                                         ("rk4", "periodic", 2), ("bt_rk4", "outflow", 2),
+                                         ("bt_rk4", "sommerfeld", 2), ("rk4", "outflow", 3),
+                                         ("bt_rk4", "sommerfeld", 3)])
+def test_one_step_on_16cubed_blocks_matches_oracle(integ, bc, nb):
+    """nb = 3 puts a MeshBlock in the middle that touches no physical face."""
     import z4c_b200 as Z
     from z4c_b200 import initial_data as ID
-    mesh = Z.Mesh((2, 2, 2), (16, 16, 16), (-4.0,) * 3, (4.0,) * 3, bc)
+    lim = 2.0 * nb
+    mesh = Z.Mesh((nb,) * 3, (16, 16, 16), (-lim,) * 3, (lim,) * 3, bc)
     params = Z.default_params(**PARAMS)
     ctx = Z.Z4c(mesh, params, integ)
     ID.load_adm(ctx, ID.punctures(mesh, params, masses=(0.5, 0.5),
