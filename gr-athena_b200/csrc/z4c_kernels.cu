@@ -1008,12 +1008,13 @@ k_alg_constr_boundary(Grid gin, DevParams P, double* __restrict__ u, const int* 
 // Only the blocks on the two faces of axis ax are visited.  One thread per
 // (face block, variable, side, transverse pair) cascades outward; the
 // fastest thread index runs along the transverse axis of smallest stride.
-template <int NX>
+template <int NX, int AX>
 __global__ void __launch_bounds__(kPointThreads)
-k_bc_axis(Grid gin, double* __restrict__ u, int nvar, int ax) {
+k_bc_axis(Grid gin, double* __restrict__ u, int nvar) {
   const Grid g = fixed_geometry<NX>(gin);
-  const int o1 = (ax == 0) ? 1 : 0;       // fastest transverse axis
-  const int o2 = (ax == 2) ? 1 : 2;       // slowest transverse axis
+  constexpr int ax = AX;                  // one instance per axis: static indexing
+  constexpr int o1 = (ax == 0) ? 1 : 0;   // fastest transverse axis
+  constexpr int o2 = (ax == 2) ? 1 : 2;   // slowest transverse axis
   const int64_t nt = (int64_t)g.nn[o1] * g.nn[o2];
   const int nfb = g.nb[o1] * g.nb[o2];    // blocks on one face
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1054,7 +1055,6 @@ k_bc_axis(Grid gin, double* __restrict__ u, int nvar, int ax) {
   if (t1 < lo[o1] || t1 > hi[o1] || t2 < lo[o2] || t2 > hi[o2]) return;
   double* ub = u + ((int64_t)b * nvar + n) * g.nvol + (int64_t)t1 * g.s[o1] + (int64_t)t2 * g.s[o2];
   const int64_t st = g.s[ax];
-  const double c[5] = {5., -10., 10., -5., 1.};
   // w[q] = the value q + 1 vertices inward of the ghost being filled; each
   // new ghost enters the window, so the cascade stays in registers
   const int dir = side ? -1 : 1;
@@ -1065,9 +1065,12 @@ k_bc_axis(Grid gin, double* __restrict__ u, int nvar, int ax) {
 #pragma unroll
   for (int gh = 1; gh <= NG; ++gh) {
     const int ia = side ? ie[ax] + gh : is[ax] - gh;
-    double v = 0.0;
-#pragma unroll
-    for (int q = 0; q < 5; ++q) v += c[q] * w[q];
+    double v = 0.0;  // coefficients 5, -10, 10, -5, 1 (NEXTRAPOLATE = 5)
+    v += 5. * w[0];
+    v += -10. * w[1];
+    v += 10. * w[2];
+    v += -5. * w[3];
+    v += 1. * w[4];
     ub[(int64_t)ia * st] = v;
 #pragma unroll
     for (int q = 4; q > 0; --q) w[q] = w[q - 1];
@@ -1605,8 +1608,11 @@ void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st) {
     const int o1 = (ax == 0) ? 1 : 0, o2 = (ax == 2) ? 1 : 2;
     const int64_t n = (int64_t)g.nn[o1] * g.nn[o2] * 2 * nvar * g.nb[o1] * g.nb[o2];
     COUNTED
-    (has_fixed_geometry(g) ? k_bc_axis<kFixedNX> : k_bc_axis<0>)<<<
-        div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, u, nvar, ax);
+    const bool fx = has_fixed_geometry(g);
+    auto kern = ax == 0 ? (fx ? k_bc_axis<kFixedNX, 0> : k_bc_axis<0, 0>)
+                : ax == 1 ? (fx ? k_bc_axis<kFixedNX, 1> : k_bc_axis<0, 1>)
+                          : (fx ? k_bc_axis<kFixedNX, 2> : k_bc_axis<0, 2>);
+    kern<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, u, nvar);
   }
 }
 
