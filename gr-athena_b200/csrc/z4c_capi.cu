@@ -15,6 +15,7 @@
 #include "../../include/z4c_b200.h"
 #include "z4c_common.cuh"
 #include "z4c_kernels.cuh"
+#include "z4c_multilevel.cuh"
 #include "z4c_restart.cuh"
 #include "z4c_wave.cuh"
 
@@ -70,8 +71,11 @@ double mesh_gen_x(int64_t index, int64_t nrange, double xmin, double xmax) {
 // Vertex coordinates x?f of one block along one axis (nn entries) and its
 // spacing, as Coordinates builds them for a uniform mesh
 // (coordinates/coordinates.cpp:170-198, mesh/mesh.cpp:2537-2556).
-double block_axis_coords(const z4c_mesh_desc_t* mesh, int loc, int axis, double* xf) {
-  const int nx = mesh->nx[axis], nb = mesh->nb[axis], nn = nx + 1 + 2 * Z4C_NG;
+// rlev: the block's level above the root level (nb << rlev blocks per axis).
+double block_axis_coords(const z4c_mesh_desc_t* mesh, int64_t loc, int axis, double* xf,
+                         int rlev = 0) {
+  const int nx = mesh->nx[axis], nn = nx + 1 + 2 * Z4C_NG;
+  const int64_t nb = (int64_t)mesh->nb[axis] << rlev;
   const int64_t nroot = (int64_t)nx * nb;
   const double x0 = mesh->xmin[axis], x1 = mesh->xmax[axis];
   const double bmin = (loc == 0) ? x0 : mesh_gen_x((int64_t)loc * nx, nroot, x0, x1);
@@ -96,6 +100,8 @@ int set_error(int code, const char* msg) {
 
 struct z4c_ctx {
   Grid g{};
+  MlPlan* ml = nullptr;         // multilevel meshes: the ghost-exchange plan
+  std::vector<long long> locs;  // multilevel meshes: {level, lx1, lx2, lx3} per block
   z4c_mesh_desc_t desc{};
   z4c_params_t params{};
   int integrator = Z4C_INTEG_RK4;
@@ -187,6 +193,15 @@ int64_t reg_elems(const z4c_ctx* c, int reg) { return (int64_t)reg_nvar_(reg) * 
 // touch no physical face, the others being constrained after their BCs.
 int exchange_into(z4c_ctx* c, const double* src, double* dst, bool alg) {
   const DevParams P = c->dev();
+  if (c->ml) {  // multilevel: the plan's exchange, then AlgConstr everywhere
+    int rc = launch_ml_exchange(*c->ml, src, dst, Z4C_NVAR, Z4C_NVAR, c->stream);
+    if (rc) return rc;
+    if (alg) {
+      launch_alg_constr(c->g, P, dst, 0, c->g.nblocks, c->stream);
+      LAUNCH_CHECK("alg_constr");
+    }
+    return Z4C_OK;
+  }
   const int fuse = !alg ? 0 : (c->has_outflow ? 2 : 1);
   launch_exchange(c->g, P, src, dst, c->nbr, fuse, c->stream);
   LAUNCH_CHECK("exchange");
@@ -311,6 +326,10 @@ void free_ctx(z4c_ctx* c) {
                   (void*)c->nbr, (void*)c->partials, (void*)c->flag, (void*)c->trk})
     if (p) cudaFree(p);
   for (auto& w : c->waves) wave_free(&w);
+  if (c->ml) {
+    ml_free(*c->ml);
+    delete c->ml;
+  }
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -345,8 +364,11 @@ const char* z4c_last_error(void) { return g_err.c_str(); }
 
 int z4c_reg_nvar(int reg) { return reg_nvar_(reg); }
 
-int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int integrator,
-               z4c_ctx** out) {
+namespace {
+// A context on a uniform block grid (locs == nullptr) or on the nblocks
+// blocks of a refined mesh given by their logical locations in gid order.
+int create_impl(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int integrator,
+                int nblocks_ml, const long long* locs, z4c_ctx** out) {
   if (!mesh || !params || !out) return fail(Z4C_EINVAL, "null argument");
   *out = nullptr;
   if (integrator != Z4C_INTEG_RK4 && integrator != Z4C_INTEG_BT_RK4)
@@ -365,10 +387,17 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
     if ((lo == Z4C_BC_PERIODIC) != (hi == Z4C_BC_PERIODIC))
       return fail(Z4C_EINVAL, "axis %d: periodic on one face only", a);
   }
+  if (locs) {
+    for (int f = 0; f < 6; ++f)
+      if (mesh->bc[f] == Z4C_BC_SOMMERFELD)
+        return fail(Z4C_EINVAL, "refined meshes take outflow or periodic faces");
+    if (nblocks_ml < 1) return fail(Z4C_EINVAL, "refined mesh without blocks");
+  }
+  const int64_t nblocks_all =
+      locs ? (int64_t)nblocks_ml : (int64_t)mesh->nb[0] * mesh->nb[1] * mesh->nb[2];
   {
     // the column passes index (block, variable, interior column) in 32 bits
-    const int64_t cols = (int64_t)(mesh->nx[0] + 1) * (mesh->nx[1] + 1) * Z4C_NVAR *
-                         mesh->nb[0] * mesh->nb[1] * mesh->nb[2];
+    const int64_t cols = (int64_t)(mesh->nx[0] + 1) * (mesh->nx[1] + 1) * Z4C_NVAR * nblocks_all;
     if (cols >= (int64_t)std::numeric_limits<int>::max())
       return fail(Z4C_EINVAL, "mesh too large: %lld interior columns x variables", (long long)cols);
   }
@@ -397,6 +426,25 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
   g.s[2] = (int64_t)g.nn[0] * g.nn[1];
   g.nvol = (int64_t)g.nn[0] * g.nn[1] * g.nn[2];
   g.nblocks = g.nb[0] * g.nb[1] * g.nb[2];
+  if (locs) {
+    // the uniform-grid kernels (exchange, BCs, Sommerfeld faces) never run on
+    // a refined mesh; the block row keeps their indexing in range
+    g.nb[0] = nblocks_ml;
+    g.nb[1] = g.nb[2] = 1;
+    g.nblocks = nblocks_ml;
+    c->locs.assign(locs, locs + 4 * (size_t)nblocks_ml);
+    c->ml = new (std::nothrow) MlPlan();
+    if (!c->ml) {
+      free_ctx(c);
+      return fail(Z4C_ENOMEM, "host allocation");
+    }
+    const int rc = ml_build(mesh->nb, mesh->nx, mesh->bc, nblocks_ml, locs, *c->ml);
+    if (rc) {
+      free_ctx(c);
+      return rc;
+    }
+  }
+  const int root_level = ml_root_level(mesh->nb);
 
   // block coordinates (coordinates/coordinates.cpp:170-198, cartesian.cpp:29)
   const int nb = g.nblocks;
@@ -407,11 +455,16 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
   std::vector<FdScale> hfd(nb);
   const double diss_scaling = std::pow(2, -2 * Z4C_NG) * (Z4C_NG % 2 == 0 ? -1 : 1);
   for (int b = 0; b < nb; ++b) {
-    const int loc[3] = {b % g.nb[0], (b / g.nb[0]) % g.nb[1], b / (g.nb[0] * g.nb[1])};
+    int64_t loc[3] = {b % g.nb[0], (b / g.nb[0]) % g.nb[1], b / (g.nb[0] * g.nb[1])};
+    int rlev = 0;
+    if (locs) {
+      rlev = (int)locs[4 * b] - root_level;
+      for (int a = 0; a < 3; ++a) loc[a] = locs[4 * b + 1 + a];
+    }
     int off = 0, offv = 0;
     for (int a = 0; a < 3; ++a) {
       double* xf = &c->h_xf[(size_t)b * nsum + off];
-      const double dx = block_axis_coords(mesh, loc[a], a, xf);
+      const double dx = block_axis_coords(mesh, loc[a], a, xf, rlev);
       double* xv = &c->h_xv[(size_t)b * (nsum - 3) + offv];
       for (int i = 0; i < g.nn[a] - 1; ++i) xv[i] = 0.5 * (xf[i + 1] + xf[i]);
       c->h_dx[(size_t)b * 3 + a] = dx;
@@ -507,6 +560,30 @@ int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int inte
   }
   c->own_stream = true;
   *out = c;
+  return Z4C_OK;
+}
+}  // namespace
+
+int z4c_create(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int integrator,
+               z4c_ctx** out) {
+  return create_impl(mesh, params, integrator, 0, nullptr, out);
+}
+
+int z4c_create_refined(const z4c_mesh_desc_t* mesh, int nblocks, const long long* locs,
+                       const z4c_params_t* params, int integrator, z4c_ctx** out) {
+  if (!locs) return fail(Z4C_EINVAL, "null argument");
+  return create_impl(mesh, params, integrator, nblocks, locs, out);
+}
+
+int z4c_mesh_loc_coords(const z4c_mesh_desc_t* mesh, const long long loc[4], int axis,
+                        double* x_out, double* dx_out) {
+  if (!mesh || !loc || !x_out || axis < 0 || axis > 2) return fail(Z4C_EINVAL, "bad argument");
+  const int rlev = (int)loc[0] - ml_root_level(mesh->nb);
+  if (rlev < 0 || rlev > 20 || mesh->nx[axis] < 1) return fail(Z4C_EINVAL, "level out of range");
+  if (loc[1 + axis] < 0 || loc[1 + axis] >= ((long long)mesh->nb[axis] << rlev))
+    return fail(Z4C_EINVAL, "logical location out of range");
+  const double dx = block_axis_coords(mesh, loc[1 + axis], axis, x_out, rlev);
+  if (dx_out) *dx_out = dx;
   return Z4C_OK;
 }
 
@@ -759,9 +836,14 @@ int z4c_ghost_fill(z4c_ctx* ctx, int reg) {
     // Mesh::CommunicateAuxZ4c: the Aux group exchange and physical BCs of the
     // Weyl register, through the work register
     double* w = ctx->reg[Z4C_REG_W];
-    launch_exchange(ctx->g, ctx->dev(), ctx->reg[reg], w, ctx->nbr, 0, ctx->stream, Z4C_NWEYL);
-    LAUNCH_CHECK("exchange");
-    if (ctx->has_outflow) {
+    if (ctx->ml) {
+      if ((rc = launch_ml_exchange(*ctx->ml, ctx->reg[reg], w, Z4C_NWEYL, Z4C_NWEYL, ctx->stream)))
+        return rc;
+    } else {
+      launch_exchange(ctx->g, ctx->dev(), ctx->reg[reg], w, ctx->nbr, 0, ctx->stream, Z4C_NWEYL);
+      LAUNCH_CHECK("exchange");
+    }
+    if (ctx->has_outflow && !ctx->ml) {
       launch_physical_bcs(ctx->g, w, Z4C_NWEYL, ctx->stream);
       LAUNCH_CHECK("physical_bcs");
     }
@@ -797,6 +879,7 @@ int z4c_sphere_grid(int nlev, double rad, int bitant, double* geo) {
 
 int z4c_wave_add(z4c_ctx* ctx, double rad, int nlev, int lmax, int bitant, int* id) {
   if (!ctx || !id) return fail(Z4C_EINVAL, "null argument");
+  if (ctx->ml) return fail(Z4C_EINVAL, "psi4 extraction needs a uniform mesh");
   if (nlev < 1 || nlev > 2000) return fail(Z4C_EINVAL, "nlev %d out of range [1, 2000]", nlev);
   if (lmax < 2 || lmax > 16) return fail(Z4C_EINVAL, "lmax %d out of range [2, 16]", lmax);
   if (!(rad > 0.0)) return fail(Z4C_EINVAL, "sphere radius must be positive");
@@ -1070,6 +1153,7 @@ long long z4c_kernel_launches(void) { return kernel_launch_count(); }
 
 int z4c_tracker_add(z4c_ctx* ctx, const double pos[3], int* id) {
   if (!ctx || !pos || !id) return fail(Z4C_EINVAL, "null argument");
+  if (ctx->ml) return fail(Z4C_EINVAL, "puncture trackers need a uniform mesh");
   if (ctx->ntrk >= kMaxTrackers) return fail(Z4C_EINVAL, "at most %d trackers", kMaxTrackers);
   const double rec[8] = {pos[0], pos[1], pos[2], NAN, NAN, NAN, 0.0, 0.0};
   CUDA_TRY(cudaMemcpyAsync(ctx->trk + 8 * ctx->ntrk, rec, sizeof(rec), cudaMemcpyHostToDevice,
@@ -1082,6 +1166,7 @@ int z4c_tracker_add(z4c_ctx* ctx, const double pos[3], int* id) {
 
 int z4c_restart_load(z4c_ctx* ctx, const char* path, z4c_restart_info_t* info_out) {
   if (!ctx || !path) return fail(Z4C_EINVAL, "null argument");
+  if (ctx->ml) return fail(Z4C_EINVAL, "restart files need a uniform mesh");
   z4c_restart_info_t info;
   std::string text, err;
   std::vector<double> u;
@@ -1112,6 +1197,7 @@ int z4c_restart_load(z4c_ctx* ctx, const char* path, z4c_restart_info_t* info_ou
 int z4c_restart_save(z4c_ctx* ctx, const char* path, const char* par_text, double time,
                      double dt, int ncycle) {
   if (!ctx || !path) return fail(Z4C_EINVAL, "null argument");
+  if (ctx->ml) return fail(Z4C_EINVAL, "restart files need a uniform mesh");
   std::vector<double> u((size_t)reg_elems(ctx, Z4C_REG_U));
   std::vector<double> trk((size_t)8 * (ctx->ntrk > 0 ? ctx->ntrk : 1));
   CUDA_TRY(cudaMemcpyAsync(u.data(), ctx->reg[Z4C_REG_U], sizeof(double) * u.size(),

@@ -1,0 +1,789 @@
+// Vertex-centred ghost exchange of a statically refined mesh (several
+// refinement levels), as the reference runs one ghost fill of the Z4c state
+// (task order of task_list/gr/task_list_gr_z4c.cpp:52-64, SEND / RECV / SETB
+// / PROLONG / PHY_BVAL):
+//   restrict   every block injects its interior into its coarse buffer
+//              (CommRegistry::SendBoundaryBuffers, comm_registry.cpp:246-296;
+//              RestrictInterior, refinement_ops.cpp:167-195)
+//   pack       one message per (receiver, neighbour entry) from the sender's
+//              pre-exchange arrays (CommChannel::PackAndSend,
+//              comm_channel.cpp:733-787; ranges index_utilities.hpp:124-216)
+//   unpack     per receiving block, in neighbour order: the fine ghosts start
+//              at zero and the interior at the block's own values; same-level
+//              data is added into the fine array and its coarse payload into
+//              the coarse buffer, data from a coarser block overwrites the
+//              coarse buffer, data from a finer block is added into the fine
+//              array; then both arrays are multiplied by the inverse node
+//              multiplicity (comm_registry.cpp:336-382,
+//              comm_channel.cpp:1278-1474, node_multiplicity.cpp:102-430)
+//   coarse BC  extrapolation on the coarse buffer's physical faces
+//              (physical_bcs.cpp:687-890)
+//   prolong    the ghosts next to each coarser neighbour from the coarse
+//              buffer (refinement_ops.cpp:24-160)
+//   fine BC    extrapolation on the fine array's physical faces
+//              (physical_bcs.cpp:506-670)
+// The host builds the op lists once (neighbour search of
+// mesh/mesh_topology.cpp:278-960 over the blocks' logical locations); each
+// receiving block replays its ops in the reference's order, so every vertex
+// sees the same additions in the same order and the result agrees bit for
+// bit.  Fine arrays [block][var][nn3][nn2][nn1], coarse buffers
+// [block][var][cn3][cn2][cn1] with cn = nx/2 + 1 + 2 NCG.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <set>
+#include <tuple>
+#include <vector>
+
+#include "../../include/z4c_b200.h"
+#include "z4c_kernels.cuh"
+#include "z4c_multilevel.cuh"
+
+namespace z4c {
+
+using refine::RefGeom;
+constexpr int kMlNcg = Z4C_NCG;
+
+namespace {
+
+// ---- kernels ---------------------------------------------------------------
+
+// RestrictVertexCenteredValues over the coarse interior [cvs, cve]^3.
+__global__ void k_ml_restrict(MlPlan P, const double* __restrict__ src, double* __restrict__ coarse,
+                              int nvar, int reg_nvar) {
+  const int c0 = P.nx[0] / 2 + 1, c1 = P.nx[1] / 2 + 1, c2 = P.nx[2] / 2 + 1;
+  const int64_t per = (int64_t)c0 * c1 * c2;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= per * nvar * P.nblocks) return;
+  const int64_t r = t % per;
+  const int n = (int)((t / per) % nvar), b = (int)(t / (per * nvar));
+  const int ci = kMlNcg + (int)(r % c0), cj = kMlNcg + (int)((r / c0) % c1),
+            ck = kMlNcg + (int)(r / ((int64_t)c0 * c1));
+  const int i = 2 * (ci - kMlNcg) + NG, j = 2 * (cj - kMlNcg) + NG, k = 2 * (ck - kMlNcg) + NG;
+  coarse[((int64_t)b * Z4C_NVAR + n) * P.cvol + ((int64_t)ck * P.cn[1] + cj) * P.cn[0] + ci] =
+      __ldg(src + ((int64_t)b * reg_nvar + n) * P.fvol + ((int64_t)k * P.nn[1] + j) * P.nn[0] + i);
+}
+
+__device__ __forceinline__ int64_t ml_index(const MlOp& o, int e, const int* dims) {
+  const int e0 = o.hi[0] - o.lo[0] + 1, e1 = o.hi[1] - o.lo[1] + 1;
+  const int i = o.lo[0] + e % e0, j = o.lo[1] + (e / e0) % e1, k = o.lo[2] + e / (e0 * e1);
+  return ((int64_t)k * dims[1] + j) * dims[0] + i;
+}
+
+// BufferUtility::PackData: one CTA per (pack op, variable).
+__global__ void k_ml_pack(MlPlan P, const double* __restrict__ src, int reg_nvar) {
+  const MlOp o = P.pack[blockIdx.x];
+  const int n = blockIdx.y;
+  const double* a = o.coarse ? P.coarse + ((int64_t)o.blk * Z4C_NVAR + n) * P.cvol
+                             : src + ((int64_t)o.blk * reg_nvar + n) * P.fvol;
+  const int* dims = o.coarse ? P.cn : P.nn;
+  double* out = P.buf + o.off + (int64_t)n * o.count;
+  for (int e = threadIdx.x; e < o.count; e += blockDim.x) out[e] = a[ml_index(o, e, dims)];
+}
+
+// SetBoundaries of one receiving block and variable: the fine array starts
+// as the block's interior with zero ghosts, then its ops run in order.
+__global__ void k_ml_unpack(MlPlan P, const double* __restrict__ src, double* __restrict__ dst,
+                            int reg_nvar) {
+  const int b = blockIdx.x, n = blockIdx.y;
+  const int64_t fo = ((int64_t)b * reg_nvar + n) * P.fvol;
+  const int nn0 = P.nn[0], nn1 = P.nn[1];
+  for (int64_t p = threadIdx.x; p < P.fvol; p += blockDim.x) {
+    const int i = (int)(p % nn0), j = (int)((p / nn0) % nn1), k = (int)(p / ((int64_t)nn0 * nn1));
+    const bool in = i >= NG && i <= NG + P.nx[0] && j >= NG && j <= NG + P.nx[1] && k >= NG &&
+                    k <= NG + P.nx[2];
+    dst[fo + p] = in ? src[fo + p] : 0.0;
+  }
+  double* cb = P.coarse + ((int64_t)b * Z4C_NVAR + n) * P.cvol;
+  for (int q = P.ustart[b]; q < P.ustart[b + 1]; ++q) {
+    __syncthreads();
+    const MlOp o = P.unpack[q];
+    double* a = o.coarse ? cb : dst + fo;
+    const int* dims = o.coarse ? P.cn : P.nn;
+    if (o.mode == kMlZeroGhosts) {
+      const int64_t vol = (int64_t)dims[0] * dims[1] * dims[2];
+      for (int64_t p = threadIdx.x; p < vol; p += blockDim.x) {
+        const int i = (int)(p % dims[0]), j = (int)((p / dims[0]) % dims[1]),
+                  k = (int)(p / ((int64_t)dims[0] * dims[1]));
+        if (i < o.lo[0] || i > o.hi[0] || j < o.lo[1] || j > o.hi[1] || k < o.lo[2] || k > o.hi[2])
+          a[p] = 0.0;
+      }
+      continue;
+    }
+    const double* in = P.buf + o.off + (int64_t)n * o.count;
+    for (int e = threadIdx.x; e < o.count; e += blockDim.x) {
+      double& d = a[ml_index(o, e, dims)];
+      if (o.mode == kMlCopy) d = in[e];
+      else if (o.mode == kMlAdd) d += in[e];
+      else d *= o.inv;
+    }
+  }
+}
+
+// ExtrapolateOutflowBC with NEXTRAPOLATE = 5 (physical_bcs.cpp:187-260),
+// InterpolateLagrangeUniformBiasR<5> weights; one CTA per (face, variable),
+// a thread per transverse vertex walking its ghosts outwards.
+template <int AX>
+__global__ void k_ml_bc(const MlBc* __restrict__ items, double* __restrict__ arr, int64_t bstride,
+                        int64_t vol, int d0, int d1, int ng) {
+  const MlBc it = items[blockIdx.x];
+  const int n = blockIdx.y;
+  constexpr int o1 = AX == 0 ? 1 : 0, o2 = AX == 2 ? 1 : 2;
+  const int64_t st[3] = {1, d0, (int64_t)d0 * d1};
+  const int w1 = it.hi[o1] - it.lo[o1] + 1, w2 = it.hi[o2] - it.lo[o2] + 1;
+  double* a = arr + (int64_t)it.blk * bstride + (int64_t)n * vol;
+  const int dir = it.outer ? -1 : 1;
+  for (int t = threadIdx.x; t < w1 * w2; t += blockDim.x) {
+    const int t1 = it.lo[o1] + t % w1, t2 = it.lo[o2] + t / w1;
+    for (int g = 1; g <= ng; ++g) {
+      const int ia = it.outer ? it.hi[AX] + g : it.lo[AX] - g;
+      const int64_t p = (int64_t)ia * st[AX] + (int64_t)t1 * st[o1] + (int64_t)t2 * st[o2];
+      const int64_t s = dir * st[AX];
+      double v = 0.0;
+      v += 5. * a[p + s];
+      v += -10. * a[p + 2 * s];
+      v += 10. * a[p + 3 * s];
+      v += -5. * a[p + 4 * s];
+      v += 1. * a[p + 5 * s];
+      a[p] = v;
+    }
+  }
+}
+
+// ProlongateVertexCenteredValues over one coarse box per CTA row.
+__global__ void k_ml_prolong(MlPlan P, double* __restrict__ dst, int reg_nvar) {
+  const RefGeom G = P.pro[blockIdx.x];
+  const int b = P.pro_blk[blockIdx.x], n = blockIdx.y;
+  const int e0 = G.fe[0] - G.f0[0] + 1, e1 = G.fe[1] - G.f0[1] + 1, e2 = G.fe[2] - G.f0[2] + 1;
+  const double* C = P.coarse + ((int64_t)b * Z4C_NVAR + n) * P.cvol;
+  double* F = dst + ((int64_t)b * reg_nvar + n) * P.fvol;
+  for (int e = threadIdx.x; e < e0 * e1 * e2; e += blockDim.x) {
+    const int f[3] = {G.f0[0] + e % e0, G.f0[1] + (e / e0) % e1, G.f0[2] + e / (e0 * e1)};
+    double v;
+    if (refine::prolong_value(G, C, f, v)) F[((int64_t)f[2] * G.nn[1] + f[1]) * G.nn[0] + f[0]] = v;
+  }
+}
+
+// ---- host plan -------------------------------------------------------------
+
+struct Loc {
+  int level;
+  long long l[3];
+  bool operator<(const Loc& o) const {
+    return std::tie(level, l[0], l[1], l[2]) < std::tie(o.level, o.l[0], o.l[1], o.l[2]);
+  }
+};
+struct Entry {
+  int gid, level, ox[3], fi[2];
+};
+
+// Index limits of one axis of the fine array (ng = NG, n = nx) or of the
+// coarse buffer (ng = NCG, n = nx/2): MeshBlock::SetIndicialParameters
+// (mesh/meshblock.cpp:850-905).
+struct Ax {
+  int vs, ve, ms, me, ps, pe, gs, ge;
+};
+Ax axis_limits(int n, int ng) {
+  return {ng, ng + n, 0, ng - 1, n + ng + 1, n + 2 * ng, 2 * ng, n};
+}
+
+struct Builder {
+  int nroot[3], nx[3], bc[6], root_level, nb;
+  const long long* locs;
+  std::map<Loc, int> leaf;
+  std::set<Loc> inner;  // refined nodes (ancestors of leaves)
+  std::vector<std::vector<Entry>> nbrs;
+  const char* err = nullptr;
+
+  Loc loc(int b) const { return {(int)locs[4 * b], {locs[4 * b + 1], locs[4 * b + 2], locs[4 * b + 3]}}; }
+
+  // MeshBlockTree::FindNeighbor (meshblock_tree.cpp:400-490): 0 beyond a
+  // non-periodic face, 1 a leaf of the same or the next coarser level, 2 a
+  // refined node (its location in nl); -1 when the 2:1 balance is broken.
+  int find(const Loc& me, const int o[3], Loc& nl, int& gid) const {
+    nl.level = me.level;
+    for (int a = 0; a < 3; ++a) {
+      const long long n = (long long)nroot[a] << (me.level - root_level);
+      nl.l[a] = me.l[a] + o[a];
+      if (nl.l[a] < 0) {
+        if (bc[2 * a] != Z4C_BC_PERIODIC) return 0;
+        nl.l[a] = n - 1;
+      }
+      if (nl.l[a] >= n) {
+        if (bc[2 * a + 1] != Z4C_BC_PERIODIC) return 0;
+        nl.l[a] = 0;
+      }
+    }
+    auto it = leaf.find(nl);
+    if (it != leaf.end()) {
+      gid = it->second;
+      return 1;
+    }
+    if (nl.level > root_level) {
+      const Loc par{nl.level - 1, {nl.l[0] >> 1, nl.l[1] >> 1, nl.l[2] >> 1}};
+      it = leaf.find(par);
+      if (it != leaf.end()) {
+        gid = it->second;
+        return 1;
+      }
+    }
+    return inner.count(nl) ? 2 : -1;
+  }
+  int child(const Loc& nl, const int c[3]) const {
+    const Loc ch{nl.level + 1, {2 * nl.l[0] + c[0], 2 * nl.l[1] + c[1], 2 * nl.l[2] + c[2]}};
+    auto it = leaf.find(ch);
+    return it == leaf.end() ? -1 : it->second;
+  }
+
+  // MeshBlock::SearchAndSetNeighbors (mesh_topology.cpp:278-960), 3-D.
+  bool neighbours(int b, std::vector<Entry>& out) {
+    const Loc me = loc(b);
+    int myox[3];
+    for (int a = 0; a < 3; ++a) myox[a] = (me.l[a] & 1) ? 1 : -1;
+    Loc nl;
+    int gid = -1;
+    auto add = [&](int g, int lev, const int o[3], int f1, int f2) -> bool {
+      if (g < 0) return false;
+      out.push_back({g, lev, {o[0], o[1], o[2]}, {f1, f2}});
+      return true;
+    };
+    for (int ax = 0; ax < 3; ++ax)  // faces
+      for (int s = -1; s <= 1; s += 2) {
+        int o[3] = {0, 0, 0};
+        o[ax] = s;
+        const int r = find(me, o, nl, gid);
+        if (r < 0) return false;
+        if (r == 0) continue;
+        if (r == 2) {
+          const int t1 = ax == 0 ? 1 : 0, t2 = ax == 2 ? 1 : 2;
+          for (int f2 = 0; f2 < 2; ++f2)
+            for (int f1 = 0; f1 < 2; ++f1) {
+              int c[3];
+              c[ax] = 1 - (s + 1) / 2;
+              c[t1] = f1;
+              c[t2] = f2;
+              if (!add(child(nl, c), me.level + 1, o, f1, f2)) return false;
+            }
+        } else {
+          add(gid, (int)locs[4 * gid], o, 0, 0);
+        }
+      }
+    static const int pairs[3][3] = {{0, 1, 2}, {0, 2, 1}, {1, 2, 0}};
+    for (int q = 0; q < 3; ++q) {  // edges x1x2, x1x3, x2x3
+      const int a0 = pairs[q][0], a1 = pairs[q][1], a2 = pairs[q][2];
+      for (int m = -1; m <= 1; m += 2)
+        for (int n = -1; n <= 1; n += 2) {
+          int o[3] = {0, 0, 0};
+          o[a0] = n;
+          o[a1] = m;
+          const int r = find(me, o, nl, gid);
+          if (r < 0) return false;
+          if (r == 0) continue;
+          if (r == 2) {
+            for (int f1 = 0; f1 < 2; ++f1) {
+              int c[3];
+              c[a0] = 1 - (n + 1) / 2;
+              c[a1] = 1 - (m + 1) / 2;
+              c[a2] = f1;
+              if (!add(child(nl, c), me.level + 1, o, f1, 0)) return false;
+            }
+          } else {
+            const int lev = (int)locs[4 * gid];
+            if (lev >= me.level || (myox[a0] == n && myox[a1] == m)) add(gid, lev, o, 0, 0);
+          }
+        }
+    }
+    for (int l = -1; l <= 1; l += 2)  // corners
+      for (int m = -1; m <= 1; m += 2)
+        for (int n = -1; n <= 1; n += 2) {
+          const int o[3] = {n, m, l};
+          const int r = find(me, o, nl, gid);
+          if (r < 0) return false;
+          if (r == 0) continue;
+          int lev;
+          if (r == 2) {
+            const int c[3] = {1 - (n + 1) / 2, 1 - (m + 1) / 2, 1 - (l + 1) / 2};
+            gid = child(nl, c);
+            if (gid < 0) return false;
+            lev = me.level + 1;
+          } else {
+            lev = (int)locs[4 * gid];
+          }
+          if (lev >= me.level || (myox[0] == n && myox[1] == m && myox[2] == l))
+            add(gid, lev, o, 0, 0);
+        }
+    return true;
+  }
+};
+
+// the sub-block index that narrows axis a of a finer neighbour's range
+// (index_utilities.cpp:830-873, 1044-1090)
+int narrowing_fi(const Entry& e, int a) {
+  if (a == 0) return e.fi[0];
+  if (a == 1) return e.ox[0] != 0 ? e.fi[0] : e.fi[1];
+  return (e.ox[0] != 0 && e.ox[1] != 0) ? e.fi[0] : e.fi[1];
+}
+
+MlOp make_op(int blk, int coarse, int mode, const int lo[3], const int hi[3]) {
+  MlOp o{};
+  o.blk = blk;
+  o.coarse = coarse;
+  o.mode = mode;
+  o.count = 1;
+  for (int a = 0; a < 3; ++a) {
+    o.lo[a] = lo[a];
+    o.hi[a] = hi[a];
+    o.count *= hi[a] - lo[a] + 1;
+  }
+  return o;
+}
+
+template <typename T>
+int upload(T** dst, const std::vector<T>& v) {
+  *dst = nullptr;
+  if (v.empty()) return Z4C_OK;
+  if (cudaMalloc((void**)dst, sizeof(T) * v.size()) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(Z4C_ENOMEM, "multilevel plan: device allocation");
+  }
+  if (cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return set_error(Z4C_ECUDA, "multilevel plan: upload");
+  return Z4C_OK;
+}
+
+}  // namespace
+
+int ml_root_level(const int nroot[3]) {
+  const int nbmax = std::max(nroot[0], std::max(nroot[1], nroot[2]));
+  int r = 0;
+  while ((1 << r) < nbmax) ++r;
+  return r;
+}
+
+void ml_free(MlPlan& p) {
+  for (void* q : {(void*)p.coarse, (void*)p.buf, (void*)p.pack, (void*)p.unpack, (void*)p.ustart,
+                  (void*)p.pro, (void*)p.pro_blk})
+    if (q) cudaFree(q);
+  for (auto& lv : p.bc)
+    for (MlBc*& q : lv) {
+      if (q) cudaFree(q);
+      q = nullptr;
+    }
+  p = MlPlan{};
+}
+
+int ml_build(const int nroot[3], const int nx[3], const int bcf[6], int nblocks,
+             const long long* locs, MlPlan& plan, int query_block, int* query_out) {
+  plan = MlPlan{};
+  if (nblocks < 1 || !locs) return set_error(Z4C_EINVAL, "multilevel mesh: no blocks");
+  Builder B;
+  for (int a = 0; a < 3; ++a) {
+    B.nroot[a] = nroot[a];
+    B.nx[a] = nx[a];
+    if (nx[a] % 2 || nx[a] < 2 * NG)
+      return set_error(Z4C_EINVAL, "multilevel mesh: block cells must be even and >= 2*ng");
+  }
+  for (int f = 0; f < 6; ++f) B.bc[f] = bcf[f];
+  B.root_level = ml_root_level(nroot);
+  B.nb = nblocks;
+  B.locs = locs;
+  // the blocks must tile the root grid: distinct leaves, none inside
+  // another, their volumes summing to the root grid's
+  int maxlev = B.root_level;
+  for (int b = 0; b < nblocks; ++b) {
+    const Loc l = B.loc(b);
+    if (l.level < B.root_level || l.level > B.root_level + 12)
+      return set_error(Z4C_EINVAL, "multilevel mesh: block level out of range");
+    for (int a = 0; a < 3; ++a)
+      if (l.l[a] < 0 || l.l[a] >= ((long long)nroot[a] << (l.level - B.root_level)))
+        return set_error(Z4C_EINVAL, "multilevel mesh: logical location outside the root grid");
+    if (!B.leaf.emplace(l, b).second) return set_error(Z4C_EINVAL, "multilevel mesh: duplicate block");
+    maxlev = std::max(maxlev, l.level);
+  }
+  long long vol = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    Loc l = B.loc(b);
+    vol += 1LL << (3 * (maxlev - l.level));
+    while (l.level > B.root_level) {
+      l = {l.level - 1, {l.l[0] >> 1, l.l[1] >> 1, l.l[2] >> 1}};
+      if (B.leaf.count(l)) return set_error(Z4C_EINVAL, "multilevel mesh: block inside another");
+      B.inner.insert(l);
+    }
+  }
+  if (vol != (long long)nroot[0] * nroot[1] * nroot[2] << (3 * (maxlev - B.root_level)))
+    return set_error(Z4C_EINVAL, "multilevel mesh: the blocks do not cover the root grid");
+  B.nbrs.resize(nblocks);
+  for (int b = 0; b < nblocks; ++b)
+    if (!B.neighbours(b, B.nbrs[b]))
+      return set_error(Z4C_EINVAL, "multilevel mesh: neighbouring levels differ by more than one");
+  if (query_out && query_block != -2) {  // the neighbour list of one block, no plan
+    if (query_block < 0 || query_block >= nblocks)
+      return set_error(Z4C_EINVAL, "multilevel mesh: block out of range");
+    int q = 0;
+    for (const Entry& e : B.nbrs[query_block]) {
+      const int row[7] = {e.gid, e.level, e.ox[0], e.ox[1], e.ox[2], e.fi[0], e.fi[1]};
+      std::memcpy(query_out + 7 * q++, row, sizeof(row));
+    }
+    return q;
+  }
+
+  Ax F[3], C[3];
+  for (int a = 0; a < 3; ++a) {
+    F[a] = axis_limits(nx[a], NG);
+    C[a] = axis_limits(nx[a] / 2, kMlNcg);
+    plan.nx[a] = nx[a];
+    plan.nn[a] = nx[a] + 1 + 2 * NG;
+    plan.cn[a] = nx[a] / 2 + 1 + 2 * kMlNcg;
+  }
+  plan.nblocks = nblocks;
+  plan.fvol = (long long)plan.nn[0] * plan.nn[1] * plan.nn[2];
+  plan.cvol = (long long)plan.cn[0] * plan.cn[1] * plan.cn[2];
+
+  std::vector<MlOp> pack;
+  std::vector<std::vector<MlOp>> unpack(nblocks);
+  long long off = 0;
+  auto push_pair = [&](int sender, int scoarse, const int slo[3], const int shi[3], int receiver,
+                       int rcoarse, int mode, const int rlo[3], const int rhi[3]) {
+    MlOp s = make_op(sender, scoarse, kMlCopy, slo, shi);
+    MlOp r = make_op(receiver, rcoarse, mode, rlo, rhi);
+    s.off = r.off = off;
+    off += (long long)s.count * Z4C_NVAR;
+    pack.push_back(s);
+    unpack[receiver].push_back(r);
+    return s.count == r.count;
+  };
+  for (int r = 0; r < nblocks; ++r) {
+    const int rlev = (int)locs[4 * r];
+    bool same = true;
+    for (const Entry& e : B.nbrs[r]) same = same && e.level == rlev;
+    {
+      const int lo[3] = {C[0].vs, C[1].vs, C[2].vs}, hi[3] = {C[0].ve, C[1].ve, C[2].ve};
+      unpack[r].push_back(make_op(r, 1, kMlZeroGhosts, lo, hi));
+    }
+    for (const Entry& e : B.nbrs[r]) {
+      const int s = e.gid;
+      const Entry* back = nullptr;  // the sender's entry pointing at r
+      for (const Entry& c : B.nbrs[s])
+        if (c.gid == r && c.ox[0] == -e.ox[0] && c.ox[1] == -e.ox[1] && c.ox[2] == -e.ox[2]) {
+          back = &c;
+          break;
+        }
+      if (!back) return set_error(Z4C_EINVAL, "multilevel mesh: asymmetric neighbour lists");
+      int slo[3], shi[3], rlo[3], rhi[3];
+      bool ok = true;
+      if (e.level == rlev) {
+        // LoadSameLevel / SetSameLevel (index_utilities.cpp:56-106, 271-318)
+        for (int a = 0; a < 3; ++a) {
+          const int so = back->ox[a], ro = e.ox[a];
+          slo[a] = so > 0 ? F[a].ge : F[a].vs;
+          shi[a] = so < 0 ? F[a].gs : F[a].ve;
+          rlo[a] = ro == 0 ? F[a].vs : (ro > 0 ? F[a].ve : F[a].ms);
+          rhi[a] = ro == 0 ? F[a].ve : (ro > 0 ? F[a].pe : F[a].vs);
+        }
+        ok = push_pair(s, 0, slo, shi, r, 0, kMlAdd, rlo, rhi);
+        if (!same) {  // the coarse payload
+          for (int a = 0; a < 3; ++a) {
+            const int so = back->ox[a], ro = e.ox[a];
+            slo[a] = so > 0 ? C[a].ge : C[a].vs;
+            shi[a] = so < 0 ? C[a].gs : C[a].ve;
+            rlo[a] = ro == 0 ? C[a].vs : (ro > 0 ? C[a].ve : C[a].ms);
+            rhi[a] = ro == 0 ? C[a].ve : (ro > 0 ? C[a].pe : C[a].vs);
+          }
+          ok = ok && push_pair(s, 1, slo, shi, r, 1, kMlAdd, rlo, rhi);
+        }
+      } else if (e.level < rlev) {
+        // the sender is coarser: LoadToFiner from its fine array, copied into
+        // the receiver's coarse buffer (SetFromCoarser)
+        for (int a = 0; a < 3; ++a) {
+          const int so = back->ox[a], ro = e.ox[a];
+          const int hs = nx[a] / 2 - kMlNcg;
+          if (so > 0) { slo[a] = F[a].ve - kMlNcg; shi[a] = F[a].ve - 1; }
+          else if (so < 0) { slo[a] = F[a].vs + 1; shi[a] = F[a].vs + kMlNcg; }
+          else {
+            slo[a] = F[a].vs;
+            shi[a] = F[a].ve;
+            if (narrowing_fi(*back, a) == 1) slo[a] += hs;
+            else shi[a] -= hs;
+          }
+          if (ro == 0) {
+            rlo[a] = C[a].vs;
+            rhi[a] = C[a].ve;
+            if ((locs[4 * r + 1 + a] & 1) == 0) rhi[a] = C[a].pe;
+            else rlo[a] = C[a].ms;
+          } else if (ro > 0) { rlo[a] = C[a].ps; rhi[a] = C[a].pe; }
+          else { rlo[a] = C[a].ms; rhi[a] = C[a].me; }
+        }
+        ok = push_pair(s, 0, slo, shi, r, 1, kMlCopy, rlo, rhi);
+      } else {
+        // the sender is finer: LoadToCoarser from its coarse buffer, added
+        // into the receiver's fine array (SetFromFiner)
+        for (int a = 0; a < 3; ++a) {
+          const int so = back->ox[a], ro = e.ox[a];
+          if (so > 0) { slo[a] = C[a].ve - NG; shi[a] = C[a].ve; }
+          else if (so < 0) { slo[a] = C[a].vs; shi[a] = C[a].vs + NG; }
+          else { slo[a] = C[a].vs; shi[a] = C[a].ve; }
+          if (ro == 0) {
+            rlo[a] = F[a].vs;
+            rhi[a] = F[a].ve;
+            if (narrowing_fi(e, a) == 1) rlo[a] += nx[a] / 2;
+            else rhi[a] -= nx[a] / 2;
+          } else if (ro > 0) { rlo[a] = F[a].ve; rhi[a] = F[a].pe; }
+          else { rlo[a] = F[a].ms; rhi[a] = F[a].vs; }
+        }
+        ok = push_pair(s, 1, slo, shi, r, 0, kMlAdd, rlo, rhi);
+      }
+      if (!ok) return set_error(Z4C_EINVAL, "multilevel mesh: message sizes disagree");
+    }
+    // node multiplicity in the 7-zone compact space (NodeMultiplicity::
+    // Precompute) and its division ops, fine array then coarse buffer
+    unsigned short mult[7][7][7];
+    std::memset(mult, 0, sizeof(mult));
+    for (int k = 1; k <= 5; ++k)
+      for (int j = 1; j <= 5; ++j)
+        for (int i = 1; i <= 5; ++i) mult[k][j][i] = 1;
+    for (const Entry& e : B.nbrs[r]) {
+      int s[3], t[3];
+      for (int a = 0; a < 3; ++a) {
+        const int ox = e.ox[a];
+        if (e.level == rlev || e.level > rlev) {
+          if (ox == 0) {
+            s[a] = 1;
+            t[a] = 5;
+            if (e.level > rlev) {
+              if (narrowing_fi(e, a) == 1) s[a] += 2;
+              else t[a] -= 2;
+            }
+          } else if (ox > 0) { s[a] = 5; t[a] = 6; }
+          else { s[a] = 0; t[a] = 1; }
+        } else {
+          if (ox == 0) {
+            s[a] = 1;
+            t[a] = 5;
+            if ((locs[4 * r + 1 + a] & 1) == 0) t[a] = 6;
+            else s[a] = 0;
+          } else if (ox > 0) { s[a] = t[a] = 6; }
+          else { s[a] = t[a] = 0; }
+        }
+      }
+      for (int k = s[2]; k <= t[2]; ++k)
+        for (int j = s[1]; j <= t[1]; ++j)
+          for (int i = s[0]; i <= t[0]; ++i) ++mult[k][j][i];
+    }
+    for (int coarse = 0; coarse < 2; ++coarse) {
+      const Ax* X = coarse ? C : F;
+      auto phys = [](int c, const Ax& a, int& lo, int& hi) {  // ApplyDivisionImpl's PhysRange
+        const int half = (a.ve - a.vs) / 2;
+        const int t[7] = {a.ms, a.vs, a.vs + 1, a.vs + half, a.ve - 1, a.ve, a.pe};
+        if (c & 1) lo = hi = t[c];
+        else if (c <= 3) { lo = t[c]; hi = t[c + 1] - 1; }
+        else { lo = t[c - 1] + 1; hi = t[c]; }
+      };
+      for (int K = 0; K < 7; ++K)
+        for (int J = 0; J < 7; ++J)
+          for (int I = 0; I < 7; ++I) {
+            if (mult[K][J][I] <= 1) continue;
+            int lo[3], hi[3];
+            phys(I, X[0], lo[0], hi[0]);
+            phys(J, X[1], lo[1], hi[1]);
+            phys(K, X[2], lo[2], hi[2]);
+            if (lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]) continue;
+            MlOp o = make_op(r, coarse, kMlScale, lo, hi);
+            o.inv = 1.0 / static_cast<double>(mult[K][J][I]);
+            unpack[r].push_back(o);
+          }
+    }
+  }
+  // physical faces: extrapolation on the coarse buffer with the vertex
+  // interior ends (ApplyPhysicalBCsOnCoarseLevel, called with the Z4c coarse
+  // indices civs..cive and NCGHOST) and on the fine array with the cell
+  // interior ends (ApplyPhysicalBCs, is..ie)
+  std::vector<MlBc> bcs[2][3];
+  std::vector<RefGeom> pro;
+  std::vector<int> pro_blk;
+  for (int b = 0; b < nblocks; ++b) {
+    const Loc l = B.loc(b);
+    int need[6];
+    for (int a = 0; a < 3; ++a) {
+      const long long n = (long long)nroot[a] << (l.level - B.root_level);
+      need[2 * a] = bcf[2 * a] != Z4C_BC_PERIODIC && l.l[a] == 0;
+      need[2 * a + 1] = bcf[2 * a + 1] != Z4C_BC_PERIODIC && l.l[a] == n - 1;
+    }
+    for (int lv = 0; lv < 2; ++lv) {
+      const int ng = lv ? kMlNcg : NG;
+      int is[3], ie[3];
+      for (int a = 0; a < 3; ++a) {
+        is[a] = lv ? C[a].vs : NG;
+        ie[a] = lv ? C[a].ve : NG + nx[a] - 1;
+      }
+      const int bis = is[0] - ng, bie = ie[0] + ng;
+      const int bjs = need[2] ? is[1] : is[1] - ng, bje = need[3] ? ie[1] : ie[1] + ng;
+      const int bks = need[4] ? is[2] : is[2] - ng, bke = need[5] ? ie[2] : ie[2] + ng;
+      for (int face = 0; face < 6; ++face) {
+        if (!need[face]) continue;
+        const int ax = face / 2;
+        MlBc it{};
+        it.blk = b;
+        it.outer = face % 2;
+        it.lo[ax] = is[ax];
+        it.hi[ax] = ie[ax];
+        if (ax == 0) { it.lo[1] = bjs; it.hi[1] = bje; it.lo[2] = bks; it.hi[2] = bke; }
+        else if (ax == 1) { it.lo[0] = bis; it.hi[0] = bie; it.lo[2] = bks; it.hi[2] = bke; }
+        else { it.lo[0] = bis; it.hi[0] = bie; it.lo[1] = is[1] - ng; it.hi[1] = ie[1] + ng; }
+        bcs[lv][ax].push_back(it);
+      }
+    }
+    // ProlongationIndices (refinement_ops.cpp:24-80) per coarser neighbour
+    bool coarser = false;
+    for (const Entry& e : B.nbrs[b]) {
+      if (e.level >= l.level) continue;
+      coarser = true;
+      const int pcng = NG / 2 + (NG % 2 != 0);
+      int box[6];
+      for (int a = 0; a < 3; ++a) {
+        const int ox = e.ox[a];
+        int s, t;
+        if (ox > 0) { s = C[a].ve + 1; t = C[a].ve + pcng; }
+        else if (ox < 0) { s = C[a].vs - pcng; t = C[a].vs - 1; }
+        else {
+          s = C[a].vs;
+          t = C[a].ve;
+          if ((l.l[a] & 1) == 0) t += pcng;
+          else s -= pcng;
+        }
+        box[2 * a] = s;
+        box[2 * a + 1] = t;
+      }
+      RefGeom G{};
+      int rc = refine::setup(nx, 1, 1, box, G, true);
+      if (rc) return rc;
+      pro.push_back(G);
+      pro_blk.push_back(b);
+    }
+    plan.ncoarser += coarser;
+  }
+  // every box, ghost write and extrapolation read stays inside its array
+  auto inside = [&](const MlOp& o) {
+    const int* d = o.coarse ? plan.cn : plan.nn;
+    for (int a = 0; a < 3; ++a)
+      if (o.lo[a] < 0 || o.hi[a] >= d[a] || o.lo[a] > o.hi[a]) return false;
+    return o.blk >= 0 && o.blk < nblocks;
+  };
+  for (const MlOp& o : pack)
+    if (!inside(o)) return set_error(Z4C_EINVAL, "multilevel plan: pack box outside the array");
+  for (const auto& v : unpack)
+    for (const MlOp& o : v)
+      if (!inside(o)) return set_error(Z4C_EINVAL, "multilevel plan: unpack box outside the array");
+  for (int lv = 0; lv < 2; ++lv)
+    for (int a = 0; a < 3; ++a)
+      for (const MlBc& it : bcs[lv][a]) {
+        const int* d = lv ? plan.cn : plan.nn;
+        const int ng = lv ? kMlNcg : NG;
+        for (int t = 0; t < 3; ++t)
+          if (t != a && (it.lo[t] < 0 || it.hi[t] >= d[t]))
+            return set_error(Z4C_EINVAL, "multilevel plan: boundary face outside the array");
+        // ghosts lo-ng..lo-1 read up to lo-1+5; ghosts hi+1..hi+ng read down to hi+1-5
+        if (it.lo[a] - ng < 0 || it.hi[a] + ng >= d[a] || it.lo[a] - 1 + 5 >= d[a] ||
+            it.hi[a] + 1 - 5 < 0)
+          return set_error(Z4C_EINVAL, "multilevel plan: boundary ghosts outside the array");
+      }
+
+  if (query_out) {  // query_block == -2: the op counts of the checked plan, no device memory
+    size_t nu = 0;
+    for (const auto& v : unpack) nu += v.size();
+    query_out[0] = (int)pack.size();
+    query_out[1] = (int)nu;
+    query_out[2] = (int)pro.size();
+    int nbc = 0;
+    for (int lv = 0; lv < 2; ++lv)
+      for (int a = 0; a < 3; ++a) nbc += (int)bcs[lv][a].size();
+    query_out[3] = nbc;
+    return 4;
+  }
+  std::vector<MlOp> uflat;
+  std::vector<int> ustart(nblocks + 1, 0);
+  for (int b = 0; b < nblocks; ++b) {
+    ustart[b] = (int)uflat.size();
+    uflat.insert(uflat.end(), unpack[b].begin(), unpack[b].end());
+  }
+  ustart[nblocks] = (int)uflat.size();
+
+  int rc = Z4C_OK;
+  auto fail_free = [&](int code) {
+    ml_free(plan);
+    return code;
+  };
+  if (cudaMalloc((void**)&plan.coarse, sizeof(double) * Z4C_NVAR * plan.cvol * nblocks) != cudaSuccess) {
+    cudaGetLastError();
+    return fail_free(set_error(Z4C_ENOMEM, "multilevel plan: coarse buffers"));
+  }
+  plan.buf_elems = std::max(off, 1LL);
+  if (cudaMalloc((void**)&plan.buf, sizeof(double) * plan.buf_elems) != cudaSuccess) {
+    cudaGetLastError();
+    return fail_free(set_error(Z4C_ENOMEM, "multilevel plan: message buffer"));
+  }
+  if ((rc = upload(&plan.pack, pack)) || (rc = upload(&plan.unpack, uflat)) ||
+      (rc = upload(&plan.ustart, ustart)) || (rc = upload(&plan.pro, pro)) ||
+      (rc = upload(&plan.pro_blk, pro_blk)))
+    return fail_free(rc);
+  plan.npack = (int)pack.size();
+  plan.nunpack = (int)uflat.size();
+  plan.npro = (int)pro.size();
+  for (int lv = 0; lv < 2; ++lv)
+    for (int a = 0; a < 3; ++a) {
+      if ((rc = upload(&plan.bc[lv][a], bcs[lv][a]))) return fail_free(rc);
+      plan.nbc[lv][a] = (int)bcs[lv][a].size();
+    }
+  return Z4C_OK;
+}
+
+int launch_ml_exchange(const MlPlan& P, const double* src, double* dst, int nvar, int reg_nvar,
+                       cudaStream_t st) {
+  if (nvar < 1 || nvar > Z4C_NVAR || reg_nvar < nvar)
+    return set_error(Z4C_EINVAL, "multilevel exchange: bad variable count");
+  long long launches = 0;
+  {
+    const int64_t n = (int64_t)(P.nx[0] / 2 + 1) * (P.nx[1] / 2 + 1) * (P.nx[2] / 2 + 1) * nvar *
+                      P.nblocks;
+    k_ml_restrict<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, src, P.coarse, nvar, reg_nvar);
+    ++launches;
+  }
+  if (P.npack > 0) {
+    k_ml_pack<<<dim3(P.npack, nvar), 128, 0, st>>>(P, src, reg_nvar);
+    ++launches;
+  }
+  k_ml_unpack<<<dim3(P.nblocks, nvar), 256, 0, st>>>(P, src, dst, reg_nvar);
+  ++launches;
+  auto bc_axis = [&](int lv, double* arr, int64_t bstride, int64_t vol, const int* dims, int ng) {
+    for (int a = 0; a < 3; ++a) {
+      if (!P.nbc[lv][a]) continue;
+      const dim3 grid(P.nbc[lv][a], nvar);
+      if (a == 0) k_ml_bc<0><<<grid, 128, 0, st>>>(P.bc[lv][a], arr, bstride, vol, dims[0], dims[1], ng);
+      else if (a == 1) k_ml_bc<1><<<grid, 128, 0, st>>>(P.bc[lv][a], arr, bstride, vol, dims[0], dims[1], ng);
+      else k_ml_bc<2><<<grid, 128, 0, st>>>(P.bc[lv][a], arr, bstride, vol, dims[0], dims[1], ng);
+      ++launches;
+    }
+  };
+  bc_axis(1, P.coarse, (int64_t)Z4C_NVAR * P.cvol, P.cvol, P.cn, kMlNcg);
+  if (P.npro > 0) {
+    k_ml_prolong<<<dim3(P.npro, nvar), 128, 0, st>>>(P, dst, reg_nvar);
+    ++launches;
+  }
+  bc_axis(0, dst, (int64_t)reg_nvar * P.fvol, P.fvol, P.nn, NG);
+  add_kernel_launches(launches);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(Z4C_ECUDA, cudaGetErrorString(e));
+  return Z4C_OK;
+}
+
+}  // namespace z4c
+
+extern "C" int z4c_refined_neighbours(const z4c_mesh_desc_t* mesh, int nblocks, const long long* locs,
+                                      int block, int* out) {
+  using namespace z4c;
+  if (!mesh || !locs || !out) return set_error(Z4C_EINVAL, "null argument");
+  MlPlan plan;
+  return ml_build(mesh->nb, mesh->nx, mesh->bc, nblocks, locs, plan, block, out);
+}

@@ -44,7 +44,8 @@ HST_COLUMNS = ("H-norm2", "M-norm2", "Mx-norm2", "My-norm2", "Mz-norm2", "Z-norm
 EXPORTS = (
     "z4c_params_default", "z4c_last_error", "z4c_create", "z4c_destroy",
     "z4c_set_stream", "z4c_sync", "z4c_num_blocks", "z4c_block_nn", "z4c_reg_nvar",
-    "z4c_dx", "z4c_block_coords", "z4c_mesh_block_coords", "z4c_mesh_new_dt", "z4c_upload", "z4c_download", "z4c_device_ptr",
+    "z4c_dx", "z4c_block_coords", "z4c_mesh_block_coords", "z4c_mesh_new_dt",
+    "z4c_mesh_loc_coords", "z4c_create_refined", "z4c_refined_neighbours", "z4c_upload", "z4c_download", "z4c_device_ptr",
     "z4c_rhs", "z4c_boundary_rhs", "z4c_add_rhs", "z4c_weighted_ave", "z4c_alg_constr", "z4c_adm_to_z4c",
     "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_weyl", "z4c_ghost_fill", "z4c_init_finalize",
     "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
@@ -116,6 +117,12 @@ def lib():
         L.z4c_block_coords.argtypes = [vp, ip, ip, dp]
         L.z4c_mesh_block_coords.argtypes = [C.POINTER(MeshDesc), ip, ip, dp, dp]
         L.z4c_mesh_new_dt.argtypes = [C.POINTER(MeshDesc), C.c_double, dp]
+        L.z4c_mesh_loc_coords.argtypes = [C.POINTER(MeshDesc), C.POINTER(C.c_longlong), ip, dp,
+                                          dp]
+        L.z4c_create_refined.argtypes = [C.POINTER(MeshDesc), ip, C.POINTER(C.c_longlong),
+                                         C.POINTER(Params), ip, C.POINTER(vp)]
+        L.z4c_refined_neighbours.argtypes = [C.POINTER(MeshDesc), ip, C.POINTER(C.c_longlong),
+                                             ip, C.POINTER(C.c_int)]
         L.z4c_upload.argtypes = [vp, ip, ip, dp]
         L.z4c_download.argtypes = [vp, ip, ip, dp]
         L.z4c_device_ptr.argtypes = [vp, ip, C.POINTER(dp)]
@@ -247,9 +254,15 @@ def default_params(**overrides):
 
 
 class Mesh:
-    """Uniform single-level block grid (reference <mesh>/<meshblock> blocks)."""
+    """Block grid of the reference's <mesh>/<meshblock> blocks: nb root
+    blocks per axis of nx cells.  With `refinement` (the <refinementN>
+    blocks: dicts of x1min, x1max, x2min, x2max, x3min, x3max and level) the
+    mesh is statically refined as Mesh's constructor builds it
+    (mesh/mesh.cpp:488-665, MeshBlockTree::AddMeshBlock / Refine,
+    mesh/meshblock_tree.cpp:108-230): `locs` then lists every MeshBlock in gid
+    order as (level, lx1, lx2, lx3)."""
 
-    def __init__(self, nb, nx, xmin, xmax, bc="periodic"):
+    def __init__(self, nb, nx, xmin, xmax, bc="periodic", refinement=None):
         self.nb = tuple(int(v) for v in nb)
         self.nx = tuple(int(v) for v in nx)
         self.xmin = tuple(float(v) for v in xmin)
@@ -257,9 +270,15 @@ class Mesh:
         if isinstance(bc, str):
             bc = [BC_NAMES[bc]] * 6
         self.bc = tuple(int(v) for v in bc)
+        self.root_level = max(0, (max(self.nb) - 1).bit_length())
+        self.locs = None
+        if refinement:
+            self.locs = _smr_blocks(self, refinement)
 
     @property
     def nblocks(self):
+        if self.locs is not None:
+            return len(self.locs)
         return self.nb[0] * self.nb[1] * self.nb[2]
 
     @property
@@ -280,19 +299,38 @@ class Mesh:
         the host exactly as the reference's Coordinates constructor does."""
         xs, dxs = [], []
         d = self.desc()
+        loc = None
+        if self.locs is not None:
+            loc = (C.c_longlong * 4)(*[int(v) for v in self.locs[block]])
         for a in range(3):
             x = np.empty(self.nn[a])
             dx = C.c_double()
-            _check(lib().z4c_mesh_block_coords(C.byref(d), block, a,
-                                               x.ctypes.data_as(C.POINTER(C.c_double)),
-                                               C.byref(dx)))
+            xp = x.ctypes.data_as(C.POINTER(C.c_double))
+            if loc is None:
+                _check(lib().z4c_mesh_block_coords(C.byref(d), block, a, xp, C.byref(dx)))
+            else:
+                _check(lib().z4c_mesh_loc_coords(C.byref(d), loc, a, xp, C.byref(dx)))
             xs.append(x)
             dxs.append(dx.value)
         return xs, dxs
 
+    def neighbours(self, block):
+        """Neighbour list of one block of a refined mesh as the context builds
+        it: rows (gid, level, ox1, ox2, ox3, fi1, fi2) in the reference's
+        order."""
+        locs = np.ascontiguousarray(self.locs, dtype=np.int64)
+        out = np.zeros((56, 7), dtype=np.int32)
+        n = lib().z4c_refined_neighbours(C.byref(self.desc()), len(locs),
+                                         locs.ctypes.data_as(C.POINTER(C.c_longlong)), int(block),
+                                         out.ctypes.data_as(C.POINTER(C.c_int)))
+        _check(min(n, 0))
+        return out[:n]
+
     def new_dt(self, cfl):
         """Time step of the mesh: NewBlockTimeStep on every block, minimum
         over blocks (cfl times the smallest cell width)."""
+        if self.locs is not None:
+            return min(min(self.block_coords(b)[1]) * float(cfl) for b in range(self.nblocks))
         dt = C.c_double()
         _check(lib().z4c_mesh_new_dt(C.byref(self.desc()), float(cfl), C.byref(dt)))
         return dt.value
@@ -375,6 +413,89 @@ def restart_write(path, par_text, mesh, u, time, dt, ncycle, trackers=()):
         t.ctypes.data_as(C.POINTER(C.c_double)) if len(t) else None))
 
 
+def _mesh_gen_x(index, nrange, x0, x1):
+    """ComputeMeshGeneratorX (symmetric interval) and UniformMeshGeneratorX1,
+    mesh/mesh.hpp:839-945."""
+    rx = float(2 * index - nrange) / float(2 * nrange)
+    return 0.5 * (x0 + x1) + (rx * x1 - rx * x0)
+
+
+def _smr_blocks(mesh, regions):
+    """Leaves of the statically refined block tree in gid order."""
+    r0 = mesh.root_level
+    leaves = {(r0, i, j, k) for k in range(mesh.nb[2]) for j in range(mesh.nb[1])
+              for i in range(mesh.nb[0])}
+    periodic = [mesh.bc[2 * a] == BC_NAMES["periodic"] for a in range(3)]
+
+    def refine(node):  # MeshBlockTree::Refine: children, then the 26 neighbours' level
+        lev, l = node[0], node[1:]
+        leaves.discard(node)
+        for c in range(8):
+            leaves.add((lev + 1, 2 * l[0] + (c & 1), 2 * l[1] + ((c >> 1) & 1),
+                        2 * l[2] + ((c >> 2) & 1)))
+        n = [mesh.nb[a] << (lev - r0) for a in range(3)]
+        for oz in (-1, 0, 1):
+            for oy in (-1, 0, 1):
+                for ox in (-1, 0, 1):
+                    if ox == oy == oz == 0:
+                        continue
+                    nl = [l[0] + ox, l[1] + oy, l[2] + oz]
+                    ok = True
+                    for a in range(3):
+                        if nl[a] < 0 or nl[a] >= n[a]:
+                            if not periodic[a]:
+                                ok = False
+                            nl[a] %= n[a]
+                    if ok:
+                        add_block((lev, *nl))
+
+    def add_block(loc):  # MeshBlockTree::AddMeshBlock from the root
+        lev = loc[0]
+        for lv in range(r0, lev):
+            anc = (lv, *[x >> (lev - lv) for x in loc[1:]])
+            if anc in leaves:
+                refine(anc)
+
+    for reg in regions:
+        level = int(reg["level"])
+        if level < 1:
+            raise ValueError("refinement level must be larger than 0")
+        lo, hi = [], []
+        for a in range(3):
+            lxmax = mesh.nb[a] << level
+            rmin, rmax = float(reg[f"x{a + 1}min"]), float(reg[f"x{a + 1}max"])
+            if rmin > rmax or rmin < mesh.xmin[a] or rmax > mesh.xmax[a]:
+                raise ValueError("invalid refinement region")
+            l0 = 0
+            while l0 < lxmax and not _mesh_gen_x(l0 + 1, lxmax, mesh.xmin[a], mesh.xmax[a]) > rmin:
+                l0 += 1
+            l1 = l0
+            while l1 < lxmax and not _mesh_gen_x(l1 + 1, lxmax, mesh.xmin[a], mesh.xmax[a]) >= rmax:
+                l1 += 1
+            if l0 % 2 == 1:
+                l0 -= 1
+            if l1 % 2 == 0:
+                l1 += 1
+            lo.append(l0)
+            hi.append(l1)
+        for k in range(lo[2], hi[2], 2):
+            for j in range(lo[1], hi[1], 2):
+                for i in range(lo[0], hi[0], 2):
+                    add_block((r0 + level, i, j, k))
+    maxlev = max(b[0] for b in leaves)
+
+    def morton(b):
+        sh = maxlev - b[0]
+        x, y, z = (v << sh for v in b[1:])
+        key = 0
+        for bit in range(maxlev + 1):
+            key |= (((x >> bit) & 1) << (3 * bit)) | (((y >> bit) & 1) << (3 * bit + 1)) \
+                | (((z >> bit) & 1) << (3 * bit + 2))
+        return key
+
+    return np.array(sorted(leaves, key=morton), dtype=np.int64)
+
+
 class Z4c:
     """A device context holding every MeshBlock of a mesh."""
 
@@ -383,8 +504,14 @@ class Z4c:
         self.params = params if params is not None else default_params()
         self.integrator = integrator
         h = C.c_void_p()
-        _check(lib().z4c_create(C.byref(mesh.desc()), C.byref(self.params),
-                                INTEG[integrator], C.byref(h)))
+        if mesh.locs is None:
+            _check(lib().z4c_create(C.byref(mesh.desc()), C.byref(self.params),
+                                    INTEG[integrator], C.byref(h)))
+        else:
+            locs = np.ascontiguousarray(mesh.locs, dtype=np.int64)
+            _check(lib().z4c_create_refined(
+                C.byref(mesh.desc()), len(locs), locs.ctypes.data_as(C.POINTER(C.c_longlong)),
+                C.byref(self.params), INTEG[integrator], C.byref(h)))
         self._h = h
         self.nblocks = mesh.nblocks
         self.nn = mesh.nn

@@ -140,6 +140,29 @@ const char *z4c_last_error(void);
  * z4c.cpp:30-217, for all blocks at once). */
 int z4c_create(const z4c_mesh_desc_t *mesh, const z4c_params_t *params,
                int integrator, z4c_ctx **out);
+/* A context on a statically refined mesh (<refinementN> blocks of the
+ * input deck): mesh->nb root blocks per axis of mesh->nx cells, and nblocks
+ * MeshBlocks given in gid order by their logical locations
+ * locs[b] = {level, lx1, lx2, lx3} (absolute levels, LogicalLocation of
+ * mesh/mesh.hpp; the root grid sits at the level ceil(log2(max nb))).  The
+ * blocks must tile the root grid with neighbouring levels differing by at
+ * most one (MeshBlockTree, mesh/meshblock_tree.cpp:108-260).  Ghost fills
+ * run the reference's multilevel vertex-centred exchange
+ * (comm/comm_registry.cpp:246-382, 533-570; comm/refinement_ops.cpp:24-195;
+ * comm/node_multiplicity.cpp; comm/physical_bcs.cpp:506-890).  Outflow and
+ * periodic faces; puncture trackers, psi4 spheres and restart files need a
+ * uniform mesh. */
+int z4c_create_refined(const z4c_mesh_desc_t *mesh, int nblocks, const long long *locs,
+                       const z4c_params_t *params, int integrator, z4c_ctx **out);
+/* The neighbour list z4c_create_refined builds for one block of a refined
+ * mesh (MeshBlock::SearchAndSetNeighbors, mesh/mesh_topology.cpp:278-960),
+ * host only: rows {gid, level, ox1, ox2, ox3, fi1, fi2} into out (room for
+ * 56 rows); returns the row count, or a negative error code when the blocks
+ * do not form a balanced tiling of the root grid.  block = -2 builds and
+ * checks the whole exchange plan instead (no device memory) and writes its
+ * sizes {pack boxes, unpack ops, prolongation boxes, boundary faces}. */
+int z4c_refined_neighbours(const z4c_mesh_desc_t *mesh, int nblocks, const long long *locs,
+                           int block, int *out);
 int z4c_destroy(z4c_ctx *ctx);
 /* Work is enqueued on this CUDA stream (a cudaStream_t; NULL = default). */
 int z4c_set_stream(z4c_ctx *ctx, void *stream);
@@ -161,6 +184,11 @@ int z4c_mesh_block_coords(const z4c_mesh_desc_t *mesh, int block, int axis, doub
 /* Z4c::NewBlockTimeStep (z4c/new_blockdt_z4c.cpp:24-70) over every block and
  * the minimum over blocks of Mesh::NewTimeStep (mesh/mesh.cpp:1753-1803):
  * cfl times the smallest cell width (host only, no context needed). */
+/* Vertex coordinates (nx + 1 + 2 NG) and spacing of the block at logical
+ * location loc = {level, lx1, lx2, lx3} along one axis
+ * (coordinates/coordinates.cpp:125-198, mesh/mesh.cpp:2526-2560). */
+int z4c_mesh_loc_coords(const z4c_mesh_desc_t *mesh, const long long loc[4], int axis,
+                        double *x_out, double *dx_out);
 int z4c_mesh_new_dt(const z4c_mesh_desc_t *mesh, double cfl, double *dt_out);
 
 /* Host <-> device copies of a register; block = -1 for the whole mesh.  The

@@ -17,8 +17,10 @@
 //   adm0               Z4cToADM(u0)
 //   con0               ADMConstraints(con, adm0, mat, u0)
 //   uadm0              ADMToZ4c(adm0) into a zeroed register
-//   gx_pre / gx_post   a block-dependent perturbation of u0 before and after
-//                      one ghost exchange + physical boundary conditions
+//   gx_pre / gx_post   a block-dependent perturbation of u0 (with <driver>
+//                      gx_hash = true: integer-hash values instead) before and
+//                      after one ghost exchange + physical boundary conditions
+//                      (+ prolongation on a multilevel mesh)
 //   rf_*               with <driver> refine_ops_only = true, only the
 //                      vertex-centred refinement operators of one block of a
 //                      multilevel mesh (see RefinementOperators) and the
@@ -168,6 +170,16 @@ void ExchangeAndBC(const std::vector<MeshBlock*>& blocks, Real t, Real dt) {
     if (all) break;
   }
   for (auto* b : blocks) b->pcomm->SetBoundaries(comm::CommGroup::Z4c);
+  // PROLONG on a multilevel mesh (GR_Z4c::Prolongation): coarse-level
+  // physical BCs, then prolongation into the ghosts next to coarser blocks
+  if (!blocks.empty() && blocks[0]->pmy_mesh->multilevel) {
+    for (auto* b : blocks) {
+      const Z4c* z = b->pz4c;
+      b->pcomm->ProlongateAndApplyPhysicalBCs(comm::CommGroup::Z4c, t, dt, z->mbi.cil,
+                                              z->mbi.ciu, z->mbi.cjl, z->mbi.cju,
+                                              z->mbi.ckl, z->mbi.cku, z->mbi.cng);
+    }
+  }
   for (auto* b : blocks) b->pcomm->ApplyPhysicalBCs(comm::CommGroup::Z4c, t, dt);
   for (auto* b : blocks)
     b->pcomm->ClearBoundary(comm::CommGroup::Z4c, comm::CommTarget::All, true);
@@ -381,6 +393,9 @@ int main(int argc, char* argv[]) {
 
   // --- ghost exchange on data whose shared vertices disagree ----------
   std::vector<AthenaArray<Real>> keep(blocks.size());
+  // <driver> gx_hash: the state is replaced by integer-hash values that any
+  // IEEE implementation reproduces exactly (so a fixture need not store it)
+  const bool gx_hash = pin->GetOrAddBoolean("driver", "gx_hash", false);
   for (size_t g = 0; g < blocks.size(); ++g) {
     Z4c* z = blocks[g]->pz4c;
     Copy(keep[g], z->storage.u);
@@ -389,7 +404,9 @@ int main(int argc, char* argv[]) {
       for (int k = 0; k < d.nn3; ++k)
         for (int j = 0; j < d.nn2; ++j)
           for (int i = 0; i < d.nn1; ++i)
-            u(n, k, j, i) += 1e-3 * (g + 1) * (1 + n) * std::sin(0.3 * i + 0.7 * j + 1.1 * k);
+            u(n, k, j, i) = gx_hash
+                ? static_cast<Real>((g * 131 + n * 31 + k * 7 + j * 3 + i) % 1009) / 1009.0 - 0.5
+                : u(n, k, j, i) + 1e-3 * (g + 1) * (1 + n) * std::sin(0.3 * i + 0.7 * j + 1.1 * k);
   }
   d.dump("gx_pre", NZ, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.u; });
   ExchangeAndBC(blocks, pm->time, 0.0);

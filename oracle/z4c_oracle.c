@@ -13,6 +13,7 @@
 #include "z4c_oracle.h"
 
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -1975,4 +1976,524 @@ void orc_hst_accumulate(const orc_block_t *b, const z4c_params_t *opt,
         out[6] += vol * (th * th);
         out[7] += vol * fabs(V(con, Z4C_CON_C)[p]);
       }
+}
+
+/* ---- multilevel (static mesh refinement) ghost exchange ------------------
+ *
+ * The vertex-centred exchange of a mesh whose MeshBlocks sit on several
+ * refinement levels, restated step by step as the reference runs it for one
+ * ghost fill of the Z4c state (task order of task_list/gr/
+ * task_list_gr_z4c.cpp:52-64: SEND, RECV, SETB, PROLONG, PHY_BVAL):
+ *   1. every block restricts its interior into its coarse buffer
+ *      (CommRegistry::SendBoundaryBuffers, comm_registry.cpp:246-296, and
+ *      RestrictInterior, refinement_ops.cpp:167-195: injection);
+ *   2. every block packs one message per neighbour from that pre-exchange
+ *      state (CommChannel::PackAndSend, comm_channel.cpp:733-787);
+ *   3. every block zeroes its fine and coarse ghosts, unpacks the messages in
+ *      neighbour order (same level: added into the fine array and, for the
+ *      coarse payload, into the coarse buffer; from a coarser block: copied
+ *      into the coarse buffer; from a finer block: added into the fine array;
+ *      comm_channel.cpp:1278-1474) and multiplies by the inverse node
+ *      multiplicity (node_multiplicity.cpp:102-430);
+ *   4. coarse-level physical BCs and prolongation into the ghosts next to
+ *      coarser blocks (CommRegistry::ProlongateAndApplyPhysicalBCs,
+ *      comm_registry.cpp:533-570; physical_bcs.cpp:687-890;
+ *      refinement_ops.cpp:24-160);
+ *   5. fine-level physical BCs (physical_bcs.cpp:506-670).
+ * The neighbour list follows mesh_topology.cpp:278-960, the index ranges
+ * comm/index_utilities.{hpp,cpp}. */
+
+typedef struct {
+  int gid, level, ox[3], fi[2];
+} ml_nb_t;
+
+typedef struct {
+  const orc_ml_mesh_t *m;
+  int nn[3], cn[3];
+  int64_t fvol, cvol;
+} ml_geo_t;
+
+static int ml_leaf(const orc_ml_mesh_t *m, int level, const int64_t l[3]) {
+  for (int b = 0; b < m->nblocks; ++b)
+    if (m->loc[4 * b] == level && m->loc[4 * b + 1] == l[0] && m->loc[4 * b + 2] == l[1] &&
+        m->loc[4 * b + 3] == l[2])
+      return b;
+  return -1;
+}
+
+/* MeshBlockTree::FindNeighbor (meshblock_tree.cpp:400-490): 0 = beyond a
+ * non-periodic face, 1 = a leaf of the same or the next coarser level
+ * (*gid), 2 = a refined node whose children are leaves (nl its location). */
+static int ml_find(const orc_ml_mesh_t *m, int level, const int64_t *loc, const int o[3],
+                   int64_t nl[3], int *gid) {
+  for (int a = 0; a < 3; ++a) {
+    const int64_t n = (int64_t)m->nroot[a] << (level - m->root_level);
+    nl[a] = loc[a] + o[a];
+    if (nl[a] < 0) {
+      if (m->bc[2 * a] != Z4C_BC_PERIODIC) return 0;
+      nl[a] = n - 1;
+    }
+    if (nl[a] >= n) {
+      if (m->bc[2 * a + 1] != Z4C_BC_PERIODIC) return 0;
+      nl[a] = 0;
+    }
+  }
+  int b = ml_leaf(m, level, nl);
+  if (b >= 0) { *gid = b; return 1; }
+  const int64_t pl[3] = {nl[0] >> 1, nl[1] >> 1, nl[2] >> 1};
+  b = ml_leaf(m, level - 1, pl);
+  if (b >= 0) { *gid = b; return 1; }
+  return 2;
+}
+
+static int ml_child(const orc_ml_mesh_t *m, int level, const int64_t nl[3], const int c[3]) {
+  const int64_t l[3] = {2 * nl[0] + c[0], 2 * nl[1] + c[1], 2 * nl[2] + c[2]};
+  return ml_leaf(m, level + 1, l);
+}
+
+/* MeshBlock::SearchAndSetNeighbors (mesh_topology.cpp:278-960), 3-D. */
+static int ml_neighbours(const orc_ml_mesh_t *m, int b, ml_nb_t *out) {
+  const int lev = m->loc[4 * b];
+  const int64_t *loc = &m->loc[4 * b + 1];
+  int myox[3];
+  for (int a = 0; a < 3; ++a) myox[a] = (loc[a] & 1) ? 1 : -1;
+  int cnt = 0, gid;
+  int64_t nl[3];
+  /* faces: x1, x2, x3, each -1 then +1; finer neighbours as 4 leaves with
+   * the two transverse child indices (f1 the lower axis) */
+  for (int ax = 0; ax < 3; ++ax)
+    for (int s = -1; s <= 1; s += 2) {
+      int o[3] = {0, 0, 0};
+      o[ax] = s;
+      const int r = ml_find(m, lev, loc, o, nl, &gid);
+      if (r == 0) continue;
+      if (r == 2) {
+        const int t1 = ax == 0 ? 1 : 0, t2 = ax == 2 ? 1 : 2;
+        for (int f2 = 0; f2 < 2; ++f2)
+          for (int f1 = 0; f1 < 2; ++f1) {
+            int c[3];
+            c[ax] = 1 - (s + 1) / 2;
+            c[t1] = f1;
+            c[t2] = f2;
+            ml_nb_t e = {ml_child(m, lev, nl, c), lev + 1, {o[0], o[1], o[2]}, {f1, f2}};
+            out[cnt++] = e;
+          }
+      } else {
+        ml_nb_t e = {gid, m->loc[4 * gid], {o[0], o[1], o[2]}, {0, 0}};
+        out[cnt++] = e;
+      }
+    }
+  /* edges x1x2, x1x3, x2x3: the second axis' offset outer, the first's inner */
+  static const int pairs[3][3] = {{0, 1, 2}, {0, 2, 1}, {1, 2, 0}};
+  for (int q = 0; q < 3; ++q) {
+    const int a0 = pairs[q][0], a1 = pairs[q][1], a2 = pairs[q][2];
+    for (int mm = -1; mm <= 1; mm += 2)
+      for (int n = -1; n <= 1; n += 2) {
+        int o[3] = {0, 0, 0};
+        o[a0] = n;
+        o[a1] = mm;
+        const int r = ml_find(m, lev, loc, o, nl, &gid);
+        if (r == 0) continue;
+        if (r == 2) {
+          for (int f1 = 0; f1 < 2; ++f1) {
+            int c[3];
+            c[a0] = 1 - (n + 1) / 2;
+            c[a1] = 1 - (mm + 1) / 2;
+            c[a2] = f1;
+            ml_nb_t e = {ml_child(m, lev, nl, c), lev + 1, {o[0], o[1], o[2]}, {f1, 0}};
+            out[cnt++] = e;
+          }
+        } else {
+          const int nlev = m->loc[4 * gid];
+          if (nlev >= lev || (myox[a0] == n && myox[a1] == mm)) {
+            ml_nb_t e = {gid, nlev, {o[0], o[1], o[2]}, {0, 0}};
+            out[cnt++] = e;
+          }
+        }
+      }
+  }
+  /* corners */
+  for (int l = -1; l <= 1; l += 2)
+    for (int mm = -1; mm <= 1; mm += 2)
+      for (int n = -1; n <= 1; n += 2) {
+        const int o[3] = {n, mm, l};
+        const int r = ml_find(m, lev, loc, o, nl, &gid);
+        if (r == 0) continue;
+        int nlev;
+        if (r == 2) {
+          const int c[3] = {1 - (n + 1) / 2, 1 - (mm + 1) / 2, 1 - (l + 1) / 2};
+          gid = ml_child(m, lev, nl, c);
+          nlev = lev + 1;
+        } else {
+          nlev = m->loc[4 * gid];
+        }
+        if (nlev >= lev || (myox[0] == n && myox[1] == mm && myox[2] == l)) {
+          ml_nb_t e = {gid, nlev, {n, mm, l}, {0, 0}};
+          out[cnt++] = e;
+        }
+      }
+  return cnt;
+}
+
+int orc_ml_neighbours(const orc_ml_mesh_t *m, int b, int *out) {
+  ml_nb_t nb[56];
+  const int cnt = ml_neighbours(m, b, nb);
+  for (int q = 0; q < cnt; ++q) {
+    int *r = out + 7 * q;
+    r[0] = nb[q].gid; r[1] = nb[q].level;
+    r[2] = nb[q].ox[0]; r[3] = nb[q].ox[1]; r[4] = nb[q].ox[2];
+    r[5] = nb[q].fi[0]; r[6] = nb[q].fi[1];
+  }
+  return cnt;
+}
+
+/* Index ranges of one axis (index_utilities.hpp:124-216) on the fine array
+ * (vs = NG, ve = NG + nx, ms = 0, pe = nx + 2 NG) or the coarse buffer
+ * (vs = NCG, ve = NCG + nx/2, ...).  fi < 0: the axis is not narrowed. */
+typedef struct { int vs, ve, ms, me, ps, pe, gs, ge, ng; } ml_ax_t;
+static ml_ax_t ml_axis(int nx, int ng) {
+  ml_ax_t a;
+  a.ng = ng; a.vs = ng; a.ve = ng + nx; a.ms = 0; a.me = ng - 1;
+  a.ps = nx + ng + 1; a.pe = nx + 2 * ng; a.gs = a.vs + ng; a.ge = a.ve - ng;
+  return a;
+}
+/* LoadRangeVC */
+static void r_load_same(int ox, ml_ax_t a, int *s, int *e) {
+  *s = ox > 0 ? a.ge : a.vs;
+  *e = ox < 0 ? a.gs : a.ve;
+}
+/* SetRangeVC */
+static void r_set_same(int ox, ml_ax_t a, int *s, int *e) {
+  if (ox == 0) { *s = a.vs; *e = a.ve; }
+  else if (ox > 0) { *s = a.ve; *e = a.pe; }
+  else { *s = a.ms; *e = a.vs; }
+}
+/* SetFromCoarserRangeVC (coarse axis) */
+static void r_set_from_coarser(int ox, ml_ax_t c, int64_t lx, int *s, int *e) {
+  if (ox == 0) {
+    *s = c.vs; *e = c.ve;
+    if ((lx & 1) == 0) *e = c.pe;
+    else *s = c.ms;
+  } else if (ox > 0) { *s = c.ps; *e = c.pe; }
+  else { *s = c.ms; *e = c.me; }
+}
+/* LoadToCoarserRangeVC (coarse axis, fine ghost width ng) */
+static void r_load_to_coarser(int ox, ml_ax_t c, int ng, int *s, int *e) {
+  if (ox > 0) { *s = c.ve - ng; *e = c.ve; }
+  else if (ox < 0) { *s = c.vs; *e = c.vs + ng; }
+  else { *s = c.vs; *e = c.ve; }
+}
+/* LoadToFinerRangeVC (fine axis, slab width cng, half size hs) */
+static void r_load_to_finer(int ox, ml_ax_t a, int cng, int fi, int hs, int *s, int *e) {
+  if (ox > 0) { *s = a.ve - cng; *e = a.ve - 1; }
+  else if (ox < 0) { *s = a.vs + 1; *e = a.vs + cng; }
+  else {
+    *s = a.vs; *e = a.ve;
+    if (fi == 1) *s += hs;
+    else *e -= hs;
+  }
+}
+/* SetFromFinerRangeVC (fine axis, half size hs) */
+static void r_set_from_finer(int ox, ml_ax_t a, int fi, int hs, int *s, int *e) {
+  if (ox == 0) {
+    *s = a.vs; *e = a.ve;
+    if (fi == 1) *s += hs;
+    else *e -= hs;
+  } else if (ox > 0) { *s = a.ve; *e = a.pe; }
+  else { *s = a.ms; *e = a.vs; }
+}
+/* which of fi1/fi2 narrows axis a (index_utilities.cpp:830-873) */
+static int ml_fi(const ml_nb_t *e, int a) {
+  if (a == 0) return e->fi[0];
+  if (a == 1) return e->ox[0] != 0 ? e->fi[0] : e->fi[1];
+  return (e->ox[0] != 0 && e->ox[1] != 0) ? e->fi[0] : e->fi[1];
+}
+
+static int64_t box_count(const int bx[6]) {
+  return (int64_t)(bx[1] - bx[0] + 1) * (bx[3] - bx[2] + 1) * (bx[5] - bx[4] + 1);
+}
+/* BufferUtility::PackData / UnpackData(Add) over n, k, j, i */
+static void box_pack(const double *a, const int dims[3], int nvar, const int bx[6], double *buf,
+                     int64_t *p) {
+  const int64_t vol = (int64_t)dims[0] * dims[1] * dims[2];
+  for (int n = 0; n < nvar; ++n)
+    for (int k = bx[4]; k <= bx[5]; ++k)
+      for (int j = bx[2]; j <= bx[3]; ++j)
+        for (int i = bx[0]; i <= bx[1]; ++i)
+          buf[(*p)++] = a[n * vol + ((int64_t)k * dims[1] + j) * dims[0] + i];
+}
+static void box_unpack(double *a, const int dims[3], int nvar, const int bx[6], const double *buf,
+                       int64_t *p, int add) {
+  const int64_t vol = (int64_t)dims[0] * dims[1] * dims[2];
+  for (int n = 0; n < nvar; ++n)
+    for (int k = bx[4]; k <= bx[5]; ++k)
+      for (int j = bx[2]; j <= bx[3]; ++j)
+        for (int i = bx[0]; i <= bx[1]; ++i) {
+          double *d = &a[n * vol + ((int64_t)k * dims[1] + j) * dims[0] + i];
+          if (add) *d += buf[(*p)++];
+          else *d = buf[(*p)++];
+        }
+}
+
+/* ExtrapolateOutflowBC with NEXTRAPOLATE = 5 on the faces need[] of one
+ * array, is/ie the interior ends the caller passes and ng the ghost width;
+ * transverse limits as ApplyPhysicalBCs / ApplyPhysicalBCsOnCoarseLevel. */
+static void ml_bcs(const int need[6], const int is[3], const int ie[3], int ng, const int dims[3],
+                   int nvar, double *u) {
+  const int64_t vol = (int64_t)dims[0] * dims[1] * dims[2];
+  const int64_t st[3] = {1, dims[0], (int64_t)dims[0] * dims[1]};
+  int bis = is[0] - ng, bie = ie[0] + ng;
+  int bjs = need[2] ? is[1] : is[1] - ng, bje = need[3] ? ie[1] : ie[1] + ng;
+  int bks = need[4] ? is[2] : is[2] - ng, bke = need[5] ? ie[2] : ie[2] + ng;
+  for (int face = 0; face < 6; ++face) {
+    if (!need[face]) continue;
+    const int ax = face / 2, outer = face % 2;
+    int lo[3], hi[3];
+    if (ax == 0) { lo[1] = bjs; hi[1] = bje; lo[2] = bks; hi[2] = bke; }
+    else if (ax == 1) { lo[0] = bis; hi[0] = bie; lo[2] = bks; hi[2] = bke; }
+    else { lo[0] = bis; hi[0] = bie; lo[1] = is[1] - ng; hi[1] = ie[1] + ng; }
+    const int o1 = (ax + 1) % 3, o2 = (ax + 2) % 3;
+    for (int n = 0; n < nvar; ++n)
+      for (int t2 = lo[o2]; t2 <= hi[o2]; ++t2)
+        for (int t1 = lo[o1]; t1 <= hi[o1]; ++t1)
+          for (int g = 1; g <= ng; ++g) {
+            const int ia = outer ? ie[ax] + g : is[ax] - g;
+            const int dir = outer ? -1 : 1;
+            const int64_t p = (int64_t)ia * st[ax] + (int64_t)t1 * st[o1] + (int64_t)t2 * st[o2];
+            double v = 0.0;
+            for (int q = 0; q < 5; ++q) v += CE[q] * u[n * vol + p + dir * (q + 1) * st[ax]];
+            u[n * vol + p] = v;
+          }
+  }
+}
+
+/* ZeroGhosts / ZeroGhostsCoarse: everything outside [vs, ve]^3 */
+static void ml_zero_ghosts(double *a, const int dims[3], int nvar, ml_ax_t x, ml_ax_t y,
+                           ml_ax_t z) {
+  const int64_t vol = (int64_t)dims[0] * dims[1] * dims[2];
+  for (int n = 0; n < nvar; ++n)
+    for (int k = 0; k < dims[2]; ++k)
+      for (int j = 0; j < dims[1]; ++j)
+        for (int i = 0; i < dims[0]; ++i)
+          if (i < x.vs || i > x.ve || j < y.vs || j > y.ve || k < z.vs || k > z.ve)
+            a[n * vol + ((int64_t)k * dims[1] + j) * dims[0] + i] = 0.0;
+}
+
+/* ApplyDivisionImpl (node_multiplicity.cpp:364-430): compact zone c of an
+ * axis -> physical range */
+static void ml_phys(int c, ml_ax_t a, int *lo, int *hi) {
+  const int half = (a.ve - a.vs) / 2;
+  const int t[7] = {a.ms, a.vs, a.vs + 1, a.vs + half, a.ve - 1, a.ve, a.pe};
+  if (c & 1) { *lo = *hi = t[c]; }
+  else if (c <= 3) { *lo = t[c]; *hi = t[c + 1] - 1; }
+  else { *lo = t[c - 1] + 1; *hi = t[c]; }
+}
+
+/* NodeMultiplicity::Precompute (node_multiplicity.cpp:102-180) */
+static void ml_multiplicity(const orc_ml_mesh_t *m, int b, const ml_nb_t *nb, int cnt,
+                            unsigned short mult[7][7][7]) {
+  const int lev = m->loc[4 * b];
+  memset(mult, 0, sizeof(unsigned short) * 343);
+  for (int k = 1; k <= 5; ++k)
+    for (int j = 1; j <= 5; ++j)
+      for (int i = 1; i <= 5; ++i) mult[k][j][i] = 1;
+  for (int q = 0; q < cnt; ++q) {
+    int s[3], e[3];
+    for (int a = 0; a < 3; ++a) {
+      const int ox = nb[q].ox[a];
+      if (nb[q].level == lev) {
+        if (ox == 0) { s[a] = 1; e[a] = 5; }
+        else if (ox > 0) { s[a] = 5; e[a] = 6; }
+        else { s[a] = 0; e[a] = 1; }
+      } else if (nb[q].level < lev) {
+        if (ox == 0) {
+          s[a] = 1; e[a] = 5;
+          if ((m->loc[4 * b + 1 + a] & 1) == 0) e[a] = 6;
+          else s[a] = 0;
+        } else if (ox > 0) { s[a] = e[a] = 6; }
+        else { s[a] = e[a] = 0; }
+      } else {
+        if (ox == 0) {
+          s[a] = 1; e[a] = 5;
+          if (ml_fi(&nb[q], a) == 1) s[a] += 2;
+          else e[a] -= 2;
+        } else if (ox > 0) { s[a] = 5; e[a] = 6; }
+        else { s[a] = 0; e[a] = 1; }
+      }
+    }
+    for (int k = s[2]; k <= e[2]; ++k)
+      for (int j = s[1]; j <= e[1]; ++j)
+        for (int i = s[0]; i <= e[0]; ++i) mult[k][j][i] += 1;
+  }
+}
+
+static void ml_divide(double *a, const int dims[3], int nvar, ml_ax_t x, ml_ax_t y, ml_ax_t z,
+                      unsigned short mult[7][7][7]) {
+  const int64_t vol = (int64_t)dims[0] * dims[1] * dims[2];
+  for (int K = 0; K < 7; ++K) {
+    int kl, ku;
+    ml_phys(K, z, &kl, &ku);
+    for (int J = 0; J < 7; ++J) {
+      int jl, ju;
+      ml_phys(J, y, &jl, &ju);
+      for (int I = 0; I < 7; ++I) {
+        const unsigned short mm = mult[K][J][I];
+        if (mm <= 1) continue;
+        int il, iu;
+        ml_phys(I, x, &il, &iu);
+        const double inv = 1.0 / (double)mm;
+        for (int n = 0; n < nvar; ++n)
+          for (int k = kl; k <= ku; ++k)
+            for (int j = jl; j <= ju; ++j)
+              for (int i = il; i <= iu; ++i) a[n * vol + ((int64_t)k * dims[1] + j) * dims[0] + i] *= inv;
+      }
+    }
+  }
+}
+
+/* the faces of block b on a non-periodic mesh boundary */
+static void ml_need(const orc_ml_mesh_t *m, int b, int need[6]) {
+  const int lev = m->loc[4 * b];
+  for (int a = 0; a < 3; ++a) {
+    const int64_t n = (int64_t)m->nroot[a] << (lev - m->root_level);
+    const int64_t l = m->loc[4 * b + 1 + a];
+    need[2 * a] = m->bc[2 * a] != Z4C_BC_PERIODIC && l == 0;
+    need[2 * a + 1] = m->bc[2 * a + 1] != Z4C_BC_PERIODIC && l == n - 1;
+  }
+}
+
+void orc_ml_exchange(const orc_ml_mesh_t *m, int nvar, double *u_all) {
+  const int nb = m->nblocks;
+  int nn[3], cn[3];
+  ml_ax_t F[3], C[3];
+  for (int a = 0; a < 3; ++a) {
+    nn[a] = m->nx[a] + 1 + 2 * NG;
+    cn[a] = m->nx[a] / 2 + 1 + 2 * ORC_NCG;
+    F[a] = ml_axis(m->nx[a], NG);
+    C[a] = ml_axis(m->nx[a] / 2, ORC_NCG);
+  }
+  const int64_t fvol = (int64_t)nn[0] * nn[1] * nn[2], cvol = (int64_t)cn[0] * cn[1] * cn[2];
+  double *coarse = (double *)calloc((size_t)nb * nvar * cvol, sizeof(double));
+  ml_nb_t(*nbs)[56] = (ml_nb_t(*)[56])malloc(sizeof(ml_nb_t) * 56 * nb);
+  int *cnt = (int *)malloc(sizeof(int) * nb);
+  for (int b = 0; b < nb; ++b) cnt[b] = ml_neighbours(m, b, nbs[b]);
+  /* 1. restriction of every interior */
+  for (int b = 0; b < nb; ++b) {
+    const int box[6] = {C[0].vs, C[0].ve, C[1].vs, C[1].ve, C[2].vs, C[2].ve};
+    orc_vc_restrict(m->nx, nvar, u_all + b * nvar * fvol, coarse + b * nvar * cvol, box);
+  }
+  /* 2. one message per (receiver, neighbour entry), packed by the sender
+   * from the entry that points back at the receiver */
+  double **msg = (double **)calloc((size_t)nb * 56, sizeof(double *));
+  for (int r = 0; r < nb; ++r)
+    for (int q = 0; q < cnt[r]; ++q) {
+      const int s = nbs[r][q].gid;
+      const ml_nb_t *e = NULL;
+      for (int t = 0; t < cnt[s]; ++t) {
+        const ml_nb_t *c = &nbs[s][t];
+        if (c->gid == r && c->ox[0] == -nbs[r][q].ox[0] && c->ox[1] == -nbs[r][q].ox[1] &&
+            c->ox[2] == -nbs[r][q].ox[2]) { e = c; break; }
+      }
+      if (!e) { fprintf(stderr, "orc_ml_exchange: no matching neighbour entry\n"); abort(); }
+      const int slev = m->loc[4 * s];
+      int fb[6], cb[6];
+      int64_t size = 0;
+      if (e->level == slev) {
+        for (int a = 0; a < 3; ++a) {
+          r_load_same(e->ox[a], F[a], &fb[2 * a], &fb[2 * a + 1]);
+          r_load_same(e->ox[a], C[a], &cb[2 * a], &cb[2 * a + 1]);
+        }
+        size = (box_count(fb) + box_count(cb)) * nvar;
+      } else if (e->level < slev) {
+        for (int a = 0; a < 3; ++a) r_load_to_coarser(e->ox[a], C[a], NG, &cb[2 * a], &cb[2 * a + 1]);
+        size = box_count(cb) * nvar;
+      } else {
+        for (int a = 0; a < 3; ++a)
+          r_load_to_finer(e->ox[a], F[a], ORC_NCG, ml_fi(e, a), m->nx[a] / 2 - ORC_NCG,
+                          &fb[2 * a], &fb[2 * a + 1]);
+        size = box_count(fb) * nvar;
+      }
+      double *buf = (double *)malloc(sizeof(double) * (size_t)size);
+      int64_t p = 0;
+      if (e->level == slev) {
+        box_pack(u_all + s * nvar * fvol, nn, nvar, fb, buf, &p);
+        box_pack(coarse + s * nvar * cvol, cn, nvar, cb, buf, &p);
+      } else if (e->level < slev) {
+        box_pack(coarse + s * nvar * cvol, cn, nvar, cb, buf, &p);
+      } else {
+        box_pack(u_all + s * nvar * fvol, nn, nvar, fb, buf, &p);
+      }
+      msg[r * 56 + q] = buf;
+    }
+  /* 3. unpack and multiplicity */
+  for (int r = 0; r < nb; ++r) {
+    double *u = u_all + r * nvar * fvol, *cu = coarse + r * nvar * cvol;
+    const int lev = m->loc[4 * r];
+    int same = 1;
+    for (int q = 0; q < cnt[r]; ++q) same = same && nbs[r][q].level == lev;
+    ml_zero_ghosts(u, nn, nvar, F[0], F[1], F[2]);
+    ml_zero_ghosts(cu, cn, nvar, C[0], C[1], C[2]);
+    for (int q = 0; q < cnt[r]; ++q) {
+      const ml_nb_t *e = &nbs[r][q];
+      const double *buf = msg[r * 56 + q];
+      int64_t p = 0;
+      int fb[6], cb[6];
+      if (e->level == lev) {
+        for (int a = 0; a < 3; ++a) {
+          r_set_same(e->ox[a], F[a], &fb[2 * a], &fb[2 * a + 1]);
+          r_set_same(e->ox[a], C[a], &cb[2 * a], &cb[2 * a + 1]);
+        }
+        box_unpack(u, nn, nvar, fb, buf, &p, 1);
+        if (!same) box_unpack(cu, cn, nvar, cb, buf, &p, 1);
+      } else if (e->level < lev) {
+        for (int a = 0; a < 3; ++a)
+          r_set_from_coarser(e->ox[a], C[a], m->loc[4 * r + 1 + a], &cb[2 * a], &cb[2 * a + 1]);
+        box_unpack(cu, cn, nvar, cb, buf, &p, 0);
+      } else {
+        for (int a = 0; a < 3; ++a)
+          r_set_from_finer(e->ox[a], F[a], ml_fi(e, a), m->nx[a] / 2, &fb[2 * a], &fb[2 * a + 1]);
+        box_unpack(u, nn, nvar, fb, buf, &p, 1);
+      }
+    }
+    unsigned short mult[7][7][7];
+    ml_multiplicity(m, r, nbs[r], cnt[r], mult);
+    ml_divide(u, nn, nvar, F[0], F[1], F[2], mult);
+    ml_divide(cu, cn, nvar, C[0], C[1], C[2], mult);
+  }
+  for (int q = 0; q < nb * 56; ++q) free(msg[q]);
+  free(msg);
+  /* 4. coarse-level BCs, prolongation from coarser neighbours; 5. fine BCs */
+  for (int b = 0; b < nb; ++b) {
+    double *u = u_all + b * nvar * fvol, *cu = coarse + b * nvar * cvol;
+    int need[6];
+    ml_need(m, b, need);
+    const int cis[3] = {C[0].vs, C[1].vs, C[2].vs}, cie[3] = {C[0].ve, C[1].ve, C[2].ve};
+    ml_bcs(need, cis, cie, ORC_NCG, cn, nvar, cu);
+    const int lev = m->loc[4 * b];
+    const int pcng = NG / 2 + (NG % 2 != 0);
+    for (int q = 0; q < cnt[b]; ++q) {
+      const ml_nb_t *e = &nbs[b][q];
+      if (e->level >= lev) continue;
+      int box[6];
+      for (int a = 0; a < 3; ++a) {
+        const int ox = e->ox[a];
+        int s, t;
+        if (ox > 0) { s = C[a].ve + 1; t = C[a].ve + pcng; }
+        else if (ox < 0) { s = C[a].vs - pcng; t = C[a].vs - 1; }
+        else {
+          s = C[a].vs; t = C[a].ve;
+          if ((m->loc[4 * b + 1 + a] & 1) == 0) t += pcng;
+          else s -= pcng;
+        }
+        box[2 * a] = s;
+        box[2 * a + 1] = t;
+      }
+      orc_vc_prolongate(m->nx, nvar, cu, u, box);
+    }
+    const int is[3] = {NG, NG, NG}, ie[3] = {NG + m->nx[0] - 1, NG + m->nx[1] - 1, NG + m->nx[2] - 1};
+    ml_bcs(need, is, ie, NG, nn, nvar, u);
+  }
+  free(coarse);
+  free(nbs);
+  free(cnt);
 }

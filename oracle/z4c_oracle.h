@@ -165,6 +165,27 @@ void orc_mesh_exchange(const orc_mesh_t *m, int nvar, double *u_all);
 void orc_block_physical_bcs(const orc_mesh_t *m, const int loc[3], int nvar,
                             double *u);
 
+/* A mesh of MeshBlocks on several refinement levels: nroot blocks per axis
+ * at the root level root_level, and per block (gid order) its logical
+ * location {level, lx1, lx2, lx3} (levels absolute, as LogicalLocation). */
+typedef struct orc_ml_mesh {
+  int nroot[3];
+  int root_level;
+  int nx[3];
+  int bc[6];
+  int nblocks;
+  const int64_t *loc;  /* [nblocks][4] */
+} orc_ml_mesh_t;
+/* The neighbour list of block b as SearchAndSetNeighbors builds it
+ * (mesh/mesh_topology.cpp:278-960): rows {gid, level, ox1, ox2, ox3, fi1,
+ * fi2}, at most 56; returns the count. */
+int orc_ml_neighbours(const orc_ml_mesh_t *m, int b, int *out);
+/* One vertex-centred ghost fill of a multilevel mesh: restriction, pack,
+ * additive unpack with node multiplicity, coarse-level BCs, prolongation
+ * from coarser neighbours, fine-level BCs (extrapolate_outflow or periodic
+ * faces). */
+void orc_ml_exchange(const orc_ml_mesh_t *m, int nvar, double *u_all);
+
 /* History-output sums (outputs/history.cpp:168-200) over the cell range of one
  * block: out[8] += {H^2, M, Mx^2, My^2, Mz^2, Z, Theta^2, C} * vol. */
 void orc_hst_accumulate(const orc_block_t *b, const z4c_params_t *p,

@@ -95,6 +95,8 @@ def lib():
         L.orc_wave_block.argtypes = [bp, dp, C.c_int, dp, C.c_double, C.c_int, C.c_int,
                                      C.POINTER(C.c_int), dp]
         L.orc_mesh_exchange.argtypes = [mp, C.c_int, dp]
+        L.orc_ml_exchange.argtypes = [C.POINTER(_MlMesh), C.c_int, dp]
+        L.orc_ml_neighbours.argtypes = [C.POINTER(_MlMesh), C.c_int, C.POINTER(C.c_int)]
         L.orc_hst_accumulate.argtypes = [bp, pp, dp, dp, dp]
         _lib = L
     return _lib
@@ -266,6 +268,42 @@ def mesh_exchange(nb, nx, bc, u_all):
     for f in range(6):
         m.bc[f] = int(bc[f])
     lib().orc_mesh_exchange(C.byref(m), int(out.shape[1]), _ptr(out))
+    return out
+
+
+class _MlMesh(C.Structure):
+    _fields_ = [("nroot", C.c_int * 3), ("root_level", C.c_int), ("nx", C.c_int * 3),
+                ("bc", C.c_int * 6), ("nblocks", C.c_int), ("loc", C.POINTER(C.c_int64))]
+
+
+def _ml_mesh(nroot, root_level, nx, bc, locs):
+    loc = np.ascontiguousarray(np.asarray(locs, dtype=np.int64).reshape(-1, 4))
+    m = _MlMesh()
+    for a in range(3):
+        m.nroot[a], m.nx[a] = int(nroot[a]), int(nx[a])
+    for f in range(6):
+        m.bc[f] = int(bc[f])
+    m.root_level, m.nblocks = int(root_level), len(loc)
+    m.loc = loc.ctypes.data_as(C.POINTER(C.c_int64))
+    return m, loc
+
+
+def ml_neighbours(nroot, root_level, nx, bc, locs, b):
+    """Neighbour list of block b on a multilevel mesh: rows (gid, level, ox1,
+    ox2, ox3, fi1, fi2) in the reference's order."""
+    m, keep = _ml_mesh(nroot, root_level, nx, bc, locs)
+    out = np.zeros((56, 7), dtype=np.int32)
+    n = lib().orc_ml_neighbours(C.byref(m), int(b), out.ctypes.data_as(C.POINTER(C.c_int)))
+    return out[:n]
+
+
+def ml_exchange(nroot, root_level, nx, bc, locs, u_all):
+    """One ghost fill of a multilevel mesh (locs: per block, gid order,
+    {level, lx1, lx2, lx3}); u_all is [nblocks][nvar][k][j][i], updated copy
+    returned."""
+    out = np.array(u_all, dtype=np.float64, copy=True, order="C")
+    m, keep = _ml_mesh(nroot, root_level, nx, bc, locs)
+    lib().orc_ml_exchange(C.byref(m), int(out.shape[1]), _ptr(out))
     return out
 
 

@@ -23,6 +23,12 @@ Fixtures (numpy .npz, compressed):
                     of one MeshBlock of a statically refined mesh, and the
                     regrid-time state transfer (coarse to fine, fine to
                     coarse) between two of its blocks
+  ml_exchange_<bc>.npz  one vertex-centred ghost fill of a two-level mesh
+                    (restriction, additive unpack with node multiplicity,
+                    coarse-level BCs, prolongation, fine-level BCs) of an
+                    integer-hash state (ml_hash_state), outflow and periodic
+                    faces, with the MeshBlocks' logical locations and
+                    coordinates
 Each fixture stores the input-deck parameters it was made with ("params",
 "mesh", "integrator" as JSON strings).
 """
@@ -248,6 +254,44 @@ def make_refine(outdir):
     return path
 
 
+# multilevel ghost exchange: the 16^3-cell mesh of REFINE with one root
+# block (x > 0, y < 0, z < 0) refined once, so that its eight children sit
+# between coarse blocks in gid order; outflow and periodic faces
+ML_REGION = dict(x1min=0.5, x1max=3.5, x2min=-3.5, x2max=-0.5, x3min=-3.5, x3max=-0.5, level=1)
+ML_VARS = [0, 13]
+
+
+def ml_hash_state(nblocks, nvar, nn):
+    """The integer-hash state the operator driver's gx_hash option writes."""
+    g, n, k, j, i = np.meshgrid(np.arange(nblocks), np.arange(nvar), np.arange(nn),
+                                np.arange(nn), np.arange(nn), indexing="ij")
+    return ((g * 131 + n * 31 + k * 7 + j * 3 + i) % 1009) / 1009.0 - 0.5
+
+
+def make_multilevel(bc, outdir):
+    case = dict(REFINE, bc=bc)
+    with tempfile.TemporaryDirectory() as tmp:
+        rec_path = os.path.join(tmp, "ml.rec")
+        inp = os.path.join(tmp, "case.inp")
+        text = deck(case, rec_path).replace("refinement = none", "refinement = static")
+        text += "gx_hash = true\n<refinement1>\n" + "".join(
+            f"{k} = {v}\n" for k, v in ML_REGION.items())
+        with open(inp, "w") as f:
+            f.write(text)
+        subprocess.run([os.path.join(REF_BIN, "z4c_ops_ref"), "-i", inp], cwd=tmp, check=True,
+                       stdout=subprocess.DEVNULL)
+        rec = read_records(rec_path)
+    pre = rec["gx_pre"]
+    assert np.array_equal(pre, ml_hash_state(*pre.shape[:2], pre.shape[2])), "gx_hash state"
+    tag = {"extrapolate_outflow": "outflow", "periodic": "periodic"}[bc]
+    path = os.path.join(outdir, f"ml_exchange_{tag}.npz")
+    np.savez_compressed(path, gx_post=rec["gx_post"][:, ML_VARS], vars=np.array(ML_VARS),
+                        meta=rec["meta"], xf=rec["xf"], dx=rec["dx"], bc=BC_CODES[bc], nb=np.array([2, 2, 2]),
+                        nx=np.array([8, 8, 8]), xmin=np.array([-4.0] * 3), xmax=np.array([4.0] * 3),
+                        region=json.dumps(ML_REGION))
+    return path
+
+
 RST_DECK = "<output2>\nfile_type = rst\ndt = 1e10\n"
 
 
@@ -296,6 +340,11 @@ def main():
             continue
         p = make_evol(name, case, HERE)
         print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
+    for bc in ("extrapolate_outflow", "periodic"):
+        tag = {"extrapolate_outflow": "outflow", "periodic": "periodic"}[bc]
+        if not only or f"ml_exchange_{tag}" in only:
+            p = make_multilevel(bc, HERE)
+            print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
     if not only or "restart_track4" in only:  # needs evol_track4
         p = make_restart(HERE)
         print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
