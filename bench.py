@@ -76,6 +76,9 @@ def parse():
                     help="launch shape point_threads,column_threads,column_slabs instead of "
                          "the autotuner's pick (profiling under ncu, whose serialised launches "
                          "would mislead the autotuner)")
+    ap.add_argument("--workload", default="uniform", choices=["uniform", "bbh_smr"],
+                    help="bbh_smr: binary punctures on a statically refined mesh of 7 levels "
+                         "(a separate measurement, not the headline line)")
     return ap.parse_args()
 
 
@@ -280,6 +283,88 @@ def whole_job_rate(units_per_rank, world, max_seconds):
     return units_per_rank * world / max_seconds
 
 
+# Binary Brill-Lindquist punctures (masses 0.5 near (+-3, 0, 0)) on
+# [-512, 512]^3 with 4^3 root MeshBlocks of 16^3 cells and seven nested
+# static refinement boxes around them (level L reaches 3 + 6 * 2^(7-L), half
+# as far along y and z from level 3 on): 3,424 MeshBlocks, finest spacing
+# 1/8.  The punctures sit a fraction of a cell off the vertices that every
+# level puts at (+-3, 0, 0), where psi diverges.
+SMR_REGIONS = [dict(x1min=-r, x1max=r, x2min=-r * f, x2max=r * f, x3min=-r * f, x3max=r * f,
+                    level=lv)
+               for lv in range(1, 8)
+               for r, f in [(min(3.0 + 6.0 * 2 ** (7 - lv), 511.0), 0.5 if lv > 2 else 1.0)]]
+SMR_CENTRES = ((3.0, 0.0625 * 0.37, 0.0625 * 0.21), (-3.0, -0.0625 * 0.37, -0.0625 * 0.21))
+
+
+def main_smr(args):
+    """Steps of the refined binary-puncture mesh: zone-updates/s through
+    the graph-captured step, and the multilevel ghost exchange alone."""
+    import torch
+    import z4c_b200 as Z
+    from z4c_b200 import initial_data as ID
+    torch.cuda.set_device(0)
+    mesh = Z.Mesh((4, 4, 4), (16, 16, 16), (-512.0,) * 3, (512.0,) * 3, "outflow",
+                  refinement=SMR_REGIONS)
+    params = Z.default_params(**PARAMS)
+    ctx = Z.Z4c(mesh, params, "rk4")
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    t0 = time.time()
+    ID.load_adm(ctx, ID.punctures(mesh, params, masses=(0.5, 0.5), centres=SMR_CENTRES))
+    ctx.sync()
+    setup_s = time.time() - t0
+    if args.shape:
+        ctx.set_tile(*(int(v) for v in args.shape.split(",")))
+    else:
+        with torch.cuda.stream(stream):
+            ctx.autotune(reps=2)
+    dt = mesh.new_dt(CFL)
+    with torch.cuda.stream(stream):
+        ctx.evolve(dt, args.warmup)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    with torch.cuda.stream(stream):
+        ctx.evolve(dt, args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    # the multilevel exchange alone (ghost fill of the 22-variable state)
+    reps = 10
+    with torch.cuda.stream(stream):
+        ctx.ghost_fill(Z.REG_U)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    with torch.cuda.stream(stream):
+        for _ in range(reps):
+            ctx.ghost_fill(Z.REG_U)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    exch_ms = ev0.elapsed_time(ev1) / reps
+    levels = np.bincount(mesh.locs[:, 0] - mesh.root_level).tolist()
+    line = {
+        "metric": "zone-updates/s", "value": mesh.zones() / (ms * 1e-3), "unit": "zone-updates/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "binary punctures (m=0.5 each near (+-3,0,0)), [-512,512]^3, "
+                               "4^3 root MeshBlocks of 16^3 cells, 7 nested static refinement "
+                               "levels, extrapolate_outflow, rk4 (2S), cfl 0.25",
+                   "meshblocks": mesh.nblocks, "blocks_per_level": levels,
+                   "finest_dx": float(min(min(mesh.block_coords(b)[1])
+                                          for b in range(mesh.nblocks) if mesh.locs[b, 0] ==
+                                          mesh.locs[:, 0].max())),
+                   "l2": "inputs larger than L2"},
+        "exchange_ms": exch_ms, "exchange_share": 4 * exch_ms / ms,
+        "setup_s": setup_s, "finite": bool(ctx.check_finite()),
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -288,6 +373,8 @@ def main():
 
     if args.impl == "reference":
         return main_reference(args, rank, world)
+    if args.workload == "bbh_smr":
+        return main_smr(args)
 
     import torch
     import torch.distributed as dist

@@ -5,11 +5,11 @@
 //   restrict   every block injects its interior into its coarse buffer
 //              (CommRegistry::SendBoundaryBuffers, comm_registry.cpp:246-296;
 //              RestrictInterior, refinement_ops.cpp:167-195)
-//   pack       one message per (receiver, neighbour entry) from the sender's
-//              pre-exchange arrays (CommChannel::PackAndSend,
-//              comm_channel.cpp:733-787; ranges index_utilities.hpp:124-216)
-//   unpack     per receiving block, in neighbour order: the fine ghosts start
-//              at zero and the interior at the block's own values; same-level
+//   unpack     per receiving block, in neighbour order, straight from the
+//              senders' pre-exchange arrays (the message each would pack,
+//              CommChannel::PackAndSend, comm_channel.cpp:733-787; ranges
+//              index_utilities.hpp:124-216): the fine and coarse ghosts
+//              start at zero and the interiors at the block's own values; same-level
 //              data is added into the fine array and its coarse payload into
 //              the coarse buffer, data from a coarser block overwrites the
 //              coarse buffer, data from a finer block is added into the fine
@@ -52,7 +52,7 @@ namespace {
 // ---- kernels ---------------------------------------------------------------
 
 // RestrictVertexCenteredValues over the coarse interior [cvs, cve]^3.
-__global__ void k_ml_restrict(MlPlan P, const double* __restrict__ src, double* __restrict__ coarse,
+__global__ void k_ml_restrict(MlPlan P, const double* __restrict__ src, double* __restrict__ csrc,
                               int nvar, int reg_nvar) {
   const int c0 = P.nx[0] / 2 + 1, c1 = P.nx[1] / 2 + 1, c2 = P.nx[2] / 2 + 1;
   const int64_t per = (int64_t)c0 * c1 * c2;
@@ -63,62 +63,67 @@ __global__ void k_ml_restrict(MlPlan P, const double* __restrict__ src, double* 
   const int ci = kMlNcg + (int)(r % c0), cj = kMlNcg + (int)((r / c0) % c1),
             ck = kMlNcg + (int)(r / ((int64_t)c0 * c1));
   const int i = 2 * (ci - kMlNcg) + NG, j = 2 * (cj - kMlNcg) + NG, k = 2 * (ck - kMlNcg) + NG;
-  coarse[((int64_t)b * Z4C_NVAR + n) * P.cvol + ((int64_t)ck * P.cn[1] + cj) * P.cn[0] + ci] =
+  csrc[((int64_t)b * Z4C_NVAR + n) * P.cvol + ((int64_t)ck * P.cn[1] + cj) * P.cn[0] + ci] =
       __ldg(src + ((int64_t)b * reg_nvar + n) * P.fvol + ((int64_t)k * P.nn[1] + j) * P.nn[0] + i);
 }
 
-__device__ __forceinline__ int64_t ml_index(const MlOp& o, int e, const int* dims) {
-  const int e0 = o.hi[0] - o.lo[0] + 1, e1 = o.hi[1] - o.lo[1] + 1;
-  const int i = o.lo[0] + e % e0, j = o.lo[1] + (e / e0) % e1, k = o.lo[2] + e / (e0 * e1);
-  return ((int64_t)k * dims[1] + j) * dims[0] + i;
+// compact zone (0..6) of index i along one axis: ghosts, the shared vertex,
+// the lower half, the midpoint, the upper half, the shared vertex, ghosts
+// (NodeMultiplicity::ApplyDivisionImpl's PhysRange, node_multiplicity.cpp:364-430)
+__device__ __forceinline__ int ml_zone(int i, int vs, int ve) {
+  const int mid = vs + (ve - vs) / 2;
+  return i < vs ? 0 : i == vs ? 1 : i < mid ? 2 : i == mid ? 3 : i < ve ? 4 : i == ve ? 5 : 6;
 }
 
-// BufferUtility::PackData: one CTA per (pack op, variable).
-__global__ void k_ml_pack(MlPlan P, const double* __restrict__ src, int reg_nvar) {
-  const MlOp o = P.pack[blockIdx.x];
-  const int n = blockIdx.y;
-  const double* a = o.coarse ? P.coarse + ((int64_t)o.blk * Z4C_NVAR + n) * P.cvol
-                             : src + ((int64_t)o.blk * reg_nvar + n) * P.fvol;
-  const int* dims = o.coarse ? P.cn : P.nn;
-  double* out = P.buf + o.off + (int64_t)n * o.count;
-  for (int e = threadIdx.x; e < o.count; e += blockDim.x) out[e] = a[ml_index(o, e, dims)];
-}
-
-// SetBoundaries of one receiving block and variable: the fine array starts
-// as the block's interior with zero ghosts, then its ops run in order.
+// SetBoundaries of one receiving block and variable as a gather: each vertex
+// starts at the block's own value (interior) or zero (ghosts), takes its
+// zone's contributions in the reference's neighbour order (add, or copy for
+// data from a coarser block) and is multiplied by the inverse node
+// multiplicity of the zone; once for the fine array, once for the coarse
+// buffer.  A warp walks rows of the array, its lanes along i.
 __global__ void k_ml_unpack(MlPlan P, const double* __restrict__ src, double* __restrict__ dst,
                             int reg_nvar) {
   const int b = blockIdx.x, n = blockIdx.y;
-  const int64_t fo = ((int64_t)b * reg_nvar + n) * P.fvol;
-  const int nn0 = P.nn[0], nn1 = P.nn[1];
-  for (int64_t p = threadIdx.x; p < P.fvol; p += blockDim.x) {
-    const int i = (int)(p % nn0), j = (int)((p / nn0) % nn1), k = (int)(p / ((int64_t)nn0 * nn1));
-    const bool in = i >= NG && i <= NG + P.nx[0] && j >= NG && j <= NG + P.nx[1] && k >= NG &&
-                    k <= NG + P.nx[2];
-    dst[fo + p] = in ? src[fo + p] : 0.0;
-  }
-  double* cb = P.coarse + ((int64_t)b * Z4C_NVAR + n) * P.cvol;
-  for (int q = P.ustart[b]; q < P.ustart[b + 1]; ++q) {
-    __syncthreads();
-    const MlOp o = P.unpack[q];
-    double* a = o.coarse ? cb : dst + fo;
-    const int* dims = o.coarse ? P.cn : P.nn;
-    if (o.mode == kMlZeroGhosts) {
-      const int64_t vol = (int64_t)dims[0] * dims[1] * dims[2];
-      for (int64_t p = threadIdx.x; p < vol; p += blockDim.x) {
-        const int i = (int)(p % dims[0]), j = (int)((p / dims[0]) % dims[1]),
-                  k = (int)(p / ((int64_t)dims[0] * dims[1]));
-        if (i < o.lo[0] || i > o.hi[0] || j < o.lo[1] || j > o.hi[1] || k < o.lo[2] || k > o.hi[2])
-          a[p] = 0.0;
+  __shared__ unsigned char mult[343];
+  __shared__ int zs[2][344];
+  for (int q = threadIdx.x; q < 343; q += blockDim.x) mult[q] = P.mult[(int64_t)b * 343 + q];
+  for (int q = threadIdx.x; q < 2 * 344; q += blockDim.x)
+    zs[q / 344][q % 344] = P.zstart[(int64_t)b * 2 * 344 + q];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int arr = 0; arr < 2; ++arr) {
+    const int ng = arr ? Z4C_NCG : NG;
+    const int d0 = arr ? P.cn[0] : P.nn[0], d1 = arr ? P.cn[1] : P.nn[1],
+              d2 = arr ? P.cn[2] : P.nn[2];
+    const int v0 = ng + (arr ? P.nx[0] / 2 : P.nx[0]), v1 = ng + (arr ? P.nx[1] / 2 : P.nx[1]),
+              v2 = ng + (arr ? P.nx[2] / 2 : P.nx[2]);
+    const int64_t vol = arr ? P.cvol : P.fvol;
+    const double* own = arr ? P.csrc + ((int64_t)b * Z4C_NVAR + n) * vol
+                            : src + ((int64_t)b * reg_nvar + n) * vol;
+    double* out = arr ? P.coarse + ((int64_t)b * Z4C_NVAR + n) * vol
+                      : dst + ((int64_t)b * reg_nvar + n) * vol;
+    for (int row = warp; row < d1 * d2; row += nwarps) {
+      const int j = row % d1, k = row / d1;
+      const int zk = ml_zone(k, ng, v2), zj = ml_zone(j, ng, v1);
+      const bool row_in = zk >= 1 && zk <= 5 && zj >= 1 && zj <= 5;
+      for (int i = lane; i < d0; i += 32) {
+        const int zi = ml_zone(i, ng, v0);
+        const int z = (zk * 7 + zj) * 7 + zi;
+        const int p = row * d0 + i;
+        double v = (row_in && zi >= 1 && zi <= 5) ? __ldg(own + p) : 0.0;
+        for (int q = zs[arr][z]; q < zs[arr][z + 1]; ++q) {
+          const MlContrib c = P.contrib[q];
+          const int64_t sv = c.scoarse ? P.cvol : P.fvol;
+          const double* s = c.scoarse ? P.csrc + ((int64_t)c.sblk * Z4C_NVAR + n) * sv
+                                      : src + ((int64_t)c.sblk * reg_nvar + n) * sv;
+          const int s0 = c.scoarse ? P.cn[0] : P.nn[0], s1 = c.scoarse ? P.cn[1] : P.nn[1];
+          const double x = __ldg(s + ((k + c.d[2]) * s1 + j + c.d[1]) * s0 + i + c.d[0]);
+          v = c.mode == kMlCopy ? x : v + x;
+        }
+        const int m = mult[z];
+        if (m > 1) v *= P.inv[m];
+        out[p] = v;
       }
-      continue;
-    }
-    const double* in = P.buf + o.off + (int64_t)n * o.count;
-    for (int e = threadIdx.x; e < o.count; e += blockDim.x) {
-      double& d = a[ml_index(o, e, dims)];
-      if (o.mode == kMlCopy) d = in[e];
-      else if (o.mode == kMlAdd) d += in[e];
-      else d *= o.inv;
     }
   }
 }
@@ -364,7 +369,7 @@ int ml_root_level(const int nroot[3]) {
 }
 
 void ml_free(MlPlan& p) {
-  for (void* q : {(void*)p.coarse, (void*)p.buf, (void*)p.pack, (void*)p.unpack, (void*)p.ustart,
+  for (void* q : {(void*)p.csrc, (void*)p.coarse, (void*)p.contrib, (void*)p.zstart, (void*)p.mult,
                   (void*)p.pro, (void*)p.pro_blk})
     if (q) cudaFree(q);
   for (auto& lv : p.bc)
@@ -442,27 +447,28 @@ int ml_build(const int nroot[3], const int nx[3], const int bcf[6], int nblocks,
   plan.fvol = (long long)plan.nn[0] * plan.nn[1] * plan.nn[2];
   plan.cvol = (long long)plan.cn[0] * plan.cn[1] * plan.cn[2];
 
-  std::vector<MlOp> pack;
   std::vector<std::vector<MlOp>> unpack(nblocks);
-  long long off = 0;
+  std::vector<unsigned char> mults((size_t)nblocks * 343);
+  long long moved = 0;
   auto push_pair = [&](int sender, int scoarse, const int slo[3], const int shi[3], int receiver,
                        int rcoarse, int mode, const int rlo[3], const int rhi[3]) {
-    MlOp s = make_op(sender, scoarse, kMlCopy, slo, shi);
     MlOp r = make_op(receiver, rcoarse, mode, rlo, rhi);
-    s.off = r.off = off;
-    off += (long long)s.count * Z4C_NVAR;
-    pack.push_back(s);
+    r.sblk = sender;
+    r.scoarse = scoarse;
+    int scount = 1;
+    for (int a = 0; a < 3; ++a) {
+      r.slo[a] = slo[a];
+      scount *= shi[a] - slo[a] + 1;
+      if (shi[a] - slo[a] != rhi[a] - rlo[a]) return false;
+    }
+    moved += r.count;
     unpack[receiver].push_back(r);
-    return s.count == r.count;
+    return scount == r.count;
   };
   for (int r = 0; r < nblocks; ++r) {
     const int rlev = (int)locs[4 * r];
     bool same = true;
     for (const Entry& e : B.nbrs[r]) same = same && e.level == rlev;
-    {
-      const int lo[3] = {C[0].vs, C[1].vs, C[2].vs}, hi[3] = {C[0].ve, C[1].ve, C[2].ve};
-      unpack[r].push_back(make_op(r, 1, kMlZeroGhosts, lo, hi));
-    }
     for (const Entry& e : B.nbrs[r]) {
       const int s = e.gid;
       const Entry* back = nullptr;  // the sender's entry pointing at r
@@ -572,29 +578,12 @@ int ml_build(const int nroot[3], const int nx[3], const int bcf[6], int nblocks,
         for (int j = s[1]; j <= t[1]; ++j)
           for (int i = s[0]; i <= t[0]; ++i) ++mult[k][j][i];
     }
-    for (int coarse = 0; coarse < 2; ++coarse) {
-      const Ax* X = coarse ? C : F;
-      auto phys = [](int c, const Ax& a, int& lo, int& hi) {  // ApplyDivisionImpl's PhysRange
-        const int half = (a.ve - a.vs) / 2;
-        const int t[7] = {a.ms, a.vs, a.vs + 1, a.vs + half, a.ve - 1, a.ve, a.pe};
-        if (c & 1) lo = hi = t[c];
-        else if (c <= 3) { lo = t[c]; hi = t[c + 1] - 1; }
-        else { lo = t[c - 1] + 1; hi = t[c]; }
-      };
-      for (int K = 0; K < 7; ++K)
-        for (int J = 0; J < 7; ++J)
-          for (int I = 0; I < 7; ++I) {
-            if (mult[K][J][I] <= 1) continue;
-            int lo[3], hi[3];
-            phys(I, X[0], lo[0], hi[0]);
-            phys(J, X[1], lo[1], hi[1]);
-            phys(K, X[2], lo[2], hi[2]);
-            if (lo[0] > hi[0] || lo[1] > hi[1] || lo[2] > hi[2]) continue;
-            MlOp o = make_op(r, coarse, kMlScale, lo, hi);
-            o.inv = 1.0 / static_cast<double>(mult[K][J][I]);
-            unpack[r].push_back(o);
-          }
-    }
+    for (int k = 0; k < 7; ++k)
+      for (int j = 0; j < 7; ++j)
+        for (int i = 0; i < 7; ++i) {
+          if (mult[k][j][i] > 63) return set_error(Z4C_EINVAL, "multilevel plan: multiplicity > 63");
+          mults[(size_t)r * 343 + (k * 7 + j) * 7 + i] = (unsigned char)mult[k][j][i];
+        }
   }
   // physical faces: extrapolation on the coarse buffer with the vertex
   // interior ends (ApplyPhysicalBCsOnCoarseLevel, called with the Z4c coarse
@@ -667,12 +656,13 @@ int ml_build(const int nroot[3], const int nx[3], const int bcf[6], int nblocks,
   // every box, ghost write and extrapolation read stays inside its array
   auto inside = [&](const MlOp& o) {
     const int* d = o.coarse ? plan.cn : plan.nn;
-    for (int a = 0; a < 3; ++a)
+    const int* sd = o.scoarse ? plan.cn : plan.nn;
+    for (int a = 0; a < 3; ++a) {
       if (o.lo[a] < 0 || o.hi[a] >= d[a] || o.lo[a] > o.hi[a]) return false;
-    return o.blk >= 0 && o.blk < nblocks;
+      if (o.slo[a] < 0 || o.slo[a] + (o.hi[a] - o.lo[a]) >= sd[a]) return false;
+    }
+    return o.blk >= 0 && o.blk < nblocks && o.sblk >= 0 && o.sblk < nblocks;
   };
-  for (const MlOp& o : pack)
-    if (!inside(o)) return set_error(Z4C_EINVAL, "multilevel plan: pack box outside the array");
   for (const auto& v : unpack)
     for (const MlOp& o : v)
       if (!inside(o)) return set_error(Z4C_EINVAL, "multilevel plan: unpack box outside the array");
@@ -690,11 +680,54 @@ int ml_build(const int nroot[3], const int nx[3], const int bcf[6], int nblocks,
           return set_error(Z4C_EINVAL, "multilevel plan: boundary ghosts outside the array");
       }
 
+  // per (block, array, compact zone) the ordered contributions
+  std::vector<MlContrib> contrib;
+  std::vector<int> zstart((size_t)nblocks * 2 * 344 + 1, 0);
+  {
+    std::vector<std::vector<MlContrib>> zl(2 * 343);
+    for (int b = 0; b < nblocks; ++b) {
+      for (auto& v : zl) v.clear();
+      for (const MlOp& o : unpack[b]) {
+        const Ax* X = o.coarse ? C : F;
+        int zlo[3], zhi[3];
+        for (int a = 0; a < 3; ++a) {
+          const int mid = X[a].vs + (X[a].ve - X[a].vs) / 2;
+          auto zone = [&](int i) {
+            return i < X[a].vs ? 0 : i == X[a].vs ? 1 : i < mid ? 2 : i == mid ? 3
+                 : i < X[a].ve ? 4 : i == X[a].ve ? 5 : 6;
+          };
+          const int zs[7] = {X[a].ms, X[a].vs, X[a].vs + 1, mid, mid + 1, X[a].ve, X[a].ve + 1};
+          const int ze[7] = {X[a].vs - 1, X[a].vs, mid - 1, mid, X[a].ve - 1, X[a].ve, X[a].pe};
+          zlo[a] = zone(o.lo[a]);
+          zhi[a] = zone(o.hi[a]);
+          if (o.lo[a] != zs[zlo[a]] || o.hi[a] != ze[zhi[a]])
+            return set_error(Z4C_EINVAL, "multilevel plan: an unpack box splits a compact zone");
+        }
+        MlContrib c{};
+        c.sblk = o.sblk;
+        c.scoarse = (short)o.scoarse;
+        c.mode = (short)o.mode;
+        for (int a = 0; a < 3; ++a) c.d[a] = (short)(o.slo[a] - o.lo[a]);
+        for (int zk = zlo[2]; zk <= zhi[2]; ++zk)
+          for (int zj = zlo[1]; zj <= zhi[1]; ++zj)
+            for (int zi = zlo[0]; zi <= zhi[0]; ++zi)
+              zl[o.coarse * 343 + (zk * 7 + zj) * 7 + zi].push_back(c);
+      }
+      for (int arr = 0; arr < 2; ++arr) {
+        for (int z = 0; z < 343; ++z) {
+          zstart[((size_t)b * 2 + arr) * 344 + z] = (int)contrib.size();
+          contrib.insert(contrib.end(), zl[arr * 343 + z].begin(), zl[arr * 343 + z].end());
+        }
+        zstart[((size_t)b * 2 + arr) * 344 + 343] = (int)contrib.size();
+      }
+    }
+  }
+
   if (query_out) {  // query_block == -2: the op counts of the checked plan, no device memory
     size_t nu = 0;
     for (const auto& v : unpack) nu += v.size();
-    query_out[0] = (int)pack.size();
-    query_out[1] = (int)nu;
+    query_out[0] = (int)nu;  // unpack ops (boxes)
+    query_out[1] = (int)std::min(moved, (long long)INT32_MAX);
     query_out[2] = (int)pro.size();
     int nbc = 0;
     for (int lv = 0; lv < 2; ++lv)
@@ -702,34 +735,23 @@ int ml_build(const int nroot[3], const int nx[3], const int bcf[6], int nblocks,
     query_out[3] = nbc;
     return 4;
   }
-  std::vector<MlOp> uflat;
-  std::vector<int> ustart(nblocks + 1, 0);
-  for (int b = 0; b < nblocks; ++b) {
-    ustart[b] = (int)uflat.size();
-    uflat.insert(uflat.end(), unpack[b].begin(), unpack[b].end());
-  }
-  ustart[nblocks] = (int)uflat.size();
-
   int rc = Z4C_OK;
   auto fail_free = [&](int code) {
     ml_free(plan);
     return code;
   };
-  if (cudaMalloc((void**)&plan.coarse, sizeof(double) * Z4C_NVAR * plan.cvol * nblocks) != cudaSuccess) {
-    cudaGetLastError();
-    return fail_free(set_error(Z4C_ENOMEM, "multilevel plan: coarse buffers"));
+  for (int m = 1; m < 64; ++m) plan.inv[m] = 1.0 / static_cast<double>(m);
+  for (double** q : {&plan.csrc, &plan.coarse}) {
+    if (cudaMalloc((void**)q, sizeof(double) * Z4C_NVAR * plan.cvol * nblocks) != cudaSuccess) {
+      cudaGetLastError();
+      return fail_free(set_error(Z4C_ENOMEM, "multilevel plan: coarse buffers"));
+    }
   }
-  plan.buf_elems = std::max(off, 1LL);
-  if (cudaMalloc((void**)&plan.buf, sizeof(double) * plan.buf_elems) != cudaSuccess) {
-    cudaGetLastError();
-    return fail_free(set_error(Z4C_ENOMEM, "multilevel plan: message buffer"));
-  }
-  if ((rc = upload(&plan.pack, pack)) || (rc = upload(&plan.unpack, uflat)) ||
-      (rc = upload(&plan.ustart, ustart)) || (rc = upload(&plan.pro, pro)) ||
+  if ((rc = upload(&plan.contrib, contrib)) || (rc = upload(&plan.zstart, zstart)) ||
+      (rc = upload(&plan.mult, mults)) || (rc = upload(&plan.pro, pro)) ||
       (rc = upload(&plan.pro_blk, pro_blk)))
     return fail_free(rc);
-  plan.npack = (int)pack.size();
-  plan.nunpack = (int)uflat.size();
+  plan.ncontrib = (int)contrib.size();
   plan.npro = (int)pro.size();
   for (int lv = 0; lv < 2; ++lv)
     for (int a = 0; a < 3; ++a) {
@@ -747,11 +769,7 @@ int launch_ml_exchange(const MlPlan& P, const double* src, double* dst, int nvar
   {
     const int64_t n = (int64_t)(P.nx[0] / 2 + 1) * (P.nx[1] / 2 + 1) * (P.nx[2] / 2 + 1) * nvar *
                       P.nblocks;
-    k_ml_restrict<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, src, P.coarse, nvar, reg_nvar);
-    ++launches;
-  }
-  if (P.npack > 0) {
-    k_ml_pack<<<dim3(P.npack, nvar), 128, 0, st>>>(P, src, reg_nvar);
+    k_ml_restrict<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, src, P.csrc, nvar, reg_nvar);
     ++launches;
   }
   k_ml_unpack<<<dim3(P.nblocks, nvar), 256, 0, st>>>(P, src, dst, reg_nvar);

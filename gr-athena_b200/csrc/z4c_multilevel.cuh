@@ -10,17 +10,29 @@
 
 namespace z4c {
 
-// One box of one block's fine array or coarse buffer.  Pack ops copy the box
-// into the message buffer; unpack ops of a receiving block run in order:
-// copy or add from the buffer, zero the ghosts of the coarse buffer, or
-// multiply by the inverse node multiplicity.
-enum MlMode { kMlCopy = 0, kMlAdd = 1, kMlZeroGhosts = 2, kMlScale = 3 };
+// One unpack op of a receiving block (host side): a box of its fine array or
+// coarse buffer receives (copy or add) the box of the same shape that starts
+// at slo in the sending block's fine array or restricted coarse interior.
+// Ops of a block run in the reference's neighbour order.
+enum MlMode { kMlCopy = 0, kMlAdd = 1 };
 struct MlOp {
   int blk, coarse, mode;
   int lo[3], hi[3];  // inclusive
   int count;         // vertices in the box
-  long long off;     // message-buffer offset of variable 0 (variable stride: count)
-  double inv;
+  int sblk, scoarse;
+  int slo[3];
+};
+
+// The ops' boxes are unions of the 7 x 7 x 7 compact zones of an array
+// (ghosts, shared vertex, lower half, midpoint, upper half, shared vertex,
+// ghosts per axis), so every vertex of a zone receives the same ordered
+// contributions: the device gathers them per vertex.  d = source index
+// minus destination index.
+struct MlContrib {
+  int sblk;
+  short scoarse, mode;
+  short d[3];
+  short pad;
 };
 
 // One physical face of one block: the extrapolation fills the ghosts beyond
@@ -34,14 +46,14 @@ struct MlPlan {
   int nblocks = 0;
   int nx[3] = {}, nn[3] = {}, cn[3] = {};
   long long fvol = 0, cvol = 0;
-  double* coarse = nullptr;  // [block][Z4C_NVAR][cvol]
-  double* buf = nullptr;     // messages of Z4C_NVAR variables
-  long long buf_elems = 0;
-  MlOp* pack = nullptr;
-  int npack = 0;
-  MlOp* unpack = nullptr;
-  int* ustart = nullptr;     // unpack ops of block b: [ustart[b], ustart[b+1])
-  int nunpack = 0;
+  double* csrc = nullptr;    // restricted interiors [block][Z4C_NVAR][cvol] (read-only in unpack)
+  double* coarse = nullptr;  // the receiving coarse buffers, same layout
+  MlContrib* contrib = nullptr;
+  int* zstart = nullptr;     // contributions of zone z of array a of block b:
+                             // [zstart[(b*2+a)*344+z], zstart[(b*2+a)*344+z+1])
+  int ncontrib = 0;
+  unsigned char* mult = nullptr;  // node multiplicity per block in the 7^3 compact zones
+  double inv[64] = {};            // 1 / m
   MlBc* bc[2][3] = {};       // [fine, coarse][axis]
   int nbc[2][3] = {};
   refine::RefGeom* pro = nullptr;  // prolongation boxes
@@ -58,8 +70,8 @@ struct MlPlan {
 // With query_out, only the checks and the neighbour list of query_block are
 // made: rows {gid, level, ox1, ox2, ox3, fi1, fi2} (at most 56), the count
 // returned; query_block == -2 builds and checks the whole plan without
-// device memory and writes its op counts {pack, unpack, prolongation boxes,
-// boundary faces}.
+// device memory and writes its sizes {unpack ops, vertices they move per
+// variable, prolongation boxes, boundary faces}.
 int ml_build(const int nroot[3], const int nx[3], const int bc[6], int nblocks,
              const long long* locs, MlPlan& plan, int query_block = -1, int* query_out = nullptr);
 void ml_free(MlPlan& plan);
