@@ -86,44 +86,42 @@ __global__ void k_ml_unpack(MlPlan P, const double* __restrict__ src, double* __
   const int b = blockIdx.x, n = blockIdx.y;
   __shared__ unsigned char mult[343];
   __shared__ int zs[2][344];
+  extern __shared__ MlContrib sc[];  // this block's contributions
   for (int q = threadIdx.x; q < 343; q += blockDim.x) mult[q] = P.mult[(int64_t)b * 343 + q];
   for (int q = threadIdx.x; q < 2 * 344; q += blockDim.x)
     zs[q / 344][q % 344] = P.zstart[(int64_t)b * 2 * 344 + q];
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int c0 = zs[0][0], nc = zs[1][343] - c0;
+  for (int q = threadIdx.x; q < nc; q += blockDim.x) sc[q] = P.contrib[c0 + q];
+  __syncthreads();
   for (int arr = 0; arr < 2; ++arr) {
     const int ng = arr ? Z4C_NCG : NG;
-    const int d0 = arr ? P.cn[0] : P.nn[0], d1 = arr ? P.cn[1] : P.nn[1],
-              d2 = arr ? P.cn[2] : P.nn[2];
+    const int d0 = arr ? P.cn[0] : P.nn[0], d1 = arr ? P.cn[1] : P.nn[1];
     const int v0 = ng + (arr ? P.nx[0] / 2 : P.nx[0]), v1 = ng + (arr ? P.nx[1] / 2 : P.nx[1]),
               v2 = ng + (arr ? P.nx[2] / 2 : P.nx[2]);
-    const int64_t vol = arr ? P.cvol : P.fvol;
+    const int vol = (int)(arr ? P.cvol : P.fvol);
     const double* own = arr ? P.csrc + ((int64_t)b * Z4C_NVAR + n) * vol
                             : src + ((int64_t)b * reg_nvar + n) * vol;
     double* out = arr ? P.coarse + ((int64_t)b * Z4C_NVAR + n) * vol
                       : dst + ((int64_t)b * reg_nvar + n) * vol;
-    for (int row = warp; row < d1 * d2; row += nwarps) {
-      const int j = row % d1, k = row / d1;
-      const int zk = ml_zone(k, ng, v2), zj = ml_zone(j, ng, v1);
-      const bool row_in = zk >= 1 && zk <= 5 && zj >= 1 && zj <= 5;
-      for (int i = lane; i < d0; i += 32) {
-        const int zi = ml_zone(i, ng, v0);
-        const int z = (zk * 7 + zj) * 7 + zi;
-        const int p = row * d0 + i;
-        double v = (row_in && zi >= 1 && zi <= 5) ? __ldg(own + p) : 0.0;
-        for (int q = zs[arr][z]; q < zs[arr][z + 1]; ++q) {
-          const MlContrib c = P.contrib[q];
-          const int64_t sv = c.scoarse ? P.cvol : P.fvol;
-          const double* s = c.scoarse ? P.csrc + ((int64_t)c.sblk * Z4C_NVAR + n) * sv
-                                      : src + ((int64_t)c.sblk * reg_nvar + n) * sv;
-          const int s0 = c.scoarse ? P.cn[0] : P.nn[0], s1 = c.scoarse ? P.cn[1] : P.nn[1];
-          const double x = __ldg(s + ((k + c.d[2]) * s1 + j + c.d[1]) * s0 + i + c.d[0]);
-          v = c.mode == kMlCopy ? x : v + x;
-        }
-        const int m = mult[z];
-        if (m > 1) v *= P.inv[m];
-        out[p] = v;
+    for (int p = threadIdx.x; p < vol; p += blockDim.x) {
+      const int i = p % d0, row = p / d0, j = row % d1, k = row / d1;
+      const int zi = ml_zone(i, ng, v0), zj = ml_zone(j, ng, v1), zk = ml_zone(k, ng, v2);
+      const int z = (zk * 7 + zj) * 7 + zi;
+      const bool in = zi >= 1 && zi <= 5 && zj >= 1 && zj <= 5 && zk >= 1 && zk <= 5;
+      double v = in ? __ldg(own + p) : 0.0;
+      for (int q = zs[arr][z] - c0; q < zs[arr][z + 1] - c0; ++q) {
+        const MlContrib c = sc[q];
+        const int64_t sv = c.scoarse ? P.cvol : P.fvol;
+        const double* s = c.scoarse ? P.csrc + ((int64_t)c.sblk * Z4C_NVAR + n) * sv
+                                    : src + ((int64_t)c.sblk * reg_nvar + n) * sv;
+        const int s0 = c.scoarse ? P.cn[0] : P.nn[0], s1 = c.scoarse ? P.cn[1] : P.nn[1];
+        const double x = __ldg(s + ((k + c.d[2]) * s1 + j + c.d[1]) * s0 + i + c.d[0]);
+        v = c.mode == kMlCopy ? x : v + x;
       }
+      const int m = mult[z];
+      if (m > 1) v *= P.inv[m];
+      out[p] = v;
     }
   }
 }
@@ -158,17 +156,38 @@ __global__ void k_ml_bc(const MlBc* __restrict__ items, double* __restrict__ arr
   }
 }
 
-// ProlongateVertexCenteredValues over one coarse box per CTA row.
+// ProlongateVertexCenteredValues over one coarse box per CTA row.  The fine
+// vertices are taken one parity class (injected or interpolated along each
+// axis) at a time, so the threads of a warp run the same interpolation.
 __global__ void k_ml_prolong(MlPlan P, double* __restrict__ dst, int reg_nvar) {
   const RefGeom G = P.pro[blockIdx.x];
   const int b = P.pro_blk[blockIdx.x], n = blockIdx.y;
-  const int e0 = G.fe[0] - G.f0[0] + 1, e1 = G.fe[1] - G.f0[1] + 1, e2 = G.fe[2] - G.f0[2] + 1;
   const double* C = P.coarse + ((int64_t)b * Z4C_NVAR + n) * P.cvol;
   double* F = dst + ((int64_t)b * reg_nvar + n) * P.fvol;
-  for (int e = threadIdx.x; e < e0 * e1 * e2; e += blockDim.x) {
-    const int f[3] = {G.f0[0] + e % e0, G.f0[1] + (e / e0) % e1, G.f0[2] + e / (e0 * e1)};
-    double v;
-    if (refine::prolong_value(G, C, f, v)) F[((int64_t)f[2] * G.nn[1] + f[1]) * G.nn[0] + f[0]] = v;
+  constexpr int hnc = refine::HNC;
+  for (int cls = 0; cls < 8; ++cls) {
+    int lo[3], cnt[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      int l, h;
+      if ((cls >> a) & 1) {  // interpolated: odd fine index, coarse sp..ep-1
+        l = 2 * (G.sp[a] - hnc) + 1;
+        h = 2 * (G.ep[a] - 1 - hnc) + 1;
+      } else {  // injected: even fine index, coarse box
+        l = 2 * (G.box[2 * a] - hnc);
+        h = 2 * (G.box[2 * a + 1] - hnc);
+      }
+      lo[a] = l;
+      cnt[a] = h >= l ? (h - l) / 2 + 1 : 0;
+    }
+    const int total = cnt[0] * cnt[1] * cnt[2];
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      const int f[3] = {lo[0] + 2 * (t % cnt[0]), lo[1] + 2 * ((t / cnt[0]) % cnt[1]),
+                        lo[2] + 2 * (t / (cnt[0] * cnt[1]))};
+      double v;
+      if (refine::prolong_value(G, C, f, v))
+        F[((int64_t)f[2] * G.nn[1] + f[1]) * G.nn[0] + f[0]] = v;
+    }
   }
 }
 
@@ -752,6 +771,10 @@ int ml_build(const int nroot[3], const int nx[3], const int bcf[6], int nblocks,
       (rc = upload(&plan.pro_blk, pro_blk)))
     return fail_free(rc);
   plan.ncontrib = (int)contrib.size();
+  for (int b = 0; b < nblocks; ++b)
+    plan.max_block_contrib = std::max(plan.max_block_contrib,
+                                      zstart[((size_t)b * 2 + 1) * 344 + 343] -
+                                          zstart[(size_t)b * 2 * 344]);
   plan.npro = (int)pro.size();
   for (int lv = 0; lv < 2; ++lv)
     for (int a = 0; a < 3; ++a) {
@@ -772,7 +795,12 @@ int launch_ml_exchange(const MlPlan& P, const double* src, double* dst, int nvar
     k_ml_restrict<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, src, P.csrc, nvar, reg_nvar);
     ++launches;
   }
-  k_ml_unpack<<<dim3(P.nblocks, nvar), 256, 0, st>>>(P, src, dst, reg_nvar);
+  const size_t smem = sizeof(MlContrib) * (size_t)std::max(P.max_block_contrib, 1);
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(k_ml_unpack, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return set_error(Z4C_ECUDA, "multilevel exchange: shared memory for the contribution lists");
+  k_ml_unpack<<<dim3(P.nblocks, nvar), 256, smem, st>>>(P, src, dst, reg_nvar);
   ++launches;
   auto bc_axis = [&](int lv, double* arr, int64_t bstride, int64_t vol, const int* dims, int ng) {
     for (int a = 0; a < 3; ++a) {

@@ -52,6 +52,7 @@ struct MlPlan {
   int* zstart = nullptr;     // contributions of zone z of array a of block b:
                              // [zstart[(b*2+a)*344+z], zstart[(b*2+a)*344+z+1])
   int ncontrib = 0;
+  int max_block_contrib = 0;  // the most contributions of one block (shared-memory size)
   unsigned char* mult = nullptr;  // node multiplicity per block in the 7^3 compact zones
   double inv[64] = {};            // 1 / m
   MlBc* bc[2][3] = {};       // [fine, coarse][axis]
