@@ -14,6 +14,12 @@ advanced one full step (the reference's zone-cycle, main.cpp:239).
 With N > 1 (torchrun) every rank evolves its own replica of the mesh
 ("replicas only": the path has no cross-GPU exchange on one-GPU meshes); the
 value is the total over ranks divided by the slowest rank's time.
+
+  python bench.py --workload bbh_smr [--steps K] [--warmup W]
+
+prints a separate line for binary punctures on a statically refined mesh of
+3,424 MeshBlocks on seven levels (SMR_REGIONS): zone-updates/s of the
+graph-captured RK4 step and the time of one multilevel ghost fill; one GPU.
 """
 import argparse
 import json
