@@ -101,6 +101,7 @@ int set_error(int code, const char* msg) {
 struct z4c_ctx {
   Grid g{};
   MlPlan* ml = nullptr;         // multilevel meshes: the ghost-exchange plan
+  unsigned char* som = nullptr; // multilevel meshes: gr_sommerfeld faces per block (device)
   std::vector<long long> locs;  // multilevel meshes: {level, lx1, lx2, lx3} per block
   z4c_mesh_desc_t desc{};
   z4c_params_t params{};
@@ -149,6 +150,7 @@ struct z4c_ctx {
     P.fd = fd;
     P.xf = xf;
     P.dx = dxd;
+    P.som = som;
     return P;
   }
 };
@@ -330,6 +332,7 @@ void free_ctx(z4c_ctx* c) {
     ml_free(*c->ml);
     delete c->ml;
   }
+  if (c->som) cudaFree(c->som);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -387,12 +390,7 @@ int create_impl(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int int
     if ((lo == Z4C_BC_PERIODIC) != (hi == Z4C_BC_PERIODIC))
       return fail(Z4C_EINVAL, "axis %d: periodic on one face only", a);
   }
-  if (locs) {
-    for (int f = 0; f < 6; ++f)
-      if (mesh->bc[f] == Z4C_BC_SOMMERFELD)
-        return fail(Z4C_EINVAL, "refined meshes take outflow or periodic faces");
-    if (nblocks_ml < 1) return fail(Z4C_EINVAL, "refined mesh without blocks");
-  }
+  if (locs && nblocks_ml < 1) return fail(Z4C_EINVAL, "refined mesh without blocks");
   const int64_t nblocks_all =
       locs ? (int64_t)nblocks_ml : (int64_t)mesh->nb[0] * mesh->nb[1] * mesh->nb[2];
   {
@@ -442,6 +440,24 @@ int create_impl(const z4c_mesh_desc_t* mesh, const z4c_params_t* params, int int
     if (rc) {
       free_ctx(c);
       return rc;
+    }
+    if (g.has_sommerfeld) {  // the blocks' gr_sommerfeld faces from their logical locations
+      const int rl = ml_root_level(mesh->nb);
+      std::vector<unsigned char> som(nblocks_ml, 0);
+      for (int b = 0; b < nblocks_ml; ++b)
+        for (int a = 0; a < 3; ++a) {
+          const long long n = (long long)mesh->nb[a] << (locs[4 * b] - rl);
+          if (mesh->bc[2 * a] == Z4C_BC_SOMMERFELD && locs[4 * b + 1 + a] == 0)
+            som[b] |= (unsigned char)(1u << (2 * a));
+          if (mesh->bc[2 * a + 1] == Z4C_BC_SOMMERFELD && locs[4 * b + 1 + a] == n - 1)
+            som[b] |= (unsigned char)(1u << (2 * a + 1));
+        }
+      if (cudaMalloc((void**)&c->som, som.size()) != cudaSuccess ||
+          cudaMemcpy(c->som, som.data(), som.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        free_ctx(c);
+        return fail(Z4C_ENOMEM, "gr_sommerfeld face table");
+      }
     }
   }
   const int root_level = ml_root_level(mesh->nb);

@@ -34,6 +34,8 @@ struct DevParams {
   const FdScale* fd;  // [nblocks]
   const double* xf;   // [nblocks][nn0+nn1+nn2] vertex coordinates (Sommerfeld faces)
   const double* dx;   // [nblocks][3] vertex spacing (Sommerfeld faces)
+  const unsigned char* som;  // refined meshes: [nblocks] gr_sommerfeld faces, bit 2*axis+outer;
+                             // null on a uniform block grid (faces from the grid position)
 };
 
 // Geometry of the uniform block grid.

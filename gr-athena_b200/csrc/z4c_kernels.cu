@@ -226,7 +226,14 @@ __device__ __forceinline__ bool sommerfeld_var(int n) {
   return n == Z4C_KHAT || n == Z4C_THETA || (n >= Z4C_AXX && n <= Z4C_GAMZ);
 }
 // Whether vertex (i, j, k) of block b lies on one of its gr_sommerfeld faces.
-__device__ __forceinline__ bool on_sommerfeld_face(const Grid& g, int b, int i, int j, int k) {
+__device__ __forceinline__ bool on_sommerfeld_face(const Grid& g, const DevParams& P, int b, int i,
+                                                   int j, int k) {
+  if (P.som) {
+    const unsigned m = P.som[b];
+    return ((m & 1u) && i == NG) || ((m & 2u) && i == NG + g.nx[0]) || ((m & 4u) && j == NG) ||
+           ((m & 8u) && j == NG + g.nx[1]) || ((m & 16u) && k == NG) ||
+           ((m & 32u) && k == NG + g.nx[2]);
+  }
   const int l0 = b % g.nb[0], l1 = (b / g.nb[0]) % g.nb[1], l2 = b / (g.nb[0] * g.nb[1]);
   return (g.bc[0] == Z4C_BC_SOMMERFELD && l0 == 0 && i == NG) ||
          (g.bc[1] == Z4C_BC_SOMMERFELD && l0 == g.nb[0] - 1 && i == NG + g.nx[0]) ||
@@ -281,7 +288,7 @@ k_sommerfeld(Grid g, DevParams P, const double* __restrict__ u, double* __restri
   const int v = rest % 11, b = block0 + rest / 11;
   const int n = (v < 2) ? (v == 0 ? Z4C_KHAT : Z4C_THETA) : Z4C_AXX + (v - 2);  // A, Gamma
   const int i = NG + l % n0, j = NG + (l / n0) % n1, k = NG + l / (n0 * n1);
-  if (!on_sommerfeld_face(g, b, i, j, k)) return;
+  if (!on_sommerfeld_face(g, P, b, i, j, k)) return;
   const int64_t q = ((int64_t)b * NVAR + n) * g.nvol + ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
   rhs[q] = sommerfeld_value(g, P, b, n, u + q, i, j, k, g.s);
 }
@@ -396,7 +403,7 @@ k_ko_stage_ls(Grid gin, DevParams P, const double* __restrict__ u,
     window_advance(f, sk, k, win);
     const int o = k * sk;
     const int64_t q = base + o;
-    const double r = (som && on_sommerfeld_face(g, c.b, c.i, c.j, k))
+    const double r = (som && on_sommerfeld_face(g, P, c.b, c.i, c.j, k))
                          ? sommerfeld_value(g, P, c.b, c.n, f + o, c.i, c.j, k, g.s)
                          : add_ko_column(__ldg(rhs + q), f + o, nn0, win, F, P.p.diss);
     const double un = win[4];
@@ -446,7 +453,7 @@ k_ko_stage_bt(Grid gin, DevParams P, const double* __restrict__ u, const double*
     window_advance(f, sk, k, win);
     const int o = k * sk;
     const int64_t q = base + o;
-    const double r = (som && on_sommerfeld_face(g, c.b, c.i, c.j, k))
+    const double r = (som && on_sommerfeld_face(g, P, c.b, c.i, c.j, k))
                          ? sommerfeld_value(g, P, c.b, c.n, f + o, c.i, c.j, k, g.s)
                          : add_ko_column(__ldg(rhs + q), f + o, nn0, win, F, P.p.diss);
     K.k[w.kslot][q] = r;
@@ -579,7 +586,7 @@ k_ko_stage_ls_slab(Grid g, DevParams P, const double* __restrict__ u,
     const int o = k * pl + j * nn0 + i;
     const int64_t qq = base + o;
     const double* v = s0 + o;
-    const double r = (som && on_sommerfeld_face(g, b, i, j, k))
+    const double r = (som && on_sommerfeld_face(g, P, b, i, j, k))
                          ? sommerfeld_value<false>(g, P, b, n, v, i, j, k, sst)
                          : add_ko_slab(__ldg(rhs + qq), v, nn0, pl, F, P.p.diss);
     const double un = *v;
@@ -626,7 +633,7 @@ k_ko_stage_bt_slab(Grid g, DevParams P, const double* __restrict__ u,
     const int o = k * pl + j * nn0 + i;
     const int64_t qq = base + o;
     const double* v = s0 + o;
-    const double r = (som && on_sommerfeld_face(g, b, i, j, k))
+    const double r = (som && on_sommerfeld_face(g, P, b, i, j, k))
                          ? sommerfeld_value<false>(g, P, b, n, v, i, j, k, sst)
                          : add_ko_slab(__ldg(rhs + qq), v, nn0, pl, F, P.p.diss);
     K.k[w.kslot][qq] = r;

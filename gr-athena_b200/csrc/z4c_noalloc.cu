@@ -156,6 +156,7 @@ extern "C" int z4c_rhs_noalloc(const double* u, double* rhs, int nblocks, const 
   P.fd = fd;
   P.xf = nullptr;  // no Sommerfeld faces: the grid below is periodic
   P.dx = nullptr;
+  P.som = nullptr;
   const size_t bstride = (size_t)Z4C_NVAR * g.nvol;
   for (int b0 = 0; b0 < nblocks; b0 += chunk) {
     const int nb = (nblocks - b0 < chunk) ? nblocks - b0 : chunk;

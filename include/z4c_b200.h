@@ -149,9 +149,9 @@ int z4c_create(const z4c_mesh_desc_t *mesh, const z4c_params_t *params,
  * most one (MeshBlockTree, mesh/meshblock_tree.cpp:108-260).  Ghost fills
  * run the reference's multilevel vertex-centred exchange
  * (comm/comm_registry.cpp:246-382, 533-570; comm/refinement_ops.cpp:24-195;
- * comm/node_multiplicity.cpp; comm/physical_bcs.cpp:506-890).  Outflow and
- * periodic faces; puncture trackers, psi4 spheres and restart files need a
- * uniform mesh. */
+ * comm/node_multiplicity.cpp; comm/physical_bcs.cpp:506-890).  Outflow,
+ * periodic and gr_sommerfeld faces; puncture trackers, psi4 spheres and
+ * restart files need a uniform mesh. */
 int z4c_create_refined(const z4c_mesh_desc_t *mesh, int nblocks, const long long *locs,
                        const z4c_params_t *params, int integrator, z4c_ctx **out);
 /* The neighbour list z4c_create_refined builds for one block of a refined

@@ -158,6 +158,15 @@ def test_exchange_matches_reference_and_oracle(bc):
     ctx.close()
 
 
+def sommerfeld_faces(mesh, b):
+    """gr_sommerfeld faces of block b of a refined mesh, from its logical
+    location at its level."""
+    lev, *loc = (int(v) for v in mesh.locs[b])
+    n = [mesh.nb[a] << (lev - mesh.root_level) for a in range(3)]
+    return [int(mesh.bc[2 * a + side] == 2 and loc[a] == (0 if side == 0 else n[a] - 1))
+            for a in range(3) for side in range(2)]
+
+
 def oracle_ml_step(mesh, p, u, dt, integ):
     """One GR_Z4c step on the oracle over a refined mesh."""
     nb = mesh.nblocks
@@ -166,9 +175,13 @@ def oracle_ml_step(mesh, p, u, dt, integ):
     for b in range(nb):
         xs, dxs = mesh.block_coords(b)
         blocks.append(O.Block(mesh.nx, dxs, xs))
+    som = [sommerfeld_faces(mesh, b) for b in range(nb)]
 
     def rhs(v):
-        return np.stack([O.rhs(blocks[b], p, v[b]) for b in range(nb)])
+        r = np.stack([O.rhs(blocks[b], p, v[b]) for b in range(nb)])
+        for b in range(nb):
+            O.boundary_rhs(blocks[b], v[b], r[b], som[b])
+        return r
 
     def exchange(v):
         v = O.ml_exchange(mesh.nb, mesh.root_level, mesh.nx, mesh.bc, mesh.locs, v)
@@ -200,14 +213,17 @@ def oracle_ml_step(mesh, p, u, dt, integ):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("integ,bc", [("rk4", "outflow"), ("bt_rk4", "outflow"),
-                                      ("rk4", "periodic")])
+                                      ("rk4", "periodic"), ("rk4", "sommerfeld"),
+                                      ("bt_rk4", "sommerfeld")])
 def test_step_on_refined_mesh_matches_oracle(integ, bc):
-    """A binary puncture straddling the level boundary: one full step."""
+    """A binary puncture straddling the level boundary: one full step
+    (gr_sommerfeld: the outflow fixture's mesh with Sommerfeld faces, whose
+    right-hand side is overridden on the coarse and the fine blocks' faces)."""
     from z4c_b200 import initial_data as ID
     params = dict(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02, damp_kappa2=0.0,
                   shift_eta=2.0, r_max_con=1e300)
-    z = _fixture(bc)
-    mesh = _mesh(z)
+    z = _fixture("outflow" if bc == "sommerfeld" else bc)
+    mesh = _mesh(z, [2] * 6 if bc == "sommerfeld" else None)
     ctx = Z.Z4c(mesh, Z.default_params(**params), integ)
     ID.load_adm(ctx, ID.punctures(mesh, ctx.params, masses=(0.5, 0.5),
                                   centres=((0.9, -1.1, -0.7), (-1.2, 0.3, 0.2))))
