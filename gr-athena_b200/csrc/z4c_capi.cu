@@ -895,7 +895,6 @@ int z4c_sphere_grid(int nlev, double rad, int bitant, double* geo) {
 
 int z4c_wave_add(z4c_ctx* ctx, double rad, int nlev, int lmax, int bitant, int* id) {
   if (!ctx || !id) return fail(Z4C_EINVAL, "null argument");
-  if (ctx->ml) return fail(Z4C_EINVAL, "psi4 extraction needs a uniform mesh");
   if (nlev < 1 || nlev > 2000) return fail(Z4C_EINVAL, "nlev %d out of range [1, 2000]", nlev);
   if (lmax < 2 || lmax > 16) return fail(Z4C_EINVAL, "lmax %d out of range [2, 16]", lmax);
   if (!(rad > 0.0)) return fail(Z4C_EINVAL, "sphere radius must be positive");
@@ -1169,7 +1168,6 @@ long long z4c_kernel_launches(void) { return kernel_launch_count(); }
 
 int z4c_tracker_add(z4c_ctx* ctx, const double pos[3], int* id) {
   if (!ctx || !pos || !id) return fail(Z4C_EINVAL, "null argument");
-  if (ctx->ml) return fail(Z4C_EINVAL, "puncture trackers need a uniform mesh");
   if (ctx->ntrk >= kMaxTrackers) return fail(Z4C_EINVAL, "at most %d trackers", kMaxTrackers);
   const double rec[8] = {pos[0], pos[1], pos[2], NAN, NAN, NAN, 0.0, 0.0};
   CUDA_TRY(cudaMemcpyAsync(ctx->trk + 8 * ctx->ntrk, rec, sizeof(rec), cudaMemcpyHostToDevice,

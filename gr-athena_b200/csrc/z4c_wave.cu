@@ -354,7 +354,8 @@ int wave_build(const Grid& g, const std::vector<double>& xf, const std::vector<d
   w->nslot = (lmax - 1) * (2 * lmax + 1);
   const std::vector<double> geo = sphere_grid(nlev, rad, bitant);
   const int nv = (int)(geo.size() / 6);
-  // blocks in gid order
+  // blocks in gid order (on a refined mesh the context's blocks already are,
+  // and their row g.nb = {nblocks, 1, 1} keeps that order below)
   std::vector<int> order(g.nblocks);
   std::vector<uint64_t> key(g.nblocks);
   for (int b = 0; b < g.nblocks; ++b) {

@@ -150,7 +150,7 @@ int z4c_create(const z4c_mesh_desc_t *mesh, const z4c_params_t *params,
  * run the reference's multilevel vertex-centred exchange
  * (comm/comm_registry.cpp:246-382, 533-570; comm/refinement_ops.cpp:24-195;
  * comm/node_multiplicity.cpp; comm/physical_bcs.cpp:506-890).  Outflow,
- * periodic and gr_sommerfeld faces; puncture trackers, psi4 spheres and
+ * periodic and gr_sommerfeld faces, puncture trackers and psi4 spheres;
  * restart files need a uniform mesh. */
 int z4c_create_refined(const z4c_mesh_desc_t *mesh, int nblocks, const long long *locs,
                        const z4c_params_t *params, int integrator, z4c_ctx **out);

@@ -237,3 +237,74 @@ def test_step_on_refined_mesh_matches_oracle(integ, bc):
     ref = oracle_ml_step(mesh, O.default_params(**params), u0, dt, integ)
     assert rel_err(got, ref) <= 1e-12
     ctx.close()
+
+
+def _refined_binary(bc="outflow", integ="rk4"):
+    from z4c_b200 import initial_data as ID
+    params = dict(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02, damp_kappa2=0.0,
+                  shift_eta=2.0, r_max_con=1e300)
+    mesh = _mesh(_fixture(bc))
+    ctx = Z.Z4c(mesh, Z.default_params(**params), integ)
+    ID.load_adm(ctx, ID.punctures(mesh, ctx.params, masses=(0.5, 0.5),
+                                  centres=((0.9, -1.1, -0.7), (-1.2, 0.3, 0.2))))
+    return mesh, ctx, params
+
+
+@pytest.mark.gpu
+def test_tracker_on_refined_mesh_matches_oracle():
+    """Two trackers, one in a fine block and one in a coarse block: the shift
+    interpolated in the owning block at the start of the step, then
+    pos -= dt beta (PunctureTracker::InterpolateShift / EvolveTracker)."""
+    mesh, ctx, _ = _refined_binary()
+    u0 = ctx.download(Z.REG_U)
+    starts = [(1.37, -0.61, -1.23), (-1.45, 0.55, 0.35)]
+    ids = [ctx.add_tracker(p) for p in starts]
+    dt = mesh.new_dt(0.25)
+    ctx.evolve(dt, 1)
+    levels = []
+    for tid, p in zip(ids, starts):
+        owners = []
+        for b in range(mesh.nblocks):
+            xs, dxs = mesh.block_coords(b)
+            blk = O.Block(mesh.nx, dxs, xs)
+            if O.contains_exclusive(blk, p):
+                owners.append(b)
+        assert len(owners) == 1
+        b = owners[0]
+        levels.append(int(mesh.locs[b, 0]))
+        xs, dxs = mesh.block_coords(b)
+        beta = O.tracker_interp(O.Block(mesh.nx, dxs, xs), u0[b], p)
+        pos, got_beta = ctx.tracker(tid)
+        assert rel_err(np.asarray(got_beta), beta) <= 1e-13
+        assert np.allclose(pos, np.asarray(p) - dt * beta, rtol=0, atol=1e-15)
+    assert sorted(levels) == [1, 2]
+    ctx.close()
+
+
+@pytest.mark.gpu
+def test_extraction_on_refined_mesh_matches_oracle():
+    """psi4 multipoles on spheres that cross both levels: per-block
+    projections summed over the blocks in gid order (the context's order on
+    a refined mesh)."""
+    mesh, ctx, _ = _refined_binary()
+    ctx.evolve(mesh.new_dt(0.25), 1)
+    spheres = [Z.WaveExtract(ctx, r, 10, 4) for r in (1.9, 3.1)]
+    psis = ctx.psi4_multipoles(spheres)
+    weyl = ctx.download(Z.REG_WEYL)
+    assert np.isfinite(weyl).all()
+    for w, psi in zip(spheres, psis):
+        geo = O.sphere_grid(w.nlev, w.radius)
+        total = np.zeros_like(psi)
+        owned, lv = 0, set()
+        for b in range(mesh.nblocks):
+            xs, dxs = mesh.block_coords(b)
+            own, loc = O.wave_block(O.Block(mesh.nx, dxs, xs), weyl[b], geo, w.radius, w.lmax)
+            if len(own):
+                lv.add(int(mesh.locs[b, 0]))
+            owned += len(own)
+            total = total + loc
+        assert w.num_points() == owned == len(geo)
+        assert lv == {1, 2}
+        assert rel_err(psi, total) <= 1e-12
+        assert np.abs(total).max() > 0
+    ctx.close()
