@@ -308,3 +308,29 @@ def test_extraction_on_refined_mesh_matches_oracle():
         assert rel_err(psi, total) <= 1e-12
         assert np.abs(total).max() > 0
     ctx.close()
+
+
+@pytest.mark.gpu
+def test_constraints_and_history_on_refined_mesh_match_oracle():
+    """ADMConstraints on every block (each with its own spacing) after a step
+    with constraints, and the history norms summed over blocks of both
+    levels, each weighted by its own cell volume."""
+    mesh, ctx, params = _refined_binary()
+    ctx.evolve(mesh.new_dt(0.25), 1, with_constraints=True)
+    u = ctx.download(Z.REG_U)
+    adm = ctx.download(Z.REG_ADM)
+    con = ctx.download(Z.REG_CON)
+    got = ctx.hst_norms()
+    p = O.default_params(**params)
+    blocks = []
+    ref_con = np.empty_like(con)
+    for b in range(mesh.nblocks):
+        xs, dxs = mesh.block_coords(b)
+        blk = O.Block(mesh.nx, dxs, xs)
+        blocks.append(blk)
+        ref_con[b] = O.adm_constraints(blk, p, adm[b], u[b])
+    assert rel_err(con, ref_con) <= 1e-11
+    ref = O.hst_norms(blocks, p, ref_con, u)
+    np.testing.assert_allclose(got, ref, rtol=1e-9)
+    assert got[0] > 0
+    ctx.close()
