@@ -591,6 +591,21 @@ int z4c_create_refined(const z4c_mesh_desc_t* mesh, int nblocks, const long long
   return create_impl(mesh, params, integrator, nblocks, locs, out);
 }
 
+int z4c_restart_locs(const char* path, long long* locs, int cap) {
+  if (!path) return fail(Z4C_EINVAL, "null argument");
+  z4c_restart_info_t info;
+  std::string text, err;
+  std::vector<long long> l;
+  const int rc = restart_read_file(path, &info, &text, nullptr, &err, &l);
+  if (rc) return fail(rc, "%s", err.c_str());
+  if (locs) {
+    if (cap < info.nbtotal) return fail(Z4C_EINVAL, "room for %d MeshBlocks, the file has %d", cap,
+                                        info.nbtotal);
+    std::memcpy(locs, l.data(), sizeof(long long) * l.size());
+  }
+  return info.nbtotal;
+}
+
 int z4c_mesh_loc_coords(const z4c_mesh_desc_t* mesh, const long long loc[4], int axis,
                         double* x_out, double* dx_out) {
   if (!mesh || !loc || !x_out || axis < 0 || axis > 2) return fail(Z4C_EINVAL, "bad argument");
@@ -1180,16 +1195,18 @@ int z4c_tracker_add(z4c_ctx* ctx, const double pos[3], int* id) {
 
 int z4c_restart_load(z4c_ctx* ctx, const char* path, z4c_restart_info_t* info_out) {
   if (!ctx || !path) return fail(Z4C_EINVAL, "null argument");
-  if (ctx->ml) return fail(Z4C_EINVAL, "restart files need a uniform mesh");
   z4c_restart_info_t info;
   std::string text, err;
   std::vector<double> u;
-  int rc = restart_read_file(path, &info, &text, &u, &err);
+  std::vector<long long> locs;
+  int rc = restart_read_file(path, &info, &text, &u, &err, &locs);
   if (rc) return fail(rc, "%s", err.c_str());
   for (int a = 0; a < 3; ++a)
-    if (info.nb[a] != ctx->g.nb[a] || info.block_nx[a] != ctx->g.nx[a] ||
+    if (info.nb[a] != ctx->desc.nb[a] || info.block_nx[a] != ctx->g.nx[a] ||
         info.xmin[a] != ctx->desc.xmin[a] || info.xmax[a] != ctx->desc.xmax[a])
       return fail(Z4C_EINVAL, "restart file %s holds another mesh than this context's", path);
+  if ((info.nlevels > 1) != (ctx->ml != nullptr) || (ctx->ml && locs != ctx->locs))
+    return fail(Z4C_EINVAL, "restart file %s holds other MeshBlocks than this context's", path);
   if (ctx->ntrk != 0 && ctx->ntrk != info.ntrackers)
     return fail(Z4C_ESTATE, "the context has %d trackers, the restart file %d", ctx->ntrk,
                 info.ntrackers);
@@ -1211,7 +1228,6 @@ int z4c_restart_load(z4c_ctx* ctx, const char* path, z4c_restart_info_t* info_ou
 int z4c_restart_save(z4c_ctx* ctx, const char* path, const char* par_text, double time,
                      double dt, int ncycle) {
   if (!ctx || !path) return fail(Z4C_EINVAL, "null argument");
-  if (ctx->ml) return fail(Z4C_EINVAL, "restart files need a uniform mesh");
   std::vector<double> u((size_t)reg_elems(ctx, Z4C_REG_U));
   std::vector<double> trk((size_t)8 * (ctx->ntrk > 0 ? ctx->ntrk : 1));
   CUDA_TRY(cudaMemcpyAsync(u.data(), ctx->reg[Z4C_REG_U], sizeof(double) * u.size(),
@@ -1225,7 +1241,8 @@ int z4c_restart_save(z4c_ctx* ctx, const char* path, const char* par_text, doubl
     for (int q = 0; q < 6; ++q) t6[6 * t + q] = trk[8 * t + q];
   std::string err;
   const int rc = restart_write_file(path, par_text ? par_text : "", ctx->desc, u.data(), time, dt,
-                                    ncycle, ctx->ntrk, t6.data(), &err);
+                                    ncycle, ctx->ntrk, t6.data(), &err,
+                                    ctx->ml ? ctx->locs.data() : nullptr, ctx->g.nblocks);
   if (rc) return fail(rc, "%s", err.c_str());
   return Z4C_OK;
 }

@@ -81,7 +81,8 @@ int level_for(int nb) {
 }  // namespace
 
 int restart_read_file(const char* path, z4c_restart_info_t* info, std::string* text,
-                      std::vector<double>* u_grid, std::string* err) {
+                      std::vector<double>* u_grid, std::string* err,
+                      std::vector<long long>* locs) {
   FILE* fp = std::fopen(path, "rb");
   if (!fp) return fail(err, std::string("cannot open restart file ") + path);
   std::fseek(fp, 0, SEEK_END);
@@ -158,15 +159,59 @@ int restart_read_file(const char* path, z4c_restart_info_t* info, std::string* t
     return fail(err, "restart file: short read");
   }
   std::vector<int64_t> loc3((size_t)3 * I.nbtotal);
+  std::vector<int> levels((size_t)I.nbtotal);
   for (int a = 0; a < 3; ++a) I.nb[a] = 0;
+  I.nlevels = 1;
+  int maxlev = I.root_level;
   for (int b = 0; b < I.nbtotal; ++b) {
-    int level = 0;
     std::memcpy(&loc3[3 * (size_t)b], &ids[(size_t)(kIdBytes * b)], 24);
-    std::memcpy(&level, &ids[(size_t)(kIdBytes * b) + 24], 4);
-    if (level != I.root_level) {
+    std::memcpy(&levels[b], &ids[(size_t)(kIdBytes * b) + 24], 4);
+    if (levels[b] < I.root_level || levels[b] > I.root_level + 20) {
       std::fclose(fp);
-      return fail(err, "restart file: MeshBlocks above the root level (refined meshes) are not supported");
+      return fail(err, "restart file: MeshBlock level out of range");
     }
+    maxlev = levels[b] > maxlev ? levels[b] : maxlev;
+  }
+  if (locs) {
+    locs->resize((size_t)4 * I.nbtotal);
+    for (int b = 0; b < I.nbtotal; ++b) {
+      (*locs)[4 * (size_t)b] = levels[b];
+      for (int a = 0; a < 3; ++a) (*locs)[4 * (size_t)b + 1 + a] = loc3[3 * (size_t)b + a];
+    }
+  }
+  if (maxlev > I.root_level) {
+    // a refined mesh: the root grid from the <meshblock> size of the
+    // parameter text, the blocks' data in gid order as stored
+    I.nlevels = maxlev - I.root_level + 1;
+    for (int a = 0; a < 3; ++a) {
+      const std::string v = param(text ? *text : std::string(), "meshblock",
+                                  std::string("nx") + char('1' + a));
+      I.block_nx[a] = v.empty() ? 0 : std::atoi(v.c_str());
+      if (I.block_nx[a] < 1 || I.mesh_nx[a] % I.block_nx[a]) {
+        std::fclose(fp);
+        return fail(err, "restart file: refined mesh without a <meshblock> size that divides the mesh");
+      }
+      I.nb[a] = I.mesh_nx[a] / I.block_nx[a];
+    }
+    const int64_t nvol = (int64_t)(I.block_nx[0] + 1 + 2 * Z4C_NG) *
+                         (I.block_nx[1] + 1 + 2 * Z4C_NG) * (I.block_nx[2] + 1 + 2 * Z4C_NG);
+    if ((int64_t)ds != (int64_t)Z4C_NVAR * nvol * 8) {
+      std::fclose(fp);
+      return fail(err, "restart file: MeshBlock data is not exactly the vertex-centred Z4c state "
+                       "(other physics or user MeshBlock data)");
+    }
+    if (u_grid) {
+      u_grid->assign((size_t)(Z4C_NVAR * nvol * I.nbtotal), 0.0);
+      if (std::fread(u_grid->data(), 1, (size_t)ds * I.nbtotal, fp) != (size_t)ds * I.nbtotal) {
+        std::fclose(fp);
+        return fail(err, "restart file: short read");
+      }
+    }
+    std::fclose(fp);
+    *info = I;
+    return Z4C_OK;
+  }
+  for (int b = 0; b < I.nbtotal; ++b) {
     for (int a = 0; a < 3; ++a) {
       const int64_t l = loc3[3 * (size_t)b + a];
       if (l < 0 || l >= (int64_t)1 << 20) {
@@ -217,7 +262,8 @@ int restart_read_file(const char* path, z4c_restart_info_t* info, std::string* t
 
 int restart_write_file(const char* path, const std::string& text_in, const z4c_mesh_desc_t& m,
                        const double* u_grid, double time, double dt, int ncycle, int ntrk,
-                       const double* trk6, std::string* err) {
+                       const double* trk6, std::string* err, const long long* locs,
+                       int nblocks_refined) {
   // the parameter text, cut after the byte that follows its first
   // "<par_end>" (appended when the text has none)
   std::string text = text_in;
@@ -234,7 +280,7 @@ int restart_write_file(const char* path, const std::string& text_in, const z4c_m
   if (npunct != ntrk)
     return fail(err, "restart write: the parameter text has npunct = " + std::to_string(npunct) +
                          " but the state has " + std::to_string(ntrk) + " tracker(s)");
-  const int nbt = m.nb[0] * m.nb[1] * m.nb[2];
+  const int nbt = locs ? nblocks_refined : m.nb[0] * m.nb[1] * m.nb[2];
   const int64_t nvol = (int64_t)(m.nx[0] + 1 + 2 * Z4C_NG) * (m.nx[1] + 1 + 2 * Z4C_NG) *
                        (m.nx[2] + 1 + 2 * Z4C_NG);
   const uint64_t ds = (uint64_t)(Z4C_NVAR * nvol * 8);
@@ -261,6 +307,23 @@ int restart_write_file(const char* path, const std::string& text_in, const z4c_m
   std::memcpy(h + o, &ds, 8);
   ok = ok && std::fwrite(h, 1, kHeaderBytes, fp) == (size_t)kHeaderBytes;
   if (ntrk > 0) ok = ok && std::fwrite(trk6, 8, (size_t)(6 * ntrk), fp) == (size_t)(6 * ntrk);
+  if (locs) {  // a refined mesh: its blocks are already in gid order
+    for (int b = 0; b < nbt; ++b) {
+      unsigned char id[kIdBytes];
+      std::memset(id, 0, sizeof(id));
+      const int64_t l[3] = {locs[4 * b + 1], locs[4 * b + 2], locs[4 * b + 3]};
+      const int lev = (int)locs[4 * b];
+      const double cost = 1.0;
+      std::memcpy(id, l, 24);
+      std::memcpy(id + 24, &lev, 4);
+      std::memcpy(id + 32, &cost, 8);
+      ok = ok && std::fwrite(id, 1, kIdBytes, fp) == (size_t)kIdBytes;
+    }
+    ok = ok && std::fwrite(u_grid, 1, (size_t)ds * nbt, fp) == (size_t)ds * nbt;
+    ok = (std::fclose(fp) == 0) && ok;
+    if (!ok) return fail(err, std::string("restart write failed: ") + path);
+    return Z4C_OK;
+  }
   // blocks in gid order: the Morton order of the logical locations
   std::vector<int> order;
   for (int64_t key = 0; (int)order.size() < nbt; ++key) {

@@ -45,7 +45,7 @@ EXPORTS = (
     "z4c_params_default", "z4c_last_error", "z4c_create", "z4c_destroy",
     "z4c_set_stream", "z4c_sync", "z4c_num_blocks", "z4c_block_nn", "z4c_reg_nvar",
     "z4c_dx", "z4c_block_coords", "z4c_mesh_block_coords", "z4c_mesh_new_dt",
-    "z4c_mesh_loc_coords", "z4c_create_refined", "z4c_refined_neighbours", "z4c_upload", "z4c_download", "z4c_device_ptr",
+    "z4c_mesh_loc_coords", "z4c_create_refined", "z4c_refined_neighbours", "z4c_restart_locs", "z4c_upload", "z4c_download", "z4c_device_ptr",
     "z4c_rhs", "z4c_boundary_rhs", "z4c_add_rhs", "z4c_weighted_ave", "z4c_alg_constr", "z4c_adm_to_z4c",
     "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_weyl", "z4c_ghost_fill", "z4c_init_finalize",
     "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
@@ -83,7 +83,7 @@ class RestartInfo(C.Structure):
                 ("time", C.c_double), ("dt", C.c_double), ("ncycle", C.c_int),
                 ("datasize", C.c_ulonglong), ("nb", C.c_int * 3), ("block_nx", C.c_int * 3),
                 ("ntrackers", C.c_int), ("trackers", (C.c_double * 6) * 8),
-                ("text_bytes", C.c_longlong)]
+                ("text_bytes", C.c_longlong), ("nlevels", C.c_int)]
 
 
 class MeshDesc(C.Structure):
@@ -121,6 +121,7 @@ def lib():
                                           dp]
         L.z4c_create_refined.argtypes = [C.POINTER(MeshDesc), ip, C.POINTER(C.c_longlong),
                                          C.POINTER(Params), ip, C.POINTER(vp)]
+        L.z4c_restart_locs.argtypes = [C.c_char_p, C.POINTER(C.c_longlong), ip]
         L.z4c_refined_neighbours.argtypes = [C.POINTER(MeshDesc), ip, C.POINTER(C.c_longlong),
                                              ip, C.POINTER(C.c_int)]
         L.z4c_upload.argtypes = [vp, ip, ip, dp]
@@ -350,7 +351,14 @@ class Mesh:
             for side in ("i", "o"):
                 v = _param(text, "mesh", f"{side}x{a}_bc")
                 bc.append(BC_NAMES[v or "periodic"])
-        return cls(info["nb"], info["block_nx"], info["xmin"], info["xmax"], bc)
+        mesh = cls(info["nb"], info["block_nx"], info["xmin"], info["xmax"], bc)
+        if info["nlevels"] > 1:  # a refined mesh: its blocks as the file lists them
+            n = _check(lib().z4c_restart_locs(path.encode(), None, 0))
+            locs = np.zeros((n, 4), dtype=np.int64)
+            _check(lib().z4c_restart_locs(path.encode(),
+                                          locs.ctypes.data_as(C.POINTER(C.c_longlong)), n))
+            mesh.locs = locs
+        return mesh
 
 
 def _param(text, block, key):
@@ -372,7 +380,7 @@ def _info_dict(I):
     return dict(nbtotal=I.nbtotal, root_level=I.root_level, xmin=tuple(I.xmin),
                 xmax=tuple(I.xmax), xrat=tuple(I.xrat), mesh_nx=tuple(I.mesh_nx), time=I.time,
                 dt=I.dt, ncycle=I.ncycle, datasize=I.datasize, nb=tuple(I.nb),
-                block_nx=tuple(I.block_nx),
+                block_nx=tuple(I.block_nx), nlevels=I.nlevels,
                 trackers=[tuple(I.trackers[t]) for t in range(I.ntrackers)])
 
 

@@ -150,8 +150,8 @@ int z4c_create(const z4c_mesh_desc_t *mesh, const z4c_params_t *params,
  * run the reference's multilevel vertex-centred exchange
  * (comm/comm_registry.cpp:246-382, 533-570; comm/refinement_ops.cpp:24-195;
  * comm/node_multiplicity.cpp; comm/physical_bcs.cpp:506-890).  Outflow,
- * periodic and gr_sommerfeld faces, puncture trackers and psi4 spheres;
- * restart files need a uniform mesh. */
+ * periodic and gr_sommerfeld faces, puncture trackers, psi4 spheres and
+ * restart files. */
 int z4c_create_refined(const z4c_mesh_desc_t *mesh, int nblocks, const long long *locs,
                        const z4c_params_t *params, int integrator, z4c_ctx **out);
 /* The neighbour list z4c_create_refined builds for one block of a refined
@@ -187,6 +187,11 @@ int z4c_mesh_block_coords(const z4c_mesh_desc_t *mesh, int block, int axis, doub
 /* Vertex coordinates (nx + 1 + 2 NG) and spacing of the block at logical
  * location loc = {level, lx1, lx2, lx3} along one axis
  * (coordinates/coordinates.cpp:125-198, mesh/mesh.cpp:2526-2560). */
+/* The MeshBlocks of a restart file, {level, lx1, lx2, lx3} each in gid
+ * order, into locs (room for cap); returns their count (locs may be NULL to
+ * ask for it).  A refined mesh's file restarts into a z4c_create_refined
+ * context over these blocks. */
+int z4c_restart_locs(const char *path, long long *locs, int cap);
 int z4c_mesh_loc_coords(const z4c_mesh_desc_t *mesh, const long long loc[4], int axis,
                         double *x_out, double *dx_out);
 int z4c_mesh_new_dt(const z4c_mesh_desc_t *mesh, double cfl, double *dt_out);
@@ -254,6 +259,7 @@ typedef struct z4c_restart_info {
   int ntrackers;         /* puncture trackers (<z4c> npunct) */
   double trackers[Z4C_MAX_TRACKERS][6];  /* position, shift there (pos, betap) */
   long long text_bytes;  /* parameter text through the byte after <par_end> */
+  int nlevels;           /* refinement levels present (1: a uniform mesh) */
 } z4c_restart_info_t;
 /* Reads the header of a restart file (no context). */
 int z4c_restart_info(const char *path, z4c_restart_info_t *info);

@@ -16,6 +16,9 @@ Fixtures (numpy .npz, compressed):
                     and after its one RK4 step; psi4 extraction (ghost
                     exchange of the Weyl register, sphere interpolation and
                     (l, m) projection) of the latter
+  restart_ml.npz    the reference's restart file after one step on the
+                    two-level mesh of ml_exchange_outflow, without its
+                    MeshBlock data
   restart_track4.npz  the reference's restart file of the evol_track4 run
                     without its MeshBlock data (that is evol_track4's final
                     state)
@@ -322,6 +325,28 @@ def make_restart(outdir):
     return path
 
 
+def make_restart_ml(outdir):
+    """The restart file the stock reference driver writes after one step
+    on the outflow two-level mesh of ml_exchange_outflow: everything before
+    the MeshBlock data (parameter text, header, ID list with the blocks'
+    levels) is stored."""
+    case = dict(REFINE, bc="extrapolate_outflow")
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = os.path.join(tmp, "case.inp")
+        text = deck(case, "unused", nlim=1).replace("refinement = none", "refinement = static")
+        text += RST_DECK + "<refinement1>\n" + "".join(f"{k} = {v}\n" for k, v in ML_REGION.items())
+        with open(inp, "w") as f:
+            f.write(text)
+        subprocess.run([os.path.join(REF_BIN, "athena_ref"), "-i", inp], cwd=tmp, check=True,
+                       stdout=subprocess.DEVNULL)
+        raw = open(os.path.join(tmp, "golden.final.rst"), "rb").read()
+    nbytes = 15 * 22 * 17 ** 3 * 8
+    prefix = np.frombuffer(raw[:len(raw) - nbytes], dtype=np.uint8)
+    path = os.path.join(outdir, "restart_ml.npz")
+    np.savez_compressed(path, prefix=prefix, data_bytes=nbytes)
+    return path
+
+
 def main():
     only = set(sys.argv[1:])  # fixture names to (re)make; all when empty
     if not only or "weyl_punc2" in only:
@@ -345,6 +370,9 @@ def main():
         if not only or f"ml_exchange_{tag}" in only:
             p = make_multilevel(bc, HERE)
             print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
+    if not only or "restart_ml" in only:
+        p = make_restart_ml(HERE)
+        print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
     if not only or "restart_track4" in only:  # needs evol_track4
         p = make_restart(HERE)
         print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")

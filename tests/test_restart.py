@@ -132,3 +132,48 @@ def test_context_load_evolve_save(tmp_path):
     assert ctx.check_finite()
     assert np.linalg.norm(ctx.tracker(0)[0] - pos) > 0
     ctx.close()
+
+
+def _reference_ml_file(tmp_path):
+    """The reference's restart file of the two-level mesh with an
+    integer-hash state in its data section (blocks in gid order)."""
+    z = np.load(os.path.join(GOLDEN, "restart_ml.npz"))
+    g, n, k, j, i = np.meshgrid(np.arange(15), np.arange(22), np.arange(17), np.arange(17),
+                                np.arange(17), indexing="ij")
+    u = ((g * 131 + n * 31 + k * 7 + j * 3 + i) % 1009) / 1009.0 - 0.5
+    assert u.nbytes == int(z["data_bytes"])
+    path = tmp_path / "golden.final.rst"
+    path.write_bytes(z["prefix"].tobytes() + u.astype("<f8").tobytes())
+    return str(path), u
+
+
+def test_refined_mesh_file_is_read():
+    """The ID list of a refined mesh's restart file: levels and locations
+    of the 15 blocks, the root grid from the <meshblock> size."""
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        from pathlib import Path
+        path, _ = _reference_ml_file(Path(d))
+        info = Z.restart_info(path)
+        assert info["nlevels"] == 2 and info["nbtotal"] == 15
+        assert info["nb"] == (2, 2, 2) and info["block_nx"] == (8, 8, 8)
+        mesh = Z.Mesh.from_restart(path)
+        ml = np.load(os.path.join(GOLDEN, "ml_exchange_outflow.npz"))
+        assert np.array_equal(mesh.locs, ml["meta"][:, 1:5])
+        assert mesh.nblocks == 15 and mesh.root_level == 1
+
+
+@pytest.mark.gpu
+def test_refined_context_load_save(tmp_path):
+    """A refined context restarts from the reference's file (state in gid
+    order) and writes it back byte for byte except for padding."""
+    path, u = _reference_ml_file(tmp_path)
+    mesh = Z.Mesh.from_restart(path)
+    ctx = Z.Z4c(mesh, Z.default_params(chi_div_floor=1e-5), "rk4")
+    info = ctx.restart_load(path)
+    assert np.array_equal(ctx.download(Z.REG_U), u)
+    out = tmp_path / "saved.rst"
+    text = Z.restart_text(path)
+    ctx.restart_save(str(out), text, info["time"], info["dt"], info["ncycle"])
+    assert _same_but_padding(out.read_bytes(), open(path, "rb").read(), len(text), 0, 15)
+    ctx.close()
