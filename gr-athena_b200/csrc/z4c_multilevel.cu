@@ -83,18 +83,18 @@ __device__ __forceinline__ int ml_zone(int i, int vs, int ve) {
 // buffer.  A warp walks rows of the array, its lanes along i.
 __global__ void k_ml_unpack(MlPlan P, const double* __restrict__ src, double* __restrict__ dst,
                             int reg_nvar) {
-  const int b = blockIdx.x, n = blockIdx.y;
+  const int b = blockIdx.x, n = blockIdx.y, arr = blockIdx.z;  // arr: 0 fine, 1 coarse
   __shared__ unsigned char mult[343];
-  __shared__ int zs[2][344];
-  extern __shared__ MlContrib sc[];  // this block's contributions
+  __shared__ int zs[1][344];
+  extern __shared__ MlContrib sc[];  // this array's contributions
   for (int q = threadIdx.x; q < 343; q += blockDim.x) mult[q] = P.mult[(int64_t)b * 343 + q];
-  for (int q = threadIdx.x; q < 2 * 344; q += blockDim.x)
-    zs[q / 344][q % 344] = P.zstart[(int64_t)b * 2 * 344 + q];
+  for (int q = threadIdx.x; q < 344; q += blockDim.x)
+    zs[0][q] = P.zstart[((int64_t)b * 2 + arr) * 344 + q];
   __syncthreads();
-  const int c0 = zs[0][0], nc = zs[1][343] - c0;
+  const int c0 = zs[0][0], nc = zs[0][343] - c0;
   for (int q = threadIdx.x; q < nc; q += blockDim.x) sc[q] = P.contrib[c0 + q];
   __syncthreads();
-  for (int arr = 0; arr < 2; ++arr) {
+  {
     const int ng = arr ? Z4C_NCG : NG;
     const int d0 = arr ? P.cn[0] : P.nn[0], d1 = arr ? P.cn[1] : P.nn[1];
     const int v0 = ng + (arr ? P.nx[0] / 2 : P.nx[0]), v1 = ng + (arr ? P.nx[1] / 2 : P.nx[1]),
@@ -110,7 +110,7 @@ __global__ void k_ml_unpack(MlPlan P, const double* __restrict__ src, double* __
       const int z = (zk * 7 + zj) * 7 + zi;
       const bool in = zi >= 1 && zi <= 5 && zj >= 1 && zj <= 5 && zk >= 1 && zk <= 5;
       double v = in ? __ldg(own + p) : 0.0;
-      for (int q = zs[arr][z] - c0; q < zs[arr][z + 1] - c0; ++q) {
+      for (int q = zs[0][z] - c0; q < zs[0][z + 1] - c0; ++q) {
         const MlContrib c = sc[q];
         const int64_t sv = c.scoarse ? P.cvol : P.fvol;
         const double* s = c.scoarse ? P.csrc + ((int64_t)c.sblk * Z4C_NVAR + n) * sv
@@ -800,7 +800,7 @@ int launch_ml_exchange(const MlPlan& P, const double* src, double* dst, int nvar
       cudaFuncSetAttribute(k_ml_unpack, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
     return set_error(Z4C_ECUDA, "multilevel exchange: shared memory for the contribution lists");
-  k_ml_unpack<<<dim3(P.nblocks, nvar), 256, smem, st>>>(P, src, dst, reg_nvar);
+  k_ml_unpack<<<dim3(P.nblocks, nvar, 2), 256, smem, st>>>(P, src, dst, reg_nvar);
   ++launches;
   auto bc_axis = [&](int lv, double* arr, int64_t bstride, int64_t vol, const int* dims, int ng) {
     for (int a = 0; a < 3; ++a) {
