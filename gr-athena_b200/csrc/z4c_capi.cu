@@ -8,6 +8,8 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <map>
+#include <tuple>
 #include <new>
 #include <string>
 #include <vector>
@@ -1180,6 +1182,100 @@ int z4c_evolve(z4c_ctx* ctx, double dt, int nsteps, int with_constraints) {
 }
 
 long long z4c_kernel_launches(void) { return kernel_launch_count(); }
+
+namespace {
+// {level, lx1, lx2, lx3} of every block of a context in its block order
+std::vector<long long> ctx_locs(const z4c_ctx* c) {
+  if (c->ml) return c->locs;
+  const int rl = ml_root_level(c->desc.nb);
+  std::vector<long long> l((size_t)4 * c->g.nblocks);
+  for (int b = 0; b < c->g.nblocks; ++b) {
+    l[4 * (size_t)b] = rl;
+    l[4 * (size_t)b + 1] = b % c->g.nb[0];
+    l[4 * (size_t)b + 2] = (b / c->g.nb[0]) % c->g.nb[1];
+    l[4 * (size_t)b + 3] = b / (c->g.nb[0] * c->g.nb[1]);
+  }
+  return l;
+}
+}  // namespace
+
+int z4c_regrid(z4c_ctx* dst, const z4c_ctx* src) {
+  if (!dst || !src) return fail(Z4C_EINVAL, "null context");
+  for (int a = 0; a < 3; ++a)
+    if (dst->desc.nb[a] != src->desc.nb[a] || dst->desc.nx[a] != src->desc.nx[a] ||
+        dst->desc.xmin[a] != src->desc.xmin[a] || dst->desc.xmax[a] != src->desc.xmax[a])
+      return fail(Z4C_EINVAL, "regrid: the contexts cover different root grids");
+  const std::vector<long long> dl = ctx_locs(dst), sl = ctx_locs(src);
+  std::map<std::tuple<long long, long long, long long, long long>, int> sidx;
+  for (int b = 0; b < src->g.nblocks; ++b)
+    sidx[std::make_tuple(sl[4 * b], sl[4 * b + 1], sl[4 * b + 2], sl[4 * b + 3])] = b;
+  // every destination block: the same block, a child of a source block or
+  // the parent of eight source blocks (one level per regrid, as the reference)
+  struct Move { int kind, from[8], oct[8][3]; };
+  std::vector<Move> moves((size_t)dst->g.nblocks);
+  for (int b = 0; b < dst->g.nblocks; ++b) {
+    const long long lv = dl[4 * b], x = dl[4 * b + 1], y = dl[4 * b + 2], z = dl[4 * b + 3];
+    Move& m = moves[b];
+    auto it = sidx.find(std::make_tuple(lv, x, y, z));
+    if (it != sidx.end()) { m.kind = 0; m.from[0] = it->second; continue; }
+    it = sidx.find(std::make_tuple(lv - 1, x >> 1, y >> 1, z >> 1));
+    if (it != sidx.end()) {
+      m.kind = 1;
+      m.from[0] = it->second;
+      m.oct[0][0] = (int)(x & 1); m.oct[0][1] = (int)(y & 1); m.oct[0][2] = (int)(z & 1);
+      continue;
+    }
+    m.kind = 2;
+    for (int c = 0; c < 8; ++c) {
+      const int o[3] = {c & 1, (c >> 1) & 1, (c >> 2) & 1};
+      it = sidx.find(std::make_tuple(lv + 1, 2 * x + o[0], 2 * y + o[1], 2 * z + o[2]));
+      if (it == sidx.end())
+        return fail(Z4C_EINVAL, "regrid: block %d is neither kept, refined nor derefined "
+                                "by one level", b);
+      m.from[c] = it->second;
+      for (int a = 0; a < 3; ++a) m.oct[c][a] = o[a];
+    }
+  }
+  double* scratch = nullptr;
+  const int64_t cvol = (int64_t)(dst->g.nx[0] / 2 + 1 + 2 * Z4C_NCG) *
+                       (dst->g.nx[1] / 2 + 1 + 2 * Z4C_NCG) * (dst->g.nx[2] / 2 + 1 + 2 * Z4C_NCG);
+  if (cudaMalloc((void**)&scratch, sizeof(double) * Z4C_NVAR * cvol) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(Z4C_ENOMEM, "regrid: coarse scratch");
+  }
+  // the source's work must be complete before the destination's stream reads it
+  cudaStreamSynchronize(src->stream);
+  const int64_t bs = (int64_t)Z4C_NVAR * dst->g.nvol;
+  const double* su = src->reg[Z4C_REG_U];
+  double* du = dst->reg[Z4C_REG_U];
+  int rc = Z4C_OK;
+  for (int b = 0; b < dst->g.nblocks && rc == Z4C_OK; ++b) {
+    const Move& m = moves[b];
+    if (m.kind == 0) {
+      if (cudaMemcpyAsync(du + b * bs, su + m.from[0] * bs, sizeof(double) * bs,
+                          cudaMemcpyDeviceToDevice, dst->stream) != cudaSuccess)
+        rc = fail(Z4C_ECUDA, "regrid: block copy");
+    } else if (m.kind == 1) {
+      rc = z4c_regrid_refine(su + m.from[0] * bs, du + b * bs, scratch, Z4C_NVAR, dst->g.nx,
+                             m.oct[0], dst->stream);
+    } else {
+      for (int c = 0; c < 8 && rc == Z4C_OK; ++c)
+        rc = z4c_regrid_derefine(su + m.from[c] * bs, du + b * bs, scratch, Z4C_NVAR, dst->g.nx,
+                                 m.oct[c], dst->stream);
+    }
+  }
+  // the puncture trackers move with the state
+  if (rc == Z4C_OK && src->ntrk > 0 &&
+      cudaMemcpyAsync(dst->trk, src->trk, sizeof(double) * 8 * src->ntrk,
+                      cudaMemcpyDeviceToDevice, dst->stream) != cudaSuccess)
+    rc = fail(Z4C_ECUDA, "regrid: trackers");
+  cudaStreamSynchronize(dst->stream);
+  cudaFree(scratch);
+  if (rc) return rc;
+  dst->ntrk = src->ntrk;
+  drop_graph(dst);
+  return Z4C_OK;
+}
 
 int z4c_tracker_add(z4c_ctx* ctx, const double pos[3], int* id) {
   if (!ctx || !pos || !id) return fail(Z4C_EINVAL, "null argument");

@@ -45,7 +45,8 @@ EXPORTS = (
     "z4c_params_default", "z4c_last_error", "z4c_create", "z4c_destroy",
     "z4c_set_stream", "z4c_sync", "z4c_num_blocks", "z4c_block_nn", "z4c_reg_nvar",
     "z4c_dx", "z4c_block_coords", "z4c_mesh_block_coords", "z4c_mesh_new_dt",
-    "z4c_mesh_loc_coords", "z4c_create_refined", "z4c_refined_neighbours", "z4c_restart_locs", "z4c_upload", "z4c_download", "z4c_device_ptr",
+    "z4c_mesh_loc_coords", "z4c_create_refined", "z4c_refined_neighbours", "z4c_restart_locs",
+    "z4c_regrid", "z4c_upload", "z4c_download", "z4c_device_ptr",
     "z4c_rhs", "z4c_boundary_rhs", "z4c_add_rhs", "z4c_weighted_ave", "z4c_alg_constr", "z4c_adm_to_z4c",
     "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_weyl", "z4c_ghost_fill", "z4c_init_finalize",
     "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
@@ -122,6 +123,7 @@ def lib():
         L.z4c_create_refined.argtypes = [C.POINTER(MeshDesc), ip, C.POINTER(C.c_longlong),
                                          C.POINTER(Params), ip, C.POINTER(vp)]
         L.z4c_restart_locs.argtypes = [C.c_char_p, C.POINTER(C.c_longlong), ip]
+        L.z4c_regrid.argtypes = [vp, vp]
         L.z4c_refined_neighbours.argtypes = [C.POINTER(MeshDesc), ip, C.POINTER(C.c_longlong),
                                              ip, C.POINTER(C.c_int)]
         L.z4c_upload.argtypes = [vp, ip, ip, dp]
@@ -695,6 +697,13 @@ class Z4c:
         for w in spheres:
             w.ReduceMultipole()
         return [w.psi for w in spheres]
+
+    def regrid_from(self, old):
+        """Carry the state and trackers of context `old` into this context
+        (the regridded mesh), then fill the ghosts (z4c_regrid +
+        z4c_init_finalize)."""
+        _check(lib().z4c_regrid(self._h, old._h))
+        self.init_finalize()
 
     def hst_norms(self):
         out = np.empty(8)

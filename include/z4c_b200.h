@@ -413,6 +413,16 @@ int z4c_regrid_refine(const double *parent, double *child, double *coarse, int n
 int z4c_regrid_derefine(const double *child, double *parent, double *coarse, int nvar,
                         const int nx[3], const int oct[3], void *stream);
 
+/* Regrid (AMRTransfer after MeshBlockTree refinement / derefinement,
+ * comm/amr_transfer.cpp:373-412, comm/amr_registry.cpp:814-1233): the Z4c
+ * state and the puncture trackers of src carried into dst, a context over the
+ * regridded block list of the same root grid (uniform or refined).  Every
+ * block of dst is a block of src (copied), a child of one (refined from it)
+ * or the parent of eight (derefined from them).  Interiors only; call
+ * z4c_init_finalize(dst) after it for the ghosts, as the reference exchanges
+ * after a regrid. */
+int z4c_regrid(z4c_ctx *dst, const z4c_ctx *src);
+
 /* ---- allocation-free variant ----------------------------------------------
  *
  * No counterpart in the reference: an addition for callers that cannot call

@@ -334,3 +334,54 @@ def test_constraints_and_history_on_refined_mesh_match_oracle():
     np.testing.assert_allclose(got, ref, rtol=1e-9)
     assert got[0] > 0
     ctx.close()
+
+
+@pytest.mark.gpu
+def test_regrid_moves_the_refined_region_like_the_oracle():
+    """A regrid that derefines the refined root block and refines another
+    one: kept blocks copied, the new children prolonged from their parent
+    (FillSameRankCoarseToFine), the new parent restricted from its eight
+    children (FillSameRankFineToCoarse), then the ghost fill of the new
+    mesh; against the oracle's transfers and exchange, and the tracker
+    carried along."""
+    mesh, ctx, params = _refined_binary()
+    ctx.add_tracker((0.31, 0.27, -0.22))
+    ctx.evolve(mesh.new_dt(0.25), 1)
+    old = ctx.download(Z.REG_U)
+    trk = ctx.tracker(0)
+    moved = Z.Mesh(mesh.nb, mesh.nx, mesh.xmin, mesh.xmax, mesh.bc,
+                   refinement=[dict(x1min=-3.5, x1max=-0.5, x2min=0.5, x2max=3.5, x3min=0.5,
+                                    x3max=3.5, level=1)])
+    new = Z.Z4c(moved, Z.default_params(**params), "rk4")
+    new.regrid_from(ctx)
+    got = new.download(Z.REG_U)
+    # the oracle: transfers block by block, then exchange + AlgConstr on ghosts
+    sidx = {tuple(l): b for b, l in enumerate(mesh.locs.tolist())}
+    ref = np.zeros_like(got)
+    kinds = set()
+    for b, (lv, x, y, z) in enumerate(moved.locs.tolist()):
+        if (lv, x, y, z) in sidx:
+            ref[b] = old[sidx[(lv, x, y, z)]]
+            kinds.add("kept")
+        elif (lv - 1, x >> 1, y >> 1, z >> 1) in sidx:
+            ref[b] = O.regrid_refine(mesh.nx, old[sidx[(lv - 1, x >> 1, y >> 1, z >> 1)]],
+                                     ref[b], (x & 1, y & 1, z & 1))
+            kinds.add("refined")
+        else:
+            for c in range(8):
+                o = (c & 1, (c >> 1) & 1, (c >> 2) & 1)
+                ch = sidx[(lv + 1, 2 * x + o[0], 2 * y + o[1], 2 * z + o[2])]
+                ref[b] = O.regrid_derefine(mesh.nx, old[ch], ref[b], o)
+            kinds.add("derefined")
+    assert kinds == {"kept", "refined", "derefined"}
+    ref = O.ml_exchange(moved.nb, moved.root_level, moved.nx, moved.bc, moved.locs, ref)
+    p = O.default_params(**params)
+    for b in range(moved.nblocks):
+        xs, dxs = moved.block_coords(b)
+        ref[b] = O.algconstr(O.Block(moved.nx, dxs, xs), p, ref[b], ghosts_only=True)
+    assert rel_err(got, ref) <= 1e-14
+    np.testing.assert_array_equal(np.concatenate(new.tracker(0)), np.concatenate(trk))
+    new.evolve(moved.new_dt(0.25), 1)
+    assert new.check_finite()
+    ctx.close()
+    new.close()
