@@ -6,8 +6,13 @@ domain [-16, 16]^3, extrapolate_outflow boundaries, 1+log slicing and
 Gamma-driver shift (eta = 2), kappa1 = 0.02, KO dissipation 0.02, low-storage
 RK4, Courant 0.25.  One step = one full RK4 step of the whole mesh (four
 stages: fused RHS+KO+stage update, ghost exchange, boundary conditions,
-AlgConstr), replayed from a captured CUDA graph.  A zone-update is one cell
+AlgConstr; Z4cToADM after the last stage, as the task list runs it every
+step), replayed from a captured CUDA graph.  A zone-update is one cell
 advanced one full step (the reference's zone-cycle, main.cpp:239).
+
+At N = 1 the line also carries "bbh_smr": the refined binary-puncture mesh
+below (3,424 MeshBlocks on seven levels), its own zone-updates/s and the time
+of one multilevel ghost fill (--no-smr skips it).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -17,9 +22,13 @@ value is the total over ranks divided by the slowest rank's time.
 
   python bench.py --workload bbh_smr [--steps K] [--warmup W]
 
-prints a separate line for binary punctures on a statically refined mesh of
-3,424 MeshBlocks on seven levels (SMR_REGIONS): zone-updates/s of the
-graph-captured RK4 step and the time of one multilevel ghost fill; one GPU.
+prints that measurement alone as a line of its own; one GPU.
+
+The CPU baseline and --impl reference time the reference's own OpenMP build
+(oracle/_ref/athena_ref_native: the reference's g++ flags with -march=native
+of the machine that built it) on all host cores; a host whose cores lack one
+of that machine's CPU flags times the portable build (-march=x86-64-v3)
+instead, and the line says which.
 """
 import argparse
 import json
@@ -46,6 +55,12 @@ WORKLOAD = dict(workload="single puncture M=1, 128^3 cells as 512 MeshBlocks of 
 PARAMS = dict(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02, damp_kappa2=0.0,
               shift_eta=2.0, r_max_con=1e300)
 CFL = 0.25
+# RK4 steps of the reference CPU build in the cpu_baseline leg (about 2 s of
+# work per step on 16 cores)
+CPU_SAMPLE_STEPS = 8
+# timed RK4 steps of the refined-mesh measurement inside the headline run
+# (about 150 ms each)
+SMR_STEPS = 10
 # Algorithmic HBM bytes of one fused stage per interior vertex: read u and u1,
 # write u' and u1' (22 FP64 variables each).
 STAGE_BYTES_PER_POINT = 4 * 22 * 8
@@ -74,6 +89,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-smr", action="store_true",
+                    help="skip the refined binary-puncture measurement of the headline line")
     ap.add_argument("--nb", type=int, default=8,
                     help="MeshBlocks per axis (8 = the 128^3 workload; smaller for profiling)")
     ap.add_argument("--profile-run", action="store_true",
@@ -166,13 +183,43 @@ def reference_deck(nlim, threads):
     return "\n".join(lines) + "\n"
 
 
+def reference_binary():
+    """The reference build to time and how it was built: athena_ref_native
+    (the reference's own g++ flags, -march=native of the machine that built
+    it) when this host's cores have every CPU flag of that machine, else the
+    portable athena_ref (-O3 -march=x86-64-v3)."""
+    ref = os.path.join(ROOT, "oracle", "_ref")
+    native = os.path.join(ref, "athena_ref_native")
+    if os.path.exists(native) and os.path.exists(native + ".isa"):
+        with open(native + ".isa") as f:
+            need = set(f.read().split())
+        have = set()
+        try:
+            with open("/proc/cpuinfo") as f:
+                for line in f:
+                    if line.startswith("flags"):
+                        have = set(line.split(":", 1)[1].split())
+                        break
+        except OSError:
+            pass
+        if need and need <= have:
+            return native, ("reference g++ flags (-O3 -fwhole-program -flto=auto "
+                            "-fprefetch-loop-arrays -march=native -ffp-contract=off)")
+        missing = sorted(need - have)[:5]
+        note = f"portable build: this host lacks CPU flags of the native build ({missing})"
+    else:
+        note = "portable build (-O3 -march=x86-64-v3): no native build present"
+    exe = os.path.join(ref, "athena_ref")
+    return (exe if os.path.exists(exe) else None), note
+
+
 def run_reference_cpu(nlim, threads):
-    """Times the reference's own OpenMP CPU build (oracle/_ref/athena_ref,
-    compiled from the reference sources) on the benchmark workload and returns
-    its printed zone-cycles/omp_wsecond (main.hpp:739-742)."""
-    exe = os.path.join(ROOT, "oracle", "_ref", "athena_ref")
-    if not os.path.exists(exe):
-        return None
+    """Times the reference's own OpenMP CPU build (oracle/_ref, compiled from
+    the reference sources) on the benchmark workload and returns its printed
+    zone-cycles/omp_wsecond (main.hpp:739-742) and the build used."""
+    exe, build = reference_binary()
+    if exe is None:
+        return None, build
     with tempfile.TemporaryDirectory() as tmp:
         inp = os.path.join(tmp, "bench.inp")
         with open(inp, "w") as f:
@@ -182,8 +229,8 @@ def run_reference_cpu(nlim, threads):
                              env=env, timeout=1800)
     m = re.search(r"zone-cycles/omp_wsecond\s*=\s*([0-9.eE+-]+)", out.stdout)
     if not m:
-        return None
-    return float(m.group(1))
+        return None, build
+    return float(m.group(1)), build
 
 
 def run_oracle_cpu(max_seconds=20.0):
@@ -303,6 +350,10 @@ SMR_CENTRES = ((3.0, 0.0625 * 0.37, 0.0625 * 0.21), (-3.0, -0.0625 * 0.37, -0.06
 
 
 def main_smr(args):
+    print(json.dumps(smr_measure(args.steps, args.warmup, args.shape)), flush=True)
+
+
+def smr_measure(steps, warmup, shape=None):
     """Steps of the refined binary-puncture mesh: zone-updates/s through
     the graph-captured step, and the multilevel ghost exchange alone."""
     import torch
@@ -319,25 +370,25 @@ def main_smr(args):
     ID.load_adm(ctx, ID.punctures(mesh, params, masses=(0.5, 0.5), centres=SMR_CENTRES))
     ctx.sync()
     setup_s = time.time() - t0
-    if args.shape:
-        ctx.set_tile(*(int(v) for v in args.shape.split(",")))
+    if shape:
+        ctx.set_tile(*(int(v) for v in shape.split(",")))
     else:
         with torch.cuda.stream(stream):
             ctx.autotune(reps=2)
     dt = mesh.new_dt(CFL)
     with torch.cuda.stream(stream):
-        ctx.evolve(dt, args.warmup)
+        ctx.evolve(dt, warmup)
     torch.cuda.synchronize()
     sampler = ClockSampler(0)
     sampler.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     with torch.cuda.stream(stream):
-        ctx.evolve(dt, args.steps)
+        ctx.evolve(dt, steps)
     ev1.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = ev0.elapsed_time(ev1) / steps
     # the multilevel exchange alone (ghost fill of the 22-variable state)
     reps = 10
     with torch.cuda.stream(stream):
@@ -353,7 +404,7 @@ def main_smr(args):
     levels = np.bincount(mesh.locs[:, 0] - mesh.root_level).tolist()
     line = {
         "metric": "zone-updates/s", "value": mesh.zones() / (ms * 1e-3), "unit": "zone-updates/s",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": ms,
         "higher_is_better": True, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "binary punctures (m=0.5 each near (+-3,0,0)), [-512,512]^3, "
                                "4^3 root MeshBlocks of 16^3 cells, 7 nested static refinement "
@@ -367,8 +418,8 @@ def main_smr(args):
         "setup_s": setup_s, "finite": bool(ctx.check_finite()),
         "clocks": clocks,
     }
-    print(json.dumps(line), flush=True)
     ctx.close()
+    return line
 
 
 def main():
@@ -515,11 +566,11 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        v = run_reference_cpu(2, threads)
+        v, build = run_reference_cpu(CPU_SAMPLE_STEPS, threads)
         if v is not None:
             cpu = {"value": v, "unit": "zone-updates/s", "cores": threads, "kind": "reference",
-                   "sample": "reference OpenMP build (oracle/_ref/athena_ref) on the full "
-                             "workload, 2 RK4 steps, zone-cycles/omp_wsecond"}
+                   "sample": f"reference OpenMP build on the full workload, {CPU_SAMPLE_STEPS} "
+                             f"RK4 steps, zone-cycles/omp_wsecond; {build}"}
         else:
             v, n = run_oracle_cpu()
             cpu = {"value": v, "unit": "zone-updates/s", "cores": 1, "kind": "port",
@@ -568,9 +619,17 @@ def main():
         "clocks": clocks,
         "psi4": psi4,
     }
+    ctx.close()
+    if world == 1 and not args.no_smr:
+        # the refined binary-puncture mesh (configs[2]'s 7-level mesh,
+        # static): its own context after this one is released
+        smr = smr_measure(SMR_STEPS, 3)
+        line["bbh_smr"] = {k: smr[k] for k in ("value", "unit", "ms_per_step", "steps",
+                                               "exchange_ms", "exchange_share", "setup_s",
+                                               "finite", "clocks")}
+        line["bbh_smr"]["config"] = smr["config"]
     if rank == 0:
         print(json.dumps(line), flush=True)
-    ctx.close()
     if world > 1:
         dist.destroy_process_group()
 
@@ -582,9 +641,9 @@ def main_reference(args, rank, world):
         return
     threads = os.cpu_count() or 1
     nlim = max(1, args.steps)
-    v = run_reference_cpu(nlim, threads)
+    v, build = run_reference_cpu(nlim, threads)
     kind = "reference"
-    sample = f"reference OpenMP build, full workload, {nlim} RK4 steps"
+    sample = f"reference OpenMP build, full workload, {nlim} RK4 steps; {build}"
     if v is None:
         v, n = run_oracle_cpu()
         kind, threads = "port", 1

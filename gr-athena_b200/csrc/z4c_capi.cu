@@ -228,7 +228,9 @@ int run_stage_body(z4c_ctx* c, int stage, double dt);
 // One stage with the puncture trackers around it: the shift is interpolated
 // from the state at the start of the step (CalculateZ4cRHS, stage 1,
 // task_list_gr_z4c.cpp:147-153) and the positions move after the last stage
-// (EvolveTracker, main.hpp:1079-1082).
+// (EvolveTracker, main.hpp:1079-1082).  The last stage also runs the
+// Z4C_TO_ADM task, which the task list schedules on every last stage
+// (task_list_gr_z4c.cpp:335-344), so the ADM register follows every step.
 int run_stage(z4c_ctx* c, int stage, double dt) {
   if (c->ntrk > 0 && stage == 1) {
     launch_track_interp(c->g, c->dev(), c->reg[Z4C_REG_U], c->trk, c->ntrk, c->stream);
@@ -236,6 +238,17 @@ int run_stage(z4c_ctx* c, int stage, double dt) {
   }
   int rc = run_stage_body(c, stage, dt);
   if (rc) return rc;
+  if (stage == 4) {
+    const DevParams P = c->dev();
+    if (!c->per_block) {
+      launch_z4c_to_adm(c->g, P, c->reg[Z4C_REG_U], c->reg[Z4C_REG_ADM], 0, c->g.nblocks,
+                        c->stream);
+    } else {
+      for (int b = 0; b < c->g.nblocks; ++b)
+        launch_z4c_to_adm(c->g, P, c->reg[Z4C_REG_U], c->reg[Z4C_REG_ADM], b, 1, c->stream);
+    }
+    LAUNCH_CHECK("z4c_to_adm");
+  }
   if (c->ntrk > 0 && stage == 4) {
     launch_track_update(c->trk, c->ntrk, dt, c->stream);
     LAUNCH_CHECK("tracker update");
@@ -1172,8 +1185,10 @@ int z4c_evolve(z4c_ctx* ctx, double dt, int nsteps, int with_constraints) {
   }
   if (with_constraints) {
     const DevParams P = ctx->dev();
-    launch_z4c_to_adm(ctx->g, P, ctx->reg[Z4C_REG_U], ctx->reg[Z4C_REG_ADM], 0, ctx->g.nblocks,
-                      ctx->stream);
+    // the captured step already ran Z4cToADM on its last stage
+    if (nsteps == 0)
+      launch_z4c_to_adm(ctx->g, P, ctx->reg[Z4C_REG_U], ctx->reg[Z4C_REG_ADM], 0, ctx->g.nblocks,
+                        ctx->stream);
     launch_adm_constraints(ctx->g, P, ctx->reg[Z4C_REG_ADM], ctx->reg[Z4C_REG_U],
                            ctx->reg[Z4C_REG_CON], ctx->xf, 0, ctx->g.nblocks, ctx->stream);
     LAUNCH_CHECK("constraints");
@@ -1201,6 +1216,19 @@ std::vector<long long> ctx_locs(const z4c_ctx* c) {
 
 int z4c_regrid(z4c_ctx* dst, const z4c_ctx* src) {
   if (!dst || !src) return fail(Z4C_EINVAL, "null context");
+  // the kernels below run on dst's stream and read src's registers directly:
+  // both contexts must live on the current device
+  {
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(Z4C_ECUDA, "regrid: no current device");
+    }
+    if (src->device != dst->device || cur != dst->device)
+      return fail(Z4C_EINVAL, "regrid: contexts on devices %d (src) and %d (dst), current "
+                              "device %d; both must be on the current device",
+                  src->device, dst->device, cur);
+  }
   for (int a = 0; a < 3; ++a)
     if (dst->desc.nb[a] != src->desc.nb[a] || dst->desc.nx[a] != src->desc.nx[a] ||
         dst->desc.xmin[a] != src->desc.xmin[a] || dst->desc.xmax[a] != src->desc.xmax[a])
@@ -1244,7 +1272,11 @@ int z4c_regrid(z4c_ctx* dst, const z4c_ctx* src) {
     return fail(Z4C_ENOMEM, "regrid: coarse scratch");
   }
   // the source's work must be complete before the destination's stream reads it
-  cudaStreamSynchronize(src->stream);
+  if (cudaStreamSynchronize(src->stream) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(scratch);
+    return fail(Z4C_ECUDA, "regrid: earlier work on the source context failed");
+  }
   const int64_t bs = (int64_t)Z4C_NVAR * dst->g.nvol;
   const double* su = src->reg[Z4C_REG_U];
   double* du = dst->reg[Z4C_REG_U];
@@ -1269,7 +1301,10 @@ int z4c_regrid(z4c_ctx* dst, const z4c_ctx* src) {
       cudaMemcpyAsync(dst->trk, src->trk, sizeof(double) * 8 * src->ntrk,
                       cudaMemcpyDeviceToDevice, dst->stream) != cudaSuccess)
     rc = fail(Z4C_ECUDA, "regrid: trackers");
-  cudaStreamSynchronize(dst->stream);
+  if (cudaStreamSynchronize(dst->stream) != cudaSuccess && rc == Z4C_OK) {
+    cudaGetLastError();
+    rc = fail(Z4C_ECUDA, "regrid: transfer into the destination context failed");
+  }
   cudaFree(scratch);
   if (rc) return rc;
   dst->ntrk = src->ntrk;

@@ -19,6 +19,12 @@
 // work overlaps on the GPU (different streams, or different host threads)
 // race on it.  Blocks are processed in chunks that fit the array; a single
 // MeshBlock whose scratch does not fit is rejected.
+//
+// The first call on a device: with CUDA's lazy module loading the address
+// lookup below is when the driver loads this library's device code on that
+// device and reserves the array, which is an allocation; callers make one
+// call at start-up, outside any stream capture, and every later call
+// allocates nothing.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -130,6 +136,18 @@ extern "C" int z4c_rhs_noalloc(const double* u, double* rhs, int nblocks, const 
   if (chunk > kMaxFd) chunk = kMaxFd;
   if (chunk > nblocks) chunk = nblocks;
 
+  // a launch failure is read back with cudaGetLastError below; an error left
+  // pending by earlier, unrelated work must not be reported as this call's
+  {
+    const cudaError_t prior = cudaPeekAtLastError();
+    if (prior != cudaSuccess) {
+      char buf[200];
+      snprintf(buf, sizeof(buf),
+               "z4c_rhs_noalloc: a CUDA error from earlier work is pending (%s); nothing was "
+               "enqueued", cudaGetErrorString(prior));
+      return set_error(Z4C_ECUDA, buf);
+    }
+  }
   double* base = nullptr;
   int rc = scratch_for_current_device(&base);
   if (rc) return rc;

@@ -325,14 +325,15 @@ int z4c_hst_norms(z4c_ctx *ctx, double out[8]);
 
 /* ---- time stepping ------------------------------------------------------ */
 
-/* One GR_Z4c stage (task_list/gr/task_list_gr_z4c.cpp:142-333) over all
- * blocks: fused RHS + KO + stage update, ghost fill, AlgConstr.  stage is
- * 1-based; dt the full step. */
+/* One GR_Z4c stage (task_list/gr/task_list_gr_z4c.cpp:142-344) over all
+ * blocks: fused RHS + KO + stage update, ghost fill, AlgConstr, and on the
+ * last stage (stage 4) Z4cToADM into the ADM register, as the Z4C_TO_ADM task
+ * does on every last stage.  stage is 1-based; dt the full step. */
 int z4c_stage(z4c_ctx *ctx, int stage, double dt);
 /* nsteps full steps (gra::evolve::Z4c_Vacuum, src/main.hpp:906-913); the
  * per-step launch sequence is captured once into a CUDA graph and replayed.
- * When with_constraints is non-zero the last stage of the last step also
- * runs Z4cToADM and ADMConstraints. */
+ * Every step ends with Z4cToADM (the last stage's Z4C_TO_ADM task); when
+ * with_constraints is non-zero the last step also runs ADMConstraints. */
 int z4c_evolve(z4c_ctx *ctx, double dt, int nsteps, int with_constraints);
 /* Z4c::Z4cRHS + GR_Z4c::IntegrateZ4c of one low-storage stage as a single
  * fused launch over all blocks, without the ghost exchange that follows:
@@ -420,7 +421,9 @@ int z4c_regrid_derefine(const double *child, double *parent, double *coarse, int
  * block of dst is a block of src (copied), a child of one (refined from it)
  * or the parent of eight (derefined from them).  Interiors only; call
  * z4c_init_finalize(dst) after it for the ghosts, as the reference exchanges
- * after a regrid. */
+ * after a regrid.  Both contexts must live on the current CUDA device
+ * (Z4C_EINVAL otherwise, before any work); a failure of earlier work on src,
+ * or of the transfer, returns Z4C_ECUDA and leaves dst's state undefined. */
 int z4c_regrid(z4c_ctx *dst, const z4c_ctx *src);
 
 /* ---- allocation-free variant ----------------------------------------------
@@ -445,7 +448,13 @@ int z4c_regrid(z4c_ctx *dst, const z4c_ctx *src);
  * Z4C_NOALLOC_SCRATCH_MIB MiB compiled into the library; every GPU that loads
  * the library holds it until the process exits.  The first call on a device
  * looks the array's device address up (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  Blocks are
+ * current; make that first call before any stream capture.  With CUDA's lazy
+ * module loading (the default) that first lookup is also when the driver
+ * loads the library's device code on that device and reserves the array: an
+ * allocation of its own.  So make one call (any size) outside the region that
+ * must not allocate, e.g. at start-up; every later call on that device
+ * allocates nothing.  A CUDA error left pending by earlier work is reported
+ * (Z4C_ECUDA) before anything is enqueued, not taken for this call's.  Blocks are
  * processed in chunks that fit the array; a MeshBlock whose scratch alone
  * (33 doubles per vertex, ghosts included, plus 28 per interior vertex)
  * exceeds it -- above roughly 45^3 cells -- is rejected with Z4C_EINVAL

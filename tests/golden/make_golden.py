@@ -101,10 +101,34 @@ EVOL = {
                    extra={"npunct": 1, "bh_0_x": 0.37, "bh_0_y": -0.21, "bh_0_z": 0.13},
                    problem={"punc_ADM_mass": 1.0}, nlim=10, tracker=True),
 }
+# The benchmark configurations at their stated sizes and lengths.  Their
+# states are too large to store (1.4 GB per register on the 512-block mesh),
+# so a fixture keeps the history table of every step, per-variable sums of
+# the initial and final states, and a strided sample of the final state on a
+# few MeshBlocks; the test regenerates the initial state on its side.
+SCALE = {
+    # configs[0] as written: 48^3 cells in one periodic block, harmonic-like
+    # lapse, zero shift, A = 0.01, KO 0.02, kappa1 0.02, 1000 rk4 steps
+    "gw48": dict(test="gauge_wave1", z4c=GAUGE_WAVE, integ="rk4", bc="periodic",
+                 mesh=[(48, -0.5, 0.5, 48)] * 3, extra={"AwA_amplitude": 0.01}, nlim=1000,
+                 stride=4, sample_blocks=[0]),
+    # configs[1] single puncture: M = 1 at the origin, pre-collapsed lapse,
+    # 128^3 cells as 512 blocks of 16^3 on [-16, 16]^3, outflow faces
+    "punc512": dict(test="one_puncture", z4c=PUNCTURE, integ="rk4", bc="extrapolate_outflow",
+                    mesh=[(128, -16.0, 16.0, 16)] * 3, extra={},
+                    problem={"punc_ADM_mass": 1.0}, nlim=40, stride=2,
+                    sample_blocks=[0, 73, 219, 292, 365, 511]),
+    # configs[1] robust stability: Minkowski plus U(-1e-10, 1e-10) on all 22
+    # Z4c variables at every vertex (initial_data.noise_state, seed 137),
+    # periodic, injected into the reference
+    "rs512": dict(test="inject", z4c=PUNCTURE, integ="rk4", bc="periodic",
+                  mesh=[(128, -16.0, 16.0, 16)] * 3, extra={}, nlim=40, stride=2,
+                  noise=dict(amplitude=1e-10, seed=137), sample_blocks=[0, 73, 219, 292, 365, 511]),
+}
 BC_CODES = {"periodic": 0, "extrapolate_outflow": 1, "gr_sommerfeld": 2}
 
 
-def deck(case, out_file, nlim=1, dump_initial="", dump_final="", hst=False):
+def deck(case, out_file, nlim=1, dump_initial="", dump_final="", hst=False, threads=1):
     lines = ["<job>", "problem_id = golden", "<z4c>"]
     for k, v in {**case["z4c"], **case.get("extra", {})}.items():
         lines.append(f"{k} = {v!r}" if isinstance(v, float) else f"{k} = {v}")
@@ -115,7 +139,7 @@ def deck(case, out_file, nlim=1, dump_initial="", dump_final="", hst=False):
         d = a + 1
         lines += [f"nx{d} = {nx}", f"x{d}min = {lo!r}", f"x{d}max = {hi!r}",
                   f"ix{d}_bc = {case['bc']}", f"ox{d}_bc = {case['bc']}"]
-    lines += ["refinement = none", "num_threads = 1", "<meshblock>"]
+    lines += ["refinement = none", f"num_threads = {threads}", "<meshblock>"]
     for a, (_, _, _, nb) in enumerate(case["mesh"]):
         lines.append(f"nx{a + 1} = {nb}")
     lines += ["<problem>", f"test = {case['test']}"]
@@ -193,6 +217,85 @@ def make_evol(name, case, outdir):
         out["tracker_start"] = np.array([case["extra"][f"bh_0_{c}"] for c in "xyz"])
     out.update(meta_json(case))
     path = os.path.join(outdir, f"evol_{name}.npz")
+    np.savez_compressed(path, **out)
+    return path
+
+
+def gid_order(nb):
+    """Grid index l0 + nb0 (l1 + nb1 l2) of every MeshBlock of a uniform
+    block grid, in gid order: the leaves of the root tree in Morton order
+    with x the lowest bit."""
+    def morton(l):
+        key = 0
+        for bit in range(16):
+            for a in range(3):
+                key |= ((l[a] >> bit) & 1) << (3 * bit + a)
+        return key
+    locs = [(i, j, k) for k in range(nb[2]) for j in range(nb[1]) for i in range(nb[0])]
+    return [l[0] + nb[0] * (l[1] + nb[1] * l[2]) for l in sorted(locs, key=morton)]
+
+
+def state_sums(u):
+    """Per-variable sum, sum of squares and largest magnitude over the
+    interior vertices of every block of a [block][var][k][j][i] state."""
+    I = u[:, :, NG_:-NG_, NG_:-NG_, NG_:-NG_]
+    return np.stack([I.sum(axis=(0, 2, 3, 4)), (I * I).sum(axis=(0, 2, 3, 4)),
+                     np.abs(I).max(axis=(0, 2, 3, 4))], axis=1)
+
+
+NG_ = 4
+
+
+def noise_state_gid(case):
+    """The robust-stability state of a SCALE case in gid order (the package's
+    seeded generator, grid order, reordered)."""
+    sys.path.insert(0, os.path.join(ROOT, "gr-athena_b200"))
+    import z4c_b200 as Z
+    from z4c_b200 import initial_data as ID
+    nb = [m[0] // m[3] for m in case["mesh"]]
+    mesh = Z.Mesh(nb, [m[3] for m in case["mesh"]], [m[1] for m in case["mesh"]],
+                  [m[2] for m in case["mesh"]], case["bc"])
+    u = ID.noise_state(mesh, **case["noise"])
+    return u[gid_order(nb)]
+
+
+def make_scale(name, case, outdir, threads=None):
+    threads = threads or os.cpu_count()
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = os.path.join(tmp, "case.inp")
+        init, final = os.path.join(tmp, "init.rec"), os.path.join(tmp, "final.rec")
+        text = deck(case, "unused", nlim=case["nlim"], dump_initial=init, dump_final=final,
+                    hst=True, threads=threads)
+        if case["test"] == "inject":
+            from z4cio import write_records
+            inj = os.path.join(tmp, "inject.rec")
+            write_records(inj, {"u": noise_state_gid(case)})
+            text = text.replace("<driver>", f"inject_file = {inj}\n<driver>")
+        with open(inp, "w") as f:
+            f.write(text)
+        subprocess.run([os.path.join(REF_BIN, "athena_ref"), "-i", inp], cwd=tmp, check=True,
+                       stdout=subprocess.DEVNULL)
+        hst = parse_hst(os.path.join(tmp, "golden.hst"))
+        r0 = read_records(init)
+        u_init_sums = state_sums(r0["u"])
+        meta = r0["meta"]
+        del r0
+        r1 = read_records(final)
+    nb = [m[0] // m[3] for m in case["mesh"]]
+    order = [int(m[2] + nb[0] * (m[3] + nb[1] * m[4])) for m in meta]
+    assert order == gid_order(nb), "gid order"
+    s = case["stride"]
+    blocks = case["sample_blocks"]  # grid indices
+    gids = [order.index(b) for b in blocks]
+    sub = r1["u"][gids][:, :, ::s, ::s, ::s]
+    out = dict(hst=hst, meta=meta, time_dt=r1["time_dt"], nlim=np.array(case["nlim"]),
+               u_init_sums=u_init_sums, u_final_sums=state_sums(r1["u"]),
+               con_final_sums=state_sums(r1["con"]), sample_blocks=np.array(blocks),
+               stride=np.array(s), u_final_sample=sub, threads=np.array(threads))
+    if "noise" in case:
+        out["noise"] = json.dumps(case["noise"])
+    out.update(meta_json(case))
+    path = os.path.join(outdir, f"scale_{name}.npz")
     np.savez_compressed(path, **out)
     return path
 
@@ -375,6 +478,11 @@ def main():
         print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
     if not only or "restart_track4" in only:  # needs evol_track4
         p = make_restart(HERE)
+        print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
+    for name, case in SCALE.items():  # minutes each: the reference at full size
+        if only and f"scale_{name}" not in only:
+            continue
+        p = make_scale(name, case, HERE)
         print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
 
 

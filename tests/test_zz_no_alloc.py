@@ -11,8 +11,11 @@ fit it.
 
 The GPU test compares it with the context-based z4c_rhs on two calls in a row
 (the second on a different state, so that the array's leftover contents from
-the first call would show), on MeshBlocks large enough that the call runs in
-two chunks.  The file is named to be collected last.
+the first call would show), on MeshBlocks of 40^3 cells, one per chunk, and on
+64 MeshBlocks of 16^3 cells, whose kernels are the compile-time-geometry
+instances, a dozen blocks per chunk.  Around the second call the device's free
+memory is read: the call must not change it.  The file is named to be
+collected last.
 """
 import ctypes as C
 
@@ -45,18 +48,23 @@ def test_rejects_bad_sizes_before_any_work():
 
 
 @pytest.mark.gpu
-def test_noalloc_rhs_matches_context_rhs_on_two_calls():
-    from z4c_b200 import initial_data as ID
-    params = Z.default_params(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02,
-                              shift_eta=2.0, r_max_con=1e300)
+@pytest.mark.parametrize("nb,nx", [
     # 8 blocks of 40^3 cells: 46.5 MB of scratch per block (33 doubles per
     # vertex, 28 per interior vertex), so the 64 MiB array takes one block
     # per chunk
-    mesh = Z.Mesh((2, 2, 2), (40, 40, 40), (-8.0,) * 3, (8.0,) * 3, "outflow")
+    ((2, 2, 2), 40),
+    # 64 blocks of 16^3 cells (5.2 MB each, 12 per chunk): the fixed-geometry
+    # kernel instances
+    ((4, 4, 4), 16)])
+def test_noalloc_rhs_matches_context_rhs_on_two_calls(nb, nx):
+    from z4c_b200 import initial_data as ID
+    import torch
+    params = Z.default_params(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02,
+                              shift_eta=2.0, r_max_con=1e300)
+    mesh = Z.Mesh(nb, (nx, nx, nx), (-8.0,) * 3, (8.0,) * 3, "outflow")
     ctx = Z.Z4c(mesh, params, "rk4")
     # one stream for the context and the allocation-free call, so that the
     # uploads, the call and the downloads are ordered
-    import torch
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
     ID.load_adm(ctx, ID.punctures(mesh, params, masses=(0.5, 0.5),
@@ -71,10 +79,14 @@ def test_noalloc_rhs_matches_context_rhs_on_two_calls():
         ctx.Z4cRHS(Z.REG_U, Z.REG_RHS, -1)
         expect = ctx.download(Z.REG_RHS)
         ctx.upload(Z.REG_W, nan_fill)  # unwritten interior entries would stay NaN
+        ctx.sync()
+        free_before = torch.cuda.mem_get_info()[0]
         rc = _call(ctx.device_ptr(Z.REG_U), ctx.device_ptr(Z.REG_W), ctx.nblocks, mesh.nx, dx,
                    params, stream.cuda_stream)
         assert rc == 0, Z.lib().z4c_last_error()
         ctx.sync()
+        if call == 1:  # the first call may load the module (documented); the second may not
+            assert torch.cuda.mem_get_info()[0] == free_before, "the call allocated"
         got = ctx.download(Z.REG_W)
         assert np.isfinite(got[I]).all(), f"call {call}: interior left unwritten"
         assert rel_err(got[I], expect[I]) <= TOL, f"call {call}"
