@@ -3,7 +3,9 @@
 The CUDA sources are compiled for sm_100a only (B200).  -fmad=false keeps
 every multiply and add of the device code separately rounded, as the
 reference CPU build (-ffp-contract=off) does; the host code (the extraction
-spheres' tables) gets -ffp-contract=off itself.
+spheres' tables) gets -ffp-contract=off itself.  The differentiated path
+(z4c_adjoint.cu) is bound to no reference rounding and contracts
+multiply-adds.
 """
 import os
 import subprocess
@@ -14,7 +16,9 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libz4c_b200.so")
 SOURCES = ["z4c_kernels.cu", "z4c_capi.cu", "z4c_refine.cu", "z4c_noalloc.cu", "z4c_wave.cu",
-           "z4c_restart.cu", "z4c_multilevel.cu"]
+           "z4c_restart.cu", "z4c_multilevel.cu", "z4c_adjoint.cu"]
+# per-file replacements of the default flags
+FILE_FLAGS = {"z4c_adjoint.cu": {"-fmad=false": "-fmad=true"}}
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
          "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
@@ -38,7 +42,8 @@ def build(force=False, verbose=False, extra=()):
     objs = []
     for src in SOURCES:
         obj = os.path.join(OUT_DIR, src.replace(".cu", ".o"))
-        cmd = [NVCC, *FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
+        flags = [FILE_FLAGS.get(src, {}).get(f, f) for f in FLAGS]
+        cmd = [NVCC, *flags, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -1,0 +1,1353 @@
+// Differentiated Z4c time stepping on the device: the tangent-linear model
+// and the hand-written adjoint of one RK4 step (low-storage 2S integrator,
+// task_list_gr_z4c.cpp:170-213 with the weights of
+// task_list_integrators_low_storage.cpp:112-142), of the objective
+// J = sum over blocks of vol * sum over cells of H^2 (the H-norm of the
+// history output, outputs/history.cpp:168-200), and the revolve-style
+// checkpointed gradient of J after n steps (z4c_adj_gradient).
+//
+// One forward stage maps (u, u1) to (u', u1'):
+//   v1 = u1 + delta u,  w = gamma1 u + gamma2 v1 + beta dt (F(u) + KO(u))
+//   u_pre = E(w)    ghost exchange (an average over the owners of each vertex,
+//                   copies into the ghosts; periodic meshes)
+//   u' = AC(u_pre)  AlgConstr at every vertex, u1' = v1
+// (u1 = 0 at stage 1).  The reverse of a stage, given the adjoints of u' and
+// u1', runs AC^T at u_pre, E^T, and the transposed stage algebra and
+// right-hand side at u.  The right-hand side reverse is split as the forward
+// is (z4c_ad.cuh): per interior vertex the reverse of the main algebra and of
+// the Ricci part write the adjoints of the vertex's local inputs into channel
+// arrays; then the transposed stencils gather those channels back onto the
+// state (centred first and second derivatives, the mixed second derivatives
+// through the stored first derivatives, Kreiss-Oliger and the upwind
+// advection with the side fixed at the linearisation point).
+//
+// Per-stage recomputation: the adjoint of a step recomputes the step from
+// the state at its start, keeping each stage's u_pre (4 registers); the
+// stage inputs are rebuilt from them (u_s = AC(u_pre_{s-1})) as the reverse
+// sweep reaches them.
+//
+// The adjoint kernels are compiled with floating-point contraction: they
+// are not bound to the reference's rounding, only to the transpose of the
+// forward map (checked against the tangent-linear model and against finite
+// differences of the forward).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "z4c_ad.cuh"
+#include "z4c_ctx.cuh"
+#include "z4c_rhs.cuh"
+
+namespace z4c {
+int set_error(int code, const char* msg);
+
+namespace {
+
+using ad::Dual;
+using ad::HLocal;
+using ad::RhsLocal;
+
+constexpr int kThreads = 128;
+// channels of the right-hand side reverse per interior vertex
+constexpr int kChSd = 0;      // 33: the stored first derivatives, slot*3 + direction
+constexpr int kChDd = 33;     // 66: second derivatives, slot*6 + pair
+constexpr int kChGam = 99;    // 9: d_b Gamma^c, b*3 + c
+constexpr int kChKhat = 108;  // 3
+constexpr int kChTheta = 111; // 3
+constexpr int kNChan = 114;
+// channels of the Hamiltonian-constraint reverse per interior vertex
+constexpr int kHChi = 0, kHGt = 1, kHAt = 7, kHKhat = 13, kHTheta = 14;  // point values
+constexpr int kHDchi = 15, kHDg = 18, kHDdchi = 36, kHDdg = 42;         // stencil inputs
+constexpr int kNHChan = 78;
+
+inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+__device__ __forceinline__ void interior_of(const Grid& g, int64_t l, int& i, int& j, int& k) {
+  const int n0 = g.nx[0] + 1, n1 = g.nx[1] + 1;
+  i = NG + (int)(l % n0);
+  j = NG + (int)((l / n0) % n1);
+  k = NG + (int)(l / ((int64_t)n0 * n1));
+}
+__device__ __forceinline__ bool is_interior(const Grid& g, int i, int j, int k) {
+  return i >= NG && i <= NG + g.nx[0] && j >= NG && j <= NG + g.nx[1] && k >= NG &&
+         k <= NG + g.nx[2];
+}
+__device__ __forceinline__ int64_t interior_index(const Grid& g, int i, int j, int k) {
+  return ((int64_t)(k - NG) * (g.nx[1] + 1) + (j - NG)) * (g.nx[0] + 1) + (i - NG);
+}
+
+// stencil weights, offset o = -R..R
+__device__ __forceinline__ double w_d1(int o) {  // FDStencilCenteredDegreeOdd<1,3>
+  switch (o) {
+    case -3: return -1.; case -2: return 9.; case -1: return -45.;
+    case 1: return 45.; case 2: return -9.; case 3: return 1.;
+    default: return 0.;
+  }
+}
+__device__ __forceinline__ double w_d2(int o) {  // FDStencilCenteredDegreeEven<2,3>
+  switch (o) {
+    case -3: case 3: return 2.; case -2: case 2: return -27.;
+    case -1: case 1: return 270.; case 0: return -490.;
+    default: return 0.;
+  }
+}
+__device__ __forceinline__ double w_ko(int o) {  // FDStencilCenteredDegreeEven<8,4>
+  switch (o) {
+    case -4: case 4: return 1.; case -3: case 3: return -8.; case -2: case 2: return 28.;
+    case -1: case 1: return -56.; case 0: return 70.;
+    default: return 0.;
+  }
+}
+// lop-sided advection, coefficient of f(p + o): left side (beta < 0) o = -4..2,
+// right side (beta >= 0) o = -2..4 (FDStencilBiased{Left,Right}<1,4,2>)
+__device__ __forceinline__ double w_lop(bool left, int o) {
+  if (left) {
+    switch (o) {
+      case -4: return 1.; case -3: return -8.; case -2: return 30.; case -1: return -80.;
+      case 0: return 35.; case 1: return 24.; case 2: return -2.;
+      default: return 0.;
+    }
+  }
+  switch (o) {
+    case -2: return 2.; case -1: return -24.; case 0: return -35.; case 1: return 80.;
+    case 2: return -30.; case 3: return 8.; case 4: return -1.;
+    default: return 0.;
+  }
+}
+
+// A field for the gathers: value array and, for the tangent-linear model, the
+// tangent array at the same offsets.
+template <class T>
+struct Fld;
+template <>
+struct Fld<double> {
+  const double* v;
+  __device__ double at(int64_t o) const { return v[o]; }
+};
+template <>
+struct Fld<Dual> {
+  const double* v;
+  const double* d;
+  __device__ Dual at(int64_t o) const { return Dual(v[o], d[o]); }
+};
+
+template <class T>
+__device__ __forceinline__ T st_d1(const Fld<T>& f, int64_t p, int64_t s, double c) {
+  T out = T(0.);
+#pragma unroll
+  for (int o = -3; o <= 3; ++o)
+    if (o != 0) out += w_d1(o) * f.at(p + o * s);
+  return out * c;
+}
+template <class T>
+__device__ __forceinline__ T st_d2(const Fld<T>& f, int64_t p, int64_t s, double c) {
+  T out = T(0.);
+#pragma unroll
+  for (int o = -3; o <= 3; ++o) out += w_d2(o) * f.at(p + o * s);
+  return out * c;
+}
+template <class T>
+__device__ __forceinline__ T st_d2x(const Fld<T>& f, int64_t p, int64_t sa, int64_t sb, double ca,
+                                   double cb) {
+  T out = T(0.);
+#pragma unroll
+  for (int o = -3; o <= 3; ++o)
+    if (o != 0) out += w_d1(o) * st_d1(f, p + o * sa, sb, cb);
+  return out * ca;
+}
+// the side's stencil sum (before the shift and the spacing factor)
+template <class T>
+__device__ __forceinline__ T st_lop(const Fld<T>& f, int64_t p, int64_t s, bool left) {
+  T out = T(0.);
+#pragma unroll
+  for (int o = -4; o <= 4; ++o) {
+    const double w = w_lop(left, o);
+    if (w != 0.) out += w * f.at(p + o * s);
+  }
+  return out;
+}
+
+// Local inputs of the right-hand side at interior vertex p of a block: U and
+// SD point at the block's state and stored first derivatives (and Ud, SDd at
+// their tangents for T = Dual).
+template <class T>
+__device__ void gather_rhs(const Grid& g, const FdScale& F, const double* U, const double* SD,
+                           const double* Ud, const double* SDd, int64_t p, RhsLocal<T>& v) {
+  const int64_t nv = g.nvol;
+  auto fld = [&](const double* base, const double* based, int64_t off) {
+    Fld<T> f;
+    f.v = base + off;
+    if constexpr (sizeof(T) == sizeof(Dual)) f.d = based + off;
+    return f;
+  };
+  for (int n = 0; n < NVAR; ++n) v.u[n] = fld(U, Ud, (int64_t)n * nv).at(p);
+  auto sdc = [&](int comp) { return fld(SD, SDd, (int64_t)comp * nv).at(p); };
+  for (int a = 0; a < 3; ++a) {
+    v.dchi[a] = sdc(a);
+    v.dalpha[a] = sdc(7 * 3 + a);
+  }
+  for (int c = 0; c < 3; ++c)
+    for (int q = 0; q < 6; ++q) v.dg[c][q] = sdc((1 + q) * 3 + c);
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) v.dbeta[b][a] = sdc((8 + a) * 3 + b);
+  for (int b = 0; b < 3; ++b) {
+    for (int c = 0; c < 3; ++c)
+      v.dGam[b][c] = st_d1(fld(U, Ud, (int64_t)(Z4C_GAMX + c) * nv), p, g.s[b], F.cidx1[b]);
+    v.dKhat[b] = st_d1(fld(U, Ud, (int64_t)Z4C_KHAT * nv), p, g.s[b], F.cidx1[b]);
+    v.dTheta[b] = st_d1(fld(U, Ud, (int64_t)Z4C_THETA * nv), p, g.s[b], F.cidx1[b]);
+  }
+  // second derivatives: Dxx on the diagonal, Dx_a of the stored Dx_b (a < b)
+  for (int slot = 0; slot < 11; ++slot) {
+    const int var = sd_field_var(slot);
+    for (int a = 0; a < 3; ++a)
+      for (int b = a; b < 3; ++b) {
+        T d;
+        if (a == b) d = st_d2(fld(U, Ud, (int64_t)var * nv), p, g.s[a], F.cidx2[a]);
+        else d = st_d1(fld(SD, SDd, (int64_t)(slot * 3 + b) * nv), p, g.s[a], F.cidx1[a]);
+        if (slot == 0) v.ddchi[ad::sid(a, b)] = d;
+        else if (slot <= 6) v.ddg[slot - 1][ad::sid(a, b)] = d;
+        else if (slot == 7) v.ddalpha[ad::sid(a, b)] = d;
+        else v.ddbeta[slot - 8][ad::sid(a, b)] = d;
+      }
+  }
+  // advection sums beta^a L_a f, the side chosen by the sign of beta^a
+  T beta[3];
+  for (int a = 0; a < 3; ++a) beta[a] = v.u[Z4C_BETAX + a];
+  for (int n = 0; n < NVAR; ++n) {
+    T acc = T(0.);
+    for (int a = 0; a < 3; ++a) {
+      const bool left = ad::val(beta[a]) < 0;
+      acc += (beta[a] * st_lop(fld(U, Ud, (int64_t)n * nv), p, g.s[a], left)) * F.lidx[a];
+    }
+    v.lv[n] = acc;
+  }
+}
+
+// ---- reverse of the right-hand side ------------------------------------------
+
+struct StageW {
+  double delta, gamma1, gamma2, beta_dt;
+  int first;  // stage 1: u1 enters as zero
+};
+
+// Per interior vertex: the reverse of the main algebra (z4c_ad.cuh
+// main_local_adj) for the right-hand side adjoint beta dt * wbar, plus the
+// shift adjoint of the advection sums and the stage algebra.  Writes the
+// channels, the Ricci-sum adjoints, the direct adjoint of u at the vertex and
+// the adjoint of u1; parameter adjoints per CTA into part.
+__global__ void __launch_bounds__(kThreads)
+k_adj_main(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
+           const double* __restrict__ rsum, const double* __restrict__ wbar,
+           double* __restrict__ u1bar, double* __restrict__ direct, double* __restrict__ chan,
+           double* __restrict__ rsb, double* __restrict__ part, StageW W) {
+  const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double pe = 0., pk = 0.;
+  if (t < npts * g.nblocks) {
+    const int b = (int)(t / npts);
+    const int64_t l = t % npts;
+    int i, j, k;
+    interior_of(g, l, i, j, k);
+    const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+    const int64_t nv = g.nvol;
+    const double* U = u + (int64_t)b * NVAR * nv;
+    const double* SD = sd + (int64_t)b * kSdComponents * nv;
+    const FdScale& F = P.fd[b];
+    RhsLocal<double> v;
+    gather_rhs<double>(g, F, U, SD, nullptr, nullptr, p, v);
+    double Rs[6];
+    const double* RS = rsum + (int64_t)b * 6 * npts + l;
+    for (int q = 0; q < 6; ++q) Rs[q] = RS[(int64_t)q * npts];
+    double ob[NVAR], wb[NVAR];
+    const double* WB = wbar + (int64_t)b * NVAR * nv + p;
+    for (int n = 0; n < NVAR; ++n) {
+      wb[n] = WB[(int64_t)n * nv];
+      ob[n] = W.beta_dt * wb[n];
+    }
+    RhsLocal<double> vb;
+    for (int q = 0; q < RhsLocal<double>::N; ++q) vb.data()[q] = 0.;
+    double Rsb[6] = {0, 0, 0, 0, 0, 0};
+    ad::ParamBar pb{0., 0.};
+    ad::main_local_adj(P.p, v, Rs, ob, vb, Rsb, pb);
+    pe = pb.shift_eta;
+    pk = pb.damp_kappa1;
+    // the advection sums' dependence on the shift at the vertex
+    for (int a = 0; a < 3; ++a) {
+      const bool left = v.u[Z4C_BETAX + a] < 0;
+      double acc = 0.;
+      for (int n = 0; n < NVAR; ++n) {
+        if (vb.lv[n] == 0.) continue;
+        Fld<double> f{U + (int64_t)n * nv};
+        acc += vb.lv[n] * st_lop(f, p, g.s[a], left);
+      }
+      vb.u[Z4C_BETAX + a] += acc * F.lidx[a];
+    }
+    // channels
+    double* C = chan + (int64_t)b * kNChan * npts + l;
+    for (int a = 0; a < 3; ++a) {
+      C[(int64_t)(kChSd + a) * npts] = vb.dchi[a];
+      C[(int64_t)(kChSd + 7 * 3 + a) * npts] = vb.dalpha[a];
+    }
+    for (int c = 0; c < 3; ++c)
+      for (int q = 0; q < 6; ++q) C[(int64_t)(kChSd + (1 + q) * 3 + c) * npts] = vb.dg[c][q];
+    for (int a = 0; a < 3; ++a)
+      for (int bb = 0; bb < 3; ++bb) C[(int64_t)(kChSd + (8 + a) * 3 + bb) * npts] = vb.dbeta[bb][a];
+    for (int q = 0; q < 6; ++q) {
+      C[(int64_t)(kChDd + 0 * 6 + q) * npts] = vb.ddchi[q];
+      C[(int64_t)(kChDd + 7 * 6 + q) * npts] = vb.ddalpha[q];
+      for (int f = 0; f < 6; ++f) C[(int64_t)(kChDd + (1 + f) * 6 + q) * npts] = vb.ddg[f][q];
+      for (int c = 0; c < 3; ++c) C[(int64_t)(kChDd + (8 + c) * 6 + q) * npts] = vb.ddbeta[c][q];
+    }
+    for (int bb = 0; bb < 3; ++bb) {
+      for (int c = 0; c < 3; ++c) C[(int64_t)(kChGam + bb * 3 + c) * npts] = vb.dGam[bb][c];
+      C[(int64_t)(kChKhat + bb) * npts] = vb.dKhat[bb];
+      C[(int64_t)(kChTheta + bb) * npts] = vb.dTheta[bb];
+    }
+    double* R = rsb + (int64_t)b * 6 * npts + l;
+    for (int q = 0; q < 6; ++q) R[(int64_t)q * npts] = Rsb[q];
+    // stage algebra: w = gamma1 u + gamma2 v1 + beta dt r, v1 = u1 + delta u
+    double* D = direct + (int64_t)b * NVAR * nv + p;
+    double* U1B = u1bar + (int64_t)b * NVAR * nv + p;
+    for (int n = 0; n < NVAR; ++n) {
+      const double v1b = (W.first ? 0. : U1B[(int64_t)n * nv]) + W.gamma2 * wb[n];
+      U1B[(int64_t)n * nv] = v1b;
+      D[(int64_t)n * nv] = vb.u[n] + W.gamma1 * wb[n] + W.delta * v1b;
+    }
+  }
+  // parameter adjoints: a fixed-order reduction per CTA
+  __shared__ double se[kThreads], sk[kThreads];
+  se[threadIdx.x] = pe;
+  sk[threadIdx.x] = pk;
+  __syncthreads();
+  for (int w = kThreads / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      se[threadIdx.x] += se[threadIdx.x + w];
+      sk[threadIdx.x] += sk[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = se[0];
+    part[2 * blockIdx.x + 1] = sk[0];
+  }
+}
+
+// Per interior vertex: the reverse of the Ricci part (ricci_local_adj) given
+// the Ricci-sum adjoints; adds to the channels and the direct adjoint.
+__global__ void __launch_bounds__(kThreads)
+k_adj_ricci(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
+            const double* __restrict__ rsb, double* __restrict__ direct,
+            double* __restrict__ chan) {
+  const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * g.nblocks) return;
+  const int b = (int)(t / npts);
+  const int64_t l = t % npts;
+  int i, j, k;
+  interior_of(g, l, i, j, k);
+  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  const int64_t nv = g.nvol;
+  const double* U = u + (int64_t)b * NVAR * nv;
+  const double* SD = sd + (int64_t)b * kSdComponents * nv;
+  RhsLocal<double> v;
+  gather_rhs<double>(g, P.fd[b], U, SD, nullptr, nullptr, p, v);
+  double Rsb[6];
+  const double* R = rsb + (int64_t)b * 6 * npts + l;
+  for (int q = 0; q < 6; ++q) Rsb[q] = R[(int64_t)q * npts];
+  RhsLocal<double> vb;
+  for (int q = 0; q < RhsLocal<double>::N; ++q) vb.data()[q] = 0.;
+  ad::ricci_local_adj(P.p, v, Rsb, vb);
+  double* C = chan + (int64_t)b * kNChan * npts + l;
+  for (int a = 0; a < 3; ++a) C[(int64_t)(kChSd + a) * npts] += vb.dchi[a];
+  for (int c = 0; c < 3; ++c)
+    for (int q = 0; q < 6; ++q) C[(int64_t)(kChSd + (1 + q) * 3 + c) * npts] += vb.dg[c][q];
+  for (int q = 0; q < 6; ++q) {
+    C[(int64_t)(kChDd + 0 * 6 + q) * npts] += vb.ddchi[q];
+    for (int f = 0; f < 6; ++f) C[(int64_t)(kChDd + (1 + f) * 6 + q) * npts] += vb.ddg[f][q];
+  }
+  for (int bb = 0; bb < 3; ++bb)
+    for (int c = 0; c < 3; ++c) C[(int64_t)(kChGam + bb * 3 + c) * npts] += vb.dGam[bb][c];
+  double* D = direct + (int64_t)b * NVAR * nv + p;
+  for (int n = 0; n < NVAR; ++n)
+    if (vb.u[n] != 0.) D[(int64_t)n * nv] += vb.u[n];
+}
+
+// Region of the stored first derivative along direction dir (as k_prep
+// fills it): the interior, extended by 3 along x for dir >= 1 and along y
+// for dir == 2.
+__device__ __forceinline__ bool in_sd_region(const Grid& g, int dir, int i, int j, int k) {
+  const int ex = (dir >= 1) ? 3 : 0, ey = (dir == 2) ? 3 : 0;
+  return i >= NG - ex && i <= NG + g.nx[0] + ex && j >= NG - ey && j <= NG + g.nx[1] + ey &&
+         k >= NG && k <= NG + g.nx[2];
+}
+
+// Adjoint of the stored first derivatives: the vertex's own channel plus the
+// transposed outer derivative of every mixed second derivative that reads it.
+// One thread per (block, component, vertex of the component's region).
+__global__ void __launch_bounds__(kThreads)
+k_adj_sdbar(Grid g, DevParams P, const double* __restrict__ chan, double* __restrict__ sdbar) {
+  const int comp = blockIdx.y, b = blockIdx.z;
+  const int slot = comp / 3, dir = comp % 3;
+  const int ex = (dir >= 1) ? 3 : 0, ey = (dir == 2) ? 3 : 0;
+  const int e0 = g.nx[0] + 1 + 2 * ex, e1 = g.nx[1] + 1 + 2 * ey, e2 = g.nx[2] + 1;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)e0 * e1 * e2) return;
+  const int i = NG - ex + (int)(t % e0), j = NG - ey + (int)((t / e0) % e1),
+            k = NG + (int)(t / ((int64_t)e0 * e1));
+  const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
+  const double* C = chan + (int64_t)b * kNChan * npts;
+  const FdScale& F = P.fd[b];
+  double acc = 0.;
+  if (is_interior(g, i, j, k)) acc = C[(int64_t)(kChSd + comp) * npts + interior_index(g, i, j, k)];
+  // D_a(stored D_dir f) for a < dir: p = r - o e_a
+  for (int a = 0; a < dir; ++a) {
+    const double* dd = C + (int64_t)(kChDd + slot * 6 + ad::sid(a, dir)) * npts;
+    double s = 0.;
+#pragma unroll
+    for (int o = -3; o <= 3; ++o) {
+      if (o == 0) continue;
+      const int pi = i - (a == 0 ? o : 0), pj = j - (a == 1 ? o : 0);
+      if (is_interior(g, pi, pj, k)) s += w_d1(o) * dd[interior_index(g, pi, pj, k)];
+    }
+    acc += s * F.cidx1[a];
+  }
+  sdbar[((int64_t)b * kSdComponents + comp) * g.nvol + ((int64_t)k * g.nn[1] + j) * g.nn[0] + i] =
+      acc;
+}
+
+// Adjoint of the stage input u at every vertex of every block: the direct
+// adjoint (interior) plus the transposed stencils of every channel, the
+// Kreiss-Oliger terms and the upwind advection.  One thread per (block,
+// variable, vertex).
+__global__ void __launch_bounds__(kThreads)
+k_adj_gather(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ wbar,
+             const double* __restrict__ direct, const double* __restrict__ chan,
+             const double* __restrict__ sdbar, double* __restrict__ ubar, double beta_dt) {
+  const int64_t nv = g.nvol;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nv * NVAR * g.nblocks) return;
+  const int64_t q = t % nv;
+  const int n = (int)((t / nv) % NVAR);
+  const int b = (int)(t / (nv * NVAR));
+  const int i = (int)(q % g.nn[0]), j = (int)((q / g.nn[0]) % g.nn[1]),
+            k = (int)(q / ((int64_t)g.nn[0] * g.nn[1]));
+  const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
+  const double* C = chan + (int64_t)b * kNChan * npts;
+  const FdScale& F = P.fd[b];
+  const int ijk[3] = {i, j, k};
+  double acc = 0.;
+  if (is_interior(g, i, j, k)) acc = direct[((int64_t)b * NVAR + n) * nv + q];
+  // 1-D transposed stencils along axis a over an interior channel
+  auto line_d1 = [&](const double* ch, int a) {
+    double s = 0.;
+#pragma unroll
+    for (int o = -3; o <= 3; ++o) {
+      if (o == 0) continue;
+      int pp[3] = {i, j, k};
+      pp[a] -= o;
+      if (is_interior(g, pp[0], pp[1], pp[2]))
+        s += w_d1(o) * ch[interior_index(g, pp[0], pp[1], pp[2])];
+    }
+    return s;
+  };
+  auto line_d2 = [&](const double* ch, int a) {
+    double s = 0.;
+#pragma unroll
+    for (int o = -3; o <= 3; ++o) {
+      int pp[3] = {i, j, k};
+      pp[a] -= o;
+      if (is_interior(g, pp[0], pp[1], pp[2]))
+        s += w_d2(o) * ch[interior_index(g, pp[0], pp[1], pp[2])];
+    }
+    return s;
+  };
+  int slot = -1;
+  for (int s = 0; s < 11; ++s)
+    if (sd_field_var(s) == n) slot = s;
+  if (slot >= 0) {
+    // D_dir^T of the stored first derivatives' adjoints (their regions)
+    for (int dir = 0; dir < 3; ++dir) {
+      const double* sb = sdbar + ((int64_t)b * kSdComponents + slot * 3 + dir) * nv;
+      double s = 0.;
+#pragma unroll
+      for (int o = -3; o <= 3; ++o) {
+        if (o == 0) continue;
+        int pp[3] = {i, j, k};
+        pp[dir] -= o;
+        if (in_sd_region(g, dir, pp[0], pp[1], pp[2]))
+          s += w_d1(o) * sb[((int64_t)pp[2] * g.nn[1] + pp[1]) * g.nn[0] + pp[0]];
+      }
+      acc += s * F.cidx1[dir];
+    }
+    // Dxx^T of the diagonal second derivatives
+    for (int a = 0; a < 3; ++a)
+      acc += line_d2(C + (int64_t)(kChDd + slot * 6 + ad::sid(a, a)) * npts, a) * F.cidx2[a];
+  }
+  int ch1 = -1;  // centred first derivatives of Gamma^c, Khat, Theta
+  if (n >= Z4C_GAMX && n <= Z4C_GAMZ) ch1 = kChGam + (n - Z4C_GAMX);
+  if (n == Z4C_KHAT) ch1 = kChKhat;
+  if (n == Z4C_THETA) ch1 = kChTheta;
+  if (ch1 >= 0)
+    for (int a = 0; a < 3; ++a) {
+      const int c = (ch1 >= kChKhat) ? ch1 + a : kChGam + a * 3 + (n - Z4C_GAMX);
+      acc += line_d1(C + (int64_t)c * npts, a) * F.cidx1[a];
+    }
+  // Kreiss-Oliger and advection from the right-hand-side adjoint beta dt wbar
+  const double* WB = wbar + ((int64_t)b * NVAR + n) * nv;
+  const double* BETA = u + ((int64_t)b * NVAR + Z4C_BETAX) * nv;
+  const double adv = ad::adv_coef(P.p, n);
+  for (int a = 0; a < 3; ++a) {
+    double sko = 0., sadv = 0.;
+    for (int o = -4; o <= 4; ++o) {
+      int pp[3] = {ijk[0], ijk[1], ijk[2]};
+      pp[a] -= o;
+      if (!is_interior(g, pp[0], pp[1], pp[2])) continue;
+      const int64_t pq = ((int64_t)pp[2] * g.nn[1] + pp[1]) * g.nn[0] + pp[0];
+      const double rb = beta_dt * WB[pq];
+      sko += w_ko(o) * rb;
+      if (adv != 0.) {
+        const double be = BETA[(int64_t)a * nv + pq];
+        const double w = w_lop(be < 0, o);
+        if (w != 0.) sadv += w * be * rb;
+      }
+    }
+    acc += sko * F.cidxd[a] * P.p.diss + sadv * adv * F.lidx[a];
+  }
+  ubar[((int64_t)b * NVAR + n) * nv + q] = acc;
+}
+
+// AlgConstr^T at every vertex: ubar (adjoint after) -> adjoint before, at the
+// pre-constraint state upre.
+__global__ void __launch_bounds__(kThreads)
+k_adj_alg(Grid g, DevParams P, const double* __restrict__ upre, double* __restrict__ ubar) {
+  const int64_t nv = g.nvol;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nv * g.nblocks) return;
+  const int b = (int)(t / nv);
+  const int64_t q = t % nv;
+  double uu[NVAR], ub[NVAR];
+  const double* UP = upre + (int64_t)b * NVAR * nv + q;
+  double* UB = ubar + (int64_t)b * NVAR * nv + q;
+  for (int n = 0; n < NVAR; ++n) {
+    uu[n] = UP[(int64_t)n * nv];
+    ub[n] = UB[(int64_t)n * nv];
+  }
+  ad::alg_constr_adj(P.p, uu, ub);
+  for (int n = 0; n < NVAR; ++n) UB[(int64_t)n * nv] = ub[n];
+}
+
+// Block grid neighbour in direction d (periodic wrap; -1 beyond a
+// non-periodic face).
+__device__ __forceinline__ int grid_neighbour(const Grid& g, int b, const int d[3]) {
+  int l[3] = {b % g.nb[0], (b / g.nb[0]) % g.nb[1], b / (g.nb[0] * g.nb[1])};
+  for (int a = 0; a < 3; ++a) {
+    l[a] += d[a];
+    if (l[a] < 0 || l[a] >= g.nb[a]) {
+      if (g.bc[2 * a] != Z4C_BC_PERIODIC) return -1;
+      l[a] = (l[a] + g.nb[a]) % g.nb[a];
+    }
+  }
+  return l[0] + g.nb[0] * (l[1] + g.nb[1] * l[2]);
+}
+
+// E^T of the same-level exchange: the adjoint of every owner copy of a
+// vertex is 1/m times the sum of the adjoints of all entries (own, other
+// owners', ghosts anywhere) that hold that vertex after the exchange.  One
+// thread per (block, variable, interior vertex); wbar receives the interior.
+__global__ void __launch_bounds__(kThreads)
+k_adj_exchange(Grid g, const double* __restrict__ ubar, double* __restrict__ wbar) {
+  const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * NVAR * g.nblocks) return;
+  const int64_t l = t % npts;
+  const int n = (int)((t / npts) % NVAR);
+  const int b = (int)(t / (npts * NVAR));
+  int i, j, k;
+  interior_of(g, l, i, j, k);
+  const int64_t nv = g.nvol;
+  double s = 0.;
+  int m = 0;
+  for (int d2 = -1; d2 <= 1; ++d2)
+    for (int d1 = -1; d1 <= 1; ++d1)
+      for (int d0 = -1; d0 <= 1; ++d0) {
+        const int d[3] = {d0, d1, d2};
+        const int nb = grid_neighbour(g, b, d);
+        if (nb < 0) continue;
+        const int li = i - d0 * g.nx[0], lj = j - d1 * g.nx[1], lk = k - d2 * g.nx[2];
+        if (li < 0 || li >= g.nn[0] || lj < 0 || lj >= g.nn[1] || lk < 0 || lk >= g.nn[2]) continue;
+        s += ubar[((int64_t)nb * NVAR + n) * nv + ((int64_t)lk * g.nn[1] + lj) * g.nn[0] + li];
+        if (is_interior(g, li, lj, lk)) ++m;
+      }
+  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  wbar[((int64_t)b * NVAR + n) * nv + p] = s / (double)m;
+}
+
+// ---- tangent-linear model ------------------------------------------------------
+
+// One low-storage stage of the tangents at every interior vertex: the
+// right-hand side's forward-mode derivative (rhs_local on dual numbers) plus
+// Kreiss-Oliger of the tangent, then the stage algebra.
+__global__ void __launch_bounds__(kThreads)
+k_tlm_stage(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
+            const double* __restrict__ ud, const double* __restrict__ sdd,
+            double* __restrict__ u1d, double* __restrict__ wd, StageW W) {
+  const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * g.nblocks) return;
+  const int b = (int)(t / npts);
+  const int64_t l = t % npts;
+  int i, j, k;
+  interior_of(g, l, i, j, k);
+  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  const int64_t nv = g.nvol;
+  const int64_t boff = (int64_t)b * NVAR * nv;
+  const FdScale& F = P.fd[b];
+  RhsLocal<Dual> v;
+  gather_rhs<Dual>(g, F, u + boff, sd + (int64_t)b * kSdComponents * nv, ud + boff,
+                   sdd + (int64_t)b * kSdComponents * nv, p, v);
+  Dual out[NVAR];
+  ad::rhs_local(P.p, v, out);
+  for (int n = 0; n < NVAR; ++n) {
+    const double* fd = ud + boff + (int64_t)n * nv;
+    double r = out[n].d;
+    for (int a = 0; a < 3; ++a) {
+      double s = 0.;
+      for (int o = -4; o <= 4; ++o) s += w_ko(o) * fd[p + o * g.s[a]];
+      r += s * F.cidxd[a] * P.p.diss;
+    }
+    const int64_t qn = boff + (int64_t)n * nv + p;
+    const double un = ud[qn];
+    const double v1 = (W.first ? 0. : u1d[qn]) + W.delta * un;
+    u1d[qn] = v1;
+    wd[qn] = W.gamma1 * un + W.gamma2 * v1 + W.beta_dt * r;
+  }
+}
+
+// AlgConstr and its tangent at every vertex: (upre, upre_dot) -> (u, u_dot).
+__global__ void __launch_bounds__(kThreads)
+k_tlm_alg(Grid g, DevParams P, const double* __restrict__ upre, const double* __restrict__ upred,
+          double* __restrict__ u, double* __restrict__ ud) {
+  const int64_t nv = g.nvol;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nv * g.nblocks) return;
+  const int b = (int)(t / nv);
+  const int64_t q = t % nv;
+  const int64_t base = (int64_t)b * NVAR * nv + q;
+  Dual x[NVAR];
+  for (int n = 0; n < NVAR; ++n) x[n] = Dual(upre[base + (int64_t)n * nv], upred[base + (int64_t)n * nv]);
+  ad::alg_constr_local(P.p, x);
+  for (int n = 0; n < NVAR; ++n) {
+    u[base + (int64_t)n * nv] = x[n].v;
+    ud[base + (int64_t)n * nv] = x[n].d;
+  }
+}
+
+// ---- the objective: vol * sum over cells of H^2 --------------------------------
+
+template <class T>
+__device__ void gather_ham(const Grid& g, const FdScale& F, const double* U, const double* Ud,
+                           int64_t p, HLocal<T>& v) {
+  const int64_t nv = g.nvol;
+  auto fld = [&](int var) {
+    Fld<T> f;
+    f.v = U + (int64_t)var * nv;
+    if constexpr (sizeof(T) == sizeof(Dual)) f.d = Ud + (int64_t)var * nv;
+    return f;
+  };
+  v.chi = fld(Z4C_CHI).at(p);
+  for (int c = 0; c < 6; ++c) {
+    v.gt[c] = fld(Z4C_GXX + c).at(p);
+    v.At[c] = fld(Z4C_AXX + c).at(p);
+  }
+  v.Khat = fld(Z4C_KHAT).at(p);
+  v.Theta = fld(Z4C_THETA).at(p);
+  for (int a = 0; a < 3; ++a) {
+    v.dchi[a] = st_d1(fld(Z4C_CHI), p, g.s[a], F.cidx1[a]);
+    for (int q = 0; q < 6; ++q) v.dg3[a][q] = st_d1(fld(Z4C_GXX + q), p, g.s[a], F.cidx1[a]);
+  }
+  for (int a = 0; a < 3; ++a)
+    for (int b = a; b < 3; ++b) {
+      const int pr = ad::sid(a, b);
+      if (a == b) {
+        v.ddchi[pr] = st_d2(fld(Z4C_CHI), p, g.s[a], F.cidx2[a]);
+        for (int q = 0; q < 6; ++q) v.ddg[q][pr] = st_d2(fld(Z4C_GXX + q), p, g.s[a], F.cidx2[a]);
+      } else {
+        v.ddchi[pr] = st_d2x(fld(Z4C_CHI), p, g.s[a], g.s[b], F.cidx1[a], F.cidx1[b]);
+        for (int q = 0; q < 6; ++q)
+          v.ddg[q][pr] = st_d2x(fld(Z4C_GXX + q), p, g.s[a], g.s[b], F.cidx1[a], F.cidx1[b]);
+      }
+    }
+}
+
+// Whether interior vertex (i, j, k) of block b is a cell of the history sum
+// (cell index range is..ie, cell-centre radius within r_max_con).
+__device__ __forceinline__ bool hst_cell(const Grid& g, const DevParams& P, const double* xv,
+                                         int b, int i, int j, int k) {
+  if (i >= NG + g.nx[0] || j >= NG + g.nx[1] || k >= NG + g.nx[2]) return false;
+  const double* x = xv + (int64_t)b * (g.nn[0] + g.nn[1] + g.nn[2] - 3);
+  const double x1 = x[i], x2 = x[g.nn[0] - 1 + j], x3 = x[g.nn[0] + g.nn[1] - 2 + k];
+  return x1 * x1 + x2 * x2 + x3 * x3 <= P.p.r_max_con * P.p.r_max_con;
+}
+// H at a vertex as ADMConstraints gives it: zero beyond r_max_con (vertex
+// radius).
+__device__ __forceinline__ bool con_live(const Grid& g, const DevParams& P, int b, int i, int j,
+                                         int k) {
+  const double* x = P.xf + (int64_t)b * (g.nn[0] + g.nn[1] + g.nn[2]);
+  const double x1 = x[i], x2 = x[g.nn[0] + j], x3 = x[g.nn[0] + g.nn[1] + k];
+  return !(x1 * x1 + x2 * x2 + x3 * x3 > P.p.r_max_con * P.p.r_max_con);
+}
+
+// Per interior vertex: H (and its tangent when ud is given), vol H^2 (and
+// 2 vol H H_dot) summed per CTA into part[2 * cta].
+template <bool TAN>
+__global__ void __launch_bounds__(kThreads)
+k_ham_obj(Grid g, DevParams P, const double* __restrict__ xv, const double* __restrict__ u,
+          const double* __restrict__ ud, double* __restrict__ part) {
+  const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double jv = 0., jd = 0.;
+  if (t < npts * g.nblocks) {
+    const int b = (int)(t / npts);
+    int i, j, k;
+    interior_of(g, t % npts, i, j, k);
+    if (hst_cell(g, P, xv, b, i, j, k) && con_live(g, P, b, i, j, k)) {
+      const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+      const int64_t boff = (int64_t)b * NVAR * g.nvol;
+      const double vol = P.dx[3 * b] * P.dx[3 * b + 1] * P.dx[3 * b + 2];
+      if (TAN) {
+        HLocal<Dual> v;
+        gather_ham<Dual>(g, P.fd[b], u + boff, ud + boff, p, v);
+        const Dual H = ad::ham_local(P.p, v);
+        jv = vol * H.v * H.v;
+        jd = 2. * vol * H.v * H.d;
+      } else {
+        HLocal<double> v;
+        gather_ham<double>(g, P.fd[b], u + boff, nullptr, p, v);
+        const double H = ad::ham_local(P.p, v);
+        jv = vol * H * H;
+      }
+    }
+  }
+  __shared__ double s0[kThreads], s1[kThreads];
+  s0[threadIdx.x] = jv;
+  s1[threadIdx.x] = jd;
+  __syncthreads();
+  for (int w = kThreads / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      s0[threadIdx.x] += s0[threadIdx.x + w];
+      s1[threadIdx.x] += s1[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = s0[0];
+    part[2 * blockIdx.x + 1] = s1[0];
+  }
+}
+
+// Reverse of the objective per interior vertex: H_bar = scale * 2 vol H, the
+// adjoints of H's local inputs into the H channels.
+__global__ void __launch_bounds__(kThreads)
+k_ham_adj(Grid g, DevParams P, const double* __restrict__ xv, const double* __restrict__ u,
+          double scale, double* __restrict__ hchan) {
+  const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * g.nblocks) return;
+  const int b = (int)(t / npts);
+  const int64_t l = t % npts;
+  int i, j, k;
+  interior_of(g, l, i, j, k);
+  HLocal<double> vb;
+  for (int q = 0; q < HLocal<double>::N; ++q) vb.data()[q] = 0.;
+  if (hst_cell(g, P, xv, b, i, j, k) && con_live(g, P, b, i, j, k)) {
+    const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+    HLocal<double> v;
+    gather_ham<double>(g, P.fd[b], u + (int64_t)b * NVAR * g.nvol, nullptr, p, v);
+    const double H = ad::ham_local(P.p, v);
+    const double vol = P.dx[3 * b] * P.dx[3 * b + 1] * P.dx[3 * b + 2];
+    ad::ham_local_adj(P.p, v, scale * 2. * vol * H, vb);
+  }
+  double* C = hchan + (int64_t)b * kNHChan * npts + l;
+  for (int q = 0; q < kNHChan; ++q) C[(int64_t)q * npts] = vb.data()[q];
+}
+
+// Adds the transposed stencils of the H channels to ubar at every vertex.
+__global__ void __launch_bounds__(kThreads)
+k_ham_gather(Grid g, DevParams P, const double* __restrict__ hchan, double* __restrict__ ubar) {
+  const int64_t nv = g.nvol;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nv * NVAR * g.nblocks) return;
+  const int64_t q = t % nv;
+  const int n = (int)((t / nv) % NVAR);
+  const int b = (int)(t / (nv * NVAR));
+  int pch = -1;  // point-value channel
+  int fq = -1;   // chi: -1 -> field index for stencils: 0 chi, 1..6 g~
+  if (n == Z4C_CHI) { pch = kHChi; fq = 0; }
+  else if (n >= Z4C_GXX && n <= Z4C_GZZ) { pch = kHGt + (n - Z4C_GXX); fq = 1 + (n - Z4C_GXX); }
+  else if (n >= Z4C_AXX && n <= Z4C_AZZ) pch = kHAt + (n - Z4C_AXX);
+  else if (n == Z4C_KHAT) pch = kHKhat;
+  else if (n == Z4C_THETA) pch = kHTheta;
+  if (pch < 0) return;
+  const int i = (int)(q % g.nn[0]), j = (int)((q / g.nn[0]) % g.nn[1]),
+            k = (int)(q / ((int64_t)g.nn[0] * g.nn[1]));
+  const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
+  const double* C = hchan + (int64_t)b * kNHChan * npts;
+  const FdScale& F = P.fd[b];
+  double acc = 0.;
+  if (is_interior(g, i, j, k)) acc = C[(int64_t)pch * npts + interior_index(g, i, j, k)];
+  if (fq >= 0) {
+    for (int a = 0; a < 3; ++a) {
+      const double* d1 = C + (int64_t)(fq == 0 ? kHDchi + a : kHDg + a * 6 + (fq - 1)) * npts;
+      const double* d2 = C + (int64_t)(fq == 0 ? kHDdchi + ad::sid(a, a)
+                                               : kHDdg + (fq - 1) * 6 + ad::sid(a, a)) * npts;
+      double s1 = 0., s2 = 0.;
+      for (int o = -3; o <= 3; ++o) {
+        int pp[3] = {i, j, k};
+        pp[a] -= o;
+        if (!is_interior(g, pp[0], pp[1], pp[2])) continue;
+        const int64_t li = interior_index(g, pp[0], pp[1], pp[2]);
+        s1 += w_d1(o) * d1[li];
+        s2 += w_d2(o) * d2[li];
+      }
+      acc += s1 * F.cidx1[a] + s2 * F.cidx2[a];
+    }
+    for (int a = 0; a < 3; ++a)
+      for (int bb = a + 1; bb < 3; ++bb) {
+        const double* dx = C + (int64_t)(fq == 0 ? kHDdchi + ad::sid(a, bb)
+                                                 : kHDdg + (fq - 1) * 6 + ad::sid(a, bb)) * npts;
+        double s = 0.;
+        for (int oa = -3; oa <= 3; ++oa) {
+          if (oa == 0) continue;
+          for (int ob = -3; ob <= 3; ++ob) {
+            if (ob == 0) continue;
+            int pp[3] = {i, j, k};
+            pp[a] -= oa;
+            pp[bb] -= ob;
+            if (!is_interior(g, pp[0], pp[1], pp[2])) continue;
+            s += w_d1(oa) * w_d1(ob) * dx[interior_index(g, pp[0], pp[1], pp[2])];
+          }
+        }
+        acc += s * F.cidx1[a] * F.cidx1[bb];
+      }
+  }
+  ubar[((int64_t)b * NVAR + n) * nv + q] += acc;
+}
+
+// acc[0..1] += the sums of part[2 i], part[2 i + 1] over i < n, in a fixed
+// order (one CTA of 256 threads)
+__global__ void k_accumulate(const double* __restrict__ part, int n, double* __restrict__ acc) {
+  __shared__ double s0[256], s1[256];
+  double a = 0., b = 0.;
+  for (int i = threadIdx.x; i < n; i += 256) {
+    a += part[2 * i];
+    b += part[2 * i + 1];
+  }
+  s0[threadIdx.x] = a;
+  s1[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      s0[threadIdx.x] += s0[threadIdx.x + w];
+      s1[threadIdx.x] += s1[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    acc[0] += s0[0];
+    acc[1] += s1[0];
+  }
+}
+
+}  // namespace
+
+// ---- buffers -------------------------------------------------------------------
+
+struct AdjState {
+  int64_t reg_elems = 0;
+  double* tan = nullptr;    // tangent of u (Z4C_REG_TAN)
+  double* tan1 = nullptr;   // tangent of u1
+  double* tanw = nullptr;   // tangent of the stage output / pre-constraint state
+  double* sdd = nullptr;    // stored first derivatives of the tangent
+  double* adj = nullptr;    // adjoint of u (Z4C_REG_ADJ)
+  double* adj1 = nullptr;   // adjoint of u1
+  double* wbar = nullptr;   // adjoint of the stage output
+  double* direct = nullptr; // direct adjoint of the stage input at interior vertices
+  double* upre[4] = {};     // pre-constraint exchanged states of the four stages
+  double* us = nullptr;     // recomputed stage input
+  double* w = nullptr;      // forward stage output
+  double* u1 = nullptr;     // forward u1
+  double* chan = nullptr;   // right-hand side reverse channels
+  double* rsb = nullptr;    // Ricci-sum adjoints
+  double* sdbar = nullptr;  // stored-first-derivative adjoints
+  double* hchan = nullptr;  // H reverse channels
+  double* part = nullptr;   // per-CTA partial sums
+  int npart = 0;
+  double* pacc = nullptr;   // device accumulators of the shift_eta, damp_kappa1 adjoints
+  std::vector<double*> snaps;  // revolve snapshots
+};
+
+void adj_free(AdjState* a) {
+  if (!a) return;
+  for (double* p : {a->tan, a->tan1, a->tanw, a->sdd, a->adj, a->adj1, a->wbar, a->direct, a->us,
+                    a->w, a->u1, a->chan, a->rsb, a->sdbar, a->hchan, a->part, a->pacc})
+    if (p) cudaFree(p);
+  for (double* p : a->upre)
+    if (p) cudaFree(p);
+  for (double* p : a->snaps)
+    if (p) cudaFree(p);
+  delete a;
+}
+
+}  // namespace z4c
+
+namespace {
+
+char g_msg[512];
+int err(int code, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+int err(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_msg, sizeof(g_msg), fmt, ap);
+  va_end(ap);
+  return z4c::set_error(code, g_msg);
+}
+
+#define ACUDA(expr)                                                                 \
+  do {                                                                              \
+    cudaError_t e_ = (expr);                                                        \
+    if (e_ != cudaSuccess) return err(Z4C_ECUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
+  } while (0)
+#define ALAUNCH(what)                                                               \
+  do {                                                                              \
+    cudaError_t e_ = cudaGetLastError();                                            \
+    if (e_ != cudaSuccess) return err(Z4C_ECUDA, "%s launch: %s", what, cudaGetErrorString(e_)); \
+  } while (0)
+
+int64_t npts_of(const Grid& g) { return (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1); }
+
+int check_ctx(z4c_ctx* c) {
+  if (!c) return err(Z4C_EINVAL, "null context");
+  if (c->ml) return err(Z4C_ESTATE, "the adjoint runs on uniform meshes (no refined levels)");
+  if (c->integrator != Z4C_INTEG_RK4) return err(Z4C_ESTATE, "the adjoint differentiates rk4 (2S)");
+  if (c->g.has_sommerfeld) return err(Z4C_ESTATE, "the adjoint has no gr_sommerfeld faces");
+  for (int f = 0; f < 6; ++f)
+    if (c->g.bc[f] != Z4C_BC_PERIODIC)
+      return err(Z4C_ESTATE, "the adjoint runs on periodic meshes");
+  if (c->params.chi_psi_power != -4.)
+    return err(Z4C_ESTATE, "the adjoint objective assumes chi_psi_power = -4");
+  if (!c->adj) return err(Z4C_ESTATE, "call z4c_adj_setup first");
+  return Z4C_OK;
+}
+
+// Forward stage s (1-based) from u (stage input, all vertices) and u1: w,
+// u1 updated, then E(w) -> upre (no constraint), AlgConstr(upre) -> uout.
+int fwd_stage(z4c_ctx* c, int s, double dt, const double* u, double* u1, double* w, double* upre,
+              double* uout) {
+  const double* wt = kLsRk4[s - 1];
+  LsStage ls{wt[0], wt[1], wt[2], wt[3], wt[4] * dt, s == 1 ? 1 : 0};
+  const DevParams P = c->dev();
+  launch_stage_ls(c->g, P, u, c->scratch(), c->reg[Z4C_REG_RHS], u1, w, ls, 0, c->g.nblocks,
+                  c->shape, c->stream);
+  ALAUNCH("stage");
+  launch_exchange(c->g, P, w, upre, c->nbr, 0, c->stream);
+  ALAUNCH("exchange");
+  if (uout) {
+    if (uout != upre)
+      ACUDA(cudaMemcpyAsync(uout, upre, sizeof(double) * c->adj->reg_elems,
+                            cudaMemcpyDeviceToDevice, c->stream));
+    launch_alg_constr(c->g, P, uout, 0, c->g.nblocks, c->stream);
+    ALAUNCH("alg_constr");
+  }
+  return Z4C_OK;
+}
+
+// One forward step of u in place (the captured step's arithmetic, separate
+// exchange and constraint passes).
+int fwd_step(z4c_ctx* c, double dt, double* u) {
+  z4c::AdjState* A = c->adj;
+  for (int s = 1; s <= 4; ++s) {
+    int rc = fwd_stage(c, s, dt, u, A->u1, A->w, A->us, u);
+    if (rc) return rc;
+  }
+  return Z4C_OK;
+}
+
+int reduce_part(z4c_ctx* c, int nblk, double out[2]) {
+  std::vector<double> h((size_t)2 * nblk);
+  ACUDA(cudaMemcpyAsync(h.data(), c->adj->part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
+                        c->stream));
+  ACUDA(cudaStreamSynchronize(c->stream));
+  out[0] = out[1] = 0.;
+  for (int i = 0; i < nblk; ++i) {
+    out[0] += h[2 * (size_t)i];
+    out[1] += h[2 * (size_t)i + 1];
+  }
+  return Z4C_OK;
+}
+
+// Adjoint of one step starting from the state u (not modified): A->adj
+// holds the adjoint of the state after the step on entry and of u on return.
+int adj_step(z4c_ctx* c, double dt, const double* u) {
+  z4c::AdjState* A = c->adj;
+  const Grid& g = c->g;
+  const DevParams P = c->dev();
+  const int64_t bytes = sizeof(double) * A->reg_elems;
+  // recompute the step, keeping each stage's pre-constraint state
+  ACUDA(cudaMemcpyAsync(A->us, u, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  for (int s = 1; s <= 4; ++s) {
+    // stage s from us; its constrained output becomes the next stage's input
+    int rc = fwd_stage(c, s, dt, A->us, A->u1, A->w, A->upre[s - 1], s < 4 ? A->us : nullptr);
+    if (rc) return rc;
+  }
+  // the adjoint of u1 after the last stage is zero: the next step starts u1 at zero
+  ACUDA(cudaMemsetAsync(A->adj1, 0, bytes, c->stream));
+  const int64_t npts = npts_of(g);
+  const int nthr = div_up(npts * g.nblocks, kThreads);
+  for (int s = 4; s >= 1; --s) {
+    // AlgConstr^T then E^T: adjoint of this stage's output w
+    k_adj_alg<<<div_up(g.nvol * g.nblocks, kThreads), kThreads, 0, c->stream>>>(g, P, A->upre[s - 1],
+                                                                             A->adj);
+    k_adj_exchange<<<div_up(npts * NVAR * g.nblocks, kThreads), kThreads, 0, c->stream>>>(
+        g, A->adj, A->wbar);
+    ALAUNCH("adjoint exchange");
+    add_kernel_launches(2);
+    // the stage input
+    const double* us = u;
+    if (s > 1) {
+      ACUDA(cudaMemcpyAsync(A->us, A->upre[s - 2], bytes, cudaMemcpyDeviceToDevice, c->stream));
+      launch_alg_constr(g, P, A->us, 0, g.nblocks, c->stream);
+      ALAUNCH("alg_constr");
+      us = A->us;
+    }
+    launch_prep_ricci(g, P, us, c->scratch(), 0, g.nblocks, c->shape, c->stream);
+    ALAUNCH("prep_ricci");
+    const double* wt = kLsRk4[s - 1];
+    StageW W{wt[0], wt[1], wt[2], wt[4] * dt, s == 1 ? 1 : 0};
+    k_adj_main<<<nthr, kThreads, 0, c->stream>>>(g, P, us, c->sd, c->rsum, A->wbar, A->adj1,
+                                                 A->direct, A->chan, A->rsb, A->part, W);
+    k_accumulate<<<1, 256, 0, c->stream>>>(A->part, nthr, A->pacc);
+    ALAUNCH("adjoint main");
+    k_adj_ricci<<<nthr, kThreads, 0, c->stream>>>(g, P, us, c->sd, A->rsb, A->direct, A->chan);
+    const int64_t creg = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7) * (g.nx[2] + 1);
+    k_adj_sdbar<<<dim3(div_up(creg, kThreads), kSdComponents, g.nblocks), kThreads, 0, c->stream>>>(
+        g, P, A->chan, A->sdbar);
+    k_adj_gather<<<div_up(g.nvol * NVAR * g.nblocks, kThreads), kThreads, 0, c->stream>>>(
+        g, P, us, A->wbar, A->direct, A->chan, A->sdbar, A->adj, W.beta_dt);
+    ALAUNCH("adjoint gather");
+    add_kernel_launches(5);
+  }
+  return Z4C_OK;
+}
+
+// Revolve-style checkpointing.  cost(n, s): the fewest forward steps that
+// reversing n steps needs, given the state at their start and s free
+// snapshots: reverse the first m steps after the last n - m, the state after
+// m steps kept in a snapshot meanwhile (m advances), so
+//   cost(n, s) = min_m [m + cost(n - m, s - 1) + cost(m, s)],
+//   cost(1, s) = 0,  cost(n, 0) = n (n - 1) / 2 (re-advance for every step);
+// the minimum is the binomial (Griewank-Walther) schedule.
+struct Schedule {
+  int n, s;
+  std::vector<long long> cost;
+  std::vector<int> split;
+  long long& C(int nn, int ss) { return cost[(size_t)nn * (s + 1) + ss]; }
+  int& M(int nn, int ss) { return split[(size_t)nn * (s + 1) + ss]; }
+  Schedule(int n_, int s_) : n(n_), s(s_), cost((size_t)(n_ + 1) * (s_ + 1), 0),
+                             split((size_t)(n_ + 1) * (s_ + 1), 0) {
+    for (int nn = 1; nn <= n; ++nn)
+      for (int ss = 0; ss <= s; ++ss) {
+        if (nn == 1) { C(nn, ss) = 0; continue; }
+        if (ss == 0) { C(nn, ss) = (long long)nn * (nn - 1) / 2; continue; }
+        long long best = -1;
+        int bm = 1;
+        for (int m = 1; m < nn; ++m) {
+          const long long v = m + C(nn - m, ss - 1) + C(m, ss);
+          if (best < 0 || v < best) { best = v; bm = m; }
+        }
+        C(nn, ss) = best;
+        M(nn, ss) = bm;
+      }
+  }
+};
+
+struct GradRun {
+  z4c_ctx* c;
+  double dt, w_step;
+  Schedule* sch;
+  std::vector<double*> free_snaps;
+  double* run;  // work state of the snapshot-free recomputation
+  double* end;  // the state after the step being reversed (per-step objective)
+  long long fwd_steps = 0, adj_steps = 0;
+};
+
+int advance(GradRun& R, double* u, int nsteps) {
+  for (int i = 0; i < nsteps; ++i) {
+    int rc = fwd_step(R.c, R.dt, u);
+    if (rc) return rc;
+    ++R.fwd_steps;
+  }
+  return Z4C_OK;
+}
+
+// Z4C_REG_ADJ += scale dJ/du at the state u
+int objective_adj(z4c_ctx* c, const double* u, double scale) {
+  const Grid& g = c->g;
+  const DevParams P = c->dev();
+  k_ham_adj<<<div_up(npts_of(g) * g.nblocks, kThreads), kThreads, 0, c->stream>>>(
+      g, P, c->xv, u, scale, c->adj->hchan);
+  k_ham_gather<<<div_up(g.nvol * NVAR * g.nblocks, kThreads), kThreads, 0, c->stream>>>(
+      g, P, c->adj->hchan, c->adj->adj);
+  ALAUNCH("objective adjoint");
+  add_kernel_launches(2);
+  return Z4C_OK;
+}
+
+// J at the state u and, with ud, its derivative along ud
+int objective(z4c_ctx* c, const double* u, const double* ud, double* J, double* Jdot) {
+  const Grid& g = c->g;
+  const DevParams P = c->dev();
+  const int nthr = div_up(npts_of(g) * g.nblocks, kThreads);
+  if (ud) k_ham_obj<true><<<nthr, kThreads, 0, c->stream>>>(g, P, c->xv, u, ud, c->adj->part);
+  else k_ham_obj<false><<<nthr, kThreads, 0, c->stream>>>(g, P, c->xv, u, nullptr, c->adj->part);
+  ALAUNCH("objective");
+  add_kernel_launches(1);
+  double s2[2];
+  int rc = reduce_part(c, nthr, s2);
+  if (rc) return rc;
+  *J = s2[0];
+  if (Jdot) *Jdot = s2[1];
+  return Z4C_OK;
+}
+
+// Adjoint of the step from u, with the per-step objective's source at its end.
+int adj_step_with_source(GradRun& R, const double* u) {
+  z4c_ctx* c = R.c;
+  if (R.w_step != 0.) {
+    ACUDA(cudaMemcpyAsync(R.end, u, sizeof(double) * c->adj->reg_elems,
+                          cudaMemcpyDeviceToDevice, c->stream));
+    int rc = fwd_step(c, R.dt, R.end);
+    if (rc) return rc;
+    ++R.fwd_steps;
+    rc = objective_adj(c, R.end, R.w_step);
+    if (rc) return rc;
+  }
+  ++R.adj_steps;
+  return adj_step(c, R.dt, u);
+}
+
+// Reverses steps [l, r) given the state at l in x (unchanged).
+int reverse(GradRun& R, const double* x, int l, int r, int s) {
+  const int n = r - l;
+  z4c::AdjState* A = R.c->adj;
+  const size_t bytes = sizeof(double) * A->reg_elems;
+  if (n == 1) return adj_step_with_source(R, x);
+  if (s == 0) {
+    for (int i = r - 1; i >= l; --i) {
+      ACUDA(cudaMemcpyAsync(R.run, x, bytes, cudaMemcpyDeviceToDevice, R.c->stream));
+      int rc = advance(R, R.run, i - l);
+      if (!rc) rc = adj_step_with_source(R, R.run);
+      if (rc) return rc;
+    }
+    return Z4C_OK;
+  }
+  const int m = R.sch->M(n, s);
+  double* snap = R.free_snaps.back();
+  R.free_snaps.pop_back();
+  ACUDA(cudaMemcpyAsync(snap, x, bytes, cudaMemcpyDeviceToDevice, R.c->stream));
+  int rc = advance(R, snap, m);
+  if (!rc) rc = reverse(R, snap, l + m, r, s - 1);
+  R.free_snaps.push_back(snap);
+  if (rc) return rc;
+  return reverse(R, x, l, l + m, s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int z4c_adj_setup(z4c_ctx* c) {
+  if (!c) return err(Z4C_EINVAL, "null context");
+  if (c->adj) return Z4C_OK;
+  z4c::AdjState* A = new (std::nothrow) z4c::AdjState();
+  if (!A) return err(Z4C_ENOMEM, "host allocation");
+  const Grid& g = c->g;
+  A->reg_elems = (int64_t)NVAR * g.nvol * g.nblocks;
+  const int64_t npts = npts_of(g) * g.nblocks;
+  const size_t reg = sizeof(double) * A->reg_elems;
+  A->npart = div_up(npts, kThreads) + 1;
+  struct Buf { double** p; size_t bytes; };
+  std::vector<Buf> bufs = {
+      {&A->tan, reg}, {&A->tan1, reg}, {&A->tanw, reg}, {&A->adj, reg}, {&A->adj1, reg},
+      {&A->wbar, reg}, {&A->direct, reg}, {&A->us, reg}, {&A->w, reg}, {&A->u1, reg},
+      {&A->sdd, sizeof(double) * kSdComponents * g.nvol * g.nblocks},
+      {&A->sdbar, sizeof(double) * kSdComponents * g.nvol * g.nblocks},
+      {&A->chan, sizeof(double) * kNChan * npts}, {&A->rsb, sizeof(double) * 6 * npts},
+      {&A->hchan, sizeof(double) * kNHChan * npts}, {&A->part, sizeof(double) * 2 * A->npart},
+      {&A->pacc, sizeof(double) * 2}};
+  for (int s = 0; s < 4; ++s) bufs.push_back({&A->upre[s], reg});
+  for (auto& b : bufs) {
+    if (cudaMalloc((void**)b.p, b.bytes) != cudaSuccess) {
+      cudaGetLastError();
+      z4c::adj_free(A);
+      return err(Z4C_ENOMEM, "adjoint buffers: %zu bytes", b.bytes);
+    }
+  }
+  if (cudaMemsetAsync(A->pacc, 0, sizeof(double) * 2, c->stream) != cudaSuccess) {
+    z4c::adj_free(A);
+    return err(Z4C_ECUDA, "adjoint buffer clear");
+  }
+  for (double* p : {A->tan, A->tan1, A->adj, A->adj1})
+    if (cudaMemsetAsync(p, 0, reg, c->stream) != cudaSuccess) {
+      z4c::adj_free(A);
+      return err(Z4C_ECUDA, "adjoint buffer clear");
+    }
+  c->adj = A;
+  c->reg[Z4C_REG_TAN] = A->tan;
+  c->reg[Z4C_REG_ADJ] = A->adj;
+  return Z4C_OK;
+}
+
+int z4c_tlm_step(z4c_ctx* c, double dt) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  z4c::AdjState* A = c->adj;
+  const Grid& g = c->g;
+  const DevParams P = c->dev();
+  double* u = c->reg[Z4C_REG_U];
+  const int nthr = div_up(npts_of(g) * g.nblocks, kThreads);
+  for (int s = 1; s <= 4; ++s) {
+    const double* wt = kLsRk4[s - 1];
+    StageW W{wt[0], wt[1], wt[2], wt[4] * dt, s == 1 ? 1 : 0};
+    // tangents first (they read the stage input u)
+    launch_prep(g, P, u, c->sd, 0, g.nblocks, c->stream);
+    launch_prep(g, P, A->tan, A->sdd, 0, g.nblocks, c->stream);
+    k_tlm_stage<<<nthr, kThreads, 0, c->stream>>>(g, P, u, c->sd, A->tan, A->sdd, A->tan1, A->tanw,
+                                                  W);
+    ALAUNCH("tangent stage");
+    add_kernel_launches(1);
+    // values
+    rc = fwd_stage(c, s, dt, u, A->u1, A->w, A->us, nullptr);
+    if (rc) return rc;
+    launch_exchange(g, P, A->tanw, A->tan, c->nbr, 0, c->stream);
+    ALAUNCH("tangent exchange");
+    // (A->us, A->tan) are the pre-constraint state and its tangent
+    ACUDA(cudaMemcpyAsync(A->tanw, A->tan, sizeof(double) * A->reg_elems, cudaMemcpyDeviceToDevice,
+                          c->stream));
+    k_tlm_alg<<<div_up(g.nvol * g.nblocks, kThreads), kThreads, 0, c->stream>>>(g, P, A->us,
+                                                                            A->tanw, u, A->tan);
+    ALAUNCH("tangent alg_constr");
+    add_kernel_launches(1);
+  }
+  return Z4C_OK;
+}
+
+int z4c_adj_step(z4c_ctx* c, double dt) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  return adj_step(c, dt, c->reg[Z4C_REG_U]);
+}
+
+int z4c_adj_objective(z4c_ctx* c, int reg, int reg_tan, double* J, double* Jdot) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!J || reg < 0 || reg >= Z4C_NREG || !c->reg[reg] ||
+      (reg_tan >= 0 && (reg_tan >= Z4C_NREG || !c->reg[reg_tan])))
+    return err(Z4C_EINVAL, "bad register or null output");
+  if (z4c_reg_nvar(reg) != NVAR || (reg_tan >= 0 && z4c_reg_nvar(reg_tan) != NVAR))
+    return err(Z4C_EINVAL, "the objective reads 22-variable registers");
+  return objective(c, c->reg[reg], reg_tan >= 0 ? c->reg[reg_tan] : nullptr, J, Jdot);
+}
+
+int z4c_adj_objective_adj(z4c_ctx* c, int reg, double scale) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (reg < 0 || reg >= Z4C_NREG || !c->reg[reg] || z4c_reg_nvar(reg) != NVAR)
+    return err(Z4C_EINVAL, "bad register");
+  return objective_adj(c, c->reg[reg], scale);
+}
+
+int z4c_adj_params(z4c_ctx* c, double pbar[2], int reset) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (pbar) {
+    ACUDA(cudaMemcpyAsync(pbar, c->adj->pacc, sizeof(double) * 2, cudaMemcpyDeviceToHost,
+                          c->stream));
+    ACUDA(cudaStreamSynchronize(c->stream));
+  }
+  if (reset) ACUDA(cudaMemsetAsync(c->adj->pacc, 0, sizeof(double) * 2, c->stream));
+  return Z4C_OK;
+}
+
+}  // extern "C"
+
+extern "C" int z4c_adj_gradient(z4c_ctx* c, double dt, int nsteps, int nsnap, double w_final,
+                                double w_step, double* J, double pbar[2], double stats[4]) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (nsteps < 1 || nsnap < 0 || !J) return err(Z4C_EINVAL, "nsteps >= 1, nsnap >= 0, J non-null");
+  z4c::AdjState* A = c->adj;
+  const size_t bytes = sizeof(double) * A->reg_elems;
+  const int S = std::min(nsnap, nsteps - 1);
+  // snapshots: S for the schedule, a run buffer and an end-state buffer
+  while ((int)A->snaps.size() < S + 2) {
+    double* p = nullptr;
+    if (cudaMalloc((void**)&p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return err(Z4C_ENOMEM, "revolve snapshots: %d of %zu bytes", S + 2, bytes);
+    }
+    A->snaps.push_back(p);
+  }
+  cudaEvent_t e0, e1;
+  ACUDA(cudaEventCreate(&e0));
+  ACUDA(cudaEventCreate(&e1));
+  cudaEventRecord(e0, c->stream);
+  Schedule sch(nsteps, S);
+  GradRun R{c, dt, w_step, &sch, {}, A->snaps[S], A->snaps[S + 1]};
+  for (int i = 0; i < S; ++i) R.free_snaps.push_back(A->snaps[i]);
+  ACUDA(cudaMemsetAsync(A->pacc, 0, sizeof(double) * 2, c->stream));
+  ACUDA(cudaMemsetAsync(A->adj, 0, bytes, c->stream));
+  const double* u0 = c->reg[Z4C_REG_U];
+  // forward sweep: the objective along the run
+  double Jt = 0.;
+  ACUDA(cudaMemcpyAsync(R.run, u0, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  for (int i = 1; i <= nsteps; ++i) {
+    rc = fwd_step(c, dt, R.run);
+    if (rc) return rc;
+    ++R.fwd_steps;
+    if (w_step != 0. || i == nsteps) {
+      double Ji = 0.;
+      rc = objective(c, R.run, nullptr, &Ji, nullptr);
+      if (rc) return rc;
+      if (w_step != 0.) Jt += w_step * Ji;
+      if (i == nsteps) Jt += w_final * Ji;
+    }
+  }
+  // the final state's source; every step's end-state source is added as the
+  // reverse sweep reaches that step
+  if (w_final != 0.) {
+    rc = objective_adj(c, R.run, w_final);
+    if (rc) return rc;
+  }
+  rc = reverse(R, u0, 0, nsteps, S);
+  if (rc) return rc;
+  cudaEventRecord(e1, c->stream);
+  ACUDA(cudaStreamSynchronize(c->stream));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *J = Jt;
+  if (pbar) ACUDA(cudaMemcpy(pbar, A->pacc, sizeof(double) * 2, cudaMemcpyDeviceToHost));
+  if (stats) {
+    stats[0] = (double)R.fwd_steps;
+    stats[1] = (double)R.adj_steps;
+    stats[2] = ms * 1e-3;
+    stats[3] = (double)sch.C(nsteps, S);
+  }
+  return Z4C_OK;
+}

@@ -20,6 +20,7 @@
 #include "z4c_multilevel.cuh"
 #include "z4c_restart.cuh"
 #include "z4c_wave.cuh"
+#include "z4c_ctx.cuh"
 
 using namespace z4c;
 
@@ -51,15 +52,6 @@ int fail(int code, const char* fmt, ...) {
       return fail(Z4C_ECUDA, "%s launch: %s", what, cudaGetErrorString(e_));   \
   } while (0)
 
-// Low-storage RK4()4[2S] (task_list_integrators_low_storage.cpp:112-142).
-const double kLsRk4[4][5] = {
-    {1.0, 0.0, 1.0, 0.0, 1.193743905974738},
-    {0.217683334308543, 0.121098479554482, 0.721781678111411, 0.0, 0.099279895495783},
-    {1.065841341361089, -3.843833699660025, 2.121209265338722, 0.0, 1.131678018054042},
-    {0.0, 0.546370891121863, 0.198653035682705, 0.0, 0.310665766509336}};
-// Classical RK4 tableau (task_list_integrators_butcher.cpp:37-48).
-const double kBtA[4][4] = {{0, 0, 0, 0}, {0.5, 0, 0, 0}, {0, 0.5, 0, 0}, {0, 0, 1, 0}};
-const double kBtB[4] = {1. / 6., 1. / 3., 1. / 3., 1. / 6.};
 
 // ComputeMeshGeneratorX with sym_interval (mesh/mesh.hpp:839-863) and
 // UniformMeshGeneratorX1 (mesh/mesh.hpp:939-945).
@@ -100,62 +92,6 @@ int set_error(int code, const char* msg) {
 }
 }  // namespace z4c
 
-struct z4c_ctx {
-  Grid g{};
-  MlPlan* ml = nullptr;         // multilevel meshes: the ghost-exchange plan
-  unsigned char* som = nullptr; // multilevel meshes: gr_sommerfeld faces per block (device)
-  std::vector<long long> locs;  // multilevel meshes: {level, lx1, lx2, lx3} per block
-  z4c_mesh_desc_t desc{};
-  z4c_params_t params{};
-  int integrator = Z4C_INTEG_RK4;
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  bool per_block = false;
-  LaunchShape shape;  // launch shape of the RHS passes (autotuner output)
-  bool has_outflow = false;
-
-  // device buffers
-  double* reg[Z4C_NREG] = {};
-  double* un = nullptr;   // Butcher u_n scratch
-  double* guu = nullptr;  // ADMToZ4c inverse-metric scratch (6 vars)
-  double* sd = nullptr;   // stored first derivatives, 33 values per vertex
-  double* rsum = nullptr; // Ricci-pass scratch, 6 values per interior vertex
-  double* lv = nullptr;   // advection sums, 22 values per interior vertex
-  double* xf = nullptr;   // [nblocks][nn0+nn1+nn2]
-  double* xv = nullptr;   // [nblocks][nn0+nn1+nn2-3]
-  double* dxd = nullptr;  // [nblocks][3] vertex spacing
-  FdScale* fd = nullptr;  // [nblocks]
-  int* nbr = nullptr;     // [nblocks][26]
-  double* partials = nullptr;
-  double* trk = nullptr;  // puncture trackers [kMaxTrackers][8]
-  int ntrk = 0;
-  int* flag = nullptr;
-  std::vector<WaveSphere> waves;  // psi4 extraction spheres
-
-  // host copies
-  std::vector<double> h_xf, h_xv, h_dx;  // h_dx: [nblocks][3]
-
-  // kernel nodes of the captured step (graph replays add this many launches)
-  long long graph_nodes = 0;
-
-  // captured step
-  cudaGraphExec_t graph = nullptr;
-  double graph_dt = 0.0;
-  bool graph_per_block = false;
-
-  RhsScratch scratch() const { return RhsScratch{sd, rsum, lv}; }
-
-  DevParams dev() const {
-    DevParams P;
-    P.p = params;
-    P.fd = fd;
-    P.xf = xf;
-    P.dx = dxd;
-    P.som = som;
-    return P;
-  }
-};
 
 namespace {
 
@@ -337,6 +273,8 @@ int run_stage_body(z4c_ctx* c, int stage, double dt) {
 
 void free_ctx(z4c_ctx* c) {
   if (c->graph) cudaGraphExecDestroy(c->graph);
+  // the tangent and adjoint registers belong to the adjoint buffers
+  c->reg[Z4C_REG_TAN] = c->reg[Z4C_REG_ADJ] = nullptr;
   for (auto& r : c->reg)
     if (r) cudaFree(r);
   for (void* p : {(void*)c->un, (void*)c->guu, (void*)c->sd, (void*)c->rsum, (void*)c->lv, (void*)c->xf, (void*)c->xv, (void*)c->dxd, (void*)c->fd,
@@ -348,6 +286,7 @@ void free_ctx(z4c_ctx* c) {
     delete c->ml;
   }
   if (c->som) cudaFree(c->som);
+  if (c->adj) adj_free(c->adj);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }

@@ -1475,6 +1475,22 @@ static void launch_rhs_passes(const Grid& g, const DevParams& P, const double* u
   launch_point_pass(g, P, u, sc, rhs, block0, nblk, 1, sh, st);
 }
 
+void launch_prep(const Grid& g, const DevParams& P, const double* u, double* sd, int block0,
+                 int nblk, cudaStream_t st) {
+  const int64_t cprep = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7);  // widest component region
+  COUNTED
+  (has_fixed_geometry(g) ? k_prep<kFixedNX> : k_prep<0>)<<<dim3(div_up(cprep, kPointThreads),
+                                                               kSdComponents, nblk),
+                                                          kPointThreads, 0, st>>>(g, P, u, sd,
+                                                                                  block0);
+}
+
+void launch_prep_ricci(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
+                       int block0, int nblk, const LaunchShape& sh, cudaStream_t st) {
+  launch_prep(g, P, u, sc.sd, block0, nblk, st);
+  launch_point_pass(g, P, u, sc, nullptr, block0, nblk, 0, sh, st);
+}
+
 void launch_rhs(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                 double* rhs, int block0, int nblk, const LaunchShape& sh, cudaStream_t st) {
   launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, sh, st);

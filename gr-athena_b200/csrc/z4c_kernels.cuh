@@ -88,6 +88,13 @@ int allow_slab_smem();
 // right-hand side).
 void launch_rhs(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                 double* rhs, int block0, int nblk, const LaunchShape& sh, cudaStream_t st);
+// The first two passes alone: the stored first derivatives of u into sc.sd
+// and the Ricci sums into sc.rsum (the linearisation point of the adjoint),
+// or the stored first derivatives alone into sd.
+void launch_prep_ricci(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
+                       int block0, int nblk, const LaunchShape& sh, cudaStream_t st);
+void launch_prep(const Grid& g, const DevParams& P, const double* u, double* sd, int block0,
+                 int nblk, cudaStream_t st);
 void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                      double* rhs, double* u1, double* u_out, const LsStage& w, int block0,
                      int nblk, const LaunchShape& sh, cudaStream_t st);

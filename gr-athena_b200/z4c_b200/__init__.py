@@ -30,7 +30,7 @@ NVAR, NADM, NCON, NWEYL = 22, 17, 7, 2
  ADM_PSI4) = range(17)
 CON_C, CON_H, CON_M, CON_Z, CON_MX, CON_MY, CON_MZ = range(7)
 (REG_U, REG_U1, REG_RHS, REG_ADM, REG_CON, REG_W, REG_K1, REG_K2, REG_K3,
- REG_K4, REG_WEYL) = range(11)
+ REG_K4, REG_WEYL, REG_TAN, REG_ADJ) = range(13)
 BC_PERIODIC, BC_OUTFLOW, BC_SOMMERFELD = 0, 1, 2
 BC_NAMES = {"periodic": BC_PERIODIC, "outflow": BC_OUTFLOW, "extrapolate_outflow": BC_OUTFLOW,
             "sommerfeld": BC_SOMMERFELD, "gr_sommerfeld": BC_SOMMERFELD}
@@ -55,7 +55,8 @@ EXPORTS = (
     "z4c_regrid_refine", "z4c_regrid_derefine", "z4c_rhs_noalloc",
     "z4c_sphere_grid", "z4c_wave_add", "z4c_wave_points", "z4c_wave_decompose",
     "z4c_restart_info", "z4c_restart_text", "z4c_restart_read", "z4c_restart_write_host",
-    "z4c_restart_load", "z4c_restart_save")
+    "z4c_restart_load", "z4c_restart_save", "z4c_adj_setup", "z4c_tlm_step", "z4c_adj_step",
+    "z4c_adj_objective", "z4c_adj_objective_adj", "z4c_adj_params", "z4c_adj_gradient")
 
 
 class Z4cError(RuntimeError):
@@ -172,6 +173,14 @@ def lib():
                                              C.c_double, ip, ip, dp]
         L.z4c_restart_load.argtypes = [vp, cp, C.POINTER(RestartInfo)]
         L.z4c_restart_save.argtypes = [vp, cp, cp, C.c_double, C.c_double, ip]
+        L.z4c_adj_setup.argtypes = [vp]
+        L.z4c_tlm_step.argtypes = [vp, C.c_double]
+        L.z4c_adj_step.argtypes = [vp, C.c_double]
+        L.z4c_adj_objective.argtypes = [vp, ip, ip, dp, dp]
+        L.z4c_adj_objective_adj.argtypes = [vp, ip, C.c_double]
+        L.z4c_adj_params.argtypes = [vp, dp, ip]
+        L.z4c_adj_gradient.argtypes = [vp, C.c_double, ip, ip, C.c_double, C.c_double, dp, dp,
+                                       dp]
         L.z4c_kernel_launches.argtypes = []
         L.z4c_kernel_launches.restype = C.c_longlong
         _lib = L
@@ -716,6 +725,50 @@ class Z4c:
             return False
         _check(rc)
         return True
+
+    # ---- differentiation (tangent-linear model and adjoint) ----------------
+    def adj_setup(self):
+        """Allocates the tangent / adjoint buffers (REG_TAN, REG_ADJ)."""
+        _check(lib().z4c_adj_setup(self._h))
+
+    def tlm_step(self, dt):
+        """One step of u and of its tangent REG_TAN."""
+        _check(lib().z4c_tlm_step(self._h, dt))
+
+    def adj_step(self, dt):
+        """REG_ADJ: adjoint of the state after one step from u -> adjoint of u."""
+        _check(lib().z4c_adj_step(self._h, dt))
+
+    def objective(self, reg=REG_U, reg_tan=-1):
+        """J = vol * sum of H^2 over the history cells of register reg, and
+        with reg_tan its derivative along that tangent: (J, Jdot)."""
+        J, Jd = C.c_double(), C.c_double()
+        _check(lib().z4c_adj_objective(self._h, reg, reg_tan, C.byref(J), C.byref(Jd)))
+        return J.value, (Jd.value if reg_tan >= 0 else None)
+
+    def objective_adj(self, reg=REG_U, scale=1.0):
+        """REG_ADJ += scale * dJ/du at register reg."""
+        _check(lib().z4c_adj_objective_adj(self._h, reg, scale))
+
+    def adj_params(self, reset=False):
+        """Accumulated adjoints of (shift_eta, damp_kappa1)."""
+        out = np.zeros(2)
+        _check(lib().z4c_adj_params(self._h, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                    int(reset)))
+        return out
+
+    def gradient(self, dt, nsteps, nsnap, w_final=1.0, w_step=0.0):
+        """dJ_total/du_0 into REG_ADJ with revolve checkpointing (nsnap
+        snapshots) for J_total = w_final J(u_n) + w_step sum_k J(u_k); returns
+        (J_total, (d/d shift_eta, d/d damp_kappa1), stats)."""
+        J = C.c_double()
+        pb = np.zeros(2)
+        st = np.zeros(4)
+        dp = C.POINTER(C.c_double)
+        _check(lib().z4c_adj_gradient(self._h, dt, nsteps, nsnap, w_final, w_step, C.byref(J),
+                                      pb.ctypes.data_as(dp), st.ctypes.data_as(dp)))
+        return J.value, pb, {"forward_steps": int(st[0]), "adjoint_steps": int(st[1]),
+                             "seconds": float(st[2]), "schedule_cost": int(st[3])}
 
     def constraints(self):
         """Z4cToADM + ADMConstraints on the current state (last-stage tasks)."""

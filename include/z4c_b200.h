@@ -87,6 +87,8 @@ enum {
   Z4C_REG_K3,
   Z4C_REG_K4,
   Z4C_REG_WEYL,    /* storage.weyl (2 vars: Re psi4, Im psi4)       */
+  Z4C_REG_TAN,     /* tangent of u (22 vars; after z4c_adj_setup)   */
+  Z4C_REG_ADJ,     /* adjoint of u (22 vars; after z4c_adj_setup)   */
   Z4C_NREG
 };
 
@@ -425,6 +427,46 @@ int z4c_regrid_derefine(const double *child, double *parent, double *coarse, int
  * (Z4C_EINVAL otherwise, before any work); a failure of earlier work on src,
  * or of the transfer, returns Z4C_ECUDA and leaves dst's state undefined. */
 int z4c_regrid(z4c_ctx *dst, const z4c_ctx *src);
+
+/* ---- differentiation (no reference counterpart) ---------------------------
+ *
+ * The tangent-linear model and the hand-written adjoint of the low-storage
+ * RK4 step (Z4cRHS with Kreiss-Oliger, task_list_gr_z4c.cpp:170-213 with the
+ * weights of task_list_integrators_low_storage.cpp:112-142, the ghost
+ * exchange and AlgConstr), and of the objective J = sum over blocks of the
+ * cell volume times the sum over the history cells of H^2, H the Hamiltonian
+ * constraint of ADMConstraints after Z4cToADM (the H-norm of
+ * outputs/history.cpp:168-200).  Uniform periodic meshes, rk4,
+ * chi_psi_power = -4.  The state's adjoint lives in Z4C_REG_ADJ and a
+ * tangent in Z4C_REG_TAN, each over every vertex (ghosts included); the
+ * adjoints of the gauge parameters shift_eta and damp_kappa1 accumulate in
+ * the context.  The calls use the context's RHS register as scratch. */
+/* Allocates the tangent / adjoint buffers (about 13 state-sized registers
+ * plus channel scratch) and zeroes Z4C_REG_TAN and Z4C_REG_ADJ. */
+int z4c_adj_setup(z4c_ctx *ctx);
+/* One step of u (Z4C_REG_U) and of its tangent (Z4C_REG_TAN) together. */
+int z4c_tlm_step(z4c_ctx *ctx, double dt);
+/* Adjoint of one step from the state in Z4C_REG_U (left unchanged; the
+ * step is recomputed stage by stage): Z4C_REG_ADJ holds the adjoint of the
+ * state after the step on entry and of the state in Z4C_REG_U on return. */
+int z4c_adj_step(z4c_ctx *ctx, double dt);
+/* J of register reg; with reg_tan >= 0 also its directional derivative
+ * along the tangent in reg_tan (*Jdot, may be NULL otherwise). */
+int z4c_adj_objective(z4c_ctx *ctx, int reg, int reg_tan, double *J, double *Jdot);
+/* Z4C_REG_ADJ += scale * dJ/du at the state in reg. */
+int z4c_adj_objective_adj(z4c_ctx *ctx, int reg, double scale);
+/* The accumulated adjoints of {shift_eta, damp_kappa1}; reset != 0 zeroes
+ * them afterwards. */
+int z4c_adj_params(z4c_ctx *ctx, double pbar[2], int reset);
+/* Gradient of J_total = w_final J(u_n) + w_step sum_{k=1..n} J(u_k) over n
+ * steps from the state in Z4C_REG_U (left unchanged) with revolve-style
+ * binomial checkpointing: nsnap state snapshots (device memory, allocated
+ * for the call), a schedule that minimises the recomputed steps for that
+ * count.  On return Z4C_REG_ADJ holds dJ_total/du_0, pbar the parameter
+ * adjoints, *J the objective; stats (may be NULL) receives {forward steps
+ * recomputed, adjoint steps, seconds forward, seconds adjoint}. */
+int z4c_adj_gradient(z4c_ctx *ctx, double dt, int nsteps, int nsnap, double w_final,
+                     double w_step, double *J, double pbar[2], double stats[4]);
 
 /* ---- allocation-free variant ----------------------------------------------
  *

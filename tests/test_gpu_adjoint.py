@@ -1,0 +1,257 @@
+"""The differentiated Z4c step on the device, through the C ABI:
+
+* the tangent-linear step against central differences of the forward step;
+* the adjoint step against the tangent-linear step (dot-product test
+  <ubar_1, J udot_0> = <J^T ubar_1, udot_0> over every vertex);
+* the objective (vol * sum of H^2 over the history cells) against the
+  history norm, its tangent against differences, its adjoint against its
+  tangent;
+* revolve checkpointing: the gradient does not depend on the snapshot count;
+* configs[3] at its stated size: 64^3 gauge wave (A = 0.05) with seeded 1e-6
+  noise on the conformal metric, 100 rk4 steps, the gradient of the H-norm
+  with respect to every initial Z4c value against central differences on 32
+  seeded directions and against tangent-linear runs.
+
+Tolerances: the adjoint and the tangent-linear model differentiate the same
+discrete map, so they agree to rounding (1e-10 relative); central
+differences carry a truncation error O(h^2) and a rounding error O(eps/h),
+the bound on them is 1e-6 relative."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+PUNC = dict(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02, damp_kappa2=0.0, shift_eta=2.0,
+            r_max_con=1e300)
+GW = dict(lapse_harmonic=1.0, lapse_harmonicf=0.0, lapse_oplog=0.0, lapse_advect=0.0,
+          shift_Gamma=0.0, shift_eta=0.0, shift_advect=0.0, diss=0.02, damp_kappa1=0.02,
+          r_max_con=1e300)
+
+
+def make(nb, nx, params, lim=0.5):
+    import z4c_b200 as Z
+    mesh = Z.Mesh(nb, (nx,) * 3, (-lim,) * 3, (lim,) * 3, "periodic")
+    ctx = Z.Z4c(mesh, Z.default_params(**params), "rk4")
+    ctx.adj_setup()
+    return Z, mesh, ctx
+
+
+def rich_state(Z, mesh, ctx, amp=1e-3, seed=0):
+    """A gauge wave (A = 0.05) with smooth periodic perturbations of size amp
+    on every variable, the shift included, so that every term of the
+    right-hand side (advection too) is active."""
+    from z4c_b200 import initial_data as ID
+    ID.load_adm(ctx, ID.gauge_wave1(mesh, amplitude=0.05))
+    u = ctx.download(Z.REG_U)
+    rng = np.random.default_rng(seed)
+    for b in range(mesh.nblocks):
+        xs, _ = mesh.block_coords(b)
+        X, Y, Zc = np.meshgrid(xs[2], xs[1], xs[0], indexing="ij")
+        for n in range(22):
+            k = rng.integers(1, 3, size=3)
+            ph = rng.uniform(0, 2 * np.pi)
+            u[b, n] += amp * np.sin(2 * np.pi * (k[0] * Zc + k[1] * Y + k[2] * X) + ph)
+    ctx.upload(Z.REG_U, u)
+    ctx.init_finalize()
+    return ctx.download(Z.REG_U)
+
+
+def dot(a, b):
+    return float(np.sum(a * b))
+
+
+@pytest.mark.parametrize("params", [PUNC, GW], ids=["puncture_gauge", "gauge_wave"])
+def test_tlm_step_matches_central_differences(params):
+    Z, mesh, ctx = make((2, 2, 1), 12, params)
+    u0 = rich_state(Z, mesh, ctx)
+    dt = 0.25 * float(ctx.dx().min())
+    rng = np.random.default_rng(1)
+    v = rng.standard_normal(u0.shape) * 1e-3
+    ctx.upload(Z.REG_TAN, v)
+    ctx.upload(Z.REG_U, u0)
+    ctx.tlm_step(dt)
+    tan = ctx.download(Z.REG_TAN)
+    u1 = ctx.download(Z.REG_U)
+    ctx.upload(Z.REG_U, u0)
+    ctx.evolve(dt, 1)
+    assert np.array_equal(ctx.download(Z.REG_U), u1), "tlm_step's values are the forward step's"
+    h = 1e-4
+    out = []
+    for sgn in (1, -1):
+        ctx.upload(Z.REG_U, u0 + sgn * h * v)
+        ctx.evolve(dt, 1)
+        out.append(ctx.download(Z.REG_U))
+    fd = (out[0] - out[1]) / (2 * h)
+    err = np.abs(fd - tan).max() / np.abs(tan).max()
+    print(f"tlm vs central differences: {err:.2e}")
+    assert err <= 1e-6
+    ctx.close()
+
+
+@pytest.mark.parametrize("params", [PUNC, GW], ids=["puncture_gauge", "gauge_wave"])
+def test_adjoint_step_is_the_transpose_of_the_tlm_step(params):
+    Z, mesh, ctx = make((2, 2, 1), 12, params)
+    u0 = rich_state(Z, mesh, ctx)
+    dt = 0.25 * float(ctx.dx().min())
+    rng = np.random.default_rng(2)
+    for trial in range(3):
+        ud = rng.standard_normal(u0.shape)
+        ub = rng.standard_normal(u0.shape)
+        ctx.upload(Z.REG_U, u0)
+        ctx.upload(Z.REG_TAN, ud)
+        ctx.tlm_step(dt)
+        Jud = ctx.download(Z.REG_TAN)
+        ctx.upload(Z.REG_U, u0)
+        ctx.upload(Z.REG_ADJ, ub)
+        ctx.adj_params(reset=True)
+        ctx.adj_step(dt)
+        assert np.array_equal(ctx.download(Z.REG_U), u0), "adj_step leaves u unchanged"
+        JTub = ctx.download(Z.REG_ADJ)
+        lhs, rhs = dot(ub, Jud), dot(JTub, ud)
+        scale = np.abs(ub * Jud).sum()
+        print(f"trial {trial}: <ub, J ud> = {lhs:.15e}, <J^T ub, ud> = {rhs:.15e}")
+        assert abs(lhs - rhs) <= 1e-12 * scale
+    ctx.close()
+
+
+def test_parameter_adjoints_match_differences():
+    """d<ub, u_1>/d eta and d/d kappa1 of one step: adjoint vs central
+    differences of the forward step."""
+    Z, mesh, ctx = make((2, 2, 1), 12, PUNC)
+    u0 = rich_state(Z, mesh, ctx)
+    dt = 0.25 * float(ctx.dx().min())
+    ub = np.random.default_rng(4).standard_normal(u0.shape)
+    ctx.upload(Z.REG_U, u0)
+    ctx.upload(Z.REG_ADJ, ub)
+    ctx.adj_params(reset=True)
+    ctx.adj_step(dt)
+    pb = ctx.adj_params()
+    ctx.close()
+    for k, name in enumerate(("shift_eta", "damp_kappa1")):
+        vals = []
+        for sgn in (1, -1):
+            p = dict(PUNC)
+            p[name] = PUNC[name] + sgn * 1e-4
+            Z2, mesh2, c2 = make((2, 2, 1), 12, p)
+            c2.upload(Z2.REG_U, u0)
+            c2.evolve(dt, 1)
+            vals.append(dot(ub, c2.download(Z2.REG_U)))
+            c2.close()
+        fd = (vals[0] - vals[1]) / 2e-4
+        print(f"{name}: adjoint {pb[k]:.12e}, differences {fd:.12e}")
+        assert abs(fd - pb[k]) <= 1e-6 * abs(fd)
+
+
+def test_objective_and_its_derivatives():
+    Z, mesh, ctx = make((2, 2, 1), 12, PUNC)
+    u0 = rich_state(Z, mesh, ctx)
+    # J equals the history output's H-norm (volume-weighted sum of H^2)
+    ctx.constraints()
+    J, _ = ctx.objective(Z.REG_U)
+    hst = ctx.hst_norms()[0]
+    assert abs(J - hst) <= 1e-12 * hst, (J, hst)
+    rng = np.random.default_rng(3)
+    v = rng.standard_normal(u0.shape) * 1e-3
+    ctx.upload(Z.REG_TAN, v)
+    J0, Jd = ctx.objective(Z.REG_U, Z.REG_TAN)
+    h = 1e-4
+    Jp = Jm = None
+    ctx.upload(Z.REG_W, u0 + h * v)
+    Jp, _ = ctx.objective(Z.REG_W)
+    ctx.upload(Z.REG_W, u0 - h * v)
+    Jm, _ = ctx.objective(Z.REG_W)
+    fd = (Jp - Jm) / (2 * h)
+    print(f"J {J0:.6e}: tangent {Jd:.12e}, differences {fd:.12e}")
+    assert abs(fd - Jd) <= 1e-7 * abs(Jd)
+    ctx.upload(Z.REG_ADJ, np.zeros_like(u0))
+    ctx.objective_adj(Z.REG_U, 1.0)
+    g = ctx.download(Z.REG_ADJ)
+    assert abs(dot(g, v) - Jd) <= 1e-12 * np.abs(g * v).sum()
+    ctx.close()
+
+
+def test_revolve_schedules_give_the_same_gradient():
+    Z, mesh, ctx = make((2, 1, 1), 12, PUNC)
+    u0 = rich_state(Z, mesh, ctx)
+    dt = 0.25 * float(ctx.dx().min())
+    nsteps = 7
+    ref = None
+    for nsnap, w_step in ((6, 0.0), (2, 0.0), (0, 0.0), (2, 0.5)):
+        ctx.upload(Z.REG_U, u0)
+        J, pb, st = ctx.gradient(dt, nsteps, nsnap, 1.0, w_step)
+        g = ctx.download(Z.REG_ADJ)
+        assert np.array_equal(ctx.download(Z.REG_U), u0)
+        assert st["adjoint_steps"] == nsteps
+        # forward sweep + schedule + (per-step source recomputation)
+        extra = nsteps if w_step else 0
+        assert st["forward_steps"] == nsteps + st["schedule_cost"] + extra, st
+        if w_step == 0.0:
+            if ref is None:
+                ref = (J, g, pb)
+            assert J == ref[0] and np.array_equal(g, ref[1]) and np.array_equal(pb, ref[2])
+        else:
+            # the time-integrated part through the step-by-step adjoint
+            ctx.upload(Z.REG_U, u0)
+            states = [u0]
+            for _ in range(nsteps):
+                ctx.evolve(dt, 1)
+                states.append(ctx.download(Z.REG_U))
+            ctx.upload(Z.REG_ADJ, np.zeros_like(u0))
+            ctx.upload(Z.REG_U, states[-1])
+            ctx.objective_adj(Z.REG_U, 1.0 + w_step)
+            for k in range(nsteps - 1, -1, -1):
+                ctx.upload(Z.REG_U, states[k])
+                ctx.adj_step(dt)
+                if k > 0:
+                    ctx.objective_adj(Z.REG_U, w_step)
+            g2 = ctx.download(Z.REG_ADJ)
+            assert np.abs(g2 - g).max() <= 1e-12 * np.abs(g).max()
+    ctx.close()
+
+
+def configs3_state(Z, mesh, ctx, seed=2024):
+    from z4c_b200 import initial_data as ID
+    ID.load_adm(ctx, ID.gauge_wave1(mesh, amplitude=0.05))
+    u = ctx.download(Z.REG_U)
+    rng = np.random.default_rng(seed)
+    u[:, Z.GXX:Z.GZZ + 1] += rng.uniform(-1e-6, 1e-6, size=u[:, Z.GXX:Z.GZZ + 1].shape)
+    ctx.upload(Z.REG_U, u)
+    ctx.init_finalize()
+    return ctx.download(Z.REG_U)
+
+
+def test_configs3_gradient_against_differences_and_tangent_linear_runs():
+    Z, mesh, ctx = make((1, 1, 1), 64, GW)
+    u0 = configs3_state(Z, mesh, ctx)
+    dt = 0.25 / 64
+    nsteps = 100
+    ctx.upload(Z.REG_U, u0)
+    J, pb, st = ctx.gradient(dt, nsteps, 9)
+    g = ctx.download(Z.REG_ADJ)
+    print(f"J = {J:.10e}, gradient in {st['seconds']:.2f} s, {st}")
+    assert np.array_equal(ctx.download(Z.REG_U), u0)
+    rng = np.random.default_rng(32)
+    worst_fd = worst_tlm = 0.0
+    h = 1e-5
+    for d in range(32):
+        v = rng.standard_normal(u0.shape) * 1e-6
+        Js = []
+        for sgn in (1, -1):
+            ctx.upload(Z.REG_U, u0 + sgn * h * v)
+            ctx.evolve(dt, nsteps)
+            Js.append(ctx.objective(Z.REG_U)[0])
+        fd = (Js[0] - Js[1]) / (2 * h)
+        ad = dot(g, v)
+        worst_fd = max(worst_fd, abs(fd - ad) / abs(ad))
+        if d < 4:  # tangent-linear runs along the first directions
+            ctx.upload(Z.REG_U, u0)
+            ctx.upload(Z.REG_TAN, v)
+            for _ in range(nsteps):
+                ctx.tlm_step(dt)
+            _, Jd = ctx.objective(Z.REG_U, Z.REG_TAN)
+            worst_tlm = max(worst_tlm, abs(Jd - ad) / abs(ad))
+    print(f"configs[3]: worst relative difference to central differences {worst_fd:.2e}, "
+          f"to tangent-linear runs {worst_tlm:.2e}")
+    assert worst_fd <= 1e-6
+    assert worst_tlm <= 1e-9
+    ctx.close()
