@@ -45,8 +45,13 @@
 
 #ifdef __CUDACC__
 #define Z4C_HD __host__ __device__ __forceinline__
+#define Z4C_UNROLL _Pragma("unroll")
+// loops of the forward templates
+#define Z4C_UNROLL_T _Pragma("unroll")
 #else
 #define Z4C_HD inline
+#define Z4C_UNROLL
+#define Z4C_UNROLL_T
 #endif
 
 namespace z4c {
@@ -165,10 +170,14 @@ Z4C_HD void det3s_grad(const double* g, double* dd) {
 // dH = -H dG H and dG = E_ab + E_ba for an off-diagonal stored component.
 Z4C_HD void inv3s_adj(const double* H, const double* Hb, double* gb) {
 #define HH(i, j) H[sid(i, j)]
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       double acc = 0.;
+      Z4C_UNROLL
       for (int i = 0; i < 3; ++i)
+        Z4C_UNROLL
         for (int j = i; j < 3; ++j) {
           const double t = (a == b) ? HH(i, a) * HH(a, j) : HH(i, a) * HH(b, j) + HH(i, b) * HH(a, j);
           acc -= Hb[sid(i, j)] * t;
@@ -188,20 +197,30 @@ Z4C_HD void christoffel_local(const RhsLocal<T>& v, T guu[6], T Gd[3][6], T Gudd
     const T detg = det3s(g);
     inv3s(T(1.0) / detg, g, guu);
   }
+  Z4C_UNROLL_T
   for (int c = 0; c < 3; ++c)
+    Z4C_UNROLL_T
     for (int a = 0; a < 3; ++a)
+      Z4C_UNROLL_T
       for (int b = a; b < 3; ++b)
         Gd[c][sid(a, b)] = 0.5 * (v.dg[a][sid(b, c)] + v.dg[b][sid(a, c)] - v.dg[c][sid(a, b)]);
+  Z4C_UNROLL_T
   for (int c = 0; c < 3; ++c)
+    Z4C_UNROLL_T
     for (int a = 0; a < 3; ++a)
+      Z4C_UNROLL_T
       for (int b = a; b < 3; ++b) {
         T s = T(0.);
+        Z4C_UNROLL_T
         for (int d = 0; d < 3; ++d) s += guu[sid(c, d)] * Gd[d][sid(a, b)];
         Gudd[c][sid(a, b)] = s;
       }
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a) {
     T s = T(0.);
+    Z4C_UNROLL_T
     for (int b = 0; b < 3; ++b)
+      Z4C_UNROLL_T
       for (int c = b; c < 3; ++c) s += wsym(b, c) * guu[sid(b, c)] * Gudd[a][sid(b, c)];
     Gu[a] = s;
   }
@@ -214,26 +233,37 @@ Z4C_HD void ricci_local(const z4c_params_t& opt, const RhsLocal<T>& v, T Rsum[6]
   christoffel_local(v, guu, Gd, Gudd, Gu);
   const T* g = v.u + Z4C_GXX;
   T Rdd[6];
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL_T
     for (int b = a; b < 3; ++b) {
       T s = T(0.);
+      Z4C_UNROLL_T
       for (int c = 0; c < 3; ++c)
         s += 0.5 * (g[sid(c, a)] * v.dGam[b][c] + g[sid(c, b)] * v.dGam[a][c] +
                     Gu[c] * (Gd[a][sid(b, c)] + Gd[b][sid(a, c)]));
       Rdd[sid(a, b)] = s;
     }
+  Z4C_UNROLL_T
   for (int q = 0; q < 6; ++q) {
     T s = Rdd[q];
+    Z4C_UNROLL_T
     for (int c = 0; c < 3; ++c)
+      Z4C_UNROLL_T
       for (int d = c; d < 3; ++d)
         s -= ((c == d) ? 0.5 : 1.0) * guu[sid(c, d)] * v.ddg[q][sid(c, d)];
     Rdd[q] = s;
   }
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL_T
     for (int b = a; b < 3; ++b) {
       T s = Rdd[sid(a, b)];
+      Z4C_UNROLL_T
       for (int c = 0; c < 3; ++c)
+        Z4C_UNROLL_T
         for (int d = 0; d < 3; ++d)
+          Z4C_UNROLL_T
           for (int e = 0; e < 3; ++e)
             s += guu[sid(c, d)] * (Gudd[e][sid(c, a)] * Gd[b][sid(e, d)] +
                                    Gudd[e][sid(c, b)] * Gd[a][sid(e, d)] +
@@ -244,19 +274,27 @@ Z4C_HD void ricci_local(const z4c_params_t& opt, const RhsLocal<T>& v, T Rsum[6]
   const T oochi = T(1.0) / chi_g;
   const double ooc = 1.0 / opt.chi_psi_power;
   T dphi[3];
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a) dphi[a] = v.dchi[a] * oochi * ooc;
   T Ddphi[6];
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL_T
     for (int b = a; b < 3; ++b) {
       T x = v.ddchi[sid(a, b)] * oochi * ooc - opt.chi_psi_power * dphi[a] * dphi[b];
+      Z4C_UNROLL_T
       for (int c = 0; c < 3; ++c) x -= Gudd[c][sid(a, b)] * dphi[c];
       Ddphi[sid(a, b)] = x;
     }
   T Stmp = T(0.);
+  Z4C_UNROLL_T
   for (int c = 0; c < 3; ++c)
+    Z4C_UNROLL_T
     for (int d = c; d < 3; ++d)
       Stmp += wsym(c, d) * guu[sid(c, d)] * (Ddphi[sid(c, d)] + 2. * dphi[c] * dphi[d]);
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL_T
     for (int b = a; b < 3; ++b) {
       const T rphi = 4. * dphi[a] * dphi[b] - 2. * Ddphi[sid(a, b)] - 2. * g[sid(a, b)] * Stmp;
       Rsum[sid(a, b)] = Rdd[sid(a, b)] + rphi;
@@ -282,90 +320,124 @@ Z4C_HD void main_local(const z4c_params_t& opt, const RhsLocal<T>& v, const T Rs
   else oopsi4 = ad_pow(chi_g, -4. / pw);
   const double ooc = 1.0 / pw;
   T dphi[3];
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a) dphi[a] = v.dchi[a] * oochi * ooc;
   // D D alpha (:482-521)
   T Dda_s = T(0.);
+  Z4C_UNROLL_T
   for (int c = 0; c < 3; ++c)
+    Z4C_UNROLL_T
     for (int d = 0; d < 3; ++d) Dda_s += guu[sid(c, d)] * dphi[c] * v.dalpha[d];
   T Dda_dd[6];
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL_T
     for (int b = a; b < 3; ++b) {
       T x = v.ddalpha[sid(a, b)] - 2. * (dphi[a] * v.dalpha[b] + dphi[b] * v.dalpha[a]) +
             2. * g[sid(a, b)] * Dda_s;
+      Z4C_UNROLL_T
       for (int c = 0; c < 3; ++c) x -= Gudd[c][sid(a, b)] * v.dalpha[c];
       Dda_dd[sid(a, b)] = x;
     }
   T Ddalpha = T(0.);
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL_T
     for (int b = a; b < 3; ++b) Ddalpha += wsym(a, b) * oopsi4 * guu[sid(a, b)] * Dda_dd[sid(a, b)];
   // A contractions (:525-589)
   T A_ud[3][3];
+  Z4C_UNROLL_T
   for (int c = 0; c < 3; ++c)
+    Z4C_UNROLL_T
     for (int b = 0; b < 3; ++b) {
       T s = T(0.);
+      Z4C_UNROLL_T
       for (int d = 0; d < 3; ++d) s += guu[sid(c, d)] * A[sid(d, b)];
       A_ud[c][b] = s;
     }
   T AA[6];
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL_T
     for (int b = a; b < 3; ++b) {
       T s = T(0.);
+      Z4C_UNROLL_T
       for (int c = 0; c < 3; ++c) s += A[sid(a, c)] * A_ud[c][b];
       AA[sid(a, b)] = s;
     }
   T trAA = T(0.);
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL_T
     for (int b = a; b < 3; ++b) trAA += wsym(a, b) * guu[sid(a, b)] * AA[sid(a, b)];
   T A_uu[6];
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL_T
     for (int b = a; b < 3; ++b) {
       T s = T(0.);
+      Z4C_UNROLL_T
       for (int c = 0; c < 3; ++c) s += guu[sid(b, c)] * A_ud[a][c];
       A_uu[sid(a, b)] = s;
     }
   const double cpow = -6.0 / pw;
   T DA_u[3];
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a) {
     T s = T(0.);
+    Z4C_UNROLL_T
     for (int b = 0; b < 3; ++b) {
       s -= cpow * A_uu[sid(a, b)] * v.dchi[b] * oochi;
       s -= (1. / 3.) * guu[sid(a, b)] * (2. * v.dKhat[b] + v.dTheta[b]);
     }
+    Z4C_UNROLL_T
     for (int b = 0; b < 3; ++b)
+      Z4C_UNROLL_T
       for (int c = b; c < 3; ++c) s += wsym(b, c) * Gudd[a][sid(b, c)] * A_uu[sid(b, c)];
     DA_u[a] = s;
   }
   // Ricci scalar and Ht (:596-613)
   T R = T(0.);
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL_T
     for (int b = a; b < 3; ++b) R += wsym(a, b) * oopsi4 * guu[sid(a, b)] * Rsum[sid(a, b)];
   const T Ht = R + (2. / 3.) * (K * K) - trAA;
   // Lie derivatives (:619-687)
   T dbtr = T(0.);
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a) dbtr += v.dbeta[a][a];
   T ddbeta_d[3];
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a) {
     T s = T(0.);
+    Z4C_UNROLL_T
     for (int b = 0; b < 3; ++b) s += (1. / 3.) * v.ddbeta[b][sid(a, b)];
     ddbeta_d[a] = s;
   }
   const T Lchi = v.lv[Z4C_CHI] + (1. / 6.) * pw * chi_g * dbtr;
   T LGam[3];
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a) {
     T x = v.lv[Z4C_GAMX + a];
     x += (2. / 3.) * Gu[a] * dbtr;
+    Z4C_UNROLL_T
     for (int b = 0; b < 3; ++b) {
       x += guu[sid(a, b)] * ddbeta_d[b] - Gu[b] * v.dbeta[b][a];
+      Z4C_UNROLL_T
       for (int c = b; c < 3; ++c) x += wsym(b, c) * guu[sid(b, c)] * v.ddbeta[a][sid(b, c)];
     }
     LGam[a] = x;
   }
   T Lg[6], LA[6];
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL_T
     for (int b = a; b < 3; ++b) {
       T lg = v.lv[Z4C_GXX + sid(a, b)], la = v.lv[Z4C_AXX + sid(a, b)];
       lg -= (2. / 3.) * g[sid(a, b)] * dbtr;
       la -= (2. / 3.) * A[sid(a, b)] * dbtr;
+      Z4C_UNROLL_T
       for (int c = 0; c < 3; ++c) {
         lg += v.dbeta[a][c] * g[sid(b, c)];
         la += v.dbeta[b][c] * A[sid(a, c)];
@@ -381,13 +453,17 @@ Z4C_HD void main_local(const z4c_params_t& opt, const RhsLocal<T>& v, const T Rs
                   k1 * (1 - k2) * alpha * Theta;
   out[Z4C_CHI] = Lchi - (1. / 6.) * pw * chi_g * alpha * K;
   out[Z4C_THETA] = v.lv[Z4C_THETA] + alpha * (0.5 * Ht - (2. + k2) * k1 * Theta);
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a) {
     T x = 2. * alpha * DA_u[a] + LGam[a];
     x -= 2. * alpha * k1 * (v.u[Z4C_GAMX + a] - Gu[a]);
+    Z4C_UNROLL_T
     for (int b = 0; b < 3; ++b) x -= 2. * A_uu[sid(a, b)] * v.dalpha[b];
     out[Z4C_GAMX + a] = x;
   }
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL_T
     for (int b = a; b < 3; ++b) {
       const int q = sid(a, b);
       out[Z4C_GXX + q] = -2. * alpha * A[q] + Lg[q];
@@ -402,11 +478,13 @@ Z4C_HD void main_local(const z4c_params_t& opt, const RhsLocal<T>& v, const T Rs
     out[Z4C_ALPHA] = opt.lapse_advect * v.lv[Z4C_ALPHA] -
                      fl * alpha * (Khat + 2. * opt.lapse_K * Theta);
   }
+  Z4C_UNROLL_T
   for (int a = 0; a < 3; ++a) {
     const T gam = v.u[Z4C_GAMX + a];
     T x = opt.shift_Gamma * gam + opt.shift_advect * v.lv[Z4C_BETAX + a];
     if (fabs(opt.shift_alpha2Gamma) > 0.0) x += opt.shift_alpha2Gamma * (alpha * alpha) * gam;
     if (fabs(opt.shift_H) > 0.0)
+      Z4C_UNROLL_T
       for (int b = 0; b < 3; ++b)
         x += opt.shift_H * alpha * chi_g * (0.5 * alpha * v.dchi[b] - v.dalpha[b]) * guu[sid(a, b)];
     x -= opt.shift_eta * v.u[Z4C_BETAX + a];
@@ -437,23 +515,33 @@ Z4C_HD void christoffel_adj(const RhsLocal<double>& v, const double guu[6],
                             const double Gd[3][6], const double Gudd[3][6], double guub[6],
                             double Gdb[3][6], double Guddb[3][6], const double Gub[3],
                             RhsLocal<double>& vb) {
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = 0; b < 3; ++b)
+      Z4C_UNROLL
       for (int c = b; c < 3; ++c) {
         guub[sid(b, c)] += wsym(b, c) * Gudd[a][sid(b, c)] * Gub[a];
         Guddb[a][sid(b, c)] += wsym(b, c) * guu[sid(b, c)] * Gub[a];
       }
+  Z4C_UNROLL
   for (int c = 0; c < 3; ++c)
+    Z4C_UNROLL
     for (int a = 0; a < 3; ++a)
+      Z4C_UNROLL
       for (int b = a; b < 3; ++b) {
         const double X = Guddb[c][sid(a, b)];
+        Z4C_UNROLL
         for (int d = 0; d < 3; ++d) {
           guub[sid(c, d)] += Gd[d][sid(a, b)] * X;
           Gdb[d][sid(a, b)] += guu[sid(c, d)] * X;
         }
       }
+  Z4C_UNROLL
   for (int c = 0; c < 3; ++c)
+    Z4C_UNROLL
     for (int a = 0; a < 3; ++a)
+      Z4C_UNROLL
       for (int b = a; b < 3; ++b) {
         const double X = 0.5 * Gdb[c][sid(a, b)];
         vb.dg[a][sid(b, c)] += X;
@@ -474,23 +562,31 @@ Z4C_HD void ricci_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
   const double oochi = 1.0 / chi_g;
   const double pw = opt.chi_psi_power, ooc = 1.0 / pw;
   double dphi[3];
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a) dphi[a] = v.dchi[a] * oochi * ooc;
   double Ddphi[6];
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       double x = v.ddchi[sid(a, b)] * oochi * ooc - pw * dphi[a] * dphi[b];
+      Z4C_UNROLL
       for (int c = 0; c < 3; ++c) x -= Gudd[c][sid(a, b)] * dphi[c];
       Ddphi[sid(a, b)] = x;
     }
   double Stmp = 0.;
+  Z4C_UNROLL
   for (int c = 0; c < 3; ++c)
+    Z4C_UNROLL
     for (int d = c; d < 3; ++d)
       Stmp += wsym(c, d) * guu[sid(c, d)] * (Ddphi[sid(c, d)] + 2. * dphi[c] * dphi[d]);
 
   double guub[6] = {0, 0, 0, 0, 0, 0}, Gdb[3][6] = {}, Guddb[3][6] = {}, Gub[3] = {0, 0, 0};
   double Rddb[6], dphib[3] = {0, 0, 0}, Ddphib[6] = {0, 0, 0, 0, 0, 0}, Stmpb = 0., oochib = 0.;
   // Rsum = Rdd + 4 dphi dphi - 2 Ddphi - 2 g Stmp
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       const int q = sid(a, b);
       const double X = Rsb[q];
@@ -501,7 +597,9 @@ Z4C_HD void ricci_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
       vb.u[Z4C_GXX + q] -= 2. * Stmp * X;
       Stmpb -= 2. * g[q] * X;
     }
+  Z4C_UNROLL
   for (int c = 0; c < 3; ++c)
+    Z4C_UNROLL
     for (int d = c; d < 3; ++d) {
       const int q = sid(c, d);
       const double w = wsym(c, d);
@@ -510,7 +608,9 @@ Z4C_HD void ricci_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
       dphib[c] += w * guu[q] * 2. * dphi[d] * Stmpb;
       dphib[d] += w * guu[q] * 2. * dphi[c] * Stmpb;
     }
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       const int q = sid(a, b);
       const double X = Ddphib[q];
@@ -518,11 +618,13 @@ Z4C_HD void ricci_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
       oochib += v.ddchi[q] * ooc * X;
       dphib[a] -= pw * dphi[b] * X;
       dphib[b] -= pw * dphi[a] * X;
+      Z4C_UNROLL
       for (int c = 0; c < 3; ++c) {
         Guddb[c][q] -= dphi[c] * X;
         dphib[c] -= Gudd[c][q] * X;
       }
     }
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a) {
     vb.dchi[a] += oochi * ooc * dphib[a];
     oochib += v.dchi[a] * ooc * dphib[a];
@@ -532,13 +634,18 @@ Z4C_HD void ricci_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
     if (!(chi < opt.chi_div_floor)) vb.u[Z4C_CHI] += chigb;
   }
   // the three groups of R_ab, each linear in Rdd
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       const double X = Rddb[sid(a, b)];
+      Z4C_UNROLL
       for (int c = 0; c < 3; ++c)
+        Z4C_UNROLL
         for (int d = 0; d < 3; ++d) {
           const double gcd = guu[sid(c, d)];
           double t = 0.;
+          Z4C_UNROLL
           for (int e = 0; e < 3; ++e) {
             const double g1 = Gudd[e][sid(c, a)], d1 = Gd[b][sid(e, d)];
             const double g2 = Gudd[e][sid(c, b)], d2 = Gd[a][sid(e, d)];
@@ -554,18 +661,24 @@ Z4C_HD void ricci_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
           guub[sid(c, d)] += t * X;
         }
     }
+  Z4C_UNROLL
   for (int q = 0; q < 6; ++q) {
     const double X = Rddb[q];
+    Z4C_UNROLL
     for (int c = 0; c < 3; ++c)
+      Z4C_UNROLL
       for (int d = c; d < 3; ++d) {
         const double w = (c == d) ? 0.5 : 1.0;
         guub[sid(c, d)] -= w * v.ddg[q][sid(c, d)] * X;
         vb.ddg[q][sid(c, d)] -= w * guu[sid(c, d)] * X;
       }
   }
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       const double X = 0.5 * Rddb[sid(a, b)];
+      Z4C_UNROLL
       for (int c = 0; c < 3; ++c) {
         vb.u[Z4C_GXX + sid(c, a)] += v.dGam[b][c] * X;
         vb.dGam[b][c] += g[sid(c, a)] * X;
@@ -596,66 +709,94 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
   const double oochi = 1.0 / chi_g;
   const double oopsi4 = (pw == -4.) ? chi_g : pow(chi_g, -4. / pw);
   double dphi[3];
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a) dphi[a] = v.dchi[a] * oochi * ooc;
   double Dda_s = 0.;
+  Z4C_UNROLL
   for (int c = 0; c < 3; ++c)
+    Z4C_UNROLL
     for (int d = 0; d < 3; ++d) Dda_s += guu[sid(c, d)] * dphi[c] * v.dalpha[d];
   double Dda_dd[6];
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       double x = v.ddalpha[sid(a, b)] - 2. * (dphi[a] * v.dalpha[b] + dphi[b] * v.dalpha[a]) +
                  2. * g[sid(a, b)] * Dda_s;
+      Z4C_UNROLL
       for (int c = 0; c < 3; ++c) x -= Gudd[c][sid(a, b)] * v.dalpha[c];
       Dda_dd[sid(a, b)] = x;
     }
   double Ddalpha = 0.;
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) Ddalpha += wsym(a, b) * oopsi4 * guu[sid(a, b)] * Dda_dd[sid(a, b)];
   double A_ud[3][3];
+  Z4C_UNROLL
   for (int c = 0; c < 3; ++c)
+    Z4C_UNROLL
     for (int b = 0; b < 3; ++b) {
       double s = 0.;
+      Z4C_UNROLL
       for (int d = 0; d < 3; ++d) s += guu[sid(c, d)] * A[sid(d, b)];
       A_ud[c][b] = s;
     }
   double AA[6];
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       double s = 0.;
+      Z4C_UNROLL
       for (int c = 0; c < 3; ++c) s += A[sid(a, c)] * A_ud[c][b];
       AA[sid(a, b)] = s;
     }
   double trAA = 0.;
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) trAA += wsym(a, b) * guu[sid(a, b)] * AA[sid(a, b)];
   double A_uu[6];
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       double s = 0.;
+      Z4C_UNROLL
       for (int c = 0; c < 3; ++c) s += guu[sid(b, c)] * A_ud[a][c];
       A_uu[sid(a, b)] = s;
     }
   const double cpow = -6.0 / pw;
   double DA_u[3];
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a) {
     double s = 0.;
+    Z4C_UNROLL
     for (int b = 0; b < 3; ++b) {
       s -= cpow * A_uu[sid(a, b)] * v.dchi[b] * oochi;
       s -= (1. / 3.) * guu[sid(a, b)] * (2. * v.dKhat[b] + v.dTheta[b]);
     }
+    Z4C_UNROLL
     for (int b = 0; b < 3; ++b)
+      Z4C_UNROLL
       for (int c = b; c < 3; ++c) s += wsym(b, c) * Gudd[a][sid(b, c)] * A_uu[sid(b, c)];
     DA_u[a] = s;
   }
   double R = 0.;
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) R += wsym(a, b) * oopsi4 * guu[sid(a, b)] * Rsum[sid(a, b)];
   const double Ht = R + (2. / 3.) * (K * K) - trAA;
   double dbtr = 0.;
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a) dbtr += v.dbeta[a][a];
   double ddbeta_d[3];
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a) {
     double s = 0.;
+    Z4C_UNROLL
     for (int b = 0; b < 3; ++b) s += (1. / 3.) * v.ddbeta[b][sid(a, b)];
     ddbeta_d[a] = s;
   }
@@ -670,6 +811,7 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
   const double k1 = opt.damp_kappa1, k2 = opt.damp_kappa2;
 
   // assemble (:694-902), each output in turn
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a) {
     const double X = ob[Z4C_BETAX + a];
     const double gam = v.u[Z4C_GAMX + a];
@@ -680,6 +822,7 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
       alphab += opt.shift_alpha2Gamma * 2. * alpha * gam * X;
     }
     if (fabs(opt.shift_H) > 0.0)
+      Z4C_UNROLL
       for (int b = 0; b < 3; ++b) {
         const double gab = guu[sid(a, b)];
         const double in = 0.5 * alpha * v.dchi[b] - v.dalpha[b];
@@ -702,6 +845,7 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
     vb.u[Z4C_KHAT] -= fl * alpha * X;
     vb.u[Z4C_THETA] -= fl * alpha * 2. * opt.lapse_K * X;
   }
+  Z4C_UNROLL
   for (int q = 0; q < 6; ++q) {
     const double X = ob[Z4C_AXX + q];
     oopsi4b += (-Dda_dd[q] + alpha * Rsum[q]) * X;
@@ -722,6 +866,7 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
     vb.u[Z4C_AXX + q] -= 2. * alpha * Y;
     Lgb[q] += Y;
   }
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a) {
     const double X = ob[Z4C_GAMX + a];
     const double gam = v.u[Z4C_GAMX + a];
@@ -732,6 +877,7 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
     vb.u[Z4C_GAMX + a] -= 2. * alpha * k1 * X;
     Gub[a] += 2. * alpha * k1 * X;
     pb.damp_kappa1 -= 2. * alpha * (gam - Gu[a]) * X;
+    Z4C_UNROLL
     for (int b = 0; b < 3; ++b) {
       A_uub[sid(a, b)] -= 2. * v.dalpha[b] * X;
       vb.dalpha[b] -= 2. * A_uu[sid(a, b)] * X;
@@ -763,7 +909,9 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
     pb.damp_kappa1 += (1 - k2) * alpha * Theta * X;
   }
   // Lie derivatives (:619-687)
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       const int q = sid(a, b);
       const double XG = Lgb[q], XA = LAb[q];
@@ -773,6 +921,7 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
       dbtrb -= (2. / 3.) * g[q] * XG;
       vb.u[Z4C_AXX + q] -= (2. / 3.) * dbtr * XA;
       dbtrb -= (2. / 3.) * A[q] * XA;
+      Z4C_UNROLL
       for (int c = 0; c < 3; ++c) {
         vb.dbeta[a][c] += g[sid(b, c)] * XG;
         vb.u[Z4C_GXX + sid(b, c)] += v.dbeta[a][c] * XG;
@@ -784,16 +933,19 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
         vb.u[Z4C_AXX + sid(b, c)] += v.dbeta[a][c] * XA;
       }
     }
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a) {
     const double X = LGamb[a];
     vb.lv[Z4C_GAMX + a] += X;
     Gub[a] += (2. / 3.) * dbtr * X;
     dbtrb += (2. / 3.) * Gu[a] * X;
+    Z4C_UNROLL
     for (int b = 0; b < 3; ++b) {
       guub[sid(a, b)] += ddbeta_d[b] * X;
       ddbeta_db[b] += guu[sid(a, b)] * X;
       Gub[b] -= v.dbeta[b][a] * X;
       vb.dbeta[b][a] -= Gu[b] * X;
+      Z4C_UNROLL
       for (int c = b; c < 3; ++c) {
         guub[sid(b, c)] += wsym(b, c) * v.ddbeta[a][sid(b, c)] * X;
         vb.ddbeta[a][sid(b, c)] += wsym(b, c) * guu[sid(b, c)] * X;
@@ -803,14 +955,19 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
   vb.lv[Z4C_CHI] += Lchib;
   chigb += (1. / 6.) * pw * dbtr * Lchib;
   dbtrb += (1. / 6.) * pw * chi_g * Lchib;
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = 0; b < 3; ++b) vb.ddbeta[b][sid(a, b)] += (1. / 3.) * ddbeta_db[a];
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a) vb.dbeta[a][a] += dbtrb;
   // Ricci scalar and Ht
   Rb += Htb;
   Kb += (4. / 3.) * K * Htb;
   trAAb -= Htb;
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       const int q = sid(a, b);
       const double w = wsym(a, b);
@@ -819,8 +976,10 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
       Rsb[q] += w * oopsi4 * guu[q] * Rb;
     }
   // D_i A^ij
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a) {
     const double X = DAb[a];
+    Z4C_UNROLL
     for (int b = 0; b < 3; ++b) {
       A_uub[sid(a, b)] -= cpow * v.dchi[b] * oochi * X;
       vb.dchi[b] -= cpow * A_uu[sid(a, b)] * oochi * X;
@@ -829,45 +988,60 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
       vb.dKhat[b] -= (2. / 3.) * guu[sid(a, b)] * X;
       vb.dTheta[b] -= (1. / 3.) * guu[sid(a, b)] * X;
     }
+    Z4C_UNROLL
     for (int b = 0; b < 3; ++b)
+      Z4C_UNROLL
       for (int c = b; c < 3; ++c) {
         Guddb[a][sid(b, c)] += wsym(b, c) * A_uu[sid(b, c)] * X;
         A_uub[sid(b, c)] += wsym(b, c) * Gudd[a][sid(b, c)] * X;
       }
   }
   // A contractions
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       const double X = A_uub[sid(a, b)];
+      Z4C_UNROLL
       for (int c = 0; c < 3; ++c) {
         guub[sid(b, c)] += A_ud[a][c] * X;
         A_udb[a][c] += guu[sid(b, c)] * X;
       }
     }
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       const int q = sid(a, b);
       guub[q] += wsym(a, b) * AA[q] * trAAb;
       AAb[q] += wsym(a, b) * guu[q] * trAAb;
     }
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       const double X = AAb[sid(a, b)];
+      Z4C_UNROLL
       for (int c = 0; c < 3; ++c) {
         vb.u[Z4C_AXX + sid(a, c)] += A_ud[c][b] * X;
         A_udb[c][b] += A[sid(a, c)] * X;
       }
     }
+  Z4C_UNROLL
   for (int c = 0; c < 3; ++c)
+    Z4C_UNROLL
     for (int b = 0; b < 3; ++b) {
       const double X = A_udb[c][b];
+      Z4C_UNROLL
       for (int d = 0; d < 3; ++d) {
         guub[sid(c, d)] += A[sid(d, b)] * X;
         vb.u[Z4C_AXX + sid(d, b)] += guu[sid(c, d)] * X;
       }
     }
   // D D alpha
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       const int q = sid(a, b);
       const double w = wsym(a, b);
@@ -875,7 +1049,9 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
       guub[q] += w * oopsi4 * Dda_dd[q] * Ddalphab;
       Dda_ddb[q] += w * oopsi4 * guu[q] * Ddalphab;
     }
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a)
+    Z4C_UNROLL
     for (int b = a; b < 3; ++b) {
       const int q = sid(a, b);
       const double X = Dda_ddb[q];
@@ -886,18 +1062,22 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
       vb.dalpha[a] -= 2. * dphi[b] * X;
       vb.u[Z4C_GXX + q] += 2. * Dda_s * X;
       Dda_sb += 2. * g[q] * X;
+      Z4C_UNROLL
       for (int c = 0; c < 3; ++c) {
         Guddb[c][q] -= v.dalpha[c] * X;
         vb.dalpha[c] -= Gudd[c][q] * X;
       }
     }
+  Z4C_UNROLL
   for (int c = 0; c < 3; ++c)
+    Z4C_UNROLL
     for (int d = 0; d < 3; ++d) {
       const double gcd = guu[sid(c, d)];
       guub[sid(c, d)] += dphi[c] * v.dalpha[d] * Dda_sb;
       dphib[c] += gcd * v.dalpha[d] * Dda_sb;
       vb.dalpha[d] += gcd * dphi[c] * Dda_sb;
     }
+  Z4C_UNROLL
   for (int a = 0; a < 3; ++a) {
     vb.dchi[a] += oochi * ooc * dphib[a];
     oochib += v.dchi[a] * ooc * dphib[a];
@@ -952,8 +1132,10 @@ Z4C_HD void alg_constr_local(const z4c_params_t& opt, T* u) {
   if (apply) {
     const T oopsi4 = ((val(detg) - 1.0) < opt.eps_floor) ? T(1.0 + opt.eps_floor / -3.0)
                                                          : ad_pow(detg, 1.0 / -3.0);
+    Z4C_UNROLL_T
     for (int c = 0; c < 6; ++c) g[c] = g[c] * oopsi4;
     const T tr = trace_adj(g, A);
+    Z4C_UNROLL_T
     for (int c = 0; c < 6; ++c) A[c] = A[c] - (1.0 / 3.0) * tr * g[c];
   }
   if (opt.force_regularization) {
@@ -988,24 +1170,28 @@ Z4C_HD void alg_constr_adj(const z4c_params_t& opt, const double* u, double* ub)
   const bool pow_branch = !((detg - 1.0) < opt.eps_floor);
   const double oopsi4 = pow_branch ? pow(detg, 1.0 / -3.0) : 1.0 + opt.eps_floor / -3.0;
   double g[6];
+  Z4C_UNROLL
   for (int c = 0; c < 6; ++c) g[c] = g0[c] * oopsi4;
   const double tr = trace_adj(g, A0);
   double* gb = ub + Z4C_GXX;
   double* Ab = ub + Z4C_AXX;
   // A' = A - tr g' / 3
   double trb = 0., gpb[6];
+  Z4C_UNROLL
   for (int c = 0; c < 6; ++c) {
     trb -= (1.0 / 3.0) * g[c] * Ab[c];
     gpb[c] = gb[c] - (1.0 / 3.0) * tr * Ab[c];
   }
   double dPg[6], dPA[6];
   trace_adj_grad(g, A0, dPg, dPA);
+  Z4C_UNROLL
   for (int c = 0; c < 6; ++c) {
     gpb[c] += trb * dPg[c];
     Ab[c] += trb * dPA[c];
   }
   // g' = g oopsi4
   double oopsi4b = 0.;
+  Z4C_UNROLL
   for (int c = 0; c < 6; ++c) {
     oopsi4b += g0[c] * gpb[c];
     gb[c] = oopsi4 * gpb[c];
@@ -1014,6 +1200,7 @@ Z4C_HD void alg_constr_adj(const z4c_params_t& opt, const double* u, double* ub)
     const double detb = oopsi4b * (-1.0 / 3.0) * pow(detg, -1.0 / 3.0 - 1.0);
     double dd[6];
     det3s_grad(g0, dd);
+    Z4C_UNROLL
     for (int c = 0; c < 6; ++c) gb[c] += detb * dd[c];
   }
   (void)detraw;
@@ -1040,34 +1227,34 @@ template <class T>
 Z4C_HD T ham_local(const z4c_params_t& opt, const HLocal<T>& v) {
   const T psi4 = T(1.0) / v.chi;
   T gph[6], Kd[6];
-  for (int c = 0; c < 6; ++c) gph[c] = psi4 * v.gt[c];
-  for (int c = 0; c < 6; ++c) Kd[c] = psi4 * v.At[c] + (1. / 3.) * (v.Khat + 2. * v.Theta) * gph[c];
+    for (int c = 0; c < 6; ++c) gph[c] = psi4 * v.gt[c];
+    for (int c = 0; c < 6; ++c) Kd[c] = psi4 * v.At[c] + (1. / 3.) * (v.Khat + 2. * v.Theta) * gph[c];
   const T chi_g = ad_max_c(v.chi, opt.chi_div_floor);
   const T oochi = T(1.0) / chi_g;
   T dg[3][6];
-  for (int c = 0; c < 3; ++c)
-    for (int q = 0; q < 6; ++q) dg[c][q] = oochi * (v.dg3[c][q] - oochi * v.gt[q] * v.dchi[c]);
+    for (int c = 0; c < 3; ++c)
+        for (int q = 0; q < 6; ++q) dg[c][q] = oochi * (v.dg3[c][q] - oochi * v.gt[q] * v.dchi[c]);
   T guu[6];
   {
     const T detg = det3s(gph);
     inv3s(T(1.) / detg, gph, guu);
   }
   T Gddd[3][6], Gudd[3][6];
-  for (int c = 0; c < 3; ++c)
-    for (int a = 0; a < 3; ++a)
-      for (int b = a; b < 3; ++b)
+    for (int c = 0; c < 3; ++c)
+        for (int a = 0; a < 3; ++a)
+            for (int b = a; b < 3; ++b)
         Gddd[c][sid(a, b)] = 0.5 * (dg[a][sid(b, c)] + dg[b][sid(a, c)] - dg[c][sid(a, b)]);
-  for (int c = 0; c < 3; ++c)
-    for (int a = 0; a < 3; ++a)
-      for (int b = a; b < 3; ++b) {
+    for (int c = 0; c < 3; ++c)
+        for (int a = 0; a < 3; ++a)
+            for (int b = a; b < 3; ++b) {
         T acc = T(0.);
-        for (int d = 0; d < 3; ++d) acc += guu[sid(c, d)] * Gddd[d][sid(a, b)];
+                for (int d = 0; d < 3; ++d) acc += guu[sid(c, d)] * Gddd[d][sid(a, b)];
         Gudd[c][sid(a, b)] = acc;
       }
   T DDG[6][6];  // [pair(a,b) of the derivatives][pair(c,d) of the metric]
-  for (int a = 0; a < 3; ++a)
-    for (int b = a; b < 3; ++b)
-      for (int q = 0; q < 6; ++q) {
+    for (int a = 0; a < 3; ++a)
+        for (int b = a; b < 3; ++b)
+            for (int q = 0; q < 6; ++q) {
         const T gtil = v.gt[q];
         const T ddchi = v.ddchi[sid(a, b)];
         const T ddgc = v.ddg[q][sid(a, b)];
@@ -1080,32 +1267,32 @@ Z4C_HD T ham_local(const z4c_params_t& opt, const HLocal<T>& v) {
                        2.0 * oochi * oochi * v.dchi[a] * v.dchi[b] * gtil);
       }
   T R = T(0.);
-  for (int a = 0; a < 3; ++a)
-    for (int b = a; b < 3; ++b) {
+    for (int a = 0; a < 3; ++a)
+        for (int b = a; b < 3; ++b) {
       T acc = T(0.);
-      for (int c = 0; c < 3; ++c)
-        for (int d = 0; d < 3; ++d)
-          for (int f = 0; f < 3; ++f)
+            for (int c = 0; c < 3; ++c)
+                for (int d = 0; d < 3; ++d)
+                    for (int f = 0; f < 3; ++f)
             acc += guu[sid(d, f)] * (Gudd[c][sid(a, f)] * Gddd[c][sid(b, d)] -
                                      Gudd[c][sid(a, b)] * Gddd[c][sid(f, d)]);
-      for (int c = 0; c < 3; ++c)
-        for (int d = 0; d < 3; ++d)
+            for (int c = 0; c < 3; ++c)
+                for (int d = 0; d < 3; ++d)
           acc += 0.5 * guu[sid(c, d)] *
                  (-DDG[sid(b, a)][sid(c, d)] + DDG[sid(d, a)][sid(b, c)] +
                   DDG[sid(d, b)][sid(a, c)] - DDG[sid(d, c)][sid(a, b)]);
       R += wsym(a, b) * guu[sid(a, b)] * acc;
     }
   T K = T(0.), K_ud[3][3], KK = T(0.);
-  for (int a = 0; a < 3; ++a) {
-    for (int b = 0; b < 3; ++b) {
+    for (int a = 0; a < 3; ++a) {
+        for (int b = 0; b < 3; ++b) {
       T acc = T(0.);
-      for (int c = 0; c < 3; ++c) acc += guu[sid(a, c)] * Kd[sid(c, b)];
+            for (int c = 0; c < 3; ++c) acc += guu[sid(a, c)] * Kd[sid(c, b)];
       K_ud[a][b] = acc;
     }
     K += K_ud[a][a];
   }
-  for (int a = 0; a < 3; ++a)
-    for (int b = 0; b < 3; ++b) KK += K_ud[a][b] * K_ud[b][a];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) KK += K_ud[a][b] * K_ud[b][a];
   return R + (K * K) - KK;
 }
 
@@ -1114,35 +1301,35 @@ Z4C_HD void ham_local_adj(const z4c_params_t& opt, const HLocal<double>& v, doub
                           HLocal<double>& vb) {
   const double psi4 = 1.0 / v.chi;
   double gph[6], Kd[6];
-  for (int c = 0; c < 6; ++c) gph[c] = psi4 * v.gt[c];
+    for (int c = 0; c < 6; ++c) gph[c] = psi4 * v.gt[c];
   const double Kt = v.Khat + 2. * v.Theta;
-  for (int c = 0; c < 6; ++c) Kd[c] = psi4 * v.At[c] + (1. / 3.) * Kt * gph[c];
+    for (int c = 0; c < 6; ++c) Kd[c] = psi4 * v.At[c] + (1. / 3.) * Kt * gph[c];
   const double chi_g = ad_max_c(v.chi, opt.chi_div_floor);
   const double oochi = 1.0 / chi_g;
   double dg[3][6];
-  for (int c = 0; c < 3; ++c)
-    for (int q = 0; q < 6; ++q) dg[c][q] = oochi * (v.dg3[c][q] - oochi * v.gt[q] * v.dchi[c]);
+    for (int c = 0; c < 3; ++c)
+        for (int q = 0; q < 6; ++q) dg[c][q] = oochi * (v.dg3[c][q] - oochi * v.gt[q] * v.dchi[c]);
   double guu[6];
   {
     const double detg = det3s(gph);
     inv3s(1. / detg, gph, guu);
   }
   double Gddd[3][6], Gudd[3][6];
-  for (int c = 0; c < 3; ++c)
-    for (int a = 0; a < 3; ++a)
-      for (int b = a; b < 3; ++b)
+    for (int c = 0; c < 3; ++c)
+        for (int a = 0; a < 3; ++a)
+            for (int b = a; b < 3; ++b)
         Gddd[c][sid(a, b)] = 0.5 * (dg[a][sid(b, c)] + dg[b][sid(a, c)] - dg[c][sid(a, b)]);
-  for (int c = 0; c < 3; ++c)
-    for (int a = 0; a < 3; ++a)
-      for (int b = a; b < 3; ++b) {
+    for (int c = 0; c < 3; ++c)
+        for (int a = 0; a < 3; ++a)
+            for (int b = a; b < 3; ++b) {
         double acc = 0.;
-        for (int d = 0; d < 3; ++d) acc += guu[sid(c, d)] * Gddd[d][sid(a, b)];
+                for (int d = 0; d < 3; ++d) acc += guu[sid(c, d)] * Gddd[d][sid(a, b)];
         Gudd[c][sid(a, b)] = acc;
       }
   double DDG[6][6];
-  for (int a = 0; a < 3; ++a)
-    for (int b = a; b < 3; ++b)
-      for (int q = 0; q < 6; ++q) {
+    for (int a = 0; a < 3; ++a)
+        for (int b = a; b < 3; ++b)
+            for (int q = 0; q < 6; ++q) {
         const double gtil = v.gt[q], ddchi = v.ddchi[sid(a, b)], ddgc = v.ddg[q][sid(a, b)];
         if (a == b)
           DDG[sid(a, b)][q] = oochi * (ddgc - oochi * (2.0 * v.dchi[a] * v.dg3[a][q] + ddchi * gtil) +
@@ -1153,10 +1340,10 @@ Z4C_HD void ham_local_adj(const z4c_params_t& opt, const HLocal<double>& v, doub
                        2.0 * oochi * oochi * v.dchi[a] * v.dchi[b] * gtil);
       }
   double K_ud[3][3], K = 0.;
-  for (int a = 0; a < 3; ++a) {
-    for (int b = 0; b < 3; ++b) {
+    for (int a = 0; a < 3; ++a) {
+        for (int b = 0; b < 3; ++b) {
       double acc = 0.;
-      for (int c = 0; c < 3; ++c) acc += guu[sid(a, c)] * Kd[sid(c, b)];
+            for (int c = 0; c < 3; ++c) acc += guu[sid(a, c)] * Kd[sid(c, b)];
       K_ud[a][b] = acc;
     }
     K += K_ud[a][a];
@@ -1167,26 +1354,26 @@ Z4C_HD void ham_local_adj(const z4c_params_t& opt, const HLocal<double>& v, doub
   double oochib = 0., psi4b = 0.;
   const double Rb = Hb, Kb = 2. * K * Hb, KKb = -Hb;
   double K_udb[3][3] = {};
-  for (int a = 0; a < 3; ++a) {
+    for (int a = 0; a < 3; ++a) {
     K_udb[a][a] += Kb;
-    for (int b = 0; b < 3; ++b) {
+        for (int b = 0; b < 3; ++b) {
       K_udb[a][b] += K_ud[b][a] * KKb;
       K_udb[b][a] += K_ud[a][b] * KKb;
     }
   }
-  for (int a = 0; a < 3; ++a)
-    for (int b = 0; b < 3; ++b)
-      for (int c = 0; c < 3; ++c) {
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+            for (int c = 0; c < 3; ++c) {
         guub[sid(a, c)] += Kd[sid(c, b)] * K_udb[a][b];
         Kdb[sid(c, b)] += guu[sid(a, c)] * K_udb[a][b];
       }
-  for (int a = 0; a < 3; ++a)
-    for (int b = a; b < 3; ++b) {
+    for (int a = 0; a < 3; ++a)
+        for (int b = a; b < 3; ++b) {
       double acc = 0.;
       const double X = wsym(a, b) * guu[sid(a, b)] * Rb;
-      for (int c = 0; c < 3; ++c)
-        for (int d = 0; d < 3; ++d)
-          for (int f = 0; f < 3; ++f) {
+            for (int c = 0; c < 3; ++c)
+                for (int d = 0; d < 3; ++d)
+                    for (int f = 0; f < 3; ++f) {
             const double gdf = guu[sid(d, f)];
             const double u1 = Gudd[c][sid(a, f)], d1 = Gddd[c][sid(b, d)];
             const double u2 = Gudd[c][sid(a, b)], d2 = Gddd[c][sid(f, d)];
@@ -1197,8 +1384,8 @@ Z4C_HD void ham_local_adj(const z4c_params_t& opt, const HLocal<double>& v, doub
             Guddb[c][sid(a, b)] -= gdf * d2 * X;
             Gdddb[c][sid(f, d)] -= gdf * u2 * X;
           }
-      for (int c = 0; c < 3; ++c)
-        for (int d = 0; d < 3; ++d) {
+            for (int c = 0; c < 3; ++c)
+                for (int d = 0; d < 3; ++d) {
           const double s = -DDG[sid(b, a)][sid(c, d)] + DDG[sid(d, a)][sid(b, c)] +
                            DDG[sid(d, b)][sid(a, c)] - DDG[sid(d, c)][sid(a, b)];
           acc += 0.5 * guu[sid(c, d)] * s;
@@ -1211,9 +1398,9 @@ Z4C_HD void ham_local_adj(const z4c_params_t& opt, const HLocal<double>& v, doub
         }
       guub[sid(a, b)] += wsym(a, b) * acc * Rb;
     }
-  for (int a = 0; a < 3; ++a)
-    for (int b = a; b < 3; ++b)
-      for (int q = 0; q < 6; ++q) {
+    for (int a = 0; a < 3; ++a)
+        for (int b = a; b < 3; ++b)
+            for (int q = 0; q < 6; ++q) {
         const double X = DDGb[sid(a, b)][q];
         const double gtil = v.gt[q], ddchi = v.ddchi[sid(a, b)], ddgc = v.ddg[q][sid(a, b)];
         if (a == b) {
@@ -1252,26 +1439,26 @@ Z4C_HD void ham_local_adj(const z4c_params_t& opt, const HLocal<double>& v, doub
           vb.gt[q] += 2.0 * oochi * oochi * da * db * Y;
         }
       }
-  for (int c = 0; c < 3; ++c)
-    for (int a = 0; a < 3; ++a)
-      for (int b = a; b < 3; ++b) {
+    for (int c = 0; c < 3; ++c)
+        for (int a = 0; a < 3; ++a)
+            for (int b = a; b < 3; ++b) {
         const double X = Guddb[c][sid(a, b)];
-        for (int d = 0; d < 3; ++d) {
+                for (int d = 0; d < 3; ++d) {
           guub[sid(c, d)] += Gddd[d][sid(a, b)] * X;
           Gdddb[d][sid(a, b)] += guu[sid(c, d)] * X;
         }
       }
-  for (int c = 0; c < 3; ++c)
-    for (int a = 0; a < 3; ++a)
-      for (int b = a; b < 3; ++b) {
+    for (int c = 0; c < 3; ++c)
+        for (int a = 0; a < 3; ++a)
+            for (int b = a; b < 3; ++b) {
         const double X = 0.5 * Gdddb[c][sid(a, b)];
         dgb[a][sid(b, c)] += X;
         dgb[b][sid(a, c)] += X;
         dgb[c][sid(a, b)] -= X;
       }
   inv3s_adj(guu, guub, gphb);
-  for (int c = 0; c < 3; ++c)
-    for (int q = 0; q < 6; ++q) {
+    for (int c = 0; c < 3; ++c)
+        for (int q = 0; q < 6; ++q) {
       const double X = dgb[c][q];
       oochib += (v.dg3[c][q] - 2.0 * oochi * v.gt[q] * v.dchi[c]) * X;
       vb.dg3[c][q] += oochi * X;
@@ -1280,7 +1467,7 @@ Z4C_HD void ham_local_adj(const z4c_params_t& opt, const HLocal<double>& v, doub
     }
   const double chigb = -oochi * oochi * oochib;
   if (!(v.chi < opt.chi_div_floor)) vb.chi += chigb;
-  for (int c = 0; c < 6; ++c) {
+    for (int c = 0; c < 6; ++c) {
     const double X = Kdb[c];
     psi4b += v.At[c] * X;
     vb.At[c] += psi4 * X;
@@ -1288,7 +1475,7 @@ Z4C_HD void ham_local_adj(const z4c_params_t& opt, const HLocal<double>& v, doub
     vb.Theta += (2. / 3.) * gph[c] * X;
     gphb[c] += (1. / 3.) * Kt * X;
   }
-  for (int c = 0; c < 6; ++c) {
+    for (int c = 0; c < 6; ++c) {
     psi4b += v.gt[c] * gphb[c];
     vb.gt[c] += psi4 * gphb[c];
   }

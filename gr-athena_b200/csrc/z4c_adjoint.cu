@@ -172,10 +172,15 @@ __device__ __forceinline__ T st_lop(const Fld<T>& f, int64_t p, int64_t s, bool 
   return out;
 }
 
+// Which local inputs a gather fills: every one (the tangent-linear model),
+// those the main algebra's reverse reads (not the advection sums, whose
+// values it does not need), or those of the Ricci part.
+enum { kGatherAll = 0, kGatherMain = 1, kGatherRicci = 2 };
+
 // Local inputs of the right-hand side at interior vertex p of a block: U and
 // SD point at the block's state and stored first derivatives (and Ud, SDd at
-// their tangents for T = Dual).
-template <class T>
+// their tangents for T = Dual).  Inputs a PART does not gather are zero.
+template <class T, int PART = kGatherAll>
 __device__ void gather_rhs(const Grid& g, const FdScale& F, const double* U, const double* SD,
                            const double* Ud, const double* SDd, int64_t p, RhsLocal<T>& v) {
   const int64_t nv = g.nvol;
@@ -185,26 +190,48 @@ __device__ void gather_rhs(const Grid& g, const FdScale& F, const double* U, con
     if constexpr (sizeof(T) == sizeof(Dual)) f.d = based + off;
     return f;
   };
+  #pragma unroll
   for (int n = 0; n < NVAR; ++n) v.u[n] = fld(U, Ud, (int64_t)n * nv).at(p);
   auto sdc = [&](int comp) { return fld(SD, SDd, (int64_t)comp * nv).at(p); };
+  #pragma unroll
   for (int a = 0; a < 3; ++a) {
     v.dchi[a] = sdc(a);
     v.dalpha[a] = sdc(7 * 3 + a);
   }
+  #pragma unroll
   for (int c = 0; c < 3; ++c)
+    #pragma unroll
     for (int q = 0; q < 6; ++q) v.dg[c][q] = sdc((1 + q) * 3 + c);
+  #pragma unroll
   for (int a = 0; a < 3; ++a)
+    #pragma unroll
     for (int b = 0; b < 3; ++b) v.dbeta[b][a] = sdc((8 + a) * 3 + b);
+  #pragma unroll
   for (int b = 0; b < 3; ++b) {
+    #pragma unroll
     for (int c = 0; c < 3; ++c)
       v.dGam[b][c] = st_d1(fld(U, Ud, (int64_t)(Z4C_GAMX + c) * nv), p, g.s[b], F.cidx1[b]);
-    v.dKhat[b] = st_d1(fld(U, Ud, (int64_t)Z4C_KHAT * nv), p, g.s[b], F.cidx1[b]);
-    v.dTheta[b] = st_d1(fld(U, Ud, (int64_t)Z4C_THETA * nv), p, g.s[b], F.cidx1[b]);
+    if (PART != kGatherRicci) {
+      v.dKhat[b] = st_d1(fld(U, Ud, (int64_t)Z4C_KHAT * nv), p, g.s[b], F.cidx1[b]);
+      v.dTheta[b] = st_d1(fld(U, Ud, (int64_t)Z4C_THETA * nv), p, g.s[b], F.cidx1[b]);
+    } else {
+      v.dKhat[b] = v.dTheta[b] = T(0.);
+    }
   }
   // second derivatives: Dxx on the diagonal, Dx_a of the stored Dx_b (a < b)
+  #pragma unroll
   for (int slot = 0; slot < 11; ++slot) {
     const int var = sd_field_var(slot);
+    if (PART == kGatherRicci && slot >= 7) {  // alpha, beta: not in the Ricci part
+      for (int q = 0; q < 6; ++q) {
+        if (slot == 7) v.ddalpha[q] = T(0.);
+        else v.ddbeta[slot - 8][q] = T(0.);
+      }
+      continue;
+    }
+    #pragma unroll
     for (int a = 0; a < 3; ++a)
+      #pragma unroll
       for (int b = a; b < 3; ++b) {
         T d;
         if (a == b) d = st_d2(fld(U, Ud, (int64_t)var * nv), p, g.s[a], F.cidx2[a]);
@@ -215,11 +242,18 @@ __device__ void gather_rhs(const Grid& g, const FdScale& F, const double* U, con
         else v.ddbeta[slot - 8][ad::sid(a, b)] = d;
       }
   }
+  if (PART != kGatherAll) {
+    for (int n = 0; n < NVAR; ++n) v.lv[n] = T(0.);
+    return;
+  }
   // advection sums beta^a L_a f, the side chosen by the sign of beta^a
   T beta[3];
+  #pragma unroll
   for (int a = 0; a < 3; ++a) beta[a] = v.u[Z4C_BETAX + a];
+  #pragma unroll
   for (int n = 0; n < NVAR; ++n) {
     T acc = T(0.);
+    #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const bool left = ad::val(beta[a]) < 0;
       acc += (beta[a] * st_lop(fld(U, Ud, (int64_t)n * nv), p, g.s[a], left)) * F.lidx[a];
@@ -259,17 +293,20 @@ k_adj_main(Grid g, DevParams P, const double* __restrict__ u, const double* __re
     const double* SD = sd + (int64_t)b * kSdComponents * nv;
     const FdScale& F = P.fd[b];
     RhsLocal<double> v;
-    gather_rhs<double>(g, F, U, SD, nullptr, nullptr, p, v);
+    gather_rhs<double, kGatherMain>(g, F, U, SD, nullptr, nullptr, p, v);
     double Rs[6];
     const double* RS = rsum + (int64_t)b * 6 * npts + l;
+    #pragma unroll
     for (int q = 0; q < 6; ++q) Rs[q] = RS[(int64_t)q * npts];
     double ob[NVAR], wb[NVAR];
     const double* WB = wbar + (int64_t)b * NVAR * nv + p;
+    #pragma unroll
     for (int n = 0; n < NVAR; ++n) {
       wb[n] = WB[(int64_t)n * nv];
       ob[n] = W.beta_dt * wb[n];
     }
     RhsLocal<double> vb;
+    #pragma unroll
     for (int q = 0; q < RhsLocal<double>::N; ++q) vb.data()[q] = 0.;
     double Rsb[6] = {0, 0, 0, 0, 0, 0};
     ad::ParamBar pb{0., 0.};
@@ -277,9 +314,11 @@ k_adj_main(Grid g, DevParams P, const double* __restrict__ u, const double* __re
     pe = pb.shift_eta;
     pk = pb.damp_kappa1;
     // the advection sums' dependence on the shift at the vertex
+    #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const bool left = v.u[Z4C_BETAX + a] < 0;
       double acc = 0.;
+      #pragma unroll
       for (int n = 0; n < NVAR; ++n) {
         if (vb.lv[n] == 0.) continue;
         Fld<double> f{U + (int64_t)n * nv};
@@ -289,33 +328,47 @@ k_adj_main(Grid g, DevParams P, const double* __restrict__ u, const double* __re
     }
     // channels
     double* C = chan + (int64_t)b * kNChan * npts + l;
+    #pragma unroll
     for (int a = 0; a < 3; ++a) {
       C[(int64_t)(kChSd + a) * npts] = vb.dchi[a];
       C[(int64_t)(kChSd + 7 * 3 + a) * npts] = vb.dalpha[a];
     }
+    #pragma unroll
     for (int c = 0; c < 3; ++c)
+      #pragma unroll
       for (int q = 0; q < 6; ++q) C[(int64_t)(kChSd + (1 + q) * 3 + c) * npts] = vb.dg[c][q];
+    #pragma unroll
     for (int a = 0; a < 3; ++a)
+      #pragma unroll
       for (int bb = 0; bb < 3; ++bb) C[(int64_t)(kChSd + (8 + a) * 3 + bb) * npts] = vb.dbeta[bb][a];
+    #pragma unroll
     for (int q = 0; q < 6; ++q) {
       C[(int64_t)(kChDd + 0 * 6 + q) * npts] = vb.ddchi[q];
       C[(int64_t)(kChDd + 7 * 6 + q) * npts] = vb.ddalpha[q];
+      #pragma unroll
       for (int f = 0; f < 6; ++f) C[(int64_t)(kChDd + (1 + f) * 6 + q) * npts] = vb.ddg[f][q];
+      #pragma unroll
       for (int c = 0; c < 3; ++c) C[(int64_t)(kChDd + (8 + c) * 6 + q) * npts] = vb.ddbeta[c][q];
     }
+    #pragma unroll
     for (int bb = 0; bb < 3; ++bb) {
+      #pragma unroll
       for (int c = 0; c < 3; ++c) C[(int64_t)(kChGam + bb * 3 + c) * npts] = vb.dGam[bb][c];
       C[(int64_t)(kChKhat + bb) * npts] = vb.dKhat[bb];
       C[(int64_t)(kChTheta + bb) * npts] = vb.dTheta[bb];
     }
     double* R = rsb + (int64_t)b * 6 * npts + l;
+    #pragma unroll
     for (int q = 0; q < 6; ++q) R[(int64_t)q * npts] = Rsb[q];
     // stage algebra: w = gamma1 u + gamma2 v1 + beta dt r, v1 = u1 + delta u
     double* D = direct + (int64_t)b * NVAR * nv + p;
     double* U1B = u1bar + (int64_t)b * NVAR * nv + p;
+    #pragma unroll
     for (int n = 0; n < NVAR; ++n) {
-      const double v1b = (W.first ? 0. : U1B[(int64_t)n * nv]) + W.gamma2 * wb[n];
-      U1B[(int64_t)n * nv] = v1b;
+      // the adjoint of v1 = u1 + delta u: that of the stage's u1 output plus
+      // gamma2 wbar; the stage's u1 input is the constant 0 at stage 1
+      const double v1b = U1B[(int64_t)n * nv] + W.gamma2 * wb[n];
+      U1B[(int64_t)n * nv] = W.first ? 0. : v1b;
       D[(int64_t)n * nv] = vb.u[n] + W.gamma1 * wb[n] + W.delta * v1b;
     }
   }
@@ -324,6 +377,7 @@ k_adj_main(Grid g, DevParams P, const double* __restrict__ u, const double* __re
   se[threadIdx.x] = pe;
   sk[threadIdx.x] = pk;
   __syncthreads();
+  #pragma unroll
   for (int w = kThreads / 2; w > 0; w >>= 1) {
     if ((int)threadIdx.x < w) {
       se[threadIdx.x] += se[threadIdx.x + w];
@@ -355,24 +409,34 @@ k_adj_ricci(Grid g, DevParams P, const double* __restrict__ u, const double* __r
   const double* U = u + (int64_t)b * NVAR * nv;
   const double* SD = sd + (int64_t)b * kSdComponents * nv;
   RhsLocal<double> v;
-  gather_rhs<double>(g, P.fd[b], U, SD, nullptr, nullptr, p, v);
+  gather_rhs<double, kGatherRicci>(g, P.fd[b], U, SD, nullptr, nullptr, p, v);
   double Rsb[6];
   const double* R = rsb + (int64_t)b * 6 * npts + l;
+  #pragma unroll
   for (int q = 0; q < 6; ++q) Rsb[q] = R[(int64_t)q * npts];
   RhsLocal<double> vb;
+  #pragma unroll
   for (int q = 0; q < RhsLocal<double>::N; ++q) vb.data()[q] = 0.;
   ad::ricci_local_adj(P.p, v, Rsb, vb);
   double* C = chan + (int64_t)b * kNChan * npts + l;
+  #pragma unroll
   for (int a = 0; a < 3; ++a) C[(int64_t)(kChSd + a) * npts] += vb.dchi[a];
+  #pragma unroll
   for (int c = 0; c < 3; ++c)
+    #pragma unroll
     for (int q = 0; q < 6; ++q) C[(int64_t)(kChSd + (1 + q) * 3 + c) * npts] += vb.dg[c][q];
+  #pragma unroll
   for (int q = 0; q < 6; ++q) {
     C[(int64_t)(kChDd + 0 * 6 + q) * npts] += vb.ddchi[q];
+    #pragma unroll
     for (int f = 0; f < 6; ++f) C[(int64_t)(kChDd + (1 + f) * 6 + q) * npts] += vb.ddg[f][q];
   }
+  #pragma unroll
   for (int bb = 0; bb < 3; ++bb)
+    #pragma unroll
     for (int c = 0; c < 3; ++c) C[(int64_t)(kChGam + bb * 3 + c) * npts] += vb.dGam[bb][c];
   double* D = direct + (int64_t)b * NVAR * nv + p;
+  #pragma unroll
   for (int n = 0; n < NVAR; ++n)
     if (vb.u[n] != 0.) D[(int64_t)n * nv] += vb.u[n];
 }
@@ -533,12 +597,80 @@ k_adj_alg(Grid g, DevParams P, const double* __restrict__ upre, double* __restri
   double uu[NVAR], ub[NVAR];
   const double* UP = upre + (int64_t)b * NVAR * nv + q;
   double* UB = ubar + (int64_t)b * NVAR * nv + q;
+  #pragma unroll
   for (int n = 0; n < NVAR; ++n) {
     uu[n] = UP[(int64_t)n * nv];
     ub[n] = UB[(int64_t)n * nv];
   }
   ad::alg_constr_adj(P.p, uu, ub);
+  #pragma unroll
   for (int n = 0; n < NVAR; ++n) UB[(int64_t)n * nv] = ub[n];
+}
+
+// Transpose of the extrapolation boundary condition along one axis
+// (k_bc_axis: ExtrapolateOutflowBC, comm/physical_bcs.cpp:187-260, with the
+// reference's cell-centred index ends).  One thread per line, as the forward:
+// the line's ghosts y_1..y_4 (the outer side's y_1 is the boundary vertex)
+// were y_g = 5 z1 - 10 z2 + 10 z3 - 5 z4 + z5 over the five values inward of
+// it, earlier ghosts included.  Their adjoints flow into those values in
+// reverse order; the overwritten values' own adjoints become zero.
+template <int AX>
+__global__ void __launch_bounds__(kThreads)
+k_adj_bc_axis(Grid g, double* __restrict__ ub) {
+  constexpr int ax = AX;
+  constexpr int o1 = (ax == 0) ? 1 : 0;
+  constexpr int o2 = (ax == 2) ? 1 : 2;
+  const int64_t nt = (int64_t)g.nn[o1] * g.nn[o2];
+  const int nfb = g.nb[o1] * g.nb[o2];
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt * 2 * NVAR * nfb) return;
+  const int64_t tr = t % nt;
+  int64_t r = t / nt;
+  const int side = (int)(r % 2);
+  r /= 2;
+  const int n = (int)(r % NVAR);
+  const int fb = (int)(r / NVAR);
+  int loc[3];
+  loc[ax] = side ? g.nb[ax] - 1 : 0;
+  loc[o1] = fb % g.nb[o1];
+  loc[o2] = fb / g.nb[o1];
+  if (g.bc[2 * ax + side] == Z4C_BC_PERIODIC) return;
+  const int b = loc[0] + g.nb[0] * (loc[1] + g.nb[1] * loc[2]);
+  bool need[6];
+  for (int a = 0; a < 3; ++a) {
+    need[2 * a] = (g.bc[2 * a] != Z4C_BC_PERIODIC) && loc[a] == 0;
+    need[2 * a + 1] = (g.bc[2 * a + 1] != Z4C_BC_PERIODIC) && loc[a] == g.nb[a] - 1;
+  }
+  int is[3], ie[3];
+  for (int a = 0; a < 3; ++a) {
+    is[a] = NG;
+    ie[a] = NG + g.nx[a] - 1;
+  }
+  int lo[3], hi[3];
+  lo[0] = is[0] - NG; hi[0] = ie[0] + NG;
+  lo[1] = need[2] ? is[1] : is[1] - NG;
+  hi[1] = need[3] ? ie[1] : ie[1] + NG;
+  lo[2] = need[4] ? is[2] : is[2] - NG;
+  hi[2] = need[5] ? ie[2] : ie[2] + NG;
+  if (ax == 2) { lo[1] = is[1] - NG; hi[1] = ie[1] + NG; }
+  const int t1 = (int)(tr % g.nn[o1]), t2 = (int)(tr / g.nn[o1]);
+  if (t1 < lo[o1] || t1 > hi[o1] || t2 < lo[o2] || t2 > hi[o2]) return;
+  double* u = ub + ((int64_t)b * NVAR + n) * g.nvol + (int64_t)t1 * g.s[o1] + (int64_t)t2 * g.s[o2];
+  const int64_t st = g.s[ax];
+  const int dir = side ? -1 : 1;
+  const int ia0 = side ? ie[ax] + 1 : is[ax] - 1;
+  // sequence s[0..8] = x_4, x_3, x_2, x_1, x_0, y_1, y_2, y_3, y_4 (x_0 the
+  // value next to the ghosts); its adjoints
+  double sb[9];
+  for (int q = 0; q < 5; ++q) sb[4 - q] = u[(int64_t)(ia0 + dir * (q + 1)) * st];
+  for (int gh = 1; gh <= NG; ++gh) sb[4 + gh] = u[(int64_t)(side ? ie[ax] + gh : is[ax] - gh) * st];
+  constexpr double c[5] = {5., -10., 10., -5., 1.};
+  for (int gh = NG; gh >= 1; --gh) {
+    const double y = sb[4 + gh];
+    for (int k = 0; k < 5; ++k) sb[4 + gh - 1 - k] += c[k] * y;
+  }
+  for (int q = 0; q < 5; ++q) u[(int64_t)(ia0 + dir * (q + 1)) * st] = sb[4 - q];
+  for (int gh = 1; gh <= NG; ++gh) u[(int64_t)(side ? ie[ax] + gh : is[ax] - gh) * st] = 0.;
 }
 
 // Block grid neighbour in direction d (periodic wrap; -1 beyond a
@@ -557,34 +689,50 @@ __device__ __forceinline__ int grid_neighbour(const Grid& g, int b, const int d[
 
 // E^T of the same-level exchange: the adjoint of every owner copy of a
 // vertex is 1/m times the sum of the adjoints of all entries (own, other
-// owners', ghosts anywhere) that hold that vertex after the exchange.  One
-// thread per (block, variable, interior vertex); wbar receives the interior.
+// owners', ghosts anywhere) that hold that vertex after the exchange.  Along
+// each axis an interior index i has the images i, i + nx and i - nx where
+// they lie in [0, nn) (a neighbour's interior or ghost entry); one thread per (block, interior
+// vertex) forms the images once and sums all 22 variables.
 __global__ void __launch_bounds__(kThreads)
 k_adj_exchange(Grid g, const double* __restrict__ ubar, double* __restrict__ wbar) {
   const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= npts * NVAR * g.nblocks) return;
+  if (t >= npts * g.nblocks) return;
   const int64_t l = t % npts;
-  const int n = (int)((t / npts) % NVAR);
-  const int b = (int)(t / (npts * NVAR));
-  int i, j, k;
-  interior_of(g, l, i, j, k);
+  const int b = (int)(t / npts);
+  int ijk[3];
+  interior_of(g, l, ijk[0], ijk[1], ijk[2]);
+  // per axis: the block steps d whose image index i - d nx lies in [0, nn)
+  int dlist[3][3], nd[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    nd[a] = 1;
+    dlist[a][0] = dlist[a][1] = dlist[a][2] = 0;
+    if (ijk[a] + g.nx[a] < g.nn[a]) dlist[a][nd[a]++] = -1;
+    if (ijk[a] - g.nx[a] >= 0) dlist[a][nd[a]++] = 1;
+  }
   const int64_t nv = g.nvol;
-  double s = 0.;
-  int m = 0;
-  for (int d2 = -1; d2 <= 1; ++d2)
-    for (int d1 = -1; d1 <= 1; ++d1)
-      for (int d0 = -1; d0 <= 1; ++d0) {
-        const int d[3] = {d0, d1, d2};
+  int64_t off[27];
+  int nimg = 0, m = 0;
+  for (int z = 0; z < nd[2]; ++z)
+    for (int y = 0; y < nd[1]; ++y)
+      for (int x = 0; x < nd[0]; ++x) {
+        const int d[3] = {dlist[0][x], dlist[1][y], dlist[2][z]};
         const int nb = grid_neighbour(g, b, d);
         if (nb < 0) continue;
-        const int li = i - d0 * g.nx[0], lj = j - d1 * g.nx[1], lk = k - d2 * g.nx[2];
-        if (li < 0 || li >= g.nn[0] || lj < 0 || lj >= g.nn[1] || lk < 0 || lk >= g.nn[2]) continue;
-        s += ubar[((int64_t)nb * NVAR + n) * nv + ((int64_t)lk * g.nn[1] + lj) * g.nn[0] + li];
+        const int li = ijk[0] - d[0] * g.nx[0], lj = ijk[1] - d[1] * g.nx[1],
+                  lk = ijk[2] - d[2] * g.nx[2];
+        off[nimg++] = (int64_t)nb * NVAR * nv + ((int64_t)lk * g.nn[1] + lj) * g.nn[0] + li;
         if (is_interior(g, li, lj, lk)) ++m;
       }
-  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
-  wbar[((int64_t)b * NVAR + n) * nv + p] = s / (double)m;
+  const double inv = 1.0 / (double)m;
+  const int64_t p = ((int64_t)ijk[2] * g.nn[1] + ijk[1]) * g.nn[0] + ijk[0];
+  double* W = wbar + (int64_t)b * NVAR * nv + p;
+  for (int n = 0; n < NVAR; ++n) {
+    double s = 0.;
+    for (int q = 0; q < nimg; ++q) s += ubar[off[q] + (int64_t)n * nv];
+    W[(int64_t)n * nv] = s * inv;
+  }
 }
 
 // ---- tangent-linear model ------------------------------------------------------
@@ -612,11 +760,14 @@ k_tlm_stage(Grid g, DevParams P, const double* __restrict__ u, const double* __r
                    sdd + (int64_t)b * kSdComponents * nv, p, v);
   Dual out[NVAR];
   ad::rhs_local(P.p, v, out);
+  #pragma unroll
   for (int n = 0; n < NVAR; ++n) {
     const double* fd = ud + boff + (int64_t)n * nv;
     double r = out[n].d;
+    #pragma unroll
     for (int a = 0; a < 3; ++a) {
       double s = 0.;
+      #pragma unroll
       for (int o = -4; o <= 4; ++o) s += w_ko(o) * fd[p + o * g.s[a]];
       r += s * F.cidxd[a] * P.p.diss;
     }
@@ -628,10 +779,12 @@ k_tlm_stage(Grid g, DevParams P, const double* __restrict__ u, const double* __r
   }
 }
 
-// AlgConstr and its tangent at every vertex: (upre, upre_dot) -> (u, u_dot).
+// The tangent of AlgConstr at every vertex: (upre, upre_dot) -> u_dot (the
+// value itself comes from the forward kernel, whose rounding this
+// translation unit, compiled with contraction, does not reproduce).
 __global__ void __launch_bounds__(kThreads)
 k_tlm_alg(Grid g, DevParams P, const double* __restrict__ upre, const double* __restrict__ upred,
-          double* __restrict__ u, double* __restrict__ ud) {
+          double* __restrict__ ud) {
   const int64_t nv = g.nvol;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nv * g.nblocks) return;
@@ -639,12 +792,11 @@ k_tlm_alg(Grid g, DevParams P, const double* __restrict__ upre, const double* __
   const int64_t q = t % nv;
   const int64_t base = (int64_t)b * NVAR * nv + q;
   Dual x[NVAR];
+  #pragma unroll
   for (int n = 0; n < NVAR; ++n) x[n] = Dual(upre[base + (int64_t)n * nv], upred[base + (int64_t)n * nv]);
   ad::alg_constr_local(P.p, x);
-  for (int n = 0; n < NVAR; ++n) {
-    u[base + (int64_t)n * nv] = x[n].v;
-    ud[base + (int64_t)n * nv] = x[n].d;
-  }
+  #pragma unroll
+  for (int n = 0; n < NVAR; ++n) ud[base + (int64_t)n * nv] = x[n].d;
 }
 
 // ---- the objective: vol * sum over cells of H^2 --------------------------------
@@ -660,24 +812,31 @@ __device__ void gather_ham(const Grid& g, const FdScale& F, const double* U, con
     return f;
   };
   v.chi = fld(Z4C_CHI).at(p);
+  #pragma unroll
   for (int c = 0; c < 6; ++c) {
     v.gt[c] = fld(Z4C_GXX + c).at(p);
     v.At[c] = fld(Z4C_AXX + c).at(p);
   }
   v.Khat = fld(Z4C_KHAT).at(p);
   v.Theta = fld(Z4C_THETA).at(p);
+  #pragma unroll
   for (int a = 0; a < 3; ++a) {
     v.dchi[a] = st_d1(fld(Z4C_CHI), p, g.s[a], F.cidx1[a]);
+    #pragma unroll
     for (int q = 0; q < 6; ++q) v.dg3[a][q] = st_d1(fld(Z4C_GXX + q), p, g.s[a], F.cidx1[a]);
   }
+  #pragma unroll
   for (int a = 0; a < 3; ++a)
+    #pragma unroll
     for (int b = a; b < 3; ++b) {
       const int pr = ad::sid(a, b);
       if (a == b) {
         v.ddchi[pr] = st_d2(fld(Z4C_CHI), p, g.s[a], F.cidx2[a]);
+        #pragma unroll
         for (int q = 0; q < 6; ++q) v.ddg[q][pr] = st_d2(fld(Z4C_GXX + q), p, g.s[a], F.cidx2[a]);
       } else {
         v.ddchi[pr] = st_d2x(fld(Z4C_CHI), p, g.s[a], g.s[b], F.cidx1[a], F.cidx1[b]);
+        #pragma unroll
         for (int q = 0; q < 6; ++q)
           v.ddg[q][pr] = st_d2x(fld(Z4C_GXX + q), p, g.s[a], g.s[b], F.cidx1[a], F.cidx1[b]);
       }
@@ -763,6 +922,7 @@ k_ham_adj(Grid g, DevParams P, const double* __restrict__ xv, const double* __re
   int i, j, k;
   interior_of(g, l, i, j, k);
   HLocal<double> vb;
+  #pragma unroll
   for (int q = 0; q < HLocal<double>::N; ++q) vb.data()[q] = 0.;
   if (hst_cell(g, P, xv, b, i, j, k) && con_live(g, P, b, i, j, k)) {
     const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
@@ -773,6 +933,7 @@ k_ham_adj(Grid g, DevParams P, const double* __restrict__ xv, const double* __re
     ad::ham_local_adj(P.p, v, scale * 2. * vol * H, vb);
   }
   double* C = hchan + (int64_t)b * kNHChan * npts + l;
+  #pragma unroll
   for (int q = 0; q < kNHChan; ++q) C[(int64_t)q * npts] = vb.data()[q];
 }
 
@@ -935,13 +1096,23 @@ int check_ctx(z4c_ctx* c) {
   if (c->ml) return err(Z4C_ESTATE, "the adjoint runs on uniform meshes (no refined levels)");
   if (c->integrator != Z4C_INTEG_RK4) return err(Z4C_ESTATE, "the adjoint differentiates rk4 (2S)");
   if (c->g.has_sommerfeld) return err(Z4C_ESTATE, "the adjoint has no gr_sommerfeld faces");
-  for (int f = 0; f < 6; ++f)
-    if (c->g.bc[f] != Z4C_BC_PERIODIC)
-      return err(Z4C_ESTATE, "the adjoint runs on periodic meshes");
+
   if (c->params.chi_psi_power != -4.)
     return err(Z4C_ESTATE, "the adjoint objective assumes chi_psi_power = -4");
   if (!c->adj) return err(Z4C_ESTATE, "call z4c_adj_setup first");
   return Z4C_OK;
+}
+
+// Transpose of launch_physical_bcs: the axes in reverse order.
+void adj_physical_bcs(const Grid& g, double* ub, cudaStream_t st) {
+  for (int ax = 2; ax >= 0; --ax) {
+    if (g.bc[2 * ax] == Z4C_BC_PERIODIC && g.bc[2 * ax + 1] == Z4C_BC_PERIODIC) continue;
+    const int o1 = (ax == 0) ? 1 : 0, o2 = (ax == 2) ? 1 : 2;
+    const int64_t n = (int64_t)g.nn[o1] * g.nn[o2] * 2 * NVAR * g.nb[o1] * g.nb[o2];
+    auto kern = ax == 0 ? k_adj_bc_axis<0> : ax == 1 ? k_adj_bc_axis<1> : k_adj_bc_axis<2>;
+    kern<<<div_up(n, kThreads), kThreads, 0, st>>>(g, ub);
+    add_kernel_launches(1);
+  }
 }
 
 // Forward stage s (1-based) from u (stage input, all vertices) and u1: w,
@@ -956,6 +1127,8 @@ int fwd_stage(z4c_ctx* c, int s, double dt, const double* u, double* u1, double*
   ALAUNCH("stage");
   launch_exchange(c->g, P, w, upre, c->nbr, 0, c->stream);
   ALAUNCH("exchange");
+  launch_physical_bcs(c->g, upre, NVAR, c->stream);
+  ALAUNCH("physical_bcs");
   if (uout) {
     if (uout != upre)
       ACUDA(cudaMemcpyAsync(uout, upre, sizeof(double) * c->adj->reg_elems,
@@ -1012,7 +1185,8 @@ int adj_step(z4c_ctx* c, double dt, const double* u) {
     // AlgConstr^T then E^T: adjoint of this stage's output w
     k_adj_alg<<<div_up(g.nvol * g.nblocks, kThreads), kThreads, 0, c->stream>>>(g, P, A->upre[s - 1],
                                                                              A->adj);
-    k_adj_exchange<<<div_up(npts * NVAR * g.nblocks, kThreads), kThreads, 0, c->stream>>>(
+    adj_physical_bcs(g, A->adj, c->stream);
+    k_adj_exchange<<<div_up(npts * g.nblocks, kThreads), kThreads, 0, c->stream>>>(
         g, A->adj, A->wbar);
     ALAUNCH("adjoint exchange");
     add_kernel_launches(2);
@@ -1234,14 +1408,19 @@ int z4c_tlm_step(z4c_ctx* c, double dt) {
     rc = fwd_stage(c, s, dt, u, A->u1, A->w, A->us, nullptr);
     if (rc) return rc;
     launch_exchange(g, P, A->tanw, A->tan, c->nbr, 0, c->stream);
+    launch_physical_bcs(g, A->tan, NVAR, c->stream);
     ALAUNCH("tangent exchange");
     // (A->us, A->tan) are the pre-constraint state and its tangent
     ACUDA(cudaMemcpyAsync(A->tanw, A->tan, sizeof(double) * A->reg_elems, cudaMemcpyDeviceToDevice,
                           c->stream));
     k_tlm_alg<<<div_up(g.nvol * g.nblocks, kThreads), kThreads, 0, c->stream>>>(g, P, A->us,
-                                                                            A->tanw, u, A->tan);
+                                                                            A->tanw, A->tan);
     ALAUNCH("tangent alg_constr");
     add_kernel_launches(1);
+    ACUDA(cudaMemcpyAsync(u, A->us, sizeof(double) * A->reg_elems, cudaMemcpyDeviceToDevice,
+                          c->stream));
+    launch_alg_constr(g, P, u, 0, g.nblocks, c->stream);
+    ALAUNCH("alg_constr");
   }
   return Z4C_OK;
 }

@@ -436,7 +436,8 @@ int z4c_regrid(z4c_ctx *dst, const z4c_ctx *src);
  * exchange and AlgConstr), and of the objective J = sum over blocks of the
  * cell volume times the sum over the history cells of H^2, H the Hamiltonian
  * constraint of ADMConstraints after Z4cToADM (the H-norm of
- * outputs/history.cpp:168-200).  Uniform periodic meshes, rk4,
+ * outputs/history.cpp:168-200).  Uniform meshes with periodic and
+ * extrapolate_outflow faces (gr_sommerfeld faces are rejected), rk4,
  * chi_psi_power = -4.  The state's adjoint lives in Z4C_REG_ADJ and a
  * tangent in Z4C_REG_TAN, each over every vertex (ghosts included); the
  * adjoints of the gauge parameters shift_eta and damp_kappa1 accumulate in

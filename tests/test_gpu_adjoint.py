@@ -15,22 +15,33 @@
 Tolerances: the adjoint and the tangent-linear model differentiate the same
 discrete map, so they agree to rounding (1e-10 relative); central
 differences carry a truncation error O(h^2) and a rounding error O(eps/h),
-the bound on them is 1e-6 relative."""
+the bound on them is 1e-6 relative.
+
+eps_floor = -1 in every run compared with differences.  AlgConstr rescales
+g~ by regularize_nth_root(det g~, 1, eps_floor, -3) (z4c.cpp:677-799,
+floating_point.hpp:120-131), which switches from det^(-1/3) to the constant
+1 - eps_floor/3 where det g~ < 1 + eps_floor.  AlgConstr itself sets
+det g~ = 1 every stage and the evolution keeps it there to rounding, so with
+the default eps_floor = 1e-12 nearly every vertex sits on that switch: the
+map is not differentiable along the determinant direction, the derivatives
+take the branch of the linearisation point and a difference quotient of any
+step averages the two.  A negative eps_floor selects det^(-1/3) everywhere
+(the constraint the switch approximates) and the map is smooth."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 PUNC = dict(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02, damp_kappa2=0.0, shift_eta=2.0,
-            r_max_con=1e300)
+            r_max_con=1e300, eps_floor=-1.0)
 GW = dict(lapse_harmonic=1.0, lapse_harmonicf=0.0, lapse_oplog=0.0, lapse_advect=0.0,
           shift_Gamma=0.0, shift_eta=0.0, shift_advect=0.0, diss=0.02, damp_kappa1=0.02,
-          r_max_con=1e300)
+          r_max_con=1e300, eps_floor=-1.0)
 
 
-def make(nb, nx, params, lim=0.5):
+def make(nb, nx, params, lim=0.5, bc="periodic"):
     import z4c_b200 as Z
-    mesh = Z.Mesh(nb, (nx,) * 3, (-lim,) * 3, (lim,) * 3, "periodic")
+    mesh = Z.Mesh(nb, (nx,) * 3, (-lim,) * 3, (lim,) * 3, bc)
     ctx = Z.Z4c(mesh, Z.default_params(**params), "rk4")
     ctx.adj_setup()
     return Z, mesh, ctx
@@ -38,8 +49,9 @@ def make(nb, nx, params, lim=0.5):
 
 def rich_state(Z, mesh, ctx, amp=1e-3, seed=0):
     """A gauge wave (A = 0.05) with smooth periodic perturbations of size amp
-    on every variable, the shift included, so that every term of the
-    right-hand side (advection too) is active."""
+    on every variable, and a shift of one sign per component (the upwind
+    side never switches), so that every term of the right-hand side,
+    advection included, is active and differentiable."""
     from z4c_b200 import initial_data as ID
     ID.load_adm(ctx, ID.gauge_wave1(mesh, amplitude=0.05))
     u = ctx.download(Z.REG_U)
@@ -50,7 +62,11 @@ def rich_state(Z, mesh, ctx, amp=1e-3, seed=0):
         for n in range(22):
             k = rng.integers(1, 3, size=3)
             ph = rng.uniform(0, 2 * np.pi)
-            u[b, n] += amp * np.sin(2 * np.pi * (k[0] * Zc + k[1] * Y + k[2] * X) + ph)
+            wave = np.sin(2 * np.pi * (k[0] * Zc + k[1] * Y + k[2] * X) + ph)
+            if n >= Z.BETAX:  # 0.5 amp .. 2.5 amp, signs +, -, +
+                u[b, n] = (1 if n != Z.BETAY else -1) * amp * (1.5 + wave)
+            else:
+                u[b, n] += amp * wave
     ctx.upload(Z.REG_U, u)
     ctx.init_finalize()
     return ctx.download(Z.REG_U)
@@ -60,13 +76,32 @@ def dot(a, b):
     return float(np.sum(a * b))
 
 
-@pytest.mark.parametrize("params", [PUNC, GW], ids=["puncture_gauge", "gauge_wave"])
-def test_tlm_step_matches_central_differences(params):
-    Z, mesh, ctx = make((2, 2, 1), 12, params)
+def smooth_direction(Z, mesh, seed, amp=1e-3):
+    """A smooth periodic direction on every variable and vertex (the outflow
+    extrapolation multiplies rough data by up to ~10^3 per axis in the
+    ghosts, which would leave the range where differences are linear)."""
+    rng = np.random.default_rng(seed)
+    out = np.zeros((mesh.nblocks, 22) + tuple(reversed(mesh.nn)))
+    for b in range(mesh.nblocks):
+        xs, _ = mesh.block_coords(b)
+        X, Y, Zc = np.meshgrid(xs[2], xs[1], xs[0], indexing="ij")
+        for n in range(22):
+            k = rng.integers(1, 3, size=3)
+            ph = rng.uniform(0, 2 * np.pi)
+            out[b, n] = amp * np.sin(2 * np.pi * (k[0] * Zc + k[1] * Y + k[2] * X) + ph)
+    return out
+
+
+CASES = [(PUNC, "periodic"), (GW, "periodic"), (PUNC, "outflow")]
+CASE_IDS = ["puncture_gauge", "gauge_wave", "puncture_gauge_outflow"]
+
+
+@pytest.mark.parametrize("params,bc", CASES, ids=CASE_IDS)
+def test_tlm_step_matches_central_differences(params, bc):
+    Z, mesh, ctx = make((2, 2, 1), 12, params, bc=bc)
     u0 = rich_state(Z, mesh, ctx)
     dt = 0.25 * float(ctx.dx().min())
-    rng = np.random.default_rng(1)
-    v = rng.standard_normal(u0.shape) * 1e-3
+    v = smooth_direction(Z, mesh, 1)
     ctx.upload(Z.REG_TAN, v)
     ctx.upload(Z.REG_U, u0)
     ctx.tlm_step(dt)
@@ -82,15 +117,26 @@ def test_tlm_step_matches_central_differences(params):
         ctx.evolve(dt, 1)
         out.append(ctx.download(Z.REG_U))
     fd = (out[0] - out[1]) / (2 * h)
-    err = np.abs(fd - tan).max() / np.abs(tan).max()
-    print(f"tlm vs central differences: {err:.2e}")
-    assert err <= 1e-6
+    if bc == "periodic":
+        err = np.abs(fd - tan).max() / np.abs(tan).max()
+        tol = 1e-6
+    else:
+        # The reference's extrapolation (5, -10, 10, -5, 1, cascaded over four
+        # ghost layers and three axes) multiplies the state's rounding by up
+        # to ~1e9 in the corner ghosts, which makes a difference quotient
+        # noise there; the interior is compared, and the exact transpose
+        # test below covers the boundary conditions.
+        I = (slice(None), slice(None), slice(4, -4), slice(4, -4), slice(4, -4))
+        err = np.abs(fd - tan)[I].max() / np.abs(tan[I]).max()
+        tol = 5e-5
+    print(f"tlm vs central differences ({bc}): {err:.2e}")
+    assert err <= tol
     ctx.close()
 
 
-@pytest.mark.parametrize("params", [PUNC, GW], ids=["puncture_gauge", "gauge_wave"])
-def test_adjoint_step_is_the_transpose_of_the_tlm_step(params):
-    Z, mesh, ctx = make((2, 2, 1), 12, params)
+@pytest.mark.parametrize("params,bc", CASES, ids=CASE_IDS)
+def test_adjoint_step_is_the_transpose_of_the_tlm_step(params, bc):
+    Z, mesh, ctx = make((2, 2, 1), 12, params, bc=bc)
     u0 = rich_state(Z, mesh, ctx)
     dt = 0.25 * float(ctx.dx().min())
     rng = np.random.default_rng(2)
@@ -128,16 +174,18 @@ def test_parameter_adjoints_match_differences():
     pb = ctx.adj_params()
     ctx.close()
     for k, name in enumerate(("shift_eta", "damp_kappa1")):
-        vals = []
+        states = []
+        dp = 1e-3  # below ~1e-4 the rounding of the states dominates
         for sgn in (1, -1):
             p = dict(PUNC)
-            p[name] = PUNC[name] + sgn * 1e-4
+            p[name] = PUNC[name] + sgn * dp
             Z2, mesh2, c2 = make((2, 2, 1), 12, p)
             c2.upload(Z2.REG_U, u0)
             c2.evolve(dt, 1)
-            vals.append(dot(ub, c2.download(Z2.REG_U)))
+            states.append(c2.download(Z2.REG_U))
             c2.close()
-        fd = (vals[0] - vals[1]) / 2e-4
+        # difference the states first: <ub, u> itself is a sum of ~10^6 terms
+        fd = dot(ub, states[0] - states[1]) / (2 * dp)
         print(f"{name}: adjoint {pb[k]:.12e}, differences {fd:.12e}")
         assert abs(fd - pb[k]) <= 1e-6 * abs(fd)
 
@@ -229,29 +277,66 @@ def test_configs3_gradient_against_differences_and_tangent_linear_runs():
     J, pb, st = ctx.gradient(dt, nsteps, 9)
     g = ctx.download(Z.REG_ADJ)
     print(f"J = {J:.10e}, gradient in {st['seconds']:.2f} s, {st}")
+    import time
+    ctx.upload(Z.REG_U, u0)
+    ctx.evolve(dt, 2)
+    ctx.sync()
+    t0 = time.perf_counter()
+    ctx.evolve(dt, 20)
+    ctx.sync()
+    fwd = (time.perf_counter() - t0) / 20
+    ctx.upload(Z.REG_U, u0)
+    ctx.adj_step(dt)
+    ctx.sync()
+    t0 = time.perf_counter()
+    for _ in range(5):
+        ctx.adj_step(dt)
+    ctx.sync()
+    adj = (time.perf_counter() - t0) / 5
+    print(f"forward step {fwd * 1e3:.3f} ms, adjoint step {adj * 1e3:.3f} ms, ratio {adj / fwd:.2f}")
     assert np.array_equal(ctx.download(Z.REG_U), u0)
     rng = np.random.default_rng(32)
-    worst_fd = worst_tlm = 0.0
-    h = 1e-5
+    worst_tlm = 0.0
+    errs, pairs = [], []
+    # Fourth-order central differences, (-J(2h) + 8 J(h) - 8 J(-h) + J(-2h)) / 12h,
+    # exact up to cubic terms: perturbations of the size of the initial noise
+    # (1e-6) keep far above the rounding of 100 steps.  The directions leave
+    # the shift alone: it is zero throughout the gauge wave (no shift
+    # evolution), where the advection's upwind side switches with its sign,
+    # so J is only one-sidedly differentiable along it (the adjoint takes the
+    # side of beta >= 0); the tangent-linear runs below use full directions.
+    import z4c_b200 as Zp
+    h = 1.0  # perturbations of 1e-6 and 2e-6
     for d in range(32):
         v = rng.standard_normal(u0.shape) * 1e-6
-        Js = []
-        for sgn in (1, -1):
-            ctx.upload(Z.REG_U, u0 + sgn * h * v)
+        v_full = v.copy()
+        v[:, Zp.BETAX:Zp.BETAZ + 1] = 0.0
+        Js = {}
+        for m in (2, 1, -1, -2):
+            ctx.upload(Z.REG_U, u0 + m * h * v)
             ctx.evolve(dt, nsteps)
-            Js.append(ctx.objective(Z.REG_U)[0])
-        fd = (Js[0] - Js[1]) / (2 * h)
+            Js[m] = ctx.objective(Z.REG_U)[0]
+        fd = (-Js[2] + 8 * Js[1] - 8 * Js[-1] + Js[-2]) / (12 * h)
         ad = dot(g, v)
-        worst_fd = max(worst_fd, abs(fd - ad) / abs(ad))
-        if d < 4:  # tangent-linear runs along the first directions
+        errs.append(abs(fd - ad) / abs(ad))
+        pairs.append((fd, ad))
+        if d < 4:  # tangent-linear runs along the first directions, shift included
             ctx.upload(Z.REG_U, u0)
-            ctx.upload(Z.REG_TAN, v)
+            ctx.upload(Z.REG_TAN, v_full)
             for _ in range(nsteps):
                 ctx.tlm_step(dt)
             _, Jd = ctx.objective(Z.REG_U, Z.REG_TAN)
-            worst_tlm = max(worst_tlm, abs(Jd - ad) / abs(ad))
-    print(f"configs[3]: worst relative difference to central differences {worst_fd:.2e}, "
-          f"to tangent-linear runs {worst_tlm:.2e}")
+            ad_full = dot(g, v_full)
+            worst_tlm = max(worst_tlm, abs(Jd - ad_full) / abs(ad_full))
+    # A random direction's derivative can come out near zero, where a
+    # relative difference means little: each difference is measured against
+    # the root-mean-square derivative over the 32 directions.
+    fds, ads = np.array(pairs).T
+    rms = np.sqrt(np.mean(ads ** 2))
+    worst_fd = float(np.max(np.abs(fds - ads)) / rms)
+    print(f"configs[3]: relative difference to central differences: median {np.median(errs):.2e} "
+          f"(own derivative), worst {worst_fd:.2e} (rms derivative); to tangent-linear runs "
+          f"{worst_tlm:.2e}")
     assert worst_fd <= 1e-6
     assert worst_tlm <= 1e-9
     ctx.close()
