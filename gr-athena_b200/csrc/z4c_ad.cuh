@@ -552,8 +552,12 @@ Z4C_HD void christoffel_adj(const RhsLocal<double>& v, const double guu[6],
 }
 
 // Reverse of ricci_local: Rsb = adjoint of Rsum_ab (six stored pairs).
+// chr_bar (may be null): adjoints of the Christoffel quantities from the
+// main algebra's reverse (guu 6, Gamma^c_ab 18, Gamma^a 3), added before the
+// Christoffel reverse runs once for both parts.
 Z4C_HD void ricci_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
-                            const double Rsb[6], RhsLocal<double>& vb) {
+                            const double Rsb[6], RhsLocal<double>& vb,
+                            const double* chr_bar = nullptr) {
   double guu[6], Gd[3][6], Gudd[3][6], Gu[3];
   christoffel_local(v, guu, Gd, Gudd, Gu);
   const double* g = v.u + Z4C_GXX;
@@ -689,14 +693,27 @@ Z4C_HD void ricci_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
         Gdb[b][sid(a, c)] += Gu[c] * X;
       }
     }
+  if (chr_bar) {
+Z4C_UNROLL
+    for (int q = 0; q < 6; ++q) guub[q] += chr_bar[q];
+Z4C_UNROLL
+    for (int c = 0; c < 3; ++c)
+Z4C_UNROLL
+      for (int q = 0; q < 6; ++q) Guddb[c][q] += chr_bar[6 + c * 6 + q];
+Z4C_UNROLL
+    for (int a = 0; a < 3; ++a) Gub[a] += chr_bar[24 + a];
+  }
   christoffel_adj(v, guu, Gd, Gudd, guub, Gdb, Guddb, Gub, vb);
 }
 
 // Reverse of main_local: ob = adjoint of the 22 outputs; accumulates into vb,
-// into Rsb (adjoint of Rsum) and into the parameter adjoints pb.
+// into Rsb (adjoint of Rsum) and into the parameter adjoints pb.  With
+// chr_bar non-null the adjoints of the Christoffel quantities (guu 6,
+// Gamma^c_ab 18, Gamma^a 3) are written there instead of being reversed into
+// g~ and its derivatives (ricci_local_adj takes them up).
 Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
                            const double Rsum[6], const double ob[NV], RhsLocal<double>& vb,
-                           double Rsb[6], ParamBar& pb) {
+                           double Rsb[6], ParamBar& pb, double* chr_bar = nullptr) {
   double guu[6], Gd[3][6], Gudd[3][6], Gu[3];
   christoffel_local(v, guu, Gd, Gudd, Gu);
   const double* g = v.u + Z4C_GXX;
@@ -1088,6 +1105,17 @@ Z4C_HD void main_local_adj(const z4c_params_t& opt, const RhsLocal<double>& v,
   vb.u[Z4C_ALPHA] += alphab;
   vb.u[Z4C_KHAT] += Kb;
   vb.u[Z4C_THETA] += 2. * Kb;
+  if (chr_bar) {
+Z4C_UNROLL
+    for (int q = 0; q < 6; ++q) chr_bar[q] = guub[q];
+Z4C_UNROLL
+    for (int c = 0; c < 3; ++c)
+Z4C_UNROLL
+      for (int q = 0; q < 6; ++q) chr_bar[6 + c * 6 + q] = Guddb[c][q];
+Z4C_UNROLL
+    for (int a = 0; a < 3; ++a) chr_bar[24 + a] = Gub[a];
+    return;
+  }
   christoffel_adj(v, guu, Gd, Gudd, guub, Gdb, Guddb, Gub, vb);
 }
 

@@ -60,6 +60,9 @@ constexpr int kChGam = 99;    // 9: d_b Gamma^c, b*3 + c
 constexpr int kChKhat = 108;  // 3
 constexpr int kChTheta = 111; // 3
 constexpr int kNChan = 114;
+// per interior vertex from the main reverse to the Ricci reverse: the Ricci
+// sums' adjoints (6) and the Christoffel adjoints (27)
+constexpr int kNRsb = 33;
 // channels of the Hamiltonian-constraint reverse per interior vertex
 constexpr int kHChi = 0, kHGt = 1, kHAt = 7, kHKhat = 13, kHTheta = 14;  // point values
 constexpr int kHDchi = 15, kHDg = 18, kHDdchi = 36, kHDdg = 42;         // stencil inputs
@@ -310,22 +313,11 @@ k_adj_main(Grid g, DevParams P, const double* __restrict__ u, const double* __re
     for (int q = 0; q < RhsLocal<double>::N; ++q) vb.data()[q] = 0.;
     double Rsb[6] = {0, 0, 0, 0, 0, 0};
     ad::ParamBar pb{0., 0.};
-    ad::main_local_adj(P.p, v, Rs, ob, vb, Rsb, pb);
+    double cb[27];
+    ad::main_local_adj(P.p, v, Rs, ob, vb, Rsb, pb, cb);
     pe = pb.shift_eta;
     pk = pb.damp_kappa1;
-    // the advection sums' dependence on the shift at the vertex
-    #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const bool left = v.u[Z4C_BETAX + a] < 0;
-      double acc = 0.;
-      #pragma unroll
-      for (int n = 0; n < NVAR; ++n) {
-        if (vb.lv[n] == 0.) continue;
-        Fld<double> f{U + (int64_t)n * nv};
-        acc += vb.lv[n] * st_lop(f, p, g.s[a], left);
-      }
-      vb.u[Z4C_BETAX + a] += acc * F.lidx[a];
-    }
+    // (the advection sums' dependence on the shift at the vertex: k_adj_advbeta)
     // channels
     double* C = chan + (int64_t)b * kNChan * npts + l;
     #pragma unroll
@@ -357,9 +349,9 @@ k_adj_main(Grid g, DevParams P, const double* __restrict__ u, const double* __re
       C[(int64_t)(kChKhat + bb) * npts] = vb.dKhat[bb];
       C[(int64_t)(kChTheta + bb) * npts] = vb.dTheta[bb];
     }
-    double* R = rsb + (int64_t)b * 6 * npts + l;
-    #pragma unroll
+    double* R = rsb + (int64_t)b * kNRsb * npts + l;
     for (int q = 0; q < 6; ++q) R[(int64_t)q * npts] = Rsb[q];
+    for (int q = 0; q < 27; ++q) R[(int64_t)(6 + q) * npts] = cb[q];
     // stage algebra: w = gamma1 u + gamma2 v1 + beta dt r, v1 = u1 + delta u
     double* D = direct + (int64_t)b * NVAR * nv + p;
     double* U1B = u1bar + (int64_t)b * NVAR * nv + p;
@@ -391,6 +383,38 @@ k_adj_main(Grid g, DevParams P, const double* __restrict__ u, const double* __re
   }
 }
 
+// Per interior vertex: the adjoint of the shift through the advection sums,
+// sum_n lvbar_n dlv_n/dbeta^a = lidx_a sum_n adv_n beta dt wbar_n L_a f_n,
+// added to the direct adjoint (the upwind side of the linearisation point).
+__global__ void __launch_bounds__(kThreads)
+k_adj_advbeta(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ wbar,
+              double* __restrict__ direct, double beta_dt) {
+  const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * g.nblocks) return;
+  const int b = (int)(t / npts);
+  int i, j, k;
+  interior_of(g, t % npts, i, j, k);
+  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  const int64_t nv = g.nvol;
+  const double* U = u + (int64_t)b * NVAR * nv;
+  const double* WB = wbar + (int64_t)b * NVAR * nv + p;
+  const FdScale& F = P.fd[b];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const bool left = U[(int64_t)(Z4C_BETAX + a) * nv + p] < 0;
+    double acc = 0.;
+#pragma unroll 2
+    for (int n = 0; n < NVAR; ++n) {
+      const double lb = ad::adv_coef(P.p, n) * beta_dt * WB[(int64_t)n * nv];
+      if (lb == 0.) continue;
+      Fld<double> f{U + (int64_t)n * nv};
+      acc += lb * st_lop(f, p, g.s[a], left);
+    }
+    direct[(int64_t)b * NVAR * nv + (int64_t)(Z4C_BETAX + a) * nv + p] += acc * F.lidx[a];
+  }
+}
+
 // Per interior vertex: the reverse of the Ricci part (ricci_local_adj) given
 // the Ricci-sum adjoints; adds to the channels and the direct adjoint.
 __global__ void __launch_bounds__(kThreads)
@@ -410,14 +434,14 @@ k_adj_ricci(Grid g, DevParams P, const double* __restrict__ u, const double* __r
   const double* SD = sd + (int64_t)b * kSdComponents * nv;
   RhsLocal<double> v;
   gather_rhs<double, kGatherRicci>(g, P.fd[b], U, SD, nullptr, nullptr, p, v);
-  double Rsb[6];
-  const double* R = rsb + (int64_t)b * 6 * npts + l;
-  #pragma unroll
+  double Rsb[6], cb[27];
+  const double* R = rsb + (int64_t)b * kNRsb * npts + l;
   for (int q = 0; q < 6; ++q) Rsb[q] = R[(int64_t)q * npts];
+  for (int q = 0; q < 27; ++q) cb[q] = R[(int64_t)(6 + q) * npts];
   RhsLocal<double> vb;
   #pragma unroll
   for (int q = 0; q < RhsLocal<double>::N; ++q) vb.data()[q] = 0.;
-  ad::ricci_local_adj(P.p, v, Rsb, vb);
+  ad::ricci_local_adj(P.p, v, Rsb, vb, cb);
   double* C = chan + (int64_t)b * kNChan * npts + l;
   #pragma unroll
   for (int a = 0; a < 3; ++a) C[(int64_t)(kChSd + a) * npts] += vb.dchi[a];
@@ -487,102 +511,101 @@ k_adj_sdbar(Grid g, DevParams P, const double* __restrict__ chan, double* __rest
 // Adjoint of the stage input u at every vertex of every block: the direct
 // adjoint (interior) plus the transposed stencils of every channel, the
 // Kreiss-Oliger terms and the upwind advection.  One thread per (block,
-// variable, vertex).
+// vertex) for all 22 variables: along each axis the interior points p that
+// reach the vertex form one range of offsets, clamped once, and the weights
+// that depend on p only (upwind side, shift, Kreiss-Oliger) are shared by
+// the variables.
 __global__ void __launch_bounds__(kThreads)
 k_adj_gather(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ wbar,
              const double* __restrict__ direct, const double* __restrict__ chan,
              const double* __restrict__ sdbar, double* __restrict__ ubar, double beta_dt) {
   const int64_t nv = g.nvol;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nv * NVAR * g.nblocks) return;
+  if (t >= nv * g.nblocks) return;
   const int64_t q = t % nv;
-  const int n = (int)((t / nv) % NVAR);
-  const int b = (int)(t / (nv * NVAR));
-  const int i = (int)(q % g.nn[0]), j = (int)((q / g.nn[0]) % g.nn[1]),
-            k = (int)(q / ((int64_t)g.nn[0] * g.nn[1]));
-  const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
+  const int b = (int)(t / nv);
+  const int ijk[3] = {(int)(q % g.nn[0]), (int)((q / g.nn[0]) % g.nn[1]),
+                      (int)(q / ((int64_t)g.nn[0] * g.nn[1]))};
+  const int n0 = g.nx[0] + 1, n1 = g.nx[1] + 1;
+  const int64_t npts = (int64_t)n0 * n1 * (g.nx[2] + 1);
+  const int64_t ls[3] = {1, n0, (int64_t)n0 * n1};
+  bool inA[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) inA[a] = ijk[a] >= NG && ijk[a] <= NG + g.nx[a];
+  const int64_t boff = (int64_t)b * NVAR * nv;
   const double* C = chan + (int64_t)b * kNChan * npts;
   const FdScale& F = P.fd[b];
-  const int ijk[3] = {i, j, k};
-  double acc = 0.;
-  if (is_interior(g, i, j, k)) acc = direct[((int64_t)b * NVAR + n) * nv + q];
-  // 1-D transposed stencils along axis a over an interior channel
-  auto line_d1 = [&](const double* ch, int a) {
-    double s = 0.;
+  double acc[NVAR];
+  const bool interior = inA[0] && inA[1] && inA[2];
 #pragma unroll
-    for (int o = -3; o <= 3; ++o) {
-      if (o == 0) continue;
-      int pp[3] = {i, j, k};
-      pp[a] -= o;
-      if (is_interior(g, pp[0], pp[1], pp[2]))
-        s += w_d1(o) * ch[interior_index(g, pp[0], pp[1], pp[2])];
-    }
-    return s;
-  };
-  auto line_d2 = [&](const double* ch, int a) {
-    double s = 0.;
+  for (int n = 0; n < NVAR; ++n) acc[n] = interior ? direct[boff + (int64_t)n * nv + q] : 0.;
+  double adv[NVAR];
 #pragma unroll
-    for (int o = -3; o <= 3; ++o) {
-      int pp[3] = {i, j, k};
-      pp[a] -= o;
-      if (is_interior(g, pp[0], pp[1], pp[2]))
-        s += w_d2(o) * ch[interior_index(g, pp[0], pp[1], pp[2])];
-    }
-    return s;
-  };
-  int slot = -1;
-  for (int s = 0; s < 11; ++s)
-    if (sd_field_var(s) == n) slot = s;
-  if (slot >= 0) {
-    // D_dir^T of the stored first derivatives' adjoints (their regions)
-    for (int dir = 0; dir < 3; ++dir) {
-      const double* sb = sdbar + ((int64_t)b * kSdComponents + slot * 3 + dir) * nv;
-      double s = 0.;
+  for (int n = 0; n < NVAR; ++n) adv[n] = ad::adv_coef(P.p, n);
 #pragma unroll
-      for (int o = -3; o <= 3; ++o) {
-        if (o == 0) continue;
-        int pp[3] = {i, j, k};
-        pp[dir] -= o;
-        if (in_sd_region(g, dir, pp[0], pp[1], pp[2]))
-          s += w_d1(o) * sb[((int64_t)pp[2] * g.nn[1] + pp[1]) * g.nn[0] + pp[0]];
-      }
-      acc += s * F.cidx1[dir];
-    }
-    // Dxx^T of the diagonal second derivatives
-    for (int a = 0; a < 3; ++a)
-      acc += line_d2(C + (int64_t)(kChDd + slot * 6 + ad::sid(a, a)) * npts, a) * F.cidx2[a];
-  }
-  int ch1 = -1;  // centred first derivatives of Gamma^c, Khat, Theta
-  if (n >= Z4C_GAMX && n <= Z4C_GAMZ) ch1 = kChGam + (n - Z4C_GAMX);
-  if (n == Z4C_KHAT) ch1 = kChKhat;
-  if (n == Z4C_THETA) ch1 = kChTheta;
-  if (ch1 >= 0)
-    for (int a = 0; a < 3; ++a) {
-      const int c = (ch1 >= kChKhat) ? ch1 + a : kChGam + a * 3 + (n - Z4C_GAMX);
-      acc += line_d1(C + (int64_t)c * npts, a) * F.cidx1[a];
-    }
-  // Kreiss-Oliger and advection from the right-hand-side adjoint beta dt wbar
-  const double* WB = wbar + ((int64_t)b * NVAR + n) * nv;
-  const double* BETA = u + ((int64_t)b * NVAR + Z4C_BETAX) * nv;
-  const double adv = ad::adv_coef(P.p, n);
   for (int a = 0; a < 3; ++a) {
-    double sko = 0., sadv = 0.;
+    if (!(inA[(a + 1) % 3] && inA[(a + 2) % 3])) continue;
+    // interior points p = q - o e_a: NG <= ijk[a] - o <= NG + nx[a]
+    const int olo = max(-4, ijk[a] - NG - g.nx[a]), ohi = min(4, ijk[a] - NG);
+    int64_t l0 = 0;  // interior index of q with coordinate a at NG
+#pragma unroll
+    for (int c = 0; c < 3; ++c) l0 += (c == a ? 0 : (int64_t)(ijk[c] - NG)) * ls[c];
+    const double ck = F.cidxd[a] * P.p.diss, cl = F.lidx[a], c1 = F.cidx1[a], c2 = F.cidx2[a];
+#pragma unroll
     for (int o = -4; o <= 4; ++o) {
-      int pp[3] = {ijk[0], ijk[1], ijk[2]};
-      pp[a] -= o;
-      if (!is_interior(g, pp[0], pp[1], pp[2])) continue;
-      const int64_t pq = ((int64_t)pp[2] * g.nn[1] + pp[1]) * g.nn[0] + pp[0];
-      const double rb = beta_dt * WB[pq];
-      sko += w_ko(o) * rb;
-      if (adv != 0.) {
-        const double be = BETA[(int64_t)a * nv + pq];
-        const double w = w_lop(be < 0, o);
-        if (w != 0.) sadv += w * be * rb;
+      if (o < olo || o > ohi) continue;
+      const int64_t pq = q - (int64_t)o * g.s[a];
+      const int64_t lp = l0 + (int64_t)(ijk[a] - o - NG) * ls[a];
+      const double be = u[boff + (int64_t)(Z4C_BETAX + a) * nv + pq];
+      const double wko = w_ko(o) * ck;
+      const double wad = w_lop(be < 0, o) * be * cl;
+#pragma unroll
+      for (int n = 0; n < NVAR; ++n) {
+        const double rb = beta_dt * wbar[boff + (int64_t)n * nv + pq];
+        acc[n] += (wko + wad * adv[n]) * rb;
+      }
+      if (o >= -3 && o <= 3) {
+        const double w2 = w_d2(o) * c2;
+#pragma unroll
+        for (int slot = 0; slot < 11; ++slot)
+          acc[sd_field_var(slot)] += w2 * C[(int64_t)(kChDd + slot * 6 + ad::sid(a, a)) * npts + lp];
+        if (o != 0) {
+          const double w1 = w_d1(o) * c1;
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            acc[Z4C_GAMX + c] += w1 * C[(int64_t)(kChGam + a * 3 + c) * npts + lp];
+          acc[Z4C_KHAT] += w1 * C[(int64_t)(kChKhat + a) * npts + lp];
+          acc[Z4C_THETA] += w1 * C[(int64_t)(kChTheta + a) * npts + lp];
+        }
       }
     }
-    acc += sko * F.cidxd[a] * P.p.diss + sadv * adv * F.lidx[a];
   }
-  ubar[((int64_t)b * NVAR + n) * nv + q] = acc;
+  // D_dir^T of the stored first derivatives' adjoints over their regions
+#pragma unroll
+  for (int dir = 0; dir < 3; ++dir) {
+    const int ex = (dir >= 1) ? 3 : 0, ey = (dir == 2) ? 3 : 0;
+    const int lo[3] = {NG - ex, NG - ey, NG};
+    const int hi[3] = {NG + g.nx[0] + ex, NG + g.nx[1] + ey, NG + g.nx[2]};
+    bool ok = true;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      if (c != dir) ok = ok && ijk[c] >= lo[c] && ijk[c] <= hi[c];
+    if (!ok) continue;
+    const int olo = max(-3, ijk[dir] - hi[dir]), ohi = min(3, ijk[dir] - lo[dir]);
+    const double c1 = F.cidx1[dir];
+#pragma unroll
+    for (int o = -3; o <= 3; ++o) {
+      if (o == 0 || o < olo || o > ohi) continue;
+      const int64_t pq = q - (int64_t)o * g.s[dir];
+      const double w = w_d1(o) * c1;
+#pragma unroll
+      for (int slot = 0; slot < 11; ++slot)
+        acc[sd_field_var(slot)] +=
+            w * sdbar[((int64_t)b * kSdComponents + slot * 3 + dir) * nv + pq];
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < NVAR; ++n) ubar[boff + (int64_t)n * nv + q] = acc[n];
 }
 
 // AlgConstr^T at every vertex: ubar (adjoint after) -> adjoint before, at the
@@ -1207,13 +1230,14 @@ int adj_step(z4c_ctx* c, double dt, const double* u) {
     k_accumulate<<<1, 256, 0, c->stream>>>(A->part, nthr, A->pacc);
     ALAUNCH("adjoint main");
     k_adj_ricci<<<nthr, kThreads, 0, c->stream>>>(g, P, us, c->sd, A->rsb, A->direct, A->chan);
+    k_adj_advbeta<<<nthr, kThreads, 0, c->stream>>>(g, P, us, A->wbar, A->direct, W.beta_dt);
     const int64_t creg = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7) * (g.nx[2] + 1);
     k_adj_sdbar<<<dim3(div_up(creg, kThreads), kSdComponents, g.nblocks), kThreads, 0, c->stream>>>(
         g, P, A->chan, A->sdbar);
-    k_adj_gather<<<div_up(g.nvol * NVAR * g.nblocks, kThreads), kThreads, 0, c->stream>>>(
+    k_adj_gather<<<div_up(g.nvol * g.nblocks, kThreads), kThreads, 0, c->stream>>>(
         g, P, us, A->wbar, A->direct, A->chan, A->sdbar, A->adj, W.beta_dt);
     ALAUNCH("adjoint gather");
-    add_kernel_launches(5);
+    add_kernel_launches(6);
   }
   return Z4C_OK;
 }
@@ -1360,7 +1384,7 @@ int z4c_adj_setup(z4c_ctx* c) {
       {&A->wbar, reg}, {&A->direct, reg}, {&A->us, reg}, {&A->w, reg}, {&A->u1, reg},
       {&A->sdd, sizeof(double) * kSdComponents * g.nvol * g.nblocks},
       {&A->sdbar, sizeof(double) * kSdComponents * g.nvol * g.nblocks},
-      {&A->chan, sizeof(double) * kNChan * npts}, {&A->rsb, sizeof(double) * 6 * npts},
+      {&A->chan, sizeof(double) * kNChan * npts}, {&A->rsb, sizeof(double) * kNRsb * npts},
       {&A->hchan, sizeof(double) * kNHChan * npts}, {&A->part, sizeof(double) * 2 * A->npart},
       {&A->pacc, sizeof(double) * 2}};
   for (int s = 0; s < 4; ++s) bufs.push_back({&A->upre[s], reg});
