@@ -89,6 +89,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint-step measurements of the headline line")
     ap.add_argument("--no-smr", action="store_true",
                     help="skip the refined binary-puncture measurement of the headline line")
     ap.add_argument("--nb", type=int, default=8,
@@ -303,6 +305,79 @@ def psi4_diagnostics(Z, ctx, stream, npts, nblocks, with_cpu):
         per_block = time.perf_counter() - t0
         out["cpu_port_ms_all_blocks"] = per_block * nblocks * 1e3
         out["cpu_sample"] = "C oracle Z4cWeyl on one MeshBlock, single thread, times the block count"
+    return out
+
+
+def time_on(stream, fn, reps):
+    """Device time of fn() per call: CUDA events on the context's stream
+    around reps calls, after one untimed call."""
+    import torch
+    with torch.cuda.stream(stream):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    with torch.cuda.stream(stream):
+        for _ in range(reps):
+            fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+# configs[3]: the gauge wave of configs[0] on 64^3 cells in one periodic
+# MeshBlock, A = 0.05, seeded U(-1e-6, 1e-6) on the conformal metric, 100 rk4
+# steps, objective = H-norm after the last step; eps_floor < 0 keeps
+# AlgConstr's determinant normalisation on every vertex (differentiable)
+ADJ_PARAMS = dict(lapse_harmonic=1.0, lapse_harmonicf=0.0, lapse_oplog=0.0, lapse_advect=0.0,
+                  shift_Gamma=0.0, shift_eta=0.0, shift_advect=0.0, diss=0.02,
+                  damp_kappa1=0.02, r_max_con=1e300, eps_floor=-1.0)
+ADJ_STEPS, ADJ_SNAPSHOTS = 100, 9
+
+
+def adjoint_diagnostics(Z, ID, head_ctx, head_stream, head_dt):
+    """The differentiated step: one adjoint step (recomputation of the step
+    included) against one forward step, on the configs[3] block and on the
+    headline mesh, and the revolve-checkpointed gradient of configs[3]."""
+    import torch
+    out = {}
+    mesh = Z.Mesh((1, 1, 1), (64, 64, 64), (-0.5,) * 3, (0.5,) * 3, "periodic")
+    ctx = Z.Z4c(mesh, Z.default_params(**ADJ_PARAMS), "rk4")
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.adj_setup()
+    ID.load_adm(ctx, ID.gauge_wave1(mesh, amplitude=0.05))
+    u = ctx.download(Z.REG_U)
+    rng = np.random.default_rng(2024)
+    u[:, Z.GXX:Z.GZZ + 1] += rng.uniform(-1e-6, 1e-6, size=u[:, Z.GXX:Z.GZZ + 1].shape)
+    ctx.upload(Z.REG_U, u)
+    ctx.init_finalize()
+    u0 = ctx.download(Z.REG_U)
+    dt = 0.25 / 64
+    fwd = time_on(stream, lambda: ctx.evolve(dt, 1), 20)
+    ctx.upload(Z.REG_U, u0)
+    adj = time_on(stream, lambda: ctx.adj_step(dt), 10)
+    ctx.upload(Z.REG_U, u0)
+    with torch.cuda.stream(stream):
+        J, pb, st = ctx.gradient(dt, ADJ_STEPS, ADJ_SNAPSHOTS)
+    torch.cuda.synchronize()
+    out["configs3"] = {
+        "workload": "gauge wave A=0.05 + U(-1e-6,1e-6) on g~, 64^3 cells, one periodic MeshBlock, "
+                    "rk4, 100 steps, objective vol*sum H^2 after the last step",
+        "forward_step_ms": fwd, "adjoint_step_ms": adj, "adjoint_over_forward": adj / fwd,
+        "gradient_seconds": st["seconds"], "gradient_forward_steps": st["forward_steps"],
+        "gradient_adjoint_steps": st["adjoint_steps"], "snapshots": ADJ_SNAPSHOTS,
+        "objective": J, "d_shift_eta": float(pb[0]), "d_damp_kappa1": float(pb[1])}
+    ctx.close()
+    # the headline mesh (512 MeshBlocks, outflow faces)
+    head_ctx.adj_setup()
+    fwd = time_on(head_stream, lambda: head_ctx.evolve(head_dt, 1), 5)
+    adj = time_on(head_stream, lambda: head_ctx.adj_step(head_dt), 3)
+    out["puncture_512"] = {"forward_step_ms": fwd, "adjoint_step_ms": adj,
+                           "adjoint_over_forward": adj / fwd}
+    out["note"] = ("adjoint_step_ms: the step recomputed stage by stage from its start state, then "
+                   "the reverse of its four stages (AlgConstr, exchange, boundary conditions, "
+                   "stage algebra, right-hand side); device time, CUDA events")
     return out
 
 
@@ -562,6 +637,11 @@ def main():
     psi4 = psi4_diagnostics(Z, ctx, stream, npts, mesh.nblocks, rank == 0 and world == 1
                             and not args.no_cpu_baseline)
 
+    # ---- differentiated step (N = 1) -----------------------------------------
+    adjoint = None
+    if world == 1 and not args.no_adjoint:
+        adjoint = adjoint_diagnostics(Z, ID, ctx, stream, dt)
+
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -618,6 +698,7 @@ def main():
         "gpu_launches": launches,
         "clocks": clocks,
         "psi4": psi4,
+        "adjoint": adjoint,
     }
     ctx.close()
     if world == 1 and not args.no_smr:

@@ -1510,5 +1510,38 @@ Z4C_HD void ham_local_adj(const z4c_params_t& opt, const HLocal<double>& v, doub
   vb.chi -= psi4 * psi4 * psi4b;
 }
 
+// ---- ADMToZ4c, pointwise part (adm_z4c.cpp:56-163) ------------------------
+// in: the ADM metric G and curvature K at a vertex (six stored components
+// each); out: chi, g~ (6), Khat, A~ (6) and the inverse conformal metric
+// guu (6) whose derivatives give Gamma~ (chi_psi_power = -4: chi =
+// cbrt(1 / det G)).  The lapse and shift are copied.
+template <class T>
+Z4C_HD T ad_cbrt(const T& x);
+template <>
+Z4C_HD double ad_cbrt(const double& x) { return cbrt(x); }
+template <>
+Z4C_HD Dual ad_cbrt(const Dual& x) {
+  const double c = cbrt(x.v);
+  return Dual(c, x.d * c / (3.0 * x.v));
+}
+template <class T>
+Z4C_HD void adm_to_z4c_local(const T G[6], const T Kd[6], T* chi, T g[6], T* Khat, T A[6],
+                             T guu[6]) {
+  const T detg = det3s(G);
+  const T oopsi4 = ad_cbrt(T(1.0) / detg);
+  *chi = oopsi4;
+  T Kt[6];
+  for (int c = 0; c < 6; ++c) {
+    g[c] = oopsi4 * G[c];
+    Kt[c] = oopsi4 * Kd[c];
+  }
+  const T detg2 = det3s(g);
+  const T kh = (T(1.0) / detg2) * trace_adj(g, Kt);
+  *Khat = kh;
+  for (int c = 0; c < 6; ++c) A[c] = Kt[c] - (1. / 3.) * kh * g[c];
+  const T detg3 = det3s(g);
+  inv3s(T(1.0) / detg3, g, guu);
+}
+
 }  // namespace ad
 }  // namespace z4c

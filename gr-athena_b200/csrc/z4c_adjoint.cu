@@ -1022,6 +1022,106 @@ k_ham_gather(Grid g, DevParams P, const double* __restrict__ hchan, double* __re
   ubar[((int64_t)b * NVAR + n) * nv + q] += acc;
 }
 
+// ---- adjoint of the initial data (ADMToZ4c + FinalizeZ4cADMGhosts) ---------
+
+// AlgConstr^T at the ghost vertices only (the ghost pass of
+// FinalizeZ4cADMGhosts); interior adjoints pass through.
+__global__ void __launch_bounds__(kThreads)
+k_adj_alg_ghosts(Grid g, DevParams P, const double* __restrict__ upre, double* __restrict__ ubar) {
+  const int64_t nv = g.nvol;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nv * g.nblocks) return;
+  const int b = (int)(t / nv);
+  const int64_t q = t % nv;
+  const int i = (int)(q % g.nn[0]), j = (int)((q / g.nn[0]) % g.nn[1]),
+            k = (int)(q / ((int64_t)g.nn[0] * g.nn[1]));
+  if (is_interior(g, i, j, k)) return;
+  double uu[NVAR], ub[NVAR];
+  const double* UP = upre + (int64_t)b * NVAR * nv + q;
+  double* UB = ubar + (int64_t)b * NVAR * nv + q;
+  for (int n = 0; n < NVAR; ++n) {
+    uu[n] = UP[(int64_t)n * nv];
+    ub[n] = UB[(int64_t)n * nv];
+  }
+  ad::alg_constr_adj(P.p, uu, ub);
+  for (int n = 0; n < NVAR; ++n) UB[(int64_t)n * nv] = ub[n];
+}
+
+// Adjoint of the inverse conformal metric through Gamma~^a = -sum_c
+// D_c g~^{ca} on the interior (adm_z4c.cpp:165-176): gub[s] at every vertex,
+// s the stored pair of g~^{ca}.
+__global__ void __launch_bounds__(kThreads)
+k_adj_adm_gam(Grid g, DevParams P, const double* __restrict__ ubar, double* __restrict__ gub) {
+  const int64_t nv = g.nvol;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nv * g.nblocks) return;
+  const int b = (int)(t / nv);
+  const int64_t q = t % nv;
+  const int ijk[3] = {(int)(q % g.nn[0]), (int)((q / g.nn[0]) % g.nn[1]),
+                      (int)(q / ((int64_t)g.nn[0] * g.nn[1]))};
+  const double* UB = ubar + (int64_t)b * NVAR * nv;
+  const FdScale& F = P.fd[b];
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int c = 0; c < 3; ++c) {
+    bool ok = true;
+    for (int e = 0; e < 3; ++e)
+      if (e != c) ok = ok && ijk[e] >= NG && ijk[e] <= NG + g.nx[e];
+    if (!ok) continue;
+    const int olo = max(-3, ijk[c] - NG - g.nx[c]), ohi = min(3, ijk[c] - NG);
+#pragma unroll
+    for (int o = -3; o <= 3; ++o) {
+      if (o == 0 || o < olo || o > ohi) continue;
+      const int64_t pq = q - (int64_t)o * g.s[c];
+      const double w = -w_d1(o) * F.cidx1[c];
+      for (int a = 0; a < 3; ++a) acc[ad::sid(c, a)] += w * UB[(int64_t)(Z4C_GAMX + a) * nv + pq];
+    }
+  }
+  for (int s = 0; s < 6; ++s) gub[((int64_t)b * 6 + s) * nv + q] = acc[s];
+}
+
+// Reverse of the pointwise ADMToZ4c at every vertex: the lapse and shift
+// through their copies, the metric and curvature through 12 forward-mode
+// directions of adm_to_z4c_local.
+__global__ void __launch_bounds__(kThreads)
+k_adj_adm_pt(Grid g, const double* __restrict__ adm, const double* __restrict__ ubar,
+             const double* __restrict__ gub, double* __restrict__ admbar) {
+  const int64_t nv = g.nvol;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nv * g.nblocks) return;
+  const int b = (int)(t / nv);
+  const int64_t q = t % nv;
+  const double* A = adm + (int64_t)b * Z4C_NADM * nv + q;
+  const double* UB = ubar + (int64_t)b * NVAR * nv + q;
+  double* AB = admbar + (int64_t)b * Z4C_NADM * nv + q;
+  AB[(int64_t)Z4C_ADM_ALPHA * nv] = UB[(int64_t)Z4C_ALPHA * nv];
+  for (int a = 0; a < 3; ++a) AB[(int64_t)(Z4C_ADM_BETAX + a) * nv] = UB[(int64_t)(Z4C_BETAX + a) * nv];
+  AB[(int64_t)Z4C_ADM_PSI4 * nv] = 0.;
+  double G[6], K[6], gb[6];
+  for (int c = 0; c < 6; ++c) {
+    G[c] = A[(int64_t)(Z4C_ADM_GXX + c) * nv];
+    K[c] = A[(int64_t)(Z4C_ADM_KXX + c) * nv];
+    gb[c] = gub[((int64_t)b * 6 + c) * nv + q];
+  }
+  double ob_chi = UB[(int64_t)Z4C_CHI * nv], ob_kh = UB[(int64_t)Z4C_KHAT * nv];
+  double ob_g[6], ob_a[6];
+  for (int c = 0; c < 6; ++c) {
+    ob_g[c] = UB[(int64_t)(Z4C_GXX + c) * nv];
+    ob_a[c] = UB[(int64_t)(Z4C_AXX + c) * nv];
+  }
+  for (int dir = 0; dir < 12; ++dir) {
+    Dual Gd[6], Kd[6];
+    for (int c = 0; c < 6; ++c) {
+      Gd[c] = Dual(G[c], dir == c ? 1. : 0.);
+      Kd[c] = Dual(K[c], dir == 6 + c ? 1. : 0.);
+    }
+    Dual chi, gt[6], kh, At[6], guu[6];
+    ad::adm_to_z4c_local(Gd, Kd, &chi, gt, &kh, At, guu);
+    double s = ob_chi * chi.d + ob_kh * kh.d;
+    for (int c = 0; c < 6; ++c) s += ob_g[c] * gt[c].d + ob_a[c] * At[c].d + gb[c] * guu[c].d;
+    AB[(int64_t)((dir < 6 ? Z4C_ADM_GXX : Z4C_ADM_KXX - 6) + dir) * nv] = s;
+  }
+}
+
 // acc[0..1] += the sums of part[2 i], part[2 i + 1] over i < n, in a fixed
 // order (one CTA of 256 threads)
 __global__ void k_accumulate(const double* __restrict__ part, int n, double* __restrict__ acc) {
@@ -1072,13 +1172,16 @@ struct AdjState {
   double* part = nullptr;   // per-CTA partial sums
   int npart = 0;
   double* pacc = nullptr;   // device accumulators of the shift_eta, damp_kappa1 adjoints
+  double* admbar = nullptr; // adjoint of the ADM register (Z4C_REG_ADM_ADJ)
+  double* gub = nullptr;    // adjoint of the inverse conformal metric of ADMToZ4c
   std::vector<double*> snaps;  // revolve snapshots
 };
 
 void adj_free(AdjState* a) {
   if (!a) return;
   for (double* p : {a->tan, a->tan1, a->tanw, a->sdd, a->adj, a->adj1, a->wbar, a->direct, a->us,
-                    a->w, a->u1, a->chan, a->rsb, a->sdbar, a->hchan, a->part, a->pacc})
+                    a->w, a->u1, a->chan, a->rsb, a->sdbar, a->hchan, a->part, a->pacc,
+                    a->admbar, a->gub})
     if (p) cudaFree(p);
   for (double* p : a->upre)
     if (p) cudaFree(p);
@@ -1386,7 +1489,9 @@ int z4c_adj_setup(z4c_ctx* c) {
       {&A->sdbar, sizeof(double) * kSdComponents * g.nvol * g.nblocks},
       {&A->chan, sizeof(double) * kNChan * npts}, {&A->rsb, sizeof(double) * kNRsb * npts},
       {&A->hchan, sizeof(double) * kNHChan * npts}, {&A->part, sizeof(double) * 2 * A->npart},
-      {&A->pacc, sizeof(double) * 2}};
+      {&A->pacc, sizeof(double) * 2},
+      {&A->admbar, sizeof(double) * Z4C_NADM * g.nvol * g.nblocks},
+      {&A->gub, sizeof(double) * 6 * g.nvol * g.nblocks}};
   for (int s = 0; s < 4; ++s) bufs.push_back({&A->upre[s], reg});
   for (auto& b : bufs) {
     if (cudaMalloc((void**)b.p, b.bytes) != cudaSuccess) {
@@ -1407,6 +1512,7 @@ int z4c_adj_setup(z4c_ctx* c) {
   c->adj = A;
   c->reg[Z4C_REG_TAN] = A->tan;
   c->reg[Z4C_REG_ADJ] = A->adj;
+  c->reg[Z4C_REG_ADM_ADJ] = A->admbar;
   return Z4C_OK;
 }
 
@@ -1552,5 +1658,39 @@ extern "C" int z4c_adj_gradient(z4c_ctx* c, double dt, int nsteps, int nsnap, do
     stats[2] = ms * 1e-3;
     stats[3] = (double)sch.C(nsteps, S);
   }
+  return Z4C_OK;
+}
+
+extern "C" int z4c_adj_adm_to_z4c(z4c_ctx* c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  z4c::AdjState* A = c->adj;
+  const Grid& g = c->g;
+  const DevParams P = c->dev();
+  const size_t bytes = sizeof(double) * A->reg_elems;
+  const int nthr_all = div_up(g.nvol * g.nblocks, kThreads);
+  const int64_t npts = npts_of(g);
+  // recompute: x1 = the pointwise map and Gamma~ (A->us), x2 = AlgConstr(x1)
+  // (A->w), x3 = the ghost fill of x2 (A->upre[0])
+  launch_adm_to_z4c(g, P, c->reg[Z4C_REG_ADM], A->us, c->guu, 0, g.nblocks, c->stream, 0);
+  ALAUNCH("adm_to_z4c");
+  ACUDA(cudaMemcpyAsync(A->w, A->us, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  launch_alg_constr(g, P, A->w, 0, g.nblocks, c->stream);
+  launch_exchange(g, P, A->w, A->upre[0], c->nbr, 0, c->stream);
+  launch_physical_bcs(g, A->upre[0], NVAR, c->stream);
+  ALAUNCH("ghost fill");
+  // reverse: AlgConstr on the ghosts, the ghost fill, AlgConstr, the map
+  k_adj_alg_ghosts<<<nthr_all, kThreads, 0, c->stream>>>(g, P, A->upre[0], A->adj);
+  adj_physical_bcs(g, A->adj, c->stream);
+  ACUDA(cudaMemsetAsync(A->wbar, 0, bytes, c->stream));
+  k_adj_exchange<<<div_up(npts * g.nblocks, kThreads), kThreads, 0, c->stream>>>(g, A->adj,
+                                                                                A->wbar);
+  k_adj_alg<<<nthr_all, kThreads, 0, c->stream>>>(g, P, A->us, A->wbar);
+  k_adj_adm_gam<<<nthr_all, kThreads, 0, c->stream>>>(g, P, A->wbar, A->gub);
+  k_adj_adm_pt<<<nthr_all, kThreads, 0, c->stream>>>(g, c->reg[Z4C_REG_ADM], A->wbar, A->gub,
+                                                     A->admbar);
+  ALAUNCH("initial-data adjoint");
+  add_kernel_launches(5);
+  ACUDA(cudaMemcpyAsync(A->adj, A->wbar, bytes, cudaMemcpyDeviceToDevice, c->stream));
   return Z4C_OK;
 }

@@ -98,6 +98,7 @@ namespace {
 int reg_nvar_(int reg) {
   switch (reg) {
     case Z4C_REG_ADM: return Z4C_NADM;
+    case Z4C_REG_ADM_ADJ: return Z4C_NADM;
     case Z4C_REG_CON: return Z4C_NCON;
     case Z4C_REG_WEYL: return Z4C_NWEYL;
     default: return (reg >= 0 && reg < Z4C_NREG) ? Z4C_NVAR : -1;
@@ -274,7 +275,7 @@ int run_stage_body(z4c_ctx* c, int stage, double dt) {
 void free_ctx(z4c_ctx* c) {
   if (c->graph) cudaGraphExecDestroy(c->graph);
   // the tangent and adjoint registers belong to the adjoint buffers
-  c->reg[Z4C_REG_TAN] = c->reg[Z4C_REG_ADJ] = nullptr;
+  c->reg[Z4C_REG_TAN] = c->reg[Z4C_REG_ADJ] = c->reg[Z4C_REG_ADM_ADJ] = nullptr;
   for (auto& r : c->reg)
     if (r) cudaFree(r);
   for (void* p : {(void*)c->un, (void*)c->guu, (void*)c->sd, (void*)c->rsum, (void*)c->lv, (void*)c->xf, (void*)c->xv, (void*)c->dxd, (void*)c->fd,

@@ -1671,7 +1671,7 @@ void launch_z4c_to_adm(const Grid& g, const DevParams& P, const double* u, doubl
 }
 
 void launch_adm_to_z4c(const Grid& g, const DevParams& P, const double* adm, double* u,
-                       double* guu_scratch, int block0, int nblk, cudaStream_t st) {
+                       double* guu_scratch, int block0, int nblk, cudaStream_t st, int alg) {
   const int64_t n = g.nvol * nblk;
   // guu_scratch is indexed by absolute block number
   COUNTED
@@ -1680,6 +1680,7 @@ void launch_adm_to_z4c(const Grid& g, const DevParams& P, const double* adm, dou
   COUNTED
   k_adm_to_z4c_gam<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, guu_scratch, u,
                                                                        block0, nblk);
+  if (!alg) return;
   COUNTED
   (has_fixed_geometry(g) ? k_alg_constr<kFixedNX> : k_alg_constr<0>)<<<
       div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, block0, nblk, 0);

@@ -129,8 +129,9 @@ void launch_add_rhs(const Grid& g, const double* rhs, double wght, double* out, 
                     int nblk, cudaStream_t st);
 void launch_z4c_to_adm(const Grid& g, const DevParams& P, const double* u, double* adm,
                        int block0, int nblk, cudaStream_t st, int ghosts_only = 0);
+// alg = 0 leaves out the final AlgConstr (the adjoint's recomputation)
 void launch_adm_to_z4c(const Grid& g, const DevParams& P, const double* adm, double* u,
-                       double* guu_scratch, int block0, int nblk, cudaStream_t st);
+                       double* guu_scratch, int block0, int nblk, cudaStream_t st, int alg = 1);
 void launch_adm_constraints(const Grid& g, const DevParams& P, const double* adm,
                             const double* u, double* con, const double* xf, int block0,
                             int nblk, cudaStream_t st);

@@ -30,7 +30,7 @@ NVAR, NADM, NCON, NWEYL = 22, 17, 7, 2
  ADM_PSI4) = range(17)
 CON_C, CON_H, CON_M, CON_Z, CON_MX, CON_MY, CON_MZ = range(7)
 (REG_U, REG_U1, REG_RHS, REG_ADM, REG_CON, REG_W, REG_K1, REG_K2, REG_K3,
- REG_K4, REG_WEYL, REG_TAN, REG_ADJ) = range(13)
+ REG_K4, REG_WEYL, REG_TAN, REG_ADJ, REG_ADM_ADJ) = range(14)
 BC_PERIODIC, BC_OUTFLOW, BC_SOMMERFELD = 0, 1, 2
 BC_NAMES = {"periodic": BC_PERIODIC, "outflow": BC_OUTFLOW, "extrapolate_outflow": BC_OUTFLOW,
             "sommerfeld": BC_SOMMERFELD, "gr_sommerfeld": BC_SOMMERFELD}
@@ -56,7 +56,8 @@ EXPORTS = (
     "z4c_sphere_grid", "z4c_wave_add", "z4c_wave_points", "z4c_wave_decompose",
     "z4c_restart_info", "z4c_restart_text", "z4c_restart_read", "z4c_restart_write_host",
     "z4c_restart_load", "z4c_restart_save", "z4c_adj_setup", "z4c_tlm_step", "z4c_adj_step",
-    "z4c_adj_objective", "z4c_adj_objective_adj", "z4c_adj_params", "z4c_adj_gradient")
+    "z4c_adj_objective", "z4c_adj_objective_adj", "z4c_adj_params", "z4c_adj_gradient",
+    "z4c_adj_adm_to_z4c")
 
 
 class Z4cError(RuntimeError):
@@ -179,6 +180,7 @@ def lib():
         L.z4c_adj_objective.argtypes = [vp, ip, ip, dp, dp]
         L.z4c_adj_objective_adj.argtypes = [vp, ip, C.c_double]
         L.z4c_adj_params.argtypes = [vp, dp, ip]
+        L.z4c_adj_adm_to_z4c.argtypes = [vp]
         L.z4c_adj_gradient.argtypes = [vp, C.c_double, ip, ip, C.c_double, C.c_double, dp, dp,
                                        dp]
         L.z4c_kernel_launches.argtypes = []
@@ -749,6 +751,11 @@ class Z4c:
     def objective_adj(self, reg=REG_U, scale=1.0):
         """REG_ADJ += scale * dJ/du at register reg."""
         _check(lib().z4c_adj_objective_adj(self._h, reg, scale))
+
+    def adj_adm_to_z4c(self):
+        """REG_ADJ (adjoint of u after ADMToZ4c + init_finalize) -> REG_ADM_ADJ,
+        the adjoint of the ADM register's data."""
+        _check(lib().z4c_adj_adm_to_z4c(self._h))
 
     def adj_params(self, reset=False):
         """Accumulated adjoints of (shift_eta, damp_kappa1)."""

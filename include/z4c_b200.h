@@ -89,6 +89,8 @@ enum {
   Z4C_REG_WEYL,    /* storage.weyl (2 vars: Re psi4, Im psi4)       */
   Z4C_REG_TAN,     /* tangent of u (22 vars; after z4c_adj_setup)   */
   Z4C_REG_ADJ,     /* adjoint of u (22 vars; after z4c_adj_setup)   */
+  Z4C_REG_ADM_ADJ, /* adjoint of the ADM register (17 vars; after
+                      z4c_adj_setup)                                */
   Z4C_NREG
 };
 
@@ -456,6 +458,14 @@ int z4c_adj_step(z4c_ctx *ctx, double dt);
 int z4c_adj_objective(z4c_ctx *ctx, int reg, int reg_tan, double *J, double *Jdot);
 /* Z4C_REG_ADJ += scale * dJ/du at the state in reg. */
 int z4c_adj_objective_adj(z4c_ctx *ctx, int reg, double scale);
+/* Adjoint of the initial data: Z4C_REG_ADJ holds the adjoint of u after
+ * z4c_adm_to_z4c(ctx, Z4C_REG_ADM, Z4C_REG_U, -1) and z4c_init_finalize (the
+ * reference's ADMToZ4c, adm_z4c.cpp:46-192, and FinalizeZ4cADMGhosts); the
+ * ADM register holds the data that mapped; the adjoint of the ADM data is
+ * written to Z4C_REG_ADM_ADJ (the lapse and shift through their copies, the
+ * metric and extrinsic curvature through the conformal decomposition and
+ * Gamma~ = -d_b g~^{ba}).  Z4C_REG_ADJ is overwritten. */
+int z4c_adj_adm_to_z4c(z4c_ctx *ctx);
 /* The accumulated adjoints of {shift_eta, damp_kappa1}; reset != 0 zeroes
  * them afterwards. */
 int z4c_adj_params(z4c_ctx *ctx, double pbar[2], int reset);

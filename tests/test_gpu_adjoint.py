@@ -340,3 +340,110 @@ def test_configs3_gradient_against_differences_and_tangent_linear_runs():
     assert worst_fd <= 1e-6
     assert worst_tlm <= 1e-9
     ctx.close()
+
+
+# ---- the chain to the initial data (configs[4]'s gradient, on a uniform mesh) ----
+
+BL_Y, BL_Z = 0.13, 0.07  # the punctures sit off the x axis and off the vertices
+
+
+def bl_adm(Z, mesh, params, m1, m2, d):
+    """Brill-Lindquist data: masses m1, m2 at (+-d/2, +-0.13, +-0.07)."""
+    from z4c_b200 import initial_data as ID
+    return ID.punctures(mesh, params, masses=(m1, m2),
+                        centres=((0.5 * d, BL_Y, BL_Z), (-0.5 * d, -BL_Y, -BL_Z)))
+
+
+@pytest.mark.parametrize("bc", ["periodic", "outflow"])
+def test_initial_data_adjoint_matches_differences(bc):
+    """The adjoint of ADMToZ4c + the initial ghost finalisation against
+    central differences of that map along a smooth direction in the ADM
+    data.  On the outflow mesh the weights ub leave out the ghosts, where
+    the extrapolation's amplification of rounding makes differences noise
+    (the transposed extrapolation is covered by the step's transpose test)."""
+    Z, mesh, ctx = make((2, 2, 1), 12, PUNC, lim=4.0, bc=bc)
+    params = Z.default_params(**PUNC)
+    adm = bl_adm(Z, mesh, params, 0.5, 0.5, 3.0)
+    rng = np.random.default_rng(9)
+    dirs = smooth_direction(Z, mesh, 11, amp=1e-2)[:, :17]
+    dirs[:, Z.ADM_PSI4] = 0.0
+
+    def u_of(a):
+        ctx.upload(Z.REG_ADM, a)
+        ctx.ADMToZ4c()
+        ctx.init_finalize()
+        return ctx.download(Z.REG_U)
+
+    u0 = u_of(adm)
+    ub = smooth_direction(Z, mesh, 12, amp=1.0) + 0.1 * rng.standard_normal(u0.shape)
+    if bc == "outflow":
+        interior = np.zeros_like(ub)
+        interior[:, :, 4:-4, 4:-4, 4:-4] = 1.0
+        ub *= interior
+    ctx.upload(Z.REG_ADM, adm)
+    ctx.upload(Z.REG_ADJ, ub)
+    ctx.adj_adm_to_z4c()
+    ab = ctx.download(Z.REG_ADM_ADJ)
+    h = 1e-4
+    fd = dot(ub, (u_of(adm + h * dirs) - u_of(adm - h * dirs))) / (2 * h)
+    ad = dot(ab, dirs)
+    print(f"initial data: adjoint {ad:.12e}, differences {fd:.12e}")
+    assert abs(fd - ad) <= 1e-7 * abs(fd)
+    ctx.close()
+
+
+def test_configs4_parameter_gradient_on_a_uniform_mesh():
+    """configs[4]'s gradient on a uniform mesh: the time-integrated H-norm
+    of a binary Brill-Lindquist evolution (outflow faces, 1+log and
+    Gamma-driver) with respect to the two masses, the separation and the
+    Gamma-driver eta, through the revolve-checkpointed adjoint, the adjoint
+    of ADMToZ4c and the derivative of the host-side initial data, against
+    central differences of the full forward run."""
+    Z, mesh, ctx = make((2, 2, 2), 12, PUNC, lim=4.0, bc="outflow")
+    params = Z.default_params(**PUNC)
+    theta = np.array([0.5, 0.45, 3.0])  # m1, m2, separation
+    dt = 0.25 * float(ctx.dx().min())
+    nsteps = 12
+
+    def run(th, eta=PUNC["shift_eta"]):
+        p = dict(PUNC, shift_eta=eta)
+        Zr, meshr, c = make((2, 2, 2), 12, p, lim=4.0, bc="outflow")
+        adm = bl_adm(Zr, meshr, Zr.default_params(**p), *th)
+        c.upload(Zr.REG_ADM, adm)
+        c.ADMToZ4c()
+        c.init_finalize()
+        J = 0.0
+        for _ in range(nsteps):
+            c.evolve(dt, 1)
+            J += dt * c.objective(Zr.REG_U)[0]
+        c.close()
+        return J
+
+    adm = bl_adm(Z, mesh, params, *theta)
+    ctx.upload(Z.REG_ADM, adm)
+    ctx.ADMToZ4c()
+    ctx.init_finalize()
+    J, pb, st = ctx.gradient(dt, nsteps, 3, w_final=0.0, w_step=dt)
+    ctx.upload(Z.REG_ADM, adm)  # the steps rewrote it (Z4cToADM)
+    ctx.adj_adm_to_z4c()
+    ab = ctx.download(Z.REG_ADM_ADJ)
+    ctx.close()
+    assert abs(J - run(theta)) <= 1e-12 * abs(J)
+    grads = []
+    for j in range(3):
+        e = np.zeros(3)
+        e[j] = 1e-6
+        dadm = (bl_adm(Z, mesh, params, *(theta + e)) - bl_adm(Z, mesh, params, *(theta - e))) / 2e-6
+        grads.append(dot(ab, dadm))
+    grads.append(pb[0])
+    fds = []
+    for j in range(3):
+        e = np.zeros(3)
+        e[j] = 1e-4
+        fds.append((run(theta + e) - run(theta - e)) / 2e-4)
+    fds.append((run(theta, PUNC["shift_eta"] + 1e-3) - run(theta, PUNC["shift_eta"] - 1e-3)) / 2e-3)
+    names = ("m1", "m2", "separation", "eta")
+    for n_, a, f in zip(names, grads, fds):
+        print(f"dJ/d{n_}: adjoint {a:.12e}, differences {f:.12e}, rel {abs(a - f) / abs(f):.2e}")
+    for a, f in zip(grads, fds):
+        assert abs(a - f) <= 1e-6 * abs(f)
