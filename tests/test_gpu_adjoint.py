@@ -447,3 +447,32 @@ def test_configs4_parameter_gradient_on_a_uniform_mesh():
         print(f"dJ/d{n_}: adjoint {a:.12e}, differences {f:.12e}, rel {abs(a - f) / abs(f):.2e}")
     for a, f in zip(grads, fds):
         assert abs(a - f) <= 1e-6 * abs(f)
+
+
+def test_torch_autograd_function_gives_the_adjoint_gradient():
+    """The torch.autograd.Function harness: J.backward() returns the adjoint
+    gradient, and a scaled upstream gradient scales it; torch's own
+    central-difference check along a direction agrees."""
+    import torch
+    from z4c_b200.autograd import Z4cObjective
+    Z, mesh, ctx = make((2, 1, 1), 12, GW)
+    u0 = rich_state(Z, mesh, ctx)
+    dt = 0.25 * float(ctx.dx().min())
+    x = torch.tensor(u0, dtype=torch.float64, requires_grad=True)
+    J = Z4cObjective.apply(x, ctx, dt, 5, 2)
+    (3.0 * J).backward()
+    ctx.upload(Z.REG_U, u0)
+    J2, _, _ = ctx.gradient(dt, 5, 2)
+    g = ctx.download(Z.REG_ADJ)
+    assert J.item() == J2
+    assert np.array_equal(x.grad.numpy(), 3.0 * g)
+    v = torch.from_numpy(smooth_direction(Z, mesh, 21))
+    h = 1e-3
+    with torch.no_grad():
+        Jp = Z4cObjective.apply(x + h * v, ctx, dt, 5, 2)
+        Jm = Z4cObjective.apply(x - h * v, ctx, dt, 5, 2)
+    fd = float(Jp - Jm) / (2 * h)
+    ad = float(torch.sum(x.grad * v)) / 3.0
+    print(f"autograd: {ad:.12e}, differences {fd:.12e}")
+    assert abs(fd - ad) <= 1e-6 * abs(fd)
+    ctx.close()
