@@ -32,6 +32,11 @@
 //                      CALC_Z4CRHS, INT_Z4C, SEND/RECV/SETB_Z4C, PHY_BVAL,
 //                      ALG_CONSTR); s<N>_adm and s<N>_con after the last stage
 //
+// Built with -DZ4C_SHIM (z4c_ops_shim) the driver calls the B200 library
+// through the reference-side adapter of z4c_b200_shim.hpp in place of
+// Z4c::Z4cRHS, Z4c::AlgConstr and Z4c::Z4cToADM, every other step unchanged,
+// and writes the same records.
+//
 // usage: z4c_ops_ref -i <input deck> [block/name=value ...]
 #include <cstdint>
 #include <iostream>
@@ -48,6 +53,9 @@
 #include "mesh/spherical_grid.hpp"
 
 #include "z4c_oracle_io.hpp"
+#ifdef Z4C_SHIM
+#include "z4c_b200_shim.hpp"
+#endif
 
 namespace z4c_oracle {
 void DumpGeometry(Mesh* pm, Writer& w);  // z4c_oracle_pgen.cpp
@@ -327,6 +335,28 @@ int main(int argc, char* argv[]) {
   std::vector<MeshBlock*>& blocks = d.by_gid;
   const int NZ = Z4c::N_Z4c;
 
+  // the three operators the shim mode swaps
+#ifdef Z4C_SHIM
+  const bool shim_bt =
+      pin->GetOrAddString("time", "integrator", "rk4").find("bt_") != std::string::npos;
+  Z4cB200 shim(pm, blocks[0], blocks[0]->pz4c, shim_bt);
+  auto OpRHS = [&](MeshBlock* b, AthenaArray<Real>& u, AthenaArray<Real>& rhs) {
+    shim.Z4cRHS(b, u, b->pz4c->storage.mat, rhs);
+  };
+  auto OpAlg = [&](MeshBlock* b, AthenaArray<Real>& u) { shim.AlgConstr(b, u); };
+  auto OpToADM = [&](MeshBlock* b, AthenaArray<Real>& u, AthenaArray<Real>& adm) {
+    shim.Z4cToADM(b, u, adm);
+  };
+#else
+  auto OpRHS = [&](MeshBlock* b, AthenaArray<Real>& u, AthenaArray<Real>& rhs) {
+    b->pz4c->Z4cRHS(u, b->pz4c->storage.mat, rhs);
+  };
+  auto OpAlg = [&](MeshBlock* b, AthenaArray<Real>& u) { b->pz4c->AlgConstr(u); };
+  auto OpToADM = [&](MeshBlock* b, AthenaArray<Real>& u, AthenaArray<Real>& adm) {
+    b->pz4c->Z4cToADM(u, adm);
+  };
+#endif
+
   {
     std::vector<double> t = {pm->time, pm->dt};
     d.w.f64("time_dt", {2}, t.data());
@@ -347,7 +377,7 @@ int main(int argc, char* argv[]) {
     Z4c* z = blocks[g]->pz4c;
     tmp[g].NewAthenaArray(NZ, d.nn3, d.nn2, d.nn1);
     z->PrepareZ4cDerivatives(z->storage.u);
-    z->Z4cRHS(z->storage.u, z->storage.mat, tmp[g]);
+    OpRHS(blocks[g], z->storage.u, tmp[g]);
   }
   d.dump("rhs0", NZ, [&](MeshBlock* b) -> AthenaArray<Real>& { return tmp[b->gid]; });
   for (size_t g = 0; g < blocks.size(); ++g) {
@@ -359,13 +389,13 @@ int main(int argc, char* argv[]) {
   for (size_t g = 0; g < blocks.size(); ++g) {
     Z4c* z = blocks[g]->pz4c;
     Copy(tmp[g], z->storage.u);
-    z->AlgConstr(tmp[g]);
+    OpAlg(blocks[g], tmp[g]);
   }
   d.dump("alg0", NZ, [&](MeshBlock* b) -> AthenaArray<Real>& { return tmp[b->gid]; });
 
   for (auto* b : blocks) {
     Z4c* z = b->pz4c;
-    z->Z4cToADM(z->storage.u, z->storage.adm);
+    OpToADM(b, z->storage.u, z->storage.adm);
     z->ADMConstraints(z->storage.con, z->storage.adm, z->storage.mat, z->storage.u);
   }
   d.dump("adm0", Z4c::N_ADM, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.adm; });
@@ -437,7 +467,7 @@ int main(int argc, char* argv[]) {
       if (is_bt) {
         bt->PrepareStageScratch(stage, b, z->bt_k, z->storage.u, z->storage.rhs);
       }
-      z->Z4cRHS(z->storage.u, z->storage.mat, z->storage.rhs);
+      OpRHS(b, z->storage.u, z->storage.rhs);
       z->Z4cBoundaryRHS(z->storage.u, z->storage.mat, z->storage.rhs);
     }
     d.dump(s + "rhs", NZ, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.rhs; });
@@ -461,14 +491,14 @@ int main(int argc, char* argv[]) {
     d.dump(s + "exch", NZ, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.u; });
     for (auto* b : blocks) {
       Z4c* z = b->pz4c;
-      z->AlgConstr(z->storage.u);
+      OpAlg(b, z->storage.u);
       z->PrepareZ4cDerivatives(z->storage.u);
     }
     d.dump(s + "alg", NZ, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.u; });
     if (stage == nstages) {
       for (auto* b : blocks) {
         Z4c* z = b->pz4c;
-        z->Z4cToADM(z->storage.u, z->storage.adm);
+        OpToADM(b, z->storage.u, z->storage.adm);
         z->ADMConstraints(z->storage.con, z->storage.adm, z->storage.mat, z->storage.u);
       }
       d.dump(s + "adm", Z4c::N_ADM, [](MeshBlock* b) -> AthenaArray<Real>& { return b->pz4c->storage.adm; });
