@@ -12,7 +12,11 @@ advanced one full step (the reference's zone-cycle, main.cpp:239).
 
 At N = 1 the line also carries "bbh_smr": the refined binary-puncture mesh
 below (3,424 MeshBlocks on seven levels), its own zone-updates/s and the time
-of one multilevel ghost fill (--no-smr skips it).
+of one multilevel ghost fill (--no-smr skips it); and "bbh_amr": the adaptive
+binary run (the same punctures on 8^3 root MeshBlocks, seven levels refined
+by the reference's Linf_box_in_box criterion around the puncture trackers,
+200 cycles with the block list changing), timed whole, regrids included, with
+the block count after every regrid (--no-amr skips it).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -21,8 +25,9 @@ With N > 1 (torchrun) every rank evolves its own replica of the mesh
 value is the total over ranks divided by the slowest rank's time.
 
   python bench.py --workload bbh_smr [--steps K] [--warmup W]
+  python bench.py --workload bbh_amr [--steps K] [--warmup W]
 
-prints that measurement alone as a line of its own; one GPU.
+print those measurements alone as a line of their own; one GPU.
 
 The CPU baseline and --impl reference time the reference's own OpenMP build
 (oracle/_ref/athena_ref_native: the reference's g++ flags with -march=native
@@ -61,6 +66,14 @@ CPU_SAMPLE_STEPS = 8
 # timed RK4 steps of the refined-mesh measurement inside the headline run
 # (about 150 ms each)
 SMR_STEPS = 10
+# cycles of the adaptive binary run (configs' 200 steps; about 160 ms each),
+# and of its shifted-gauge variant
+AMR_STEPS = 200
+AMR_SHIFTED_STEPS = 60
+# initial shift of the shifted-gauge variant: the same data in a gauge whose
+# constant beta^x carries both trackers about 0.25 along +x (the Gamma-driver
+# damps it with eta = 2), past the first refinement boundaries at 0.094
+AMR_SHIFT = (-0.5, 0.0, 0.0)
 # Algorithmic HBM bytes of one fused stage per interior vertex: read u and u1,
 # write u' and u1' (22 FP64 variables each).
 STAGE_BYTES_PER_POINT = 4 * 22 * 8
@@ -93,6 +106,8 @@ def parse():
                     help="skip the adjoint-step measurements of the headline line")
     ap.add_argument("--no-smr", action="store_true",
                     help="skip the refined binary-puncture measurement of the headline line")
+    ap.add_argument("--no-amr", action="store_true",
+                    help="skip the adaptive binary-puncture run of the headline line")
     ap.add_argument("--nb", type=int, default=8,
                     help="MeshBlocks per axis (8 = the 128^3 workload; smaller for profiling)")
     ap.add_argument("--profile-run", action="store_true",
@@ -101,9 +116,10 @@ def parse():
                     help="launch shape point_threads,column_threads,column_slabs instead of "
                          "the autotuner's pick (profiling under ncu, whose serialised launches "
                          "would mislead the autotuner)")
-    ap.add_argument("--workload", default="uniform", choices=["uniform", "bbh_smr"],
-                    help="bbh_smr: binary punctures on a statically refined mesh of 7 levels "
-                         "(a separate measurement, not the headline line)")
+    ap.add_argument("--workload", default="uniform", choices=["uniform", "bbh_smr", "bbh_amr"],
+                    help="bbh_smr: binary punctures on a statically refined mesh of 7 levels; "
+                         "bbh_amr: the adaptive run (separate measurements, not the headline "
+                         "line)")
     return ap.parse_args()
 
 
@@ -424,6 +440,90 @@ SMR_REGIONS = [dict(x1min=-r, x1max=r, x2min=-r * f, x2max=r * f, x3min=-r * f, 
 SMR_CENTRES = ((3.0, 0.0625 * 0.37, 0.0625 * 0.21), (-3.0, -0.0625 * 0.37, -0.0625 * 0.21))
 
 
+# The adaptive binary: the punctures of SMR_CENTRES on [-512, 512]^3 with 8^3
+# root MeshBlocks of 16^3 cells (dx 8) and 7 levels (finest dx 1/8), refined
+# by Linf_box_in_box with par_b = 3 around the two puncture trackers, the
+# reference's default derefinement count of 10 cycles.
+AMR_MESH = dict(nb=(8, 8, 8), nx=(16, 16, 16), xmin=(-512.0,) * 3, xmax=(512.0,) * 3,
+                numlevel=7, derefine_count=10, par_b=3.0)
+
+
+def amr_measure(steps, warmup, shift=(0.0, 0.0, 0.0)):
+    """The adaptive binary run: `warmup` cycles, then `steps` cycles timed
+    whole on the device stream (RK steps, the host's refinement flags, which
+    overlap the step, and every regrid: new context, state transfer, ghost
+    finalisation, graph capture), with zone-updates counted per cycle on the
+    mesh that cycle stepped.  `shift`: the initial shift (zero in the
+    configuration as written)."""
+    import torch
+    import z4c_b200 as Z
+    from z4c_b200 import amr as A
+    from z4c_b200 import initial_data as ID
+    torch.cuda.set_device(0)
+    m = AMR_MESH
+    params = Z.default_params(**PARAMS)
+    stream = torch.cuda.Stream()
+    ref = A.Refinement(m["nb"], m["nx"], m["xmin"], m["xmax"], Z.Mesh(
+        m["nb"], m["nx"], m["xmin"], m["xmax"], "outflow").bc, m["numlevel"],
+        m["derefine_count"], m["par_b"])
+    t0 = time.time()
+    with torch.cuda.stream(stream):
+        run = A.AdaptiveEvolution(
+            ref, params, "rk4",
+            lambda mesh: ID.punctures(mesh, params, masses=(0.5, 0.5), centres=SMR_CENTRES,
+                                      shift=shift),
+            SMR_CENTRES, cfl=CFL, history=False, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        setup_s = time.time() - t0
+        run.ctx.autotune(reps=2)
+        run.tile = run.ctx.get_tile()
+        initial_blocks = run.mesh.nblocks
+        for _ in range(warmup):
+            run.step()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(0)
+        sampler.start()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        zones, regrids, regrid_s = 0, [], []
+        p0 = np.array(run.trackers())
+        ev0.record(stream)
+        w0 = time.time()
+        for _ in range(steps):
+            zones += run.mesh.zones()
+            t = time.time()
+            if run.step():
+                regrids.append([run.ncycle, run.mesh.nblocks])
+                regrid_s.append(time.time() - t)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.time() - w0
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    moved = float(np.abs(np.array(run.trackers()) - p0).max())
+    finite = bool(run.ctx.check_finite())
+    final_blocks = run.mesh.nblocks
+    run.close()
+    return {
+        "metric": "zone-updates/s", "value": zones / (ms * 1e-3), "unit": "zone-updates/s",
+        "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": ms / steps,
+        "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "binary Brill-Lindquist punctures (m=0.5 each near (+-3,0,0)), "
+                               "[-512,512]^3, 8^3 root MeshBlocks of 16^3 cells, 7 levels "
+                               "refined by Linf_box_in_box (par_b 3) around the puncture "
+                               "trackers, derefine_count 10, extrapolate_outflow, rk4 (2S), "
+                               "cfl 0.25", "initial_shift": list(shift),
+                   "l2": "inputs larger than L2"},
+        "initial_meshblocks": initial_blocks, "final_meshblocks": final_blocks,
+        "regrids": regrids, "regrid_cycle_s": regrid_s, "tracker_displacement": moved,
+        "wall_s": wall, "setup_s": setup_s, "finite": finite, "clocks": clocks,
+    }
+
+
+def main_amr(args):
+    print(json.dumps(amr_measure(args.steps, args.warmup)), flush=True)
+    print(json.dumps(amr_measure(AMR_SHIFTED_STEPS, args.warmup, AMR_SHIFT)), flush=True)
+
+
 def main_smr(args):
     print(json.dumps(smr_measure(args.steps, args.warmup, args.shape)), flush=True)
 
@@ -507,6 +607,8 @@ def main():
         return main_reference(args, rank, world)
     if args.workload == "bbh_smr":
         return main_smr(args)
+    if args.workload == "bbh_amr":
+        return main_amr(args)
 
     import torch
     import torch.distributed as dist
@@ -709,6 +811,17 @@ def main():
                                                "exchange_ms", "exchange_share", "setup_s",
                                                "finite", "clocks")}
         line["bbh_smr"]["config"] = smr["config"]
+    if world == 1 and not args.no_amr:
+        # configs[2]'s adaptive run: 200 cycles, block list changing
+        keys = ("value", "unit", "ms_per_step", "steps", "initial_meshblocks",
+                "final_meshblocks", "regrids", "regrid_cycle_s", "tracker_displacement",
+                "wall_s", "setup_s", "finite", "clocks", "config")
+        amr = amr_measure(AMR_STEPS, 3)
+        line["bbh_amr"] = {k: amr[k] for k in keys}
+        # the same data in a shifted gauge: the trackers cross refinement
+        # boundaries, so the regrid path runs at this size
+        amr = amr_measure(AMR_SHIFTED_STEPS, 3, AMR_SHIFT)
+        line["bbh_amr_shifted"] = {k: amr[k] for k in keys}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

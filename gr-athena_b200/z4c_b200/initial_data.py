@@ -49,12 +49,13 @@ def _psi4_regularized(psi4_bare, chi_div_floor, chi_psi_power):
     return min(t, psi4_bare) if math.isfinite(psi4_bare) else t
 
 
-def punctures(mesh, params, masses=(1.0,), centres=((0.0, 0.0, 0.0),)):
-    """Conformally flat punctures with psi = 1 + sum_i m_i / (2 r_i) and the
-    precollapsed lapse alpha = psi^-2.  One puncture is Z4c::ADMOnePuncture +
-    GaugePreCollapsedLapse (z4c/one_puncture_z4c.cpp:22-60, gauge.cpp:46-60);
-    two or more give Brill-Lindquist data, the same construction summed over
-    punctures (no reference counterpart: the reference ships no BL data)."""
+def punctures(mesh, params, masses=(1.0,), centres=((0.0, 0.0, 0.0),), shift=(0.0, 0.0, 0.0)):
+    """Conformally flat punctures with psi = 1 + sum_i m_i / (2 r_i), the
+    precollapsed lapse alpha = psi^-2 and a constant shift (zero by
+    default).  One puncture is Z4c::ADMOnePuncture + GaugePreCollapsedLapse
+    (z4c/one_puncture_z4c.cpp:22-60, gauge.cpp:46-60); two or more give
+    Brill-Lindquist data, the same construction summed over punctures (no
+    reference counterpart: the reference ships no BL data)."""
     pw = params.chi_psi_power
     out = []
     for b in range(mesh.nblocks):
@@ -74,12 +75,16 @@ def punctures(mesh, params, masses=(1.0,), centres=((0.0, 0.0, 0.0),)):
             else:
                 psi = psi + term
         psi4_bare = pow_(psi, 4.).astype(np.float64)
-        reg = np.frompyfunc(lambda v: _psi4_regularized(v, params.chi_div_floor, pw), 1, 1)
-        psi4 = reg(psi4_bare).astype(np.float64)
+        # _psi4_regularized over the array: the threshold once, then
+        # std::min(T, v) (v where v < T, else T) and T where v is not finite
+        t = math.pow(params.chi_div_floor, 4. / pw)
+        psi4 = np.where(np.isfinite(psi4_bare) & (psi4_bare < t), psi4_bare, t)
         adm[ADM_PSI4] = psi4
         for c in (ADM_GXX, ADM_GYY, ADM_GZZ):
             adm[c] = psi4
         adm[ADM_ALPHA] = pow_(psi4, -0.5).astype(np.float64)
+        for a in range(3):
+            adm[ADM_BETAX + a] = float(shift[a])
         out.append(adm)
     return np.stack(out)
 

@@ -14,10 +14,23 @@
 //   inject_adm        ADM state read from <problem>/inject_file (record "adm",
 //                     [nblocks, 17, ...]) with lapse/shift from it, then
 //                     ADMToZ4c.
+//   brill_lindquist   conformally flat punctures psi = 1 + sum m_n / (2 r_n)
+//                     of masses <problem>/bl_m_<n> at the puncture trackers'
+//                     starting points <z4c>/bh_<n>_{x,y,z}, n < <z4c>/npunct
+//                     (ADMOnePuncture, z4c/one_puncture_z4c.cpp:22-60, summed
+//                     over punctures), pre-collapsed lapse and the constant
+//                     shift <problem>/shift_{x,y,z} (default 0), then ADMToZ4c.
 //
 // Mesh hooks: <problem>/dump_initial and <problem>/dump_final name record files
 // that receive the state of every block before the first and after the last
-// step (u, adm, con and the block geometry).
+// step (u, adm, con and the block geometry).  <problem>/dump_blocks names a
+// record file that receives, after the run, the MeshBlock list at the top of
+// every main-loop iteration (after the previous iteration's regrid).
+//
+// With <mesh>/refinement = adaptive the refinement condition is the
+// reference's Z4c_AMR::ShouldIRefine (z4c/z4c_amr.cpp:376-404), the one the
+// two-puncture problem generator enrolls (pgen/z4c_two_punctures.cpp:225-237).
+#include <cmath>
 #include <cstdint>
 #include <iostream>
 #include <string>
@@ -29,6 +42,8 @@
 #include "mesh/mesh.hpp"
 #include "parameter_input.hpp"
 #include "z4c/z4c.hpp"
+#include "z4c/puncture_tracker.hpp"
+#include "z4c/z4c_amr.hpp"
 
 #include "z4c_oracle_io.hpp"
 
@@ -52,6 +67,84 @@ void FillBlockArray(AthenaArray<Real>& a, int nvar, const double* src) {
     for (int k = 0; k < nn3; ++k)
       for (int j = 0; j < nn2; ++j)
         for (int i = 0; i < nn1; ++i) a(n, k, j, i) = src[p++];
+}
+
+// Brill-Lindquist data of the brill_lindquist test (see the header).
+void BrillLindquist(ParameterInput* pin, Z4c* z) {
+  const int np = pin->GetOrAddInteger("z4c", "npunct", 0);
+  std::vector<Real> m(np), c(3 * np);
+  for (int n = 0; n < np; ++n) {
+    const std::string id = std::to_string(n);
+    m[n] = pin->GetReal("problem", "bl_m_" + id);
+    c[3 * n + 0] = pin->GetReal("z4c", "bh_" + id + "_x");
+    c[3 * n + 1] = pin->GetReal("z4c", "bh_" + id + "_y");
+    c[3 * n + 2] = pin->GetReal("z4c", "bh_" + id + "_z");
+  }
+  const Real shift[3] = {pin->GetOrAddReal("problem", "shift_x", 0.0),
+                         pin->GetOrAddReal("problem", "shift_y", 0.0),
+                         pin->GetOrAddReal("problem", "shift_z", 0.0)};
+  AthenaArray<Real>& u_adm = z->storage.adm;
+  z->ADMMinkowski(u_adm);
+  Z4c::ADM_vars adm;
+  Z4c::SetADMAliases(u_adm, adm);
+  const int nn3 = z->mbi.nn3, nn2 = z->mbi.nn2, nn1 = z->mbi.nn1;
+  for (int k = 0; k < nn3; ++k)
+    for (int j = 0; j < nn2; ++j)
+      for (int i = 0; i < nn1; ++i) {
+        Real psi = 1.0;
+        for (int n = 0; n < np; ++n) {
+          const Real dx = z->mbi.x1(i) - c[3 * n + 0];
+          const Real dy = z->mbi.x2(j) - c[3 * n + 1];
+          const Real dz = z->mbi.x3(k) - c[3 * n + 2];
+          const Real r = std::sqrt(dx * dx + dy * dy + dz * dz);
+          psi = psi + 0.5 * m[n] / r;
+        }
+        adm.psi4(k, j, i) = z->psi4Regularized(std::pow(psi, 4.));
+        for (int a = 0; a < 3; ++a)
+          for (int b = a; b < 3; ++b) adm.g_dd(a, b, k, j, i) *= adm.psi4(k, j, i);
+      }
+  z->GaugePreCollapsedLapse(u_adm, z->storage.u);
+  Z4c::Z4c_vars zv;
+  Z4c::SetZ4cAliases(z->storage.u, zv);
+  for (int a = 0; a < 3; ++a)
+    for (int k = 0; k < nn3; ++k)
+      for (int j = 0; j < nn2; ++j)
+        for (int i = 0; i < nn1; ++i) {
+          zv.beta_u(a, k, j, i) = shift[a];
+          adm.beta_u(a, k, j, i) = shift[a];
+        }
+}
+
+// Z4c_AMR::ShouldIRefine of the block (1 refine, -1 derefine, 0 keep).
+int Z4cRefinementCondition(MeshBlock* pmb) {
+  return pmb->pz4c->pz4c_amr->ShouldIRefine(pmb);
+}
+
+// MeshBlock lists seen at the top of each main-loop iteration (dump_blocks):
+// rows of (ncycle, gid, level, lx1, lx2, lx3), (ncycle, time, dt) and the
+// puncture trackers' positions then (the ones the iteration's refinement
+// flags see).
+std::vector<std::int32_t> g_block_rows;
+std::vector<double> g_cycle_rows;
+std::vector<double> g_tracker_rows;
+
+void RecordBlocks(Mesh* pm) {
+  const auto& blocks = pm->GetMeshBlocksCached();
+  std::vector<const MeshBlock*> by_gid(blocks.size(), nullptr);
+  for (auto* b : blocks) by_gid.at(b->gid) = b;
+  for (const MeshBlock* b : by_gid) {
+    g_block_rows.push_back(pm->ncycle);
+    g_block_rows.push_back(b->gid);
+    g_block_rows.push_back(b->loc.level);
+    g_block_rows.push_back(static_cast<std::int32_t>(b->loc.lx1));
+    g_block_rows.push_back(static_cast<std::int32_t>(b->loc.lx2));
+    g_block_rows.push_back(static_cast<std::int32_t>(b->loc.lx3));
+  }
+  g_cycle_rows.push_back(pm->ncycle);
+  g_cycle_rows.push_back(pm->time);
+  g_cycle_rows.push_back(pm->dt);
+  for (auto* t : pm->pz4c_tracker)
+    for (int a = 0; a < 3; ++a) g_tracker_rows.push_back(t->GetPos(a));
 }
 
 }  // namespace
@@ -151,6 +244,8 @@ void MeshBlock::ProblemGenerator(ParameterInput* pin) {
   } else if (test == "minkowski") {
     z->ADMMinkowski(z->storage.adm);
     z->GaugeGeodesic(z->storage.u);
+  } else if (test == "brill_lindquist") {
+    BrillLindquist(pin, z);
   } else if (test == "inject" || test == "inject_adm") {
     const std::string path = pin->GetString("problem", "inject_file");
     const auto recs = z4c_oracle::read_all(path);
@@ -190,6 +285,10 @@ void MeshBlock::ProblemGenerator(ParameterInput* pin) {
   z->ADMToZ4c(z->storage.adm, z->storage.u);
 }
 
+void Mesh::InitUserMeshData(ParameterInput* pin) {
+  if (adaptive) EnrollUserRefinementCondition(Z4cRefinementCondition);
+}
+
 // Called at the top of every main-loop iteration (main.cpp:167): only the
 // first call sees the initial state.
 void Mesh::UserWorkBeforeLoop(ParameterInput* pin) {
@@ -197,9 +296,21 @@ void Mesh::UserWorkBeforeLoop(ParameterInput* pin) {
   const std::string path = pin->GetOrAddString("problem", "dump_initial", "");
   if (!path.empty() && !dumped) z4c_oracle::DumpMesh(this, path);
   dumped = true;
+  if (!pin->GetOrAddString("problem", "dump_blocks", "").empty()) RecordBlocks(this);
 }
 
 void Mesh::UserWorkAfterLoop(ParameterInput* pin) {
   const std::string path = pin->GetOrAddString("problem", "dump_final", "");
   if (!path.empty()) z4c_oracle::DumpMesh(this, path);
+  const std::string blocks = pin->GetOrAddString("problem", "dump_blocks", "");
+  if (!blocks.empty()) {
+    RecordBlocks(this);  // the list the last iteration's regrid left
+    z4c_oracle::Writer w(blocks);
+    const std::int64_t nrow = static_cast<std::int64_t>(g_block_rows.size() / 6);
+    const std::int64_t ncyc = static_cast<std::int64_t>(g_cycle_rows.size() / 3);
+    w.i32("blocks", {nrow, 6}, g_block_rows.data());
+    w.f64("cycles", {ncyc, 3}, g_cycle_rows.data());
+    const std::int64_t ntr = static_cast<std::int64_t>(pz4c_tracker.size());
+    if (ntr > 0) w.f64("trackers", {ncyc, ntr, 3}, g_tracker_rows.data());
+  }
 }

@@ -26,6 +26,10 @@ Fixtures (numpy .npz, compressed):
                     of one MeshBlock of a statically refined mesh, and the
                     regrid-time state transfer (coarse to fine, fine to
                     coarse) between two of its blocks
+  amr_<case>.npz    an adaptive run of the stock reference driver: MeshBlock
+                    lists, dt and puncture-tracker positions of every cycle,
+                    the history table, sums and samples of the initial and
+                    final states
   ml_exchange_<bc>.npz  one vertex-centred ghost fill of a two-level mesh
                     (restriction, additive unpack with node multiplicity,
                     coarse-level BCs, prolongation, fine-level BCs) of an
@@ -127,6 +131,27 @@ SCALE = {
 }
 BC_CODES = {"periodic": 0, "extrapolate_outflow": 1, "gr_sommerfeld": 2}
 
+# An adaptive run in the manner of configs[2], small: Brill-Lindquist
+# punctures (m = 0.5 each, a fraction of a cell off (+-1.5, 0, 0)) on
+# [-8, 8]^3 with 2^3 root MeshBlocks of 8^3, 4 levels, refined by the
+# reference's Linf_box_in_box criterion around the two puncture trackers
+# (par_b = 1.5), derefinement after 3 flagged cycles.  A constant initial
+# shift beta^x = -1 with a weak Gamma-driver damping (eta = 0.5) carries the
+# trackers across the refinement boundaries: the run refines at cycle 17 and
+# derefines at cycle 44 of its 60.
+AMR = {
+    "bbh_amr": dict(test="brill_lindquist", z4c=dict(PUNCTURE, shift_eta=0.5), integ="rk4",
+                    bc="extrapolate_outflow", mesh=[(16, -8.0, 8.0, 8)] * 3,
+                    amr=dict(numlevel=4, derefine_count=3),
+                    extra={"npunct": 2,
+                           "bh_0_x": 1.5 + 0.0625 * 0.37, "bh_0_y": 0.0625 * 0.21,
+                           "bh_0_z": 0.0625 * 0.13,
+                           "bh_1_x": -1.5 - 0.0625 * 0.37, "bh_1_y": -0.0625 * 0.21,
+                           "bh_1_z": -0.0625 * 0.13},
+                    problem={"bl_m_0": 0.5, "bl_m_1": 0.5, "par_b": 1.5, "shift_x": -1.0},
+                    nlim=60, stride=2, tracker=True),
+}
+
 
 def deck(case, out_file, nlim=1, dump_initial="", dump_final="", hst=False, threads=1):
     lines = ["<job>", "problem_id = golden", "<z4c>"]
@@ -139,7 +164,13 @@ def deck(case, out_file, nlim=1, dump_initial="", dump_final="", hst=False, thre
         d = a + 1
         lines += [f"nx{d} = {nx}", f"x{d}min = {lo!r}", f"x{d}max = {hi!r}",
                   f"ix{d}_bc = {case['bc']}", f"ox{d}_bc = {case['bc']}"]
-    lines += ["refinement = none", f"num_threads = {threads}", "<meshblock>"]
+    amr = case.get("amr")
+    if amr:
+        lines += ["refinement = adaptive", f"numlevel = {amr['numlevel']}",
+                  f"derefine_count = {amr['derefine_count']}"]
+    else:
+        lines.append("refinement = none")
+    lines += [f"num_threads = {threads}", "<meshblock>"]
     for a, (_, _, _, nb) in enumerate(case["mesh"]):
         lines.append(f"nx{a + 1} = {nb}")
     lines += ["<problem>", f"test = {case['test']}"]
@@ -296,6 +327,50 @@ def make_scale(name, case, outdir, threads=None):
         out["noise"] = json.dumps(case["noise"])
     out.update(meta_json(case))
     path = os.path.join(outdir, f"scale_{name}.npz")
+    np.savez_compressed(path, **out)
+    return path
+
+
+def make_amr(name, case, outdir, threads=None):
+    """The stock reference driver on an adaptive mesh (AMR cases): the
+    MeshBlock list, time, dt and puncture-tracker positions at the top of
+    every cycle (the oracle problem generator's dump_blocks), the history
+    table, and sums plus a strided sample (four MeshBlocks) of the initial
+    and final states."""
+    threads = threads or os.cpu_count()
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = os.path.join(tmp, "case.inp")
+        init, final = os.path.join(tmp, "init.rec"), os.path.join(tmp, "final.rec")
+        blocks = os.path.join(tmp, "blocks.rec")
+        text = deck(case, "unused", nlim=case["nlim"], dump_initial=init, dump_final=final,
+                    hst=True, threads=threads)
+        text = text.replace("<driver>", f"dump_blocks = {blocks}\n<driver>")
+        with open(inp, "w") as f:
+            f.write(text)
+        subprocess.run([os.path.join(REF_BIN, "athena_ref"), "-i", inp], cwd=tmp, check=True,
+                       stdout=subprocess.DEVNULL)
+        hst = parse_hst(os.path.join(tmp, "golden.hst"))
+        rb = read_records(blocks)
+        s = case["stride"]
+        out = dict(hst=hst, blocks=rb["blocks"], cycles=rb["cycles"], trackers=rb["trackers"],
+                   nlim=np.array(case["nlim"]), stride=np.array(s), threads=np.array(threads))
+        for tag, path in (("init", init), ("final", final)):
+            r = read_records(path)
+            nb = r["u"].shape[0]
+            pick = np.array(sorted({0, nb // 3, (2 * nb) // 3, nb - 1}))
+            out[f"{tag}_meta"] = r["meta"]
+            out[f"{tag}_sample_blocks"] = pick
+            out[f"u_{tag}_sample"] = r["u"][pick][:, :, ::s, ::s, ::s]
+            out[f"u_{tag}_sums"] = state_sums(r["u"])
+            if tag == "final":
+                out["con_final_sums"] = state_sums(r["con"])
+                out["time_dt"] = r["time_dt"]
+            del r
+    out.update(meta_json(case))
+    out["amr"] = json.dumps(case["amr"])
+    out["extra"] = json.dumps(case["extra"])
+    out["problem"] = json.dumps(case["problem"])
+    path = os.path.join(outdir, f"amr_{name}.npz")
     np.savez_compressed(path, **out)
     return path
 
@@ -478,6 +553,11 @@ def main():
         print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
     if not only or "restart_track4" in only:  # needs evol_track4
         p = make_restart(HERE)
+        print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
+    for name, case in AMR.items():
+        if only and f"amr_{name}" not in only:
+            continue
+        p = make_amr(name, case, HERE)
         print(f"{p}: {os.path.getsize(p) / 1e6:.2f} MB")
     for name, case in SCALE.items():  # minutes each: the reference at full size
         if only and f"scale_{name}" not in only:
