@@ -66,7 +66,7 @@ CPU_SAMPLE_STEPS = 8
 # timed RK4 steps of the refined-mesh measurement inside the headline run
 # (about 150 ms each)
 SMR_STEPS = 10
-# cycles of the adaptive binary run (configs' 200 steps; about 160 ms each),
+# cycles of the adaptive binary run (200 as the benchmark states; about 160 ms each),
 # and of its shifted-gauge variant
 AMR_STEPS = 200
 AMR_SHIFTED_STEPS = 60
@@ -341,7 +341,7 @@ def time_on(stream, fn, reps):
     return e0.elapsed_time(e1) / reps
 
 
-# the gauge wave of configs[0] on 64^3 cells in one periodic
+# The adjoint benchmark: the 48^3 gauge-wave benchmark's physics on 64^3 cells in one periodic
 # MeshBlock, A = 0.05, seeded U(-1e-6, 1e-6) on the conformal metric, 100 rk4
 # steps, objective = H-norm after the last step; eps_floor < 0 keeps
 # AlgConstr's determinant normalisation on every vertex (differentiable)
@@ -353,8 +353,8 @@ ADJ_STEPS, ADJ_SNAPSHOTS = 100, 9
 
 def adjoint_diagnostics(Z, ID, head_ctx, head_stream, head_dt):
     """The differentiated step: one adjoint step (recomputation of the step
-    included) against one forward step, on the configs[3] block and on the
-    headline mesh, and the revolve-checkpointed gradient of configs[3]."""
+    included) against one forward step, on the 64^3 adjoint block and on the
+    headline mesh, and the revolve-checkpointed gradient of the 64^3 adjoint benchmark."""
     import torch
     out = {}
     mesh = Z.Mesh((1, 1, 1), (64, 64, 64), (-0.5,) * 3, (0.5,) * 3, "periodic")
@@ -377,7 +377,7 @@ def adjoint_diagnostics(Z, ID, head_ctx, head_stream, head_dt):
     with torch.cuda.stream(stream):
         J, pb, st = ctx.gradient(dt, ADJ_STEPS, ADJ_SNAPSHOTS)
     torch.cuda.synchronize()
-    out["configs3"] = {
+    out["gw64_adjoint"] = {
         "workload": "gauge wave A=0.05 + U(-1e-6,1e-6) on g~, 64^3 cells, one periodic MeshBlock, "
                     "rk4, 100 steps, objective vol*sum H^2 after the last step",
         "forward_step_ms": fwd, "adjoint_step_ms": adj, "adjoint_over_forward": adj / fwd,
@@ -804,7 +804,7 @@ def main():
     }
     ctx.close()
     if world == 1 and not args.no_smr:
-        # the refined binary-puncture mesh (configs[2]'s 7-level mesh,
+        # the refined binary-puncture mesh (the adaptive benchmark's 7 levels,
         # static): its own context after this one is released
         smr = smr_measure(SMR_STEPS, 3)
         line["bbh_smr"] = {k: smr[k] for k in ("value", "unit", "ms_per_step", "steps",
@@ -812,7 +812,7 @@ def main():
                                                "finite", "clocks")}
         line["bbh_smr"]["config"] = smr["config"]
     if world == 1 and not args.no_amr:
-        # configs[2]'s adaptive run: 200 cycles, block list changing
+        # the adaptive binary-puncture run: 200 cycles, block list changing
         keys = ("value", "unit", "ms_per_step", "steps", "initial_meshblocks",
                 "final_meshblocks", "regrids", "regrid_cycle_s", "tracker_displacement",
                 "wall_s", "setup_s", "finite", "clocks", "config")

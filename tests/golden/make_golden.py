@@ -67,10 +67,10 @@ PUNCTURE = dict(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02, damp_kappa2=0.0
                 shift_eta=2.0, r_max_con=1e300)
 
 CASES = {
-    # configs[0] physics on one 8^3 block (periodic)
+    # the gauge-wave benchmark's physics on one 8^3 block (periodic)
     "gw1": dict(test="gauge_wave1", z4c=GAUGE_WAVE, integ="rk4", bc="periodic",
                 mesh=[(8, -0.5, 0.5, 8)] * 3, extra={"AwA_amplitude": 0.01}),
-    # one puncture, two blocks along x, outflow faces (configs[1] gauge)
+    # one puncture, two blocks along x, outflow faces (the puncture benchmark's gauge)
     "punc2": dict(test="one_puncture", z4c=PUNCTURE, integ="rk4", bc="extrapolate_outflow",
                   mesh=[(16, -4.0, 4.0, 8), (8, -2.0, 2.0, 8), (8, -2.0, 2.0, 8)],
                   extra={}, problem={"punc_ADM_mass": 1.0}),
@@ -87,7 +87,7 @@ CASES = {
 OPS_OPTIONAL = ["brhs0"]
 
 EVOL = {
-    # configs[0] gauge wave, one 16^3 block, 40 steps, history every step
+    # the benchmark gauge wave, one 16^3 block, 40 steps, history every step
     "gw16": dict(test="gauge_wave1", z4c=GAUGE_WAVE, integ="rk4", bc="periodic",
                  mesh=[(16, -0.5, 0.5, 16)] * 3, extra={"AwA_amplitude": 0.01}, nlim=40),
     # one puncture on 2x2x1 blocks with outflow boundaries, 12 steps
@@ -111,18 +111,18 @@ EVOL = {
 # the initial and final states, and a strided sample of the final state on a
 # few MeshBlocks; the test regenerates the initial state on its side.
 SCALE = {
-    # configs[0] as written: 48^3 cells in one periodic block, harmonic-like
+    # the gauge-wave benchmark as written: 48^3 cells in one periodic block, harmonic-like
     # lapse, zero shift, A = 0.01, KO 0.02, kappa1 0.02, 1000 rk4 steps
     "gw48": dict(test="gauge_wave1", z4c=GAUGE_WAVE, integ="rk4", bc="periodic",
                  mesh=[(48, -0.5, 0.5, 48)] * 3, extra={"AwA_amplitude": 0.01}, nlim=1000,
                  stride=4, sample_blocks=[0]),
-    # configs[1] single puncture: M = 1 at the origin, pre-collapsed lapse,
+    # the single-puncture benchmark: M = 1 at the origin, pre-collapsed lapse,
     # 128^3 cells as 512 blocks of 16^3 on [-16, 16]^3, outflow faces
     "punc512": dict(test="one_puncture", z4c=PUNCTURE, integ="rk4", bc="extrapolate_outflow",
                     mesh=[(128, -16.0, 16.0, 16)] * 3, extra={},
                     problem={"punc_ADM_mass": 1.0}, nlim=40, stride=2,
                     sample_blocks=[0, 73, 219, 292, 365, 511]),
-    # configs[1] robust stability: Minkowski plus U(-1e-10, 1e-10) on all 22
+    # the robust-stability benchmark: Minkowski plus U(-1e-10, 1e-10) on all 22
     # Z4c variables at every vertex (initial_data.noise_state, seed 137),
     # periodic, injected into the reference
     "rs512": dict(test="inject", z4c=PUNCTURE, integ="rk4", bc="periodic",
@@ -131,7 +131,7 @@ SCALE = {
 }
 BC_CODES = {"periodic": 0, "extrapolate_outflow": 1, "gr_sommerfeld": 2}
 
-# An adaptive run in the manner of configs[2], small: Brill-Lindquist
+# An adaptive run in the manner of the adaptive binary benchmark, small: Brill-Lindquist
 # punctures (m = 0.5 each, a fraction of a cell off (+-1.5, 0, 0)) on
 # [-8, 8]^3 with 2^3 root MeshBlocks of 8^3, 4 levels, refined by the
 # reference's Linf_box_in_box criterion around the two puncture trackers

@@ -21,9 +21,9 @@ SRC = os.path.join(ROOT, "tests", "ad", "ad_point_check.cpp")
 DP = C.POINTER(C.c_double)
 
 PARAM_SETS = {
-    # configs[1]-[4] gauge: 1+log, Gamma-driver, damping
+    # the puncture benchmarks' gauge: 1+log, Gamma-driver, damping
     "puncture": dict(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02, shift_eta=2.0),
-    # configs[0]/[3] gauge: harmonic lapse, zero shift, kappa2 != 0
+    # the gauge-wave benchmarks' gauge: harmonic lapse, zero shift, kappa2 != 0
     "gauge_wave": dict(lapse_harmonic=1.0, lapse_harmonicf=0.0, lapse_oplog=0.0,
                        lapse_advect=0.0, shift_Gamma=0.0, shift_eta=0.0, shift_advect=0.0,
                        damp_kappa1=0.02, damp_kappa2=0.3),

@@ -7,7 +7,7 @@
   history norm, its tangent against differences, its adjoint against its
   tangent;
 * revolve checkpointing: the gradient does not depend on the snapshot count;
-* configs[3] at its stated size: 64^3 gauge wave (A = 0.05) with seeded 1e-6
+* the gauge-wave adjoint benchmark at its stated size: 64^3 gauge wave (A = 0.05) with seeded 1e-6
   noise on the conformal metric, 100 rk4 steps, the gradient of the H-norm
   with respect to every initial Z4c value against central differences on 32
   seeded directions and against tangent-linear runs.
@@ -257,7 +257,7 @@ def test_revolve_schedules_give_the_same_gradient():
     ctx.close()
 
 
-def configs3_state(Z, mesh, ctx, seed=2024):
+def gw64_adjoint_state(Z, mesh, ctx, seed=2024):
     from z4c_b200 import initial_data as ID
     ID.load_adm(ctx, ID.gauge_wave1(mesh, amplitude=0.05))
     u = ctx.download(Z.REG_U)
@@ -268,9 +268,9 @@ def configs3_state(Z, mesh, ctx, seed=2024):
     return ctx.download(Z.REG_U)
 
 
-def test_configs3_gradient_against_differences_and_tangent_linear_runs():
+def test_gw64_gradient_against_differences_and_tangent_linear_runs():
     Z, mesh, ctx = make((1, 1, 1), 64, GW)
-    u0 = configs3_state(Z, mesh, ctx)
+    u0 = gw64_adjoint_state(Z, mesh, ctx)
     dt = 0.25 / 64
     nsteps = 100
     ctx.upload(Z.REG_U, u0)
@@ -334,7 +334,7 @@ def test_configs3_gradient_against_differences_and_tangent_linear_runs():
     fds, ads = np.array(pairs).T
     rms = np.sqrt(np.mean(ads ** 2))
     worst_fd = float(np.max(np.abs(fds - ads)) / rms)
-    print(f"configs[3]: relative difference to central differences: median {np.median(errs):.2e} "
+    print(f"64^3 gauge wave: relative difference to central differences: median {np.median(errs):.2e} "
           f"(own derivative), worst {worst_fd:.2e} (rms derivative); to tangent-linear runs "
           f"{worst_tlm:.2e}")
     assert worst_fd <= 1e-6
@@ -342,7 +342,7 @@ def test_configs3_gradient_against_differences_and_tangent_linear_runs():
     ctx.close()
 
 
-# ---- the chain to the initial data (configs[4]'s gradient, on a uniform mesh) ----
+# ---- the chain to the initial data (the binary adjoint benchmark's gradient, on a uniform mesh) ----
 
 BL_Y, BL_Z = 0.13, 0.07  # the punctures sit off the x axis and off the vertices
 
@@ -392,8 +392,8 @@ def test_initial_data_adjoint_matches_differences(bc):
     ctx.close()
 
 
-def test_configs4_parameter_gradient_on_a_uniform_mesh():
-    """configs[4]'s gradient on a uniform mesh: the time-integrated H-norm
+def test_binary_parameter_gradient_on_a_uniform_mesh():
+    """The binary adjoint benchmark's gradient on a uniform mesh: the time-integrated H-norm
     of a binary Brill-Lindquist evolution (outflow faces, 1+log and
     Gamma-driver) with respect to the two masses, the separation and the
     Gamma-driver eta, through the revolve-checkpointed adjoint, the adjoint

@@ -2,12 +2,12 @@
 device, against the reference's own runs of them (fixtures scale_*.npz made by
 tests/golden/make_golden.py with the reference build):
 
-  scale_gw48     the gauge wave of configs[0] as written: 48^3 cells in one
+  scale_gw48     the gauge-wave benchmark as written: 48^3 cells in one
                  periodic MeshBlock, harmonic-like lapse, zero shift,
                  A = 0.01, KO 0.02, kappa1 0.02, 1000 rk4 steps
-  scale_punc512  the single puncture of configs[1]: 128^3 cells as 512
+  scale_punc512  the single-puncture benchmark: 128^3 cells as 512
                  MeshBlocks of 16^3, outflow faces, 40 rk4 steps
-  scale_rs512    the robust-stability run of configs[1]: Minkowski plus
+  scale_rs512    the robust-stability benchmark: Minkowski plus
                  U(-1e-10, 1e-10) on all 22 variables, periodic, 40 steps
 
 The reference's state is too large to store (1.4 GB per register on the

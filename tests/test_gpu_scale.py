@@ -91,7 +91,7 @@ def test_noise_state_periodic_translation_symmetry():
 
 
 def test_gauge_wave_convergence_order():
-    """The configs[0] gauge wave converges at the scheme's order: the error of
+    """The benchmark gauge wave converges at the scheme's order: the error of
     the physical g_xx against the exact wave 1 - A sin(2 pi (x - t))."""
     import z4c_b200 as Z
     from z4c_b200 import initial_data as ID
