@@ -85,14 +85,15 @@ FP64_OPS_PER_POINT_STAGE = 7697 + 154
 # The launches of one fused stage and their measured DRAM traffic per interior
 # vertex (ncu dram__bytes_read.sum + dram__bytes_write.sum summed over them,
 # 64-block capture scaled by the vertex count; see profiles/).
-STAGE_KERNELS = "k_prep, k_ricci, k_adv, k_main, k_ko_stage_ls"
+STAGE_KERNELS = {0: "k_prep, k_ricci, k_adv, k_main, k_ko_stage_ls",
+                 1: "k_prep, k_ricci_fast, k_main_fast, k_col_fast"}
 # FP64 operations of PrepareZ4cDerivatives + Z4cWeyl per interior vertex
 # (oracle/opcount), for the psi4 diagnostics line.
 FP64_OPS_PER_POINT_WEYL = 7409
 # psi4 extraction spheres of the diagnostics: (radius, nlev, lmax) inside
 # the [-16,16]^3 domain
 WAVE_SPHERES = ((6.0, 30, 8), (12.0, 30, 8))
-STAGE_TRAFFIC_PER_POINT = 1350.0e6 / (64 * 17 ** 3)
+STAGE_TRAFFIC_PER_POINT = {0: 1350.0e6 / (64 * 17 ** 3), 1: 1025.6e6 / (64 * 17 ** 3)}
 
 
 def parse():
@@ -108,6 +109,10 @@ def parse():
                     help="skip the refined binary-puncture measurement of the headline line")
     ap.add_argument("--no-amr", action="store_true",
                     help="skip the adaptive binary-puncture run of the headline line")
+    ap.add_argument("--contract", type=int, default=1, choices=[0, 1],
+                    help="1: the contracted path (fused multiply-adds, four launches per "
+                         "stage; the headline); 0: the exact path, bit for bit the "
+                         "reference's arithmetic (also measured in the headline line)")
     ap.add_argument("--nb", type=int, default=8,
                     help="MeshBlocks per axis (8 = the 128^3 workload; smaller for profiling)")
     ap.add_argument("--profile-run", action="store_true",
@@ -351,7 +356,7 @@ ADJ_PARAMS = dict(lapse_harmonic=1.0, lapse_harmonicf=0.0, lapse_oplog=0.0, laps
 ADJ_STEPS, ADJ_SNAPSHOTS = 100, 9
 
 
-def adjoint_diagnostics(Z, ID, head_ctx, head_stream, head_dt):
+def adjoint_diagnostics(Z, ID, head_ctx, head_stream, head_dt, exact_shape=None):
     """The differentiated step: one adjoint step (recomputation of the step
     included) against one forward step, on the 64^3 adjoint block and on the
     headline mesh, and the revolve-checkpointed gradient of the 64^3 adjoint benchmark."""
@@ -385,10 +390,19 @@ def adjoint_diagnostics(Z, ID, head_ctx, head_stream, head_dt):
         "gradient_adjoint_steps": st["adjoint_steps"], "snapshots": ADJ_SNAPSHOTS,
         "objective": J, "d_shift_eta": float(pb[0]), "d_damp_kappa1": float(pb[1])}
     ctx.close()
-    # the headline mesh (512 MeshBlocks, outflow faces)
+    # the headline mesh (512 MeshBlocks, outflow faces), on the exact path the
+    # adjoint differentiates
+    contract, tile, regs = head_ctx.get_contract(), head_ctx.get_tile(), head_ctx.get_point_regs()
+    head_ctx.set_contract(False)
+    if exact_shape:  # the exact path's own autotuned shape
+        head_ctx.set_tile(*exact_shape[0])
+        head_ctx.set_point_regs(exact_shape[1])
     head_ctx.adj_setup()
     fwd = time_on(head_stream, lambda: head_ctx.evolve(head_dt, 1), 5)
     adj = time_on(head_stream, lambda: head_ctx.adj_step(head_dt), 3)
+    head_ctx.set_contract(contract)
+    head_ctx.set_tile(*tile)
+    head_ctx.set_point_regs(regs)
     out["puncture_512"] = {"forward_step_ms": fwd, "adjoint_step_ms": adj,
                            "adjoint_over_forward": adj / fwd}
     out["note"] = ("adjoint_step_ms: the step recomputed stage by stage from its start state, then "
@@ -448,13 +462,13 @@ AMR_MESH = dict(nb=(8, 8, 8), nx=(16, 16, 16), xmin=(-512.0,) * 3, xmax=(512.0,)
                 numlevel=7, derefine_count=10, par_b=3.0)
 
 
-def amr_measure(steps, warmup, shift=(0.0, 0.0, 0.0)):
+def amr_measure(steps, warmup, shift=(0.0, 0.0, 0.0), contract=1):
     """The adaptive binary run: `warmup` cycles, then `steps` cycles timed
     whole on the device stream (RK steps, the host's refinement flags, which
     overlap the step, and every regrid: new context, state transfer, ghost
     finalisation, graph capture), with zone-updates counted per cycle on the
     mesh that cycle stepped.  `shift`: the initial shift (zero in the
-    configuration as written)."""
+    configuration as written); `contract`: the right-hand-side path."""
     import torch
     import z4c_b200 as Z
     from z4c_b200 import amr as A
@@ -475,8 +489,11 @@ def amr_measure(steps, warmup, shift=(0.0, 0.0, 0.0)):
             SMR_CENTRES, cfl=CFL, history=False, stream=stream.cuda_stream)
         torch.cuda.synchronize()
         setup_s = time.time() - t0
+        run.contract = bool(contract)
+        run.ctx.set_contract(run.contract)
         run.ctx.autotune(reps=2)
         run.tile = run.ctx.get_tile()
+        run.point_regs = run.ctx.get_point_regs()
         initial_blocks = run.mesh.nblocks
         for _ in range(warmup):
             run.step()
@@ -512,6 +529,7 @@ def amr_measure(steps, warmup, shift=(0.0, 0.0, 0.0)):
                                "refined by Linf_box_in_box (par_b 3) around the puncture "
                                "trackers, derefine_count 10, extrapolate_outflow, rk4 (2S), "
                                "cfl 0.25", "initial_shift": list(shift),
+                   "path": "contracted" if contract else "exact",
                    "l2": "inputs larger than L2"},
         "initial_meshblocks": initial_blocks, "final_meshblocks": final_blocks,
         "regrids": regrids, "regrid_cycle_s": regrid_s, "tracker_displacement": moved,
@@ -520,15 +538,17 @@ def amr_measure(steps, warmup, shift=(0.0, 0.0, 0.0)):
 
 
 def main_amr(args):
-    print(json.dumps(amr_measure(args.steps, args.warmup)), flush=True)
-    print(json.dumps(amr_measure(AMR_SHIFTED_STEPS, args.warmup, AMR_SHIFT)), flush=True)
+    print(json.dumps(amr_measure(args.steps, args.warmup, contract=args.contract)), flush=True)
+    print(json.dumps(amr_measure(AMR_SHIFTED_STEPS, args.warmup, AMR_SHIFT,
+                                 contract=args.contract)), flush=True)
 
 
 def main_smr(args):
-    print(json.dumps(smr_measure(args.steps, args.warmup, args.shape)), flush=True)
+    print(json.dumps(smr_measure(args.steps, args.warmup, args.shape, args.contract)),
+          flush=True)
 
 
-def smr_measure(steps, warmup, shape=None):
+def smr_measure(steps, warmup, shape=None, contract=1):
     """Steps of the refined binary-puncture mesh: zone-updates/s through
     the graph-captured step, and the multilevel ghost exchange alone."""
     import torch
@@ -539,6 +559,7 @@ def smr_measure(steps, warmup, shape=None):
                   refinement=SMR_REGIONS)
     params = Z.default_params(**PARAMS)
     ctx = Z.Z4c(mesh, params, "rk4")
+    ctx.set_contract(bool(contract))
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
     t0 = time.time()
@@ -584,6 +605,7 @@ def smr_measure(steps, warmup, shape=None):
         "config": {"workload": "binary punctures (m=0.5 each near (+-3,0,0)), [-512,512]^3, "
                                "4^3 root MeshBlocks of 16^3 cells, 7 nested static refinement "
                                "levels, extrapolate_outflow, rk4 (2S), cfl 0.25",
+                   "path": "contracted" if contract else "exact",
                    "meshblocks": mesh.nblocks, "blocks_per_level": levels,
                    "finest_dx": float(min(min(mesh.block_coords(b)[1])
                                           for b in range(mesh.nblocks) if mesh.locs[b, 0] ==
@@ -625,6 +647,7 @@ def main():
     mesh = Z.Mesh(nb, WORKLOAD["nx"], [-lim] * 3, [lim] * 3, "outflow")
     params = Z.default_params(**PARAMS)
     ctx = Z.Z4c(mesh, params, "rk4")
+    ctx.set_contract(bool(args.contract))
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
     adm = ID.punctures(mesh, params, masses=(1.0,), centres=((0.0, 0.0, 0.0),))
@@ -638,6 +661,7 @@ def main():
     else:
         with torch.cuda.stream(stream):
             tile, _ = ctx.autotune(reps=3)
+    point_regs = ctx.get_point_regs()
     dt = CFL * float(np.min(ctx.dx()))
     zones = mesh.zones()
     npts = mesh.nblocks * 17 ** 3
@@ -673,20 +697,45 @@ def main():
     finite = ctx.check_finite()
 
     # ---- dominant kernel: the fused RHS+KO+stage kernel, timed alone -------
-    stage_ms = None
-    with torch.cuda.stream(stream):
-        ctx.upload(Z.REG_U, u_init)
-        ctx.init_finalize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        reps = 5
-        times = []
-        for _ in range(reps):
+    def time_stage_seq():
+        with torch.cuda.stream(stream):
+            ctx.upload(Z.REG_U, u_init)
+            ctx.init_finalize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            times = []
+            for _ in range(5):
+                e0.record(stream)
+                ctx.rhs_stage(2, dt)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                times.append(e0.elapsed_time(e1))
+        return sorted(times)[len(times) // 2]
+    stage_ms = time_stage_seq()
+
+    # ---- the exact path (bit for bit the reference's arithmetic) -----------
+    exact = None
+    if args.contract and not args.profile_run:
+        ctx.set_contract(False)
+        with torch.cuda.stream(stream):
+            ctx.upload(Z.REG_U, u_init)
+            ctx.init_finalize()
+            etile, _ = ctx.autotune(reps=3)
+            ctx.evolve(dt, args.warmup)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            ctx.rhs_stage(2, dt)
+            ctx.evolve(dt, args.steps)
             e1.record(stream)
-            torch.cuda.synchronize()
-            times.append(e0.elapsed_time(e1))
-        stage_ms = sorted(times)[len(times) // 2]
+        torch.cuda.synchronize()
+        ems = max_over_ranks(e0.elapsed_time(e1))
+        estage = time_stage_seq()
+        exact = {"value": whole_job_rate(zones * args.steps, world, ems * 1e-3),
+                 "ms_per_step": ems / args.steps, "stage_ms": estage, "launch_shape": etile,
+                 "stage_kernels": STAGE_KERNELS[0],
+                 "stage_traffic": STAGE_TRAFFIC_PER_POINT[0] * npts}
+        exact["point_regs"] = ctx.get_point_regs()
+        ctx.set_contract(True)
+        ctx.set_tile(*tile)
+        ctx.set_point_regs(point_regs)
 
     if args.profile_run:
         if rank == 0:
@@ -742,7 +791,9 @@ def main():
     # ---- differentiated step (N = 1) -----------------------------------------
     adjoint = None
     if world == 1 and not args.no_adjoint:
-        adjoint = adjoint_diagnostics(Z, ID, ctx, stream, dt)
+        adjoint = adjoint_diagnostics(
+            Z, ID, ctx, stream, dt,
+            (tuple(exact["launch_shape"]), exact["point_regs"]) if exact else None)
 
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
     cpu = None
@@ -774,12 +825,13 @@ def main():
             "peak_source": "measured in this run: dependent DFMA chains on every SM "
                            "(2 flops per DFMA); MEASURED_PEAKS.json has no FP64 figure",
             "frac_of_unfused_ceiling": achieved_tf / (0.5 * fp64_peak_tf),
-            "traffic": STAGE_TRAFFIC_PER_POINT * npts,
+            "traffic": STAGE_TRAFFIC_PER_POINT[args.contract] * npts,
             "algorithmic_bytes": STAGE_BYTES_PER_POINT * npts,
             "hbm_achieved_gbs": achieved_gbs, "hbm_peak_gbs": hbm_peak,
             "hbm_frac": achieved_gbs / hbm_peak, "hbm_peak_source": "MEASURED_PEAKS.json",
-            "kernel": "RHS+KO+stage launch sequence (" + STAGE_KERNELS + "), one stage, "
-                      "all 512 MeshBlocks",
+            "kernel": ("contracted" if args.contract else "exact") +
+                      " RHS+KO+stage launch sequence (" + STAGE_KERNELS[args.contract] +
+                      "), one stage, all 512 MeshBlocks",
             "kernel_ms": stage_ms, "fp64_ops_per_vertex": FP64_OPS_PER_POINT_STAGE}
 
     line = {
@@ -788,6 +840,9 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (analytic puncture initial data)",
         "config": dict(WORKLOAD, nb=nb, parallelism=f"replicas{world}", launch_shape=tile,
+                       point_regs=point_regs,
+                       path="contracted (fused multiply-adds; RHS within 1e-12 of the "
+                            "reference's)" if args.contract else "exact (bit for bit)",
                        l2="inputs larger than L2 (1.4 GB per register)",
                        per_block_value=pb_value, batched_over_per_block=value / world / pb_value,
                        state_finite=finite),
@@ -801,12 +856,13 @@ def main():
         "clocks": clocks,
         "psi4": psi4,
         "adjoint": adjoint,
+        "exact_path": exact,
     }
     ctx.close()
     if world == 1 and not args.no_smr:
         # the refined binary-puncture mesh (the adaptive benchmark's 7 levels,
         # static): its own context after this one is released
-        smr = smr_measure(SMR_STEPS, 3)
+        smr = smr_measure(SMR_STEPS, 3, contract=args.contract)
         line["bbh_smr"] = {k: smr[k] for k in ("value", "unit", "ms_per_step", "steps",
                                                "exchange_ms", "exchange_share", "setup_s",
                                                "finite", "clocks")}
@@ -816,11 +872,11 @@ def main():
         keys = ("value", "unit", "ms_per_step", "steps", "initial_meshblocks",
                 "final_meshblocks", "regrids", "regrid_cycle_s", "tracker_displacement",
                 "wall_s", "setup_s", "finite", "clocks", "config")
-        amr = amr_measure(AMR_STEPS, 3)
+        amr = amr_measure(AMR_STEPS, 3, contract=args.contract)
         line["bbh_amr"] = {k: amr[k] for k in keys}
         # the same data in a shifted gauge: the trackers cross refinement
         # boundaries, so the regrid path runs at this size
-        amr = amr_measure(AMR_SHIFTED_STEPS, 3, AMR_SHIFT)
+        amr = amr_measure(AMR_SHIFTED_STEPS, 3, AMR_SHIFT, contract=args.contract)
         line["bbh_amr_shifted"] = {k: amr[k] for k in keys}
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -16,9 +16,11 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libz4c_b200.so")
 SOURCES = ["z4c_kernels.cu", "z4c_capi.cu", "z4c_refine.cu", "z4c_noalloc.cu", "z4c_wave.cu",
-           "z4c_restart.cu", "z4c_multilevel.cu", "z4c_adjoint.cu"]
-# per-file replacements of the default flags
-FILE_FLAGS = {"z4c_adjoint.cu": {"-fmad=false": "-fmad=true"}}
+           "z4c_restart.cu", "z4c_multilevel.cu", "z4c_adjoint.cu", "z4c_fast.cu"]
+# per-file replacements of the default flags: the adjoint and the contracted
+# right-hand side are built with floating-point contraction
+FILE_FLAGS = {"z4c_adjoint.cu": {"-fmad=false": "-fmad=true"},
+              "z4c_fast.cu": {"-fmad=false": "-fmad=true"}}
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
          "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",

@@ -1026,7 +1026,7 @@ int time_stage(z4c_ctx* ctx, const LaunchShape& sh, int reps, float* best_ms) {
 
 int z4c_set_tile(z4c_ctx* ctx, int ti, int tj, int tk) {
   if (!ctx) return fail(Z4C_EINVAL, "null context");
-  LaunchShape sh;
+  LaunchShape sh = ctx->shape;
   sh.point_threads = ti;
   sh.column_threads = tj;
   sh.column_slabs = tk;
@@ -1035,6 +1035,38 @@ int z4c_set_tile(z4c_ctx* ctx, int ti, int tj, int tk) {
                 "column threads 128/256/512, column slabs 0-4", ti, tj, tk);
   ctx->shape = sh;
   drop_graph(ctx);
+  return Z4C_OK;
+}
+
+int z4c_set_point_regs(z4c_ctx* ctx, int regs) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  if (regs != 0 && regs != kPointRegsHigh)
+    return fail(Z4C_EINVAL, "register budget %d: 0 or %d", regs, kPointRegsHigh);
+  if (ctx->shape.point_regs != regs) {
+    ctx->shape.point_regs = regs;
+    drop_graph(ctx);
+  }
+  return Z4C_OK;
+}
+
+int z4c_get_point_regs(const z4c_ctx* ctx, int* regs) {
+  if (!ctx || !regs) return fail(Z4C_EINVAL, "null argument");
+  *regs = ctx->shape.point_regs;
+  return Z4C_OK;
+}
+
+int z4c_set_contract(z4c_ctx* ctx, int on) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  if (ctx->shape.contract != (on != 0)) {
+    ctx->shape.contract = on != 0;
+    drop_graph(ctx);
+  }
+  return Z4C_OK;
+}
+
+int z4c_get_contract(const z4c_ctx* ctx, int* on) {
+  if (!ctx || !on) return fail(Z4C_EINVAL, "null argument");
+  *on = ctx->shape.contract;
   return Z4C_OK;
 }
 
@@ -1056,21 +1088,27 @@ int z4c_autotune(z4c_ctx* ctx, int reps, float* best_ms_out) {
   LaunchShape best = ctx->shape;
   float best_ms = 1e30f, ms = 0.f;
   int rc;
-  for (int pt : {64, 128, 256}) {
-    LaunchShape sh = best;
-    sh.point_threads = pt;
-    if ((rc = time_stage(ctx, sh, reps, &ms))) return rc;
-    if (ms < best_ms) {
-      best_ms = ms;
-      best.point_threads = pt;
+  for (int pt : {64, 128, 256})
+    for (int regs : {0, kPointRegsHigh}) {
+      if (regs && (pt == 256 || !has_fixed_geometry(ctx->g))) continue;
+      LaunchShape sh = best;
+      sh.point_threads = pt;
+      sh.point_regs = regs;
+      if ((rc = time_stage(ctx, sh, reps, &ms))) return rc;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best.point_threads = pt;
+        best.point_regs = regs;
+      }
     }
-  }
   for (int ct : {128, 256, 512})
     for (int ns : {0, 1, 2, 3, 4}) {
       LaunchShape sh = best;
       sh.column_threads = ct;
       sh.column_slabs = ns;
       if (ns > 0 && !slabs_fit(ctx->g, sh)) continue;
+      // the contracted path has no slab variant
+      if (ns > 0 && sh.contract && !ctx->g.has_sommerfeld) continue;
       if ((rc = time_stage(ctx, sh, reps, &ms))) return rc;
       if (ms < best_ms) {
         best_ms = ms;

@@ -9,6 +9,7 @@
 #include "z4c_common.cuh"
 #include "z4c_kernels.cuh"
 #include "z4c_rhs.cuh"
+#include "z4c_stencil.cuh"
 #include "z4c_weyl.cuh"
 
 namespace z4c {
@@ -91,8 +92,8 @@ k_prep(Grid gin, DevParams P, const double* __restrict__ u, double* __restrict__
 }
 
 // ---- first pass: Ricci tensor + conformal-factor part per interior vertex --
-template <int THREADS, int NX>
-__global__ void __launch_bounds__(THREADS, 1)
+template <int THREADS, int NX, int MINB = 1>
+__global__ void __launch_bounds__(THREADS, MINB)
 k_ricci(Grid gin, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
         double* __restrict__ rsum, int block0, int nblk) {
   const Grid g = fixed_geometry<NX>(gin);
@@ -112,108 +113,6 @@ k_ricci(Grid gin, DevParams P, const double* __restrict__ u, const double* __res
   for (int q = 0; q < 6; ++q) rs[(int64_t)q * npts] = R[q];
 }
 
-
-// ---- per-variable passes: advection sums and Kreiss-Oliger -------------------
-// One thread per (block, variable, interior (i, j)) column, looping over the
-// interior k.  Stencils along x and y read their lines directly; along z the
-// nine-vertex window slides in registers.  Index arithmetic is 32-bit (the
-// launcher checks that the thread count fits).
-struct Column {
-  int b, n, i, j;
-};
-__device__ __forceinline__ bool column_index(const Grid& g, int block0, int nblk, Column& c) {
-  const int n0 = g.nx[0] + 1, per = n0 * (g.nx[1] + 1);
-  const int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-  if (t >= per * NVAR * nblk) return false;
-  const int ij = t % per, rest = t / per;
-  c.n = rest % NVAR;
-  c.b = block0 + rest / NVAR;
-  c.i = NG + ij % n0;
-  c.j = NG + ij / n0;
-  return true;
-}
-
-// Loads for the stencil helpers below: read-only cache path for global
-// memory (GL = true), plain loads for shared memory.
-template <bool GL>
-__device__ __forceinline__ double ld(const double* p) {
-  if (GL) return __ldg(p);
-  return *p;
-}
-
-// Lop-sided advection along one direction (FDStencilBiased{Left,Right}<1,4,2>,
-// finite_differencing.tpp:175-191): only the side the sign of vx selects is
-// evaluated; its value is the reference's, which evaluates both and keeps one.
-template <bool GL = true>
-__device__ __forceinline__ double fd_lx_side(const double* __restrict__ u, int st, double vx,
-                                             double lidx) {
-  if (vx < 0) {
-    double dl = 0.;
-    dl += 1. * ld<GL>(u - 4 * st);
-    dl += -8. * ld<GL>(u - 3 * st);
-    dl += 30. * ld<GL>(u - 2 * st);
-    dl += -80. * ld<GL>(u - st);
-    dl += 35. * ld<GL>(u);
-    dl += 24. * ld<GL>(u + st);
-    dl += -2. * ld<GL>(u + 2 * st);
-    return (vx * dl) * lidx;
-  }
-  double dr = 0.;
-  dr += -1. * ld<GL>(u + 4 * st);
-  dr += 8. * ld<GL>(u + 3 * st);
-  dr += -30. * ld<GL>(u + 2 * st);
-  dr += 80. * ld<GL>(u + st);
-  dr += -35. * ld<GL>(u);
-  dr += -24. * ld<GL>(u - st);
-  dr += 2. * ld<GL>(u - 2 * st);
-  return (vx * dr) * lidx;
-}
-// The same along z from the window w[0..8] = f(k-4..k+4).
-__device__ __forceinline__ double fd_lx_window(const double w[9], double vx, double lidx) {
-  if (vx < 0) {
-    double dl = 0.;
-    dl += 1. * w[0];
-    dl += -8. * w[1];
-    dl += 30. * w[2];
-    dl += -80. * w[3];
-    dl += 35. * w[4];
-    dl += 24. * w[5];
-    dl += -2. * w[6];
-    return (vx * dl) * lidx;
-  }
-  double dr = 0.;
-  dr += -1. * w[8];
-  dr += 8. * w[7];
-  dr += -30. * w[6];
-  dr += 80. * w[5];
-  dr += -35. * w[4];
-  dr += -24. * w[3];
-  dr += 2. * w[2];
-  return (vx * dr) * lidx;
-}
-
-// Kreiss-Oliger along one direction (FDStencilCenteredDegreeEven<8,4>,
-// finite_differencing.tpp:335-368) from a line pointer or from the window.
-template <bool GL = true>
-__device__ __forceinline__ double fd_diss_line(const double* __restrict__ u, int st, double cidxd,
-                                               double diss) {
-  double out = 0.;
-  out += 1. * (ld<GL>(u - 4 * st) + ld<GL>(u + 4 * st));
-  out += -8. * (ld<GL>(u - 3 * st) + ld<GL>(u + 3 * st));
-  out += 28. * (ld<GL>(u - 2 * st) + ld<GL>(u + 2 * st));
-  out += -56. * (ld<GL>(u - st) + ld<GL>(u + st));
-  out += 70. * ld<GL>(u);
-  return out * cidxd * diss;
-}
-__device__ __forceinline__ double fd_diss_window(const double w[9], double cidxd, double diss) {
-  double out = 0.;
-  out += 1. * (w[0] + w[8]);
-  out += -8. * (w[1] + w[7]);
-  out += 28. * (w[2] + w[6]);
-  out += -56. * (w[3] + w[5]);
-  out += 70. * w[4];
-  return out * cidxd * diss;
-}
 
 // ---- Sommerfeld boundary right-hand side (Z4c::Z4cBoundaryRHS) -----------
 // z4c/boundary_conditions.cpp:16-174.  On a gr_sommerfeld face's vertex
@@ -293,21 +192,6 @@ k_sommerfeld(Grid g, DevParams P, const double* __restrict__ u, double* __restri
   rhs[q] = sommerfeld_value(g, P, b, n, u + q, i, j, k, g.s);
 }
 
-// Fills the z window of column c at the first interior k.
-__device__ __forceinline__ void window_init(const double* __restrict__ f, int sk, int k0,
-                                            double w[9]) {
-#pragma unroll
-  for (int q = 0; q < 8; ++q) w[q] = __ldg(f + (k0 - 4 + q) * sk);
-}
-__device__ __forceinline__ void window_advance(const double* __restrict__ f, int sk, int k,
-                                               double w[9]) {
-  w[8] = __ldg(f + (k + 4) * sk);
-}
-__device__ __forceinline__ void window_shift(double w[9]) {
-#pragma unroll
-  for (int q = 0; q < 8; ++q) w[q] = w[q + 1];
-}
-
 // Advection sums (calculate_z4c_rhs.cpp:184-226): lv [block][22][interior vertex]
 template <int UNROLL, int NX>
 __global__ void __launch_bounds__(kColumnMaxThreads)
@@ -339,17 +223,6 @@ k_adv(Grid gin, DevParams P, const double* __restrict__ u, double* __restrict__ 
     out[(k - NG) * n0 * n1] = acc;
     window_shift(w);
   }
-}
-
-// Kreiss-Oliger added to one right-hand-side value in the reference's
-// order, rhs += Diss_x; rhs += Diss_y; rhs += Diss_z (:908-915).
-__device__ __forceinline__ double add_ko_column(double r, const double* __restrict__ fo, int nn0,
-                                                const double w[9], const FdScale& F,
-                                                double diss) {
-  r += fd_diss_line(fo, 1, F.cidxd[0], diss);
-  r += fd_diss_line(fo, nn0, F.cidxd[1], diss);
-  r += fd_diss_window(w, F.cidxd[2], diss);
-  return r;
 }
 
 // Z4cRHS tail: rhs += KO, in place.
@@ -406,21 +279,8 @@ k_ko_stage_ls(Grid gin, DevParams P, const double* __restrict__ u,
     const double r = (som && on_sommerfeld_face(g, P, c.b, c.i, c.j, k))
                          ? sommerfeld_value(g, P, c.b, c.n, f + o, c.i, c.j, k, g.s)
                          : add_ko_column(__ldg(rhs + q), f + o, nn0, win, F, P.p.diss);
-    const double un = win[4];
-    double v1 = w.u1_zero ? 0.0 : u1[q];
-    if (w.delta != 0.0) v1 += w.delta * un;  // w0 == 1, w2 == 0 branch
-    double v;
-    if (w.gamma1 == 1.0) {  // gamma3 == 0 for every 2S integrator accepted
-      v = un;
-      if (w.gamma2 != 0.0) v += w.gamma2 * v1;
-    } else if (w.gamma1 == 0.0) {
-      if (w.gamma2 == 1.0) v = v1;
-      else v = w.gamma2 * v1;
-    } else {
-      if (w.gamma2 != 0.0) v = w.gamma1 * un + w.gamma2 * v1;
-      else v = un * w.gamma1;
-    }
-    v += w.beta_dt * r;
+    double v1, v;
+    ls_update(w, win[4], w.u1_zero ? 0.0 : u1[q], r, v1, v);
     u1[q] = v1;
     u_out[q] = v;
     window_shift(win);
@@ -589,21 +449,8 @@ k_ko_stage_ls_slab(Grid g, DevParams P, const double* __restrict__ u,
     const double r = (som && on_sommerfeld_face(g, P, b, i, j, k))
                          ? sommerfeld_value<false>(g, P, b, n, v, i, j, k, sst)
                          : add_ko_slab(__ldg(rhs + qq), v, nn0, pl, F, P.p.diss);
-    const double un = *v;
-    double v1 = w.u1_zero ? 0.0 : u1[qq];
-    if (w.delta != 0.0) v1 += w.delta * un;  // w0 == 1, w2 == 0 branch
-    double x;
-    if (w.gamma1 == 1.0) {  // gamma3 == 0 for every 2S integrator accepted
-      x = un;
-      if (w.gamma2 != 0.0) x += w.gamma2 * v1;
-    } else if (w.gamma1 == 0.0) {
-      if (w.gamma2 == 1.0) x = v1;
-      else x = w.gamma2 * v1;
-    } else {
-      if (w.gamma2 != 0.0) x = w.gamma1 * un + w.gamma2 * v1;
-      else x = un * w.gamma1;
-    }
-    x += w.beta_dt * r;
+    double v1, x;
+    ls_update(w, *v, w.u1_zero ? 0.0 : u1[qq], r, v1, x);
     u1[qq] = v1;
     u_out[qq] = x;
   }
@@ -671,8 +518,8 @@ k_ko_rhs_slab(Grid g, DevParams P, const double* __restrict__ u, double* __restr
 }
 
 // ---- main pass: the right-hand side without the Kreiss-Oliger terms -------
-template <int THREADS, int NX>
-__global__ void __launch_bounds__(THREADS, 1)
+template <int THREADS, int NX, int MINB = 1>
+__global__ void __launch_bounds__(THREADS, MINB)
 k_main(Grid gin, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
        const double* __restrict__ rsum, const double* __restrict__ lv, double* __restrict__ rhs,
        int block0, int nblk) {
@@ -1377,7 +1224,8 @@ static int64_t columns(const Grid& g, int nblk) {
 }
 
 bool valid_shape(const LaunchShape& sh) {
-  return (sh.point_threads == 64 || sh.point_threads == 128 || sh.point_threads == 256) &&
+  return (sh.point_regs == 0 || sh.point_regs == kPointRegsHigh) &&
+         (sh.point_threads == 64 || sh.point_threads == 128 || sh.point_threads == 256) &&
          (sh.column_threads == 128 || sh.column_threads == 256 ||
           sh.column_threads == 512) &&
          (sh.column_slabs >= 0 && sh.column_slabs <= 4);
@@ -1421,26 +1269,38 @@ int allow_slab_smem() {
   return (int)e;
 }
 
-template <int T>
+// MINB: CTAs per SM the heavy passes are compiled for (1: up to 255
+// registers per thread; kPointMinb(T): 168, three resident CTAs of 128 or
+// six of 64, for 1.5x the warps at a few dozen bytes of spill).
+template <int T, int MINB>
 static void launch_point_passes_t(const Grid& g, const DevParams& P, const double* u,
                                   const RhsScratch& sc, double* rhs, int block0, int nblk,
                                   int which, cudaStream_t st) {
   const int64_t n = interior_count(g) * nblk;
   COUNTED
   if (which == 0)
-    (has_fixed_geometry(g) ? k_ricci<T, kFixedNX> : k_ricci<T, 0>)<<<div_up(n, T), T, 0, st>>>(
+    (has_fixed_geometry(g) ? k_ricci<T, kFixedNX, MINB> : k_ricci<T, 0, MINB>)<<<div_up(n, T), T,
+                                                                                0, st>>>(
         g, P, u, sc.sd, sc.rsum, block0, nblk);
   else
-    (has_fixed_geometry(g) ? k_main<T, kFixedNX> : k_main<T, 0>)<<<div_up(n, T), T, 0, st>>>(
+    (has_fixed_geometry(g) ? k_main<T, kFixedNX, MINB> : k_main<T, 0, MINB>)<<<div_up(n, T), T,
+                                                                              0, st>>>(
         g, P, u, sc.sd, sc.rsum, sc.lv, rhs, block0, nblk);
 }
 static void launch_point_pass(const Grid& g, const DevParams& P, const double* u,
                               const RhsScratch& sc, double* rhs, int block0, int nblk, int which,
                               const LaunchShape& sh, cudaStream_t st) {
+  const bool hi = sh.point_regs == kPointRegsHigh && has_fixed_geometry(g);
   switch (sh.point_threads) {
-    case 64: launch_point_passes_t<64>(g, P, u, sc, rhs, block0, nblk, which, st); break;
-    case 256: launch_point_passes_t<256>(g, P, u, sc, rhs, block0, nblk, which, st); break;
-    default: launch_point_passes_t<128>(g, P, u, sc, rhs, block0, nblk, which, st); break;
+    case 64:
+      if (hi) launch_point_passes_t<64, 6>(g, P, u, sc, rhs, block0, nblk, which, st);
+      else launch_point_passes_t<64, 1>(g, P, u, sc, rhs, block0, nblk, which, st);
+      break;
+    case 256: launch_point_passes_t<256, 1>(g, P, u, sc, rhs, block0, nblk, which, st); break;
+    default:
+      if (hi) launch_point_passes_t<128, 3>(g, P, u, sc, rhs, block0, nblk, which, st);
+      else launch_point_passes_t<128, 1>(g, P, u, sc, rhs, block0, nblk, which, st);
+      break;
   }
 }
 
@@ -1493,6 +1353,10 @@ void launch_prep_ricci(const Grid& g, const DevParams& P, const double* u, const
 
 void launch_rhs(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                 double* rhs, int block0, int nblk, const LaunchShape& sh, cudaStream_t st) {
+  if (sh.contract && !g.has_sommerfeld) {
+    launch_rhs_fast(g, P, u, sc, rhs, block0, nblk, sh, st);
+    return;
+  }
   launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, sh, st);
   size_t smem;
   const SlabGeom S = slab_geom(g, sh, &smem);
@@ -1511,6 +1375,10 @@ void launch_rhs(const Grid& g, const DevParams& P, const double* u, const RhsScr
 void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                      double* rhs, double* u1, double* u_out, const LsStage& w, int block0,
                      int nblk, const LaunchShape& sh, cudaStream_t st) {
+  if (sh.contract && !g.has_sommerfeld) {
+    launch_stage_ls_fast(g, P, u, sc, rhs, u1, u_out, w, block0, nblk, sh, st);
+    return;
+  }
   launch_rhs_passes(g, P, u, sc, rhs, block0, nblk, sh, st);
   size_t smem;
   const SlabGeom S = slab_geom(g, sh, &smem);

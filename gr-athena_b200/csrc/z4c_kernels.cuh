@@ -68,10 +68,22 @@ constexpr int kSdComponents = 33;
 // passes (128, 256, 512) and the number of z-slabs per block in which those
 // passes stage a variable in shared memory (1-4; 0 or a slab whose planes do
 // not fit: global-memory pencils instead).
+// contract: the contracted path (z4c_fast.cu) on meshes without
+// gr_sommerfeld faces: floating-point contraction, the advection sums and the
+// Kreiss-Oliger terms added in one pass, the stage update fused with the main
+// pass; the right-hand side agrees with the exact path to round-off instead
+// of bit for bit.
+// point_regs: register budget of the heavy per-vertex passes on fixed-geometry
+// meshes: 0 (up to 255 per thread, two CTAs of 128 per SM) or
+// kPointRegsHigh (168: three CTAs of 128 or six of 64 per SM, 1.5x the
+// resident warps); point_threads 256 always takes 255.
+constexpr int kPointRegsHigh = 168;
 struct LaunchShape {
   int point_threads = 128;
   int column_threads = 128;
   int column_slabs = 0;
+  int contract = 0;
+  int point_regs = 0;
 };
 bool valid_shape(const LaunchShape& sh);
 // Whether the shape's slabs fit in shared memory on this grid.
@@ -98,6 +110,18 @@ void launch_prep(const Grid& g, const DevParams& P, const double* u, double* sd,
 void launch_stage_ls(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                      double* rhs, double* u1, double* u_out, const LsStage& w, int block0,
                      int nblk, const LaunchShape& sh, cudaStream_t st);
+// The contracted path (LaunchShape::contract): four launches, stored first
+// derivatives (exact), Ricci, the main pass into rhs without the advection
+// sums and Kreiss-Oliger, then one column pass that adds both and runs the
+// stage update (launch_stage_ls_fast) or writes the right-hand side back
+// (launch_rhs_fast).  Not for meshes with gr_sommerfeld faces (the launchers
+// above fall back to the exact path).
+void launch_stage_ls_fast(const Grid& g, const DevParams& P, const double* u,
+                          const RhsScratch& sc, double* rhs, double* u1, double* u_out,
+                          const LsStage& w, int block0, int nblk, const LaunchShape& sh,
+                          cudaStream_t st);
+void launch_rhs_fast(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
+                     double* rhs, int block0, int nblk, const LaunchShape& sh, cudaStream_t st);
 void launch_stage_bt(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                      double* rhs, const double* un, double* const* k, double* u_out,
                      const BtStage& w, int block0, int nblk, const LaunchShape& sh,

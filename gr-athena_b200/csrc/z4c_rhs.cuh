@@ -233,7 +233,10 @@ GATHER_LOOP
 
 // The 22 right-hand-side values at one interior vertex without the
 // Kreiss-Oliger terms, given Rsum_ab (rsum[q * stride]) and the advection sums
-// (lv[n * stride]).
+// (lv[n * stride]).  With LV = false the advection sums are left out (read
+// as zero; lv is not read): the contracted path adds them, scaled, with the
+// Kreiss-Oliger terms afterwards.
+template <bool LV = true>
 __device__ __forceinline__ void rhs_point(const double* __restrict__ u,
                                           const double* __restrict__ sd, int64_t nvol,
                                           int64_t p, const int64_t s[3],
@@ -372,7 +375,10 @@ GATHER_LOOP
 #pragma unroll
   for (int a = 0; a < 3; ++a) beta_u[a] = __ldg(UV(Z4C_BETAX + a));
   // the advection sums, each read where it enters (lv[n * stride])
-  auto Lv = [&](int n) { return __ldg(lv + (int64_t)n * stride); };
+  auto Lv = [&](int n) {
+    if constexpr (LV) return __ldg(lv + (int64_t)n * stride);
+    else return 0.0;
+  };
   double LGam_u[3], Lg_dd[6], LA_dd[6];
 
   // finalize Lie derivatives, :619-687

@@ -57,7 +57,8 @@ EXPORTS = (
     "z4c_restart_info", "z4c_restart_text", "z4c_restart_read", "z4c_restart_write_host",
     "z4c_restart_load", "z4c_restart_save", "z4c_adj_setup", "z4c_tlm_step", "z4c_adj_step",
     "z4c_adj_objective", "z4c_adj_objective_adj", "z4c_adj_params", "z4c_adj_gradient",
-    "z4c_adj_adm_to_z4c")
+    "z4c_adj_adm_to_z4c", "z4c_set_contract", "z4c_get_contract", "z4c_set_point_regs",
+    "z4c_get_point_regs")
 
 
 class Z4cError(RuntimeError):
@@ -148,6 +149,10 @@ def lib():
         L.z4c_set_per_block.argtypes = [vp, ip]
         L.z4c_set_tile.argtypes = [vp, ip, ip, ip]
         L.z4c_get_tile.argtypes = [vp, C.POINTER(C.c_int)]
+        L.z4c_set_contract.argtypes = [vp, ip]
+        L.z4c_get_contract.argtypes = [vp, C.POINTER(C.c_int)]
+        L.z4c_set_point_regs.argtypes = [vp, ip]
+        L.z4c_get_point_regs.argtypes = [vp, C.POINTER(C.c_int)]
         L.z4c_autotune.argtypes = [vp, ip, C.POINTER(C.c_float)]
         L.z4c_check_finite.argtypes = [vp, ip]
         L.z4c_rhs_stage.argtypes = [vp, ip, C.c_double]
@@ -658,6 +663,25 @@ class Z4c:
         """Launch shape of the RHS passes (see z4c_set_tile)."""
         _check(lib().z4c_set_tile(self._h, int(point_threads), int(column_threads),
                                   int(column_slabs)))
+
+    def set_contract(self, on=True):
+        """Contracted right-hand side on or off (see z4c_set_contract)."""
+        _check(lib().z4c_set_contract(self._h, int(bool(on))))
+
+    def set_point_regs(self, regs):
+        """Register budget of the heavy RHS passes (0 or 168, see
+        z4c_set_point_regs)."""
+        _check(lib().z4c_set_point_regs(self._h, int(regs)))
+
+    def get_point_regs(self):
+        v = C.c_int()
+        _check(lib().z4c_get_point_regs(self._h, C.byref(v)))
+        return v.value
+
+    def get_contract(self):
+        v = C.c_int()
+        _check(lib().z4c_get_contract(self._h, C.byref(v)))
+        return bool(v.value)
 
     def get_tile(self):
         t = (C.c_int * 3)()

@@ -356,7 +356,9 @@ class AdaptiveEvolution:
     trackers: starting points of the puncture trackers (the refinement
     criterion's punctures).  `tile`, when set (point_threads,
     column_threads, column_slabs, e.g. an autotuner's pick), is the launch
-    shape of every context the run creates.  `initial` may instead be a
+    shape of every context the run creates, `point_regs` and `contract`
+    their register budget and right-hand-side path (see Z4c.set_point_regs,
+    Z4c.set_contract).  `initial` may instead be a
     callable load(ctx) that fills the first context's Z4c state itself
     (pass load=True)."""
 
@@ -370,6 +372,8 @@ class AdaptiveEvolution:
         self.history = history
         self.stream = stream
         self.tile = None
+        self.point_regs = 0
+        self.contract = False
         self.start = [tuple(float(v) for v in p) for p in trackers]
         self.ncycle = 0
         self.nregrid = 0
@@ -399,6 +403,8 @@ class AdaptiveEvolution:
             ctx.set_stream(self.stream)
         if self.tile is not None:
             ctx.set_tile(*self.tile)
+        ctx.set_point_regs(self.point_regs)
+        ctx.set_contract(self.contract)
         return ctx
 
     def _regrid(self):

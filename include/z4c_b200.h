@@ -360,6 +360,27 @@ int z4c_set_per_block(z4c_ctx *ctx, int per_block);
  * Z4C_EINVAL.  Results do not depend on the shape. */
 int z4c_set_tile(z4c_ctx *ctx, int ti, int tj, int tk);
 int z4c_get_tile(const z4c_ctx *ctx, int tile_out[3]);
+/* Contracted right-hand side (no reference counterpart): with on != 0 every
+ * later z4c_rhs, stage and step of the context takes the contracted path:
+ * floating-point contraction (fused multiply-adds), the advection sums and
+ * the Kreiss-Oliger terms added in one per-variable pass, and the stage
+ * update fused with the main right-hand-side pass, four launches per stage.
+ * Its right-hand side agrees with the exact path's (which matches the
+ * reference bit for bit) to round-off, within the 1e-12 relative bound per
+ * evaluation; meshes with gr_sommerfeld faces and the Butcher integrator keep
+ * the exact path.  Off by default; switching drops the captured step graph,
+ * and the autotuner times the path that is switched on. */
+int z4c_set_contract(z4c_ctx *ctx, int on);
+/* Register budget of the heavy per-vertex right-hand-side passes on meshes of
+ * 16^3 MeshBlocks (no reference counterpart): 0 lets them use up to 255
+ * registers per thread (two CTAs of 128 threads per SM), 168 compiles them
+ * for three CTAs of 128 or six of 64 per SM (1.5x the resident warps for a
+ * few dozen bytes of spill); 256-thread CTAs always take 255.  The arithmetic
+ * is the same either way.  The autotuner tries both; switching drops the
+ * captured step graph. */
+int z4c_set_point_regs(z4c_ctx *ctx, int regs);
+int z4c_get_point_regs(const z4c_ctx *ctx, int *regs);
+int z4c_get_contract(const z4c_ctx *ctx, int *on);
 /* Autotuner (no reference counterpart): times one fused low-storage stage on
  * the context's current state for each candidate shape (the Ricci/main CTA
  * size first, then the column-pass shape; reps timed launches each after a
