@@ -46,6 +46,7 @@ namespace z4c {
 
 using refine::RefGeom;
 constexpr int kMlNcg = Z4C_NCG;
+constexpr int kMlUnpackThreads = 512;
 
 namespace {
 
@@ -75,42 +76,49 @@ __device__ __forceinline__ int ml_zone(int i, int vs, int ve) {
   return i < vs ? 0 : i == vs ? 1 : i < mid ? 2 : i == mid ? 3 : i < ve ? 4 : i == ve ? 5 : 6;
 }
 
-// SetBoundaries of one receiving block and variable as a gather: each vertex
-// starts at the block's own value (interior) or zero (ghosts), takes its
-// zone's contributions in the reference's neighbour order (add, or copy for
-// data from a coarser block) and is multiplied by the inverse node
-// multiplicity of the zone; once for the fine array, once for the coarse
-// buffer.  A warp walks rows of the array, its lanes along i.
-__global__ void k_ml_unpack(MlPlan P, const double* __restrict__ src, double* __restrict__ dst,
-                            int reg_nvar) {
-  const int b = blockIdx.x, n = blockIdx.y, arr = blockIdx.z;  // arr: 0 fine, 1 coarse
+// SetBoundaries of one receiving block as a gather, every variable at once:
+// each vertex starts at the block's own value (interior) or zero (ghosts),
+// takes its zone's contributions in the reference's neighbour order (add, or
+// copy for data from a coarser block) and is multiplied by the inverse node
+// multiplicity of the zone; blockIdx.y selects the fine array (0) or the
+// coarse buffer (1).  The vertex's zone, multiplicity and contribution range
+// are found once and serve all nvar variables, whose loads are independent
+// of one another; the threads of a warp take consecutive vertices.
+__global__ void __launch_bounds__(kMlUnpackThreads)
+k_ml_unpack(MlPlan P, const double* __restrict__ src, double* __restrict__ dst, int nvar,
+            int reg_nvar) {
+  const int b = blockIdx.x, arr = blockIdx.y;  // arr: 0 fine, 1 coarse
   __shared__ unsigned char mult[343];
-  __shared__ int zs[1][344];
+  __shared__ int zs[344];
   extern __shared__ MlContrib sc[];  // this array's contributions
   for (int q = threadIdx.x; q < 343; q += blockDim.x) mult[q] = P.mult[(int64_t)b * 343 + q];
   for (int q = threadIdx.x; q < 344; q += blockDim.x)
-    zs[0][q] = P.zstart[((int64_t)b * 2 + arr) * 344 + q];
+    zs[q] = P.zstart[((int64_t)b * 2 + arr) * 344 + q];
   __syncthreads();
-  const int c0 = zs[0][0], nc = zs[0][343] - c0;
+  const int c0 = zs[0], nc = zs[343] - c0;
   for (int q = threadIdx.x; q < nc; q += blockDim.x) sc[q] = P.contrib[c0 + q];
   __syncthreads();
-  {
-    const int ng = arr ? Z4C_NCG : NG;
-    const int d0 = arr ? P.cn[0] : P.nn[0], d1 = arr ? P.cn[1] : P.nn[1];
-    const int v0 = ng + (arr ? P.nx[0] / 2 : P.nx[0]), v1 = ng + (arr ? P.nx[1] / 2 : P.nx[1]),
-              v2 = ng + (arr ? P.nx[2] / 2 : P.nx[2]);
-    const int vol = (int)(arr ? P.cvol : P.fvol);
-    const double* own = arr ? P.csrc + ((int64_t)b * Z4C_NVAR + n) * vol
-                            : src + ((int64_t)b * reg_nvar + n) * vol;
-    double* out = arr ? P.coarse + ((int64_t)b * Z4C_NVAR + n) * vol
-                      : dst + ((int64_t)b * reg_nvar + n) * vol;
-    for (int p = threadIdx.x; p < vol; p += blockDim.x) {
-      const int i = p % d0, row = p / d0, j = row % d1, k = row / d1;
-      const int zi = ml_zone(i, ng, v0), zj = ml_zone(j, ng, v1), zk = ml_zone(k, ng, v2);
-      const int z = (zk * 7 + zj) * 7 + zi;
-      const bool in = zi >= 1 && zi <= 5 && zj >= 1 && zj <= 5 && zk >= 1 && zk <= 5;
-      double v = in ? __ldg(own + p) : 0.0;
-      for (int q = zs[0][z] - c0; q < zs[0][z + 1] - c0; ++q) {
+  const int ng = arr ? Z4C_NCG : NG;
+  const int d0 = arr ? P.cn[0] : P.nn[0], d1 = arr ? P.cn[1] : P.nn[1];
+  const int v0 = ng + (arr ? P.nx[0] / 2 : P.nx[0]), v1 = ng + (arr ? P.nx[1] / 2 : P.nx[1]),
+            v2 = ng + (arr ? P.nx[2] / 2 : P.nx[2]);
+  const int64_t vol = arr ? P.cvol : P.fvol;
+  // variable stride of the arrays read and written
+  const int64_t vs = vol;
+  const double* own = arr ? P.csrc + (int64_t)b * Z4C_NVAR * vol : src + (int64_t)b * reg_nvar * vol;
+  double* out = arr ? P.coarse + (int64_t)b * Z4C_NVAR * vol : dst + (int64_t)b * reg_nvar * vol;
+  for (int p = threadIdx.x; p < vol; p += blockDim.x) {
+    const int i = p % d0, row = p / d0, j = row % d1, k = row / d1;
+    const int zi = ml_zone(i, ng, v0), zj = ml_zone(j, ng, v1), zk = ml_zone(k, ng, v2);
+    const int z = (zk * 7 + zj) * 7 + zi;
+    const bool in = zi >= 1 && zi <= 5 && zj >= 1 && zj <= 5 && zk >= 1 && zk <= 5;
+    const int qb = zs[z] - c0, qe = zs[z + 1] - c0;
+    const int m = mult[z];
+    const double inv = m > 1 ? P.inv[m] : 1.0;
+#pragma unroll 2
+    for (int n = 0; n < nvar; ++n) {
+      double v = in ? __ldg(own + n * vs + p) : 0.0;
+      for (int q = qb; q < qe; ++q) {
         const MlContrib c = sc[q];
         const int64_t sv = c.scoarse ? P.cvol : P.fvol;
         const double* s = c.scoarse ? P.csrc + ((int64_t)c.sblk * Z4C_NVAR + n) * sv
@@ -119,9 +127,8 @@ __global__ void k_ml_unpack(MlPlan P, const double* __restrict__ src, double* __
         const double x = __ldg(s + ((k + c.d[2]) * s1 + j + c.d[1]) * s0 + i + c.d[0]);
         v = c.mode == kMlCopy ? x : v + x;
       }
-      const int m = mult[z];
-      if (m > 1) v *= P.inv[m];
-      out[p] = v;
+      if (m > 1) v *= inv;
+      out[n * vs + p] = v;
     }
   }
 }
@@ -800,7 +807,7 @@ int launch_ml_exchange(const MlPlan& P, const double* src, double* dst, int nvar
       cudaFuncSetAttribute(k_ml_unpack, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
     return set_error(Z4C_ECUDA, "multilevel exchange: shared memory for the contribution lists");
-  k_ml_unpack<<<dim3(P.nblocks, nvar, 2), 256, smem, st>>>(P, src, dst, reg_nvar);
+  k_ml_unpack<<<dim3(P.nblocks, 2), kMlUnpackThreads, smem, st>>>(P, src, dst, nvar, reg_nvar);
   ++launches;
   auto bc_axis = [&](int lv, double* arr, int64_t bstride, int64_t vol, const int* dims, int ng) {
     for (int a = 0; a < 3; ++a) {
