@@ -277,11 +277,13 @@ struct StageW {
 // shift adjoint of the advection sums and the stage algebra.  Writes the
 // channels, the Ricci-sum adjoints, the direct adjoint of u at the vertex and
 // the adjoint of u1; parameter adjoints per CTA into part.
+template <int NX>
 __global__ void __launch_bounds__(kThreads)
-k_adj_main(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
+k_adj_main(Grid gin, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
            const double* __restrict__ rsum, const double* __restrict__ wbar,
            double* __restrict__ u1bar, double* __restrict__ direct, double* __restrict__ chan,
            double* __restrict__ rsb, double* __restrict__ part, StageW W) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double pe = 0., pk = 0.;
@@ -386,9 +388,11 @@ k_adj_main(Grid g, DevParams P, const double* __restrict__ u, const double* __re
 // Per interior vertex: the adjoint of the shift through the advection sums,
 // sum_n lvbar_n dlv_n/dbeta^a = lidx_a sum_n adv_n beta dt wbar_n L_a f_n,
 // added to the direct adjoint (the upwind side of the linearisation point).
+template <int NX>
 __global__ void __launch_bounds__(kThreads)
-k_adj_advbeta(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ wbar,
+k_adj_advbeta(Grid gin, DevParams P, const double* __restrict__ u, const double* __restrict__ wbar,
               double* __restrict__ direct, double beta_dt) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts * g.nblocks) return;
@@ -417,10 +421,12 @@ k_adj_advbeta(Grid g, DevParams P, const double* __restrict__ u, const double* _
 
 // Per interior vertex: the reverse of the Ricci part (ricci_local_adj) given
 // the Ricci-sum adjoints; adds to the channels and the direct adjoint.
+template <int NX>
 __global__ void __launch_bounds__(kThreads)
-k_adj_ricci(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
+k_adj_ricci(Grid gin, DevParams P, const double* __restrict__ u, const double* __restrict__ sd,
             const double* __restrict__ rsb, double* __restrict__ direct,
             double* __restrict__ chan) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts * g.nblocks) return;
@@ -477,8 +483,10 @@ __device__ __forceinline__ bool in_sd_region(const Grid& g, int dir, int i, int 
 // Adjoint of the stored first derivatives: the vertex's own channel plus the
 // transposed outer derivative of every mixed second derivative that reads it.
 // One thread per (block, component, vertex of the component's region).
+template <int NX>
 __global__ void __launch_bounds__(kThreads)
-k_adj_sdbar(Grid g, DevParams P, const double* __restrict__ chan, double* __restrict__ sdbar) {
+k_adj_sdbar(Grid gin, DevParams P, const double* __restrict__ chan, double* __restrict__ sdbar) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int comp = blockIdx.y, b = blockIdx.z;
   const int slot = comp / 3, dir = comp % 3;
   const int ex = (dir >= 1) ? 3 : 0, ey = (dir == 2) ? 3 : 0;
@@ -515,10 +523,12 @@ k_adj_sdbar(Grid g, DevParams P, const double* __restrict__ chan, double* __rest
 // reach the vertex form one range of offsets, clamped once, and the weights
 // that depend on p only (upwind side, shift, Kreiss-Oliger) are shared by
 // the variables.
+template <int NX>
 __global__ void __launch_bounds__(kThreads)
-k_adj_gather(Grid g, DevParams P, const double* __restrict__ u, const double* __restrict__ wbar,
+k_adj_gather(Grid gin, DevParams P, const double* __restrict__ u, const double* __restrict__ wbar,
              const double* __restrict__ direct, const double* __restrict__ chan,
              const double* __restrict__ sdbar, double* __restrict__ ubar, double beta_dt) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int64_t nv = g.nvol;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nv * g.nblocks) return;
@@ -610,8 +620,10 @@ k_adj_gather(Grid g, DevParams P, const double* __restrict__ u, const double* __
 
 // AlgConstr^T at every vertex: ubar (adjoint after) -> adjoint before, at the
 // pre-constraint state upre.
+template <int NX>
 __global__ void __launch_bounds__(kThreads)
-k_adj_alg(Grid g, DevParams P, const double* __restrict__ upre, double* __restrict__ ubar) {
+k_adj_alg(Grid gin, DevParams P, const double* __restrict__ upre, double* __restrict__ ubar) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int64_t nv = g.nvol;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nv * g.nblocks) return;
@@ -716,8 +728,10 @@ __device__ __forceinline__ int grid_neighbour(const Grid& g, int b, const int d[
 // each axis an interior index i has the images i, i + nx and i - nx where
 // they lie in [0, nn) (a neighbour's interior or ghost entry); one thread per (block, interior
 // vertex) forms the images once and sums all 22 variables.
+template <int NX>
 __global__ void __launch_bounds__(kThreads)
-k_adj_exchange(Grid g, const double* __restrict__ ubar, double* __restrict__ wbar) {
+k_adj_exchange(Grid gin, const double* __restrict__ ubar, double* __restrict__ wbar) {
+  const Grid g = fixed_geometry<NX>(gin);
   const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npts * g.nblocks) return;
@@ -1309,10 +1323,10 @@ int adj_step(z4c_ctx* c, double dt, const double* u) {
   const int nthr = div_up(npts * g.nblocks, kThreads);
   for (int s = 4; s >= 1; --s) {
     // AlgConstr^T then E^T: adjoint of this stage's output w
-    k_adj_alg<<<div_up(g.nvol * g.nblocks, kThreads), kThreads, 0, c->stream>>>(g, P, A->upre[s - 1],
+    (has_fixed_geometry(g) ? k_adj_alg<kFixedNX> : k_adj_alg<0>)<<<div_up(g.nvol * g.nblocks, kThreads), kThreads, 0, c->stream>>>(g, P, A->upre[s - 1],
                                                                              A->adj);
     adj_physical_bcs(g, A->adj, c->stream);
-    k_adj_exchange<<<div_up(npts * g.nblocks, kThreads), kThreads, 0, c->stream>>>(
+    (has_fixed_geometry(g) ? k_adj_exchange<kFixedNX> : k_adj_exchange<0>)<<<div_up(npts * g.nblocks, kThreads), kThreads, 0, c->stream>>>(
         g, A->adj, A->wbar);
     ALAUNCH("adjoint exchange");
     add_kernel_launches(2);
@@ -1328,16 +1342,16 @@ int adj_step(z4c_ctx* c, double dt, const double* u) {
     ALAUNCH("prep_ricci");
     const double* wt = kLsRk4[s - 1];
     StageW W{wt[0], wt[1], wt[2], wt[4] * dt, s == 1 ? 1 : 0};
-    k_adj_main<<<nthr, kThreads, 0, c->stream>>>(g, P, us, c->sd, c->rsum, A->wbar, A->adj1,
+    (has_fixed_geometry(g) ? k_adj_main<kFixedNX> : k_adj_main<0>)<<<nthr, kThreads, 0, c->stream>>>(g, P, us, c->sd, c->rsum, A->wbar, A->adj1,
                                                  A->direct, A->chan, A->rsb, A->part, W);
     k_accumulate<<<1, 256, 0, c->stream>>>(A->part, nthr, A->pacc);
     ALAUNCH("adjoint main");
-    k_adj_ricci<<<nthr, kThreads, 0, c->stream>>>(g, P, us, c->sd, A->rsb, A->direct, A->chan);
-    k_adj_advbeta<<<nthr, kThreads, 0, c->stream>>>(g, P, us, A->wbar, A->direct, W.beta_dt);
+    (has_fixed_geometry(g) ? k_adj_ricci<kFixedNX> : k_adj_ricci<0>)<<<nthr, kThreads, 0, c->stream>>>(g, P, us, c->sd, A->rsb, A->direct, A->chan);
+    (has_fixed_geometry(g) ? k_adj_advbeta<kFixedNX> : k_adj_advbeta<0>)<<<nthr, kThreads, 0, c->stream>>>(g, P, us, A->wbar, A->direct, W.beta_dt);
     const int64_t creg = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7) * (g.nx[2] + 1);
-    k_adj_sdbar<<<dim3(div_up(creg, kThreads), kSdComponents, g.nblocks), kThreads, 0, c->stream>>>(
+    (has_fixed_geometry(g) ? k_adj_sdbar<kFixedNX> : k_adj_sdbar<0>)<<<dim3(div_up(creg, kThreads), kSdComponents, g.nblocks), kThreads, 0, c->stream>>>(
         g, P, A->chan, A->sdbar);
-    k_adj_gather<<<div_up(g.nvol * g.nblocks, kThreads), kThreads, 0, c->stream>>>(
+    (has_fixed_geometry(g) ? k_adj_gather<kFixedNX> : k_adj_gather<0>)<<<div_up(g.nvol * g.nblocks, kThreads), kThreads, 0, c->stream>>>(
         g, P, us, A->wbar, A->direct, A->chan, A->sdbar, A->adj, W.beta_dt);
     ALAUNCH("adjoint gather");
     add_kernel_launches(6);
@@ -1683,9 +1697,9 @@ extern "C" int z4c_adj_adm_to_z4c(z4c_ctx* c) {
   k_adj_alg_ghosts<<<nthr_all, kThreads, 0, c->stream>>>(g, P, A->upre[0], A->adj);
   adj_physical_bcs(g, A->adj, c->stream);
   ACUDA(cudaMemsetAsync(A->wbar, 0, bytes, c->stream));
-  k_adj_exchange<<<div_up(npts * g.nblocks, kThreads), kThreads, 0, c->stream>>>(g, A->adj,
+  (has_fixed_geometry(g) ? k_adj_exchange<kFixedNX> : k_adj_exchange<0>)<<<div_up(npts * g.nblocks, kThreads), kThreads, 0, c->stream>>>(g, A->adj,
                                                                                 A->wbar);
-  k_adj_alg<<<nthr_all, kThreads, 0, c->stream>>>(g, P, A->us, A->wbar);
+  (has_fixed_geometry(g) ? k_adj_alg<kFixedNX> : k_adj_alg<0>)<<<nthr_all, kThreads, 0, c->stream>>>(g, P, A->us, A->wbar);
   k_adj_adm_gam<<<nthr_all, kThreads, 0, c->stream>>>(g, P, A->wbar, A->gub);
   k_adj_adm_pt<<<nthr_all, kThreads, 0, c->stream>>>(g, c->reg[Z4C_REG_ADM], A->wbar, A->gub,
                                                      A->admbar);
