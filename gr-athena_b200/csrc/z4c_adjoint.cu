@@ -1188,6 +1188,7 @@ struct AdjState {
   double* pacc = nullptr;   // device accumulators of the shift_eta, damp_kappa1 adjoints
   double* admbar = nullptr; // adjoint of the ADM register (Z4C_REG_ADM_ADJ)
   double* gub = nullptr;    // adjoint of the inverse conformal metric of ADMToZ4c
+  int* pro_owner = nullptr; // refined meshes: the prolongation box that carries each fine vertex
   std::vector<double*> snaps;  // revolve snapshots
 };
 
@@ -1201,6 +1202,7 @@ void adj_free(AdjState* a) {
     if (p) cudaFree(p);
   for (double* p : a->snaps)
     if (p) cudaFree(p);
+  if (a->pro_owner) cudaFree(a->pro_owner);
   delete a;
 }
 
@@ -1233,7 +1235,6 @@ int64_t npts_of(const Grid& g) { return (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) *
 
 int check_ctx(z4c_ctx* c) {
   if (!c) return err(Z4C_EINVAL, "null context");
-  if (c->ml) return err(Z4C_ESTATE, "the adjoint runs on uniform meshes (no refined levels)");
   if (c->integrator != Z4C_INTEG_RK4) return err(Z4C_ESTATE, "the adjoint differentiates rk4 (2S)");
   if (c->g.has_sommerfeld) return err(Z4C_ESTATE, "the adjoint has no gr_sommerfeld faces");
 
@@ -1255,6 +1256,35 @@ void adj_physical_bcs(const Grid& g, double* ub, cudaStream_t st) {
   }
 }
 
+// The ghost fill of the step without AlgConstr (the same-level exchange and
+// the physical BCs, or the multilevel fill with its BCs): src's interiors to
+// every vertex of dst.
+int fill_fwd(z4c_ctx* c, const double* src, double* dst) {
+  if (c->ml) return launch_ml_exchange(*c->ml, src, dst, NVAR, NVAR, c->stream);
+  launch_exchange(c->g, c->dev(), src, dst, c->nbr, 0, c->stream);
+  launch_physical_bcs(c->g, dst, NVAR, c->stream);
+  ALAUNCH("exchange");
+  return Z4C_OK;
+}
+
+// Its transpose: ubar (the adjoint of every vertex after the fill) is
+// consumed; wbar receives the adjoint of the interiors, and zero ghosts
+// where the caller reads them (clear_ghosts; the multilevel transpose
+// clears wbar in any case).
+int fill_adj(z4c_ctx* c, double* ubar, double* wbar, bool clear_ghosts) {
+  const Grid& g = c->g;
+  if (c->ml)
+    return launch_ml_exchange_adj(*c->ml, ubar, wbar, c->adj->pro_owner, NVAR, NVAR, c->stream);
+  adj_physical_bcs(g, ubar, c->stream);
+  if (clear_ghosts)
+    ACUDA(cudaMemsetAsync(wbar, 0, sizeof(double) * c->adj->reg_elems, c->stream));
+  (has_fixed_geometry(g) ? k_adj_exchange<kFixedNX> : k_adj_exchange<0>)<<<
+      div_up(npts_of(g) * g.nblocks, kThreads), kThreads, 0, c->stream>>>(g, ubar, wbar);
+  ALAUNCH("adjoint exchange");
+  add_kernel_launches(1);
+  return Z4C_OK;
+}
+
 // Forward stage s (1-based) from u (stage input, all vertices) and u1: w,
 // u1 updated, then E(w) -> upre (no constraint), AlgConstr(upre) -> uout.
 int fwd_stage(z4c_ctx* c, int s, double dt, const double* u, double* u1, double* w, double* upre,
@@ -1265,10 +1295,8 @@ int fwd_stage(z4c_ctx* c, int s, double dt, const double* u, double* u1, double*
   launch_stage_ls(c->g, P, u, c->scratch(), c->reg[Z4C_REG_RHS], u1, w, ls, 0, c->g.nblocks,
                   c->shape, c->stream);
   ALAUNCH("stage");
-  launch_exchange(c->g, P, w, upre, c->nbr, 0, c->stream);
-  ALAUNCH("exchange");
-  launch_physical_bcs(c->g, upre, NVAR, c->stream);
-  ALAUNCH("physical_bcs");
+  int rc = fill_fwd(c, w, upre);
+  if (rc) return rc;
   if (uout) {
     if (uout != upre)
       ACUDA(cudaMemcpyAsync(uout, upre, sizeof(double) * c->adj->reg_elems,
@@ -1325,11 +1353,9 @@ int adj_step(z4c_ctx* c, double dt, const double* u) {
     // AlgConstr^T then E^T: adjoint of this stage's output w
     (has_fixed_geometry(g) ? k_adj_alg<kFixedNX> : k_adj_alg<0>)<<<div_up(g.nvol * g.nblocks, kThreads), kThreads, 0, c->stream>>>(g, P, A->upre[s - 1],
                                                                              A->adj);
-    adj_physical_bcs(g, A->adj, c->stream);
-    (has_fixed_geometry(g) ? k_adj_exchange<kFixedNX> : k_adj_exchange<0>)<<<div_up(npts * g.nblocks, kThreads), kThreads, 0, c->stream>>>(
-        g, A->adj, A->wbar);
-    ALAUNCH("adjoint exchange");
-    add_kernel_launches(2);
+    add_kernel_launches(1);
+    int rc = fill_adj(c, A->adj, A->wbar, false);
+    if (rc) return rc;
     // the stage input
     const double* us = u;
     if (s > 1) {
@@ -1523,6 +1549,17 @@ int z4c_adj_setup(z4c_ctx* c) {
       z4c::adj_free(A);
       return err(Z4C_ECUDA, "adjoint buffer clear");
     }
+  if (c->ml) {  // the prolongation owners of the ghost fill's transpose
+    if (cudaMalloc((void**)&A->pro_owner, sizeof(int) * g.nvol * g.nblocks) != cudaSuccess) {
+      cudaGetLastError();
+      z4c::adj_free(A);
+      return err(Z4C_ENOMEM, "prolongation owner table");
+    }
+    if (launch_ml_prolong_owner(*c->ml, A->pro_owner, c->stream) != Z4C_OK) {
+      z4c::adj_free(A);
+      return err(Z4C_ECUDA, "prolongation owner table");
+    }
+  }
   c->adj = A;
   c->reg[Z4C_REG_TAN] = A->tan;
   c->reg[Z4C_REG_ADJ] = A->adj;
@@ -1551,9 +1588,8 @@ int z4c_tlm_step(z4c_ctx* c, double dt) {
     // values
     rc = fwd_stage(c, s, dt, u, A->u1, A->w, A->us, nullptr);
     if (rc) return rc;
-    launch_exchange(g, P, A->tanw, A->tan, c->nbr, 0, c->stream);
-    launch_physical_bcs(g, A->tan, NVAR, c->stream);
-    ALAUNCH("tangent exchange");
+    rc = fill_fwd(c, A->tanw, A->tan);
+    if (rc) return rc;
     // (A->us, A->tan) are the pre-constraint state and its tangent
     ACUDA(cudaMemcpyAsync(A->tanw, A->tan, sizeof(double) * A->reg_elems, cudaMemcpyDeviceToDevice,
                           c->stream));
@@ -1690,15 +1726,11 @@ extern "C" int z4c_adj_adm_to_z4c(z4c_ctx* c) {
   ALAUNCH("adm_to_z4c");
   ACUDA(cudaMemcpyAsync(A->w, A->us, bytes, cudaMemcpyDeviceToDevice, c->stream));
   launch_alg_constr(g, P, A->w, 0, g.nblocks, c->stream);
-  launch_exchange(g, P, A->w, A->upre[0], c->nbr, 0, c->stream);
-  launch_physical_bcs(g, A->upre[0], NVAR, c->stream);
-  ALAUNCH("ghost fill");
+  ALAUNCH("alg_constr");
+  if ((rc = fill_fwd(c, A->w, A->upre[0]))) return rc;
   // reverse: AlgConstr on the ghosts, the ghost fill, AlgConstr, the map
   k_adj_alg_ghosts<<<nthr_all, kThreads, 0, c->stream>>>(g, P, A->upre[0], A->adj);
-  adj_physical_bcs(g, A->adj, c->stream);
-  ACUDA(cudaMemsetAsync(A->wbar, 0, bytes, c->stream));
-  (has_fixed_geometry(g) ? k_adj_exchange<kFixedNX> : k_adj_exchange<0>)<<<div_up(npts * g.nblocks, kThreads), kThreads, 0, c->stream>>>(g, A->adj,
-                                                                                A->wbar);
+  if ((rc = fill_adj(c, A->adj, A->wbar, true))) return rc;
   (has_fixed_geometry(g) ? k_adj_alg<kFixedNX> : k_adj_alg<0>)<<<nthr_all, kThreads, 0, c->stream>>>(g, P, A->us, A->wbar);
   k_adj_adm_gam<<<nthr_all, kThreads, 0, c->stream>>>(g, P, A->wbar, A->gub);
   k_adj_adm_pt<<<nthr_all, kThreads, 0, c->stream>>>(g, c->reg[Z4C_REG_ADM], A->wbar, A->gub,

@@ -198,6 +198,160 @@ __global__ void k_ml_prolong(MlPlan P, double* __restrict__ dst, int reg_nvar) {
   }
 }
 
+// ---- transpose of the ghost fill (the adjoint of a step on refined meshes) --
+// The fill is linear in the blocks' interiors.  Its transpose runs the
+// pieces backwards: fine BCs, prolongation, coarse BCs, unpack, restriction,
+// each transposed.  Adjoint contributions from several receivers meet at one
+// source value, so the unpack and the prolongation scatter with atomic adds
+// (their sums are exact up to the order of the additions).
+
+// ExtrapolateOutflowBC transposed along one column: the ghosts in reverse
+// order push their adjoint to the five values each was formed from, and
+// lose it (the forward overwrote them).
+template <int AX>
+__global__ void k_ml_bc_adj(const MlBc* __restrict__ items, double* __restrict__ arr,
+                            int64_t bstride, int64_t vol, int d0, int d1, int ng) {
+  const MlBc it = items[blockIdx.x];
+  const int n = blockIdx.y;
+  constexpr int o1 = AX == 0 ? 1 : 0, o2 = AX == 2 ? 1 : 2;
+  const int64_t st[3] = {1, d0, (int64_t)d0 * d1};
+  const int w1 = it.hi[o1] - it.lo[o1] + 1, w2 = it.hi[o2] - it.lo[o2] + 1;
+  double* a = arr + (int64_t)it.blk * bstride + (int64_t)n * vol;
+  const int dir = it.outer ? -1 : 1;
+  constexpr double c[5] = {5., -10., 10., -5., 1.};
+  for (int t = threadIdx.x; t < w1 * w2; t += blockDim.x) {
+    const int t1 = it.lo[o1] + t % w1, t2 = it.lo[o2] + t / w1;
+    for (int g = ng; g >= 1; --g) {
+      const int ia = it.outer ? it.hi[AX] + g : it.lo[AX] - g;
+      const int64_t p = (int64_t)ia * st[AX] + (int64_t)t1 * st[o1] + (int64_t)t2 * st[o2];
+      const int64_t s = dir * st[AX];
+      const double y = a[p];
+      a[p] = 0.0;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) a[p + (q + 1) * s] += c[q] * y;
+    }
+  }
+}
+
+// For every fine vertex a prolongation box writes, the first box (in plan
+// order) of its block that writes it: the one whose transpose carries it.
+__global__ void k_ml_prolong_owner(MlPlan P, int* __restrict__ owner) {
+  const RefGeom G = P.pro[blockIdx.x];
+  const int b = P.pro_blk[blockIdx.x];
+  const int nf[3] = {G.fe[0] - G.f0[0] + 1, G.fe[1] - G.f0[1] + 1, G.fe[2] - G.f0[2] + 1};
+  const int total = nf[0] * nf[1] * nf[2];
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int f[3] = {G.f0[0] + t % nf[0], G.f0[1] + (t / nf[0]) % nf[1],
+                      G.f0[2] + t / (nf[0] * nf[1])};
+    int c[3];
+    bool ok = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const bool prl = (f[a] & 1) != 0;
+      c[a] = (prl ? (f[a] - 1) : f[a]) / 2 + refine::HNC;
+      ok &= prl ? (c[a] >= G.sp[a] && c[a] < G.ep[a])
+                : (c[a] >= G.box[2 * a] && c[a] <= G.box[2 * a + 1]);
+    }
+    if (ok)
+      atomicMin(owner + (int64_t)b * P.fvol + ((int64_t)f[2] * G.nn[1] + f[1]) * G.nn[0] + f[0],
+                (int)blockIdx.x);
+  }
+}
+
+// ProlongateVertexCenteredValues transposed: each fine vertex a box owns
+// moves its adjoint into the coarse buffer's adjoint and loses it.
+__global__ void k_ml_prolong_adj(MlPlan P, double* __restrict__ fbar, const int* __restrict__ owner,
+                                 int reg_nvar) {
+  const RefGeom G = P.pro[blockIdx.x];
+  const int b = P.pro_blk[blockIdx.x], n = blockIdx.y;
+  double* Cb = P.coarse + ((int64_t)b * Z4C_NVAR + n) * P.cvol;
+  double* F = fbar + ((int64_t)b * reg_nvar + n) * P.fvol;
+  const int* O = owner + (int64_t)b * P.fvol;
+  const int nf[3] = {G.fe[0] - G.f0[0] + 1, G.fe[1] - G.f0[1] + 1, G.fe[2] - G.f0[2] + 1};
+  const int total = nf[0] * nf[1] * nf[2];
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int f[3] = {G.f0[0] + t % nf[0], G.f0[1] + (t / nf[0]) % nf[1],
+                      G.f0[2] + t / (nf[0] * nf[1])};
+    const int64_t q = ((int64_t)f[2] * G.nn[1] + f[1]) * G.nn[0] + f[0];
+    if (O[q] != (int)blockIdx.x) continue;
+    const double a = F[q];
+    if (refine::prolong_adj(G, Cb, f, a)) F[q] = 0.0;
+  }
+}
+
+// The unpack transposed: the adjoint y of every receiving vertex, times 1/m,
+// goes to the contributions in reverse list order until one that copied
+// (everything before it was overwritten), and then to the vertex's own value
+// when no copy intervened.  Sources are the fine arrays' adjoint (wbar) or
+// the restricted snapshot's adjoint (P.csrc); the receiving coarse buffers'
+// adjoint is P.coarse.
+__global__ void __launch_bounds__(kMlUnpackThreads)
+k_ml_unpack_adj(MlPlan P, const double* __restrict__ ybar, double* __restrict__ wbar, int nvar,
+                int reg_nvar) {
+  const int b = blockIdx.x, arr = blockIdx.y;
+  __shared__ unsigned char mult[343];
+  __shared__ int zs[344];
+  extern __shared__ MlContrib sc[];
+  for (int q = threadIdx.x; q < 343; q += blockDim.x) mult[q] = P.mult[(int64_t)b * 343 + q];
+  for (int q = threadIdx.x; q < 344; q += blockDim.x)
+    zs[q] = P.zstart[((int64_t)b * 2 + arr) * 344 + q];
+  __syncthreads();
+  const int c0 = zs[0], nc = zs[343] - c0;
+  for (int q = threadIdx.x; q < nc; q += blockDim.x) sc[q] = P.contrib[c0 + q];
+  __syncthreads();
+  const int ng = arr ? Z4C_NCG : NG;
+  const int d0 = arr ? P.cn[0] : P.nn[0], d1 = arr ? P.cn[1] : P.nn[1];
+  const int v0 = ng + (arr ? P.nx[0] / 2 : P.nx[0]), v1 = ng + (arr ? P.nx[1] / 2 : P.nx[1]),
+            v2 = ng + (arr ? P.nx[2] / 2 : P.nx[2]);
+  const int64_t vol = arr ? P.cvol : P.fvol;
+  const double* yb = arr ? P.coarse + (int64_t)b * Z4C_NVAR * vol : ybar + (int64_t)b * reg_nvar * vol;
+  double* own = arr ? P.csrc + (int64_t)b * Z4C_NVAR * vol : wbar + (int64_t)b * reg_nvar * vol;
+  for (int p = threadIdx.x; p < vol; p += blockDim.x) {
+    const int i = p % d0, row = p / d0, j = row % d1, k = row / d1;
+    const int zi = ml_zone(i, ng, v0), zj = ml_zone(j, ng, v1), zk = ml_zone(k, ng, v2);
+    const int z = (zk * 7 + zj) * 7 + zi;
+    const bool in = zi >= 1 && zi <= 5 && zj >= 1 && zj <= 5 && zk >= 1 && zk <= 5;
+    const int qb = zs[z] - c0, qe = zs[z + 1] - c0;
+    const int m = mult[z];
+    const double inv = m > 1 ? P.inv[m] : 1.0;
+    for (int n = 0; n < nvar; ++n) {
+      double a = yb[n * vol + p];
+      if (a == 0.0) continue;
+      if (m > 1) a *= inv;
+      bool copied = false;
+      for (int q = qe - 1; q >= qb; --q) {
+        const MlContrib c = sc[q];
+        const int64_t sv = c.scoarse ? P.cvol : P.fvol;
+        double* s = c.scoarse ? P.csrc + ((int64_t)c.sblk * Z4C_NVAR + n) * sv
+                              : wbar + ((int64_t)c.sblk * reg_nvar + n) * sv;
+        const int s0 = c.scoarse ? P.cn[0] : P.nn[0], s1 = c.scoarse ? P.cn[1] : P.nn[1];
+        atomicAdd(s + ((k + c.d[2]) * s1 + j + c.d[1]) * s0 + i + c.d[0], a);
+        if (c.mode == kMlCopy) {
+          copied = true;
+          break;
+        }
+      }
+      if (!copied && in) atomicAdd(own + n * vol + p, a);
+    }
+  }
+}
+
+// RestrictInterior transposed: the snapshot's adjoint back onto the fine
+// vertices it was injected from.
+__global__ void k_ml_restrict_adj(MlPlan P, double* __restrict__ wbar, int nvar, int reg_nvar) {
+  const int c0 = P.nx[0] / 2 + 1, c1 = P.nx[1] / 2 + 1, c2 = P.nx[2] / 2 + 1;
+  const int64_t per = (int64_t)c0 * c1 * c2;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= per * nvar * P.nblocks) return;
+  const int64_t r = t % per;
+  const int n = (int)((t / per) % nvar), b = (int)(t / (per * nvar));
+  const int ci = kMlNcg + (int)(r % c0), cj = kMlNcg + (int)((r / c0) % c1),
+            ck = kMlNcg + (int)(r / ((int64_t)c0 * c1));
+  const int i = 2 * (ci - kMlNcg) + NG, j = 2 * (cj - kMlNcg) + NG, k = 2 * (ck - kMlNcg) + NG;
+  wbar[((int64_t)b * reg_nvar + n) * P.fvol + ((int64_t)k * P.nn[1] + j) * P.nn[0] + i] +=
+      P.csrc[((int64_t)b * Z4C_NVAR + n) * P.cvol + ((int64_t)ck * P.cn[1] + cj) * P.cn[0] + ci];
+}
+
 // ---- host plan -------------------------------------------------------------
 
 struct Loc {
@@ -825,6 +979,65 @@ int launch_ml_exchange(const MlPlan& P, const double* src, double* dst, int nvar
     ++launches;
   }
   bc_axis(0, dst, (int64_t)reg_nvar * P.fvol, P.fvol, P.nn, NG);
+  add_kernel_launches(launches);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(Z4C_ECUDA, cudaGetErrorString(e));
+  return Z4C_OK;
+}
+
+int launch_ml_prolong_owner(const MlPlan& P, int* owner, cudaStream_t st) {
+  if (cudaMemsetAsync(owner, 0x7f, sizeof(int) * (size_t)P.fvol * P.nblocks, st) != cudaSuccess)
+    return set_error(Z4C_ECUDA, "multilevel transpose: owner table");
+  if (P.npro > 0) {
+    k_ml_prolong_owner<<<P.npro, 128, 0, st>>>(P, owner);
+    add_kernel_launches(1);
+  }
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? Z4C_OK : set_error(Z4C_ECUDA, cudaGetErrorString(e));
+}
+
+int launch_ml_exchange_adj(const MlPlan& P, double* ubar, double* wbar, const int* owner, int nvar,
+                           int reg_nvar, cudaStream_t st) {
+  if (nvar < 1 || nvar > Z4C_NVAR || reg_nvar < nvar)
+    return set_error(Z4C_EINVAL, "multilevel transpose: bad variable count");
+  long long launches = 0;
+  auto bc_axis = [&](int lv, double* arr, int64_t bstride, int64_t vol, const int* dims, int ng) {
+    for (int a = 2; a >= 0; --a) {
+      if (!P.nbc[lv][a]) continue;
+      const dim3 grid(P.nbc[lv][a], nvar);
+      if (a == 0) k_ml_bc_adj<0><<<grid, 128, 0, st>>>(P.bc[lv][a], arr, bstride, vol, dims[0], dims[1], ng);
+      else if (a == 1) k_ml_bc_adj<1><<<grid, 128, 0, st>>>(P.bc[lv][a], arr, bstride, vol, dims[0], dims[1], ng);
+      else k_ml_bc_adj<2><<<grid, 128, 0, st>>>(P.bc[lv][a], arr, bstride, vol, dims[0], dims[1], ng);
+      ++launches;
+    }
+  };
+  // fine BCs, then prolongation, in reverse
+  bc_axis(0, ubar, (int64_t)reg_nvar * P.fvol, P.fvol, P.nn, NG);
+  const size_t cbytes = sizeof(double) * (size_t)Z4C_NVAR * P.cvol * P.nblocks;
+  if (cudaMemsetAsync(P.coarse, 0, cbytes, st) != cudaSuccess ||
+      cudaMemsetAsync(P.csrc, 0, cbytes, st) != cudaSuccess ||
+      cudaMemsetAsync(wbar, 0, sizeof(double) * (size_t)reg_nvar * P.fvol * P.nblocks, st) !=
+          cudaSuccess)
+    return set_error(Z4C_ECUDA, "multilevel transpose: clearing the adjoints");
+  if (P.npro > 0) {
+    k_ml_prolong_adj<<<dim3(P.npro, nvar), 128, 0, st>>>(P, ubar, owner, reg_nvar);
+    ++launches;
+  }
+  bc_axis(1, P.coarse, (int64_t)Z4C_NVAR * P.cvol, P.cvol, P.cn, kMlNcg);
+  const size_t smem = sizeof(MlContrib) * (size_t)std::max(P.max_block_contrib, 1);
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(k_ml_unpack_adj, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return set_error(Z4C_ECUDA, "multilevel transpose: shared memory for the contribution lists");
+  k_ml_unpack_adj<<<dim3(P.nblocks, 2), kMlUnpackThreads, smem, st>>>(P, ubar, wbar, nvar,
+                                                                      reg_nvar);
+  ++launches;
+  {
+    const int64_t n = (int64_t)(P.nx[0] / 2 + 1) * (P.nx[1] / 2 + 1) * (P.nx[2] / 2 + 1) * nvar *
+                      P.nblocks;
+    k_ml_restrict_adj<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, wbar, nvar, reg_nvar);
+    ++launches;
+  }
   add_kernel_launches(launches);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(Z4C_ECUDA, cudaGetErrorString(e));

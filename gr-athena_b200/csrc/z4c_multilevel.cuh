@@ -80,6 +80,14 @@ void ml_free(MlPlan& plan);
 // the blocks' interiors, dst receives interiors and ghosts.
 int launch_ml_exchange(const MlPlan& plan, const double* src, double* dst, int nvar, int reg_nvar,
                        cudaStream_t st);
+// The transpose of launch_ml_exchange (the adjoint of a ghost fill): ubar, the
+// adjoint of dst (every vertex), is consumed in place; wbar receives the
+// adjoint of src (the interiors; ghosts zero).  The plan's coarse buffers
+// serve as scratch.  owner: the prolongation owner table that
+// launch_ml_prolong_owner fills (an int per fine vertex of every block).
+int launch_ml_exchange_adj(const MlPlan& plan, double* ubar, double* wbar, const int* owner,
+                           int nvar, int reg_nvar, cudaStream_t st);
+int launch_ml_prolong_owner(const MlPlan& plan, int* owner, cudaStream_t st);
 // The root level of a root grid of nroot blocks per axis.
 int ml_root_level(const int nroot[3]);
 

@@ -113,6 +113,52 @@ __device__ __forceinline__ bool prolong_value(const RefGeom& G, const double* __
   return true;
 }
 
+// Transpose of prolong_value: Cb (the coarse array's adjoint, one variable)
+// += the weight of every coarse value in the interpolation of fine vertex f
+// times a (f's adjoint).  Atomic adds: fine vertices of one box share coarse
+// values.  Returns false where prolong_value writes nothing.
+__device__ __forceinline__ bool prolong_adj(const RefGeom& G, double* __restrict__ Cb,
+                                            const int f[3], double a) {
+  int c[3];
+  bool prl[3];
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    prl[ax] = (f[ax] & 1) != 0;
+    c[ax] = (prl[ax] ? (f[ax] - 1) : f[ax]) / 2 + HNC;
+    const bool ok = prl[ax] ? (c[ax] >= G.sp[ax] && c[ax] < G.ep[ax])
+                            : (c[ax] >= G.box[2 * ax] && c[ax] <= G.box[2 * ax + 1]);
+    if (!ok) return false;
+  }
+  auto add = [&](int k, int j, int i, double w) {
+    atomicAdd(Cb + ((int64_t)k * G.cn[1] + j) * G.cn[0] + i, w);
+  };
+  // per axis the taps (index, weight): the vertex itself where injected, the
+  // 2 HSZ symmetric Lagrange taps where interpolated
+  int idx[3][2 * HSZ];
+  double wt[3][2 * HSZ];
+  int nt[3];
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    if (!prl[ax]) {
+      idx[ax][0] = c[ax];
+      wt[ax][0] = 1.0;
+      nt[ax] = 1;
+    } else {
+      for (int d = 0; d < HSZ; ++d) {
+        idx[ax][2 * d] = c[ax] - d;
+        idx[ax][2 * d + 1] = c[ax] + d + 1;
+        wt[ax][2 * d] = wt[ax][2 * d + 1] = lag3(HSZ - d - 1);
+      }
+      nt[ax] = 2 * HSZ;
+    }
+  }
+  for (int tk = 0; tk < nt[2]; ++tk)
+    for (int tj = 0; tj < nt[1]; ++tj)
+      for (int ti = 0; ti < nt[0]; ++ti)
+        add(idx[2][tk], idx[1][tj], idx[0][ti], a * (wt[2][tk] * wt[1][tj] * wt[0][ti]));
+  return true;
+}
+
 inline int setup(const int nx[3], int nvar, int nblocks, const int box[6], RefGeom& G, bool prolong) {
   if (!nx || !box) return set_error(Z4C_EINVAL, "refinement operator: null argument");
   if (nvar < 1 || nblocks < 1) return set_error(Z4C_EINVAL, "refinement operator: empty input");

@@ -459,14 +459,19 @@ int z4c_regrid(z4c_ctx *dst, const z4c_ctx *src);
  * exchange and AlgConstr), and of the objective J = sum over blocks of the
  * cell volume times the sum over the history cells of H^2, H the Hamiltonian
  * constraint of ADMConstraints after Z4cToADM (the H-norm of
- * outputs/history.cpp:168-200).  Uniform meshes with periodic and
+ * outputs/history.cpp:168-200).  Uniform and statically refined meshes
+ * (on the latter the transpose of the multilevel ghost fill: fine-level BCs,
+ * prolongation, coarse-level BCs, the contribution-list gather and the
+ * restriction, transposed; its scatters add atomically, so its sums are
+ * ordered differently from run to run) with periodic and
  * extrapolate_outflow faces (gr_sommerfeld faces are rejected), rk4,
  * chi_psi_power = -4.  The state's adjoint lives in Z4C_REG_ADJ and a
  * tangent in Z4C_REG_TAN, each over every vertex (ghosts included); the
  * adjoints of the gauge parameters shift_eta and damp_kappa1 accumulate in
  * the context.  The calls use the context's RHS register as scratch. */
 /* Allocates the tangent / adjoint buffers (about 13 state-sized registers
- * plus channel scratch) and zeroes Z4C_REG_TAN and Z4C_REG_ADJ. */
+ * plus channel scratch; on refined meshes also an int per vertex for the
+ * prolongation's transpose) and zeroes Z4C_REG_TAN and Z4C_REG_ADJ. */
 int z4c_adj_setup(z4c_ctx *ctx);
 /* One step of u (Z4C_REG_U) and of its tangent (Z4C_REG_TAN) together. */
 int z4c_tlm_step(z4c_ctx *ctx, double dt);
