@@ -121,7 +121,8 @@ def parse():
                     help="launch shape point_threads,column_threads,column_slabs instead of "
                          "the autotuner's pick (profiling under ncu, whose serialised launches "
                          "would mislead the autotuner)")
-    ap.add_argument("--workload", default="uniform", choices=["uniform", "bbh_smr", "bbh_amr"],
+    ap.add_argument("--workload", default="uniform",
+                    choices=["uniform", "bbh_smr", "bbh_amr", "bbh_adjoint"],
                     help="bbh_smr: binary punctures on a statically refined mesh of 7 levels; "
                          "bbh_amr: the adaptive run (separate measurements, not the headline "
                          "line)")
@@ -537,6 +538,105 @@ def amr_measure(steps, warmup, shift=(0.0, 0.0, 0.0), contract=1):
     }
 
 
+# The adjoint at scale: the binary of the adaptive runs on the same domain
+# and finest spacing, with 4^3 root MeshBlocks (dx 16) and 8 levels, refined
+# by Linf_box_in_box around the punctures at t = 0: 848 MeshBlocks.  (The
+# 3,424-block mesh of 8^3 roots does not fit: its context holds ~72 GB and
+# the adjoint's buffers ~13 state-sized registers of 9.4 GB more.)  The
+# gradient of the time-integrated H-norm over 400 steps with respect to the
+# masses, the separation and eta, revolve snapshots sized to the free HBM.
+ADJ_BBH = dict(nb=(4, 4, 4), nx=(16, 16, 16), xmin=(-512.0,) * 3, xmax=(512.0,) * 3,
+               numlevel=8, par_b=3.0, masses=(0.5, 0.5), separation=6.0, steps=400)
+
+
+def bbh_adjoint_measure(steps=None, fd=True):
+    """The revolve-checkpointed gradient on the refined binary mesh: J, the
+    four parameter derivatives (the state's adjoint chained through
+    ADMToZ4c and the host data's derivative), timings, snapshots; with fd a
+    central difference of the full forward run in eta as a check."""
+    import torch
+    import z4c_b200 as Z
+    from z4c_b200 import amr as A
+    from z4c_b200 import initial_data as ID
+    torch.cuda.set_device(0)
+    c = ADJ_BBH
+    steps = steps or c["steps"]
+    bc = Z.Mesh(c["nb"], c["nx"], c["xmin"], c["xmax"], "outflow").bc
+    ref = A.Refinement(c["nb"], c["nx"], c["xmin"], c["xmax"], bc, c["numlevel"], 10, c["par_b"])
+    off = (0.0625 * 0.37, 0.0625 * 0.21)
+
+    def centres(d):
+        return ((0.5 * d, off[0], off[1]), (-0.5 * d, -off[0], -off[1]))
+
+    ref.build_initial(centres(c["separation"]))
+    mesh = ref.mesh()
+    pdict = dict(PARAMS, eps_floor=-1.0)
+
+    def data(m, th):
+        return ID.punctures(m, Z.default_params(**pdict), masses=tuple(th[:2]),
+                            centres=centres(th[2]))
+
+    theta = np.array([c["masses"][0], c["masses"][1], c["separation"]])
+    ctx = Z.Z4c(mesh, Z.default_params(**pdict), "rk4")
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.adj_setup()
+    adm = data(mesh, theta)
+    dt = mesh.new_dt(CFL)
+    with torch.cuda.stream(stream):
+        ctx.upload(Z.REG_ADM, adm)
+        ctx.ADMToZ4c()
+        ctx.init_finalize()
+        u0 = ctx.download(Z.REG_U)
+        fwd = time_on(stream, lambda: ctx.evolve(dt, 1), 3)
+        ctx.upload(Z.REG_U, u0)
+        adj = time_on(stream, lambda: ctx.adj_step(dt), 2)
+        ctx.upload(Z.REG_U, u0)
+        nsnap = ctx.snapshots(steps)
+        J, pb, st = ctx.gradient(dt, steps, nsnap, w_final=0.0, w_step=dt)
+        ctx.upload(Z.REG_ADM, adm)
+        ctx.adj_adm_to_z4c()
+        ab = ctx.download(Z.REG_ADM_ADJ)
+    torch.cuda.synchronize()
+    grads = {}
+    for j, name in enumerate(("m1", "m2", "separation")):
+        e = np.zeros(3)
+        e[j] = 1e-6
+        dadm = (data(mesh, theta + e) - data(mesh, theta - e)) / 2e-6
+        grads[name] = float(np.sum(ab * dadm))
+    grads["eta"] = float(pb[0])
+    out = {"workload": "binary Brill-Lindquist punctures (m=0.5 each near (+-3,0,0)), "
+                       "[-512,512]^3, 4^3 root MeshBlocks of 16^3 cells, 8 levels refined by "
+                       "Linf_box_in_box (par_b 3) around the punctures at t=0, finest dx 1/8, "
+                       f"outflow, rk4, {steps} steps, objective dt * sum_k vol * sum H^2",
+           "meshblocks": mesh.nblocks, "steps": steps, "snapshots": nsnap,
+           "forward_step_ms": fwd, "adjoint_step_ms": adj, "adjoint_over_forward": adj / fwd,
+           "gradient_seconds": st["seconds"], "gradient_forward_steps": st["forward_steps"],
+           "gradient_adjoint_steps": st["adjoint_steps"], "objective": J, "gradient": grads}
+    ctx.close()
+    if fd:
+        # the full forward run at eta +- h (the objective reads the adjoint
+        # buffers' scratch, hence adj_setup)
+        def run_ctx(eta):
+            cr = Z.Z4c(mesh, Z.default_params(**dict(pdict, shift_eta=eta)), "rk4")
+            cr.set_stream(stream.cuda_stream)
+            cr.adj_setup()
+            with torch.cuda.stream(stream):
+                cr.upload(Z.REG_U, u0)
+                tot = 0.0
+                for _ in range(steps):
+                    cr.evolve(dt, 1)
+                    tot += dt * cr.objective()[0]
+            cr.close()
+            return tot
+        h = 1e-3
+        eta0 = pdict["shift_eta"]
+        fd_eta = (run_ctx(eta0 + h) - run_ctx(eta0 - h)) / (2 * h)
+        out["fd_eta"] = fd_eta
+        out["fd_eta_rel"] = abs(grads["eta"] - fd_eta) / abs(fd_eta)
+    return out
+
+
 def main_amr(args):
     print(json.dumps(amr_measure(args.steps, args.warmup, contract=args.contract)), flush=True)
     print(json.dumps(amr_measure(AMR_SHIFTED_STEPS, args.warmup, AMR_SHIFT,
@@ -631,6 +731,10 @@ def main():
         return main_smr(args)
     if args.workload == "bbh_amr":
         return main_amr(args)
+    if args.workload == "bbh_adjoint":
+        print(json.dumps(bbh_adjoint_measure(args.steps if args.steps != 60 else None)),
+              flush=True)
+        return
 
     import torch
     import torch.distributed as dist
@@ -867,6 +971,11 @@ def main():
                                                "exchange_ms", "exchange_share", "setup_s",
                                                "finite", "clocks")}
         line["bbh_smr"]["config"] = smr["config"]
+    if world == 1 and not args.no_adjoint:
+        # the gradient at scale on the refined binary mesh (40 of its 400 steps
+        # here; bench.py --workload bbh_adjoint runs all 400), with the check
+        # against differences of the full forward run in eta
+        line["adjoint"]["bbh_refined"] = bbh_adjoint_measure(40)
     if world == 1 and not args.no_amr:
         # the adaptive binary-puncture run: 200 cycles, block list changing
         keys = ("value", "unit", "ms_per_step", "steps", "initial_meshblocks",

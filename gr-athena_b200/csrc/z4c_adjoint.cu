@@ -1644,11 +1644,30 @@ int z4c_adj_params(z4c_ctx* c, double pbar[2], int reset) {
 
 }  // extern "C"
 
+extern "C" int z4c_adj_snapshots(z4c_ctx* c, int nsteps, int* nsnap) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (nsteps < 1 || !nsnap) return err(Z4C_EINVAL, "nsteps >= 1, nsnap non-null");
+  const size_t bytes = sizeof(double) * c->adj->reg_elems;
+  size_t free_b = 0, total_b = 0;
+  ACUDA(cudaMemGetInfo(&free_b, &total_b));
+  // keep 2 GiB and 2% of the device free for the library's other scratch
+  const size_t margin = (size_t)2 << 30;
+  const size_t keep = margin + total_b / 50;
+  const long long have = (long long)c->adj->snaps.size();
+  long long fit = free_b > keep ? (long long)((free_b - keep) / bytes) : 0;
+  fit += have - 2;  // the run and end-state buffers come first
+  if (fit < 0) return err(Z4C_ENOMEM, "revolve: no room for the run and end-state buffers");
+  *nsnap = (int)std::min<long long>(fit, nsteps - 1);
+  return Z4C_OK;
+}
+
 extern "C" int z4c_adj_gradient(z4c_ctx* c, double dt, int nsteps, int nsnap, double w_final,
                                 double w_step, double* J, double pbar[2], double stats[4]) {
   int rc = check_ctx(c);
   if (rc) return rc;
-  if (nsteps < 1 || nsnap < 0 || !J) return err(Z4C_EINVAL, "nsteps >= 1, nsnap >= 0, J non-null");
+  if (nsteps < 1 || !J) return err(Z4C_EINVAL, "nsteps >= 1, J non-null");
+  if (nsnap < 0 && (rc = z4c_adj_snapshots(c, nsteps, &nsnap))) return rc;
   z4c::AdjState* A = c->adj;
   const size_t bytes = sizeof(double) * A->reg_elems;
   const int S = std::min(nsnap, nsteps - 1);

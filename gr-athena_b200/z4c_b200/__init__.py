@@ -58,7 +58,7 @@ EXPORTS = (
     "z4c_restart_load", "z4c_restart_save", "z4c_adj_setup", "z4c_tlm_step", "z4c_adj_step",
     "z4c_adj_objective", "z4c_adj_objective_adj", "z4c_adj_params", "z4c_adj_gradient",
     "z4c_adj_adm_to_z4c", "z4c_set_contract", "z4c_get_contract", "z4c_set_point_regs",
-    "z4c_get_point_regs")
+    "z4c_get_point_regs", "z4c_adj_snapshots")
 
 
 class Z4cError(RuntimeError):
@@ -152,6 +152,7 @@ def lib():
         L.z4c_set_contract.argtypes = [vp, ip]
         L.z4c_get_contract.argtypes = [vp, C.POINTER(C.c_int)]
         L.z4c_set_point_regs.argtypes = [vp, ip]
+        L.z4c_adj_snapshots.argtypes = [vp, ip, C.POINTER(C.c_int)]
         L.z4c_get_point_regs.argtypes = [vp, C.POINTER(C.c_int)]
         L.z4c_autotune.argtypes = [vp, ip, C.POINTER(C.c_float)]
         L.z4c_check_finite.argtypes = [vp, ip]
@@ -788,9 +789,16 @@ class Z4c:
                                     int(reset)))
         return out
 
-    def gradient(self, dt, nsteps, nsnap, w_final=1.0, w_step=0.0):
+    def snapshots(self, nsteps):
+        """Revolve snapshots the free device memory holds for nsteps steps."""
+        v = C.c_int()
+        _check(lib().z4c_adj_snapshots(self._h, int(nsteps), C.byref(v)))
+        return v.value
+
+    def gradient(self, dt, nsteps, nsnap=-1, w_final=1.0, w_step=0.0):
         """dJ_total/du_0 into REG_ADJ with revolve checkpointing (nsnap
-        snapshots) for J_total = w_final J(u_n) + w_step sum_k J(u_k); returns
+        snapshots; -1: as many as free device memory holds) for
+        J_total = w_final J(u_n) + w_step sum_k J(u_k); returns
         (J_total, (d/d shift_eta, d/d damp_kappa1), stats)."""
         J = C.c_double()
         pb = np.zeros(2)

@@ -497,13 +497,20 @@ int z4c_adj_adm_to_z4c(z4c_ctx *ctx);
 int z4c_adj_params(z4c_ctx *ctx, double pbar[2], int reset);
 /* Gradient of J_total = w_final J(u_n) + w_step sum_{k=1..n} J(u_k) over n
  * steps from the state in Z4C_REG_U (left unchanged) with revolve-style
- * binomial checkpointing: nsnap state snapshots (device memory, allocated
- * for the call), a schedule that minimises the recomputed steps for that
+ * binomial checkpointing: nsnap state snapshots (device memory, kept in the
+ * context for later calls; nsnap < 0: as many as z4c_adj_snapshots finds
+ * room for), a schedule that minimises the recomputed steps for that
  * count.  On return Z4C_REG_ADJ holds dJ_total/du_0, pbar the parameter
  * adjoints, *J the objective; stats (may be NULL) receives {forward steps
- * recomputed, adjoint steps, seconds forward, seconds adjoint}. */
+ * (the first sweep and every recomputation), adjoint steps, seconds, the
+ * schedule's recomputed steps}. */
 int z4c_adj_gradient(z4c_ctx *ctx, double dt, int nsteps, int nsnap, double w_final,
                      double w_step, double *J, double pbar[2], double stats[4]);
+/* The number of revolve snapshots a gradient over nsteps steps can hold in
+ * the device memory that is free now (state-sized buffers; 2 GiB and 2% of
+ * the device are left over), at most nsteps - 1: the checkpointing sized to
+ * HBM. */
+int z4c_adj_snapshots(z4c_ctx *ctx, int nsteps, int *nsnap);
 
 /* ---- allocation-free variant ----------------------------------------------
  *
