@@ -1543,5 +1543,176 @@ Z4C_HD void adm_to_z4c_local(const T G[6], const T Kd[6], T* chi, T g[6], T* Kha
   inv3s(T(1.0) / detg3, g, guu);
 }
 
+
+// ---- psi4 of Z4cWeyl from its local inputs (the Weyl-scalar objective) ---
+Z4C_HD double ad_sqrt(double x) { return sqrt(x); }
+Z4C_HD Dual ad_sqrt(const Dual& x) {
+  const double r = sqrt(x.v);
+  return Dual(r, 0.5 * x.d / r);
+}
+
+// The inputs of weyl_point at one interior vertex (chi_psi_power = -4): the
+// conformal metric and chi, the ADM curvature and metric, the stored first
+// derivatives of chi and g~, the second derivatives (Dxx on the diagonal,
+// D_a of the stored D_b off it), and the first derivatives of the ADM
+// curvature.
+template <class T>
+struct WeylLocal {
+  T chi, gt[6];      // Z4c chi, g~_q
+  T Kd[6], gph[6];   // ADM K_q, gamma_q
+  T dchi[3];         // stored d_a chi
+  T dg3[3][6];       // stored d_c g~_q  [c][q]
+  T ddchi[6];        // d_a d_b chi, pair (a,b)
+  T ddg[6][6];       // d_a d_b g~_cd  [pair(a,b)][cd]
+  T dK[3][6];        // d_c K_q  [c][q]
+  static constexpr int N = 1 + 6 + 6 + 6 + 3 + 18 + 6 + 36 + 18;
+  Z4C_HD T* data() { return &chi; }
+  Z4C_HD const T* data() const { return &chi; }
+};
+
+// Re, Im psi4 of weyl_point (z4c/calculate_weyl_scalars.cpp:44-630) from
+// the local inputs, in its operation order, for T = double or Dual.
+template <class T>
+Z4C_HD void weyl_local(const z4c_params_t& opt, const WeylLocal<T>& v, double x1, double x2,
+                       double x3, T& rpsi4, T& ipsi4) {
+  const T chi_g = ad_max_c(v.chi, opt.chi_div_floor);
+  const T oochi = T(1.0) / chi_g;
+  T dg[3][6];
+  for (int c = 0; c < 3; ++c)
+    for (int q = 0; q < 6; ++q) dg[c][q] = oochi * (v.dg3[c][q] - oochi * v.gt[q] * v.dchi[c]);
+  T DDG[6][6];
+  for (int ab = 0; ab < 6; ++ab) {
+    const int a = ab < 3 ? 0 : (ab < 5 ? 1 : 2), b = ab < 3 ? ab : (ab < 5 ? ab - 2 : 2);
+    const T ddchi = v.ddchi[ab];
+    const T dchi_a = v.dchi[a], dchi_b = v.dchi[b];
+    for (int cd = 0; cd < 6; ++cd) {
+      const T gtil = v.gt[cd];
+      const T ddg_conf = v.ddg[ab][cd];
+      const T da3 = v.dg3[a][cd], db3 = v.dg3[b][cd];
+      T w;
+      if (a == b)
+        w = oochi * (ddg_conf - oochi * (2.0 * dchi_a * da3 + ddchi * gtil) +
+                     2.0 * oochi * oochi * dchi_a * dchi_a * gtil);
+      else
+        w = oochi * (ddg_conf - oochi * (dchi_a * db3 + dchi_b * da3 + ddchi * gtil) +
+                     2.0 * oochi * oochi * dchi_a * dchi_b * gtil);
+      DDG[ab][cd] = w;
+    }
+  }
+  T g_uu[6];
+  {
+    const T detg = det3s(v.gph);
+    inv3s(T(1.) / detg, v.gph, g_uu);
+  }
+  T Gddd[3][6], Gudd[3][6];
+  for (int c = 0; c < 3; ++c)
+    for (int a = 0; a < 3; ++a)
+      for (int b = a; b < 3; ++b)
+        Gddd[c][sid(a, b)] = 0.5 * (dg[a][sid(b, c)] + dg[b][sid(a, c)] - dg[c][sid(a, b)]);
+  for (int c = 0; c < 3; ++c)
+    for (int a = 0; a < 3; ++a)
+      for (int b = a; b < 3; ++b) {
+        T acc = T(0.0);
+        for (int d = 0; d < 3; ++d) acc += g_uu[sid(c, d)] * Gddd[d][sid(a, b)];
+        Gudd[c][sid(a, b)] = acc;
+      }
+  T Rd[6], R = T(0.0);
+  for (int a = 0; a < 3; ++a)
+    for (int b = a; b < 3; ++b) {
+      T acc = T(0.0);
+      for (int c = 0; c < 3; ++c)
+        for (int d = 0; d < 3; ++d) {
+          for (int e = 0; e < 3; ++e) {
+            acc += g_uu[sid(c, d)] * Gudd[e][sid(a, c)] * Gddd[e][sid(b, d)];
+            acc -= g_uu[sid(c, d)] * Gudd[e][sid(a, b)] * Gddd[e][sid(c, d)];
+          }
+          acc += 0.5 * g_uu[sid(c, d)] *
+                 (-DDG[sid(c, d)][sid(a, b)] - DDG[sid(a, b)][sid(c, d)] +
+                  DDG[sid(a, c)][sid(b, d)] + DDG[sid(b, c)][sid(a, d)]);
+        }
+      Rd[sid(a, b)] = acc;
+      R += wsym(a, b) * g_uu[sid(a, b)] * acc;
+    }
+  T K = T(0.0);
+  for (int a = 0; a < 3; ++a) {
+    T kaa = T(0.0);
+    for (int c = 0; c < 3; ++c) kaa += g_uu[sid(a, c)] * v.Kd[sid(c, a)];
+    K += kaa;
+  }
+  T DK[3][6];
+  for (int a = 0; a < 3; ++a)
+    for (int lo = 0; lo < 3; ++lo)
+      for (int hi = lo; hi < 3; ++hi) {
+        const int b = hi, c = lo;
+        T w = v.dK[a][sid(b, c)];
+        for (int d = 0; d < 3; ++d) {
+          w -= Gudd[d][sid(a, b)] * v.Kd[sid(d, c)];
+          w -= Gudd[d][sid(a, c)] * v.Kd[sid(b, d)];
+        }
+        DK[a][sid(lo, hi)] = w;
+      }
+  double xx = x1;
+  if (x1 * x1 + x2 * x2 < 1e-10) xx = xx + 1e-8;
+  T uv[3] = {T(xx), T(x2), T(x3)};
+  T vv[3] = {T(xx * x3), T(x2 * x3), T(-(xx * xx) - (x2 * x2))};
+  T wv[3] = {T(x2 * -1.0), T(xx), T(0.0)};
+  auto gdot = [&](const T* l, const T* r) -> T {
+    T acc = T(0.0);
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) acc += v.gph[sid(a, b)] * l[a] * r[b];
+    return acc;
+  };
+  T dot = gdot(wv, wv);
+  for (int a = 0; a < 3; ++a) wv[a] = wv[a] / ad_sqrt(dot);
+  dot = gdot(wv, uv);
+  for (int a = 0; a < 3; ++a) uv[a] -= dot * wv[a];
+  dot = gdot(uv, uv);
+  for (int a = 0; a < 3; ++a) uv[a] = uv[a] / ad_sqrt(dot);
+  dot = gdot(wv, vv);
+  const T dot2 = gdot(uv, vv);
+  for (int a = 0; a < 3; ++a) vv[a] -= dot * wv[a] + dot2 * uv[a];
+  dot = gdot(vv, vv);
+  for (int a = 0; a < 3; ++a) vv[a] = vv[a] / ad_sqrt(dot);
+  const double FR4 = 0.25;
+  T rp = T(0.0), ip = T(0.0);
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      T R4 = Rd[sid(a, b)] + K * v.Kd[sid(a, b)];
+      for (int c = 0; c < 3; ++c)
+        for (int d = 0; d < 3; ++d) R4 -= g_uu[sid(c, d)] * v.Kd[sid(a, c)] * v.Kd[sid(d, b)];
+      const T Tr = vv[a] * vv[b] - wv[a] * wv[b];
+      const T Ti = -vv[a] * wv[b] - wv[a] * vv[b];
+      rp += -FR4 * R4 * Tr;
+      ip += -FR4 * R4 * Ti;
+    }
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      const T Tr = vv[a] * vv[b] - wv[a] * wv[b];
+      const T Ti = -vv[a] * wv[b] - wv[a] * vv[b];
+      for (int c = 0; c < 3; ++c) {
+        const T R4 = -(DK[b][sid(a, c)] - DK[c][sid(a, b)]);
+        rp += 0.5 * R4 * uv[c] * Tr;
+        ip += 0.5 * R4 * uv[c] * Ti;
+      }
+    }
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      const T Tr = vv[a] * vv[b] - wv[a] * wv[b];
+      const T Ti = -vv[a] * wv[b] - wv[a] * vv[b];
+      for (int c = 0; c < 3; ++c)
+        for (int d = 0; d < 3; ++d) {
+          const T R4 = v.gph[sid(d, c)] * Rd[sid(a, b)] + v.gph[sid(a, b)] * Rd[sid(d, c)] -
+                       v.gph[sid(d, b)] * Rd[sid(a, c)] - v.gph[sid(a, c)] * Rd[sid(d, b)] -
+                       0.5 * R * (v.gph[sid(d, c)] * v.gph[sid(a, b)] -
+                                  v.gph[sid(d, b)] * v.gph[sid(a, c)]) +
+                       v.Kd[sid(d, c)] * v.Kd[sid(a, b)] - v.Kd[sid(d, b)] * v.Kd[sid(a, c)];
+          rp += -FR4 * R4 * uv[d] * uv[c] * Tr;
+          ip += -FR4 * R4 * uv[d] * uv[c] * Ti;
+        }
+    }
+  rpsi4 = rp;
+  ipsi4 = ip;
+}
+
 }  // namespace ad
 }  // namespace z4c

@@ -649,7 +649,7 @@ k_adj_alg(Grid gin, DevParams P, const double* __restrict__ upre, double* __rest
 // were y_g = 5 z1 - 10 z2 + 10 z3 - 5 z4 + z5 over the five values inward of
 // it, earlier ghosts included.  Their adjoints flow into those values in
 // reverse order; the overwritten values' own adjoints become zero.
-template <int AX>
+template <int AX, int NVB = NVAR>
 __global__ void __launch_bounds__(kThreads)
 k_adj_bc_axis(Grid g, double* __restrict__ ub) {
   constexpr int ax = AX;
@@ -658,13 +658,13 @@ k_adj_bc_axis(Grid g, double* __restrict__ ub) {
   const int64_t nt = (int64_t)g.nn[o1] * g.nn[o2];
   const int nfb = g.nb[o1] * g.nb[o2];
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nt * 2 * NVAR * nfb) return;
+  if (t >= nt * 2 * NVB * nfb) return;
   const int64_t tr = t % nt;
   int64_t r = t / nt;
   const int side = (int)(r % 2);
   r /= 2;
-  const int n = (int)(r % NVAR);
-  const int fb = (int)(r / NVAR);
+  const int n = (int)(r % NVB);
+  const int fb = (int)(r / NVB);
   int loc[3];
   loc[ax] = side ? g.nb[ax] - 1 : 0;
   loc[o1] = fb % g.nb[o1];
@@ -690,7 +690,7 @@ k_adj_bc_axis(Grid g, double* __restrict__ ub) {
   if (ax == 2) { lo[1] = is[1] - NG; hi[1] = ie[1] + NG; }
   const int t1 = (int)(tr % g.nn[o1]), t2 = (int)(tr / g.nn[o1]);
   if (t1 < lo[o1] || t1 > hi[o1] || t2 < lo[o2] || t2 > hi[o2]) return;
-  double* u = ub + ((int64_t)b * NVAR + n) * g.nvol + (int64_t)t1 * g.s[o1] + (int64_t)t2 * g.s[o2];
+  double* u = ub + ((int64_t)b * NVB + n) * g.nvol + (int64_t)t1 * g.s[o1] + (int64_t)t2 * g.s[o2];
   const int64_t st = g.s[ax];
   const int dir = side ? -1 : 1;
   const int ia0 = side ? ie[ax] + 1 : is[ax] - 1;
@@ -728,7 +728,7 @@ __device__ __forceinline__ int grid_neighbour(const Grid& g, int b, const int d[
 // each axis an interior index i has the images i, i + nx and i - nx where
 // they lie in [0, nn) (a neighbour's interior or ghost entry); one thread per (block, interior
 // vertex) forms the images once and sums all 22 variables.
-template <int NX>
+template <int NX, int NVB = NVAR>
 __global__ void __launch_bounds__(kThreads)
 k_adj_exchange(Grid gin, const double* __restrict__ ubar, double* __restrict__ wbar) {
   const Grid g = fixed_geometry<NX>(gin);
@@ -759,17 +759,204 @@ k_adj_exchange(Grid gin, const double* __restrict__ ubar, double* __restrict__ w
         if (nb < 0) continue;
         const int li = ijk[0] - d[0] * g.nx[0], lj = ijk[1] - d[1] * g.nx[1],
                   lk = ijk[2] - d[2] * g.nx[2];
-        off[nimg++] = (int64_t)nb * NVAR * nv + ((int64_t)lk * g.nn[1] + lj) * g.nn[0] + li;
+        off[nimg++] = (int64_t)nb * NVB * nv + ((int64_t)lk * g.nn[1] + lj) * g.nn[0] + li;
         if (is_interior(g, li, lj, lk)) ++m;
       }
   const double inv = 1.0 / (double)m;
   const int64_t p = ((int64_t)ijk[2] * g.nn[1] + ijk[1]) * g.nn[0] + ijk[0];
-  double* W = wbar + (int64_t)b * NVAR * nv + p;
-  for (int n = 0; n < NVAR; ++n) {
+  double* W = wbar + (int64_t)b * NVB * nv + p;
+  for (int n = 0; n < NVB; ++n) {
     double s = 0.;
     for (int q = 0; q < nimg; ++q) s += ubar[off[q] + (int64_t)n * nv];
     W[(int64_t)n * nv] = s * inv;
   }
+}
+
+// ---- the Weyl-scalar objective ---------------------------------------------
+// J_W = sum over the sphere's owned vertices p of w_p (Re psi4(p)^2 +
+// Im psi4(p)^2), w_p the vertex's quadrature weight: psi4 of Z4cWeyl after
+// Z4cToADM, the Weyl register's ghost fill and the sphere interpolation.  Its
+// adjoint runs the chain backwards: the interpolation and the ghost fill
+// transposed give the adjoint of psi4 at the interior vertices; at each one
+// the adjoints of weyl_local's 100 local inputs come from 100 forward-mode
+// evaluations (one input seeded each); the inputs that are stored or second
+// derivatives of chi and g~ go into the right-hand side's channels (and
+// through k_adj_sdbar and k_adj_gather's transposed stencils into u), the
+// ADM ones (K, gamma and d K) through Z4cToADM transposed.
+constexpr int kNWAdm = 30;  // ADM channels: K_q 6, gamma_q 6, d_c K_q 18
+
+__device__ void gather_weyl(const Grid& g, const FdScale& F, const double* __restrict__ U,
+                            const double* __restrict__ ADM, const double* __restrict__ SD,
+                            int64_t p, ad::WeylLocal<double>& v) {
+  const int64_t nv = g.nvol;
+  auto UV = [&](int n) { return U + (int64_t)n * nv + p; };
+  auto AV = [&](int n) { return ADM + (int64_t)n * nv + p; };
+  auto SDC = [&](int slot, int dir) { return SD + ((int64_t)slot * 3 + dir) * nv + p; };
+  v.chi = __ldg(UV(Z4C_CHI));
+  for (int q = 0; q < 6; ++q) {
+    v.gt[q] = __ldg(UV(Z4C_GXX + q));
+    v.Kd[q] = __ldg(AV(Z4C_ADM_KXX + q));
+    v.gph[q] = __ldg(AV(Z4C_ADM_GXX + q));
+  }
+  for (int a = 0; a < 3; ++a) {
+    v.dchi[a] = __ldg(SDC(kSdChi, a));
+    for (int q = 0; q < 6; ++q) v.dg3[a][q] = __ldg(SDC(kSdG + q, a));
+  }
+  for (int ab = 0; ab < 6; ++ab) {
+    const int a = pair_a(ab), b = pair_b(ab);
+    if (a == b) {
+      v.ddchi[ab] = fd_dxx(UV(Z4C_CHI), g.s[a], F.cidx2[a]);
+      for (int cd = 0; cd < 6; ++cd) v.ddg[ab][cd] = fd_dxx(UV(Z4C_GXX + cd), g.s[a], F.cidx2[a]);
+    } else {
+      v.ddchi[ab] = fd_dx(SDC(kSdChi, b), g.s[a], F.cidx1[a]);
+      for (int cd = 0; cd < 6; ++cd)
+        v.ddg[ab][cd] = fd_dx(SDC(kSdG + cd, b), g.s[a], F.cidx1[a]);
+    }
+  }
+  for (int c = 0; c < 3; ++c)
+    for (int q = 0; q < 6; ++q) v.dK[c][q] = fd_dx(AV(Z4C_ADM_KXX + q), g.s[c], F.cidx1[c]);
+}
+
+// The local inputs' adjoints at every interior vertex whose psi4 adjoint
+// (wb2, [block][2][vertex]) is non-zero; channels and direct are cleared
+// beforehand.
+template <int NX>
+__global__ void __launch_bounds__(kThreads)
+k_weyl_adj(Grid gin, DevParams P, const double* __restrict__ u, const double* __restrict__ adm,
+           const double* __restrict__ sd, const double* __restrict__ xf,
+           const double* __restrict__ wb2, double* __restrict__ chan,
+           double* __restrict__ direct, double* __restrict__ wadm) {
+  const Grid g = fixed_geometry<NX>(gin);
+  const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * g.nblocks) return;
+  const int b = (int)(t / npts);
+  const int64_t l = t % npts;
+  int i, j, k;
+  interior_of(g, l, i, j, k);
+  const int64_t nv = g.nvol;
+  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  const double pr = wb2[(int64_t)b * 2 * nv + p], pi = wb2[((int64_t)b * 2 + 1) * nv + p];
+  if (pr == 0.0 && pi == 0.0) return;
+  using WL = ad::WeylLocal<double>;
+  WL v;
+  gather_weyl(g, P.fd[b], u + (int64_t)b * NVAR * nv, adm + (int64_t)b * Z4C_NADM * nv,
+              sd + (int64_t)b * kSdComponents * nv, p, v);
+  const double* x = xf + (int64_t)b * (g.nn[0] + g.nn[1] + g.nn[2]);
+  const double x1 = x[i], x2 = x[g.nn[0] + j], x3 = x[g.nn[0] + g.nn[1] + k];
+  double* C = chan + (int64_t)b * kNChan * npts + l;
+  double* D = direct + (int64_t)b * NVAR * nv + p;
+  double* W = wadm + (int64_t)b * kNWAdm * npts + l;
+  const double* src = v.data();
+  for (int kk = 0; kk < WL::N; ++kk) {
+    ad::WeylLocal<ad::Dual> vd;
+    ad::Dual* dst = vd.data();
+    for (int m = 0; m < WL::N; ++m) dst[m] = ad::Dual(src[m], m == kk ? 1.0 : 0.0);
+    ad::Dual rp, ip;
+    ad::weyl_local(P.p, vd, x1, x2, x3, rp, ip);
+    const double bar = pr * rp.d + pi * ip.d;
+    // the input's place: chi 0, g~ 1-6, K 7-12, gamma 13-18, d chi 19-21,
+    // d g~ 22-39 [c][q], dd chi 40-45, dd g~ 46-81 [ab][cd], d K 82-99 [c][q]
+    if (kk == 0) D[(int64_t)Z4C_CHI * nv] = bar;
+    else if (kk < 7) D[(int64_t)(Z4C_GXX + kk - 1) * nv] = bar;
+    else if (kk < 13) W[(int64_t)(kk - 7) * npts] = bar;
+    else if (kk < 19) W[(int64_t)(6 + kk - 13) * npts] = bar;
+    else if (kk < 22) C[(int64_t)(kChSd + kSdChi * 3 + (kk - 19)) * npts] = bar;
+    else if (kk < 40) {
+      const int c = (kk - 22) / 6, q = (kk - 22) % 6;
+      C[(int64_t)(kChSd + (kSdG + q) * 3 + c) * npts] = bar;
+    } else if (kk < 46) {
+      C[(int64_t)(kChDd + kSdChi * 6 + (kk - 40)) * npts] = bar;
+    } else if (kk < 82) {
+      const int ab = (kk - 46) / 6, cd = (kk - 46) % 6;
+      C[(int64_t)(kChDd + (kSdG + cd) * 6 + ab) * npts] = bar;
+    } else {
+      W[(int64_t)(12 + (kk - 82)) * npts] = bar;
+    }
+  }
+}
+
+// The ADM channels' adjoint (K and gamma at the vertex, the transposed
+// first-derivative stencil of K) at every vertex, through Z4cToADM
+// transposed (chi_psi_power = -4: psi4 = 1/chi, gamma = psi4 g~,
+// K = psi4 A~ + (Khat + 2 Theta)/3 gamma), added to ubar.
+template <int NX>
+__global__ void __launch_bounds__(kThreads)
+k_weyl_adm_gather(Grid gin, DevParams P, const double* __restrict__ u,
+                  const double* __restrict__ wadm, double* __restrict__ ubar) {
+  const Grid g = fixed_geometry<NX>(gin);
+  const int64_t nv = g.nvol;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nv * g.nblocks) return;
+  const int64_t q = t % nv;
+  const int b = (int)(t / nv);
+  const int ijk[3] = {(int)(q % g.nn[0]), (int)((q / g.nn[0]) % g.nn[1]),
+                      (int)(q / ((int64_t)g.nn[0] * g.nn[1]))};
+  const int64_t npts = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * (g.nx[2] + 1);
+  const double* W = wadm + (int64_t)b * kNWAdm * npts;
+  const FdScale& F = P.fd[b];
+  double Kb[6], Gb[6];
+  const bool interior = is_interior(g, ijk[0], ijk[1], ijk[2]);
+  const int64_t lq = interior ? interior_index(g, ijk[0], ijk[1], ijk[2]) : 0;
+  for (int c = 0; c < 6; ++c) {
+    Kb[c] = interior ? W[(int64_t)c * npts + lq] : 0.0;
+    Gb[c] = interior ? W[(int64_t)(6 + c) * npts + lq] : 0.0;
+  }
+  bool any = interior;
+  for (int c = 0; c < 3; ++c) {
+    for (int o = -3; o <= 3; ++o) {
+      if (o == 0) continue;
+      int pp[3] = {ijk[0], ijk[1], ijk[2]};
+      pp[c] -= o;
+      if (!is_interior(g, pp[0], pp[1], pp[2])) continue;
+      const int64_t lp = interior_index(g, pp[0], pp[1], pp[2]);
+      const double w = w_d1(o) * F.cidx1[c];
+      for (int qq = 0; qq < 6; ++qq) Kb[qq] += w * W[(int64_t)(12 + c * 6 + qq) * npts + lp];
+      any = true;
+    }
+  }
+  if (!any) return;
+  const double* U = u + (int64_t)b * NVAR * nv + q;
+  double* UB = ubar + (int64_t)b * NVAR * nv + q;
+  const double chi = U[(int64_t)Z4C_CHI * nv];
+  const double psi4 = 1.0 / chi;
+  const double Ktr = U[(int64_t)Z4C_KHAT * nv] + 2.0 * U[(int64_t)Z4C_THETA * nv];
+  double psi4b = 0.0, trb = 0.0;
+  for (int c = 0; c < 6; ++c) {
+    const double gt = U[(int64_t)(Z4C_GXX + c) * nv], At = U[(int64_t)(Z4C_AXX + c) * nv];
+    const double gph = psi4 * gt;
+    UB[(int64_t)(Z4C_AXX + c) * nv] += psi4 * Kb[c];
+    psi4b += At * Kb[c];
+    trb += (1.0 / 3.0) * gph * Kb[c];
+    const double gphb = Gb[c] + (1.0 / 3.0) * Ktr * Kb[c];
+    UB[(int64_t)(Z4C_GXX + c) * nv] += psi4 * gphb;
+    psi4b += gt * gphb;
+  }
+  UB[(int64_t)Z4C_KHAT * nv] += trb;
+  UB[(int64_t)Z4C_THETA * nv] += 2.0 * trb;
+  UB[(int64_t)Z4C_CHI * nv] += -psi4 * psi4 * psi4b;
+}
+
+__global__ void k_axpy(int64_t n, double a, const double* __restrict__ x, double* __restrict__ y) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) y[t] += a * x[t];
+}
+
+// Per-CTA partial sums of x . y (added on the host in CTA order).
+__global__ void __launch_bounds__(256) k_dot(int64_t n, const double* __restrict__ x,
+                                             const double* __restrict__ y, double* __restrict__ part) {
+  __shared__ double sm[256];
+  double acc = 0.0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x)
+    acc += x[t] * y[t];
+  sm[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sm[0];
 }
 
 // ---- tangent-linear model ------------------------------------------------------
@@ -1190,6 +1377,16 @@ struct AdjState {
   double* gub = nullptr;    // adjoint of the inverse conformal metric of ADMToZ4c
   int* pro_owner = nullptr; // refined meshes: the prolongation box that carries each fine vertex
   std::vector<double*> snaps;  // revolve snapshots
+  // the Weyl-scalar objective term (z4c_adj_set_weyl)
+  int wsphere = -1;         // the psi4 sphere of the term; -1: no term
+  double wweight = 0.0;     // its weight in J
+  double* admw = nullptr;   // ADM state of the evaluation point
+  double* wreg = nullptr;   // psi4 (2 variables) before the ghost fill
+  double* wtmp = nullptr;   // psi4 after the fill; its interiors' adjoint on the way back
+  double* wregb = nullptr;  // adjoint of the filled psi4 register
+  double* wadm = nullptr;   // ADM channels [block][kNWAdm][interior vertex]
+  double* databar = nullptr;  // adjoint of the sphere values [2][npts]
+  double* dpart = nullptr;  // dot-product partial sums
 };
 
 void adj_free(AdjState* a) {
@@ -1203,6 +1400,8 @@ void adj_free(AdjState* a) {
   for (double* p : a->snaps)
     if (p) cudaFree(p);
   if (a->pro_owner) cudaFree(a->pro_owner);
+  for (double* p : {a->admw, a->wreg, a->wtmp, a->wregb, a->wadm, a->databar, a->dpart})
+    if (p) cudaFree(p);
   delete a;
 }
 
@@ -1245,12 +1444,14 @@ int check_ctx(z4c_ctx* c) {
 }
 
 // Transpose of launch_physical_bcs: the axes in reverse order.
+template <int NVB = NVAR>
 void adj_physical_bcs(const Grid& g, double* ub, cudaStream_t st) {
   for (int ax = 2; ax >= 0; --ax) {
     if (g.bc[2 * ax] == Z4C_BC_PERIODIC && g.bc[2 * ax + 1] == Z4C_BC_PERIODIC) continue;
     const int o1 = (ax == 0) ? 1 : 0, o2 = (ax == 2) ? 1 : 2;
-    const int64_t n = (int64_t)g.nn[o1] * g.nn[o2] * 2 * NVAR * g.nb[o1] * g.nb[o2];
-    auto kern = ax == 0 ? k_adj_bc_axis<0> : ax == 1 ? k_adj_bc_axis<1> : k_adj_bc_axis<2>;
+    const int64_t n = (int64_t)g.nn[o1] * g.nn[o2] * 2 * NVB * g.nb[o1] * g.nb[o2];
+    auto kern = ax == 0 ? k_adj_bc_axis<0, NVB>
+                        : ax == 1 ? k_adj_bc_axis<1, NVB> : k_adj_bc_axis<2, NVB>;
     kern<<<div_up(n, kThreads), kThreads, 0, st>>>(g, ub);
     add_kernel_launches(1);
   }
@@ -1436,6 +1637,126 @@ int advance(GradRun& R, double* u, int nsteps) {
 }
 
 // Z4C_REG_ADJ += scale dJ/du at the state u
+// ---- the Weyl-scalar objective term (host) ----
+// psi4 of the state u at the term's sphere vertices into the sphere's data
+// array: Z4cToADM, Z4cWeyl, the Weyl register's ghost fill, the
+// interpolation.
+int weyl_psi(z4c_ctx* c, const double* u) {
+  z4c::AdjState* A = c->adj;
+  const Grid& g = c->g;
+  const DevParams P = c->dev();
+  launch_z4c_to_adm(g, P, u, A->admw, 0, g.nblocks, c->stream);
+  launch_weyl(g, P, A->admw, u, c->sd, A->wreg, c->xf, 0, g.nblocks, c->stream);
+  ALAUNCH("Weyl");
+  if (c->ml) {
+    int rc = launch_ml_exchange(*c->ml, A->wreg, A->wtmp, Z4C_NWEYL, Z4C_NWEYL, c->stream);
+    if (rc) return rc;
+  } else {
+    launch_exchange(g, P, A->wreg, A->wtmp, c->nbr, 0, c->stream, Z4C_NWEYL);
+    if (c->has_outflow) launch_physical_bcs(g, A->wtmp, Z4C_NWEYL, c->stream);
+    ALAUNCH("Weyl ghost fill");
+  }
+  launch_wave_interp(g, c->waves[A->wsphere], A->wtmp, c->stream);
+  ALAUNCH("sphere interpolation");
+  return Z4C_OK;
+}
+
+// J_W at u; with databar, also the adjoint of the sphere values for the
+// scale (scale * 2 w_p psi4(p)), uploaded to A->databar.
+int weyl_J(z4c_ctx* c, const double* u, double* J, double scale, bool databar) {
+  z4c::AdjState* A = c->adj;
+  const WaveSphere& w = c->waves[A->wsphere];
+  int rc = weyl_psi(c, u);
+  if (rc) return rc;
+  std::vector<double> d((size_t)2 * w.npts), pw((size_t)2 * w.npts);
+  ACUDA(cudaMemcpyAsync(d.data(), w.data, sizeof(double) * d.size(), cudaMemcpyDeviceToHost,
+                        c->stream));
+  ACUDA(cudaMemcpyAsync(pw.data(), w.pw, sizeof(double) * pw.size(), cudaMemcpyDeviceToHost,
+                        c->stream));
+  ACUDA(cudaStreamSynchronize(c->stream));
+  double s = 0.0;
+  for (int p = 0; p < w.npts; ++p) {
+    const double dr = d[p], di = d[(size_t)w.npts + p];
+    s += pw[2 * (size_t)p] * (dr * dr + di * di);
+    if (databar) {
+      d[p] = scale * 2.0 * pw[2 * (size_t)p] * dr;
+      d[(size_t)w.npts + p] = scale * 2.0 * pw[2 * (size_t)p] * di;
+    }
+  }
+  if (J) *J = s;
+  if (databar)
+    ACUDA(cudaMemcpyAsync(A->databar, d.data(), sizeof(double) * d.size(),
+                          cudaMemcpyHostToDevice, c->stream));
+  return Z4C_OK;
+}
+
+// out (22 variables, every vertex) = scale dJ_W/du at u.
+int weyl_adj(z4c_ctx* c, const double* u, double scale, double* out) {
+  z4c::AdjState* A = c->adj;
+  const Grid& g = c->g;
+  const DevParams P = c->dev();
+  int rc = weyl_J(c, u, nullptr, scale, true);
+  if (rc) return rc;
+  const size_t wbytes = sizeof(double) * Z4C_NWEYL * g.nvol * g.nblocks;
+  ACUDA(cudaMemsetAsync(A->wregb, 0, wbytes, c->stream));
+  launch_wave_interp_adj(g, c->waves[A->wsphere], A->databar, A->wregb, c->stream);
+  ALAUNCH("sphere interpolation transpose");
+  // the Weyl register's ghost fill transposed: the interiors' adjoint in wtmp
+  if (c->ml) {
+    if ((rc = launch_ml_exchange_adj(*c->ml, A->wregb, A->wtmp, A->pro_owner, Z4C_NWEYL,
+                                     Z4C_NWEYL, c->stream)))
+      return rc;
+  } else {
+    if (c->has_outflow) adj_physical_bcs<Z4C_NWEYL>(g, A->wregb, c->stream);
+    (has_fixed_geometry(g) ? k_adj_exchange<kFixedNX, Z4C_NWEYL> : k_adj_exchange<0, Z4C_NWEYL>)<<<
+        div_up(npts_of(g) * g.nblocks, kThreads), kThreads, 0, c->stream>>>(g, A->wregb, A->wtmp);
+    ALAUNCH("Weyl ghost fill transpose");
+    add_kernel_launches(1);
+  }
+  const int64_t npts = npts_of(g) * g.nblocks;
+  const size_t reg = sizeof(double) * A->reg_elems;
+  ACUDA(cudaMemsetAsync(A->chan, 0, sizeof(double) * kNChan * npts, c->stream));
+  ACUDA(cudaMemsetAsync(A->direct, 0, reg, c->stream));
+  ACUDA(cudaMemsetAsync(A->wadm, 0, sizeof(double) * kNWAdm * npts, c->stream));
+  const bool fx = has_fixed_geometry(g);
+  (fx ? k_weyl_adj<kFixedNX> : k_weyl_adj<0>)<<<div_up(npts, kThreads), kThreads, 0, c->stream>>>(
+      g, P, u, A->admw, c->sd, c->xf, A->wtmp, A->chan, A->direct, A->wadm);
+  ALAUNCH("Weyl reverse");
+  const int64_t creg = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7) * (g.nx[2] + 1);
+  (fx ? k_adj_sdbar<kFixedNX> : k_adj_sdbar<0>)<<<dim3(div_up(creg, kThreads), kSdComponents,
+                                                      g.nblocks), kThreads, 0, c->stream>>>(
+      g, P, A->chan, A->sdbar);
+  ACUDA(cudaMemsetAsync(A->wbar, 0, reg, c->stream));  // no stage terms
+  (fx ? k_adj_gather<kFixedNX> : k_adj_gather<0>)<<<div_up(g.nvol * g.nblocks, kThreads),
+                                                    kThreads, 0, c->stream>>>(
+      g, P, u, A->wbar, A->direct, A->chan, A->sdbar, out, 0.0);
+  (fx ? k_weyl_adm_gather<kFixedNX> : k_weyl_adm_gather<0>)<<<div_up(g.nvol * g.nblocks, kThreads),
+                                                              kThreads, 0, c->stream>>>(
+      g, P, u, A->wadm, out);
+  ALAUNCH("Weyl adjoint gather");
+  add_kernel_launches(4);
+  return Z4C_OK;
+}
+
+// x . y over n values (per-CTA partials added on the host in order).
+int dot_dev(z4c_ctx* c, const double* x, const double* y, int64_t n, double* out) {
+  z4c::AdjState* A = c->adj;
+  const int nb = 1024;
+  k_dot<<<nb, 256, 0, c->stream>>>(n, x, y, A->dpart);
+  ALAUNCH("dot");
+  add_kernel_launches(1);
+  std::vector<double> h(nb);
+  ACUDA(cudaMemcpyAsync(h.data(), A->dpart, sizeof(double) * nb, cudaMemcpyDeviceToHost,
+                        c->stream));
+  ACUDA(cudaStreamSynchronize(c->stream));
+  double s = 0.0;
+  for (double v : h) s += v;
+  *out = s;
+  return Z4C_OK;
+}
+
+bool weyl_on(const z4c_ctx* c) { return c->adj && c->adj->wsphere >= 0 && c->adj->wweight != 0.0; }
+
 int objective_adj(z4c_ctx* c, const double* u, double scale) {
   const Grid& g = c->g;
   const DevParams P = c->dev();
@@ -1445,6 +1766,14 @@ int objective_adj(z4c_ctx* c, const double* u, double scale) {
       g, P, c->adj->hchan, c->adj->adj);
   ALAUNCH("objective adjoint");
   add_kernel_launches(2);
+  if (weyl_on(c)) {  // REG_ADJ += scale * weight * dJ_W/du
+    z4c::AdjState* A = c->adj;
+    int rc = weyl_adj(c, u, scale * A->wweight, A->tanw);
+    if (rc) return rc;
+    k_axpy<<<div_up(A->reg_elems, 256), 256, 0, c->stream>>>(A->reg_elems, 1.0, A->tanw, A->adj);
+    ALAUNCH("axpy");
+    add_kernel_launches(1);
+  }
   return Z4C_OK;
 }
 
@@ -1462,6 +1791,18 @@ int objective(z4c_ctx* c, const double* u, const double* ud, double* J, double* 
   if (rc) return rc;
   *J = s2[0];
   if (Jdot) *Jdot = s2[1];
+  if (weyl_on(c)) {
+    z4c::AdjState* A = c->adj;
+    double Jw = 0.0;
+    if ((rc = weyl_J(c, u, &Jw, 0.0, false))) return rc;
+    *J += A->wweight * Jw;
+    if (Jdot && ud) {  // the tangent of J_W: its gradient along ud
+      if ((rc = weyl_adj(c, u, A->wweight, A->tanw))) return rc;
+      double dj = 0.0;
+      if ((rc = dot_dev(c, A->tanw, ud, A->reg_elems, &dj))) return rc;
+      *Jdot += dj;
+    }
+  }
   return Z4C_OK;
 }
 
@@ -1643,6 +1984,41 @@ int z4c_adj_params(z4c_ctx* c, double pbar[2], int reset) {
 }
 
 }  // extern "C"
+
+extern "C" int z4c_adj_set_weyl(z4c_ctx* c, int sphere, double weight) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  z4c::AdjState* A = c->adj;
+  if (sphere < 0) {
+    A->wsphere = -1;
+    A->wweight = 0.0;
+    return Z4C_OK;
+  }
+  if (sphere >= (int)c->waves.size()) return err(Z4C_EINVAL, "no psi4 sphere %d", sphere);
+  if (c->waves[sphere].bitant) return err(Z4C_EINVAL, "the Weyl objective takes full spheres");
+  const Grid& g = c->g;
+  const int64_t npts = npts_of(g) * g.nblocks;
+  const size_t wreg = sizeof(double) * Z4C_NWEYL * g.nvol * g.nblocks;
+  struct Buf { double** p; size_t bytes; };
+  const Buf bufs[] = {{&A->admw, sizeof(double) * Z4C_NADM * g.nvol * g.nblocks},
+                      {&A->wreg, wreg}, {&A->wtmp, wreg}, {&A->wregb, wreg},
+                      {&A->wadm, sizeof(double) * kNWAdm * npts}, {&A->dpart, sizeof(double) * 1024}};
+  for (const Buf& b : bufs)
+    if (!*b.p && cudaMalloc((void**)b.p, b.bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return err(Z4C_ENOMEM, "Weyl objective buffers: %zu bytes", b.bytes);
+    }
+  if (A->databar) cudaFree(A->databar);
+  A->databar = nullptr;
+  if (cudaMalloc((void**)&A->databar, sizeof(double) * 2 * std::max(1, c->waves[sphere].npts)) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return err(Z4C_ENOMEM, "Weyl objective buffers");
+  }
+  A->wsphere = sphere;
+  A->wweight = weight;
+  return Z4C_OK;
+}
 
 extern "C" int z4c_adj_snapshots(z4c_ctx* c, int nsteps, int* nsnap) {
   int rc = check_ctx(c);

@@ -463,4 +463,43 @@ void launch_wave(const Grid& g, const WaveSphere& w, const double* weyl, cudaStr
   add_kernel_launches(1);
 }
 
+void launch_wave_interp(const Grid& g, const WaveSphere& w, const double* weyl, cudaStream_t st) {
+  if (w.npts <= 0) return;
+  k_wave_interp<<<(w.npts + 127) / 128, 128, 0, st>>>(g, weyl, w.blk, w.base, w.coef, w.data,
+                                                     w.npts);
+  add_kernel_launches(1);
+}
+
+// Transpose of k_wave_interp: every sphere vertex's adjoint (databar, Re and
+// Im, [2][npts]) scattered onto its 8^3 stencil of the Weyl register's
+// adjoint with the interpolation weights; atomic adds (neighbouring sphere
+// vertices share stencil vertices).
+__global__ void k_wave_interp_adj(Grid g, const int* __restrict__ blk, const int* __restrict__ base,
+                                  const double* __restrict__ coef,
+                                  const double* __restrict__ databar, double* __restrict__ wbar,
+                                  int npts) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npts) return;
+  const double* cf = coef + (int64_t)p * 3 * kSten;
+  for (int v = 0; v < 2; ++v) {
+    const double a = databar[(int64_t)v * npts + p];
+    if (a == 0.0) continue;
+    double* f = wbar + ((int64_t)blk[p] * 2 + v) * g.nvol + base[p];
+    for (int ez = 0; ez < kSten; ++ez)
+      for (int ey = 0; ey < kSten; ++ey) {
+        const double wzy = cf[2 * kSten + ez] * cf[kSten + ey] * a;
+        double* row = f + ez * g.s[2] + ey * g.s[1];
+        for (int i = 0; i < kSten; ++i) atomicAdd(row + i, cf[i] * wzy);
+      }
+  }
+}
+
+void launch_wave_interp_adj(const Grid& g, const WaveSphere& w, const double* databar,
+                            double* wbar, cudaStream_t st) {
+  if (w.npts <= 0) return;
+  k_wave_interp_adj<<<(w.npts + 127) / 128, 128, 0, st>>>(g, w.blk, w.base, w.coef, databar,
+                                                         wbar, w.npts);
+  add_kernel_launches(1);
+}
+
 }  // namespace z4c

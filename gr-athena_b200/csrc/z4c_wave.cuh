@@ -50,5 +50,10 @@ void wave_free(WaveSphere* w);
 // Interpolation, projection and reduction on the Weyl register (2 variables,
 // ghosts filled); the result is left in w.psi.
 void launch_wave(const Grid& g, const WaveSphere& w, const double* weyl, cudaStream_t st);
+// The interpolation alone (w.data), and its transpose: databar ([2][npts])
+// added onto wbar (a Weyl-shaped register) with the same weights.
+void launch_wave_interp(const Grid& g, const WaveSphere& w, const double* weyl, cudaStream_t st);
+void launch_wave_interp_adj(const Grid& g, const WaveSphere& w, const double* databar,
+                            double* wbar, cudaStream_t st);
 
 }  // namespace z4c

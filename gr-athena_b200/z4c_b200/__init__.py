@@ -58,7 +58,7 @@ EXPORTS = (
     "z4c_restart_load", "z4c_restart_save", "z4c_adj_setup", "z4c_tlm_step", "z4c_adj_step",
     "z4c_adj_objective", "z4c_adj_objective_adj", "z4c_adj_params", "z4c_adj_gradient",
     "z4c_adj_adm_to_z4c", "z4c_set_contract", "z4c_get_contract", "z4c_set_point_regs",
-    "z4c_get_point_regs", "z4c_adj_snapshots")
+    "z4c_get_point_regs", "z4c_adj_snapshots", "z4c_adj_set_weyl")
 
 
 class Z4cError(RuntimeError):
@@ -153,6 +153,7 @@ def lib():
         L.z4c_get_contract.argtypes = [vp, C.POINTER(C.c_int)]
         L.z4c_set_point_regs.argtypes = [vp, ip]
         L.z4c_adj_snapshots.argtypes = [vp, ip, C.POINTER(C.c_int)]
+        L.z4c_adj_set_weyl.argtypes = [vp, ip, C.c_double]
         L.z4c_get_point_regs.argtypes = [vp, C.POINTER(C.c_int)]
         L.z4c_autotune.argtypes = [vp, ip, C.POINTER(C.c_float)]
         L.z4c_check_finite.argtypes = [vp, ip]
@@ -788,6 +789,13 @@ class Z4c:
         _check(lib().z4c_adj_params(self._h, out.ctypes.data_as(C.POINTER(C.c_double)),
                                     int(reset)))
         return out
+
+    def adj_set_weyl(self, sphere, weight=1.0):
+        """Adds weight * J_W (the weighted |psi4|^2 over the sphere's
+        vertices; sphere: a WaveExtract or its id, None removes the term) to
+        the objective of objective, objective_adj and gradient."""
+        sid = -1 if sphere is None else int(getattr(sphere, "id", sphere))
+        _check(lib().z4c_adj_set_weyl(self._h, sid, float(weight)))
 
     def snapshots(self, nsteps):
         """Revolve snapshots the free device memory holds for nsteps steps."""

@@ -506,6 +506,18 @@ int z4c_adj_params(z4c_ctx *ctx, double pbar[2], int reset);
  * schedule's recomputed steps}. */
 int z4c_adj_gradient(z4c_ctx *ctx, double dt, int nsteps, int nsnap, double w_final,
                      double w_step, double *J, double pbar[2], double stats[4]);
+/* The Weyl-scalar term of the objective: with sphere >= 0 (a z4c_wave_add
+ * sphere, full, not bitant) the objective of z4c_adj_objective,
+ * z4c_adj_objective_adj and z4c_adj_gradient becomes J + weight J_W,
+ * J_W = sum over the sphere's owned vertices p of w_p |psi4(p)|^2 (w_p the
+ * vertex's quadrature weight, rad^2 times its dual cell's area; psi4 of
+ * Z4cWeyl after Z4cToADM, the Weyl register's ghost fill and the sphere
+ * interpolation).  Its adjoint: the interpolation and the ghost fill
+ * transposed, at each interior vertex the adjoints of psi4's local inputs by
+ * forward-mode differentiation, then the transposed stencils and Z4cToADM
+ * transposed.  sphere < 0 removes the term.  Allocates the term's buffers
+ * (an ADM register, three Weyl registers, 30 values per interior vertex). */
+int z4c_adj_set_weyl(z4c_ctx *ctx, int sphere, double weight);
 /* The number of revolve snapshots a gradient over nsteps steps can hold in
  * the device memory that is free now (state-sized buffers; 2 GiB and 2% of
  * the device are left over), at most nsteps - 1: the checkpointing sized to

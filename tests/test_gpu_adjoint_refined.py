@@ -244,3 +244,100 @@ def test_binary_parameter_gradient_on_the_refined_mesh():
         print(f"dJ/d{n_}: adjoint {a:.12e}, differences {f:.12e}, rel {abs(a - f) / abs(f):.2e}")
     for a, f in zip(grads, fds):
         assert abs(a - f) <= 1e-6 * abs(f)
+
+
+# ---- the Weyl-scalar term of the objective ----
+
+def weyl_setup(Z, ctx, radius=2.3, weight=1e3):
+    w = Z.WaveExtract(ctx, radius=radius, nlev=6, lmax=2)
+    ctx.adj_set_weyl(w, weight)
+    return w
+
+
+@pytest.mark.parametrize("bc", ["periodic", "outflow"])
+def test_weyl_objective_gradient_against_differences(bc):
+    """J = H-norm + weight * sum_p w_p |psi4(p)|^2 over a sphere of radius
+    2.3 (crossing both levels) at one state: its adjoint (the interpolation
+    and the Weyl ghost fill transposed, psi4's local inputs by forward mode,
+    the transposed stencils and Z4cToADM) against fourth-order central
+    differences along smooth directions, and the tangent the objective
+    reports (the adjoint along the direction) against them too."""
+    Z, mesh, ctx = make(bc)
+    u0 = rich_state(Z, mesh, ctx, amp=3e-2)
+    weyl_setup(Z, ctx)
+    ctx.upload(Z.REG_U, u0)
+    J0 = ctx.objective()[0]
+    ctx.adj_set_weyl(None)
+    JH = ctx.objective()[0]
+    ctx.adj_set_weyl(0, 1e3)
+    assert J0 > JH > 0
+    ctx.upload(Z.REG_ADJ, np.zeros_like(u0))
+    ctx.objective_adj(Z.REG_U, 1.0)
+    grad = ctx.download(Z.REG_ADJ)
+    for seed in (7, 8):
+        v = smooth_field(Z, mesh, seed, 1.0)
+        if bc == "outflow":  # directions the ghost fill reproduces: interior only
+            v[:, :, :4] = v[:, :, -4:] = 0
+            v[:, :, :, :4] = v[:, :, :, -4:] = 0
+            v[:, :, :, :, :4] = v[:, :, :, :, -4:] = 0
+        h = 1e-4
+
+        def J(x):
+            ctx.upload(Z.REG_U, x)
+            return ctx.objective()[0]
+        f = [J(u0 + s_ * h * v) for s_ in (2, 1, -1, -2)]
+        fd = (-f[0] + 8 * f[1] - 8 * f[2] + f[3]) / (12 * h)
+        ad = dot(grad, v)
+        ctx.upload(Z.REG_U, u0)
+        ctx.upload(Z.REG_TAN, v)
+        jd = ctx.objective(reg_tan=Z.REG_TAN)[1]
+        print(f"{bc} direction {seed}: adjoint {ad:.12e} tangent {jd:.12e} fd {fd:.12e}")
+        assert abs(ad - fd) <= 1e-6 * abs(fd)
+        assert abs(jd - ad) <= 1e-12 * abs(ad)
+    ctx.close()
+
+
+def test_binary_gradient_with_the_weyl_term():
+    """The binary parameter gradient of the time-integrated H-norm plus the
+    Weyl term on the sphere of radius 2.3 (two-level outflow mesh, 6 steps)
+    against fourth-order differences of the full forward run."""
+    Z, mesh, ctx = make("outflow")
+    params = Z.default_params(**PUNC)
+    theta = np.array([0.5, 0.45, 3.0])
+    dt = 0.25 * min(min(mesh.block_coords(b)[1]) for b in range(mesh.nblocks))
+    nsteps = 6
+
+    def run(th):
+        Zr, meshr, c = make("outflow")
+        weyl_setup(Zr, c)
+        c.upload(Zr.REG_ADM, bl_adm(Zr, meshr, params, *th))
+        c.ADMToZ4c()
+        c.init_finalize()
+        J = 0.0
+        for _ in range(nsteps):
+            c.evolve(dt, 1)
+            J += dt * c.objective(Zr.REG_U)[0]
+        c.close()
+        return J
+
+    weyl_setup(Z, ctx)
+    adm = bl_adm(Z, mesh, params, *theta)
+    ctx.upload(Z.REG_ADM, adm)
+    ctx.ADMToZ4c()
+    ctx.init_finalize()
+    J, pb, st = ctx.gradient(dt, nsteps, 2, w_final=0.0, w_step=dt)
+    ctx.upload(Z.REG_ADM, adm)
+    ctx.adj_adm_to_z4c()
+    ab = ctx.download(Z.REG_ADM_ADJ)
+    ctx.close()
+    assert abs(J - run(theta)) <= 1e-12 * abs(J)
+    for j, name in enumerate(("m1", "m2", "separation")):
+        e = np.zeros(3)
+        e[j] = 1e-6
+        dadm = (bl_adm(Z, mesh, params, *(theta + e)) - bl_adm(Z, mesh, params, *(theta - e))) / 2e-6
+        g = dot(ab, dadm)
+        e[j] = 1e-4
+        f = [run(theta + s_ * e) for s_ in (2, 1, -1, -2)]
+        fd = (-f[0] + 8 * f[1] - 8 * f[2] + f[3]) / (12 * 1e-4)
+        print(f"dJ/d{name}: adjoint {g:.12e}, differences {fd:.12e}, rel {abs(g - fd) / abs(fd):.2e}")
+        assert abs(g - fd) <= 1e-6 * abs(fd)
