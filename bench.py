@@ -543,10 +543,13 @@ def amr_measure(steps, warmup, shift=(0.0, 0.0, 0.0), contract=1):
 # by Linf_box_in_box around the punctures at t = 0: 848 MeshBlocks.  (The
 # 3,424-block mesh of 8^3 roots does not fit: its context holds ~72 GB and
 # the adjoint's buffers ~13 state-sized registers of 9.4 GB more.)  The
-# gradient of the time-integrated H-norm over 400 steps with respect to the
+# gradient over 400 steps of the time-integrated H-norm plus the Weyl-scalar
+# proxy on the sphere of radius 50 (the weighted |psi4|^2 over its vertices,
+# weighted so that both terms are equal at t = 0) with respect to the
 # masses, the separation and eta, revolve snapshots sized to the free HBM.
 ADJ_BBH = dict(nb=(4, 4, 4), nx=(16, 16, 16), xmin=(-512.0,) * 3, xmax=(512.0,) * 3,
-               numlevel=8, par_b=3.0, masses=(0.5, 0.5), separation=6.0, steps=400)
+               numlevel=8, par_b=3.0, masses=(0.5, 0.5), separation=6.0, steps=400,
+               weyl_radius=50.0, weyl_nlev=30)
 
 
 def bbh_adjoint_measure(steps=None, fd=True):
@@ -588,6 +591,13 @@ def bbh_adjoint_measure(steps=None, fd=True):
         ctx.ADMToZ4c()
         ctx.init_finalize()
         u0 = ctx.download(Z.REG_U)
+        # the Weyl term, normalised to the H-norm term at t = 0
+        sphere = Z.WaveExtract(ctx, radius=c["weyl_radius"], nlev=c["weyl_nlev"], lmax=2)
+        JH0 = ctx.objective()[0]
+        ctx.adj_set_weyl(sphere, 1.0)
+        JW0 = ctx.objective()[0] - JH0
+        weyl_weight = JH0 / JW0
+        ctx.adj_set_weyl(sphere, weyl_weight)
         fwd = time_on(stream, lambda: ctx.evolve(dt, 1), 3)
         ctx.upload(Z.REG_U, u0)
         adj = time_on(stream, lambda: ctx.adj_step(dt), 2)
@@ -608,11 +618,14 @@ def bbh_adjoint_measure(steps=None, fd=True):
     out = {"workload": "binary Brill-Lindquist punctures (m=0.5 each near (+-3,0,0)), "
                        "[-512,512]^3, 4^3 root MeshBlocks of 16^3 cells, 8 levels refined by "
                        "Linf_box_in_box (par_b 3) around the punctures at t=0, finest dx 1/8, "
-                       f"outflow, rk4, {steps} steps, objective dt * sum_k vol * sum H^2",
+                       f"outflow, rk4, {steps} steps, objective dt * sum_k (vol * sum H^2 "
+                       f"+ w * sum_p w_p |psi4(p)|^2 on the r = {c['weyl_radius']:g} sphere)",
            "meshblocks": mesh.nblocks, "steps": steps, "snapshots": nsnap,
            "forward_step_ms": fwd, "adjoint_step_ms": adj, "adjoint_over_forward": adj / fwd,
            "gradient_seconds": st["seconds"], "gradient_forward_steps": st["forward_steps"],
-           "gradient_adjoint_steps": st["adjoint_steps"], "objective": J, "gradient": grads}
+           "gradient_adjoint_steps": st["adjoint_steps"], "objective": J, "gradient": grads,
+           "weyl_term": {"radius": c["weyl_radius"], "sphere_vertices": sphere.num_points(),
+                         "weight": weyl_weight, "J_H_t0": JH0, "J_W_t0": JW0}}
     ctx.close()
     if fd:
         # the full forward run at eta +- h (the objective reads the adjoint
@@ -621,6 +634,8 @@ def bbh_adjoint_measure(steps=None, fd=True):
             cr = Z.Z4c(mesh, Z.default_params(**dict(pdict, shift_eta=eta)), "rk4")
             cr.set_stream(stream.cuda_stream)
             cr.adj_setup()
+            cr.adj_set_weyl(Z.WaveExtract(cr, radius=c["weyl_radius"], nlev=c["weyl_nlev"],
+                                          lmax=2), weyl_weight)
             with torch.cuda.stream(stream):
                 cr.upload(Z.REG_U, u0)
                 tot = 0.0
