@@ -1,6 +1,6 @@
-"""The contracted path (z4c_set_contract: fused multiply-adds, advection and
-Kreiss-Oliger in one per-variable pass, the stage update fused with the main
-pass) against the reference's own outputs.  Its right-hand side is not the
+"""The contracted path (z4c_set_contract: fused multiply-adds; advection,
+Kreiss-Oliger and the stage update in one per-variable column pass after the
+main pass) against the reference's own outputs.  Its right-hand side is not the
 reference's bit for bit, so every check is a bound:
 
   right-hand side      normwise relative 1e-12 per register (the FP64
@@ -16,9 +16,9 @@ reference's bit for bit, so every check is a bound:
                        reference's own rounding of those terms is what
                        contraction changes, so the difference is measured
                        against them; on the other states it is also within
-                       1e-12 of the right-hand side itself.  (Per variable the difference can reach
-                       1e-10 of that variable's own size for the same
-                       reason.)
+                       1e-12 of the right-hand side itself.  (Per variable
+                       the difference can reach 1e-10 of that variable's
+                       own size for the same reason.)
   one RK4 step         every stage's state within 1e-12 of the reference's
                        on the interior (ghosts: see GHOST_TOL)
   evolution            the history norms of the 12-step puncture run within
