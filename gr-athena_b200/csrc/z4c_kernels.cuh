@@ -69,10 +69,10 @@ constexpr int kSdComponents = 33;
 // passes stage a variable in shared memory (1-4; 0 or a slab whose planes do
 // not fit: global-memory pencils instead).
 // contract: the contracted path (z4c_fast.cu) on meshes without
-// gr_sommerfeld faces: floating-point contraction, the advection sums and the
-// Kreiss-Oliger terms added in one pass, the stage update fused with the main
-// pass; the right-hand side agrees with the exact path to round-off instead
-// of bit for bit.
+// gr_sommerfeld faces: floating-point contraction, and the advection sums,
+// the Kreiss-Oliger terms and the stage update in one per-variable column
+// pass after the main pass; the right-hand side agrees with the exact path to
+// round-off instead of bit for bit.
 // point_regs: register budget of the heavy per-vertex passes on fixed-geometry
 // meshes: 0 (up to 255 per thread, two CTAs of 128 per SM) or
 // kPointRegsHigh (168: three CTAs of 128 or six of 64 per SM, 1.5x the
