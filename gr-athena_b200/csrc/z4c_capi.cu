@@ -288,6 +288,22 @@ void free_ctx(z4c_ctx* c) {
   }
   if (c->som) cudaFree(c->som);
   if (c->adj) adj_free(c->adj);
+  if (c->jobs) {
+    JobPipe* J = c->jobs;
+    for (cudaStream_t s : {J->h2d, J->d2h})
+      if (s) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+      }
+    for (int k = 0; k < 2; ++k) {
+      for (cudaEvent_t e : {J->in_ready[k], J->in_free[k], J->out_ready[k], J->out_free[k]})
+        if (e) cudaEventDestroy(e);
+      for (void* p : {(void*)J->in[k], (void*)J->out[k], (void*)J->part[k]})
+        if (p) cudaFree(p);
+      if (J->hpart[k]) cudaFreeHost(J->hpart[k]);
+    }
+    delete J;
+  }
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -1175,6 +1191,116 @@ int z4c_evolve(z4c_ctx* ctx, double dt, int nsteps, int with_constraints) {
 }
 
 long long z4c_kernel_launches(void) { return kernel_launch_count(); }
+
+namespace {
+// Staging of z4c_evolve_jobs, allocated once per context.
+int jobs_setup(z4c_ctx* c) {
+  if (c->jobs) return Z4C_OK;
+  JobPipe* J = new JobPipe;
+  c->jobs = J;  // released by free_ctx whatever happens below
+  const size_t reg = sizeof(double) * (size_t)reg_elems(c, Z4C_REG_U);
+  const size_t part = sizeof(double) * 8 * (size_t)c->g.nblocks;
+  for (int k = 0; k < 2; ++k) {
+    CUDA_TRY(cudaMalloc(&J->in[k], reg));
+    CUDA_TRY(cudaMalloc(&J->out[k], reg));
+    CUDA_TRY(cudaMalloc(&J->part[k], part));
+    CUDA_TRY(cudaMallocHost(&J->hpart[k], part));
+    for (cudaEvent_t* e : {&J->in_ready[k], &J->in_free[k], &J->out_ready[k], &J->out_free[k]})
+      CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  }
+  CUDA_TRY(cudaStreamCreateWithFlags(&J->h2d, cudaStreamNonBlocking));
+  CUDA_TRY(cudaStreamCreateWithFlags(&J->d2h, cudaStreamNonBlocking));
+  return Z4C_OK;
+}
+
+// Issues job j: its evolution and history partials on the context's stream,
+// the download of its result on the download stream.
+int jobs_issue(z4c_ctx* c, int j, double* host_out, double dt, int nsteps) {
+  JobPipe* J = c->jobs;
+  const int s = j & 1;
+  const size_t reg = sizeof(double) * (size_t)reg_elems(c, Z4C_REG_U);
+  const size_t part = sizeof(double) * 8 * (size_t)c->g.nblocks;
+  CUDA_TRY(cudaStreamWaitEvent(c->stream, J->in_ready[s], 0));
+  CUDA_TRY(cudaMemcpyAsync(c->reg[Z4C_REG_U], J->in[s], reg, cudaMemcpyDeviceToDevice, c->stream));
+  CUDA_TRY(cudaEventRecord(J->in_free[s], c->stream));
+  int rc = z4c_evolve(c, dt, nsteps, 1);
+  if (rc) return rc;
+  launch_hst(c->g, c->dev(), c->reg[Z4C_REG_CON], c->reg[Z4C_REG_U], c->xv, c->partials, c->stream);
+  LAUNCH_CHECK("hst");
+  // the output slot is free once the download of job j - 2 has left it
+  CUDA_TRY(cudaStreamWaitEvent(c->stream, J->out_free[s], 0));
+  CUDA_TRY(cudaMemcpyAsync(J->out[s], c->reg[Z4C_REG_U], reg, cudaMemcpyDeviceToDevice, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(J->part[s], c->partials, part, cudaMemcpyDeviceToDevice, c->stream));
+  CUDA_TRY(cudaEventRecord(J->out_ready[s], c->stream));
+  CUDA_TRY(cudaStreamWaitEvent(J->d2h, J->out_ready[s], 0));
+  CUDA_TRY(cudaMemcpyAsync(host_out, J->out[s], reg, cudaMemcpyDeviceToHost, J->d2h));
+  CUDA_TRY(cudaMemcpyAsync(J->hpart[s], J->part[s], part, cudaMemcpyDeviceToHost, J->d2h));
+  CUDA_TRY(cudaEventRecord(J->out_free[s], J->d2h));
+  return Z4C_OK;
+}
+
+// Issues the upload of job j into its input slot, after the evolution of
+// job j - 2 has copied that slot out.
+int jobs_upload(z4c_ctx* c, int j, const double* host_in) {
+  JobPipe* J = c->jobs;
+  const int s = j & 1;
+  const size_t reg = sizeof(double) * (size_t)reg_elems(c, Z4C_REG_U);
+  CUDA_TRY(cudaStreamWaitEvent(J->h2d, J->in_free[s], 0));
+  CUDA_TRY(cudaMemcpyAsync(J->in[s], host_in, reg, cudaMemcpyHostToDevice, J->h2d));
+  CUDA_TRY(cudaEventRecord(J->in_ready[s], J->h2d));
+  return Z4C_OK;
+}
+}  // namespace
+
+// History norms of job j from the page-locked partials of its slot, summed
+// as z4c_hst_norms sums them; waits for the slot's download.
+static int jobs_hst(z4c_ctx* c, int j, double* hst_out) {
+  JobPipe* J = c->jobs;
+  CUDA_TRY(cudaEventSynchronize(J->out_free[j & 1]));
+  if (!hst_out) return Z4C_OK;
+  double* o = hst_out + (size_t)8 * j;
+  const double* h = J->hpart[j & 1];
+  for (int q = 0; q < 8; ++q) o[q] = 0.0;
+  for (int b = 0; b < c->g.nblocks; ++b) {
+    const double* dx = &c->h_dx[(size_t)b * 3];
+    const double vol = dx[0] * dx[1] * dx[2];
+    for (int q = 0; q < 8; ++q) o[q] += vol * h[(size_t)b * 8 + q];
+  }
+  return Z4C_OK;
+}
+
+int z4c_evolve_jobs(z4c_ctx* ctx, int njobs, const double* const* host_in,
+                    double* const* host_out, double* hst_out, double dt, int nsteps) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  if (njobs < 1 || !host_in || !host_out) return fail(Z4C_EINVAL, "need njobs >= 1 and job arrays");
+  if (nsteps < 0) return fail(Z4C_EINVAL, "negative step count");
+  for (int j = 0; j < njobs; ++j)
+    if (!host_in[j] || !host_out[j]) return fail(Z4C_EINVAL, "null host buffer of job %d", j);
+  int rc = jobs_setup(ctx);
+  if (rc) return rc;
+  JobPipe* J = ctx->jobs;
+  // upload j + 1 is issued before evolution j, so that it runs beside it;
+  // download j is issued right after it and runs beside evolution j + 1.
+  // Job j reuses the slots of job j - 2, whose partials are summed first.
+  rc = jobs_upload(ctx, 0, host_in[0]);
+  int summed = 0;  // jobs whose history norms are taken
+  for (int j = 0; j < njobs && rc == Z4C_OK; ++j) {
+    if (j + 1 < njobs) rc = jobs_upload(ctx, j + 1, host_in[j + 1]);
+    if (rc == Z4C_OK && j >= 2) rc = jobs_hst(ctx, summed++, hst_out);
+    if (rc == Z4C_OK) rc = jobs_issue(ctx, j, host_out[j], dt, nsteps);
+  }
+  // every job has finished (or failed) before the buffers are handed back
+  const cudaError_t e1 = cudaStreamSynchronize(J->h2d);
+  const cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+  const cudaError_t e3 = cudaStreamSynchronize(J->d2h);
+  if (rc) return rc;
+  for (cudaError_t e : {e1, e2, e3})
+    if (e != cudaSuccess) return fail(Z4C_ECUDA, "evolve_jobs: %s", cudaGetErrorString(e));
+  while (summed < njobs)
+    if ((rc = jobs_hst(ctx, summed++, hst_out))) return rc;
+  return Z4C_OK;
+}
+
 
 namespace {
 // {level, lx1, lx2, lx3} of every block of a context in its block order

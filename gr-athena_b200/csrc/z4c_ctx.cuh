@@ -31,6 +31,18 @@ constexpr double kBtB[4] = {1. / 6., 1. / 3., 1. / 3., 1. / 6.};
 
 using namespace z4c;
 
+// Device staging and copy streams of z4c_evolve_jobs (allocated on its first
+// call): two input and two output registers and per-block history partials,
+// so that the copies of one job overlap the evolution of the next.
+struct JobPipe {
+  double* in[2] = {};
+  double* out[2] = {};
+  double* part[2] = {};
+  double* hpart[2] = {};  // page-locked host copies of part
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t in_ready[2] = {}, in_free[2] = {}, out_ready[2] = {}, out_free[2] = {};
+};
+
 struct z4c_ctx {
   Grid g{};
   MlPlan* ml = nullptr;         // multilevel meshes: the ghost-exchange plan
@@ -64,6 +76,7 @@ struct z4c_ctx {
   int* flag = nullptr;
   std::vector<WaveSphere> waves;  // psi4 extraction spheres
   z4c::AdjState* adj = nullptr;   // tangent-linear / adjoint buffers (z4c_adj_setup)
+  JobPipe* jobs = nullptr;        // z4c_evolve_jobs staging
 
   // host copies
   std::vector<double> h_xf, h_xv, h_dx;  // h_dx: [nblocks][3]

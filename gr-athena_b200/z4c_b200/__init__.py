@@ -49,7 +49,7 @@ EXPORTS = (
     "z4c_regrid", "z4c_upload", "z4c_download", "z4c_device_ptr",
     "z4c_rhs", "z4c_boundary_rhs", "z4c_add_rhs", "z4c_weighted_ave", "z4c_alg_constr", "z4c_adm_to_z4c",
     "z4c_z4c_to_adm", "z4c_adm_constraints", "z4c_weyl", "z4c_ghost_fill", "z4c_init_finalize",
-    "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_set_per_block", "z4c_set_tile",
+    "z4c_hst_norms", "z4c_stage", "z4c_evolve", "z4c_evolve_jobs", "z4c_set_per_block", "z4c_set_tile",
     "z4c_get_tile", "z4c_autotune", "z4c_check_finite", "z4c_kernel_launches", "z4c_rhs_stage",
     "z4c_fp64_probe", "z4c_tracker_add", "z4c_tracker_get", "z4c_vc_restrict", "z4c_vc_prolongate",
     "z4c_regrid_refine", "z4c_regrid_derefine", "z4c_rhs_noalloc",
@@ -146,6 +146,7 @@ def lib():
         L.z4c_hst_norms.argtypes = [vp, dp]
         L.z4c_stage.argtypes = [vp, ip, C.c_double]
         L.z4c_evolve.argtypes = [vp, C.c_double, ip, ip]
+        L.z4c_evolve_jobs.argtypes = [vp, ip, C.POINTER(vp), C.POINTER(vp), dp, C.c_double, ip]
         L.z4c_set_per_block.argtypes = [vp, ip]
         L.z4c_set_tile.argtypes = [vp, ip, ip, ip]
         L.z4c_get_tile.argtypes = [vp, C.POINTER(C.c_int)]
@@ -741,6 +742,27 @@ class Z4c:
         z4c_init_finalize)."""
         _check(lib().z4c_regrid(self._h, old._h))
         self.init_finalize()
+
+    def evolve_jobs(self, inputs, outputs, dt, nsteps, hst=None):
+        """Evolves independent states from host memory (z4c_evolve_jobs):
+        inputs[j] (u registers) -> outputs[j] after nsteps steps of dt, with
+        the copies of one job overlapping the evolution of the next; returns
+        the history norms, one row of eight per job.  Page-locked arrays
+        (e.g. torch's pin_memory) let the copies overlap."""
+        n = len(inputs)
+        if n < 1 or len(outputs) != n:
+            raise ValueError("need as many outputs as inputs, at least one")
+        shape = self.shape(REG_U)
+        for a in list(inputs) + list(outputs):
+            if a.shape != shape or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("job arrays must be contiguous float64 u registers")
+        hin = (C.c_void_p * n)(*[a.ctypes.data for a in inputs])
+        hout = (C.c_void_p * n)(*[a.ctypes.data for a in outputs])
+        h = np.empty((n, 8)) if hst is None else hst
+        _check(lib().z4c_evolve_jobs(self._h, n, hin, hout,
+                                     h.ctypes.data_as(C.POINTER(C.c_double)), float(dt),
+                                     int(nsteps)))
+        return h
 
     def hst_norms(self):
         out = np.empty(8)

@@ -339,6 +339,22 @@ int z4c_stage(z4c_ctx *ctx, int stage, double dt);
  * Every step ends with Z4cToADM (the last stage's Z4C_TO_ADM task); when
  * with_constraints is non-zero the last step also runs ADMConstraints. */
 int z4c_evolve(z4c_ctx *ctx, double dt, int nsteps, int with_constraints);
+/* Independent evolutions from host memory (no counterpart in the reference,
+ * whose state lives in host memory): for each of njobs jobs, host_in[j] (a
+ * whole u register, the layout of z4c_upload) is evolved nsteps steps of dt
+ * as z4c_evolve(ctx, dt, nsteps, 1) does, and the final u register is written
+ * to host_out[j] and its history norms (those of z4c_hst_norms) to
+ * hst_out[8*j .. 8*j+7] (hst_out may be NULL).  The copies overlap the
+ * evolutions: job j+1 is uploaded and job j-1 downloaded while job j
+ * evolves, on two copy streams of the library, through two input and two
+ * output device registers allocated on the first call and held until
+ * z4c_destroy.  Host buffers should be page-locked (cudaHostAlloc or
+ * cudaHostRegister) for the copies to overlap; pageable ones give the same
+ * results without the overlap.  Returns once every job has finished; u then
+ * holds the last job's final state.  For ensembles and parameter sweeps whose
+ * states are produced and consumed on the host. */
+int z4c_evolve_jobs(z4c_ctx *ctx, int njobs, const double *const *host_in,
+                    double *const *host_out, double *hst_out, double dt, int nsteps);
 /* Z4c::Z4cRHS + GR_Z4c::IntegrateZ4c of one low-storage stage as a single
  * fused launch over all blocks, without the ghost exchange that follows:
  * reads u and u1, writes the updated interior into the work register and
