@@ -304,6 +304,7 @@ void free_ctx(z4c_ctx* c) {
     }
     delete J;
   }
+  if (c->merged) free_ctx(c->merged);  // its stream is c's
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -1086,6 +1087,22 @@ int z4c_get_contract(const z4c_ctx* ctx, int* on) {
   return Z4C_OK;
 }
 
+namespace {
+bool merge_eligible(const z4c_ctx* c);
+}
+
+int z4c_set_merged(z4c_ctx* ctx, int on) {
+  if (!ctx) return fail(Z4C_EINVAL, "null context");
+  ctx->merge = on != 0;
+  return Z4C_OK;
+}
+
+int z4c_get_merged(const z4c_ctx* ctx, int* on) {
+  if (!ctx || !on) return fail(Z4C_EINVAL, "null argument");
+  *on = ctx->merge && merge_eligible(ctx);
+  return Z4C_OK;
+}
+
 int z4c_get_tile(const z4c_ctx* ctx, int tile_out[3]) {
   if (!ctx || !tile_out) return fail(Z4C_EINVAL, "null argument");
   tile_out[0] = ctx->shape.point_threads;
@@ -1138,9 +1155,218 @@ int z4c_autotune(z4c_ctx* ctx, int reps, float* best_ms_out) {
   return Z4C_OK;
 }
 
+namespace {
+// ---- merged vertex grid of a uniform mesh ---------------------------------
+// The blocks of a uniform mesh tile one vertex grid of nb*nx cells per axis;
+// vertex (I, J, K) of that grid (ghosts included) is vertex (I - bx nx,
+// J - by nx, K - bz nx) of block (bx, by, bz), bx the highest block whose
+// interior starts at or below it (clamped to the mesh), so a vertex on a
+// shared face comes from the upper block, one on the mesh's outer ghosts
+// from the boundary block.  The merged grid's own step runs the same
+// kernels as one block of nb*nx cells.  Block b sits at (b % nb0, (b / nb0) % nb1,
+// b / (nb0 nb1)), the order of the uniform context.
+__global__ void k_merge_scatter(Grid g, Grid m, const double* __restrict__ blk,
+                                double* __restrict__ mg, int nvar) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= m.nvol * nvar) return;
+  const int n = (int)(t / m.nvol);
+  const int64_t p = t % m.nvol;
+  const int v[3] = {(int)(p % m.nn[0]), (int)((p / m.nn[0]) % m.nn[1]),
+                    (int)(p / ((int64_t)m.nn[0] * m.nn[1]))};
+  int bl[3], l[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int q = v[a] - NG;
+    int b = q < 0 ? 0 : q / g.nx[a];
+    if (b > g.nb[a] - 1) b = g.nb[a] - 1;
+    bl[a] = b;
+    l[a] = v[a] - b * g.nx[a];
+  }
+  const int64_t bi = ((int64_t)bl[2] * g.nb[1] + bl[1]) * g.nb[0] + bl[0];
+  mg[t] = blk[(bi * nvar + n) * g.nvol + ((int64_t)l[2] * g.nn[1] + l[1]) * g.nn[0] + l[0]];
+}
+// What the block path's ghost fill leaves at local vertex l of the block at
+// loc after a step: 0 nothing (the value stays from step to step), 1 the
+// value of the merged grid, 2 a copy the exchange took from the owner before
+// the owner's extrapolation overwrote it (the upper boundary vertices are
+// extrapolated too, physical_bcs.cpp's cell ranges) and that the block's
+// own extrapolation passes do not reach: AlgConstr of the last stage's
+// output there.  The block's own vertices and the ghosts another block owns
+// are written by the exchange; the extrapolation passes (k_bc_axis) write
+// the ghosts below a lower face and the boundary vertex and the ghosts above
+// an upper face up to nn - 2, within their transverse ranges.
+__device__ int block_fill_class(const Grid& g, const int loc[3], const int l[3]) {
+  bool own = true, held = true, upper = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    own = own && l[a] >= NG && l[a] <= NG + g.nx[a];
+    const int G = l[a] + loc[a] * g.nx[a];
+    held = held && G >= NG && G <= NG + g.nb[a] * g.nx[a];
+    upper = upper || G == NG + g.nb[a] * g.nx[a];
+  }
+  if (own) return 1;
+  bool need[6];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    need[2 * a] = loc[a] == 0;
+    need[2 * a + 1] = loc[a] == g.nb[a] - 1;
+  }
+  int lo[3], hi[3];
+  lo[0] = 0;
+  hi[0] = 2 * NG + g.nx[0] - 1;
+  lo[1] = need[2] ? NG : 0;
+  hi[1] = need[3] ? NG + g.nx[1] - 1 : 2 * NG + g.nx[1] - 1;
+  lo[2] = need[4] ? NG : 0;
+  hi[2] = need[5] ? NG + g.nx[2] - 1 : 2 * NG + g.nx[2] - 1;
+  bool bc = false;
+  for (int ax = 0; ax < 3 && !bc; ++ax) {
+    const int o1 = ax == 0 ? 1 : 0, o2 = ax == 2 ? 1 : 2;
+    int lo2 = lo[o2], hi2 = hi[o2];
+    if (ax == 2) {  // the x3 faces take the whole x2 range
+      lo2 = 0;
+      hi2 = 2 * NG + g.nx[1] - 1;
+    }
+    if (l[o1] < lo[o1] || l[o1] > hi[o1] || l[o2] < lo2 || l[o2] > hi2) continue;
+    bc = (need[2 * ax] && l[ax] < NG) ||
+         (need[2 * ax + 1] && l[ax] >= NG + g.nx[ax] && l[ax] <= 2 * NG + g.nx[ax] - 1);
+  }
+  if (bc) return 1;
+  if (held) return upper ? 2 : 1;
+  return 0;
+}
+
+__device__ __forceinline__ void block_vertex(const Grid& g, int64_t t, int nvar, int& b, int& n,
+                                             int loc[3], int l[3]) {
+  const int64_t p = t % g.nvol;
+  const int64_t bn = t / g.nvol;
+  n = (int)(bn % nvar);
+  b = (int)(bn / nvar);
+  l[0] = (int)(p % g.nn[0]);
+  l[1] = (int)((p / g.nn[0]) % g.nn[1]);
+  l[2] = (int)(p / ((int64_t)g.nn[0] * g.nn[1]));
+  loc[0] = b % g.nb[0];
+  loc[1] = (b / g.nb[0]) % g.nb[1];
+  loc[2] = b / (g.nb[0] * g.nb[1]);
+}
+
+// The class-1 vertices of every block from the merged grid.
+__global__ void k_merge_gather(Grid g, Grid m, const double* __restrict__ mg,
+                               double* __restrict__ blk, int nvar) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)g.nblocks * nvar * g.nvol) return;
+  int b, n, loc[3], l[3];
+  block_vertex(g, t, nvar, b, n, loc, l);
+  if (block_fill_class(g, loc, l) != 1) return;
+  const int I = loc[0] * g.nx[0] + l[0], J = loc[1] * g.nx[1] + l[1], K = loc[2] * g.nx[2] + l[2];
+  blk[t] = mg[(int64_t)n * m.nvol + ((int64_t)K * m.nn[1] + J) * m.nn[0] + I];
+}
+
+// The class-2 vertices of the u register: the merged grid's last stage
+// output (mw) at the vertex with AlgConstr applied, as the block that holds
+// the copy constrains it after its own extrapolation.
+__global__ void k_merge_gather_copies(Grid g, Grid m, DevParams P, const double* __restrict__ mw,
+                                      double* __restrict__ u) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)g.nblocks * g.nvol) return;
+  int b, n, loc[3], l[3];
+  block_vertex(g, t, 1, b, n, loc, l);
+  if (block_fill_class(g, loc, l) != 2) return;
+  const int I = loc[0] * g.nx[0] + l[0], J = loc[1] * g.nx[1] + l[1], K = loc[2] * g.nx[2] + l[2];
+  const double* src = mw + ((int64_t)K * m.nn[1] + J) * m.nn[0] + I;
+  double* dst = u + (int64_t)b * NVAR * g.nvol + t % g.nvol;
+  double v[NVAR];
+#pragma unroll
+  for (int q = 0; q < NVAR; ++q) v[q] = src[(int64_t)q * m.nvol];
+  alg_constr_point(P.p, v + Z4C_GXX, v + Z4C_AXX, v + Z4C_CHI, v + Z4C_ALPHA);
+#pragma unroll
+  for (int q = 0; q < NVAR; ++q) dst[(int64_t)q * g.nvol] = v[q];
+}
+
+int merge_launch(const z4c_ctx* c, const z4c_ctx* m, int reg, bool to_merged) {
+  const int nv = reg_nvar_(reg);
+  const int64_t n = to_merged ? m->g.nvol * nv : (int64_t)c->g.nblocks * nv * c->g.nvol;
+  const unsigned grid = (unsigned)((n + 255) / 256);
+  if (to_merged)
+    k_merge_scatter<<<grid, 256, 0, c->stream>>>(c->g, m->g, c->reg[reg], m->reg[reg], nv);
+  else
+    k_merge_gather<<<grid, 256, 0, c->stream>>>(c->g, m->g, m->reg[reg], c->reg[reg], nv);
+  add_kernel_launches(1);
+  LAUNCH_CHECK("merge");
+  return Z4C_OK;
+}
+
+// Steps of z4c_evolve that run on the merged grid: uniform single-level
+// meshes with outflow faces on the contracted low-storage path.
+bool merge_eligible(const z4c_ctx* c) {
+  if (!c->merge || !c->shape.contract || c->ml || c->per_block || c->g.nblocks < 2 ||
+      c->integrator != Z4C_INTEG_RK4)
+    return false;
+  for (int f = 0; f < 6; ++f)
+    if (c->desc.bc[f] != Z4C_BC_OUTFLOW) return false;
+  return true;
+}
+
+int merged_evolve(z4c_ctx* c, double dt, int nsteps, int with_constraints) {
+  if (!c->merged) {
+    z4c_mesh_desc_t d = c->desc;
+    for (int a = 0; a < 3; ++a) {
+      d.nx[a] = c->desc.nx[a] * c->desc.nb[a];
+      d.nb[a] = 1;
+    }
+    z4c_ctx* m = nullptr;
+    int rc = create_impl(&d, &c->params, c->integrator, 0, nullptr, &m);
+    if (rc) return rc;
+    m->merge = false;
+    c->merged = m;
+  }
+  z4c_ctx* m = c->merged;
+  if (m->stream != c->stream) z4c_set_stream(m, c->stream);
+  if (m->shape.point_threads != c->shape.point_threads ||
+      m->shape.column_threads != c->shape.column_threads ||
+      m->shape.column_slabs != c->shape.column_slabs || m->shape.contract != c->shape.contract ||
+      m->shape.point_regs != c->shape.point_regs) {
+    m->shape = c->shape;
+    drop_graph(m);
+  }
+  if (m->ntrk != c->ntrk) {
+    m->ntrk = c->ntrk;
+    drop_graph(m);
+  }
+  int rc;
+  if (c->ntrk > 0)
+    CUDA_TRY(cudaMemcpyAsync(m->trk, c->trk, sizeof(double) * 8 * c->ntrk,
+                             cudaMemcpyDeviceToDevice, c->stream));
+  if ((rc = merge_launch(c, m, Z4C_REG_U, true))) return rc;
+  if ((rc = z4c_evolve(m, dt, nsteps, with_constraints))) return rc;
+  if ((rc = merge_launch(c, m, Z4C_REG_U, false))) return rc;
+  {
+    const int64_t n = (int64_t)c->g.nblocks * c->g.nvol;
+    k_merge_gather_copies<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+        c->g, m->g, c->dev(), m->reg[Z4C_REG_W], c->reg[Z4C_REG_U]);
+    add_kernel_launches(1);
+    LAUNCH_CHECK("merge");
+  }
+  // the ADM variables and the constraints of the final state, on the blocks,
+  // as the block path leaves them
+  const DevParams P = c->dev();
+  launch_z4c_to_adm(c->g, P, c->reg[Z4C_REG_U], c->reg[Z4C_REG_ADM], 0, c->g.nblocks, c->stream);
+  LAUNCH_CHECK("z4c_to_adm");
+  if (with_constraints) {
+    launch_adm_constraints(c->g, P, c->reg[Z4C_REG_ADM], c->reg[Z4C_REG_U],
+                           c->reg[Z4C_REG_CON], c->xf, 0, c->g.nblocks, c->stream);
+    LAUNCH_CHECK("constraints");
+  }
+  if (c->ntrk > 0)
+    CUDA_TRY(cudaMemcpyAsync(c->trk, m->trk, sizeof(double) * 8 * c->ntrk,
+                             cudaMemcpyDeviceToDevice, c->stream));
+  return Z4C_OK;
+}
+}  // namespace
+
 int z4c_evolve(z4c_ctx* ctx, double dt, int nsteps, int with_constraints) {
   if (!ctx) return fail(Z4C_EINVAL, "null context");
   if (nsteps < 0) return fail(Z4C_EINVAL, "negative step count");
+  if (nsteps > 0 && merge_eligible(ctx)) return merged_evolve(ctx, dt, nsteps, with_constraints);
   // The four stages of a step, captured once into a graph and replayed.  The
   // register pointers inside the graph are fixed: a step leaves u in the same
   // buffer it started from (exchange writes back into u), so replays are

@@ -80,6 +80,16 @@ __host__ __device__ __forceinline__ Grid fixed_geometry(const Grid& g) {
 __host__ __forceinline__ bool has_fixed_geometry(const Grid& g) {
   return kFixedNX > 0 && g.nx[0] == kFixedNX && g.nx[1] == kFixedNX && g.nx[2] == kFixedNX;
 }
+// The merged vertex grid of a uniform mesh (z4c_evolve on the contracted
+// path) is one block of nb * nx cells per axis; kMergedNX is the size whose
+// right-hand-side passes get fixed instances as well (0 disables them).
+#ifndef Z4C_MERGED_NX
+#define Z4C_MERGED_NX 128
+#endif
+constexpr int kMergedNX = Z4C_MERGED_NX;
+__host__ __forceinline__ bool has_merged_geometry(const Grid& g) {
+  return kMergedNX > 0 && g.nx[0] == kMergedNX && g.nx[1] == kMergedNX && g.nx[2] == kMergedNX;
+}
 
 // ---- stencils -----------------------------------------------------------
 

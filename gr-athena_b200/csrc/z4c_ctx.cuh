@@ -77,6 +77,11 @@ struct z4c_ctx {
   std::vector<WaveSphere> waves;  // psi4 extraction spheres
   z4c::AdjState* adj = nullptr;   // tangent-linear / adjoint buffers (z4c_adj_setup)
   JobPipe* jobs = nullptr;        // z4c_evolve_jobs staging
+  // Uniform meshes on the contracted path: z4c_evolve runs the steps on one
+  // vertex grid holding every block (merged, created on first use); merge
+  // switches it (z4c_set_merged).
+  z4c_ctx* merged = nullptr;
+  bool merge = true;
 
   // host copies
   std::vector<double> h_xf, h_xv, h_dx;  // h_dx: [nblocks][3]

@@ -128,10 +128,12 @@ template <int T, int MINB>
 void launch_points(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
                    double* rhs, int block0, int nblk, cudaStream_t st) {
   const int64_t n = interior_count(g) * nblk;
-  const bool fx = has_fixed_geometry(g);
-  (fx ? k_ricci_fast<T, kFixedNX, MINB> : k_ricci_fast<T, 0, 1>)<<<div_up(n, T), T, 0, st>>>(
+  const bool fx = has_fixed_geometry(g), fm = has_merged_geometry(g);
+  (fx ? k_ricci_fast<T, kFixedNX, MINB>
+      : fm ? k_ricci_fast<T, kMergedNX, 1> : k_ricci_fast<T, 0, 1>)<<<div_up(n, T), T, 0, st>>>(
       g, P, u, sc.sd, sc.rsum, block0, nblk);
-  (fx ? k_main_fast<T, kFixedNX, MINB> : k_main_fast<T, 0, 1>)<<<div_up(n, T), T, 0, st>>>(
+  (fx ? k_main_fast<T, kFixedNX, MINB>
+      : fm ? k_main_fast<T, kMergedNX, 1> : k_main_fast<T, 0, 1>)<<<div_up(n, T), T, 0, st>>>(
       g, P, u, sc.sd, sc.rsum, rhs, block0, nblk);
 }
 
@@ -150,8 +152,9 @@ void launch_fast(const Grid& g, const DevParams& P, const double* u, const RhsSc
   }
   const int ct = sh.column_threads;
   const int64_t cols = (int64_t)(g.nx[0] + 1) * (g.nx[1] + 1) * NVAR * nblk;
-  (has_fixed_geometry(g) ? k_col_fast<kFixedNX + 1, kFixedNX, STAGE>
-                         : k_col_fast<4, 0, STAGE>)<<<div_up(cols, ct), ct, 0, st>>>(
+  (has_fixed_geometry(g)    ? k_col_fast<kFixedNX + 1, kFixedNX, STAGE>
+   : has_merged_geometry(g) ? k_col_fast<4, kMergedNX, STAGE>
+                            : k_col_fast<4, 0, STAGE>)<<<div_up(cols, ct), ct, 0, st>>>(
       g, P, u, rhs, u1, u_out, w, block0, nblk);
   add_kernel_launches(3);
 }

@@ -57,7 +57,7 @@ template <int NX>
 __global__ void __launch_bounds__(kPointThreads)
 k_prep(Grid gin, DevParams P, const double* __restrict__ u, double* __restrict__ sd, int block0) {
   const Grid g = fixed_geometry<NX>(gin);
-  constexpr int kUnroll = NX > 0 ? NX + 1 : 4;  // the whole z loop when fixed
+  constexpr int kUnroll = NX > 0 && NX <= 16 ? NX + 1 : 4;  // the whole z loop of a small block
   const int comp = blockIdx.y;
   const int slot = comp / 3, dir = comp % 3;
   const int b = block0 + (int)blockIdx.z;
@@ -1322,7 +1322,8 @@ static void launch_rhs_passes(const Grid& g, const DevParams& P, const double* u
   } else {
     const int64_t cprep = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7);  // widest component region
     COUNTED
-    (has_fixed_geometry(g) ? k_prep<kFixedNX> : k_prep<0>)<<<dim3(div_up(cprep, kPointThreads),
+    (has_fixed_geometry(g) ? k_prep<kFixedNX>
+                         : has_merged_geometry(g) ? k_prep<kMergedNX> : k_prep<0>)<<<dim3(div_up(cprep, kPointThreads),
                                                                  kSdComponents, nblk),
                                                             kPointThreads, 0, st>>>(
         g, P, u, sc.sd, block0);

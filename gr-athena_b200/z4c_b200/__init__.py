@@ -58,7 +58,8 @@ EXPORTS = (
     "z4c_restart_load", "z4c_restart_save", "z4c_adj_setup", "z4c_tlm_step", "z4c_adj_step",
     "z4c_adj_objective", "z4c_adj_objective_adj", "z4c_adj_params", "z4c_adj_gradient",
     "z4c_adj_adm_to_z4c", "z4c_set_contract", "z4c_get_contract", "z4c_set_point_regs",
-    "z4c_get_point_regs", "z4c_adj_snapshots", "z4c_adj_set_weyl")
+    "z4c_get_point_regs", "z4c_adj_snapshots", "z4c_adj_set_weyl", "z4c_set_merged",
+    "z4c_get_merged")
 
 
 class Z4cError(RuntimeError):
@@ -151,6 +152,8 @@ def lib():
         L.z4c_set_tile.argtypes = [vp, ip, ip, ip]
         L.z4c_get_tile.argtypes = [vp, C.POINTER(C.c_int)]
         L.z4c_set_contract.argtypes = [vp, ip]
+        L.z4c_set_merged.argtypes = [vp, ip]
+        L.z4c_get_merged.argtypes = [vp, C.POINTER(C.c_int)]
         L.z4c_get_contract.argtypes = [vp, C.POINTER(C.c_int)]
         L.z4c_set_point_regs.argtypes = [vp, ip]
         L.z4c_adj_snapshots.argtypes = [vp, ip, C.POINTER(C.c_int)]
@@ -684,6 +687,17 @@ class Z4c:
     def get_contract(self):
         v = C.c_int()
         _check(lib().z4c_get_contract(self._h, C.byref(v)))
+        return bool(v.value)
+
+    def set_merged(self, on):
+        """Allows (True, the default) or forbids the merged vertex grid of
+        z4c_evolve on uniform meshes (see z4c_set_merged)."""
+        _check(lib().z4c_set_merged(self._h, int(bool(on))))
+
+    def get_merged(self):
+        """Whether the next evolve runs on the merged vertex grid."""
+        v = C.c_int()
+        _check(lib().z4c_get_merged(self._h, C.byref(v)))
         return bool(v.value)
 
     def get_tile(self):

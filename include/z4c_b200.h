@@ -397,6 +397,22 @@ int z4c_set_contract(z4c_ctx *ctx, int on);
 int z4c_set_point_regs(z4c_ctx *ctx, int regs);
 int z4c_get_point_regs(const z4c_ctx *ctx, int *regs);
 int z4c_get_contract(const z4c_ctx *ctx, int *on);
+/* Merged grid (no reference counterpart): on a uniform single-level mesh
+ * with outflow faces, the contracted path with the low-storage integrator
+ * runs the steps of z4c_evolve on one vertex grid that holds every block
+ * (nb*nx cells per axis plus the ghosts), so that no vertex is stored twice
+ * and no ghost exchange runs between the blocks; the state (u, and the ADM
+ * and constraint registers the step writes) is copied from the blocks at the
+ * start of the call and back to them, every vertex and ghost, at its end.
+ * The blocks' shared vertices then hold one value where the reference
+ * averages its owners' copies (equal up to rounding), so results agree with
+ * the block-by-block evolution to round-off, as the contracted path does
+ * anyway.  It assumes the state's ghosts are those of a ghost fill (as every
+ * state this library or the reference produces).  on = 1 (the default)
+ * allows it, 0 keeps the blocks; z4c_get_merged reports whether the next
+ * z4c_evolve will use it. */
+int z4c_set_merged(z4c_ctx *ctx, int on);
+int z4c_get_merged(const z4c_ctx *ctx, int *on);
 /* Autotuner (no reference counterpart): times one fused low-storage stage on
  * the context's current state for each candidate shape (the Ricci/main CTA
  * size first, then the column-pass shape; reps timed launches each after a
