@@ -122,6 +122,9 @@ def parse():
                     help="MeshBlocks per axis (8 = the 128^3 workload; smaller for profiling)")
     ap.add_argument("--profile-run", action="store_true",
                     help="graph-captured steps and the stage kernel only (for ncu)")
+    ap.add_argument("--stage-profile", action="store_true",
+                    help="profiling aid: only the contracted stage sequence, three times, on "
+                         "the merged grid of --nb^3 MeshBlocks (one block of 16 nb cells)")
     ap.add_argument("--shape", default=None,
                     help="launch shape point_threads,column_threads,column_slabs instead of "
                          "the autotuner's pick (profiling under ncu, whose serialised launches "
@@ -762,6 +765,23 @@ def main():
     from z4c_b200 import initial_data as ID
 
     torch.cuda.set_device(local_rank)
+    if args.stage_profile:
+        n_m, lim = 16 * args.nb, 2.0 * args.nb
+        mmesh = Z.Mesh([1] * 3, [n_m] * 3, [-lim] * 3, [lim] * 3, "outflow")
+        params = Z.default_params(**PARAMS)
+        sctx = Z.Z4c(mmesh, params, "rk4")
+        sctx.set_contract(True)
+        if args.shape:
+            sctx.set_tile(*(int(v) for v in args.shape.split(",")))
+        ID.load_adm(sctx, ID.punctures(mmesh, params, masses=(1.0,), centres=((0.0, 0.0, 0.0),)))
+        sctx.init_finalize()
+        dt = CFL * float(np.min(sctx.dx()))
+        for _ in range(3):
+            sctx.rhs_stage(2, dt)
+        sctx.sync()
+        print(json.dumps({"stage_profile": True, "cells": n_m}), flush=True)
+        sctx.close()
+        return
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))

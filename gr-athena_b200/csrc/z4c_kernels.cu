@@ -1340,10 +1340,10 @@ void launch_prep(const Grid& g, const DevParams& P, const double* u, double* sd,
                  int nblk, cudaStream_t st) {
   const int64_t cprep = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7);  // widest component region
   COUNTED
-  (has_fixed_geometry(g) ? k_prep<kFixedNX> : k_prep<0>)<<<dim3(div_up(cprep, kPointThreads),
-                                                               kSdComponents, nblk),
-                                                          kPointThreads, 0, st>>>(g, P, u, sd,
-                                                                                  block0);
+  (has_fixed_geometry(g)    ? k_prep<kFixedNX>
+   : has_merged_geometry(g) ? k_prep<kMergedNX>
+                            : k_prep<0>)<<<dim3(div_up(cprep, kPointThreads), kSdComponents, nblk),
+                                            kPointThreads, 0, st>>>(g, P, u, sd, block0);
 }
 
 void launch_prep_ricci(const Grid& g, const DevParams& P, const double* u, const RhsScratch& sc,
