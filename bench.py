@@ -98,7 +98,7 @@ WAVE_SPHERES = ((6.0, 30, 8), (12.0, 30, 8))
 STAGE_TRAFFIC_PER_POINT = {0: 1350.0e6 / (64 * 17 ** 3), 1: 1025.6e6 / (64 * 17 ** 3),
                            # the contracted stage on a merged grid: ncu on the 97^3-vertex
                            # grid of 6^3 blocks (registers 204 MB), per vertex
-                           "merged": 2154.3e6 / 97 ** 3}
+                           "merged": 2153.4e6 / 97 ** 3}
 
 
 def parse():
