@@ -162,6 +162,25 @@ int exchange_into(z4c_ctx* c, const double* src, double* dst, bool alg) {
 // operator sequence with one RHS launch per block.
 int run_stage_body(z4c_ctx* c, int stage, double dt);
 
+// The vertices of one block on its three upper boundary planes (index
+// NG + nx along one axis), every variable, from w into out; a thread per
+// (variable, axis, vertex of the largest plane).
+__global__ void k_save_upper_planes(Grid g, const double* __restrict__ w,
+                                    double* __restrict__ out, int64_t plane) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 3 * plane * Z4C_NVAR) return;
+  const int64_t q = t % plane;
+  const int ax = (int)((t / plane) % 3), n = (int)(t / (3 * plane));
+  const int o1 = ax == 0 ? 1 : 0, o2 = ax == 2 ? 1 : 2;
+  if (q >= (int64_t)g.nn[o1] * g.nn[o2]) return;
+  int idx[3];
+  idx[ax] = NG + g.nx[ax];
+  idx[o1] = (int)(q % g.nn[o1]);
+  idx[o2] = (int)(q / g.nn[o1]);
+  const int64_t p = ((int64_t)idx[2] * g.nn[1] + idx[1]) * g.nn[0] + idx[0];
+  out[(int64_t)n * g.nvol + p] = w[(int64_t)n * g.nvol + p];
+}
+
 // One stage with the puncture trackers around it: the shift is interpolated
 // from the state at the start of the step (CalculateZ4cRHS, stage 1,
 // task_list_gr_z4c.cpp:147-153) and the positions move after the last stage
@@ -207,6 +226,28 @@ int run_stage_body(z4c_ctx* c, int stage, double dt) {
       launch_stage_ls(g, P, u, c->scratch(), c->reg[Z4C_REG_RHS], c->reg[Z4C_REG_U1], w, ls, 0,
                       g.nblocks, c->shape, c->stream);
       LAUNCH_CHECK("stage_ls");
+      if (c->in_place_fill) {
+        // a single block has no neighbours: its fill is the extrapolation and
+        // AlgConstr on every vertex, which run on w itself; the exchange
+        // would only copy w's vertices into u.  The last stage's values on
+        // the upper boundary planes, which the extrapolation overwrites, are
+        // kept in rhs (free until the next step) for the copy back to blocks.
+        if (stage == 4) {
+          const int64_t plane = std::max({(int64_t)g.nn[1] * g.nn[2], (int64_t)g.nn[0] * g.nn[2],
+                                          (int64_t)g.nn[0] * g.nn[1]});
+          const int64_t n = 3 * plane * Z4C_NVAR;
+          k_save_upper_planes<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+              g, w, c->reg[Z4C_REG_RHS], plane);
+          add_kernel_launches(1);
+          LAUNCH_CHECK("save planes");
+        }
+        launch_physical_bcs(g, w, Z4C_NVAR, c->stream);
+        LAUNCH_CHECK("physical_bcs");
+        launch_alg_constr_boundary(g, P, w, c->nbr, c->stream);
+        LAUNCH_CHECK("alg_constr");
+        std::swap(c->reg[Z4C_REG_U], c->reg[Z4C_REG_W]);
+        return Z4C_OK;
+      }
       return exchange_into(c, w, u, true);
     }
     // plain path, every operator launched per block as the task list calls
@@ -1262,8 +1303,9 @@ __global__ void k_merge_gather(Grid g, Grid m, const double* __restrict__ mg,
 }
 
 // The class-2 vertices of the u register: the merged grid's last stage
-// output (mw) at the vertex with AlgConstr applied, as the block that holds
-// the copy constrains it after its own extrapolation.
+// output at the vertex (mw: the upper boundary planes kept before the
+// extrapolation) with AlgConstr applied, as the block that holds the copy
+// constrains it after its own extrapolation.
 __global__ void k_merge_gather_copies(Grid g, Grid m, DevParams P, const double* __restrict__ mw,
                                       double* __restrict__ u) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1317,6 +1359,7 @@ int merged_evolve(z4c_ctx* c, double dt, int nsteps, int with_constraints) {
     int rc = create_impl(&d, &c->params, c->integrator, 0, nullptr, &m);
     if (rc) return rc;
     m->merge = false;
+    m->in_place_fill = true;
     c->merged = m;
   }
   z4c_ctx* m = c->merged;
@@ -1342,7 +1385,7 @@ int merged_evolve(z4c_ctx* c, double dt, int nsteps, int with_constraints) {
   {
     const int64_t n = (int64_t)c->g.nblocks * c->g.nvol;
     k_merge_gather_copies<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
-        c->g, m->g, c->dev(), m->reg[Z4C_REG_W], c->reg[Z4C_REG_U]);
+        c->g, m->g, c->dev(), m->reg[Z4C_REG_RHS], c->reg[Z4C_REG_U]);
     add_kernel_launches(1);
     LAUNCH_CHECK("merge");
   }

@@ -82,6 +82,10 @@ struct z4c_ctx {
   // switches it (z4c_set_merged).
   z4c_ctx* merged = nullptr;
   bool merge = true;
+  // The merged grid itself (one block, every face extrapolated): a stage's
+  // fill runs on the stage output, which then becomes u (u and w swap; the
+  // four stages of a step return u to its buffer).
+  bool in_place_fill = false;
 
   // host copies
   std::vector<double> h_xf, h_xv, h_dx;  // h_dx: [nblocks][3]

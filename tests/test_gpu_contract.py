@@ -164,10 +164,11 @@ def test_register_budget_changes_no_bits(contract, threads):
 
 
 @pytest.mark.parametrize("nb,lim,steps", [
-    (2, 4.0, (6, 4)),
+    ((2, 2, 2), (4.0, 4.0, 4.0), (6, 4)),
+    ((3, 2, 2), (6.0, 4.0, 4.0), (3, 3)),  # a merged grid of 48 x 32 x 32 cells
     # the benchmark's mesh: 512 blocks of 16^3, whose merged 128^3 grid runs
     # the compile-time-geometry instances of the passes
-    (8, 16.0, (2, 2))])
+    ((8, 8, 8), (16.0, 16.0, 16.0), (2, 2))])
 def test_merged_grid_evolution_matches_blocks(nb, lim, steps):
     """On a uniform outflow mesh the contracted path's z4c_evolve runs on one
     vertex grid holding every block; against the block-by-block evolution
@@ -179,7 +180,7 @@ def test_merged_grid_evolution_matches_blocks(nb, lim, steps):
     after these 10 steps)."""
     import z4c_b200 as Z
     from z4c_b200 import initial_data as ID
-    mesh = Z.Mesh((nb,) * 3, (16, 16, 16), (-lim,) * 3, (lim,) * 3, "outflow")
+    mesh = Z.Mesh(nb, (16, 16, 16), tuple(-v for v in lim), lim, "outflow")
     params = Z.default_params(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02, shift_eta=2.0,
                               r_max_con=1e300)
     adm = ID.punctures(mesh, params, masses=(1.0,), centres=((0.3, 0.15, -0.1),))
