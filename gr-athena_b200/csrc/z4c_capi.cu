@@ -1349,6 +1349,12 @@ bool merge_eligible(const z4c_ctx* c) {
 }
 
 int merged_evolve(z4c_ctx* c, double dt, int nsteps, int with_constraints) {
+  {  // the merged grid lives on the context's device, which must be current
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != c->device)
+      return fail(Z4C_EINVAL, "z4c_evolve: device %d is current, the context lives on %d", cur,
+                  c->device);
+  }
   if (!c->merged) {
     z4c_mesh_desc_t d = c->desc;
     for (int a = 0; a < 3; ++a) {
@@ -1545,6 +1551,12 @@ int z4c_evolve_jobs(z4c_ctx* ctx, int njobs, const double* const* host_in,
   if (nsteps < 0) return fail(Z4C_EINVAL, "negative step count");
   for (int j = 0; j < njobs; ++j)
     if (!host_in[j] || !host_out[j]) return fail(Z4C_EINVAL, "null host buffer of job %d", j);
+  {  // the staging and copy streams live on the context's device
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != ctx->device)
+      return fail(Z4C_EINVAL, "z4c_evolve_jobs: device %d is current, the context lives on %d",
+                  cur, ctx->device);
+  }
   int rc = jobs_setup(ctx);
   if (rc) return rc;
   JobPipe* J = ctx->jobs;
