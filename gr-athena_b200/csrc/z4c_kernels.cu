@@ -1487,8 +1487,10 @@ void launch_alg_constr_boundary(const Grid& g, const DevParams& P, double* u, co
                                 cudaStream_t st) {
   const int64_t n = g.nvol * g.nblocks;
   COUNTED
-  (has_fixed_geometry(g) ? k_alg_constr_boundary<kFixedNX> : k_alg_constr_boundary<0>)<<<
-      div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, P, u, nbr);
+  (has_fixed_geometry(g)    ? k_alg_constr_boundary<kFixedNX>
+   : has_merged_geometry(g) ? k_alg_constr_boundary<kMergedNX>
+                            : k_alg_constr_boundary<0>)<<<div_up(n, kPointThreads), kPointThreads,
+                                                         0, st>>>(g, P, u, nbr);
 }
 
 void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st) {
@@ -1500,10 +1502,10 @@ void launch_physical_bcs(const Grid& g, double* u, int nvar, cudaStream_t st) {
     const int o1 = (ax == 0) ? 1 : 0, o2 = (ax == 2) ? 1 : 2;
     const int64_t n = (int64_t)g.nn[o1] * g.nn[o2] * 2 * nvar * g.nb[o1] * g.nb[o2];
     COUNTED
-    const bool fx = has_fixed_geometry(g);
-    auto kern = ax == 0 ? (fx ? k_bc_axis<kFixedNX, 0> : k_bc_axis<0, 0>)
-                : ax == 1 ? (fx ? k_bc_axis<kFixedNX, 1> : k_bc_axis<0, 1>)
-                          : (fx ? k_bc_axis<kFixedNX, 2> : k_bc_axis<0, 2>);
+    const bool fx = has_fixed_geometry(g), fm = has_merged_geometry(g);
+    auto kern = ax == 0   ? (fx ? k_bc_axis<kFixedNX, 0> : fm ? k_bc_axis<kMergedNX, 0> : k_bc_axis<0, 0>)
+                : ax == 1 ? (fx ? k_bc_axis<kFixedNX, 1> : fm ? k_bc_axis<kMergedNX, 1> : k_bc_axis<0, 1>)
+                          : (fx ? k_bc_axis<kFixedNX, 2> : fm ? k_bc_axis<kMergedNX, 2> : k_bc_axis<0, 2>);
     kern<<<div_up(n, kPointThreads), kPointThreads, 0, st>>>(g, u, nvar);
   }
 }
