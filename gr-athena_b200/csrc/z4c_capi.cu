@@ -1504,11 +1504,14 @@ int jobs_issue(z4c_ctx* c, int j, double* host_out, double dt, int nsteps) {
   LAUNCH_CHECK("hst");
   // the output slot is free once the download of job j - 2 has left it
   CUDA_TRY(cudaStreamWaitEvent(c->stream, J->out_free[s], 0));
-  CUDA_TRY(cudaMemcpyAsync(J->out[s], c->reg[Z4C_REG_U], reg, cudaMemcpyDeviceToDevice, c->stream));
+  if (host_out)
+    CUDA_TRY(cudaMemcpyAsync(J->out[s], c->reg[Z4C_REG_U], reg, cudaMemcpyDeviceToDevice,
+                             c->stream));
   CUDA_TRY(cudaMemcpyAsync(J->part[s], c->partials, part, cudaMemcpyDeviceToDevice, c->stream));
   CUDA_TRY(cudaEventRecord(J->out_ready[s], c->stream));
   CUDA_TRY(cudaStreamWaitEvent(J->d2h, J->out_ready[s], 0));
-  CUDA_TRY(cudaMemcpyAsync(host_out, J->out[s], reg, cudaMemcpyDeviceToHost, J->d2h));
+  if (host_out)
+    CUDA_TRY(cudaMemcpyAsync(host_out, J->out[s], reg, cudaMemcpyDeviceToHost, J->d2h));
   CUDA_TRY(cudaMemcpyAsync(J->hpart[s], J->part[s], part, cudaMemcpyDeviceToHost, J->d2h));
   CUDA_TRY(cudaEventRecord(J->out_free[s], J->d2h));
   return Z4C_OK;
@@ -1547,10 +1550,11 @@ static int jobs_hst(z4c_ctx* c, int j, double* hst_out) {
 int z4c_evolve_jobs(z4c_ctx* ctx, int njobs, const double* const* host_in,
                     double* const* host_out, double* hst_out, double dt, int nsteps) {
   if (!ctx) return fail(Z4C_EINVAL, "null context");
-  if (njobs < 1 || !host_in || !host_out) return fail(Z4C_EINVAL, "need njobs >= 1 and job arrays");
+  if (njobs < 1 || !host_in) return fail(Z4C_EINVAL, "need njobs >= 1 and the input array");
   if (nsteps < 0) return fail(Z4C_EINVAL, "negative step count");
   for (int j = 0; j < njobs; ++j)
-    if (!host_in[j] || !host_out[j]) return fail(Z4C_EINVAL, "null host buffer of job %d", j);
+    if (!host_in[j] || (host_out && !host_out[j]))
+      return fail(Z4C_EINVAL, "null host buffer of job %d", j);
   {  // the staging and copy streams live on the context's device
     int cur = -1;
     if (cudaGetDevice(&cur) != cudaSuccess || cur != ctx->device)
@@ -1568,7 +1572,7 @@ int z4c_evolve_jobs(z4c_ctx* ctx, int njobs, const double* const* host_in,
   for (int j = 0; j < njobs && rc == Z4C_OK; ++j) {
     if (j + 1 < njobs) rc = jobs_upload(ctx, j + 1, host_in[j + 1]);
     if (rc == Z4C_OK && j >= 2) rc = jobs_hst(ctx, summed++, hst_out);
-    if (rc == Z4C_OK) rc = jobs_issue(ctx, j, host_out[j], dt, nsteps);
+    if (rc == Z4C_OK) rc = jobs_issue(ctx, j, host_out ? host_out[j] : nullptr, dt, nsteps);
   }
   // every job has finished (or failed) before the buffers are handed back
   const cudaError_t e1 = cudaStreamSynchronize(J->h2d);

@@ -761,17 +761,18 @@ class Z4c:
         """Evolves independent states from host memory (z4c_evolve_jobs):
         inputs[j] (u registers) -> outputs[j] after nsteps steps of dt, with
         the copies of one job overlapping the evolution of the next; returns
-        the history norms, one row of eight per job.  Page-locked arrays
-        (e.g. torch's pin_memory) let the copies overlap."""
+        the history norms, one row of eight per job.  outputs None: the norms
+        only.  Page-locked arrays (e.g. torch's pin_memory) let the copies
+        overlap."""
         n = len(inputs)
-        if n < 1 or len(outputs) != n:
+        if n < 1 or (outputs is not None and len(outputs) != n):
             raise ValueError("need as many outputs as inputs, at least one")
         shape = self.shape(REG_U)
-        for a in list(inputs) + list(outputs):
+        for a in list(inputs) + list(outputs or []):
             if a.shape != shape or a.dtype != np.float64 or not a.flags.c_contiguous:
                 raise ValueError("job arrays must be contiguous float64 u registers")
         hin = (C.c_void_p * n)(*[a.ctypes.data for a in inputs])
-        hout = (C.c_void_p * n)(*[a.ctypes.data for a in outputs])
+        hout = None if outputs is None else (C.c_void_p * n)(*[a.ctypes.data for a in outputs])
         h = np.empty((n, 8)) if hst is None else hst
         _check(lib().z4c_evolve_jobs(self._h, n, hin, hout,
                                      h.ctypes.data_as(C.POINTER(C.c_double)), float(dt),

@@ -4,7 +4,8 @@ copies of one job overlapping the evolution of the next.
 Every job must give what the sequential calls give (upload, z4c_evolve with
 the constraints, z4c_hst_norms, download) bit for bit: the pipeline changes
 where the copies run, not the arithmetic.  Five jobs exercise the reuse of
-the two staging slots; page-locked and pageable host buffers both run.
+the two staging slots; page-locked and pageable host buffers both run, and
+so does a call that downloads the norms only.
 """
 import ctypes as C
 
@@ -75,4 +76,8 @@ def test_jobs_match_sequential_calls(pinned):
     # a single job
     hst = ctx.evolve_jobs(inputs[1:2], outputs[:1], dt, nsteps)
     assert np.array_equal(outputs[0], expect[1]) and np.array_equal(hst[0], expect_hst[1])
+    # the norms only
+    hst = ctx.evolve_jobs(inputs, None, dt, nsteps)
+    for j in range(len(states)):
+        assert np.array_equal(hst[j], expect_hst[j]), f"job {j}, norms only"
     ctx.close()
