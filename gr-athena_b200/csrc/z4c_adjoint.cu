@@ -1646,7 +1646,7 @@ int weyl_psi(z4c_ctx* c, const double* u) {
   const Grid& g = c->g;
   const DevParams P = c->dev();
   launch_z4c_to_adm(g, P, u, A->admw, 0, g.nblocks, c->stream);
-  launch_weyl(g, P, A->admw, u, c->sd, A->wreg, c->xf, 0, g.nblocks, c->stream);
+  launch_weyl(g, P, A->admw, u, c->sd, c->rsum, c->lv, A->wreg, c->xf, 0, g.nblocks, c->stream);
   ALAUNCH("Weyl");
   if (c->ml) {
     int rc = launch_ml_exchange(*c->ml, A->wreg, A->wtmp, Z4C_NWEYL, Z4C_NWEYL, c->stream);

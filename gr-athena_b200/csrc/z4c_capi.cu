@@ -866,7 +866,7 @@ int z4c_weyl(z4c_ctx* ctx, int reg_adm, int reg_u, int reg_weyl, int block) {
       reg_nvar_(reg_weyl) != Z4C_NWEYL)
     return fail(Z4C_EINVAL, "Z4cWeyl needs the ADM, a Z4c and the Weyl register");
   if ((rc = check_block(ctx, block, &b0, &nb))) return rc;
-  launch_weyl(ctx->g, ctx->dev(), ctx->reg[reg_adm], ctx->reg[reg_u], ctx->sd,
+  launch_weyl(ctx->g, ctx->dev(), ctx->reg[reg_adm], ctx->reg[reg_u], ctx->sd, ctx->rsum, ctx->lv,
               ctx->reg[reg_weyl], ctx->xf, b0, nb, ctx->stream);
   LAUNCH_CHECK("weyl");
   return Z4C_OK;

@@ -1093,11 +1093,51 @@ k_adm_constraints(Grid gin, DevParams P, const double* __restrict__ adm,
 // ---- Weyl scalar psi4 (z4c/calculate_weyl_scalars.cpp:44-630) --------------
 // One thread per vertex of the requested blocks; interior vertices get psi4,
 // every other vertex NaN (the reference fills the register with NaN first).
-template <int NX>
+// In three passes over the interior vertices: the Ricci tensor and its trace
+// (k_weyl_curv<NX, 0>: Rd into rs [block][6][interior vertex], R into ks
+// [block][22][...] slot 19), K and its covariant derivative (k_weyl_curv<NX,
+// 1>: DK into ks slots 0-17, K into slot 18), then the tetrad and the
+// contractions per vertex (k_weyl_psi), NaN outside the interior.  The
+// single pass spilled; each part holds about half its state.
+template <int NX, int PART>
 __global__ void __launch_bounds__(128, 1)
-k_weyl(Grid gin, DevParams P, const double* __restrict__ adm, const double* __restrict__ u,
-       const double* __restrict__ sd, double* __restrict__ weyl, const double* __restrict__ xf,
-       int block0, int nblk) {
+k_weyl_curv(Grid gin, DevParams P, const double* __restrict__ adm, const double* __restrict__ u,
+            const double* __restrict__ sd, double* __restrict__ rs, double* __restrict__ ks,
+            int block0, int nblk) {
+  const Grid g = fixed_geometry<NX>(gin);
+  const int64_t npts = interior_count(g);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * nblk) return;
+  const int b = block0 + (int)(t / npts);
+  const int64_t l = t % npts;
+  int i, j, k;
+  interior_ijk(g, l, i, j, k);
+  const int64_t p = ((int64_t)k * g.nn[1] + j) * g.nn[0] + i;
+  double Rd[6], R, K, DK[3][6];
+  weyl_curvature<PART == 0, PART == 1>(u + (int64_t)b * NVAR * g.nvol,
+                                       adm + (int64_t)b * Z4C_NADM * g.nvol,
+                                       sd + (int64_t)b * kSdComponents * g.nvol, g.nvol, p, g.s,
+                                       P, P.fd[b], Rd, R, K, DK);
+  double* q = ks + (int64_t)b * NVAR * npts + l;
+  if constexpr (PART == 0) {
+    double* r = rs + (int64_t)b * 6 * npts + l;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) r[(int64_t)c * npts] = Rd[c];
+    q[19 * npts] = R;
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) q[(int64_t)(a * 6 + c) * npts] = DK[a][c];
+    q[18 * npts] = K;
+  }
+}
+
+template <int NX>
+__global__ void __launch_bounds__(128)
+k_weyl_psi(Grid gin, const double* __restrict__ adm, const double* __restrict__ rs,
+           const double* __restrict__ ks, double* __restrict__ weyl,
+           const double* __restrict__ xf, int block0, int nblk) {
   const Grid g = fixed_geometry<NX>(gin);
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.nvol * nblk) return;
@@ -1111,10 +1151,25 @@ k_weyl(Grid gin, DevParams P, const double* __restrict__ adm, const double* __re
                   k <= NG + g.nx[2];
   double rp = __longlong_as_double(0x7ff8000000000000LL), ip = rp;
   if (in) {
+    const int64_t npts = interior_count(g);
+    const int64_t l = ((int64_t)(k - NG) * (g.nx[1] + 1) + (j - NG)) * (g.nx[0] + 1) + (i - NG);
+    const double* r = rs + (int64_t)b * 6 * npts + l;
+    const double* q = ks + (int64_t)b * NVAR * npts + l;
+    const double* A = adm + (int64_t)b * Z4C_NADM * g.nvol + p;
+    double Rd[6], DK[3][6], gph[6], Kd[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      Rd[c] = r[(int64_t)c * npts];
+      gph[c] = A[(int64_t)(Z4C_ADM_GXX + c) * g.nvol];
+      Kd[c] = A[(int64_t)(Z4C_ADM_KXX + c) * g.nvol];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) DK[a][c] = q[(int64_t)(a * 6 + c) * npts];
     const double* x = xf + (int64_t)b * (g.nn[0] + g.nn[1] + g.nn[2]);
-    weyl_point(u + (int64_t)b * NVAR * g.nvol, adm + (int64_t)b * Z4C_NADM * g.nvol,
-               sd + (int64_t)b * kSdComponents * g.nvol, g.nvol, p, g.s, P, P.fd[b], x[i],
-               x[g.nn[0] + j], x[g.nn[0] + g.nn[1] + k], &rp, &ip);
+    weyl_contract(gph, Kd, Rd, q[19 * npts], q[18 * npts], DK, x[i], x[g.nn[0] + j],
+                  x[g.nn[0] + g.nn[1] + k], &rp, &ip);
   }
   wb[0] = rp;
   wb[g.nvol] = ip;
@@ -1567,18 +1622,26 @@ void launch_adm_constraints(const Grid& g, const DevParams& P, const double* adm
 }
 
 void launch_weyl(const Grid& g, const DevParams& P, const double* adm, const double* u,
-                 double* sd, double* weyl, const double* xf, int block0, int nblk,
-                 cudaStream_t st) {
+                 double* sd, double* rs, double* ks, double* weyl, const double* xf, int block0,
+                 int nblk, cudaStream_t st) {
   const int64_t cprep = (int64_t)(g.nx[0] + 7) * (g.nx[1] + 7);  // widest component region
   COUNTED
   (has_fixed_geometry(g) ? k_prep<kFixedNX> : k_prep<0>)<<<dim3(div_up(cprep, kPointThreads),
                                                                kSdComponents, nblk),
                                                           kPointThreads, 0, st>>>(
       g, P, u, sd, block0);
+  const int64_t m = interior_count(g) * nblk;
+  const bool fx = has_fixed_geometry(g);
+  COUNTED
+  (fx ? k_weyl_curv<kFixedNX, 0> : k_weyl_curv<0, 0>)<<<div_up(m, 128), 128, 0, st>>>(
+      g, P, adm, u, sd, rs, ks, block0, nblk);
+  COUNTED
+  (fx ? k_weyl_curv<kFixedNX, 1> : k_weyl_curv<0, 1>)<<<div_up(m, 128), 128, 0, st>>>(
+      g, P, adm, u, sd, rs, ks, block0, nblk);
   const int64_t n = g.nvol * nblk;
   COUNTED
-  (has_fixed_geometry(g) ? k_weyl<kFixedNX> : k_weyl<0>)<<<div_up(n, 128), 128, 0, st>>>(
-      g, P, adm, u, sd, weyl, xf, block0, nblk);
+  (has_fixed_geometry(g) ? k_weyl_psi<kFixedNX> : k_weyl_psi<0>)<<<div_up(n, 128), 128, 0, st>>>(
+      g, adm, rs, ks, weyl, xf, block0, nblk);
 }
 
 void launch_hst(const Grid& g, const DevParams& P, const double* con, const double* u,

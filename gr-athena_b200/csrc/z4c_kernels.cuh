@@ -160,10 +160,11 @@ void launch_adm_constraints(const Grid& g, const DevParams& P, const double* adm
                             const double* u, double* con, const double* xf, int block0,
                             int nblk, cudaStream_t st);
 // Z4cWeyl on blocks [block0, block0+nblk): the stored first derivatives of u
-// into sd (k_prep), then psi4 (2 variables) into weyl.
+// into sd (k_prep), the curvature terms into the scratch rs (6 values per
+// interior vertex) and ks (22), then psi4 (2 variables) into weyl.
 void launch_weyl(const Grid& g, const DevParams& P, const double* adm, const double* u,
-                 double* sd, double* weyl, const double* xf, int block0, int nblk,
-                 cudaStream_t st);
+                 double* sd, double* rs, double* ks, double* weyl, const double* xf, int block0,
+                 int nblk, cudaStream_t st);
 void launch_hst(const Grid& g, const DevParams& P, const double* con, const double* u,
                 const double* xv, double* partials, cudaStream_t st);
 void launch_check_finite(const Grid& g, const double* u, int nvar, int* flag, cudaStream_t st);

@@ -15,12 +15,18 @@
 
 namespace z4c {
 
-__device__ __forceinline__ void weyl_point(const double* __restrict__ uB,
-                                           const double* __restrict__ admB,
-                                           const double* __restrict__ sdB, int64_t nvol,
-                                           int64_t p, const int64_t s[3], const DevParams& P,
-                                           const FdScale& F, double x1, double x2, double x3,
-                                           double* rpsi4, double* ipsi4) {
+// First phase: with RICCI the spatial Ricci tensor Rd (symmetric, 6) and its
+// trace R with the physical inverse metric, with DKPART the trace K of the
+// extrinsic curvature and its covariant derivative DK[a][sym(b,c)] = D_a K_bc
+// (18); each part recomputes the metric derivatives and Christoffels it
+// needs, so that either runs on half the live state.
+template <bool RICCI = true, bool DKPART = true>
+__device__ __forceinline__ void weyl_curvature(const double* __restrict__ uB,
+                                               const double* __restrict__ admB,
+                                               const double* __restrict__ sdB, int64_t nvol,
+                                               int64_t p, const int64_t s[3], const DevParams& P,
+                                               const FdScale& F, double Rd[6], double& R,
+                                               double& K, double DK[3][6]) {
   const z4c_params_t& opt = P.p;
   const double* U = uB + p;
   const double* AD = admB + p;
@@ -52,38 +58,40 @@ __device__ __forceinline__ void weyl_point(const double* __restrict__ uB,
       const double d3 = WSDV(kSdG + q, c);
       if (pw == -4.) dg[c][q] = oochi * (d3 - oochi * gt[q] * dchi[c]);
       else dg[c][q] = psi4c * (d3 + fac * oochi * gt[q] * dchi[c]);
-      dK[c][q] = fd_dx(AV(Z4C_ADM_KXX + q), s[c], F.cidx1[c]);
+      if constexpr (DKPART) dK[c][q] = fd_dx(AV(Z4C_ADM_KXX + q), s[c], F.cidx1[c]);
     }
-  // pass 2: physical second derivatives ddg(a,b,c,d) = d_a d_b gamma_cd; the
-  // mixed a < b ones are D_a of the stored D_b g~_cd
   double DDG[6][6];  // [sym(a,b)][sym(c,d)]
+  if constexpr (RICCI) {
+    // pass 2: physical second derivatives ddg(a,b,c,d) = d_a d_b gamma_cd; the
+    // mixed a < b ones are D_a of the stored D_b g~_cd
 #pragma unroll
-  for (int ab = 0; ab < 6; ++ab) {
-    const int a = pair_a(ab), b = pair_b(ab);
-    const double ddchi = fd_d2(UV(Z4C_CHI), WSDF(kSdChi), nvol, ab, s, F);
-    const double dchi_a = dchi[a], dchi_b = dchi[b];
+    for (int ab = 0; ab < 6; ++ab) {
+      const int a = pair_a(ab), b = pair_b(ab);
+      const double ddchi = fd_d2(UV(Z4C_CHI), WSDF(kSdChi), nvol, ab, s, F);
+      const double dchi_a = dchi[a], dchi_b = dchi[b];
 #pragma unroll
-    for (int cd = 0; cd < 6; ++cd) {
-      const double gtil = gt[cd];
-      const double ddg_conf = fd_d2(UV(Z4C_GXX + cd), WSDF(kSdG + cd), nvol, ab, s, F);
-      const double da3 = WSDV(kSdG + cd, a), db3 = WSDV(kSdG + cd, b);
-      double v;
-      if (a == b) {
-        if (pw == -4.)
-          v = oochi * (ddg_conf - oochi * (2.0 * dchi_a * da3 + ddchi * gtil) +
-                       2.0 * oochi * oochi * dchi_a * dchi_a * gtil);
-        else
-          v = psi4c * (ddg_conf + fac * oochi * (2.0 * dchi_a * da3 + ddchi * gtil) +
-                       fac * fac2 * oochi * oochi * dchi_a * dchi_a * gtil);
-      } else {
-        if (pw == -4.)
-          v = oochi * (ddg_conf - oochi * (dchi_a * db3 + dchi_b * da3 + ddchi * gtil) +
-                       2.0 * oochi * oochi * dchi_a * dchi_b * gtil);
-        else
-          v = psi4c * (ddg_conf + fac * oochi * (dchi_a * db3 + dchi_b * da3 + ddchi * gtil) +
-                       fac * fac2 * oochi * oochi * dchi_a * dchi_b * gtil);
+      for (int cd = 0; cd < 6; ++cd) {
+        const double gtil = gt[cd];
+        const double ddg_conf = fd_d2(UV(Z4C_GXX + cd), WSDF(kSdG + cd), nvol, ab, s, F);
+        const double da3 = WSDV(kSdG + cd, a), db3 = WSDV(kSdG + cd, b);
+        double v;
+        if (a == b) {
+          if (pw == -4.)
+            v = oochi * (ddg_conf - oochi * (2.0 * dchi_a * da3 + ddchi * gtil) +
+                         2.0 * oochi * oochi * dchi_a * dchi_a * gtil);
+          else
+            v = psi4c * (ddg_conf + fac * oochi * (2.0 * dchi_a * da3 + ddchi * gtil) +
+                         fac * fac2 * oochi * oochi * dchi_a * dchi_a * gtil);
+        } else {
+          if (pw == -4.)
+            v = oochi * (ddg_conf - oochi * (dchi_a * db3 + dchi_b * da3 + ddchi * gtil) +
+                         2.0 * oochi * oochi * dchi_a * dchi_b * gtil);
+          else
+            v = psi4c * (ddg_conf + fac * oochi * (dchi_a * db3 + dchi_b * da3 + ddchi * gtil) +
+                         fac * fac2 * oochi * oochi * dchi_a * dchi_b * gtil);
+        }
+        DDG[ab][cd] = v;
       }
-      DDG[ab][cd] = v;
     }
   }
   // inverse physical metric
@@ -113,57 +121,80 @@ __device__ __forceinline__ void weyl_point(const double* __restrict__ uB,
         for (int d = 0; d < 3; ++d) acc += GUU(c, d) * Gddd[d][sidx(a, b)];
         Gudd[c][sidx(a, b)] = acc;
       }
-  // Ricci tensor and scalar
-  double Rd[6], R = 0.0;
+  if constexpr (RICCI) {
+    // Ricci tensor and scalar
+    R = 0.0;
 #pragma unroll
-  for (int a = 0; a < 3; ++a)
+    for (int a = 0; a < 3; ++a)
 #pragma unroll
-    for (int b = a; b < 3; ++b) {
-      double acc = 0.0;
+      for (int b = a; b < 3; ++b) {
+        double acc = 0.0;
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
+        for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
+          for (int d = 0; d < 3; ++d) {
 #pragma unroll
-          for (int e = 0; e < 3; ++e) {
-            acc += GUU(c, d) * Gudd[e][sidx(a, c)] * Gddd[e][sidx(b, d)];
-            acc -= GUU(c, d) * Gudd[e][sidx(a, b)] * Gddd[e][sidx(c, d)];
+            for (int e = 0; e < 3; ++e) {
+              acc += GUU(c, d) * Gudd[e][sidx(a, c)] * Gddd[e][sidx(b, d)];
+              acc -= GUU(c, d) * Gudd[e][sidx(a, b)] * Gddd[e][sidx(c, d)];
+            }
+            acc += 0.5 * GUU(c, d) *
+                   (-DDG[sidx(c, d)][sidx(a, b)] - DDG[sidx(a, b)][sidx(c, d)] +
+                    DDG[sidx(a, c)][sidx(b, d)] + DDG[sidx(b, c)][sidx(a, d)]);
           }
-          acc += 0.5 * GUU(c, d) *
-                 (-DDG[sidx(c, d)][sidx(a, b)] - DDG[sidx(a, b)][sidx(c, d)] +
-                  DDG[sidx(a, c)][sidx(b, d)] + DDG[sidx(b, c)][sidx(a, d)]);
-        }
-      Rd[sidx(a, b)] = acc;
-      R += ((a == b) ? 1.0 : 2.0) * GUU(a, b) * acc;
-    }
-  // trace of K and its covariant derivative DK(a,b,c) = D_a K_bc
-  double K = 0.0;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    double kaa = 0.0;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) kaa += GUU(a, c) * Kd[sidx(c, a)];
-    K += kaa;
-  }
-  // DK is stored symmetric in (b,c) and filled over all (b,c): the entry
-  // b < c keeps the value of the later (c,b) pass, whose two subtractions run
-  // in the other order
-  double DK[3][6];
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int lo = 0; lo < 3; ++lo)
-#pragma unroll
-      for (int hi = lo; hi < 3; ++hi) {
-        const int b = hi, c = lo;
-        double v = dK[a][sidx(b, c)];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          v -= Gudd[d][sidx(a, b)] * Kd[sidx(d, c)];
-          v -= Gudd[d][sidx(a, c)] * Kd[sidx(b, d)];
-        }
-        DK[a][sidx(lo, hi)] = v;
+        Rd[sidx(a, b)] = acc;
+        R += ((a == b) ? 1.0 : 2.0) * GUU(a, b) * acc;
       }
+  }
+  if constexpr (DKPART) {
+    // trace of K and its covariant derivative DK(a,b,c) = D_a K_bc
+    K = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      double kaa = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) kaa += GUU(a, c) * Kd[sidx(c, a)];
+      K += kaa;
+    }
+    // DK is stored symmetric in (b,c) and filled over all (b,c): the entry
+    // b < c keeps the value of the later (c,b) pass, whose two subtractions run
+    // in the other order
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int lo = 0; lo < 3; ++lo)
+#pragma unroll
+        for (int hi = lo; hi < 3; ++hi) {
+          const int b = hi, c = lo;
+          double v = dK[a][sidx(b, c)];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            v -= Gudd[d][sidx(a, b)] * Kd[sidx(d, c)];
+            v -= Gudd[d][sidx(a, c)] * Kd[sidx(b, d)];
+          }
+          DK[a][sidx(lo, hi)] = v;
+        }
+  }
+#undef GUU
+#undef UV
+#undef AV
+#undef WSDF
+#undef WSDV
+}
+
+// Second phase at the vertex (x1, x2, x3): the Gram-Schmidt tetrad and the
+// three accumulation phases of psi4 from the physical metric gph and K_ab
+// (Kd) at the vertex and the first phase's Rd, R, K, DK.
+__device__ __forceinline__ void weyl_contract(const double gph[6], const double Kd[6],
+                                              const double Rd[6], double R, double K,
+                                              const double DK[3][6], double x1, double x2,
+                                              double x3, double* rpsi4, double* ipsi4) {
+  double g_uu[6];
+  {
+    const double detg = det3(gph[0], gph[1], gph[2], gph[3], gph[4], gph[5]);
+    inv3(1. / detg, gph, g_uu);
+  }
+#define GUU(a, b) g_uu[sidx(a, b)]
   // tetrad, orthonormalised with the physical metric
   double xx = x1;
   if (x1 * x1 + x2 * x2 < 1e-10) xx = xx + 1e-8;
@@ -250,10 +281,23 @@ __device__ __forceinline__ void weyl_point(const double* __restrict__ uB,
   *rpsi4 = rp;
   *ipsi4 = ip;
 #undef GUU
-#undef UV
-#undef AV
-#undef WSDF
-#undef WSDV
+}
+
+// Both phases at one interior vertex.
+__device__ __forceinline__ void weyl_point(const double* __restrict__ uB,
+                                           const double* __restrict__ admB,
+                                           const double* __restrict__ sdB, int64_t nvol,
+                                           int64_t p, const int64_t s[3], const DevParams& P,
+                                           const FdScale& F, double x1, double x2, double x3,
+                                           double* rpsi4, double* ipsi4) {
+  double Rd[6], R, K, DK[3][6], gph[6], Kd[6];
+  weyl_curvature(uB, admB, sdB, nvol, p, s, P, F, Rd, R, K, DK);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    gph[q] = __ldg(admB + p + (int64_t)(Z4C_ADM_GXX + q) * nvol);
+    Kd[q] = __ldg(admB + p + (int64_t)(Z4C_ADM_KXX + q) * nvol);
+  }
+  weyl_contract(gph, Kd, Rd, R, K, DK, x1, x2, x3, rpsi4, ipsi4);
 }
 
 }  // namespace z4c
