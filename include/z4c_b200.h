@@ -409,9 +409,11 @@ int z4c_get_contract(const z4c_ctx *ctx, int *on);
  * averages its owners' copies (equal up to rounding), so results agree with
  * the block-by-block evolution to round-off, as the contracted path does
  * anyway.  It assumes the state's ghosts are those of a ghost fill (as every
- * state this library or the reference produces).  on = 1 (the default)
- * allows it, 0 keeps the blocks; z4c_get_merged reports whether the next
- * z4c_evolve will use it. */
+ * state this library or the reference produces).  The merged grid is a
+ * second, single-block context (about a third of the blocks' memory on 16^3
+ * blocks), created by the first z4c_evolve that uses it and held until
+ * z4c_destroy.  on = 1 (the default) allows it, 0 keeps the blocks;
+ * z4c_get_merged reports whether the next z4c_evolve will use it. */
 int z4c_set_merged(z4c_ctx *ctx, int on);
 int z4c_get_merged(const z4c_ctx *ctx, int *on);
 /* Autotuner (no reference counterpart): times one fused low-storage stage on
