@@ -1386,7 +1386,8 @@ int merged_evolve(z4c_ctx* c, double dt, int nsteps, int with_constraints) {
     CUDA_TRY(cudaMemcpyAsync(m->trk, c->trk, sizeof(double) * 8 * c->ntrk,
                              cudaMemcpyDeviceToDevice, c->stream));
   if ((rc = merge_launch(c, m, Z4C_REG_U, true))) return rc;
-  if ((rc = z4c_evolve(m, dt, nsteps, with_constraints))) return rc;
+  // the constraints are evaluated on the blocks below, not on the merged grid
+  if ((rc = z4c_evolve(m, dt, nsteps, 0))) return rc;
   if ((rc = merge_launch(c, m, Z4C_REG_U, false))) return rc;
   {
     const int64_t n = (int64_t)c->g.nblocks * c->g.nvol;
