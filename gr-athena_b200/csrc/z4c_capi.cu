@@ -1237,6 +1237,7 @@ __global__ void k_merge_scatter(Grid g, Grid m, const double* __restrict__ blk,
 // the ghosts below a lower face and the boundary vertex and the ghosts above
 // an upper face up to nn - 2, within their transverse ranges.
 __device__ int block_fill_class(const Grid& g, const int loc[3], const int l[3]) {
+  if (g.bc[0] == Z4C_BC_PERIODIC) return 1;  // periodic: the exchange writes every ghost
   bool own = true, held = true, upper = false;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -1338,13 +1339,16 @@ int merge_launch(const z4c_ctx* c, const z4c_ctx* m, int reg, bool to_merged) {
 }
 
 // Steps of z4c_evolve that run on the merged grid: uniform single-level
-// meshes with outflow faces on the contracted low-storage path.
+// meshes whose faces are all outflow or all periodic, on the contracted
+// low-storage path.
 bool merge_eligible(const z4c_ctx* c) {
   if (!c->merge || !c->shape.contract || c->ml || c->per_block || c->g.nblocks < 2 ||
       c->integrator != Z4C_INTEG_RK4)
     return false;
-  for (int f = 0; f < 6; ++f)
-    if (c->desc.bc[f] != Z4C_BC_OUTFLOW) return false;
+  const int kind = c->desc.bc[0];
+  if (kind != Z4C_BC_OUTFLOW && kind != Z4C_BC_PERIODIC) return false;
+  for (int f = 1; f < 6; ++f)
+    if (c->desc.bc[f] != kind) return false;
   return true;
 }
 
@@ -1365,7 +1369,8 @@ int merged_evolve(z4c_ctx* c, double dt, int nsteps, int with_constraints) {
     int rc = create_impl(&d, &c->params, c->integrator, 0, nullptr, &m);
     if (rc) return rc;
     m->merge = false;
-    m->in_place_fill = true;
+    // a periodic single block still runs the exchange (with itself)
+    m->in_place_fill = c->desc.bc[0] == Z4C_BC_OUTFLOW;
     c->merged = m;
   }
   z4c_ctx* m = c->merged;

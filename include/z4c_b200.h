@@ -399,7 +399,7 @@ int z4c_set_point_regs(z4c_ctx *ctx, int regs);
 int z4c_get_point_regs(const z4c_ctx *ctx, int *regs);
 int z4c_get_contract(const z4c_ctx *ctx, int *on);
 /* Merged grid (no reference counterpart): on a uniform single-level mesh
- * with outflow faces, the contracted path with the low-storage integrator
+ * whose faces are all outflow or all periodic, the contracted path with the low-storage integrator
  * runs the steps of z4c_evolve on one vertex grid that holds every block
  * (nb*nx cells per axis plus the ghosts), so that no vertex is stored twice
  * and no ghost exchange runs between the blocks; the state (u, and the ADM
