@@ -68,6 +68,8 @@ CPU_SAMPLE_STEPS = 8
 # timed RK4 steps of the refined-mesh measurement inside the headline run
 # (about 150 ms each)
 SMR_STEPS = 10
+# timed RK4 steps of the robust-stability measurement in the headline run
+RS_STEPS = 20
 # cycles of the adaptive binary run (200 as the benchmark states; about 160 ms each),
 # and of its shifted-gauge variant
 AMR_STEPS = 200
@@ -671,6 +673,42 @@ def main_smr(args):
           flush=True)
 
 
+def rs_measure(steps, warmup, contract=1):
+    """The robust-stability workload of the same batched mesh: Minkowski plus
+    seeded uniform noise of amplitude 1e-10 on every Z4c variable, 512
+    MeshBlocks of 16^3, periodic, the puncture run's gauge and damping;
+    graph-captured steps timed with CUDA events."""
+    import torch
+    import z4c_b200 as Z
+    from z4c_b200 import initial_data as ID
+    mesh = Z.Mesh([8] * 3, [16] * 3, [-16.0] * 3, [16.0] * 3, "periodic")
+    params = Z.default_params(**PARAMS)
+    ctx = Z.Z4c(mesh, params, "rk4")
+    ctx.set_contract(bool(contract))
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ID.load_z4c(ctx, ID.noise_state(mesh))
+    dt = CFL * float(np.min(ctx.dx()))
+    with torch.cuda.stream(stream):
+        ctx.evolve(dt, warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    with torch.cuda.stream(stream):
+        ctx.evolve(dt, steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out = {"value": mesh.zones() * steps / (ms * 1e-3), "unit": "zone-updates/s",
+           "ms_per_step": ms / steps, "steps": steps, "merged_grid": ctx.get_merged(),
+           "finite": ctx.check_finite(),
+           "config": "robust stability: Minkowski + uniform noise 1e-10 (seeded) on all Z4c "
+                     "variables, 128^3 cells as 512 MeshBlocks of 16^3, periodic, 1+log + "
+                     "Gamma-driver (eta=2), kappa1=0.02, diss=0.02, rk4 (2S), cfl 0.25"}
+    ctx.close()
+    return out
+
+
 def smr_measure(steps, warmup, shape=None, contract=1):
     """Steps of the refined binary-puncture mesh: zone-updates/s through
     the graph-captured step, and the multilevel ghost exchange alone."""
@@ -1059,6 +1097,8 @@ def main():
     }
     ctx.close()
     if world == 1 and not args.no_smr:
+        # the configuration's other workload on the same batched mesh
+        line["robust_stability"] = rs_measure(RS_STEPS, 3, contract=args.contract)
         # the refined binary-puncture mesh (the adaptive benchmark's 7 levels,
         # static): its own context after this one is released
         smr = smr_measure(SMR_STEPS, 3, contract=args.contract)
