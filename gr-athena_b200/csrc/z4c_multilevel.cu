@@ -88,6 +88,8 @@ __global__ void __launch_bounds__(kMlUnpackThreads)
 k_ml_unpack(MlPlan P, const double* __restrict__ src, double* __restrict__ dst, int nvar,
             int reg_nvar) {
   const int b = blockIdx.x, arr = blockIdx.y;  // arr: 0 fine, 1 coarse
+  // a coarse buffer that no prolongation reads is not filled
+  if (arr == 1 && !P.coarser[b]) return;
   __shared__ unsigned char mult[343];
   __shared__ int zs[344];
   extern __shared__ MlContrib sc[];  // this array's contributions
@@ -550,7 +552,7 @@ int ml_root_level(const int nroot[3]) {
 
 void ml_free(MlPlan& p) {
   for (void* q : {(void*)p.csrc, (void*)p.coarse, (void*)p.contrib, (void*)p.zstart, (void*)p.mult,
-                  (void*)p.pro, (void*)p.pro_blk})
+                  (void*)p.pro, (void*)p.pro_blk, (void*)p.coarser})
     if (q) cudaFree(q);
   for (auto& lv : p.bc)
     for (MlBc*& q : lv) {
@@ -772,6 +774,7 @@ int ml_build(const int nroot[3], const int nx[3], const int bcf[6], int nblocks,
   std::vector<MlBc> bcs[2][3];
   std::vector<RefGeom> pro;
   std::vector<int> pro_blk;
+  std::vector<unsigned char> coarser_of(nblocks, 0);
   for (int b = 0; b < nblocks; ++b) {
     const Loc l = B.loc(b);
     int need[6];
@@ -832,6 +835,7 @@ int ml_build(const int nroot[3], const int nx[3], const int bcf[6], int nblocks,
       pro_blk.push_back(b);
     }
     plan.ncoarser += coarser;
+    coarser_of[b] = coarser;
   }
   // every box, ghost write and extrapolation read stays inside its array
   auto inside = [&](const MlOp& o) {
@@ -929,7 +933,7 @@ int ml_build(const int nroot[3], const int nx[3], const int bcf[6], int nblocks,
   }
   if ((rc = upload(&plan.contrib, contrib)) || (rc = upload(&plan.zstart, zstart)) ||
       (rc = upload(&plan.mult, mults)) || (rc = upload(&plan.pro, pro)) ||
-      (rc = upload(&plan.pro_blk, pro_blk)))
+      (rc = upload(&plan.pro_blk, pro_blk)) || (rc = upload(&plan.coarser, coarser_of)))
     return fail_free(rc);
   plan.ncontrib = (int)contrib.size();
   for (int b = 0; b < nblocks; ++b)

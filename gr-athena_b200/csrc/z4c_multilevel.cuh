@@ -61,6 +61,8 @@ struct MlPlan {
   int* pro_blk = nullptr;
   int npro = 0;
   int ncoarser = 0;          // blocks with a coarser neighbour
+  unsigned char* coarser = nullptr;  // [block] 1 where a coarser neighbour is prolonged
+                                     // from the coarse buffer (no other reads it)
 };
 
 // Builds the plan for nblocks MeshBlocks of nx cells given in gid order by
