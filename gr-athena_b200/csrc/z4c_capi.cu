@@ -1524,13 +1524,33 @@ int jobs_issue(z4c_ctx* c, int j, double* host_out, double dt, int nsteps) {
 }
 
 // Issues the upload of job j into its input slot, after the evolution of
-// job j - 2 has copied that slot out.
-int jobs_upload(z4c_ctx* c, int j, const double* host_in) {
+// job j - 2 has copied that slot out.  partial: the steps run on the merged
+// grid, whose copy from the blocks reads, of a block not on a z face of the
+// mesh, only the vertex planes k = NG .. NG + nx; those blocks' planes go up
+// as one pitched copy (the other planes of the slot keep older values, which
+// nothing reads), the blocks on the z faces whole.
+int jobs_upload(z4c_ctx* c, int j, const double* host_in, bool partial) {
   JobPipe* J = c->jobs;
   const int s = j & 1;
   const size_t reg = sizeof(double) * (size_t)reg_elems(c, Z4C_REG_U);
   CUDA_TRY(cudaStreamWaitEvent(J->h2d, J->in_free[s], 0));
-  CUDA_TRY(cudaMemcpyAsync(J->in[s], host_in, reg, cudaMemcpyHostToDevice, J->h2d));
+  if (!partial) {
+    CUDA_TRY(cudaMemcpyAsync(J->in[s], host_in, reg, cudaMemcpyHostToDevice, J->h2d));
+  } else {
+    const Grid& g = c->g;
+    const size_t per = (size_t)Z4C_NVAR * g.nvol;             // values per block
+    const size_t layer = (size_t)g.nb[0] * g.nb[1];            // blocks per z layer
+    const size_t plane = (size_t)g.nn[0] * g.nn[1];            // values per vertex plane
+    const size_t top = layer * (g.nb[2] - 1);                  // first block of the top layer
+    CUDA_TRY(cudaMemcpyAsync(J->in[s], host_in, sizeof(double) * per * layer,
+                             cudaMemcpyHostToDevice, J->h2d));
+    const size_t off = per * layer + plane * NG;
+    CUDA_TRY(cudaMemcpy2DAsync(J->in[s] + off, sizeof(double) * g.nvol, host_in + off,
+                               sizeof(double) * g.nvol, sizeof(double) * plane * (g.nx[2] + 1),
+                               (top - layer) * Z4C_NVAR, cudaMemcpyHostToDevice, J->h2d));
+    CUDA_TRY(cudaMemcpyAsync(J->in[s] + per * top, host_in + per * top,
+                             sizeof(double) * per * layer, cudaMemcpyHostToDevice, J->h2d));
+  }
   CUDA_TRY(cudaEventRecord(J->in_ready[s], J->h2d));
   return Z4C_OK;
 }
@@ -1570,13 +1590,16 @@ int z4c_evolve_jobs(z4c_ctx* ctx, int njobs, const double* const* host_in,
   int rc = jobs_setup(ctx);
   if (rc) return rc;
   JobPipe* J = ctx->jobs;
+  // norms only, on a merged grid of three or more block layers in z: the
+  // planes the merged grid reads
+  const bool partial = !host_out && merge_eligible(ctx) && ctx->g.nb[2] > 2;
   // upload j + 1 is issued before evolution j, so that it runs beside it;
   // download j is issued right after it and runs beside evolution j + 1.
   // Job j reuses the slots of job j - 2, whose partials are summed first.
-  rc = jobs_upload(ctx, 0, host_in[0]);
+  rc = jobs_upload(ctx, 0, host_in[0], partial);
   int summed = 0;  // jobs whose history norms are taken
   for (int j = 0; j < njobs && rc == Z4C_OK; ++j) {
-    if (j + 1 < njobs) rc = jobs_upload(ctx, j + 1, host_in[j + 1]);
+    if (j + 1 < njobs) rc = jobs_upload(ctx, j + 1, host_in[j + 1], partial);
     if (rc == Z4C_OK && j >= 2) rc = jobs_hst(ctx, summed++, hst_out);
     if (rc == Z4C_OK) rc = jobs_issue(ctx, j, host_out ? host_out[j] : nullptr, dt, nsteps);
   }

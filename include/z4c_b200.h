@@ -345,7 +345,11 @@ int z4c_evolve(z4c_ctx *ctx, double dt, int nsteps, int with_constraints);
  * as z4c_evolve(ctx, dt, nsteps, 1) does, and the final u register is written
  * to host_out[j] and its history norms (those of z4c_hst_norms) to
  * hst_out[8*j .. 8*j+7] (hst_out may be NULL; host_out NULL downloads the
- * norms only, for runs that keep only the diagnostics).  The copies overlap the
+ * norms only, for runs that keep only the diagnostics: then, when the steps
+ * run on a merged grid (z4c_set_merged) of three or more block layers in z,
+ * only the vertex planes that grid reads are uploaded of the blocks off the
+ * mesh's z faces, about three quarters of the register on 8^3 blocks of
+ * 16^3, and u keeps older values in the others).  The copies overlap the
  * evolutions: job j+1 is uploaded and job j-1 downloaded while job j
  * evolves, on two copy streams of the library, through two input and two
  * output device registers allocated on the first call and held until

@@ -81,3 +81,35 @@ def test_jobs_match_sequential_calls(pinned):
     for j in range(len(states)):
         assert np.array_equal(hst[j], expect_hst[j]), f"job {j}, norms only"
     ctx.close()
+
+
+@pytest.mark.gpu
+def test_norms_only_jobs_on_three_block_layers():
+    """With the norms only and three or more block layers in z, the library
+    uploads only the vertex planes the merged grid reads of the blocks off
+    the z faces; the norms are still those of the separate calls, bit for
+    bit."""
+    import torch
+    from z4c_b200 import initial_data as ID
+    params = Z.default_params(diss=0.02, chi_div_floor=1e-5, damp_kappa1=0.02, shift_eta=2.0,
+                              r_max_con=1e300)
+    mesh = Z.Mesh((2, 2, 3), (16, 16, 16), (-4.0, -4.0, -6.0), (4.0, 4.0, 6.0), "outflow")
+    ctx = Z.Z4c(mesh, params, "rk4")
+    ctx.set_contract(True)
+    assert ctx.get_merged()
+    dt = 0.25 * float(np.min(ctx.dx()))
+    states = _states(mesh, params, ctx, ID)[:4]
+    expect_hst = []
+    for st in states:
+        ctx.upload(Z.REG_U, st)
+        ctx.evolve(dt, 2, with_constraints=True)
+        expect_hst.append(ctx.hst_norms())
+    inputs = []
+    for st in states:
+        t = torch.from_numpy(st.copy()).pin_memory()
+        inputs.append(t.numpy())
+    for _ in range(2):
+        hst = ctx.evolve_jobs(inputs, None, dt, 2)
+        for j in range(len(states)):
+            assert np.array_equal(hst[j], expect_hst[j]), f"job {j}"
+    ctx.close()
